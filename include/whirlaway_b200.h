@@ -1,0 +1,128 @@
+/* C ABI of the B200 Whirlaway prover path (Poseidon2-KoalaBear AIR).
+ *
+ * The reference exposes this path as a Rust library API (no FFI):
+ *   AirTable::prove   crates/air/src/prove.rs:49-66   (witness by value, proof into a
+ *                     caller-owned ProverState, read back via proof_data())
+ *   AirTable::verify  crates/air/src/verify.rs:55-69
+ *   AirSettings       crates/air/src/lib.rs:13-41 (+ WHIR_POW_BITS, lib.rs:9)
+ *   sumcheck::prove   crates/sumcheck/src/prove.rs:22-35
+ *   prove_poseidon2   src/examples/poseidon2.rs:85-200 (workload: constants, inputs, trace)
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Field values cross the ABI as canonical little-endian u32 (KoalaBear, p = 2^31 - 2^24 + 1).
+ *    Extension elements are 8 consecutive u32, lowest degree first.
+ *  - A proof is the reference's proof_data: a sequence of field elements.
+ *  - Every function returns a wl_status; nothing aborts across the boundary. The message of
+ *    the last failure on a context is available from wl_last_error.
+ *  - A context is single-owner: calls on one context must not overlap.
+ */
+#ifndef WHIRLAWAY_B200_H
+#define WHIRLAWAY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  WL_OK = 0,
+  WL_E_INVALID_ARG = 1,
+  WL_E_CUDA = 2,
+  WL_E_OOM = 3,
+  WL_E_BUFFER_TOO_SMALL = 4,
+  WL_E_INTERNAL = 5,
+  WL_E_BUDGET = 6,
+  /* verifier outcomes, mirroring AirVerifError (crates/air/src/verify.rs:26-34) */
+  WL_E_INVALID_PCS_COMMITMENT = 11,
+  WL_E_INVALID_PCS_OPENING = 12,
+  WL_E_FS = 13,
+  WL_E_SUMCHECK = 14,
+  WL_E_BOUNDARY = 15,
+  WL_E_SUM_MISMATCH = 16
+} wl_status;
+
+/* AirSettings (crates/air/src/lib.rs:13-41) with the folding factor
+ * ConstantFromSecondRound(fold_first, fold_rest) and WHIR_POW_BITS (lib.rs:9).
+ * Soundness is CapacityBound. Defaults: {128, 1, 7, 4, 4, 5, 16} (src/main.rs:13-24). */
+typedef struct {
+  int32_t security_bits;
+  int32_t log_inv_rate;
+  int32_t fold_first;
+  int32_t fold_rest;
+  int32_t univariate_skips;
+  int32_t rs_domain_initial_reduction;
+  int32_t whir_pow_bits;
+} wl_air_settings;
+
+typedef struct wl_ctx wl_ctx;
+typedef struct wl_witness wl_witness;
+
+/* Number of AIR columns (165) and of u32 in a constants blob (AIR round constants 148,
+ * Poseidon16 148, Poseidon24 215; each in the order beginning/initial, partial/terminal...). */
+int32_t wl_air_columns(void);
+int32_t wl_constants_len(void);
+void wl_default_settings(wl_air_settings* out);
+
+/* Context on one CUDA device. hbm_budget_bytes bounds the device memory a context admits
+ * for serving (0: no bound). */
+wl_status wl_ctx_create(int32_t device, uint64_t hbm_budget_bytes, wl_ctx** out);
+void wl_ctx_destroy(wl_ctx* ctx);
+const char* wl_last_error(const wl_ctx* ctx);
+
+/* Workload of src/examples/poseidon2.rs:104-151 on the host: one StdRng(seed 0) stream
+ * gives the AIR round constants, then 16 * 2^log_n inputs (row-major), then the Poseidon16
+ * and Poseidon24 constants. With input_seed >= 0 the constants come from that stream with
+ * the inputs skipped and the inputs from StdRng::seed_from_u64(input_seed).
+ * constants_out: wl_constants_len() u32; inputs_out: 16 << log_n u32 (may be NULL). */
+wl_status wl_generate_workload(int32_t log_n, int64_t input_seed, uint32_t* constants_out, uint32_t* inputs_out);
+
+/* Device-resident witness (165 columns of 2^log_n values, column-major).
+ * wl_witness_generate replaces generate_trace_rows(...).transpose() (poseidon2.rs:122-131)
+ * with a GPU trace generator; wl_witness_upload takes the reference's
+ * Vec<EvaluationsList<F>> layout from host memory. */
+wl_status wl_witness_upload(wl_ctx* ctx, int32_t log_n, const uint32_t* witness_colmajor, wl_witness** out);
+wl_status wl_witness_generate(wl_ctx* ctx, const uint32_t* constants, int32_t log_n, const uint32_t* inputs,
+                              wl_witness** out);
+wl_status wl_witness_download(wl_ctx* ctx, const wl_witness* w, uint32_t* witness_colmajor);
+void wl_witness_free(wl_ctx* ctx, wl_witness* w);
+
+/* Upper bound of the proof length (u32 elements) for log_n. */
+wl_status wl_proof_len_bound(const wl_air_settings* settings, int32_t log_n, size_t* out);
+
+/* AirTable::prove (crates/air/src/prove.rs:49-66) with the WHIR parameters, domain separator
+ * and challenger set up as in poseidon2.rs:155-163. The witness is a host buffer of 165
+ * columns of 2^log_n values (column-major). proof_out receives proof_data; *proof_len is its
+ * capacity on entry and the length on return (WL_E_BUFFER_TOO_SMALL if short).
+ * timings_ms (may be NULL): commit, zerocheck, inner, whir, total. */
+wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
+                   const uint32_t* witness_colmajor, uint32_t* proof_out, size_t* proof_len, double* timings_ms);
+/* Same, with a device-resident witness. */
+wl_status wl_prove_witness(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants,
+                           const wl_witness* w, uint32_t* proof_out, size_t* proof_len, double* timings_ms);
+
+/* Batch of independent proofs (each with its own witness and transcript), run back to back
+ * on the context's stream; proofs are written at proof_out + i * stride. */
+wl_status wl_prove_batch(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants, int32_t n,
+                         const wl_witness* const* witnesses, uint32_t* proof_out, size_t stride, size_t* proof_lens);
+
+/* sumcheck::prove (crates/sumcheck/src/prove.rs:22-35) for the zerocheck of
+ * eq(r, x) * (a(x) * b(x) - c(x)) with a univariate skip of `skips` variables; r is sampled
+ * from a fresh challenger on Poseidon16 (p16_constants: 148 u32), the three final folded
+ * values are appended. a, b, c: host arrays of 2^log_n. round_ms (may be NULL) receives
+ * log_n - skips + 1 per-round device times. */
+wl_status wl_sumcheck_abc_prove(wl_ctx* ctx, const uint32_t* p16_constants, int32_t log_n, int32_t skips,
+                                const uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t* proof_out,
+                                size_t* proof_len, float* round_ms);
+/* Same with device-resident inputs (canonical u32 device pointers, left unchanged). */
+wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constants, int32_t log_n, int32_t skips,
+                                       const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
+                                       uint32_t* proof_out, size_t* proof_len, float* round_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WHIRLAWAY_B200_H */

@@ -1,0 +1,260 @@
+"""B200 prover path for Whirlaway's Poseidon2-KoalaBear AIR.
+
+A thin Python face over the C ABI in include/whirlaway_b200.h, shaped like the reference's
+Rust API: ``AirSettings`` (crates/air/src/lib.rs:13-41), ``AirTable.prove`` /
+``AirTable.verify`` (crates/air/src/prove.rs:49-66, verify.rs:55-69) and the standalone
+``sumcheck`` prover (crates/sumcheck/src/prove.rs:22-35). All compute runs in the CUDA
+library built from ``csrc/``; there is no CPU fallback, and loading fails loudly when the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, astuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libwhirlaway_b200.so")
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_sizep = ctypes.POINTER(ctypes.c_size_t)
+
+STATUS = {
+    0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "OOM", 4: "BUFFER_TOO_SMALL", 5: "INTERNAL", 6: "BUDGET",
+    11: "INVALID_PCS_COMMITMENT", 12: "INVALID_PCS_OPENING", 13: "FS", 14: "SUMCHECK", 15: "BOUNDARY",
+    16: "SUM_MISMATCH",
+}
+
+
+class ProverError(RuntimeError):
+    """A non-OK wl_status from the library."""
+
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+
+
+class _Settings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "security_bits", "log_inv_rate", "fold_first", "fold_rest", "univariate_skips",
+        "rs_domain_initial_reduction", "whir_pow_bits")]
+
+
+@dataclass(frozen=True)
+class AirSettings:
+    """AirSettings with the reference defaults of src/main.rs:13-24."""
+    security_bits: int = 128
+    log_inv_rate: int = 1
+    fold_first: int = 7
+    fold_rest: int = 4
+    univariate_skips: int = 4
+    rs_domain_initial_reduction: int = 5
+    whir_pow_bits: int = 16
+
+    def _c(self) -> _Settings:
+        return _Settings(*astuple(self))
+
+    def as_array(self) -> np.ndarray:
+        return np.array(astuple(self), dtype=np.int32)
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"CUDA library not built: {path} (run whirlaway_b200.build.build())")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "wl_air_columns": (ctypes.c_int32, []),
+        "wl_constants_len": (ctypes.c_int32, []),
+        "wl_ctx_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]),
+        "wl_ctx_destroy": (None, [vp]),
+        "wl_last_error": (ctypes.c_char_p, [vp]),
+        "wl_generate_workload": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _u32p, _u32p]),
+        "wl_witness_upload": (ctypes.c_int, [vp, ctypes.c_int32, _u32p, ctypes.POINTER(vp)]),
+        "wl_witness_generate": (ctypes.c_int, [vp, _u32p, ctypes.c_int32, _u32p, ctypes.POINTER(vp)]),
+        "wl_witness_download": (ctypes.c_int, [vp, vp, _u32p]),
+        "wl_witness_free": (None, [vp, vp]),
+        "wl_proof_len_bound": (ctypes.c_int, [ctypes.POINTER(_Settings), ctypes.c_int32, _sizep]),
+        "wl_prove": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, _u32p, _sizep,
+                                    ctypes.POINTER(ctypes.c_double)]),
+        "wl_prove_witness": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, vp, _u32p, _sizep,
+                                            ctypes.POINTER(ctypes.c_double)]),
+        "wl_prove_batch": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
+                                          ctypes.POINTER(vp), _u32p, ctypes.c_size_t, _sizep]),
+        "wl_sumcheck_abc_prove": (ctypes.c_int, [vp, _u32p, ctypes.c_int32, ctypes.c_int32, _u32p, _u32p, _u32p,
+                                                 _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
+        "wl_sumcheck_abc_prove_device": (ctypes.c_int, [vp, _u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
+                                                        _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u32p)
+
+
+def air_columns() -> int:
+    return load_library().wl_air_columns()
+
+
+def constants_len() -> int:
+    return load_library().wl_constants_len()
+
+
+def generate_workload(log_n: int, input_seed: int = -1, with_inputs: bool = True):
+    """Constants blob and row-major inputs of src/examples/poseidon2.rs:104-151."""
+    lib = load_library()
+    consts = np.zeros(constants_len(), np.uint32)
+    inputs = np.zeros(16 << log_n, np.uint32) if with_inputs else None
+    st = lib.wl_generate_workload(log_n, input_seed, _ptr(consts), _ptr(inputs) if with_inputs else None)
+    if st:
+        raise ProverError(st, "generate_workload")
+    return consts, inputs
+
+
+class Context:
+    """One CUDA device; owns the stream, the twiddle table and pooled device memory."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        st = self._lib.wl_ctx_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if st:
+            raise ProverError(st, f"wl_ctx_create(device={device})")
+        self.handle = h
+
+    def check(self, st: int, what: str):
+        if st:
+            msg = self._lib.wl_last_error(self.handle).decode(errors="replace")
+            raise ProverError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.wl_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Witness:
+    """Device-resident witness: 165 columns of 2^log_n values."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p, log_n: int):
+        self.ctx, self.handle, self.log_n = ctx, handle, log_n
+
+    @classmethod
+    def upload(cls, ctx: Context, witness_colmajor: np.ndarray, log_n: int) -> "Witness":
+        w = np.ascontiguousarray(witness_colmajor, dtype=np.uint32).reshape(-1)
+        if w.size != air_columns() << log_n:
+            raise ValueError("witness must hold 165 columns of 2^log_n values")
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.wl_witness_upload(ctx.handle, log_n, _ptr(w), ctypes.byref(h)), "witness_upload")
+        return cls(ctx, h, log_n)
+
+    @classmethod
+    def generate(cls, ctx: Context, constants: np.ndarray, inputs: np.ndarray, log_n: int) -> "Witness":
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.wl_witness_generate(ctx.handle, _ptr(constants), log_n, _ptr(inputs), ctypes.byref(h)),
+                  "witness_generate")
+        return cls(ctx, h, log_n)
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(air_columns() << self.log_n, np.uint32)
+        self.ctx.check(self.ctx._lib.wl_witness_download(self.ctx.handle, self.handle, _ptr(out)), "download")
+        return out
+
+    def free(self):
+        if self.handle:
+            self.ctx._lib.wl_witness_free(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def proof_len_bound(settings: AirSettings, log_n: int) -> int:
+    n = ctypes.c_size_t()
+    st = load_library().wl_proof_len_bound(ctypes.byref(settings._c()), log_n, ctypes.byref(n))
+    if st:
+        raise ProverError(st, "proof_len_bound")
+    return n.value
+
+
+class AirTable:
+    """The Poseidon2-KoalaBear AIR table (crates/air/src/table.rs:15-99) bound to a device."""
+
+    def __init__(self, ctx: Context, constants: np.ndarray, log_n: int, settings: AirSettings = AirSettings()):
+        self.ctx, self.log_n, self.settings = ctx, log_n, settings
+        self.constants = np.ascontiguousarray(constants, dtype=np.uint32)
+        self.last_timings_ms = None
+
+    def _call(self, fn, *args):
+        cap = proof_len_bound(self.settings, self.log_n)
+        out = np.zeros(cap, np.uint32)
+        n = ctypes.c_size_t(cap)
+        tm = (ctypes.c_double * 5)()
+        self.ctx.check(fn(self.ctx.handle, ctypes.byref(self.settings._c()), _ptr(self.constants), *args, _ptr(out),
+                          ctypes.byref(n), tm), fn.__name__)
+        self.last_timings_ms = dict(zip(("commit", "zerocheck", "inner", "whir", "total"), list(tm)))
+        return out[: n.value].copy()
+
+    def prove(self, witness_colmajor: np.ndarray) -> np.ndarray:
+        """AirTable::prove with a host witness; returns proof_data (canonical u32)."""
+        w = np.ascontiguousarray(witness_colmajor, dtype=np.uint32).reshape(-1)
+        if w.size != air_columns() << self.log_n:
+            raise ValueError("witness must hold 165 columns of 2^log_n values")
+        return self._call(self.ctx._lib.wl_prove, self.log_n, _ptr(w))
+
+    def prove_witness(self, w: Witness) -> np.ndarray:
+        """AirTable::prove with a device-resident witness."""
+        if w.log_n != self.log_n:
+            raise ValueError("witness height does not match the table")
+        return self._call(self.ctx._lib.wl_prove_witness, w.handle)
+
+
+def sumcheck_abc_prove(ctx: Context, p16_constants: np.ndarray, log_n: int, skips: int, a, b, c, device=False):
+    """Zerocheck of eq(r, x) * (a*b - c) with a univariate skip; returns (proof, per-round ms)."""
+    lib = ctx._lib
+    cap = 8 * (3 * ((1 << skips) - 1) + 1 + 4 * (log_n - skips) + 3) + 64
+    out = np.zeros(cap, np.uint32)
+    n = ctypes.c_size_t(cap)
+    ms = (ctypes.c_float * (log_n - skips + 1))()
+    p16 = np.ascontiguousarray(p16_constants, dtype=np.uint32)
+    if device:
+        ptrs = [ctypes.c_void_p(int(t.data_ptr())) for t in (a, b, c)]
+        st = lib.wl_sumcheck_abc_prove_device(ctx.handle, _ptr(p16), log_n, skips, *ptrs, _ptr(out), ctypes.byref(n),
+                                              ms)
+    else:
+        arrs = [np.ascontiguousarray(t, dtype=np.uint32) for t in (a, b, c)]
+        st = lib.wl_sumcheck_abc_prove(ctx.handle, _ptr(p16), log_n, skips, *[_ptr(t) for t in arrs], _ptr(out),
+                                       ctypes.byref(n), ms)
+    ctx.check(st, "sumcheck_abc_prove")
+    return out[: n.value].copy(), list(ms)

@@ -1,0 +1,297 @@
+// C ABI (include/whirlaway_b200.h): argument checks, error mapping, witness handles.
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+
+#include "../../include/whirlaway_b200.h"
+#include "prover.h"
+
+struct wl_ctx {
+  std::unique_ptr<wl::Context> c;
+  std::string err;
+};
+struct wl_witness {
+  int log_n = 0;
+  wl::DBuf data;  // Montgomery form, 165 columns
+};
+
+namespace {
+
+wl_status fail(wl_ctx* ctx, wl_status st, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return st;
+}
+
+template <class F>
+wl_status guarded(wl_ctx* ctx, F&& f) {
+  try {
+    return f();
+  } catch (const wl::CudaError& e) {
+    cudaGetLastError();
+    wl_status st = (e.code == cudaErrorMemoryAllocation) ? WL_E_OOM : WL_E_CUDA;
+    return fail(ctx, st, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(ctx, WL_E_INVALID_ARG, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, WL_E_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ctx, WL_E_INTERNAL, e.what());
+  } catch (...) {
+    return fail(ctx, WL_E_INTERNAL, "unknown error");
+  }
+}
+
+bool settings_ok(const wl_air_settings* s, int log_n, std::string& why) {
+  if (!s) { why = "settings is NULL"; return false; }
+  if (s->security_bits < 1 || s->security_bits > 256) { why = "security_bits out of range"; return false; }
+  if (s->log_inv_rate < 1 || s->log_inv_rate > 4) { why = "log_inv_rate must be in [1, 4]"; return false; }
+  if (s->fold_first != 7 || s->fold_rest != 4) { why = "folding factors must be (7, 4)"; return false; }
+  if (s->univariate_skips < 1 || s->univariate_skips > 4) { why = "univariate_skips must be in [1, 4]"; return false; }
+  if (s->univariate_skips >= log_n) { why = "univariate_skips must be < log_n"; return false; }
+  if (s->rs_domain_initial_reduction < 1 || s->rs_domain_initial_reduction > s->fold_first) {
+    why = "rs_domain_initial_reduction out of range";
+    return false;
+  }
+  if (s->whir_pow_bits < 0 || s->whir_pow_bits > 30) { why = "whir_pow_bits out of range"; return false; }
+  if (log_n < 2 || log_n > 22) { why = "log_n must be in [2, 22]"; return false; }
+  return true;
+}
+
+wl::Settings to_settings(const wl_air_settings* s) {
+  wl::Settings r;
+  r.security_bits = s->security_bits;
+  r.log_inv_rate = s->log_inv_rate;
+  r.fold_first = s->fold_first;
+  r.fold_rest = s->fold_rest;
+  r.univariate_skips = s->univariate_skips;
+  r.rs_reduction = s->rs_domain_initial_reduction;
+  r.whir_pow_bits = s->whir_pow_bits;
+  return r;
+}
+
+wl::ProofJob make_job(const wl_air_settings* s, const uint32_t* constants, int log_n) {
+  wl::ProofJob job;
+  job.settings = to_settings(s);
+  job.log_n = log_n;
+  job.air = wl::air_consts_from(constants);
+  job.p16 = wl::perm_consts_from<16>(constants + wl::N_AIR_CONSTS);
+  job.p24 = wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS);
+  return job;
+}
+
+wl_status emit_proof(wl_ctx* ctx, const std::vector<uint32_t>& pr, uint32_t* out, size_t* len) {
+  if (*len < pr.size() || !out) {
+    size_t cap = *len;
+    *len = pr.size();
+    return fail(ctx, WL_E_BUFFER_TOO_SMALL,
+                "proof needs " + std::to_string(pr.size()) + " elements, buffer holds " + std::to_string(cap));
+  }
+  memcpy(out, pr.data(), pr.size() * sizeof(uint32_t));
+  *len = pr.size();
+  return WL_OK;
+}
+
+void store_timings(const wl::Timings& t, double* out) {
+  if (!out) return;
+  out[0] = t.commit_ms;
+  out[1] = t.zerocheck_ms;
+  out[2] = t.inner_ms;
+  out[3] = t.whir_ms;
+  out[4] = t.total_ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t wl_air_columns(void) { return wl::AIR_W; }
+int32_t wl_constants_len(void) { return wl::N_CONSTS; }
+void wl_default_settings(wl_air_settings* out) {
+  if (out) *out = wl_air_settings{128, 1, 7, 4, 4, 5, 16};
+}
+
+wl_status wl_ctx_create(int32_t device, uint64_t budget, wl_ctx** out) {
+  if (!out) return WL_E_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return WL_E_CUDA;
+  }
+  if (device < 0 || device >= count) return WL_E_INVALID_ARG;
+  try {
+    auto* c = new wl_ctx;
+    c->c = std::make_unique<wl::Context>(device, budget);
+    *out = c;
+    return WL_OK;
+  } catch (const wl::CudaError& e) {
+    cudaGetLastError();
+    return e.code == cudaErrorMemoryAllocation ? WL_E_OOM : WL_E_CUDA;
+  } catch (...) {
+    return WL_E_INTERNAL;
+  }
+}
+
+void wl_ctx_destroy(wl_ctx* ctx) { delete ctx; }
+
+const char* wl_last_error(const wl_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+wl_status wl_generate_workload(int32_t log_n, int64_t input_seed, uint32_t* constants_out, uint32_t* inputs_out) {
+  if (!constants_out || log_n < 0 || log_n > 24) return WL_E_INVALID_ARG;
+  wl::StdRng rng(0);
+  int ci = 0;
+  for (int i = 0; i < wl::N_AIR_CONSTS; i++) constants_out[ci++] = rng.random_f();
+  const size_t n = size_t(16) << log_n;
+  if (input_seed < 0) {
+    for (size_t i = 0; i < n; i++) {
+      uint32_t v = rng.random_f();
+      if (inputs_out) inputs_out[i] = v;
+    }
+  } else if (inputs_out) {
+    wl::StdRng r2((uint64_t)input_seed);
+    for (size_t i = 0; i < n; i++) inputs_out[i] = r2.random_f();
+  }
+  for (int i = 0; i < wl::N_P16_CONSTS + wl::N_P24_CONSTS; i++) constants_out[ci++] = rng.random_f();
+  return WL_OK;
+}
+
+wl_status wl_witness_upload(wl_ctx* ctx, int32_t log_n, const uint32_t* host, wl_witness** out) {
+  if (!ctx || !host || !out || log_n < 2 || log_n > 22) return fail(ctx, WL_E_INVALID_ARG, "bad witness arguments");
+  return guarded(ctx, [&] {
+    auto w = std::make_unique<wl_witness>();
+    w->log_n = log_n;
+    const size_t n = size_t(wl::AIR_W) << log_n;
+    w->data = wl::DBuf(n * 4, ctx->c->stream);
+    WL_CUDA(cudaMemcpyAsync(w->data.as<void>(), host, n * 4, cudaMemcpyHostToDevice, ctx->c->stream));
+    wl::launch_to_mont(w->data.as<uint32_t>(), n, ctx->c->stream);
+    WL_CUDA(cudaStreamSynchronize(ctx->c->stream));
+    *out = w.release();
+    return WL_OK;
+  });
+}
+
+wl_status wl_witness_generate(wl_ctx* ctx, const uint32_t* constants, int32_t log_n, const uint32_t* inputs,
+                              wl_witness** out) {
+  if (!ctx || !constants || !inputs || !out || log_n < 2 || log_n > 22)
+    return fail(ctx, WL_E_INVALID_ARG, "bad witness arguments");
+  return guarded(ctx, [&] {
+    auto w = std::make_unique<wl_witness>();
+    w->log_n = log_n;
+    cudaStream_t st = ctx->c->stream;
+    const size_t n_in = size_t(16) << log_n;
+    wl::DBuf din(n_in * 4, st);
+    WL_CUDA(cudaMemcpyAsync(din.as<void>(), inputs, n_in * 4, cudaMemcpyHostToDevice, st));
+    w->data = wl::DBuf((size_t(wl::AIR_W) << log_n) * 4, st);
+    wl::launch_trace_gen(din.as<uint32_t>(), wl::air_consts_from(constants), w->data.as<uint32_t>(), log_n, st);
+    WL_CUDA(cudaStreamSynchronize(st));
+    *out = w.release();
+    return WL_OK;
+  });
+}
+
+wl_status wl_witness_download(wl_ctx* ctx, const wl_witness* w, uint32_t* host) {
+  if (!ctx || !w || !host) return fail(ctx, WL_E_INVALID_ARG, "bad witness arguments");
+  return guarded(ctx, [&] {
+    const size_t n = size_t(wl::AIR_W) << w->log_n;
+    WL_CUDA(cudaMemcpyAsync(host, w->data.as<void>(), n * 4, cudaMemcpyDeviceToHost, ctx->c->stream));
+    WL_CUDA(cudaStreamSynchronize(ctx->c->stream));
+    for (size_t i = 0; i < n; i++) host[i] = kb::from_mont(host[i]);
+    return WL_OK;
+  });
+}
+
+void wl_witness_free(wl_ctx* ctx, wl_witness* w) {
+  if (!w) return;
+  if (ctx) cudaSetDevice(ctx->c->device);
+  delete w;
+}
+
+wl_status wl_proof_len_bound(const wl_air_settings* s, int32_t log_n, size_t* out) {
+  std::string why;
+  if (!out || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
+  try {
+    *out = wl::proof_len_bound(to_settings(s), log_n);
+    return WL_OK;
+  } catch (...) {
+    return WL_E_INVALID_ARG;
+  }
+}
+
+wl_status wl_prove_witness(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, const wl_witness* w,
+                           uint32_t* proof_out, size_t* proof_len, double* timings_ms) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  std::string why;
+  if (!w || !constants || !proof_len) return fail(ctx, WL_E_INVALID_ARG, "NULL argument");
+  if (!settings_ok(s, w->log_n, why)) return fail(ctx, WL_E_INVALID_ARG, why);
+  return guarded(ctx, [&] {
+    wl::ProofJob job = make_job(s, constants, w->log_n);
+    wl::Timings t;
+    std::vector<uint32_t> pr = wl::prove_air(*ctx->c, job, w->data.as<uint32_t>(), &t);
+    store_timings(t, timings_ms);
+    return emit_proof(ctx, pr, proof_out, proof_len);
+  });
+}
+
+wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, int32_t log_n,
+                   const uint32_t* witness, uint32_t* proof_out, size_t* proof_len, double* timings_ms) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  std::string why;
+  if (!settings_ok(s, log_n, why)) return fail(ctx, WL_E_INVALID_ARG, why);
+  wl_witness* w = nullptr;
+  wl_status st = wl_witness_upload(ctx, log_n, witness, &w);
+  if (st != WL_OK) return st;
+  st = wl_prove_witness(ctx, s, constants, w, proof_out, proof_len, timings_ms);
+  wl_witness_free(ctx, w);
+  return st;
+}
+
+wl_status wl_prove_batch(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, int32_t n,
+                         const wl_witness* const* ws, uint32_t* proof_out, size_t stride, size_t* proof_lens) {
+  if (!ctx || !ws || !proof_out || !proof_lens || n < 0) return fail(ctx, WL_E_INVALID_ARG, "bad batch arguments");
+  for (int i = 0; i < n; i++) {
+    size_t len = stride;
+    wl_status st = wl_prove_witness(ctx, s, constants, ws[i], proof_out + size_t(i) * stride, &len, nullptr);
+    proof_lens[i] = len;
+    if (st != WL_OK) return st;
+  }
+  return WL_OK;
+}
+
+static wl_status abc_common(wl_ctx* ctx, const uint32_t* p16c, int32_t log_n, int32_t skips, const uint32_t* a,
+                            const uint32_t* b, const uint32_t* c, bool device, uint32_t* proof_out, size_t* proof_len,
+                            float* round_ms) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  if (!p16c || !a || !b || !c || !proof_len || log_n < 2 || log_n > 26 || skips < 1 || skips > 4 || skips >= log_n)
+    return fail(ctx, WL_E_INVALID_ARG, "bad sumcheck arguments");
+  return guarded(ctx, [&] {
+    cudaStream_t st = ctx->c->stream;
+    const size_t N = size_t(1) << log_n;
+    wl::DBuf d(N * 12, st);
+    uint32_t* da = d.as<uint32_t>();
+    auto kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    WL_CUDA(cudaMemcpyAsync(da, a, N * 4, kind, st));
+    WL_CUDA(cudaMemcpyAsync(da + N, b, N * 4, kind, st));
+    WL_CUDA(cudaMemcpyAsync(da + 2 * N, c, N * 4, kind, st));
+    wl::launch_to_mont(da, 3 * N, st);
+    kb::P16Consts p16 = wl::perm_consts_from<16>(p16c);
+    std::vector<float> ms;
+    std::vector<uint32_t> pr = wl::prove_abc(*ctx->c, p16, log_n, skips, da, da + N, da + 2 * N, &ms);
+    if (round_ms) std::copy(ms.begin(), ms.end(), round_ms);
+    return emit_proof(ctx, pr, proof_out, proof_len);
+  });
+}
+
+wl_status wl_sumcheck_abc_prove(wl_ctx* ctx, const uint32_t* p16c, int32_t log_n, int32_t skips, const uint32_t* a,
+                                const uint32_t* b, const uint32_t* c, uint32_t* proof_out, size_t* proof_len,
+                                float* round_ms) {
+  return abc_common(ctx, p16c, log_n, skips, a, b, c, false, proof_out, proof_len, round_ms);
+}
+
+wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16c, int32_t log_n, int32_t skips,
+                                       const uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t* proof_out,
+                                       size_t* proof_len, float* round_ms) {
+  return abc_common(ctx, p16c, log_n, skips, a, b, c, true, proof_out, proof_len, round_ms);
+}
+
+}  // extern "C"

@@ -1,0 +1,507 @@
+// Sumcheck kernels: the AIR zerocheck (univariate-skip first round over the base field,
+// later rounds over the extension field), the folds between rounds, the inner-phase
+// helpers and the standalone a*b - c zerocheck. They compute the sums of
+// crates/sumcheck/src/prove.rs:97-335 (sc_round / compute_over_hypercube) and the folds of
+// crates/utils/src/multilinear.rs; the transcript work between rounds stays on the host.
+//
+// Column conventions: the witness is column-major (column c at wit + c * 2^n, Montgomery).
+// "up" columns replace the last row by the one before it and "down" columns shift by one
+// row and repeat the last (crates/air/src/utils.rs:140-160); neither is materialised.
+// Folded columns are extension-field arrays, column c at cols + c * len.
+#include "kernels.h"
+
+namespace wl {
+
+namespace {
+using namespace kb;
+
+__device__ __forceinline__ size_t up_row(size_t i, size_t N) { return i == N - 1 ? N - 2 : i; }
+__device__ __forceinline__ size_t down_row(size_t i, size_t N) { return i == N - 1 ? N - 1 : i + 1; }
+
+// ------------------------------------------------------------------ eq tables
+// out[x] = prod_i (x_i ? r_i : 1 - r_i), x_1 = most significant bit of x.
+__global__ void k_eq_table(const ef* __restrict__ pt, int nvars, ef* __restrict__ out) {
+  __shared__ ef hi_val;
+  const int nlo = nvars < 10 ? nvars : 10;
+  const int nhi = nvars - nlo;
+  const size_t xhi = blockIdx.x;
+  if (threadIdx.x == 0) {
+    ef h = ef_one();
+    for (int i = 0; i < nhi; i++) {
+      bool bit = (xhi >> (nhi - 1 - i)) & 1;
+      h = ef_mul(h, bit ? pt[i] : ef_sub(ef_one(), pt[i]));
+    }
+    hi_val = h;
+  }
+  __syncthreads();
+  const uint32_t xlo = threadIdx.x;
+  if (xlo >= (1u << nlo)) return;
+  ef v = hi_val;
+  for (int i = 0; i < nlo; i++) {
+    bool bit = (xlo >> (nlo - 1 - i)) & 1;
+    const ef& r = pt[nhi + i];
+    v = ef_mul(v, bit ? r : ef_sub(ef_one(), r));
+  }
+  out[(xhi << nlo) + xlo] = v;
+}
+
+__global__ void k_eq_table_f(const uint32_t* __restrict__ pts, int npts, int nvars, uint32_t* __restrict__ out) {
+  size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  size_t n = size_t(npts) << nvars;
+  if (i >= n) return;
+  size_t p = i >> nvars;
+  uint32_t x = uint32_t(i & ((size_t(1) << nvars) - 1));
+  uint32_t v = R_MOD_P;
+  for (int k = 0; k < nvars; k++) {
+    uint32_t r = pts[p * nvars + k];
+    bool bit = (x >> (nvars - 1 - k)) & 1;
+    v = mul(v, bit ? r : sub(R_MOD_P, r));
+  }
+  out[i] = v;
+}
+
+__global__ void k_reduce_partials(const ef* __restrict__ partial, int nblk, int k, ef* __restrict__ out) {
+  __shared__ ef scratch[32];
+  const int j = blockIdx.x;
+  ef acc = ef_zero();
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc = ef_add(acc, partial[size_t(b) * k + j]);
+  acc = block_reduce_ef(acc, scratch);
+  if (threadIdx.x == 0) out[j] = acc;
+}
+
+// ------------------------------------------------------------------ AIR zerocheck
+constexpr int ZC0_X = 32, ZC0_Z = 10;
+
+// Thread (x, z): the up columns are extended from their values at j * 2^(n-k) + x,
+// j < 2^k, to the point z by the Lagrange weights lw[z]; the batched constraint over
+// those values is weighted by eq[x]. One warp holds 32 consecutive x for one z.
+__global__ void __launch_bounds__(ZC0_X * ZC0_Z) k_zc0_eval(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                            int nz, const uint32_t* __restrict__ lw,
+                                                            const ef* __restrict__ eq,
+                                                            const ef* __restrict__ alphas_g,
+                                                            const __grid_constant__ AirConsts K,
+                                                            ef* __restrict__ partial) {
+  __shared__ ef alphas[AIR_NC];
+  __shared__ uint32_t w_s[ZC0_Z * 16];
+  const int tid = threadIdx.y * ZC0_X + threadIdx.x;
+  for (int i = tid; i < AIR_NC; i += ZC0_X * ZC0_Z) alphas[i] = alphas_g[i];
+  const int zi = blockIdx.y * ZC0_Z + threadIdx.y;
+  const int nsk = 1 << k;
+  for (int i = tid; i < ZC0_Z * nsk; i += ZC0_X * ZC0_Z) {
+    int zz = blockIdx.y * ZC0_Z + i / nsk;
+    w_s[i] = zz < nz ? lw[zz * nsk + i % nsk] : 0u;
+  }
+  __syncthreads();
+  const size_t N = size_t(1) << log_n;
+  const size_t S = N >> k;
+  const size_t x = size_t(blockIdx.x) * ZC0_X + threadIdx.x;
+  const uint32_t* wz = w_s + threadIdx.y * nsk;
+  const bool active = zi < nz && x < S;
+  auto get = [&](int c) -> uint32_t {
+    const uint32_t* col = wit + size_t(c) * N;
+    uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (j < nsk) {
+        size_t row = up_row(size_t(j) * S + x, N);
+        uint64_t t = wmul(wz[j], col[row]);
+        if ((j & 3) == 0) s0 += t;
+        else if ((j & 3) == 1) s1 += t;
+        else if ((j & 3) == 2) s2 += t;
+        else s3 += t;
+      }
+    }
+    return add(add(redc(s0), redc(s1)), add(redc(s2), redc(s3)));
+  };
+  EfMacF m;
+  m.init();
+  ef res = ef_zero();
+  if (active) {
+    air_eval_f(
+        K, get, [&](uint32_t h, int i) { m.mac(alphas[i], h); }, [&]() { m.flush(); });
+    res = ef_mul(m.acc, eq[x]);
+  }
+  res = warp_reduce_ef(res);
+  if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
+}
+
+// out[c * S + x] = sum_j sel[j] * up_c[j * S + x]
+__global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ sel_g,
+                           ef* __restrict__ out) {
+  __shared__ ef sel[16];
+  const int nsk = 1 << k;
+  if (threadIdx.x < nsk) sel[threadIdx.x] = sel_g[threadIdx.x];
+  __syncthreads();
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (x >= S) return;
+  const uint32_t* col = wit + size_t(c) * N;
+  EfMacF m;
+  m.init();
+  for (int j = 0; j < nsk; j++) {
+    m.mac(sel[j], col[up_row(size_t(j) * S + x, N)]);
+    if ((j & 3) == 3 || j == nsk - 1) m.flush();
+  }
+  out[size_t(c) * S + x] = m.acc;
+}
+
+constexpr int ZCE_X = 32;
+
+// Rounds >= 1: thread (x, z) with z in {0, 2, 3} (index zi = 0, 1, 2).
+__global__ void __launch_bounds__(ZCE_X * 3) k_zc_eval_ef(const ef* __restrict__ cols, int m,
+                                                          const ef* __restrict__ eq,
+                                                          const ef* __restrict__ alphas_g,
+                                                          const __grid_constant__ AirConsts K,
+                                                          ef* __restrict__ partial) {
+  __shared__ ef alphas[AIR_NC];
+  const int tid = threadIdx.y * ZCE_X + threadIdx.x;
+  for (int i = tid; i < AIR_NC; i += ZCE_X * 3) alphas[i] = alphas_g[i];
+  __syncthreads();
+  const size_t len = size_t(1) << m, half = len >> 1;
+  const size_t x = size_t(blockIdx.x) * ZCE_X + threadIdx.x;
+  const int zi = threadIdx.y;
+  ef res = ef_zero();
+  if (x < half) {
+    auto get = [&](int c) -> ef {
+      const ef lo = cols[size_t(c) * len + x];
+      const ef hi = cols[size_t(c) * len + half + x];
+      if (zi == 0) return lo;
+      ef d = ef_sub(hi, lo);
+      ef v = ef_add(hi, d);             // z = 2: 2 hi - lo
+      return zi == 1 ? v : ef_add(v, d);  // z = 3: 3 hi - 2 lo
+    };
+    res = ef_mul(air_eval_ef(K, alphas, get), eq[x]);
+  }
+  res = warp_reduce_ef(res);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 3 + zi] = res;
+}
+
+__global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, const ef* __restrict__ r) {
+  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (x >= half) return;
+  const ef* src = in + size_t(c) * 2 * half;
+  out[size_t(c) * half + x] = ef_lerp(src[x], src[half + x], *r);
+}
+
+// partial[(c * 2^k + j)] = sum_x eqt[x] * up_c[j S + x] (and the same for down)
+__global__ void k_inner_sums(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ eqt,
+                             ef* __restrict__ pu, ef* __restrict__ pd) {
+  __shared__ ef scratch[32];
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const int c = blockIdx.x, j = blockIdx.y;
+  const uint32_t* col = wit + size_t(c) * N;
+  EfMacF mu, md;
+  mu.init();
+  md.init();
+  int cnt = 0;
+  for (size_t x = threadIdx.x; x < S; x += blockDim.x) {
+    size_t i = size_t(j) * S + x;
+    const ef e = eqt[x];
+    mu.mac(e, col[up_row(i, N)]);
+    md.mac(e, col[down_row(i, N)]);
+    if (++cnt == 4) { mu.flush(); md.flush(); cnt = 0; }
+  }
+  mu.flush();
+  md.flush();
+  ef u = block_reduce_ef(mu.acc, scratch);
+  ef d = block_reduce_ef(md.acc, scratch);
+  if (threadIdx.x == 0) {
+    pu[size_t(c) * gridDim.y + j] = u;
+    pd[size_t(c) * gridDim.y + j] = d;
+  }
+}
+
+// out[c] = sum_j sel[j] * partial[c * nsk + j]
+__global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int ncols,
+                              ef* __restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  ef acc = ef_zero();
+  for (int j = 0; j < nsk; j++) acc = ef_add(acc, ef_mul(sel[j], partial[size_t(c) * nsk + j]));
+  out[c] = acc;
+}
+
+// ------------------------------------------------------------------ inner phase
+__global__ void k_batch_cols(const uint32_t* __restrict__ wit, int log_n, const ef* __restrict__ eqc_g,
+                             ef* __restrict__ out) {
+  __shared__ ef eqc[AIR_W];
+  for (int i = threadIdx.x; i < AIR_W; i += blockDim.x) eqc[i] = eqc_g[i];
+  __syncthreads();
+  const size_t N = size_t(1) << log_n;
+  const size_t row = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (row >= N) return;
+  EfMacF m;
+  m.init();
+  for (int c = 0; c < AIR_W; c++) {
+    m.mac(eqc[c], wit[size_t(c) * N + row]);
+    if ((c & 3) == 3) m.flush();
+  }
+  m.flush();
+  out[row] = m.acc;
+}
+
+constexpr int SUB_THREADS = 256, SUB_PER_THREAD = 16;
+
+// partial[(chunk * 2^k + j) * 2 + {0,1}] = sum_x eqt[x] * B[up/down(j S + x)] over the chunk's x
+__global__ void k_sub_evals(const ef* __restrict__ B, int log_n, int k, const ef* __restrict__ eqt,
+                            ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const int j = blockIdx.y;
+  const size_t chunk = blockIdx.x;
+  ef u = ef_zero(), d = ef_zero();
+  for (int q = 0; q < SUB_PER_THREAD; q++) {
+    size_t x = (chunk * SUB_PER_THREAD + q) * SUB_THREADS + threadIdx.x;
+    if (x < S) {
+      size_t i = size_t(j) * S + x;
+      const ef e = eqt[x];
+      u = ef_add(u, ef_mul(e, B[up_row(i, N)]));
+      d = ef_add(d, ef_mul(e, B[down_row(i, N)]));
+    }
+  }
+  u = block_reduce_ef(u, scratch);
+  d = block_reduce_ef(d, scratch);
+  if (threadIdx.x == 0) {
+    size_t o = (chunk * gridDim.y + j) * 2;
+    partial[o] = u;
+    partial[o + 1] = d;
+  }
+}
+
+// A[y] = up-shift matrix row + alpha2 * down-shift matrix row, folded at the point whose
+// eq table is e (crates/air/src/uni_skip_utils.rs:5-34).
+__global__ void k_inner_mle(const ef* __restrict__ e, int log_n, const ef* __restrict__ alpha2, ef* __restrict__ out) {
+  const size_t N = size_t(1) << log_n;
+  const size_t y = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (y >= N) return;
+  const ef last = e[N - 1];
+  ef mu = e[y];
+  if (y == N - 2) mu = ef_add(mu, last);
+  if (y == N - 1) mu = ef_zero();
+  ef md = y >= 1 ? e[y - 1] : ef_zero();
+  if (y == N - 1) md = ef_add(md, last);
+  out[y] = ef_add(mu, ef_mul(*alpha2, md));
+}
+
+constexpr int PROD_THREADS = 256, PROD_PER_THREAD = 8;
+
+__global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, size_t half, ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  ef s0 = ef_zero(), s2 = ef_zero();
+  for (int q = 0; q < PROD_PER_THREAD; q++) {
+    size_t x = (size_t(blockIdx.x) * PROD_PER_THREAD + q) * PROD_THREADS + threadIdx.x;
+    if (x < half) {
+      ef al = a[x], ah = a[x + half], bl = b[x], bh = b[x + half];
+      s0 = ef_add(s0, ef_mul(al, bl));
+      ef a2 = ef_sub(ef_add(ah, ah), al), b2 = ef_sub(ef_add(bh, bh), bl);
+      s2 = ef_add(s2, ef_mul(a2, b2));
+    }
+  }
+  s0 = block_reduce_ef(s0, scratch);
+  s2 = block_reduce_ef(s2, scratch);
+  if (threadIdx.x == 0) {
+    partial[size_t(blockIdx.x) * 2] = s0;
+    partial[size_t(blockIdx.x) * 2 + 1] = s2;
+  }
+}
+
+__global__ void k_fold2(const ef* __restrict__ a, const ef* __restrict__ b, ef* __restrict__ oa, ef* __restrict__ ob,
+                        size_t half, const ef* __restrict__ r) {
+  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= half) return;
+  const ef rr = *r;
+  oa[x] = ef_lerp(a[x], a[x + half], rr);
+  ob[x] = ef_lerp(b[x], b[x + half], rr);
+}
+
+// ------------------------------------------------------------------ a*b - c
+constexpr int ABC_X = 32;
+
+__global__ void k_abc0_eval(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                            const uint32_t* __restrict__ c, int log_n, int k, int nz, const uint32_t* __restrict__ lw,
+                            const ef* __restrict__ eq, ef* __restrict__ partial) {
+  __shared__ uint32_t w_s[32 * 16];
+  const int nsk = 1 << k;
+  const int tid = threadIdx.y * ABC_X + threadIdx.x;
+  for (int i = tid; i < nz * nsk; i += ABC_X * blockDim.y) w_s[i] = lw[i];
+  __syncthreads();
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const size_t x = size_t(blockIdx.x) * ABC_X + threadIdx.x;
+  const int zi = threadIdx.y;
+  ef res = ef_zero();
+  if (x < S && zi < nz) {
+    const uint32_t* wz = w_s + zi * nsk;
+    uint64_t sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0}, sc[4] = {0, 0, 0, 0};
+    for (int j = 0; j < nsk; j++) {
+      size_t i = size_t(j) * S + x;
+      sa[j & 3] += wmul(wz[j], a[i]);
+      sb[j & 3] += wmul(wz[j], b[i]);
+      sc[j & 3] += wmul(wz[j], c[i]);
+    }
+    auto fin = [](uint64_t* s) { return add(add(redc(s[0]), redc(s[1])), add(redc(s[2]), redc(s[3]))); };
+    uint32_t v = sub(mul(fin(sa), fin(sb)), fin(sc));
+    res = ef_mul_f(eq[x], v);
+  }
+  res = warp_reduce_ef(res);
+  if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
+}
+
+__global__ void k_abc0_fold(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                            const uint32_t* __restrict__ c, int log_n, int k, const ef* __restrict__ sel_g,
+                            ef* __restrict__ out) {
+  __shared__ ef sel[16];
+  const int nsk = 1 << k;
+  if (threadIdx.x < nsk) sel[threadIdx.x] = sel_g[threadIdx.x];
+  __syncthreads();
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= S) return;
+  const uint32_t* src = blockIdx.y == 0 ? a : blockIdx.y == 1 ? b : c;
+  EfMacF m;
+  m.init();
+  for (int j = 0; j < nsk; j++) {
+    m.mac(sel[j], src[size_t(j) * S + x]);
+    if ((j & 3) == 3 || j == nsk - 1) m.flush();
+  }
+  out[size_t(blockIdx.y) * S + x] = m.acc;
+}
+
+__global__ void k_abc_eval_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq, ef* __restrict__ partial) {
+  const size_t len = size_t(1) << m, half = len >> 1;
+  const size_t x = size_t(blockIdx.x) * 32 + threadIdx.x;
+  const int zi = threadIdx.y;  // z = 0 or 2
+  ef res = ef_zero();
+  if (x < half) {
+    ef v[3];
+    for (int q = 0; q < 3; q++) {
+      ef lo = cols[q * len + x], hi = cols[q * len + half + x];
+      v[q] = zi == 0 ? lo : ef_sub(ef_add(hi, hi), lo);
+    }
+    res = ef_mul(ef_sub(ef_mul(v[0], v[1]), v[2]), eq[x]);
+  }
+  res = warp_reduce_ef(res);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 2 + zi] = res;
+}
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+void launch_eq_table(const ef* point, int nvars, ef* out, cudaStream_t s) {
+  int nlo = nvars < 10 ? nvars : 10;
+  k_eq_table<<<(unsigned)(size_t(1) << (nvars - nlo)), 1u << nlo, 0, s>>>(point, nvars, out);
+  WL_LAUNCH_CHECK();
+}
+void launch_eq_table_f(const uint32_t* pts, int npts, int nvars, uint32_t* out, cudaStream_t s) {
+  size_t n = size_t(npts) << nvars;
+  if (!n) return;
+  k_eq_table_f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pts, npts, nvars, out);
+  WL_LAUNCH_CHECK();
+}
+void launch_reduce_partials(const ef* partial, int nblk, int k, ef* out, cudaStream_t s) {
+  k_reduce_partials<<<k, 256, 0, s>>>(partial, nblk, k, out);
+  WL_LAUNCH_CHECK();
+}
+
+int zc0_blocks(int log_n, int k) {
+  size_t S = size_t(1) << (log_n - k);
+  return (int)((S + ZC0_X - 1) / ZC0_X);
+}
+void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
+                     const ef* alphas, const AirConsts& K, ef* partial, cudaStream_t s) {
+  dim3 grid(zc0_blocks(log_n, k), (nz + ZC0_Z - 1) / ZC0_Z), block(ZC0_X, ZC0_Z);
+  k_zc0_eval<<<grid, block, 0, s>>>(wit, log_n, k, nz, lw, eq, alphas, K, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {
+  size_t S = size_t(1) << (log_n - k);
+  dim3 grid((unsigned)((S + 255) / 256), AIR_W);
+  k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
+  WL_LAUNCH_CHECK();
+}
+int zc_ef_blocks(int m) {
+  size_t half = size_t(1) << (m - 1);
+  return (int)((half + ZCE_X - 1) / ZCE_X);
+}
+void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const AirConsts& K, ef* partial,
+                       cudaStream_t s) {
+  k_zc_eval_ef<<<zc_ef_blocks(m), dim3(ZCE_X, 3), 0, s>>>(cols, m, eq, alphas, K, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s) {
+  dim3 grid((unsigned)((half + 255) / 256), ncols);
+  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, r);
+  WL_LAUNCH_CHECK();
+}
+void launch_inner_sums(const uint32_t* wit, int log_n, int k, const ef* eqt, const ef* sel, ef* out_up,
+                       ef* out_down, cudaStream_t s) {
+  // out_up / out_down first hold the (column, j) partials (AIR_W * 2^k each) and then,
+  // at their start, the AIR_W combined values; the partials live past that prefix.
+  const int nsk = 1 << k;
+  ef* pu = out_up + AIR_W;
+  ef* pd = out_down + AIR_W;
+  k_inner_sums<<<dim3(AIR_W, nsk), 256, 0, s>>>(wit, log_n, k, eqt, pu, pd);
+  WL_LAUNCH_CHECK();
+  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pu, sel, nsk, AIR_W, out_up);
+  WL_LAUNCH_CHECK();
+  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pd, sel, nsk, AIR_W, out_down);
+  WL_LAUNCH_CHECK();
+}
+
+void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s) {
+  size_t N = size_t(1) << log_n;
+  k_batch_cols<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(wit, log_n, eqc, out);
+  WL_LAUNCH_CHECK();
+}
+int sub_eval_blocks(int log_n, int k) {
+  size_t S = size_t(1) << (log_n - k);
+  size_t per = size_t(SUB_THREADS) * SUB_PER_THREAD;
+  return (int)((S + per - 1) / per);
+}
+void launch_sub_evals(const ef* B, int log_n, int k, const ef* alpha2, const ef* eqt, ef* partial, cudaStream_t s) {
+  (void)alpha2;
+  dim3 grid(sub_eval_blocks(log_n, k), 1u << k);
+  k_sub_evals<<<grid, SUB_THREADS, 0, s>>>(B, log_n, k, eqt, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_inner_mle(const ef* e, int log_n, const ef* alpha2, ef* out, cudaStream_t s) {
+  size_t N = size_t(1) << log_n;
+  k_inner_mle<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(e, log_n, alpha2, out);
+  WL_LAUNCH_CHECK();
+}
+int prod_blocks(size_t half) {
+  size_t per = size_t(PROD_THREADS) * PROD_PER_THREAD;
+  return (int)((half + per - 1) / per);
+}
+void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s) {
+  k_prod_eval<<<prod_blocks(half), PROD_THREADS, 0, s>>>(a, b, half, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s) {
+  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, r);
+  WL_LAUNCH_CHECK();
+}
+
+int abc0_blocks(int log_n, int k) {
+  size_t S = size_t(1) << (log_n - k);
+  return (int)((S + ABC_X - 1) / ABC_X);
+}
+void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
+                      const uint32_t* lw, const ef* eq, ef* partial, cudaStream_t s) {
+  if (nz > 32 || k > 4) throw std::runtime_error("abc round 0: too many points");
+  k_abc0_eval<<<abc0_blocks(log_n, k), dim3(ABC_X, nz), 0, s>>>(a, b, c, log_n, k, nz, lw, eq, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_abc0_fold(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, const ef* sel,
+                      ef* out, cudaStream_t s) {
+  size_t S = size_t(1) << (log_n - k);
+  k_abc0_fold<<<dim3((unsigned)((S + 255) / 256), 3), 256, 0, s>>>(a, b, c, log_n, k, sel, out);
+  WL_LAUNCH_CHECK();
+}
+void launch_abc_eval_ef(const ef* cols, int m, const ef* eq, ef* partial, cudaStream_t s) {
+  size_t half = size_t(1) << (m - 1);
+  k_abc_eval_ef<<<(unsigned)((half + 31) / 32), dim3(32, 2), 0, s>>>(cols, m, eq, partial);
+  WL_LAUNCH_CHECK();
+}
+
+}  // namespace wl

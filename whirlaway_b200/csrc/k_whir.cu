@@ -1,0 +1,218 @@
+// WHIR kernels (the bulk work of whir-p3's Prover::prove, reached from
+// crates/air/src/prove.rs:216-225): partial evaluations of the committed base-field table
+// for the initial constraints, the fold of that table after the first sumcheck block,
+// accumulation of equality-weight terms for OOD / STIR constraints, the weighted sumcheck
+// rounds and OOD answers of extension-field polynomials.
+//
+// Equality polynomials over m variables are factored as eq(pt, v) = hi(v_hi) * lo(v_lo)
+// with v_lo the low ll bits, so a table of 2^m entries costs 2^lh + 2^ll to build.
+#include "kernels.h"
+
+namespace wl {
+
+namespace {
+using namespace kb;
+
+constexpr int MPB_SPLIT = 4;  // v_hi groups per column block
+
+// out[(j * 2^lu + u) * MPB_SPLIT + g] = sum over v_hi in group g, v_lo of
+//   T[u * 2^lv + v] * hi_j[v_hi] * lo_j[v_lo]
+template <int J>
+__global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len, int lu, int lh, int ll,
+                                   const ef* __restrict__ hi, const ef* __restrict__ lo, ef* __restrict__ out) {
+  __shared__ ef scratch[32];
+  const int u = blockIdx.x, g = blockIdx.y;
+  const size_t lv = size_t(lh + ll);
+  const size_t base = size_t(u) << lv;
+  const uint32_t nlo = 1u << ll;
+  const uint32_t nhi = 1u << lh;
+  const uint32_t per = (nhi + MPB_SPLIT - 1) / MPB_SPLIT;
+  const uint32_t h0 = g * per, h1 = min(nhi, h0 + per);
+  ef res[J];
+  for (int j = 0; j < J; j++) res[j] = ef_zero();
+  if (base < t_len) {
+    for (uint32_t vlo = threadIdx.x; vlo < nlo; vlo += blockDim.x) {
+      EfMacF m[J];
+      for (int j = 0; j < J; j++) m[j].init();
+      int cnt = 0;
+      for (uint32_t vh = h0; vh < h1; vh++) {
+        size_t idx = base + (size_t(vh) << ll) + vlo;
+        uint32_t t = idx < t_len ? T[idx] : 0u;
+#pragma unroll
+        for (int j = 0; j < J; j++) m[j].mac(hi[size_t(j) * nhi + vh], t);
+        if (++cnt == 4) {
+#pragma unroll
+          for (int j = 0; j < J; j++) m[j].flush();
+          cnt = 0;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < J; j++) {
+        m[j].flush();
+        res[j] = ef_add(res[j], ef_mul(m[j].acc, lo[size_t(j) * nlo + vlo]));
+      }
+    }
+  }
+  for (int j = 0; j < J; j++) {
+    ef r = block_reduce_ef(res[j], scratch);
+    if (threadIdx.x == 0) out[((size_t(j) << lu) + u) * MPB_SPLIT + g] = r;
+  }
+}
+
+__global__ void k_sum_split(const ef* __restrict__ in, size_t n, ef* __restrict__ out) {
+  size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ef acc = ef_zero();
+  for (int g = 0; g < MPB_SPLIT; g++) acc = ef_add(acc, in[i * MPB_SPLIT + g]);
+  out[i] = acc;
+}
+
+// out[v] = sum_u eqr[u] * T[u * 2^lv + v]
+__global__ void k_whir_fold_T(const uint32_t* __restrict__ T, size_t t_len, int lu, int lv,
+                              const ef* __restrict__ eqr_g, ef* __restrict__ out) {
+  extern __shared__ ef eqr[];
+  const int nu = 1 << lu;
+  for (int i = threadIdx.x; i < nu; i += blockDim.x) eqr[i] = eqr_g[i];
+  __syncthreads();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= (size_t(1) << lv)) return;
+  EfMacF m;
+  m.init();
+  int cnt = 0;
+  for (int u = 0; u < nu; u++) {
+    size_t idx = (size_t(u) << lv) + v;
+    if (idx >= t_len) break;
+    m.mac(eqr[u], T[idx]);
+    if (++cnt == 4) { m.flush(); cnt = 0; }
+  }
+  m.flush();
+  out[v] = m.acc;
+}
+
+// w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (base-field points)
+__global__ void k_add_eq_terms_f(ef* __restrict__ w, int lh, int ll, int npts, const uint32_t* __restrict__ hi,
+                                 const uint32_t* __restrict__ lo, const ef* __restrict__ coefs_g) {
+  extern __shared__ ef coefs[];
+  for (int i = threadIdx.x; i < npts; i += blockDim.x) coefs[i] = coefs_g[i];
+  __syncthreads();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= (size_t(1) << (lh + ll))) return;
+  const size_t vh = v >> ll, vl = v & ((size_t(1) << ll) - 1);
+  const size_t nhi = size_t(1) << lh, nlo = size_t(1) << ll;
+  EfMacF m;
+  m.init();
+  m.acc = w[v];
+  int cnt = 0;
+  for (int t = 0; t < npts; t++) {
+    uint32_t e = mul(hi[t * nhi + vh], lo[t * nlo + vl]);
+    m.mac(coefs[t], e);
+    if (++cnt == 4) { m.flush(); cnt = 0; }
+  }
+  m.flush();
+  w[v] = m.acc;
+}
+
+// w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (extension-field points)
+__global__ void k_add_eq_terms_ef(ef* __restrict__ w, int lh, int ll, int npts, const ef* __restrict__ hi,
+                                  const ef* __restrict__ lo, const ef* __restrict__ coefs) {
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= (size_t(1) << (lh + ll))) return;
+  const size_t vh = v >> ll, vl = v & ((size_t(1) << ll) - 1);
+  const size_t nhi = size_t(1) << lh, nlo = size_t(1) << ll;
+  ef acc = w[v];
+  for (int t = 0; t < npts; t++) acc = ef_add(acc, ef_mul(ef_mul(coefs[t], hi[t * nhi + vh]), lo[t * nlo + vl]));
+  w[v] = acc;
+}
+
+constexpr int WSC_THREADS = 256, WSC_PER_THREAD = 8;
+
+__global__ void k_whir_sc_eval(const ef* __restrict__ g, const ef* __restrict__ w, size_t half,
+                               ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  ef s0 = ef_zero(), s1 = ef_zero(), s2 = ef_zero();
+  for (int q = 0; q < WSC_PER_THREAD; q++) {
+    size_t x = (size_t(blockIdx.x) * WSC_PER_THREAD + q) * WSC_THREADS + threadIdx.x;
+    if (x < half) {
+      ef gl = g[x], gh = g[x + half], wl_ = w[x], wh = w[x + half];
+      s0 = ef_add(s0, ef_mul(gl, wl_));
+      s1 = ef_add(s1, ef_mul(gh, wh));
+      s2 = ef_add(s2, ef_mul(ef_sub(ef_add(gh, gh), gl), ef_sub(ef_add(wh, wh), wl_)));
+    }
+  }
+  s0 = block_reduce_ef(s0, scratch);
+  s1 = block_reduce_ef(s1, scratch);
+  s2 = block_reduce_ef(s2, scratch);
+  if (threadIdx.x == 0) {
+    partial[size_t(blockIdx.x) * 3] = s0;
+    partial[size_t(blockIdx.x) * 3 + 1] = s1;
+    partial[size_t(blockIdx.x) * 3 + 2] = s2;
+  }
+}
+
+// partial[v_hi] = hi[v_hi] * sum_{v_lo} g[v] * lo[v_lo]  (one block per v_hi)
+__global__ void k_mle_eval_ef(const ef* __restrict__ g, int lh, int ll, const ef* __restrict__ hi,
+                              const ef* __restrict__ lo, ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  const size_t vh = blockIdx.x;
+  const size_t nlo = size_t(1) << ll;
+  ef acc = ef_zero();
+  for (size_t vl = threadIdx.x; vl < nlo; vl += blockDim.x) acc = ef_add(acc, ef_mul(g[(vh << ll) + vl], lo[vl]));
+  acc = block_reduce_ef(acc, scratch);
+  if (threadIdx.x == 0) partial[vh] = ef_mul(acc, hi[vh]);
+}
+}  // namespace
+
+void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, int ll, int J, const ef* hi,
+                             const ef* lo, ef* out, cudaStream_t s) {
+  // `out` must hold J * 2^lu * (MPB_SPLIT + 1) elements; the split partials go past the
+  // first J * 2^lu results.
+  ef* tmp = out + (size_t(J) << lu);
+  dim3 grid(1u << lu, MPB_SPLIT);
+  int threads = (1 << ll) < 256 ? (1 << ll) : 256;
+  if (threads < 32) threads = 32;
+  if (J == 1) k_mle_partial_base<1><<<grid, threads, 0, s>>>(T, t_len, lu, lh, ll, hi, lo, tmp);
+  else if (J == 2) k_mle_partial_base<2><<<grid, threads, 0, s>>>(T, t_len, lu, lh, ll, hi, lo, tmp);
+  else throw std::runtime_error("mle_partial_base: J must be 1 or 2");
+  WL_LAUNCH_CHECK();
+  size_t n = size_t(J) << lu;
+  k_sum_split<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(tmp, n, out);
+  WL_LAUNCH_CHECK();
+}
+
+void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s) {
+  size_t n = size_t(1) << lv;
+  k_whir_fold_T<<<(unsigned)((n + 255) / 256), 256, sizeof(ef) << lu, s>>>(T, t_len, lu, lv, eqr, out);
+  WL_LAUNCH_CHECK();
+}
+
+void launch_add_eq_terms_f(ef* w, int lh, int ll, int npts, const uint32_t* hi, const uint32_t* lo, const ef* coefs,
+                           cudaStream_t s) {
+  if (!npts) return;
+  size_t n = size_t(1) << (lh + ll);
+  k_add_eq_terms_f<<<(unsigned)((n + 255) / 256), 256, sizeof(ef) * npts, s>>>(w, lh, ll, npts, hi, lo, coefs);
+  WL_LAUNCH_CHECK();
+}
+void launch_add_eq_terms_ef(ef* w, int lh, int ll, int npts, const ef* hi, const ef* lo, const ef* coefs,
+                            cudaStream_t s) {
+  if (!npts) return;
+  size_t n = size_t(1) << (lh + ll);
+  k_add_eq_terms_ef<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(w, lh, ll, npts, hi, lo, coefs);
+  WL_LAUNCH_CHECK();
+}
+int whir_sc_blocks(size_t half) {
+  size_t per = size_t(WSC_THREADS) * WSC_PER_THREAD;
+  return (int)((half + per - 1) / per);
+}
+void launch_whir_sc_eval(const ef* g, const ef* w, size_t half, ef* partial, cudaStream_t s) {
+  k_whir_sc_eval<<<whir_sc_blocks(half), WSC_THREADS, 0, s>>>(g, w, half, partial);
+  WL_LAUNCH_CHECK();
+}
+int mle_ef_blocks(int lh) { return 1 << lh; }
+void launch_mle_eval_ef(const ef* g, int lh, int ll, const ef* hi, const ef* lo, ef* partial, cudaStream_t s) {
+  int threads = (1 << ll) < 256 ? (1 << ll) : 256;
+  if (threads < 32) threads = 32;
+  k_mle_eval_ef<<<1u << lh, threads, 0, s>>>(g, lh, ll, hi, lo, partial);
+  WL_LAUNCH_CHECK();
+}
+
+}  // namespace wl

@@ -1,0 +1,103 @@
+// Host-side launchers for the device kernels. All buffers are device pointers, all
+// field values Montgomery form, extension elements `kb::ef` (8 u32, lowest degree first).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "air.cuh"
+#include "common.cuh"
+
+namespace wl {
+
+// --------------------------------------------------------------- elementwise / trace
+void launch_to_mont(uint32_t* x, size_t n, cudaStream_t s);
+void launch_trace_gen(const uint32_t* inputs_canonical, const AirConsts& K, uint32_t* wit, int log_n, cudaStream_t s);
+
+// --------------------------------------------------------------- Reed-Solomon + Merkle
+// Source of a commitment: an m-variable multilinear given by its evaluation table.
+// Column `col` (< n_cols) of the codeword matrix reads src[(col / elem) * (elem << L) +
+// (col % elem) + s * elem] for s < 2^L (L = m - fold), zero beyond `src_len`.
+struct LdeSource {
+  const uint32_t* src;
+  size_t src_len;
+  int elem;      // 1: base field, 8: extension field (coordinates are separate columns)
+  int L;         // log2 of the column length before the rate expansion
+  int rho;       // log2 of the rate expansion
+  int n_cols;    // stored columns per row (leading columns; the rest are zero)
+};
+void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_t* twiddles, cudaStream_t s);
+// Twiddle table: tw[j] = w^j, w of order 2^24, j < 2^23.
+void launch_twiddles(uint32_t* tw, cudaStream_t s);
+// Leaf digests of rows of `row_cols` (= 128) values, of which the first `n_cols` are
+// stored; the row is Moebius-transformed over the bits [log2(elem), 7) of the column index
+// before hashing.
+void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
+                      uint32_t* digests, cudaStream_t s);
+void launch_merkle_level(const uint32_t* child, uint32_t* parent, size_t n_parent, const kb::P16Consts& p16,
+                         cudaStream_t s);
+// Gathers rows (raw, `n_cols` stored columns, zero padded to 128) and digests.
+void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s);
+
+// --------------------------------------------------------------- PoW
+// Smallest w in [base, base + count) with from_mont(sample) & mask == 0 after observing w.
+void launch_grind(const kb::P16Consts& p16, const uint32_t* state16, const uint32_t* inbuf, int inlen, int bits,
+                  uint32_t base, uint32_t count, uint32_t* result, cudaStream_t s);
+
+// --------------------------------------------------------------- eq tables / reductions
+void launch_eq_table(const ef* point, int nvars, ef* out, cudaStream_t s);
+void launch_eq_table_f(const uint32_t* points, int npts, int nvars, uint32_t* out, cudaStream_t s);
+void launch_reduce_partials(const ef* partial, int nblk, int k, ef* out, cudaStream_t s);
+
+// --------------------------------------------------------------- AIR zerocheck
+// Round 0 with univariate skip over the top k variables: partial[blk * nz + z] sums, for
+// the nz points z_0.. given by their Lagrange weights lw[z * 2^k + j], the eq-weighted
+// batched constraint over the up columns.
+int zc0_blocks(int log_n, int k);
+void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
+                     const ef* alphas, const AirConsts& K, ef* partial, cudaStream_t s);
+void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
+int zc_ef_blocks(int m);
+void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const AirConsts& K, ef* partial,
+                       cudaStream_t s);
+void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s);
+// Up/down evaluations of every column at (r0; tail): per (column, j) partial sums.
+void launch_inner_sums(const uint32_t* wit, int log_n, int k, const ef* eqt, const ef* sel, ef* out_up,
+                       ef* out_down, cudaStream_t s);
+
+// --------------------------------------------------------------- inner phase
+void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s);
+int sub_eval_blocks(int log_n, int k);
+void launch_sub_evals(const ef* batched, int log_n, int k, const ef* alpha2, const ef* eqt, ef* partial,
+                      cudaStream_t s);
+void launch_inner_mle(const ef* eqp, int log_n, const ef* alpha2, ef* out, cudaStream_t s);
+int prod_blocks(size_t half);
+void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s);
+void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s);
+
+// --------------------------------------------------------------- a*b - c zerocheck
+void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
+                      const uint32_t* lw, const ef* eq, ef* partial, cudaStream_t s);
+int abc0_blocks(int log_n, int k);
+void launch_abc0_fold(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, const ef* sel,
+                      ef* out, cudaStream_t s);
+void launch_abc_eval_ef(const ef* cols, int m, const ef* eq, ef* partial, cudaStream_t s);
+
+// --------------------------------------------------------------- WHIR
+// F_j[u] = sum_v T[u * 2^lv + v] * eq(pt_j, v) for J points given as factored tables
+// hi_j (2^lh entries) x lo_j (2^ll entries), lv = lh + ll; T is the zero-padded packed
+// witness of `t_len` values. out[j * 2^lu + u].
+void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, int ll, int J, const ef* hi,
+                             const ef* lo, ef* out, cudaStream_t s);
+void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s);
+void launch_add_eq_terms_f(ef* w, int lh, int ll, int npts, const uint32_t* hi, const uint32_t* lo, const ef* coefs,
+                           cudaStream_t s);
+void launch_add_eq_terms_ef(ef* w, int lh, int ll, int npts, const ef* hi, const ef* lo, const ef* coefs,
+                            cudaStream_t s);
+int whir_sc_blocks(size_t half);
+void launch_whir_sc_eval(const ef* g, const ef* w, size_t half, ef* partial, cudaStream_t s);
+int mle_ef_blocks(int lh);
+void launch_mle_eval_ef(const ef* g, int lh, int ll, const ef* hi, const ef* lo, ef* partial, cudaStream_t s);
+
+}  // namespace wl

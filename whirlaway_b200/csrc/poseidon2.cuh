@@ -1,0 +1,177 @@
+// Poseidon2 over KoalaBear for widths 16 and 24 (S-box x^3, 8 full rounds, 20 / 23
+// partial rounds), host and device. Replaces Plonky3's Poseidon2KoalaBear<16/24>
+// (reference: src/examples/poseidon2.rs:22-26,148-151) and the linear layers of
+// GenericPoseidon2LinearLayersKoalaBear used by the AIR.
+//
+// External layer: circ(2*M4, M4, ..., M4), M4 = [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]].
+// Internal layer: J + diag(V) (state_i <- V_i * state_i + sum(state)).
+// Round constants are runtime data (drawn from the workload's StdRng stream) and are
+// kept in Montgomery form.
+#pragma once
+#include "kb.cuh"
+
+namespace kb {
+
+namespace detail {
+constexpr uint64_t cpow(uint64_t a, uint64_t e) {
+  uint64_t r = 1;
+  a %= P;
+  while (e) {
+    if (e & 1) r = r * a % P;
+    a = a * a % P;
+    e >>= 1;
+  }
+  return r;
+}
+constexpr uint32_t cm(int64_t x) {  // Montgomery form of a signed small constant
+  uint64_t v = uint64_t(((x % int64_t(P)) + int64_t(P)) % int64_t(P));
+  return uint32_t((v << 32) % P);
+}
+constexpr uint32_t cm_inv2(int k, bool negative) {  // Montgomery form of +-1/2^k
+  uint64_t v = cpow(cpow(2, k), P - 2);
+  if (negative) v = (P - v) % P;
+  return uint32_t((v << 32) % P);
+}
+}  // namespace detail
+
+// Internal-layer diagonals V (Montgomery form); the internal matrix is J + diag(V).
+//   width 16: [-2, 1, 2, 1/2, 3, 4, -1/2, -3, -4, 1/2^8, 1/8, 1/2^24, -1/2^8, -1/8, -1/16, -1/2^24]
+//   width 24: [-2, 1, 2, 1/2, 3, 4, -1/2, -3, -4, 1/2^8, 1/4, 1/8, 1/16, 1/32, 1/64, 1/2^24,
+//              -1/2^8, -1/8, -1/16, -1/32, -1/64, -1/2^7, -1/2^9, -1/2^24]
+template <int W>
+KB_HD constexpr uint32_t p2_diag(int i) {
+  using detail::cm;
+  using detail::cm_inv2;
+  switch (i) {
+    case 0: return cm(-2);
+    case 1: return cm(1);
+    case 2: return cm(2);
+    case 3: return cm_inv2(1, false);
+    case 4: return cm(3);
+    case 5: return cm(4);
+    case 6: return cm_inv2(1, true);
+    case 7: return cm(-3);
+    case 8: return cm(-4);
+    case 9: return cm_inv2(8, false);
+    default: break;
+  }
+  if (W == 16) {
+    switch (i) {
+      case 10: return cm_inv2(3, false);
+      case 11: return cm_inv2(24, false);
+      case 12: return cm_inv2(8, true);
+      case 13: return cm_inv2(3, true);
+      case 14: return cm_inv2(4, true);
+      default: return cm_inv2(24, true);
+    }
+  }
+  switch (i) {
+    case 10: return cm_inv2(2, false);
+    case 11: return cm_inv2(3, false);
+    case 12: return cm_inv2(4, false);
+    case 13: return cm_inv2(5, false);
+    case 14: return cm_inv2(6, false);
+    case 15: return cm_inv2(24, false);
+    case 16: return cm_inv2(8, true);
+    case 17: return cm_inv2(3, true);
+    case 18: return cm_inv2(4, true);
+    case 19: return cm_inv2(5, true);
+    case 20: return cm_inv2(6, true);
+    case 21: return cm_inv2(7, true);
+    case 22: return cm_inv2(9, true);
+    default: return cm_inv2(24, true);
+  }
+}
+
+template <int W>
+struct P2Consts {
+  static constexpr int RP = W == 16 ? 20 : 23;
+  uint32_t ext_init[4 * W];
+  uint32_t ext_term[4 * W];
+  uint32_t internal[RP];
+};
+using P16Consts = P2Consts<16>;
+using P24Consts = P2Consts<24>;
+
+template <int W>
+KB_HD void mds_light(uint32_t* s) {
+#pragma unroll
+  for (int c = 0; c < W; c += 4) {
+    uint32_t x0 = s[c], x1 = s[c + 1], x2 = s[c + 2], x3 = s[c + 3];
+    uint32_t t01 = add(x0, x1), t23 = add(x2, x3), t0123 = add(t01, t23);
+    uint32_t t01123 = add(t0123, x1), t01233 = add(t0123, x3);
+    s[c + 3] = add(t01233, dbl(x0));
+    s[c + 1] = add(t01123, dbl(x2));
+    s[c + 0] = add(t01123, t01);
+    s[c + 2] = add(t01233, t23);
+  }
+  uint32_t sums[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    sums[k] = s[k];
+#pragma unroll
+    for (int j = 4 + k; j < W; j += 4) sums[k] = add(sums[k], s[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = add(s[i], sums[i & 3]);
+}
+
+template <int W>
+KB_HD void internal_layer(uint32_t* s) {
+  uint32_t sum = s[0];
+#pragma unroll
+  for (int i = 1; i < W; i++) sum = add(sum, s[i]);
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = add(mul(s[i], p2_diag<W>(i)), sum);
+}
+
+template <int W>
+KB_HD void p2_permute(uint32_t* s, const P2Consts<W>& c) {
+  mds_light<W>(s);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) s[i] = cube(add(s[i], c.ext_init[r * W + i]));
+    mds_light<W>(s);
+  }
+#pragma unroll 1
+  for (int r = 0; r < P2Consts<W>::RP; r++) {
+    s[0] = cube(add(s[0], c.internal[r]));
+    internal_layer<W>(s);
+  }
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) s[i] = cube(add(s[i], c.ext_term[r * W + i]));
+    mds_light<W>(s);
+  }
+}
+
+// Extension-field versions of the linear layers (constraint evaluation over EF).
+KB_HD void mds_light_ef16(ef* s) {
+#pragma unroll
+  for (int c = 0; c < 16; c += 4) {
+    ef x0 = s[c], x1 = s[c + 1], x2 = s[c + 2], x3 = s[c + 3];
+    ef t01 = ef_add(x0, x1), t23 = ef_add(x2, x3), t0123 = ef_add(t01, t23);
+    ef t01123 = ef_add(t0123, x1), t01233 = ef_add(t0123, x3);
+    s[c + 3] = ef_add(t01233, ef_add(x0, x0));
+    s[c + 1] = ef_add(t01123, ef_add(x2, x2));
+    s[c + 0] = ef_add(t01123, t01);
+    s[c + 2] = ef_add(t01233, t23);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    ef sk = ef_add(ef_add(s[k], s[4 + k]), ef_add(s[8 + k], s[12 + k]));
+#pragma unroll
+    for (int j = k; j < 16; j += 4) s[j] = ef_add(s[j], sk);
+  }
+}
+KB_HD void internal_layer_ef16(ef* s) {
+  ef sum = s[0];
+#pragma unroll
+  for (int i = 1; i < 16; i++) sum = ef_add(sum, s[i]);
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = ef_add(ef_mul_f(s[i], p2_diag<16>(i)), sum);
+}
+
+}  // namespace kb

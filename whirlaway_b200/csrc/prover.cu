@@ -1,0 +1,818 @@
+// GPU prover orchestration. The order of transcript operations is that of
+// AirTable::prove (crates/air/src/prove.rs:49-226), sumcheck::prove / sc_round
+// (crates/sumcheck/src/prove.rs:22-254) and the WHIR prover; heavy work runs in the
+// kernels of k_commit.cu, k_sumcheck.cu and k_whir.cu, the transcript and the
+// small-polynomial arithmetic between rounds run on the host.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+
+#include "prover.h"
+
+namespace wl {
+
+// ------------------------------------------------------------------ memory
+DBuf::DBuf(size_t bytes, cudaStream_t s) : bytes_(bytes), s_(s) {
+  if (bytes) {
+    cudaError_t e = cudaMallocAsync(&p_, bytes, s);
+    if (e != cudaSuccess) {
+      p_ = nullptr;
+      bytes_ = 0;
+      cudaGetLastError();
+      throw CudaError(e, "cudaMallocAsync(" + std::to_string(bytes) + " bytes)");
+    }
+  }
+}
+DBuf::~DBuf() { reset(); }
+void DBuf::reset() {
+  if (p_) cudaFreeAsync(p_, s_);
+  p_ = nullptr;
+  bytes_ = 0;
+}
+DBuf& DBuf::operator=(DBuf&& o) noexcept {
+  if (this != &o) {
+    reset();
+    p_ = o.p_;
+    bytes_ = o.bytes_;
+    s_ = o.s_;
+    o.p_ = nullptr;
+    o.bytes_ = 0;
+  }
+  return *this;
+}
+
+namespace {
+constexpr size_t kUpBytes = 4 << 20;    // pinned upload ring
+constexpr size_t kDownBytes = 4 << 20;  // pinned download staging
+thread_local size_t g_up_off = 0;
+}  // namespace
+
+Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
+  WL_CUDA(cudaSetDevice(dev));
+  WL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cudaMemPool_t pool;
+  WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = UINT64_MAX;
+  WL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  WL_CUDA(cudaMalloc(&twiddles, sizeof(uint32_t) << 23));
+  launch_twiddles(twiddles, stream);
+  pinned_bytes = kUpBytes + kDownBytes;
+  WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
+  WL_CUDA(cudaStreamSynchronize(stream));
+}
+Context::~Context() {
+  cudaSetDevice(device);
+  cudaStreamSynchronize(stream);
+  cudaFree(twiddles);
+  cudaFreeHost(pinned);
+  cudaStreamDestroy(stream);
+}
+void Context::to_host(void* dst, const void* src, size_t bytes) {
+  char* down = static_cast<char*>(pinned) + kUpBytes;
+  if (bytes <= kDownBytes) {
+    WL_CUDA(cudaMemcpyAsync(down, src, bytes, cudaMemcpyDeviceToHost, stream));
+    WL_CUDA(cudaStreamSynchronize(stream));
+    memcpy(dst, down, bytes);
+  } else {
+    WL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+    WL_CUDA(cudaStreamSynchronize(stream));
+  }
+  g_up_off = 0;  // every earlier upload has completed
+}
+void Context::to_device(void* dst, const void* src, size_t bytes) {
+  if (bytes > kUpBytes) {
+    WL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    WL_CUDA(cudaStreamSynchronize(stream));
+    g_up_off = 0;
+    return;
+  }
+  if (g_up_off + bytes > kUpBytes) {
+    WL_CUDA(cudaStreamSynchronize(stream));
+    g_up_off = 0;
+  }
+  char* up = static_cast<char*>(pinned) + g_up_off;
+  memcpy(up, src, bytes);
+  WL_CUDA(cudaMemcpyAsync(dst, up, bytes, cudaMemcpyHostToDevice, stream));
+  g_up_off += (bytes + 255) & ~size_t(255);
+}
+
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <class T>
+DBuf upload(Context& ctx, const std::vector<T>& v) {
+  DBuf b(v.size() * sizeof(T), ctx.stream);
+  if (!v.empty()) ctx.to_device(b.as<void>(), v.data(), v.size() * sizeof(T));
+  return b;
+}
+
+std::vector<ef> reduce_to_host(Context& ctx, const ef* partial, int nblk, int k) {
+  DBuf out(sizeof(ef) * k, ctx.stream);
+  launch_reduce_partials(partial, nblk, k, out.as<ef>(), ctx.stream);
+  std::vector<ef> h(k);
+  ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * k);
+  return h;
+}
+
+DBuf eq_table_dev(Context& ctx, const std::vector<ef>& pt) {
+  DBuf out(sizeof(ef) << pt.size(), ctx.stream);
+  if (pt.empty()) {
+    std::vector<ef> one{kb::ef_one()};
+    ctx.to_device(out.as<void>(), one.data(), sizeof(ef));
+    return out;
+  }
+  DBuf p = upload(ctx, pt);
+  launch_eq_table(p.as<ef>(), (int)pt.size(), out.as<ef>(), ctx.stream);
+  return out;
+}
+
+DBuf scalar_dev(Context& ctx, const ef& v) { return upload(ctx, std::vector<ef>{v}); }
+
+// Grinding: the smallest witness (searched on the device in batches), then the host
+// challenger replays observe(w) + sample_bits exactly as check_witness does.
+void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
+  if (bits <= 0) return;
+  DBuf res(sizeof(uint32_t), ctx.stream);
+  const uint32_t batch = 1u << 20;
+  for (uint64_t base = 0; base < kb::P; base += batch) {
+    uint32_t init = UINT32_MAX;
+    ctx.to_device(res.as<void>(), &init, 4);
+    launch_grind(p16, ts.ch.state, ts.ch.in, ts.ch.in_len, bits, (uint32_t)base, batch, res.as<uint32_t>(),
+                 ctx.stream);
+    uint32_t r;
+    ctx.to_host(&r, res.as<uint32_t>(), 4);
+    if (r != UINT32_MAX) {
+      uint32_t w = kb::to_mont(r);
+      ts.ch.observe(w);
+      if (ts.ch.sample_bits(bits) != 0) throw std::runtime_error("grinding witness failed on the host");
+      ts.proof.push_back(w);
+      return;
+    }
+  }
+  throw std::runtime_error("grinding: no witness");
+}
+
+// ------------------------------------------------------------------ commitments
+struct Commitment {
+  int num_vars = 0, fold = 0, elem = 1, log_leaves = 0, n_cols = 0;
+  DBuf lde, tree;
+  uint32_t root[8];
+};
+size_t level_offset(int LL, int l) { return (size_t(1) << (LL + 1)) - (size_t(1) << (LL + 1 - l)); }
+
+Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, const kb::P24Consts& p24,
+                  const kb::P16Consts& p16) {
+  Commitment c;
+  c.num_vars = num_vars;
+  c.fold = fold;
+  c.elem = src.elem;
+  c.log_leaves = src.L + src.rho;
+  c.n_cols = src.n_cols;
+  if ((src.elem << fold) != 128) throw std::invalid_argument("leaf rows must hold 128 base-field values");
+  const size_t rows = size_t(1) << c.log_leaves;
+  c.lde = DBuf(rows * c.n_cols * sizeof(uint32_t), ctx.stream);
+  launch_lde(src, nullptr, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream);
+  const int LL = c.log_leaves;
+  c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
+  uint32_t* t = c.tree.as<uint32_t>();
+  launch_leaf_hash(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, t, ctx.stream);
+  for (int l = 1; l <= LL; l++)
+    launch_merkle_level(t + level_offset(LL, l - 1) * 8, t + level_offset(LL, l) * 8, size_t(1) << (LL - l), p16,
+                        ctx.stream);
+  ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
+  return c;
+}
+
+std::vector<uint32_t> sample_queries(Transcript& ts, int log_leaves, int count) {
+  std::vector<uint32_t> q(count);
+  for (auto& x : q) x = ts.ch.sample_bits(log_leaves);
+  std::sort(q.begin(), q.end());
+  q.erase(std::unique(q.begin(), q.end()), q.end());
+  return q;
+}
+
+// Appends rows (Moebius-transformed over the position bits, as hashed) and
+// authentication paths as hints; returns the rows.
+std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const std::vector<uint32_t>& idx,
+                                        Transcript& ts) {
+  const int LL = c.log_leaves, nq = (int)idx.size();
+  std::vector<uint64_t> ridx(idx.begin(), idx.end()), didx;
+  for (uint32_t i : idx)
+    for (int l = 0; l < LL; l++) didx.push_back(level_offset(LL, l) + ((i >> l) ^ 1u));
+  DBuf dr = upload(ctx, ridx), dd = upload(ctx, didx);
+  DBuf rows(sizeof(uint32_t) * c.n_cols * std::max(nq, 1), ctx.stream);
+  DBuf digs(sizeof(uint32_t) * 8 * std::max<size_t>(didx.size(), 1), ctx.stream);
+  launch_gather_u32(c.lde.as<uint32_t>(), dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream);
+  launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream);
+  std::vector<uint32_t> hr(size_t(c.n_cols) * nq), hd(didx.size() * 8);
+  if (nq) {
+    ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
+    ctx.to_host(hd.data(), digs.as<uint32_t>(), hd.size() * 4);
+  }
+  const int log_elem = c.elem == 8 ? 3 : 0;
+  std::vector<std::vector<uint32_t>> out;
+  for (int q = 0; q < nq; q++) {
+    std::vector<uint32_t> row(128, 0);
+    for (int i = 0; i < c.n_cols; i++) row[i] = hr[size_t(q) * c.n_cols + i];
+    for (int b = log_elem; b < 7; b++)
+      for (int i = 0; i < 128; i++)
+        if (!(i & (1 << b))) row[i + (1 << b)] = kb::sub(row[i + (1 << b)], row[i]);
+    ts.hint(row.data(), 128);
+    ts.hint(&hd[size_t(q) * LL * 8], size_t(LL) * 8);
+    out.push_back(row);
+  }
+  return out;
+}
+
+// Coefficient-form multilinear evaluation of a (transformed) row at r (row MSB <-> r_1).
+ef fold_row(const std::vector<uint32_t>& row, int fold, int elem, const std::vector<ef>& r) {
+  std::vector<ef> v(size_t(1) << fold);
+  for (size_t p = 0; p < v.size(); p++) {
+    v[p] = kb::ef_zero();
+    for (int e = 0; e < elem; e++) v[p].c[e] = row[p * elem + e];
+  }
+  for (int i = 0; i < fold; i++) {
+    size_t h = v.size() / 2;
+    for (size_t q = 0; q < h; q++) v[q] = kb::ef_add(v[q], kb::ef_mul(r[i], v[q + h]));
+    v.resize(h);
+  }
+  return v[0];
+}
+
+void split_vars(int lv, int& lh, int& ll) {
+  ll = std::min(10, lv);
+  lh = lv - ll;
+}
+
+// Factored eq tables of an extension point: hi over pt[0..lh), lo over pt[lh..).
+struct EqPair {
+  DBuf hi, lo;
+};
+EqPair eq_pair(Context& ctx, const std::vector<ef>& pt, int lh) {
+  EqPair e;
+  e.hi = eq_table_dev(ctx, std::vector<ef>(pt.begin(), pt.begin() + lh));
+  e.lo = eq_table_dev(ctx, std::vector<ef>(pt.begin() + lh, pt.end()));
+  return e;
+}
+
+// Adds sum_t coefs[t] * eq(points[t], .) for extension-field points.
+void add_eq_ef(Context& ctx, ef* w, int m, const std::vector<std::vector<ef>>& pts, const std::vector<ef>& coefs) {
+  int lh, ll;
+  split_vars(m, lh, ll);
+  const int np = (int)pts.size();
+  if (!np) return;
+  DBuf hi(sizeof(ef) * (size_t(np) << lh), ctx.stream), lo(sizeof(ef) * (size_t(np) << ll), ctx.stream);
+  for (int t = 0; t < np; t++) {
+    EqPair e = eq_pair(ctx, pts[t], lh);
+    WL_CUDA(cudaMemcpyAsync(hi.as<ef>() + (size_t(t) << lh), e.hi.as<ef>(), sizeof(ef) << lh,
+                            cudaMemcpyDeviceToDevice, ctx.stream));
+    WL_CUDA(cudaMemcpyAsync(lo.as<ef>() + (size_t(t) << ll), e.lo.as<ef>(), sizeof(ef) << ll,
+                            cudaMemcpyDeviceToDevice, ctx.stream));
+  }
+  DBuf dc = upload(ctx, coefs);
+  launch_add_eq_terms_ef(w, lh, ll, np, hi.as<ef>(), lo.as<ef>(), dc.as<ef>(), ctx.stream);
+}
+
+// Adds sum_t coefs[t] * eq(points[t], .) for base-field points (STIR queries).
+void add_eq_f(Context& ctx, ef* w, int m, const std::vector<std::vector<uint32_t>>& pts,
+              const std::vector<ef>& coefs) {
+  int lh, ll;
+  split_vars(m, lh, ll);
+  const int np = (int)pts.size();
+  if (!np) return;
+  std::vector<uint32_t> ph, pl;
+  for (auto& p : pts) {
+    ph.insert(ph.end(), p.begin(), p.begin() + lh);
+    pl.insert(pl.end(), p.begin() + lh, p.end());
+  }
+  DBuf dph = upload(ctx, ph.empty() ? std::vector<uint32_t>{0} : ph), dpl = upload(ctx, pl);
+  DBuf hi(sizeof(uint32_t) * (size_t(np) << lh), ctx.stream), lo(sizeof(uint32_t) * (size_t(np) << ll), ctx.stream);
+  launch_eq_table_f(dph.as<uint32_t>(), np, lh, hi.as<uint32_t>(), ctx.stream);
+  launch_eq_table_f(dpl.as<uint32_t>(), np, ll, lo.as<uint32_t>(), ctx.stream);
+  DBuf dc = upload(ctx, coefs);
+  launch_add_eq_terms_f(w, lh, ll, np, hi.as<uint32_t>(), lo.as<uint32_t>(), dc.as<ef>(), ctx.stream);
+}
+
+// g(pt) for a device extension table g over m variables.
+ef mle_eval_dev(Context& ctx, const ef* g, int m, const std::vector<ef>& pt) {
+  int lh, ll;
+  split_vars(m, lh, ll);
+  EqPair e = eq_pair(ctx, pt, lh);
+  DBuf part(sizeof(ef) << lh, ctx.stream);
+  launch_mle_eval_ef(g, lh, ll, e.hi.as<ef>(), e.lo.as<ef>(), part.as<ef>(), ctx.stream);
+  return reduce_to_host(ctx, part.as<ef>(), 1 << lh, 1)[0];
+}
+
+// k rounds of the WHIR sumcheck on device tables (g, w), both of size 2^m on entry.
+void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, ef& sigma, int rounds, int pow_bits,
+                       const kb::P16Consts& p16, std::vector<ef>& rnd) {
+  for (int t = 0; t < rounds; t++) {
+    size_t half = size_t(1) << (m - 1);
+    int nb = whir_sc_blocks(half);
+    DBuf part(sizeof(ef) * 3 * nb, ctx.stream);
+    launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part.as<ef>(), ctx.stream);
+    std::vector<ef> h = reduce_to_host(ctx, part.as<ef>(), nb, 3);
+    ts.add_ext(h.data(), 3);
+    grind(ctx, ts, p16, pow_bits);
+    ef r = ts.sample_ext();
+    rnd.push_back(r);
+    sigma = quad_eval(h.data(), r);
+    DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
+    DBuf dr = scalar_dev(ctx, r);
+    launch_fold2(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, dr.as<ef>(), ctx.stream);
+    g = std::move(ng);
+    w = std::move(nw);
+    m--;
+  }
+}
+
+// Host sumcheck on small tables (initial WHIR block and the final rounds).
+void whir_sumcheck_host(Context& ctx, Transcript& ts, std::vector<std::vector<ef>>& G, std::vector<std::vector<ef>>& E,
+                        const std::vector<ef>& coef, ef& sigma, int rounds, int pow_bits, const kb::P16Consts& p16,
+                        std::vector<ef>& rnd) {
+  for (int t = 0; t < rounds; t++) {
+    size_t half = G[0].size() / 2;
+    ef h[3] = {kb::ef_zero(), kb::ef_zero(), kb::ef_zero()};
+    for (size_t j = 0; j < G.size(); j++) {
+      ef s[3] = {kb::ef_zero(), kb::ef_zero(), kb::ef_zero()};
+      for (size_t x = 0; x < half; x++) {
+        const ef &gl = G[j][x], &gh = G[j][x + half], &el = E[j][x], &eh = E[j][x + half];
+        s[0] = kb::ef_add(s[0], kb::ef_mul(gl, el));
+        s[1] = kb::ef_add(s[1], kb::ef_mul(gh, eh));
+        s[2] = kb::ef_add(s[2], kb::ef_mul(kb::ef_sub(kb::ef_add(gh, gh), gl), kb::ef_sub(kb::ef_add(eh, eh), el)));
+      }
+      for (int q = 0; q < 3; q++) h[q] = kb::ef_add(h[q], kb::ef_mul(coef[j], s[q]));
+    }
+    ts.add_ext(h, 3);
+    grind(ctx, ts, p16, pow_bits);
+    ef r = ts.sample_ext();
+    rnd.push_back(r);
+    sigma = quad_eval(h, r);
+    for (size_t j = 0; j < G.size(); j++) {
+      for (size_t x = 0; x < half; x++) {
+        G[j][x] = kb::ef_lerp(G[j][x], G[j][x + half], r);
+        E[j][x] = kb::ef_lerp(E[j][x], E[j][x + half], r);
+      }
+      G[j].resize(half);
+      E[j].resize(half);
+    }
+  }
+}
+
+std::vector<uint32_t> to_canonical(const std::vector<uint32_t>& v) {
+  std::vector<uint32_t> out(v.size());
+  for (size_t i = 0; i < v.size(); i++) out[i] = kb::from_mont(v[i]);
+  return out;
+}
+
+}  // namespace
+
+size_t proof_len_bound(const Settings& s, int log_n) {
+  WhirSchedule w = WhirSchedule::build(log_n + AIR_LOG_W, s);
+  const int k = s.univariate_skips;
+  size_t n = 8 + 8 * w.c[0].ood;                              // root + OOD answers
+  n += 8 * size_t(4 * ((1 << k) - 1) + 1);                    // zerocheck round 0
+  n += 8 * size_t(5) * (log_n - k);                           // zerocheck rounds >= 1
+  n += 8 * size_t(2 * AIR_W) + 8 * (size_t(1) << k);          // inner sums, sub-evaluations
+  n += 8 * size_t(3) * log_n;                                 // inner sumcheck
+  n += 16;                                                    // grinding witnesses (generous)
+  n += 8 * 3 * size_t(w.num_vars);                            // WHIR sumcheck messages
+  for (int j = 0; j <= w.num_rounds; j++) {
+    const WhirRound& r = w.c[j];
+    if (j > 0) n += 8 + 8 * r.ood;
+    n += size_t(r.queries) * (128 + 8 * size_t(r.log_leaves())) + 2;
+  }
+  n += 8 * (size_t(1) << w.final_vars);
+  return n;
+}
+
+std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit, Timings* tm) {
+  const Settings& s = job.settings;
+  const int n = job.log_n, k = s.univariate_skips, W = AIR_W;
+  if (k >= n) throw std::invalid_argument("univariate_skips must be smaller than log_n_rows");
+  if (s.fold_first != 7 || s.fold_rest != 4) throw std::invalid_argument("folding factors other than (7, 4)");
+  const size_t N = size_t(1) << n, S = N >> k;
+  const int m0 = n + AIR_LOG_W;
+  const WhirSchedule ws = WhirSchedule::build(m0, s);
+  cudaStream_t st = ctx.stream;
+  Transcript ts(&job.p16);
+  for (uint32_t x : ws.domain_separator()) ts.ch.observe(kb::to_mont(x));
+  const double t0 = now_ms();
+
+  // ---------------------------------------------------------------- 1) commit
+  const size_t t_len = size_t(W) * N;
+  const int lu = ws.c[0].fold, lv = m0 - lu;
+  int lh_v, ll_v;
+  split_vars(lv, lh_v, ll_v);
+  LdeSource src0{wit, t_len, 1, lv, ws.c[0].log_inv_rate, 0};
+  src0.n_cols = (int)(((t_len + (size_t(1) << lv) - 1) >> lv) + 7) / 8 * 8;
+  Commitment c0 = commit(ctx, src0, m0, ws.c[0].fold, job.p24, job.p16);
+  ts.add_base(c0.root, 8);
+  // Commitment OOD: F_0[u] = sum_v T[u, v] eq(pt_v, v), answer = sum_u eq(pt_u, u) F_0[u].
+  std::vector<std::vector<ef>> ood_pts;
+  std::vector<ef> ood_vals;
+  std::vector<std::vector<ef>> Fu;  // per initial constraint, the 2^lu partial evaluations
+  auto partial_eval = [&](const std::vector<ef>& pt) {
+    std::vector<ef> pv(pt.begin() + lu, pt.end());
+    EqPair e = eq_pair(ctx, pv, lh_v);
+    DBuf out(sizeof(ef) * (size_t(1) << lu) * 5, st);
+    launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st);
+    std::vector<ef> h(size_t(1) << lu);
+    ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * h.size());
+    return h;
+  };
+  for (int q = 0; q < ws.c[0].ood; q++) {
+    ef z = ts.sample_ext();
+    std::vector<ef> pt = pow_point(z, m0);
+    std::vector<ef> f = partial_eval(pt);
+    std::vector<ef> eu = eq_table_host(std::vector<ef>(pt.begin(), pt.begin() + lu));
+    ef y = kb::ef_zero();
+    for (size_t u = 0; u < f.size(); u++) y = kb::ef_add(y, kb::ef_mul(eu[u], f[u]));
+    ts.add_ext(&y, 1);
+    ood_pts.push_back(pt);
+    ood_vals.push_back(y);
+    Fu.push_back(f);
+  }
+  const double t1 = now_ms();
+
+  // ---------------------------------------------------------------- 2) challenges
+  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, log2_up(AIR_NC)));
+  ef alpha = ts.sample_ext();
+  std::vector<ef> alphas(AIR_NC);
+  alphas[0] = kb::ef_one();
+  for (int i = 1; i < AIR_NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
+  DBuf d_alphas = upload(ctx, alphas);
+  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, n));
+  std::vector<ef> zc(n + 1 - k);
+  for (auto& x : zc) x = ts.sample_ext();
+
+  // ---------------------------------------------------------------- 3) zerocheck
+  const int nsk = 1 << k;
+  const auto sel = [&] {
+    auto b = lagrange_basis(nsk);
+    return b;
+  }();  // L_i on {0..2^k-1}
+  const int nz = 3 * (nsk - 1) - nsk + 1;
+  std::vector<ef> zc_tail(zc.begin() + 1, zc.end());
+  DBuf eq0 = eq_table_dev(ctx, zc_tail);
+  std::vector<ef> challenges;
+  ef sum = kb::ef_zero();
+  ef mmf = kb::ef_one();
+  DBuf cols;
+  {
+    std::vector<uint32_t> lw(size_t(nz) * nsk);
+    for (int zi = 0; zi < nz; zi++)
+      for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
+    DBuf d_lw = upload(ctx, lw);
+    const int nb = zc0_blocks(n, k);
+    DBuf part(sizeof(ef) * size_t(nb) * nz, st);
+    launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st);
+    std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
+    std::vector<ef> ys(nsk, kb::ef_zero());
+    ys.insert(ys.end(), sums.begin(), sums.end());
+    std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
+    std::vector<ef> qv(nsk);
+    for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], zc[0]);
+    p = poly_mul(p, interpolate(sel, qv));
+    const int deg = 4 * (nsk - 1);
+    p.resize(deg + 1, kb::ef_zero());
+    ts.add_ext(p.data(), p.size());
+    ef r0 = ts.sample_ext();
+    challenges.push_back(r0);
+    sum = poly_eval(p, r0);
+    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, deg));
+    std::vector<ef> selr(nsk);
+    mmf = kb::ef_zero();
+    for (int i = 0; i < nsk; i++) {
+      selr[i] = upoly_eval(sel[i], r0);
+      mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
+    }
+    DBuf d_sel = upload(ctx, selr);
+    cols = DBuf(sizeof(ef) * size_t(W) * S, st);
+    launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st);
+  }
+  const auto basis4 = lagrange_basis(4);
+  for (int round = 1; round <= n - k; round++) {
+    const int m = n - k - round + 1;  // variables of the current columns
+    const size_t half = size_t(1) << (m - 1);
+    DBuf eqr = eq_table_dev(ctx, std::vector<ef>(zc.begin() + 1 + round, zc.end()));
+    const int nb = zc_ef_blocks(m);
+    DBuf part(sizeof(ef) * size_t(nb) * 3, st);
+    launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st);
+    std::vector<ef> s3 = reduce_to_host(ctx, part.as<ef>(), nb, 3);
+    const ef& r = zc[round];
+    ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
+    ef e1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(e0, kb::ef_sub(kb::ef_one(), r))), kb::ef_inv(r));
+    std::vector<ef> p = interpolate(basis4, {e0, e1, e2, e3});
+    p = poly_mul(p, {kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_add(r, r), kb::ef_one())});
+    ts.add_ext(p.data(), p.size());
+    ef c = ts.sample_ext();
+    challenges.push_back(c);
+    sum = poly_eval(p, c);
+    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 4));
+    mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
+                     mmf);
+    DBuf nc(sizeof(ef) * size_t(W) * half, st);
+    DBuf dc = scalar_dev(ctx, c);
+    launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st);
+    cols = std::move(nc);
+  }
+  // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
+  // The zerocheck's returned challenges replace the eq challenges from here on
+  // (crates/air/src/prove.rs:109 rebinds zerocheck_challenges).
+  std::vector<ef> inner_up(W), inner_down(W);
+  const std::vector<ef> rtail(challenges.begin() + 1, challenges.end());
+  DBuf eqt = eq_table_dev(ctx, rtail);
+  {
+    std::vector<ef> selr(nsk);
+    for (int i = 0; i < nsk; i++) selr[i] = upoly_eval(sel[i], challenges[0]);
+    DBuf d_sel = upload(ctx, selr);
+    DBuf up(sizeof(ef) * size_t(W) * (1 + nsk), st), down(sizeof(ef) * size_t(W) * (1 + nsk), st);
+    launch_inner_sums(wit, n, k, eqt.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st);
+    ctx.to_host(inner_up.data(), up.as<ef>(), sizeof(ef) * W);
+    ctx.to_host(inner_down.data(), down.as<ef>(), sizeof(ef) * W);
+  }
+  cols.reset();
+  const double t2 = now_ms();
+
+  // ---------------------------------------------------------------- 4) inner sumcheck
+  ts.add_ext(inner_up.data(), W);
+  ts.add_ext(inner_down.data(), W);
+  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, AIR_LOG_W));
+  std::vector<ef> cbs(AIR_LOG_W);
+  for (auto& x : cbs) x = ts.sample_ext();
+  std::vector<ef> eqc = eq_table_host(cbs);
+  eqc.resize(W);
+  DBuf d_eqc = upload(ctx, eqc);
+  DBuf B(sizeof(ef) * N, st);
+  launch_batch_cols(wit, n, d_eqc.as<ef>(), B.as<ef>(), st);
+  ef alpha2 = ts.sample_ext();
+  std::vector<ef> sub(nsk);
+  {
+    const int nb = sub_eval_blocks(n, k);
+    DBuf part(sizeof(ef) * size_t(nb) * nsk * 2, st);
+    launch_sub_evals(B.as<ef>(), n, k, nullptr, eqt.as<ef>(), part.as<ef>(), st);
+    std::vector<ef> ud = reduce_to_host(ctx, part.as<ef>(), nb, nsk * 2);
+    for (int j = 0; j < nsk; j++) sub[j] = kb::ef_add(ud[2 * j], kb::ef_mul(alpha2, ud[2 * j + 1]));
+  }
+  ts.add_ext(sub.data(), sub.size());
+  std::vector<ef> eps(k);
+  for (auto& x : eps) x = ts.sample_ext();
+  std::vector<ef> point = eps;
+  point.insert(point.end(), rtail.begin(), rtail.end());
+  DBuf A(sizeof(ef) * N, st);
+  {
+    DBuf ep = eq_table_dev(ctx, point);
+    DBuf da2 = scalar_dev(ctx, alpha2);
+    launch_inner_mle(ep.as<ef>(), n, da2.as<ef>(), A.as<ef>(), st);
+  }
+  ef inner_sum = kb::ef_zero();
+  {
+    std::vector<ef> ee = eq_table_host(eps);
+    for (int j = 0; j < nsk; j++) inner_sum = kb::ef_add(inner_sum, kb::ef_mul(ee[j], sub[j]));
+  }
+  const auto basis3 = lagrange_basis(3);
+  std::vector<ef> inner_ch;
+  for (int round = 0; round < n; round++) {
+    const size_t half = N >> (round + 1);
+    const int nb = prod_blocks(half);
+    DBuf part(sizeof(ef) * size_t(nb) * 2, st);
+    launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part.as<ef>(), st);
+    std::vector<ef> s02 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
+    ef s1 = kb::ef_sub(inner_sum, s02[0]);
+    std::vector<ef> p = interpolate(basis3, {s02[0], s1, s02[1]});
+    ts.add_ext(p.data(), p.size());
+    ef c = ts.sample_ext();
+    inner_ch.push_back(c);
+    inner_sum = poly_eval(p, c);
+    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 2));
+    DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
+    DBuf dc = scalar_dev(ctx, c);
+    launch_fold2(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, dc.as<ef>(), st);
+    A = std::move(na);
+    B = std::move(nbuf);
+  }
+  ef packed_value;
+  ctx.to_host(&packed_value, B.as<ef>(), sizeof(ef));
+  A.reset();
+  B.reset();
+  std::vector<ef> final_point = cbs;
+  final_point.insert(final_point.end(), inner_ch.begin(), inner_ch.end());
+  const double t3 = now_ms();
+
+  // ---------------------------------------------------------------- 5) WHIR opening
+  {
+    // initial constraints: the commitment OOD points, then the statement
+    std::vector<std::vector<ef>> pts = ood_pts;
+    pts.push_back(final_point);
+    std::vector<ef> vals = ood_vals;
+    vals.push_back(packed_value);
+    Fu.push_back(partial_eval(final_point));
+    ef gamma = ts.sample_ext();
+    std::vector<ef> coef(pts.size());
+    ef sigma = kb::ef_zero(), cur = kb::ef_one();
+    for (size_t j = 0; j < pts.size(); j++) {
+      coef[j] = cur;
+      sigma = kb::ef_add(sigma, kb::ef_mul(cur, vals[j]));
+      cur = kb::ef_mul(cur, gamma);
+    }
+    // first folding block on the 2^lu partial evaluations
+    std::vector<std::vector<ef>> E;
+    for (auto& pt : pts) E.push_back(eq_table_host(std::vector<ef>(pt.begin(), pt.begin() + lu)));
+    std::vector<std::vector<ef>> G = Fu;
+    std::vector<ef> r0;
+    whir_sumcheck_host(ctx, ts, G, E, coef, sigma, lu, ws.fold_pow_bits, job.p16, r0);
+    // g_1 = T(r0, .), w_1 = sum_j coef_j eq(pt_j^u, r0) eq(pt_j^v, .)
+    int m = m0 - lu;
+    DBuf g(sizeof(ef) << m, st), w(sizeof(ef) << m, st);
+    {
+      DBuf er = upload(ctx, eq_table_host(r0));
+      launch_whir_fold_T(wit, t_len, lu, m, er.as<ef>(), g.as<ef>(), st);
+      WL_CUDA(cudaMemsetAsync(w.as<void>(), 0, sizeof(ef) << m, st));
+      std::vector<std::vector<ef>> pv;
+      std::vector<ef> cv;
+      for (size_t j = 0; j < pts.size(); j++) {
+        pv.emplace_back(pts[j].begin() + lu, pts[j].end());
+        cv.push_back(kb::ef_mul(coef[j], E[j][0]));
+      }
+      add_eq_ef(ctx, w.as<ef>(), m, pv, cv);
+    }
+    std::vector<ef> last_r = r0;
+    std::deque<Commitment> commits;  // stable addresses: `prev` points into it
+    const Commitment* prev = &c0;
+    for (int i = 0; i < ws.num_rounds; i++) {
+      const WhirRound& ci = ws.c[i];
+      const WhirRound& cn = ws.c[i + 1];
+      LdeSource src{g.as<uint32_t>(), size_t(8) << m, 8, m - cn.fold, cn.log_inv_rate, 128};
+      commits.push_back(commit(ctx, src, m, cn.fold, job.p24, job.p16));
+      const Commitment& cd = commits.back();
+      ts.add_base(cd.root, 8);
+      std::vector<std::vector<ef>> npts_ef;
+      std::vector<ef> nvals;
+      for (int q = 0; q < cn.ood; q++) {
+        ef z = ts.sample_ext();
+        std::vector<ef> pt = pow_point(z, m);
+        ef y = mle_eval_dev(ctx, g.as<ef>(), m, pt);
+        ts.add_ext(&y, 1);
+        npts_ef.push_back(pt);
+        nvals.push_back(y);
+      }
+      grind(ctx, ts, job.p16, ci.pow_bits);
+      std::vector<uint32_t> q = sample_queries(ts, prev->log_leaves, ci.queries);
+      auto rows = open(ctx, *prev, q, ts);
+      const uint32_t gen = kb::two_adic_gen_m(prev->log_leaves);
+      std::vector<std::vector<uint32_t>> stir_pts;
+      std::vector<ef> stir_vals;
+      for (size_t t = 0; t < q.size(); t++) {
+        uint32_t y = kb::pow_m(gen, q[t]);
+        std::vector<uint32_t> pt(m);
+        for (int b = 0; b < m; b++) { pt[b] = y; y = kb::mul(y, y); }
+        stir_pts.push_back(pt);
+        stir_vals.push_back(fold_row(rows[t], prev->fold, prev->elem, last_r));
+      }
+      ef gm = ts.sample_ext();
+      std::vector<ef> coef_ef, coef_f;
+      ef cc = kb::ef_one();
+      for (size_t t = 0; t < npts_ef.size(); t++) {
+        coef_ef.push_back(cc);
+        sigma = kb::ef_add(sigma, kb::ef_mul(cc, nvals[t]));
+        cc = kb::ef_mul(cc, gm);
+      }
+      for (size_t t = 0; t < stir_pts.size(); t++) {
+        coef_f.push_back(cc);
+        sigma = kb::ef_add(sigma, kb::ef_mul(cc, stir_vals[t]));
+        cc = kb::ef_mul(cc, gm);
+      }
+      add_eq_ef(ctx, w.as<ef>(), m, npts_ef, coef_ef);
+      add_eq_f(ctx, w.as<ef>(), m, stir_pts, coef_f);
+      last_r.clear();
+      whir_sumcheck_dev(ctx, ts, g, w, m, sigma, cn.fold, ws.fold_pow_bits, job.p16, last_r);
+      prev = &cd;
+    }
+    // final round
+    std::vector<ef> gf(size_t(1) << m), wf(size_t(1) << m);
+    ctx.to_host(gf.data(), g.as<ef>(), sizeof(ef) << m);
+    ctx.to_host(wf.data(), w.as<ef>(), sizeof(ef) << m);
+    ts.add_ext(gf.data(), gf.size());
+    const WhirRound& cl = ws.c[ws.num_rounds];
+    grind(ctx, ts, job.p16, cl.pow_bits);
+    std::vector<uint32_t> q = sample_queries(ts, prev->log_leaves, cl.queries);
+    open(ctx, *prev, q, ts);
+    std::vector<std::vector<ef>> Gf{gf}, Wf{wf};
+    std::vector<ef> fr;
+    whir_sumcheck_host(ctx, ts, Gf, Wf, {kb::ef_one()}, sigma, ws.final_vars, ws.fold_pow_bits, job.p16, fr);
+  }
+  const double t4 = now_ms();
+  if (tm) {
+    tm->commit_ms = t1 - t0;
+    tm->zerocheck_ms = t2 - t1;
+    tm->inner_ms = t3 - t2;
+    tm->whir_ms = t4 - t3;
+    tm->total_ms = t4 - t0;
+  }
+  return to_canonical(ts.proof);
+}
+
+// ------------------------------------------------------------------ a*b - c zerocheck
+std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, int k, const uint32_t* a,
+                                const uint32_t* b, const uint32_t* c, std::vector<float>* round_ms) {
+  if (k < 1 || k > 4 || k >= n) throw std::invalid_argument("skips must be in [1, 4] and below log_n");
+  cudaStream_t st = ctx.stream;
+  Transcript ts(&p16);
+  const int nsk = 1 << k;
+  const size_t S = size_t(1) << (n - k);
+  std::vector<ef> r(n + 1 - k);
+  for (auto& x : r) x = ts.sample_ext();
+  auto sel = lagrange_basis(nsk);
+  const int nz = 2 * (nsk - 1) - nsk + 1;
+  ef sum = kb::ef_zero(), mmf;
+  std::vector<ef> ch;
+  cudaEvent_t e0, e1;
+  WL_CUDA(cudaEventCreate(&e0));
+  WL_CUDA(cudaEventCreate(&e1));
+  auto tick = [&]() { WL_CUDA(cudaEventRecord(e0, st)); };
+  auto tock = [&]() {
+    WL_CUDA(cudaEventRecord(e1, st));
+    WL_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    WL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (round_ms) round_ms->push_back(ms);
+  };
+  DBuf cols;
+  {
+    tick();
+    std::vector<uint32_t> lw(size_t(nz) * nsk);
+    for (int zi = 0; zi < nz; zi++)
+      for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
+    DBuf d_lw = upload(ctx, lw);
+    DBuf eq = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1, r.end()));
+    const int nb = abc0_blocks(n, k);
+    DBuf part(sizeof(ef) * size_t(nb) * nz, st);
+    launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq.as<ef>(), part.as<ef>(), st);
+    std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
+    std::vector<ef> ys(nsk, kb::ef_zero());
+    ys.insert(ys.end(), sums.begin(), sums.end());
+    std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
+    std::vector<ef> qv(nsk);
+    for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], r[0]);
+    p = poly_mul(p, interpolate(sel, qv));
+    const int deg = 3 * (nsk - 1);
+    p.resize(deg + 1, kb::ef_zero());
+    ts.add_ext(p.data(), p.size());
+    ef c0 = ts.sample_ext();
+    ch.push_back(c0);
+    sum = poly_eval(p, c0);
+    grind(ctx, ts, p16, sumcheck_pow_bits(128, deg));
+    std::vector<ef> selr(nsk);
+    mmf = kb::ef_zero();
+    for (int i = 0; i < nsk; i++) {
+      selr[i] = upoly_eval(sel[i], c0);
+      mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
+    }
+    DBuf d_sel = upload(ctx, selr);
+    cols = DBuf(sizeof(ef) * 3 * S, st);
+    launch_abc0_fold(a, b, c, n, k, d_sel.as<ef>(), cols.as<ef>(), st);
+    tock();
+  }
+  const auto basis3 = lagrange_basis(3);
+  for (int round = 1; round <= n - k; round++) {
+    tick();
+    const int m = n - k - round + 1;
+    const size_t half = size_t(1) << (m - 1);
+    DBuf eqr = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1 + round, r.end()));
+    const int nb = (int)((half + 31) / 32);
+    DBuf part(sizeof(ef) * size_t(nb) * 2, st);
+    launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part.as<ef>(), st);
+    std::vector<ef> s2 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
+    const ef& rr = r[round];
+    ef v0 = kb::ef_mul(s2[0], mmf), v2 = kb::ef_mul(s2[1], mmf);
+    ef v1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(v0, kb::ef_sub(kb::ef_one(), rr))), kb::ef_inv(rr));
+    std::vector<ef> p = interpolate(basis3, {v0, v1, v2});
+    p = poly_mul(p, {kb::ef_sub(kb::ef_one(), rr), kb::ef_sub(kb::ef_add(rr, rr), kb::ef_one())});
+    ts.add_ext(p.data(), p.size());
+    ef cc = ts.sample_ext();
+    ch.push_back(cc);
+    sum = poly_eval(p, cc);
+    grind(ctx, ts, p16, sumcheck_pow_bits(128, 3));
+    mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), rr), kb::ef_sub(kb::ef_one(), cc)),
+                                kb::ef_mul(rr, cc)),
+                     mmf);
+    DBuf nc(sizeof(ef) * 3 * half, st);
+    DBuf dc = scalar_dev(ctx, cc);
+    launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st);
+    cols = std::move(nc);
+    tock();
+  }
+  ef fin[3];
+  ctx.to_host(fin, cols.as<ef>(), sizeof(fin));
+  ts.add_ext(fin, 3);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return to_canonical(ts.proof);
+}
+
+}  // namespace wl

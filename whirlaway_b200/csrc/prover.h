@@ -1,0 +1,73 @@
+// The GPU prover: host orchestration of the device kernels in the transcript order of
+// AirTable::prove (crates/air/src/prove.rs:49-226).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "host.h"
+#include "kernels.h"
+
+namespace wl {
+
+// Stream-ordered device buffer (pooled by the CUDA async allocator).
+class DBuf {
+ public:
+  DBuf() = default;
+  DBuf(size_t bytes, cudaStream_t s);
+  ~DBuf();
+  DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+  DBuf& operator=(DBuf&& o) noexcept;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  template <class T>
+  T* as() const { return static_cast<T*>(p_); }
+  size_t bytes() const { return bytes_; }
+  void reset();
+
+ private:
+  void* p_ = nullptr;
+  size_t bytes_ = 0;
+  cudaStream_t s_ = nullptr;
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t hbm_budget = 0;
+  uint32_t* twiddles = nullptr;  // w^j for w of order 2^24, j < 2^23
+  void* pinned = nullptr;        // staging for small device-to-host reads
+  size_t pinned_bytes = 0;
+  std::string last_error;
+  Context(int device, uint64_t budget);
+  ~Context();
+  void to_host(void* dst, const void* src, size_t bytes);
+  void to_device(void* dst, const void* src, size_t bytes);
+};
+
+struct Timings {
+  double commit_ms = 0, zerocheck_ms = 0, inner_ms = 0, whir_ms = 0, total_ms = 0;
+};
+
+struct ProofJob {
+  Settings settings;
+  int log_n = 0;
+  AirConsts air;
+  kb::P16Consts p16;
+  kb::P24Consts p24;
+};
+
+// Proves with a device-resident, Montgomery-form, column-major witness (165 columns of
+// 2^log_n values). Returns the proof in canonical form.
+std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit_dev, Timings* t);
+
+// Standalone zerocheck of eq(r, x) * (a * b - c) with a univariate skip; a, b, c device
+// Montgomery arrays of 2^log_n. Returns the proof (canonical) and per-round device times.
+std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int log_n, int skips, const uint32_t* a,
+                                const uint32_t* b, const uint32_t* c, std::vector<float>* round_ms);
+
+size_t proof_len_bound(const Settings& s, int log_n);
+
+}  // namespace wl
