@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark: Poseidon2 permutations proven per second with the B200 Whirlaway prover.
+
+A step is one plain proof of the Poseidon2-KoalaBear width-16 AIR over 2^log_n
+permutations (one per trace row; default 2^20, the plain-at-scale configuration) with the
+reference's default parameters (rate 1/2, folding 7 then 4, univariate skip 4, 128-bit
+security, 16 PoW bits). Inputs are uniform KoalaBear elements from StdRng in the
+reference's draw order (synthetic, as in the reference example).
+
+  value  throughput with the witness resident in HBM (AirTable::prove on a device witness)
+  e2e    the same through the C ABI with the witness in pinned host memory: the host-to-device
+         copy of the witness and the device-to-host copy of the proof are inside the timed region
+
+N > 1 GPUs: one process per GPU (torchrun), each proving its own independent instances
+(replicas: proofs share nothing, so there is no collective on the data path); the timed
+region is bracketed by a barrier and the maximum over ranks is reported.
+
+--impl reference runs the CPU restatement of the reference prover (the oracle; the Rust
+reference cannot be built here) with all host threads on a bounded sample of the workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Poseidon2 perms proven/sec on 1 B200 (plain single proof)"
+P24_MODMUL = 8 * 24 * 2 + 23 * (2 + 24)   # Montgomery products per Poseidon2-24 permutation
+P16_MODMUL = 8 * 16 * 2 + 20 * (2 + 16)
+ZC0_MODMUL_PER_POINT = 165 * 16 + 148 * 8 + 8 * 16 * 2 + 20 * (2 + 16)  # extension + batching + AIR
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log-n", type=int, default=20)
+    ap.add_argument("--cpu-sample-log-n", type=int, default=15,
+                    help="trace height of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(log_n):
+    return {
+        "workload": f"plain single proof, Poseidon2-KoalaBear width-16 AIR, 2^{log_n} permutations (one per row)",
+        "log_n_rows": log_n,
+        "air_columns": 165,
+        "whir": "rate 1/2, folding 7 then 4, RS domain reduction 2^5, 16 PoW bits, 128-bit CapacityBound",
+        "univariate_skips": 4,
+        "extension": "KoalaBear^8 (X^8 - 3)",
+        "inputs": "uniform KoalaBear from StdRng, reference draw order",
+        "l2": "inputs larger than L2 (witness 165 x 2^log_n x 4 B, LDE 88 x 2^(log_n+2) x 4 B)",
+        "parallelism": "replicas",
+    }
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1].split()[0]))
+                    smax.append(float(parts[2].split()[0]))
+                    power.append(float(parts[3].split()[0]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_prove_rate(log_n, steps, warmup, threads=None):
+    """The oracle (CPU restatement of the reference prover) on 2^log_n rows: perms/s."""
+    from tests import oracle_lib
+    oracle = oracle_lib.load()
+    if threads:
+        oracle.lib.wlo_set_threads(threads)
+    cores = oracle.lib.wlo_max_threads()
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    for _ in range(warmup):
+        oracle.prove(log_n, consts, wit)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        proof, _ = oracle.prove(log_n, consts, wit)
+    dt = time.perf_counter() - t0
+    assert oracle.verify(log_n, consts, proof) == 0
+    return steps * (1 << log_n) / dt, cores, dt / steps
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    log_n = min(args.cpu_sample_log_n, args.log_n)
+    rate, cores, sec = cpu_prove_rate(log_n, args.steps, args.warmup)
+    sample = (f"CPU oracle (restatement of the reference prover, {cores} threads) proving 2^{log_n} rows per step; "
+              f"{sec:.2f} s per step")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "perms/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear Montgomery)", "data": "synthetic",
+        "config": workload_config(args.log_n),
+        "cpu_baseline": {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "perms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def whir_rows_hashed(log_n):
+    """Leaf rows hashed per proof (all WHIR commitments) under the default parameters."""
+    m = log_n + 8
+    ld = m + 1
+    rows = [1 << (ld - 7)]
+    rest = m - 7
+    rounds = 0 if rest < 6 else (rest - 6 + 3) // 4
+    ld -= 5
+    m -= 7
+    for _ in range(rounds):
+        rows.append(1 << (ld - 4))
+        ld -= 1
+        m -= 4
+    return rows
+
+
+def roofline(profile, log_n, modmul_peak, hbm_peak_gbs, launches_per_step, steps):
+    """Roofline of the dominant kernel class over the timed region."""
+    name, (ms, launches) = max(profile.items(), key=lambda kv: kv[1][0])
+    N = 1 << log_n
+    rows = whir_rows_hashed(log_n)
+    per_launch_ms = ms / max(launches, 1)
+    out = {"kernel": name, "launches": launches, "avg_launch_ms": per_launch_ms,
+           "share_of_profiled_time": ms / sum(v[0] for v in profile.values())}
+    if name == "leaf_hash":
+        work = sum(rows) * 8 * P24_MODMUL * steps
+        byts = (rows[0] * (88 * 4 + 32) + sum(r * (128 * 4 + 32) for r in rows[1:])) * steps
+    elif name == "zc0_eval":
+        work = (N >> 4) * 30 * ZC0_MODMUL_PER_POINT * steps
+        byts = 165 * N * 4 * steps
+    elif name == "merkle":
+        work = sum(rows) * P16_MODMUL * steps
+        byts = sum(rows) * 2 * 32 * steps
+    else:
+        work, byts = None, None
+    if work is not None:
+        achieved = work / (ms * 1e-3) / 1e9
+        peak = modmul_peak / 1e9
+        out.update({"bound": "int", "achieved": achieved, "peak": peak, "unit": "Gmodmul/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": "measured in this run: independent Montgomery-product chains from registers",
+                    "hbm": {"achieved": byts / (ms * 1e-3) / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
+                            "frac": byts / (ms * 1e-3) / 1e9 / hbm_peak_gbs,
+                            "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+    return out
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import whirlaway_b200 as wl
+
+    torch.cuda.set_device(local)
+    log_n = args.log_n
+    ctx = wl.Context(local)
+    consts, inputs = wl.generate_workload(log_n, -1 if world == 1 else rank)
+    table = wl.AirTable(ctx, consts, log_n)
+    wit = wl.Witness.generate(ctx, consts, inputs, log_n)
+    modmul_peak, p24_peak = ctx.probe_int_peaks(consts)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    for _ in range(args.warmup):
+        table.prove_witness(wit)
+    sampler = ClockSampler(local)
+    ctx.profile(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = wl.kernel_launch_count()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        proof = table.prove_witness(wit)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(world)
+    launches = wl.kernel_launch_count() - launches0
+    elapsed_ms = dist_max(e0.elapsed_time(e1), world)
+    profile = ctx.profile_report()
+    ctx.profile(False)
+    value = args.steps * (1 << log_n) * world / (elapsed_ms * 1e-3)
+
+    # end to end through the C ABI with a pinned host witness
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(165 << log_n, dtype=torch.int32, pin_memory=True)
+        host_np = host.numpy().view(np.uint32)
+        host_np[:] = wit.download()
+        for _ in range(max(1, args.warmup // 2)):
+            table.prove(host_np)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            p2 = table.prove(host_np)
+        e1.record(stream)
+        e1.synchronize()
+        barrier(world)
+        e2e_ms = dist_max(e0.elapsed_time(e1), world)
+        assert np.array_equal(p2, proof)
+        e2e = {"value": args.steps * (1 << log_n) * world / (e2e_ms * 1e-3), "unit": "perms/s",
+               "h2d_bytes_per_step": int(host_np.nbytes), "d2h_bytes_per_step": int(p2.nbytes),
+               "ms_per_step": e2e_ms / args.steps}
+
+    if rank != 0:
+        return
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm_peak = json.load(f)["hbm_gbs"]
+    except (OSError, KeyError, ValueError):
+        hbm_peak = 6650.0
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cl = min(args.cpu_sample_log_n, log_n)
+        rate, cores, sec = cpu_prove_rate(cl, 1, 0)
+        cpu = {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port",
+               "sample": f"one CPU-oracle proof of 2^{cl} rows ({sec:.2f} s), all host threads"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "perms/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear Montgomery; exact modular integer)",
+        "data": "synthetic", "config": workload_config(log_n),
+        "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        "roofline": roofline(profile, log_n, modmul_peak, hbm_peak, None, args.steps),
+        "cpu_baseline": cpu,
+        "int_peaks": {"modmul_per_s": modmul_peak, "p24_perms_per_s": p24_peak},
+        "phases_ms": table.last_timings_ms,
+        "kernel_profile_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(profile.items(),
+                                                                                  key=lambda kv: -kv[1][0])},
+        "proof_len": int(proof.size),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -121,6 +121,20 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                        uint32_t* proof_out, size_t* proof_len, float* round_ms);
 
+/* Instrumentation (no reference counterpart; the reference profiles with tracing spans,
+ * src/examples/poseidon2.rs:91-100). With profiling on, every kernel class launched on the
+ * context is bracketed by CUDA events on the context's stream; wl_profile_json writes
+ * {"class": [total_ms, launches], ...} for everything since the last enable. */
+wl_status wl_profile_enable(wl_ctx* ctx, int32_t on);
+wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap);
+/* Measured integer-pipe ceilings on the context's device: Montgomery products per second and
+ * Poseidon2-24 permutations per second (p24 constants from a constants blob). */
+wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* modmul_per_s, double* p24_per_s);
+/* The context's CUDA stream (a cudaStream_t), for callers that time work with their own
+ * events, and the number of kernels the library has launched in this process. */
+void* wl_ctx_stream(wl_ctx* ctx);
+uint64_t wl_kernel_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                  _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
         "wl_sumcheck_abc_prove_device": (ctypes.c_int, [vp, _u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
                                                         _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
+        "wl_ctx_stream": (vp, [vp]),
+        "wl_kernel_launch_count": (ctypes.c_uint64, []),
+        "wl_profile_enable": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
+        "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -106,6 +112,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 def _ptr(a: np.ndarray):
     assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(_u32p)
+
+
+def kernel_launch_count() -> int:
+    """Kernels launched by the library in this process."""
+    return load_library().wl_kernel_launch_count()
 
 
 def air_columns() -> int:
@@ -142,6 +153,29 @@ class Context:
         if st:
             msg = self._lib.wl_last_error(self.handle).decode(errors="replace")
             raise ProverError(st, f"{what}: {msg}")
+
+    @property
+    def stream_ptr(self) -> int:
+        """Raw cudaStream_t the library launches on (for torch.cuda.ExternalStream)."""
+        return self._lib.wl_ctx_stream(self.handle) or 0
+
+    def profile(self, on: bool = True):
+        """Starts (or stops) per-kernel-class CUDA-event timing; totals restart."""
+        self.check(self._lib.wl_profile_enable(self.handle, int(on)), "profile_enable")
+
+    def profile_report(self) -> dict:
+        """{kernel class: (total ms, launches)} since profiling was enabled."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self._lib.wl_profile_json(self.handle, buf, len(buf)), "profile_json")
+        return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
+
+    def probe_int_peaks(self, constants: np.ndarray):
+        """Measured (Montgomery products/s, Poseidon2-24 permutations/s) from registers."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        c = np.ascontiguousarray(constants, dtype=np.uint32)
+        self.check(self._lib.wl_probe_int_peaks(self.handle, _ptr(c), ctypes.byref(a), ctypes.byref(b)), "probe")
+        return a.value, b.value
 
     def close(self):
         if getattr(self, "handle", None):

@@ -294,4 +294,46 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16c, int32_
   return abc_common(ctx, p16c, log_n, skips, a, b, c, true, proof_out, proof_len, round_ms);
 }
 
+wl_status wl_profile_enable(wl_ctx* ctx, int32_t on) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  return guarded(ctx, [&] {
+    ctx->c->prof_flush();
+    ctx->c->prof_totals.clear();
+    ctx->c->profile = on != 0;
+    return WL_OK;
+  });
+}
+
+wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
+  if (!ctx || !buf) return WL_E_INVALID_ARG;
+  return guarded(ctx, [&] {
+    ctx->c->prof_flush();
+    std::string js = "{";
+    bool first = true;
+    for (auto& kv : ctx->c->prof_totals) {
+      if (!first) js += ", ";
+      first = false;
+      js += "\"" + kv.first + "\": [" + std::to_string(kv.second.first) + ", " + std::to_string(kv.second.second) + "]";
+    }
+    js += "}";
+    if (js.size() + 1 > cap) return fail(ctx, WL_E_BUFFER_TOO_SMALL, "profile buffer too small");
+    memcpy(buf, js.c_str(), js.size() + 1);
+    return WL_OK;
+  });
+}
+
+wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* modmul_per_s, double* p24_per_s) {
+  if (!ctx || !constants) return WL_E_INVALID_ARG;
+  return guarded(ctx, [&] {
+    if (modmul_per_s) *modmul_per_s = wl::bench_modmul_per_s(*ctx->c);
+    if (p24_per_s)
+      *p24_per_s = wl::bench_p24_per_s(*ctx->c,
+                                       wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS));
+    return WL_OK;
+  });
+}
+
+void* wl_ctx_stream(wl_ctx* ctx) { return ctx ? (void*)ctx->c->stream : nullptr; }
+uint64_t wl_kernel_launch_count(void) { return wl::launch_counter().load(); }
+
 }  // extern "C"

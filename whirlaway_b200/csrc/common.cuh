@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstdint>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -21,7 +23,16 @@ struct CudaError : std::runtime_error {
     cudaError_t e_ = (expr);                                                 \
     if (e_ != cudaSuccess) throw ::wl::CudaError(e_, std::string(#expr)); \
   } while (0)
-#define WL_LAUNCH_CHECK() WL_CUDA(cudaGetLastError())
+// Every kernel launch in the library is followed by WL_LAUNCH_CHECK, which also counts it.
+inline std::atomic<uint64_t>& launch_counter() {
+  static std::atomic<uint64_t> n{0};
+  return n;
+}
+#define WL_LAUNCH_CHECK()                      \
+  do {                                         \
+    ::wl::launch_counter().fetch_add(1);       \
+    WL_CUDA(cudaGetLastError());               \
+  } while (0)
 
 using kb::ef;
 

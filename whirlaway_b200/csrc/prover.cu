@@ -64,10 +64,53 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
 Context::~Context() {
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
+  for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+  for (auto e : event_pool) cudaEventDestroy(e);
   cudaFree(twiddles);
   cudaFreeHost(pinned);
   cudaStreamDestroy(stream);
 }
+cudaEvent_t Context::take_event() {
+  if (!event_pool.empty()) {
+    cudaEvent_t e = event_pool.back();
+    event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  WL_CUDA(cudaEventCreate(&e));
+  return e;
+}
+void Context::prof_flush() {
+  if (pending.empty()) return;
+  WL_CUDA(cudaStreamSynchronize(stream));
+  for (auto& p : pending) {
+    float ms = 0;
+    WL_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+    auto& t = prof_totals[p.name];
+    t.first += ms;
+    t.second += 1;
+    event_pool.push_back(p.a);
+    event_pool.push_back(p.b);
+  }
+  pending.clear();
+}
+ProfScope::ProfScope(Context& ctx, const char* n) : c(ctx), name(n) {
+  if (!c.profile) return;
+  a = c.take_event();
+  WL_CUDA(cudaEventRecord(a, c.stream));
+}
+ProfScope::~ProfScope() {
+  if (!c.profile || !a) return;
+  cudaEvent_t b = nullptr;
+  try {
+    b = c.take_event();
+  } catch (...) {
+    return;
+  }
+  cudaEventRecord(b, c.stream);
+  c.pending.push_back({name, a, b});
+}
+
 void Context::to_host(void* dst, const void* src, size_t bytes) {
   char* down = static_cast<char*>(pinned) + kUpBytes;
   if (bytes <= kDownBytes) {
@@ -112,7 +155,7 @@ DBuf upload(Context& ctx, const std::vector<T>& v) {
 
 std::vector<ef> reduce_to_host(Context& ctx, const ef* partial, int nblk, int k) {
   DBuf out(sizeof(ef) * k, ctx.stream);
-  launch_reduce_partials(partial, nblk, k, out.as<ef>(), ctx.stream);
+  { ProfScope _ps(ctx, "reduce"); launch_reduce_partials(partial, nblk, k, out.as<ef>(), ctx.stream); }
   std::vector<ef> h(k);
   ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * k);
   return h;
@@ -126,7 +169,7 @@ DBuf eq_table_dev(Context& ctx, const std::vector<ef>& pt) {
     return out;
   }
   DBuf p = upload(ctx, pt);
-  launch_eq_table(p.as<ef>(), (int)pt.size(), out.as<ef>(), ctx.stream);
+  { ProfScope _ps(ctx, "eq_table"); launch_eq_table(p.as<ef>(), (int)pt.size(), out.as<ef>(), ctx.stream); }
   return out;
 }
 
@@ -141,8 +184,8 @@ void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
   for (uint64_t base = 0; base < kb::P; base += batch) {
     uint32_t init = UINT32_MAX;
     ctx.to_device(res.as<void>(), &init, 4);
-    launch_grind(p16, ts.ch.state, ts.ch.in, ts.ch.in_len, bits, (uint32_t)base, batch, res.as<uint32_t>(),
-                 ctx.stream);
+    { ProfScope _ps(ctx, "grind"); launch_grind(p16, ts.ch.state, ts.ch.in, ts.ch.in_len, bits, (uint32_t)base, batch, res.as<uint32_t>(),
+                 ctx.stream); }
     uint32_t r;
     ctx.to_host(&r, res.as<uint32_t>(), 4);
     if (r != UINT32_MAX) {
@@ -175,14 +218,14 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   if ((src.elem << fold) != 128) throw std::invalid_argument("leaf rows must hold 128 base-field values");
   const size_t rows = size_t(1) << c.log_leaves;
   c.lde = DBuf(rows * c.n_cols * sizeof(uint32_t), ctx.stream);
-  launch_lde(src, nullptr, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream);
+  { ProfScope _ps(ctx, "lde"); launch_lde(src, nullptr, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
   const int LL = c.log_leaves;
   c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
   uint32_t* t = c.tree.as<uint32_t>();
-  launch_leaf_hash(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, t, ctx.stream);
+  { ProfScope _ps(ctx, "leaf_hash"); launch_leaf_hash(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, t, ctx.stream); }
   for (int l = 1; l <= LL; l++)
-    launch_merkle_level(t + level_offset(LL, l - 1) * 8, t + level_offset(LL, l) * 8, size_t(1) << (LL - l), p16,
-                        ctx.stream);
+    { ProfScope _ps(ctx, "merkle"); launch_merkle_level(t + level_offset(LL, l - 1) * 8, t + level_offset(LL, l) * 8, size_t(1) << (LL - l), p16,
+                        ctx.stream); }
   ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
   return c;
 }
@@ -206,8 +249,8 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   DBuf dr = upload(ctx, ridx), dd = upload(ctx, didx);
   DBuf rows(sizeof(uint32_t) * c.n_cols * std::max(nq, 1), ctx.stream);
   DBuf digs(sizeof(uint32_t) * 8 * std::max<size_t>(didx.size(), 1), ctx.stream);
-  launch_gather_u32(c.lde.as<uint32_t>(), dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream);
-  launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream);
+  { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.lde.as<uint32_t>(), dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream); }
+  { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream); }
   std::vector<uint32_t> hr(size_t(c.n_cols) * nq), hd(didx.size() * 8);
   if (nq) {
     ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
@@ -274,7 +317,7 @@ void add_eq_ef(Context& ctx, ef* w, int m, const std::vector<std::vector<ef>>& p
                             cudaMemcpyDeviceToDevice, ctx.stream));
   }
   DBuf dc = upload(ctx, coefs);
-  launch_add_eq_terms_ef(w, lh, ll, np, hi.as<ef>(), lo.as<ef>(), dc.as<ef>(), ctx.stream);
+  { ProfScope _ps(ctx, "add_eq"); launch_add_eq_terms_ef(w, lh, ll, np, hi.as<ef>(), lo.as<ef>(), dc.as<ef>(), ctx.stream); }
 }
 
 // Adds sum_t coefs[t] * eq(points[t], .) for base-field points (STIR queries).
@@ -291,10 +334,10 @@ void add_eq_f(Context& ctx, ef* w, int m, const std::vector<std::vector<uint32_t
   }
   DBuf dph = upload(ctx, ph.empty() ? std::vector<uint32_t>{0} : ph), dpl = upload(ctx, pl);
   DBuf hi(sizeof(uint32_t) * (size_t(np) << lh), ctx.stream), lo(sizeof(uint32_t) * (size_t(np) << ll), ctx.stream);
-  launch_eq_table_f(dph.as<uint32_t>(), np, lh, hi.as<uint32_t>(), ctx.stream);
-  launch_eq_table_f(dpl.as<uint32_t>(), np, ll, lo.as<uint32_t>(), ctx.stream);
+  { ProfScope _ps(ctx, "eq_table"); launch_eq_table_f(dph.as<uint32_t>(), np, lh, hi.as<uint32_t>(), ctx.stream); }
+  { ProfScope _ps(ctx, "eq_table"); launch_eq_table_f(dpl.as<uint32_t>(), np, ll, lo.as<uint32_t>(), ctx.stream); }
   DBuf dc = upload(ctx, coefs);
-  launch_add_eq_terms_f(w, lh, ll, np, hi.as<uint32_t>(), lo.as<uint32_t>(), dc.as<ef>(), ctx.stream);
+  { ProfScope _ps(ctx, "add_eq"); launch_add_eq_terms_f(w, lh, ll, np, hi.as<uint32_t>(), lo.as<uint32_t>(), dc.as<ef>(), ctx.stream); }
 }
 
 // g(pt) for a device extension table g over m variables.
@@ -303,7 +346,7 @@ ef mle_eval_dev(Context& ctx, const ef* g, int m, const std::vector<ef>& pt) {
   split_vars(m, lh, ll);
   EqPair e = eq_pair(ctx, pt, lh);
   DBuf part(sizeof(ef) << lh, ctx.stream);
-  launch_mle_eval_ef(g, lh, ll, e.hi.as<ef>(), e.lo.as<ef>(), part.as<ef>(), ctx.stream);
+  { ProfScope _ps(ctx, "mle_eval"); launch_mle_eval_ef(g, lh, ll, e.hi.as<ef>(), e.lo.as<ef>(), part.as<ef>(), ctx.stream); }
   return reduce_to_host(ctx, part.as<ef>(), 1 << lh, 1)[0];
 }
 
@@ -314,7 +357,7 @@ void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, e
     size_t half = size_t(1) << (m - 1);
     int nb = whir_sc_blocks(half);
     DBuf part(sizeof(ef) * 3 * nb, ctx.stream);
-    launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part.as<ef>(), ctx.stream);
+    { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part.as<ef>(), ctx.stream); }
     std::vector<ef> h = reduce_to_host(ctx, part.as<ef>(), nb, 3);
     ts.add_ext(h.data(), 3);
     grind(ctx, ts, p16, pow_bits);
@@ -323,7 +366,7 @@ void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, e
     sigma = quad_eval(h.data(), r);
     DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
     DBuf dr = scalar_dev(ctx, r);
-    launch_fold2(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, dr.as<ef>(), ctx.stream);
+    { ProfScope _ps(ctx, "fold"); launch_fold2(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, dr.as<ef>(), ctx.stream); }
     g = std::move(ng);
     w = std::move(nw);
     m--;
@@ -420,7 +463,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     std::vector<ef> pv(pt.begin() + lu, pt.end());
     EqPair e = eq_pair(ctx, pv, lh_v);
     DBuf out(sizeof(ef) * (size_t(1) << lu) * 5, st);
-    launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st);
+    { ProfScope _ps(ctx, "whir_partial_eval"); launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st); }
     std::vector<ef> h(size_t(1) << lu);
     ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * h.size());
     return h;
@@ -470,7 +513,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     DBuf d_lw = upload(ctx, lw);
     const int nb = zc0_blocks(n, k);
     DBuf part(sizeof(ef) * size_t(nb) * nz, st);
-    launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st);
+    { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st); }
     std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
@@ -493,7 +536,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     }
     DBuf d_sel = upload(ctx, selr);
     cols = DBuf(sizeof(ef) * size_t(W) * S, st);
-    launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st);
+    { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
   }
   const auto basis4 = lagrange_basis(4);
   for (int round = 1; round <= n - k; round++) {
@@ -502,7 +545,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     DBuf eqr = eq_table_dev(ctx, std::vector<ef>(zc.begin() + 1 + round, zc.end()));
     const int nb = zc_ef_blocks(m);
     DBuf part(sizeof(ef) * size_t(nb) * 3, st);
-    launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st);
+    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st); }
     std::vector<ef> s3 = reduce_to_host(ctx, part.as<ef>(), nb, 3);
     const ef& r = zc[round];
     ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
@@ -518,7 +561,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
                      mmf);
     DBuf nc(sizeof(ef) * size_t(W) * half, st);
     DBuf dc = scalar_dev(ctx, c);
-    launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st); }
     cols = std::move(nc);
   }
   // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
@@ -532,7 +575,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     for (int i = 0; i < nsk; i++) selr[i] = upoly_eval(sel[i], challenges[0]);
     DBuf d_sel = upload(ctx, selr);
     DBuf up(sizeof(ef) * size_t(W) * (1 + nsk), st), down(sizeof(ef) * size_t(W) * (1 + nsk), st);
-    launch_inner_sums(wit, n, k, eqt.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st);
+    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, eqt.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st); }
     ctx.to_host(inner_up.data(), up.as<ef>(), sizeof(ef) * W);
     ctx.to_host(inner_down.data(), down.as<ef>(), sizeof(ef) * W);
   }
@@ -549,13 +592,13 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   eqc.resize(W);
   DBuf d_eqc = upload(ctx, eqc);
   DBuf B(sizeof(ef) * N, st);
-  launch_batch_cols(wit, n, d_eqc.as<ef>(), B.as<ef>(), st);
+  { ProfScope _ps(ctx, "batch_cols"); launch_batch_cols(wit, n, d_eqc.as<ef>(), B.as<ef>(), st); }
   ef alpha2 = ts.sample_ext();
   std::vector<ef> sub(nsk);
   {
     const int nb = sub_eval_blocks(n, k);
     DBuf part(sizeof(ef) * size_t(nb) * nsk * 2, st);
-    launch_sub_evals(B.as<ef>(), n, k, nullptr, eqt.as<ef>(), part.as<ef>(), st);
+    { ProfScope _ps(ctx, "sub_evals"); launch_sub_evals(B.as<ef>(), n, k, nullptr, eqt.as<ef>(), part.as<ef>(), st); }
     std::vector<ef> ud = reduce_to_host(ctx, part.as<ef>(), nb, nsk * 2);
     for (int j = 0; j < nsk; j++) sub[j] = kb::ef_add(ud[2 * j], kb::ef_mul(alpha2, ud[2 * j + 1]));
   }
@@ -568,7 +611,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   {
     DBuf ep = eq_table_dev(ctx, point);
     DBuf da2 = scalar_dev(ctx, alpha2);
-    launch_inner_mle(ep.as<ef>(), n, da2.as<ef>(), A.as<ef>(), st);
+    { ProfScope _ps(ctx, "inner_mle"); launch_inner_mle(ep.as<ef>(), n, da2.as<ef>(), A.as<ef>(), st); }
   }
   ef inner_sum = kb::ef_zero();
   {
@@ -581,7 +624,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     const size_t half = N >> (round + 1);
     const int nb = prod_blocks(half);
     DBuf part(sizeof(ef) * size_t(nb) * 2, st);
-    launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part.as<ef>(), st);
+    { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part.as<ef>(), st); }
     std::vector<ef> s02 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
     ef s1 = kb::ef_sub(inner_sum, s02[0]);
     std::vector<ef> p = interpolate(basis3, {s02[0], s1, s02[1]});
@@ -592,7 +635,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 2));
     DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
     DBuf dc = scalar_dev(ctx, c);
-    launch_fold2(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, dc.as<ef>(), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold2(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, dc.as<ef>(), st); }
     A = std::move(na);
     B = std::move(nbuf);
   }
@@ -631,7 +674,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     DBuf g(sizeof(ef) << m, st), w(sizeof(ef) << m, st);
     {
       DBuf er = upload(ctx, eq_table_host(r0));
-      launch_whir_fold_T(wit, t_len, lu, m, er.as<ef>(), g.as<ef>(), st);
+      { ProfScope _ps(ctx, "whir_fold_T"); launch_whir_fold_T(wit, t_len, lu, m, er.as<ef>(), g.as<ef>(), st); }
       WL_CUDA(cudaMemsetAsync(w.as<void>(), 0, sizeof(ef) << m, st));
       std::vector<std::vector<ef>> pv;
       std::vector<ef> cv;
@@ -752,7 +795,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     DBuf eq = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1, r.end()));
     const int nb = abc0_blocks(n, k);
     DBuf part(sizeof(ef) * size_t(nb) * nz, st);
-    launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq.as<ef>(), part.as<ef>(), st);
+    { ProfScope _ps(ctx, "abc0_eval"); launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq.as<ef>(), part.as<ef>(), st); }
     std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
@@ -775,7 +818,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     }
     DBuf d_sel = upload(ctx, selr);
     cols = DBuf(sizeof(ef) * 3 * S, st);
-    launch_abc0_fold(a, b, c, n, k, d_sel.as<ef>(), cols.as<ef>(), st);
+    { ProfScope _ps(ctx, "abc0_fold"); launch_abc0_fold(a, b, c, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
     tock();
   }
   const auto basis3 = lagrange_basis(3);
@@ -786,7 +829,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     DBuf eqr = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1 + round, r.end()));
     const int nb = (int)((half + 31) / 32);
     DBuf part(sizeof(ef) * size_t(nb) * 2, st);
-    launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part.as<ef>(), st);
+    { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part.as<ef>(), st); }
     std::vector<ef> s2 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
     const ef& rr = r[round];
     ef v0 = kb::ef_mul(s2[0], mmf), v2 = kb::ef_mul(s2[1], mmf);
@@ -803,7 +846,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
                      mmf);
     DBuf nc(sizeof(ef) * 3 * half, st);
     DBuf dc = scalar_dev(ctx, cc);
-    launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st); }
     cols = std::move(nc);
     tock();
   }

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "host.h"
@@ -45,6 +47,27 @@ struct Context {
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
   void to_device(void* dst, const void* src, size_t bytes);
+
+  // Optional per-kernel-class timing with CUDA events on `stream`.
+  bool profile = false;
+  struct Pending {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::map<std::string, std::pair<double, long>> prof_totals;  // name -> (ms, launches)
+  cudaEvent_t take_event();
+  void prof_flush();  // resolves pending events (synchronises the stream)
+};
+
+// Scoped timer of one kernel class (no-op unless ctx.profile).
+struct ProfScope {
+  Context& c;
+  const char* name;
+  cudaEvent_t a = nullptr;
+  ProfScope(Context& ctx, const char* n);
+  ~ProfScope();
 };
 
 struct Timings {
@@ -69,5 +92,10 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int log_
                                 const uint32_t* b, const uint32_t* c, std::vector<float>* round_ms);
 
 size_t proof_len_bound(const Settings& s, int log_n);
+
+// Throughput probes used as measured compute peaks: Montgomery products per second and
+// Poseidon2-24 permutations per second, both from registers (no memory traffic).
+double bench_modmul_per_s(Context& ctx);
+double bench_p24_per_s(Context& ctx, const kb::P24Consts& c);
 
 }  // namespace wl
