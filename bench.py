@@ -130,13 +130,20 @@ def dist_setup(args):
 
 
 def dist_max(value, world):
+    """Maximum of a per-rank value over all ranks (the job time of a replica run)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_input_seed(world, rank):
+    """Input stream of a replica: the reference's single stream alone, one seed per rank otherwise."""
+    return -1 if world == 1 else rank
 
 
 def barrier(world):
@@ -238,7 +245,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     log_n = args.log_n
     ctx = wl.Context(local)
-    consts, inputs = wl.generate_workload(log_n, -1 if world == 1 else rank)
+    consts, inputs = wl.generate_workload(log_n, replica_input_seed(world, rank))
     table = wl.AirTable(ctx, consts, log_n)
     wit = wl.Witness.generate(ctx, consts, inputs, log_n)
     modmul_peak, p24_peak = ctx.probe_int_peaks(consts)

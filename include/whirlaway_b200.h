@@ -121,6 +121,30 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                        uint32_t* proof_out, size_t* proof_len, float* round_ms);
 
+/* Serving and batching (no counterpart in the reference, which proves one instance at a time
+ * in src/examples/poseidon2.rs:153-174). A server runs `workers` proofs concurrently on one
+ * device, each worker on its own stream; queued jobs are admitted first-in first-out when a
+ * worker is idle and the job's estimated device footprint (wl_proof_footprint_bytes) fits in
+ * the remaining HBM budget. A job is the reference example's input: a constants blob, 2^log_n
+ * rows of 16 inputs (copied at submission) and settings; the server generates the trace on
+ * the GPU and proves it with its own transcript, so the proof equals wl_prove's for the same
+ * witness. Tickets are thread-safe to submit, poll and wait on. */
+typedef struct wl_server wl_server;
+typedef enum { WL_JOB_QUEUED = 0, WL_JOB_RUNNING = 1, WL_JOB_DONE = 2, WL_JOB_FAILED = 3 } wl_job_state;
+uint64_t wl_proof_footprint_bytes(int32_t log_n);
+wl_status wl_server_create(int32_t device, int32_t workers, uint64_t hbm_budget_bytes, wl_server** out);
+void wl_server_destroy(wl_server* server); /* finishes queued and running jobs first */
+const char* wl_server_last_error(const wl_server* server);
+wl_status wl_server_submit(wl_server* server, const wl_air_settings* settings, const uint32_t* constants,
+                           int32_t log_n, const uint32_t* inputs, uint64_t* ticket);
+wl_status wl_server_poll(wl_server* server, uint64_t ticket, int32_t* state);
+/* Blocks until the job ends. On success copies the proof (WL_E_BUFFER_TOO_SMALL keeps the
+ * result and reports the length) and releases the ticket. times_ms (may be NULL): queued,
+ * running, submit-to-finish latency. */
+wl_status wl_server_wait(wl_server* server, uint64_t ticket, uint32_t* proof_out, size_t* proof_len,
+                         double* times_ms);
+wl_status wl_server_stats(wl_server* server, uint64_t* peak_bytes_admitted, int32_t* peak_running);
+
 /* Instrumentation (no reference counterpart; the reference profiles with tracing spans,
  * src/examples/poseidon2.rs:91-100). With profiling on, every kernel class launched on the
  * context is bracketed by CUDA events on the context's stream; wl_profile_json writes

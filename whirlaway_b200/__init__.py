@@ -96,6 +96,15 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                         _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
         "wl_ctx_stream": (vp, [vp]),
         "wl_kernel_launch_count": (ctypes.c_uint64, []),
+        "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
+        "wl_server_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]),
+        "wl_server_destroy": (None, [vp]),
+        "wl_server_last_error": (ctypes.c_char_p, [vp]),
+        "wl_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+        "wl_server_poll": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]),
+        "wl_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, _u32p, _sizep, ctypes.POINTER(ctypes.c_double)]),
+        "wl_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32)]),
         "wl_profile_enable": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
@@ -292,3 +301,80 @@ def sumcheck_abc_prove(ctx: Context, p16_constants: np.ndarray, log_n: int, skip
                                        ctypes.byref(n), ms)
     ctx.check(st, "sumcheck_abc_prove")
     return out[: n.value].copy(), list(ms)
+
+
+def proof_footprint_bytes(log_n: int) -> int:
+    """Device bytes the server reserves for one proof of 2^log_n rows."""
+    return load_library().wl_proof_footprint_bytes(log_n)
+
+
+class Server:
+    """Concurrent proving on one device: `workers` proofs in flight, FIFO admission by
+    estimated HBM footprint against `hbm_budget_bytes` (0: unbounded)."""
+
+    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, device: int = 0, workers: int = 8, hbm_budget_bytes: int = 0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        st = self._lib.wl_server_create(device, workers, hbm_budget_bytes, ctypes.byref(h))
+        if st:
+            raise ProverError(st, f"wl_server_create(device={device}, workers={workers})")
+        self.handle = h
+
+    def _check(self, st, what):
+        if st:
+            raise ProverError(st, f"{what}: {self._lib.wl_server_last_error(self.handle).decode(errors='replace')}")
+
+    def submit(self, constants: np.ndarray, inputs: np.ndarray, log_n: int, settings: AirSettings = AirSettings()):
+        t = ctypes.c_uint64()
+        c = np.ascontiguousarray(constants, dtype=np.uint32)
+        i = np.ascontiguousarray(inputs, dtype=np.uint32)
+        if i.size != 16 << log_n:
+            raise ValueError("inputs must hold 16 values per row")
+        self._check(self._lib.wl_server_submit(self.handle, ctypes.byref(settings._c()), _ptr(c), log_n, _ptr(i),
+                                               ctypes.byref(t)), "submit")
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        s = ctypes.c_int32()
+        self._check(self._lib.wl_server_poll(self.handle, ticket, ctypes.byref(s)), "poll")
+        return s.value
+
+    def wait(self, ticket: int, log_n: int, settings: AirSettings = AirSettings()):
+        """Blocks until done; returns (proof, {queued_ms, run_ms, latency_ms})."""
+        cap = proof_len_bound(settings, log_n)
+        out = np.zeros(cap, np.uint32)
+        n = ctypes.c_size_t(cap)
+        tm = (ctypes.c_double * 3)()
+        self._check(self._lib.wl_server_wait(self.handle, ticket, _ptr(out), ctypes.byref(n), tm), "wait")
+        return out[: n.value].copy(), {"queued_ms": tm[0], "run_ms": tm[1], "latency_ms": tm[2]}
+
+    def stats(self):
+        b, r = ctypes.c_uint64(), ctypes.c_int32()
+        self._check(self._lib.wl_server_stats(self.handle, ctypes.byref(b), ctypes.byref(r)), "stats")
+        return {"peak_bytes_admitted": b.value, "peak_running": r.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.wl_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def batch_prove(server: Server, jobs, settings: AirSettings = AirSettings()):
+    """Proves independent jobs [(constants, inputs, log_n), ...] concurrently; returns the
+    proofs in job order."""
+    tickets = [server.submit(c, i, n, settings) for c, i, n in jobs]
+    return [server.wait(t, n, settings)[0] for t, (_, _, n) in zip(tickets, jobs)]

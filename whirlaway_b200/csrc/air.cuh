@@ -49,9 +49,9 @@ __host__ __device__ __forceinline__ void air_trace_row(const AirConsts& K, const
   }
 #pragma unroll 1
   for (int r = 0; r < 20; r++) {
-    s[0] = kb::cube(kb::add(s[0], K.partial[r]));
-    out[size_t(col++) * stride] = s[0];
-    kb::internal_layer<16>(s);
+    const uint32_t x0 = kb::cube(kb::add(s[0], K.partial[r]));
+    out[size_t(col++) * stride] = x0;
+    kb::internal_layer_with0<16>(s, x0);
   }
 #pragma unroll 1
   for (int r = 0; r < 4; r++) {
@@ -91,11 +91,10 @@ __device__ __forceinline__ void air_eval_f(const AirConsts& K, Get&& get, Acc&& 
   for (int r4 = 0; r4 < 20; r4 += 4) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      s[0] = kb::cube(kb::add(s[0], K.partial[r4 + q]));
-      uint32_t p = get(col++);
-      acc(kb::sub(s[0], p), 64 + r4 + q);
-      s[0] = p;
-      kb::internal_layer<16>(s);
+      const uint32_t x0 = kb::cube(kb::add(s[0], K.partial[r4 + q]));
+      const uint32_t p = get(col++);
+      acc(kb::sub(x0, p), 64 + r4 + q);
+      kb::internal_layer_with0<16>(s, p);
     }
     flush();
   }

@@ -6,9 +6,14 @@
 
 #include "../../include/whirlaway_b200.h"
 #include "prover.h"
+#include "server.h"
 
 struct wl_ctx {
   std::unique_ptr<wl::Context> c;
+  std::string err;
+};
+struct wl_server {
+  std::unique_ptr<wl::Server> s;
   std::string err;
 };
 struct wl_witness {
@@ -331,6 +336,102 @@ wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* mod
                                        wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS));
     return WL_OK;
   });
+}
+
+uint64_t wl_proof_footprint_bytes(int32_t log_n) { return wl::proof_footprint_bytes(log_n); }
+
+wl_status wl_server_create(int32_t device, int32_t workers, uint64_t budget, wl_server** out) {
+  if (!out || workers < 1 || workers > 64) return WL_E_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return WL_E_CUDA;
+  }
+  if (device < 0 || device >= count) return WL_E_INVALID_ARG;
+  try {
+    auto* s = new wl_server;
+    s->s = std::make_unique<wl::Server>(device, workers, budget);
+    *out = s;
+    return WL_OK;
+  } catch (const wl::CudaError& e) {
+    cudaGetLastError();
+    return e.code == cudaErrorMemoryAllocation ? WL_E_OOM : WL_E_CUDA;
+  } catch (...) {
+    return WL_E_INTERNAL;
+  }
+}
+
+void wl_server_destroy(wl_server* s) { delete s; }
+
+const char* wl_server_last_error(const wl_server* s) { return s ? s->err.c_str() : "no server"; }
+
+static wl_status server_fail(wl_server* s, wl_status st, const std::string& m) {
+  if (s) s->err = m;
+  return st;
+}
+
+wl_status wl_server_submit(wl_server* s, const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
+                           const uint32_t* inputs, uint64_t* ticket) {
+  if (!s || !constants || !inputs || !ticket) return server_fail(s, WL_E_INVALID_ARG, "NULL argument");
+  std::string why;
+  if (!settings_ok(settings, log_n, why)) return server_fail(s, WL_E_INVALID_ARG, why);
+  try {
+    wl::ServeJob job;
+    job.settings = to_settings(settings);
+    job.log_n = log_n;
+    job.constants.assign(constants, constants + wl::N_CONSTS);
+    job.inputs.assign(inputs, inputs + (size_t(16) << log_n));
+    *ticket = s->s->submit(std::move(job));
+    return WL_OK;
+  } catch (const std::invalid_argument& e) {
+    return server_fail(s, WL_E_BUDGET, e.what());
+  } catch (const std::exception& e) {
+    return server_fail(s, WL_E_INTERNAL, e.what());
+  }
+}
+
+wl_status wl_server_poll(wl_server* s, uint64_t ticket, int32_t* state) {
+  if (!s || !state) return WL_E_INVALID_ARG;
+  try {
+    *state = (int32_t)s->s->poll(ticket);
+    return WL_OK;
+  } catch (const std::exception& e) {
+    return server_fail(s, WL_E_INVALID_ARG, e.what());
+  }
+}
+
+wl_status wl_server_wait(wl_server* s, uint64_t ticket, uint32_t* proof_out, size_t* proof_len, double* times_ms) {
+  if (!s || !proof_len) return WL_E_INVALID_ARG;
+  try {
+    wl::ServeResult r = s->s->wait(ticket, false);
+    if (times_ms) {
+      times_ms[0] = r.start_ms - r.submit_ms;
+      times_ms[1] = r.end_ms - r.start_ms;
+      times_ms[2] = r.end_ms - r.submit_ms;
+    }
+    if (r.state == wl::JOB_FAILED) {
+      s->s->release(ticket);
+      return server_fail(s, WL_E_INTERNAL, r.error);
+    }
+    if (!proof_out || *proof_len < r.proof.size()) {
+      *proof_len = r.proof.size();
+      return server_fail(s, WL_E_BUFFER_TOO_SMALL, "proof buffer too small");
+    }
+    memcpy(proof_out, r.proof.data(), r.proof.size() * 4);
+    *proof_len = r.proof.size();
+    s->s->release(ticket);
+    return WL_OK;
+  } catch (const std::exception& e) {
+    return server_fail(s, WL_E_INVALID_ARG, e.what());
+  }
+}
+
+wl_status wl_server_stats(wl_server* s, uint64_t* peak_bytes, int32_t* peak_running) {
+  if (!s) return WL_E_INVALID_ARG;
+  if (peak_bytes) *peak_bytes = s->s->peak_in_use();
+  if (peak_running) *peak_running = s->s->peak_running();
+  return WL_OK;
 }
 
 void* wl_ctx_stream(wl_ctx* ctx) { return ctx ? (void*)ctx->c->stream : nullptr; }

@@ -25,23 +25,66 @@ constexpr int NTT_THREADS = 512;
 // Shared-memory tile: CT columns of 2^B points, column-major with one word of padding.
 __device__ __forceinline__ uint32_t sidx(uint32_t col, uint32_t i, int B) { return col * ((1u << B) + 1) + i; }
 
-// One fused Moebius + DIT stage on local bit tl. The twiddle exponent of a pair is its
-// global index modulo 2^(t-1): lo_global plus the local bits below tl shifted by lo_bits.
-__device__ __forceinline__ void butterfly_stage(uint32_t* sm, int B, int tl, int t, uint32_t lo_global, int lo_bits,
-                                                const uint32_t* __restrict__ tw) {
-  const uint32_t hl = 1u << tl;
-  const uint32_t npairs = 1u << (B - 1);
-  for (uint32_t bf = threadIdx.x; bf < (uint32_t)CT * npairs; bf += blockDim.x) {
-    uint32_t col = bf / npairs, m = bf % npairs;
-    uint32_t a = ((m >> tl) << (tl + 1)) | (m & (hl - 1));
-    uint32_t twi = lo_global + ((m & (hl - 1)) << lo_bits);
-    uint32_t w = tw[twi << (24 - t)];
-    uint32_t ia = sidx(col, a, B), ib = sidx(col, a + hl, B);
-    uint32_t u = sm[ia], v = sm[ib];
-    v = kb::sub(v, u);
-    uint32_t wv = kb::mul(w, v);
-    sm[ia] = kb::add(u, wv);
-    sm[ib] = kb::sub(u, wv);
+// Per-block twiddle table: for local bit tl (global stage t = tl + 1 + lo_bits) the 2^tl
+// factors w_{2^t}^(lo_global + (m << lo_bits)), m < 2^tl, at offset 2^tl - 1.
+__device__ __forceinline__ void load_twiddles(uint32_t* tab, int B, int tl0, uint32_t lo_global, int lo_bits,
+                                              const uint32_t* __restrict__ tw) {
+  for (uint32_t e = threadIdx.x; e < (1u << B) - 1; e += blockDim.x) {
+    const int tl = 31 - __clz(e + 1);  // e + 1 in [2^tl, 2^(tl+1))
+    if (tl < tl0) continue;
+    const uint32_t m = e + 1 - (1u << tl);
+    const int t = tl + 1 + lo_bits;
+    tab[e] = tw[(lo_global + (m << lo_bits)) << (24 - t)];
+  }
+}
+
+// Fused Moebius + DIT butterfly on (u, v) with twiddle w.
+__device__ __forceinline__ void bfly(uint32_t& u, uint32_t& v, uint32_t w) {
+  const uint32_t d = kb::mul(w, kb::sub(v, u));
+  v = kb::sub(u, d);
+  u = kb::add(u, d);
+}
+
+// Stages on local bits [tl0, tl1) of the 2^B points of CT columns in shared memory: two
+// bits per shared-memory round trip (radix 4), a final single bit if the count is odd.
+__device__ __forceinline__ void run_stages(uint32_t* sm, const uint32_t* tab, int B, int tl0, int tl1) {
+  const uint32_t npts = 1u << B;
+  int tl = tl0;
+  for (; tl + 1 < tl1; tl += 2) {
+    const uint32_t h = 1u << tl;
+    const uint32_t ngroups = npts >> 2;
+    for (uint32_t g = threadIdx.x; g < (uint32_t)CT * ngroups; g += blockDim.x) {
+      const uint32_t col = g / ngroups, q = g % ngroups;
+      const uint32_t r = q & (h - 1);
+      const uint32_t a = ((q >> tl) << (tl + 2)) | r;
+      uint32_t* base = sm + sidx(col, a, B);
+      uint32_t x0 = base[0], x1 = base[h], x2 = base[2 * h], x3 = base[3 * h];
+      const uint32_t w1 = tab[h - 1 + r];
+      bfly(x0, x1, w1);
+      bfly(x2, x3, w1);
+      bfly(x0, x2, tab[2 * h - 1 + r]);
+      bfly(x1, x3, tab[2 * h - 1 + h + r]);
+      base[0] = x0;
+      base[h] = x1;
+      base[2 * h] = x2;
+      base[3 * h] = x3;
+    }
+    __syncthreads();
+  }
+  if (tl < tl1) {
+    const uint32_t h = 1u << tl;
+    const uint32_t npairs = npts >> 1;
+    for (uint32_t g = threadIdx.x; g < (uint32_t)CT * npairs; g += blockDim.x) {
+      const uint32_t col = g / npairs, m = g % npairs;
+      const uint32_t r = m & (h - 1);
+      const uint32_t a = ((m >> tl) << (tl + 1)) | r;
+      uint32_t* base = sm + sidx(col, a, B);
+      uint32_t x0 = base[0], x1 = base[h];
+      bfly(x0, x1, tab[h - 1 + r]);
+      base[0] = x0;
+      base[h] = x1;
+    }
+    __syncthreads();
   }
 }
 
@@ -49,10 +92,12 @@ __device__ __forceinline__ void butterfly_stage(uint32_t* sm, int B, int tl, int
 // realises the zero-padded stages 1..rho as copies; then stages rho+1..B.
 __global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, const uint32_t* __restrict__ tw) {
   extern __shared__ uint32_t sm[];
+  uint32_t* tab = sm + CT * ((1u << B) + 1);
   const int tile = blockIdx.y;
   const size_t i0 = size_t(blockIdx.x) << B;
   const uint32_t npts = 1u << B;
   const size_t col_block = size_t(in.elem) << in.L;
+  load_twiddles(tab, B, in.rho, 0, 0, tw);
   for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
     uint32_t col, il;
     if (in.elem == 1) { il = idx % npts; col = idx / npts; }
@@ -63,10 +108,7 @@ __global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, con
     sm[sidx(col, il, B)] = (gcol < (uint32_t)in.n_cols && addr < in.src_len) ? in.src[addr] : 0u;
   }
   __syncthreads();
-  for (int t = in.rho + 1; t <= B; t++) {
-    butterfly_stage(sm, B, t - 1, t, 0, 0, tw);
-    __syncthreads();
-  }
+  if (in.rho < B) run_stages(sm, tab, B, in.rho, B);
   for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
     uint32_t col = idx % CT, il = idx / CT;
     uint32_t gcol = tile * CT + col;
@@ -79,11 +121,14 @@ __global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, con
 __global__ void k_ntt_mid(uint32_t* __restrict__ data, int n_cols, int B0, int Bp, int rho,
                           const uint32_t* __restrict__ tw) {
   extern __shared__ uint32_t sm[];
+  uint32_t* tab = sm + CT * ((1u << Bp) + 1);
   const int tile = blockIdx.y;
   const size_t g = blockIdx.x;
   const uint32_t lo = uint32_t(g & ((size_t(1) << B0) - 1));
   const size_t hi = g >> B0;
   auto row_of = [&](uint32_t j) -> size_t { return lo + (size_t(j) << B0) + (hi << (B0 + Bp)); };
+  const int tl0 = rho > B0 ? rho - B0 : 0;
+  load_twiddles(tab, Bp, tl0, lo, B0, tw);
   const uint32_t npts = 1u << Bp;
   for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
     uint32_t col = idx % CT, j = idx / CT;
@@ -91,12 +136,7 @@ __global__ void k_ntt_mid(uint32_t* __restrict__ data, int n_cols, int B0, int B
     sm[sidx(col, j, Bp)] = gcol < (uint32_t)n_cols ? data[row_of(j) * n_cols + gcol] : 0u;
   }
   __syncthreads();
-  for (int tl = 0; tl < Bp; tl++) {
-    int t = B0 + 1 + tl;
-    if (t <= rho) continue;
-    butterfly_stage(sm, Bp, tl, t, lo, B0, tw);
-    __syncthreads();
-  }
+  if (tl0 < Bp) run_stages(sm, tab, Bp, tl0, Bp);
   for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
     uint32_t col = idx % CT, j = idx / CT;
     uint32_t gcol = tile * CT + col;
@@ -118,56 +158,101 @@ __global__ void k_twiddles(uint32_t* tw, uint32_t w24) {
   if (j < (1u << 23)) tw[j] = pow_dev(w24, j);
 }
 
-constexpr int LEAF_ROWS = 64;
+constexpr int LEAF_ROWS = 128;
 constexpr int LEAF_PAD = 129;
+constexpr int SUBTREE_LEVELS = 7;  // levels folded per pass (2^7 digests per block)
 
-__global__ void k_leaf_hash(const uint32_t* __restrict__ lde, size_t rows, int n_cols, int log_elem,
-                            const __grid_constant__ kb::P24Consts c, uint32_t* __restrict__ dig) {
-  __shared__ uint32_t sm[LEAF_ROWS * LEAF_PAD];
+// Tree layout: level l (2^(LL-l) digests of 8 words) starts at digest offset
+// 2^(LL+1) - 2^(LL+1-l).
+__device__ __forceinline__ size_t tree_off(int LL, int l) {
+  return (size_t(1) << (LL + 1)) - (size_t(1) << (LL + 1 - l));
+}
+
+// `d` holds cnt digests of level l0 whose first global index is `first`; compresses
+// `levels` levels in shared memory and writes every new level to the tree.
+__device__ __forceinline__ void subtree_reduce(uint32_t (*d)[8], int cnt, int levels, uint32_t* __restrict__ tree,
+                                               int LL, int l0, size_t first, const kb::P16Consts& c) {
+  for (int lev = 1; lev <= levels; lev++) {
+    const int m = cnt >> lev;
+    const int t = threadIdx.x;
+    uint32_t st[16];
+    const bool act = t < m;
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        st[i] = d[2 * t][i];
+        st[8 + i] = d[2 * t + 1][i];
+      }
+      kb::p2_permute<16>(st, c);
+    }
+    __syncthreads();
+    if (act) {
+      uint32_t* o = tree + (tree_off(LL, l0 + lev) + (first >> lev) + t) * 8;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        d[t][i] = st[i];
+        o[i] = st[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Leaf digests of 128 rows per block (the row is Moebius-transformed over the position
+// bits of its column index first), then the first levels of the tree above them.
+__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, size_t rows, int n_cols,
+                                                         int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                         const __grid_constant__ kb::P16Consts c16,
+                                                         uint32_t* __restrict__ tree, int LL, int levels) {
+  extern __shared__ uint32_t sm[];
   const size_t row0 = size_t(blockIdx.x) * LEAF_ROWS;
+  const int nrows = (rows - row0) < size_t(LEAF_ROWS) ? int(rows - row0) : LEAF_ROWS;
   for (uint32_t idx = threadIdx.x; idx < LEAF_ROWS * 128; idx += blockDim.x) {
     uint32_t r = idx / 128, col = idx % 128;
-    size_t row = row0 + r;
-    sm[r * LEAF_PAD + col] = (col < (uint32_t)n_cols && row < rows) ? lde[row * n_cols + col] : 0u;
+    sm[r * LEAF_PAD + col] = (col < (uint32_t)n_cols && (int)r < nrows) ? lde[(row0 + r) * n_cols + col] : 0u;
   }
   __syncthreads();
   const int t = threadIdx.x;
-  if (t >= LEAF_ROWS || row0 + t >= rows) return;
-  uint32_t* r = sm + t * LEAF_PAD;
-  for (int b = log_elem; b < 7; b++) {
-    int h = 1 << b;
-    for (int i = 0; i < 128; i++)
-      if (!(i & h)) r[i + h] = kb::sub(r[i + h], r[i]);
-  }
   uint32_t st[24];
+  if (t < nrows) {
+    uint32_t* r = sm + t * LEAF_PAD;
+    for (int b = log_elem; b < 7; b++) {
+      const int h = 1 << b;
+      for (int i = 0; i < 128; i++)
+        if (!(i & h)) r[i + h] = kb::sub(r[i + h], r[i]);
+    }
 #pragma unroll
-  for (int i = 0; i < 24; i++) st[i] = 0;
+    for (int i = 0; i < 24; i++) st[i] = 0;
 #pragma unroll 1
-  for (int ch = 0; ch < 8; ch++) {
+    for (int ch = 0; ch < 8; ch++) {
 #pragma unroll
-    for (int i = 0; i < 16; i++) st[i] = r[ch * 16 + i];
-    kb::p2_permute<24>(st, c);
+      for (int i = 0; i < 16; i++) st[i] = r[ch * 16 + i];
+      kb::p2_permute<24>(st, c);
+    }
+    uint32_t* o = tree + (row0 + t) * 8;
+#pragma unroll
+    for (int i = 0; i < 8; i++) o[i] = st[i];
   }
-  uint32_t* o = dig + (row0 + t) * 8;
+  __syncthreads();
+  uint32_t(*d)[8] = reinterpret_cast<uint32_t(*)[8]>(sm);
+  if (t < nrows) {
 #pragma unroll
-  for (int i = 0; i < 8; i++) o[i] = st[i];
+    for (int i = 0; i < 8; i++) d[t][i] = st[i];
+  }
+  __syncthreads();
+  subtree_reduce(d, nrows, levels, tree, LL, 0, row0, c16);
 }
 
-__global__ void k_merkle_level(const uint32_t* __restrict__ child, uint32_t* __restrict__ parent, size_t n,
-                               const __grid_constant__ kb::P16Consts c) {
-  size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t st[16];
-  const uint4* src = reinterpret_cast<const uint4*>(child + i * 16);
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    uint4 v = src[q];
-    st[4 * q] = v.x; st[4 * q + 1] = v.y; st[4 * q + 2] = v.z; st[4 * q + 3] = v.w;
-  }
-  kb::p2_permute<16>(st, c);
-  uint4* dst = reinterpret_cast<uint4*>(parent + i * 8);
-  dst[0] = make_uint4(st[0], st[1], st[2], st[3]);
-  dst[1] = make_uint4(st[4], st[5], st[6], st[7]);
+// Levels l0+1 .. l0+levels from 2^levels level-l0 digests per block.
+__global__ void k_merkle_subtree(uint32_t* __restrict__ tree, int LL, int l0, int levels,
+                                 const __grid_constant__ kb::P16Consts c) {
+  __shared__ uint32_t d[1 << SUBTREE_LEVELS][8];
+  const int cnt = 1 << levels;
+  const size_t first = size_t(blockIdx.x) * cnt;
+  const uint32_t* src = tree + (tree_off(LL, l0) + first) * 8;
+  for (int i = threadIdx.x; i < cnt * 8; i += blockDim.x) d[i / 8][i % 8] = src[i];
+  __syncthreads();
+  subtree_reduce(d, cnt, levels, tree, LL, l0, first, c);
 }
 
 __global__ void k_gather(const uint32_t* __restrict__ src, const uint64_t* __restrict__ idx, int width, int n,
@@ -241,36 +326,36 @@ void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_
   if (T > 2 * MAXB || T > 24) throw std::runtime_error("LDE size beyond two shared-memory passes");
   const int tiles = (in.n_cols + CT - 1) / CT;
   const int B0 = T <= MAXB ? T : (T + 1) / 2;
-  const size_t smem_max = size_t(CT) * ((1u << MAXB) + 1) * 4;
-  static bool attr_set = false;
-  if (!attr_set) {
-    WL_CUDA(cudaFuncSetAttribute(k_ntt_first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-    WL_CUDA(cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-    attr_set = true;
-  }
+  const size_t smem_max = (size_t(CT) * ((1u << MAXB) + 1) + (1u << MAXB)) * 4;
+  WL_CUDA(cudaFuncSetAttribute(k_ntt_first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+  WL_CUDA(cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
   dim3 g1((unsigned)(size_t(1) << (T - B0)), tiles);
-  k_ntt_first<<<g1, NTT_THREADS, size_t(CT) * ((1u << B0) + 1) * 4, s>>>(in, B0, out, tw);
+  k_ntt_first<<<g1, NTT_THREADS, (size_t(CT) * ((1u << B0) + 1) + (1u << B0)) * 4, s>>>(in, B0, out, tw);
   WL_LAUNCH_CHECK();
   if (B0 < T) {
     const int Bp = T - B0;
     dim3 g2((unsigned)(size_t(1) << (T - Bp)), tiles);
-    k_ntt_mid<<<g2, NTT_THREADS, size_t(CT) * ((1u << Bp) + 1) * 4, s>>>(out, in.n_cols, B0, Bp, in.rho, tw);
+    k_ntt_mid<<<g2, NTT_THREADS, (size_t(CT) * ((1u << Bp) + 1) + (1u << Bp)) * 4, s>>>(out, in.n_cols, B0, Bp, in.rho,
+                                                                                        tw);
     WL_LAUNCH_CHECK();
   }
 }
 
-void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
-                      uint32_t* digests, cudaStream_t s) {
-  int log_elem = elem == 8 ? 3 : 0;
-  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), 128, 0, s>>>(lde, rows, n_cols, log_elem, p24,
-                                                                            digests);
+void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
+                        const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s) {
+  const int log_elem = elem == 8 ? 3 : 0;
+  const size_t smem = size_t(LEAF_ROWS) * LEAF_PAD * 4;
+  WL_CUDA(cudaFuncSetAttribute(k_leaf_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int first_levels = LL < SUBTREE_LEVELS ? LL : SUBTREE_LEVELS;
+  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, smem, s>>>(lde, rows, n_cols, log_elem, p24,
+                                                                                     p16, tree, LL, first_levels);
   WL_LAUNCH_CHECK();
-}
-
-void launch_merkle_level(const uint32_t* child, uint32_t* parent, size_t n, const kb::P16Consts& p16,
-                         cudaStream_t s) {
-  k_merkle_level<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(child, parent, n, p16);
-  WL_LAUNCH_CHECK();
+  for (int l0 = first_levels; l0 < LL; l0 += SUBTREE_LEVELS) {
+    const int lv = (LL - l0) < SUBTREE_LEVELS ? (LL - l0) : SUBTREE_LEVELS;
+    const unsigned blocks = 1u << (LL - l0 - lv);
+    k_merkle_subtree<<<blocks, 1 << (lv - 1), 0, s>>>(tree, LL, l0, lv, p16);
+    WL_LAUNCH_CHECK();
+  }
 }
 
 void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s) {

@@ -70,57 +70,88 @@ __global__ void k_reduce_partials(const ef* __restrict__ partial, int nblk, int 
 }
 
 // ------------------------------------------------------------------ AIR zerocheck
-constexpr int ZC0_X = 32, ZC0_Z = 10;
+constexpr int ZC0_X = 32, ZC0_Z = 15;
+constexpr int ZC0_STAGES = 4;   // columns in flight
+constexpr int ZC0_PAD = 20;     // words per x in a staged column tile (16 values + padding)
 
-// Thread (x, z): the up columns are extended from their values at j * 2^(n-k) + x,
-// j < 2^k, to the point z by the Lagrange weights lw[z]; the batched constraint over
-// those values is weighted by eq[x]. One warp holds 32 consecutive x for one z.
-__global__ void __launch_bounds__(ZC0_X * ZC0_Z) k_zc0_eval(const uint32_t* __restrict__ wit, int log_n, int k,
-                                                            int nz, const uint32_t* __restrict__ lw,
-                                                            const ef* __restrict__ eq,
-                                                            const ef* __restrict__ alphas_g,
-                                                            const __grid_constant__ AirConsts K,
-                                                            ef* __restrict__ partial) {
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Thread (x, z): the up columns are extended from their values at j * 2^(n-k) + x, j < 2^k,
+// to the point z by the Lagrange weights L_j(z); the batched constraint over those values is
+// weighted by eq[x]. A warp holds 32 consecutive x for one z. The 2^k x 32 values of each
+// column are staged in shared memory by a cp.async pipeline (the constraint reads columns
+// 1..164 in increasing order, each exactly once), so the extension reads shared memory only.
+__global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                               int nz, const uint32_t* __restrict__ lw,
+                                                               const ef* __restrict__ eq,
+                                                               const ef* __restrict__ alphas_g,
+                                                               const __grid_constant__ AirConsts K,
+                                                               ef* __restrict__ partial) {
   __shared__ ef alphas[AIR_NC];
-  __shared__ uint32_t w_s[ZC0_Z * 16];
+  __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_X * ZC0_PAD];
   const int tid = threadIdx.y * ZC0_X + threadIdx.x;
-  for (int i = tid; i < AIR_NC; i += ZC0_X * ZC0_Z) alphas[i] = alphas_g[i];
+  constexpr int NT = ZC0_X * ZC0_Z;
+  for (int i = tid; i < AIR_NC; i += NT) alphas[i] = alphas_g[i];
   const int zi = blockIdx.y * ZC0_Z + threadIdx.y;
   const int nsk = 1 << k;
-  for (int i = tid; i < ZC0_Z * nsk; i += ZC0_X * ZC0_Z) {
-    int zz = blockIdx.y * ZC0_Z + i / nsk;
-    w_s[i] = zz < nz ? lw[zz * nsk + i % nsk] : 0u;
-  }
-  __syncthreads();
   const size_t N = size_t(1) << log_n;
   const size_t S = N >> k;
-  const size_t x = size_t(blockIdx.x) * ZC0_X + threadIdx.x;
-  const uint32_t* wz = w_s + threadIdx.y * nsk;
-  const bool active = zi < nz && x < S;
+  const size_t x0 = size_t(blockIdx.x) * ZC0_X;
+  const size_t x = x0 + threadIdx.x;
+  uint32_t w[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) w[j] = (zi < nz && j < nsk) ? lw[zi * nsk + j] : 0u;
+
+  // producer: column c's tile -> slot, tile[slot][xl * PAD + j] = up_c[j * S + x0 + xl]
+  auto issue = [&](int c) {
+    if (c < AIR_W) {
+      uint32_t* dst = tile[c % ZC0_STAGES];
+      const uint32_t* col = wit + size_t(c) * N;
+      for (int idx = tid; idx < 16 * ZC0_X; idx += NT) {
+        const int j = idx / ZC0_X, xl = idx % ZC0_X;
+        if (j < nsk) {
+          size_t xx = x0 + xl;
+          if (xx >= S) xx = 0;
+          cp_async4(dst + xl * ZC0_PAD + j, col + up_row(size_t(j) * S + xx, N));
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  for (int c = 1; c < 1 + ZC0_STAGES - 1; c++) issue(c);
+  int next = ZC0_STAGES;  // next column to prefetch
   auto get = [&](int c) -> uint32_t {
-    const uint32_t* col = wit + size_t(c) * N;
+    cp_async_wait<ZC0_STAGES - 2>();
+    __syncthreads();
+    issue(next++);
+    const uint4* row = reinterpret_cast<const uint4*>(tile[c % ZC0_STAGES] + threadIdx.x * ZC0_PAD);
     uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-      if (j < nsk) {
-        size_t row = up_row(size_t(j) * S + x, N);
-        uint64_t t = wmul(wz[j], col[row]);
-        if ((j & 3) == 0) s0 += t;
-        else if ((j & 3) == 1) s1 += t;
-        else if ((j & 3) == 2) s2 += t;
-        else s3 += t;
+    for (int q = 0; q < 4; q++) {
+      if (4 * q < nsk) {
+        uint4 v = row[q];
+        s0 += wmul(w[4 * q], v.x);
+        s1 += wmul(w[4 * q + 1], v.y);
+        s2 += wmul(w[4 * q + 2], v.z);
+        s3 += wmul(w[4 * q + 3], v.w);
       }
     }
     return add(add(redc(s0), redc(s1)), add(redc(s2), redc(s3)));
   };
+  __syncthreads();  // alphas
   EfMacF m;
   m.init();
-  ef res = ef_zero();
-  if (active) {
-    air_eval_f(
-        K, get, [&](uint32_t h, int i) { m.mac(alphas[i], h); }, [&]() { m.flush(); });
-    res = ef_mul(m.acc, eq[x]);
-  }
+  air_eval_f(
+      K, get, [&](uint32_t h, int i) { m.mac(alphas[i], h); }, [&]() { m.flush(); });
+  cp_async_wait<0>();
+  const bool active = zi < nz && x < S;
+  ef res = active ? ef_mul(m.acc, eq[x]) : ef_zero();
   res = warp_reduce_ef(res);
   if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
 }
@@ -146,35 +177,149 @@ __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, c
   out[size_t(c) * S + x] = m.acc;
 }
 
-constexpr int ZCE_X = 32;
+constexpr int ZCE_T = 128;  // (x, z) points per block
 
-// Rounds >= 1: thread (x, z) with z in {0, 2, 3} (index zi = 0, 1, 2).
-__global__ void __launch_bounds__(ZCE_X * 3) k_zc_eval_ef(const ef* __restrict__ cols, int m,
-                                                          const ef* __restrict__ eq,
-                                                          const ef* __restrict__ alphas_g,
-                                                          const __grid_constant__ AirConsts K,
-                                                          ef* __restrict__ partial) {
-  __shared__ ef alphas[AIR_NC];
-  const int tid = threadIdx.y * ZCE_X + threadIdx.x;
-  for (int i = tid; i < AIR_NC; i += ZCE_X * 3) alphas[i] = alphas_g[i];
+// The 16 extension-field state words of each thread live in shared memory as two planes
+// of uint4 (coordinates 0-3 and 4-7), so that a warp's 128-bit accesses are conflict-free.
+struct SmemState {
+  uint4* p0;
+  uint4* p1;
+  int t;
+  __device__ __forceinline__ ef get(int i) const {
+    uint4 a = p0[i * ZCE_T + t], b = p1[i * ZCE_T + t];
+    return ef{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
+  }
+  __device__ __forceinline__ void set(int i, const ef& v) const {
+    p0[i * ZCE_T + t] = make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]);
+    p1[i * ZCE_T + t] = make_uint4(v.c[4], v.c[5], v.c[6], v.c[7]);
+  }
+};
+
+__device__ __forceinline__ ef ef_diag16(int i, const ef& a) {
+  ef r;
+#pragma unroll
+  for (int k = 0; k < 8; k++) r.c[k] = p2_diag_mul<16>(i, a.c[k]);
+  return r;
+}
+
+__device__ void mds_light_smem(const SmemState& S) {
+#pragma unroll 1
+  for (int c = 0; c < 16; c += 4) {
+    ef x0 = S.get(c), x1 = S.get(c + 1), x2 = S.get(c + 2), x3 = S.get(c + 3);
+    ef t01 = ef_add(x0, x1), t23 = ef_add(x2, x3), t0123 = ef_add(t01, t23);
+    ef t01123 = ef_add(t0123, x1), t01233 = ef_add(t0123, x3);
+    S.set(c + 3, ef_add(t01233, ef_add(x0, x0)));
+    S.set(c + 1, ef_add(t01123, ef_add(x2, x2)));
+    S.set(c, ef_add(t01123, t01));
+    S.set(c + 2, ef_add(t01233, t23));
+  }
+#pragma unroll 1
+  for (int k = 0; k < 4; k++) {
+    ef a = S.get(k), b = S.get(4 + k), c = S.get(8 + k), d = S.get(12 + k);
+    ef sk = ef_add(ef_add(a, b), ef_add(c, d));
+    S.set(k, ef_add(a, sk));
+    S.set(4 + k, ef_add(b, sk));
+    S.set(8 + k, ef_add(c, sk));
+    S.set(12 + k, ef_add(d, sk));
+  }
+}
+
+// Internal layer with lane 0 replaced by x0.
+__device__ void internal_layer_smem_with0(const SmemState& S, const ef& x0) {
+  ef sum = x0;
+#pragma unroll 1
+  for (int i = 1; i < 16; i++) sum = ef_add(sum, S.get(i));
+  S.set(0, ef_add(ef_diag16(0, x0), sum));
+#pragma unroll 1
+  for (int i = 1; i < 16; i++) S.set(i, ef_add(ef_diag16(i, S.get(i)), sum));
+}
+
+constexpr int ZCE_SEGMENTS = 9;
+
+// Rounds >= 1. Block (x range, z, segment), z = 0, 2, 3 for blockIdx.y = 0, 1, 2. The 148
+// constraints split into 9 independent segments: the 4 beginning full rounds (each starts
+// from committed columns), the 20 partial rounds, and the 4 ending full rounds; the first
+// ending round starts from the state after the partial rounds, which is linear in the
+// committed columns (internal layers only). Each thread evaluates one segment at one
+// (x, z), so a point's work is spread over 9 threads; the per-segment sums add up in the
+// partial reduction. Loops stay rolled (small code) and the state lives in shared memory.
+__global__ void __launch_bounds__(ZCE_T) k_zc_eval_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
+                                                     const ef* __restrict__ alphas_g,
+                                                     const __grid_constant__ AirConsts K, ef* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  ef* alphas = reinterpret_cast<ef*>(smraw);
+  uint4* planes = reinterpret_cast<uint4*>(smraw + sizeof(ef) * AIR_NC);
+  for (int i = threadIdx.x; i < AIR_NC; i += ZCE_T) alphas[i] = alphas_g[i];
+  const SmemState S{planes, planes + 16 * ZCE_T, (int)threadIdx.x};
   __syncthreads();
   const size_t len = size_t(1) << m, half = len >> 1;
-  const size_t x = size_t(blockIdx.x) * ZCE_X + threadIdx.x;
-  const int zi = threadIdx.y;
-  ef res = ef_zero();
-  if (x < half) {
-    auto get = [&](int c) -> ef {
-      const ef lo = cols[size_t(c) * len + x];
-      const ef hi = cols[size_t(c) * len + half + x];
-      if (zi == 0) return lo;
-      ef d = ef_sub(hi, lo);
-      ef v = ef_add(hi, d);             // z = 2: 2 hi - lo
-      return zi == 1 ? v : ef_add(v, d);  // z = 3: 3 hi - 2 lo
-    };
-    res = ef_mul(air_eval_ef(K, alphas, get), eq[x]);
+  const size_t x = size_t(blockIdx.x) * ZCE_T + threadIdx.x;
+  const int zi = blockIdx.y, seg = blockIdx.z;
+  const size_t xs = x < half ? x : 0;
+  auto get = [&](int c) -> ef {
+    const ef lo = cols[size_t(c) * len + xs];
+    if (zi == 0) return lo;
+    const ef hi = cols[size_t(c) * len + half + xs];
+    ef d = ef_sub(hi, lo);
+    ef v = ef_add(hi, d);               // z = 2: 2 hi - lo
+    return zi == 1 ? v : ef_add(v, d);  // z = 3: 3 hi - 2 lo
+  };
+  ef acc = ef_zero();
+  if (seg == 4) {
+#pragma unroll 1
+    for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
+#pragma unroll 1
+    for (int r = 0; r < 20; r++) {
+      const ef x0 = ef_cube(ef_add_f(S.get(0), K.partial[r]));
+      const ef p = get(81 + r);
+      acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(x0, p)));
+      internal_layer_smem_with0(S, p);
+    }
+  } else {
+    const uint32_t* rc;
+    int post, cidx;
+    if (seg < 4) {
+      rc = K.begin[seg];
+      post = 17 + 16 * seg;
+      cidx = 16 * seg;
+      const int src = seg == 0 ? 1 : post - 16;
+#pragma unroll 1
+      for (int i = 0; i < 16; i++) S.set(i, get(src + i));
+      if (seg == 0) mds_light_smem(S);
+    } else {
+      const int e = seg - 5;
+      rc = K.end[e];
+      post = 101 + 16 * e;
+      cidx = 84 + 16 * e;
+      if (e == 0) {
+#pragma unroll 1
+        for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
+#pragma unroll 1
+        for (int r = 0; r < 20; r++) internal_layer_smem_with0(S, get(81 + r));
+      } else {
+#pragma unroll 1
+        for (int i = 0; i < 16; i++) S.set(i, get(post - 16 + i));
+      }
+    }
+#pragma unroll 1
+    for (int i = 0; i < 16; i++) S.set(i, ef_cube(ef_add_f(S.get(i), rc[i])));
+    mds_light_smem(S);
+#pragma unroll 1
+    for (int i = 0; i < 16; i++) {
+      const ef p = get(post + i);
+      acc = ef_add(acc, ef_mul(alphas[cidx + i], ef_sub(S.get(i), p)));
+    }
   }
+  ef res = x < half ? ef_mul(acc, eq[x]) : ef_zero();
   res = warp_reduce_ef(res);
-  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 3 + zi] = res;
+  __shared__ ef wsum[ZCE_T / 32];
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = res;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ef tot = wsum[0];
+    for (int w = 1; w < ZCE_T / 32; w++) tot = ef_add(tot, wsum[w]);
+    partial[(size_t(blockIdx.x) * ZCE_SEGMENTS + seg) * 3 + zi] = tot;
+  }
 }
 
 __global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, const ef* __restrict__ r) {
@@ -419,13 +564,16 @@ void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* o
   k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
-int zc_ef_blocks(int m) {
+int zc_ef_blocks(int m) {  // partial sums per z (blocks x segments)
   size_t half = size_t(1) << (m - 1);
-  return (int)((half + ZCE_X - 1) / ZCE_X);
+  return (int)((half + ZCE_T - 1) / ZCE_T) * ZCE_SEGMENTS;
 }
 void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const AirConsts& K, ef* partial,
                        cudaStream_t s) {
-  k_zc_eval_ef<<<zc_ef_blocks(m), dim3(ZCE_X, 3), 0, s>>>(cols, m, eq, alphas, K, partial);
+  const size_t smem = sizeof(ef) * AIR_NC + sizeof(uint4) * 2 * 16 * ZCE_T;
+  WL_CUDA(cudaFuncSetAttribute(k_zc_eval_ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned xb = (unsigned)(zc_ef_blocks(m) / ZCE_SEGMENTS);
+  k_zc_eval_ef<<<dim3(xb, 3, ZCE_SEGMENTS), ZCE_T, smem, s>>>(cols, m, eq, alphas, K, partial);
   WL_LAUNCH_CHECK();
 }
 void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s) {

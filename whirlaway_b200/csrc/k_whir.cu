@@ -34,16 +34,28 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
     for (uint32_t vlo = threadIdx.x; vlo < nlo; vlo += blockDim.x) {
       EfMacF m[J];
       for (int j = 0; j < J; j++) m[j].init();
-      int cnt = 0;
-      for (uint32_t vh = h0; vh < h1; vh++) {
+      uint32_t vh = h0;
+      for (; vh + 4 <= h1; vh += 4) {  // four loads in flight per thread
+        uint32_t t[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          size_t idx = base + (size_t(vh + q) << ll) + vlo;
+          t[q] = idx < t_len ? T[idx] : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+          for (int j = 0; j < J; j++) m[j].mac(hi[size_t(j) * nhi + vh + q], t[q]);
+#pragma unroll
+        for (int j = 0; j < J; j++) m[j].flush();
+      }
+      for (; vh < h1; vh++) {
         size_t idx = base + (size_t(vh) << ll) + vlo;
         uint32_t t = idx < t_len ? T[idx] : 0u;
 #pragma unroll
-        for (int j = 0; j < J; j++) m[j].mac(hi[size_t(j) * nhi + vh], t);
-        if (++cnt == 4) {
-#pragma unroll
-          for (int j = 0; j < J; j++) m[j].flush();
-          cnt = 0;
+        for (int j = 0; j < J; j++) {
+          m[j].mac(hi[size_t(j) * nhi + vh], t);
+          m[j].flush();
         }
       }
 #pragma unroll

@@ -31,13 +31,22 @@ KB_HD uint32_t umulhi(uint32_t a, uint32_t b) {
 #endif
 }
 
+KB_HD uint32_t umin(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return ::min(a, b);
+#else
+  return a < b ? a : b;
+#endif
+}
+// For a, b < p: a + b - p wraps above a + b exactly when a + b < p, so the unsigned
+// minimum selects the reduced sum (and likewise for the difference).
 KB_HD uint32_t add(uint32_t a, uint32_t b) {
   uint32_t r = a + b;
-  return r >= P ? r - P : r;
+  return umin(r, r - P);
 }
 KB_HD uint32_t sub(uint32_t a, uint32_t b) {
   uint32_t r = a - b;
-  return a < b ? r + P : r;
+  return umin(r, r + P);
 }
 KB_HD uint32_t neg(uint32_t a) { return a ? P - a : 0; }
 KB_HD uint32_t dbl(uint32_t a) { return add(a, a); }
@@ -48,7 +57,7 @@ KB_HD uint32_t mul(uint32_t a, uint32_t b) {
   uint32_t m = lo * PINV;
   uint32_t mh = umulhi(m, P);
   uint32_t r = hi - mh;
-  return hi < mh ? r + P : r;
+  return hi < mh ? r + P : r;  // measured faster than the unsigned-min form for products
 }
 
 // Montgomery reduction of a lazily accumulated sum t < 4p^2 (at most four products).
@@ -56,10 +65,20 @@ KB_HD uint32_t redc(uint64_t t) {
   uint32_t lo = uint32_t(t), hi = uint32_t(t >> 32);
   uint32_t m = lo * PINV;
   uint32_t mh = umulhi(m, P);
-  uint32_t r = hi - mh;
-  if (hi < mh) return r + P;
-  return r >= P ? r - P : r;
+  uint32_t r = hi - mh;  // in (-p, 2p): 3p > 2^32, so the sign needs the comparison
+  r = hi < mh ? r + P : r;
+  return umin(r, r - P);
 }
+// x * 2^-k for 1 <= k <= 31 (Montgomery form is preserved): REDC(x * 2^(32 - k)).
+KB_HD uint32_t mul_inv_pow2(uint32_t x, int k) {
+  uint64_t t = uint64_t(x) << (32 - k);
+  uint32_t lo = uint32_t(t), hi = uint32_t(t >> 32);
+  uint32_t m = lo * PINV;
+  uint32_t mh = umulhi(m, P);
+  uint32_t r = hi - mh;
+  return umin(r, r + P);
+}
+KB_HD uint32_t halve(uint32_t x) { return (x & 1) ? (x >> 1) + ((P + 1) >> 1) : (x >> 1); }
 KB_HD uint64_t wmul(uint32_t a, uint32_t b) { return uint64_t(a) * b; }
 
 KB_HD uint32_t to_mont(uint32_t x) { return mul(x % P, R2_MOD_P); }

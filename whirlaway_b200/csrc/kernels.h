@@ -30,13 +30,13 @@ struct LdeSource {
 void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_t* twiddles, cudaStream_t s);
 // Twiddle table: tw[j] = w^j, w of order 2^24, j < 2^23.
 void launch_twiddles(uint32_t* tw, cudaStream_t s);
-// Leaf digests of rows of `row_cols` (= 128) values, of which the first `n_cols` are
-// stored; the row is Moebius-transformed over the bits [log2(elem), 7) of the column index
-// before hashing.
-void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
-                      uint32_t* digests, cudaStream_t s);
-void launch_merkle_level(const uint32_t* child, uint32_t* parent, size_t n_parent, const kb::P16Consts& p16,
-                         cudaStream_t s);
+// Merkle tree over the rows of an LDE matrix (rows of 128 values, the first `n_cols`
+// stored): leaf digests (each row Moebius-transformed over the bits [log2(elem), 7) of the
+// column index, then PaddingFreeSponge over Poseidon2-24) and 2-to-1 compressions
+// (Poseidon2-16), written level by level into `tree` (level l at digest offset
+// 2^(LL+1) - 2^(LL+1-l), LL = log2(rows)).
+void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
+                        const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s);
 // Gathers rows (raw, `n_cols` stored columns, zero padded to 128) and digests.
 void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s);
 

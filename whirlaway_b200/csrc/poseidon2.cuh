@@ -83,6 +83,51 @@ KB_HD constexpr uint32_t p2_diag(int i) {
   }
 }
 
+// v * x for the diagonal entry v = V_i, using doublings, halvings and shifted reductions
+// instead of a general product; equal to mul(x, p2_diag<W>(i)).
+template <int W>
+KB_HD uint32_t p2_diag_mul(int i, uint32_t x) {
+  switch (i) {
+    case 0: return neg(dbl(x));
+    case 1: return x;
+    case 2: return dbl(x);
+    case 3: return halve(x);
+    case 4: return add(dbl(x), x);
+    case 5: return dbl(dbl(x));
+    case 6: return neg(halve(x));
+    case 7: return neg(add(dbl(x), x));
+    case 8: return neg(dbl(dbl(x)));
+    case 9: return mul_inv_pow2(x, 8);
+    default: break;
+  }
+  if (W == 16) {
+    switch (i) {
+      case 10: return mul_inv_pow2(x, 3);
+      case 11: return mul_inv_pow2(x, 24);
+      case 12: return neg(mul_inv_pow2(x, 8));
+      case 13: return neg(mul_inv_pow2(x, 3));
+      case 14: return neg(mul_inv_pow2(x, 4));
+      default: return neg(mul_inv_pow2(x, 24));
+    }
+  }
+  switch (i) {
+    case 10: return mul_inv_pow2(x, 2);
+    case 11: return mul_inv_pow2(x, 3);
+    case 12: return mul_inv_pow2(x, 4);
+    case 13: return mul_inv_pow2(x, 5);
+    case 14: return mul_inv_pow2(x, 6);
+    case 15: return mul_inv_pow2(x, 24);
+    case 16: return neg(mul_inv_pow2(x, 8));
+    case 17: return neg(mul_inv_pow2(x, 3));
+    case 18: return neg(mul_inv_pow2(x, 4));
+    case 19: return neg(mul_inv_pow2(x, 5));
+    case 20: return neg(mul_inv_pow2(x, 6));
+    case 21: return neg(mul_inv_pow2(x, 7));
+    case 22: return neg(mul_inv_pow2(x, 9));
+    default: return neg(mul_inv_pow2(x, 24));
+  }
+}
+
 template <int W>
 struct P2Consts {
   static constexpr int RP = W == 16 ? 20 : 23;
@@ -92,6 +137,16 @@ struct P2Consts {
 };
 using P16Consts = P2Consts<16>;
 using P24Consts = P2Consts<24>;
+
+// Pairwise (depth log2 N) sum; the modular additions do not reassociate on their own.
+template <int N>
+KB_HD uint32_t tree_sum(const uint32_t* v) {
+  if constexpr (N == 1) {
+    return v[0];
+  } else {
+    return add(tree_sum<N / 2>(v), tree_sum<N - N / 2>(v + N / 2));
+  }
+}
 
 template <int W>
 KB_HD void mds_light(uint32_t* s) {
@@ -108,21 +163,27 @@ KB_HD void mds_light(uint32_t* s) {
   uint32_t sums[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    sums[k] = s[k];
+    uint32_t v[W / 4];
 #pragma unroll
-    for (int j = 4 + k; j < W; j += 4) sums[k] = add(sums[k], s[j]);
+    for (int j = 0; j < W / 4; j++) v[j] = s[4 * j + k];
+    sums[k] = tree_sum<W / 4>(v);
   }
 #pragma unroll
   for (int i = 0; i < W; i++) s[i] = add(s[i], sums[i & 3]);
 }
 
+// Internal layer applied to the state with s[0] replaced by x0 (the S-box output of a
+// partial round); the sum of the other lanes does not wait for the S-box.
+template <int W>
+KB_HD void internal_layer_with0(uint32_t* s, uint32_t x0) {
+  const uint32_t sum = add(tree_sum<W - 1>(s + 1), x0);
+  s[0] = add(p2_diag_mul<W>(0, x0), sum);
+#pragma unroll
+  for (int i = 1; i < W; i++) s[i] = add(p2_diag_mul<W>(i, s[i]), sum);
+}
 template <int W>
 KB_HD void internal_layer(uint32_t* s) {
-  uint32_t sum = s[0];
-#pragma unroll
-  for (int i = 1; i < W; i++) sum = add(sum, s[i]);
-#pragma unroll
-  for (int i = 0; i < W; i++) s[i] = add(mul(s[i], p2_diag<W>(i)), sum);
+  internal_layer_with0<W>(s, s[0]);
 }
 
 template <int W>
@@ -135,10 +196,7 @@ KB_HD void p2_permute(uint32_t* s, const P2Consts<W>& c) {
     mds_light<W>(s);
   }
 #pragma unroll 1
-  for (int r = 0; r < P2Consts<W>::RP; r++) {
-    s[0] = cube(add(s[0], c.internal[r]));
-    internal_layer<W>(s);
-  }
+  for (int r = 0; r < P2Consts<W>::RP; r++) internal_layer_with0<W>(s, cube(add(s[0], c.internal[r])));
 #pragma unroll 1
   for (int r = 0; r < 4; r++) {
 #pragma unroll

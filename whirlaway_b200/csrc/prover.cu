@@ -180,7 +180,7 @@ DBuf scalar_dev(Context& ctx, const ef& v) { return upload(ctx, std::vector<ef>{
 void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
   if (bits <= 0) return;
   DBuf res(sizeof(uint32_t), ctx.stream);
-  const uint32_t batch = 1u << 20;
+  const uint32_t batch = 1u << std::min(22, bits + 3);
   for (uint64_t base = 0; base < kb::P; base += batch) {
     uint32_t init = UINT32_MAX;
     ctx.to_device(res.as<void>(), &init, 4);
@@ -222,10 +222,7 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   const int LL = c.log_leaves;
   c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
   uint32_t* t = c.tree.as<uint32_t>();
-  { ProfScope _ps(ctx, "leaf_hash"); launch_leaf_hash(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, t, ctx.stream); }
-  for (int l = 1; l <= LL; l++)
-    { ProfScope _ps(ctx, "merkle"); launch_merkle_level(t + level_offset(LL, l - 1) * 8, t + level_offset(LL, l) * 8, size_t(1) << (LL - l), p16,
-                        ctx.stream); }
+  { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_tree(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, p16, t, LL, ctx.stream); }
   ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
   return c;
 }

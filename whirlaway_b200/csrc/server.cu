@@ -1,0 +1,155 @@
+// Batched / served proving (see server.h).
+#include <chrono>
+
+#include "server.h"
+
+namespace wl {
+
+namespace {
+double steady_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+uint64_t proof_footprint_bytes(int log_n) {
+  const uint64_t N = uint64_t(1) << log_n;
+  uint64_t b = 0;
+  b += uint64_t(AIR_W) * N * 4;         // witness
+  b += 88ull * 4 * N * 4;               // first commitment: LDE (88 stored columns, rate 1/2, fold 2^7)
+  b += 2ull * 4 * N * 32;               // its Merkle tree
+  b += uint64_t(AIR_W) * (N / 16) * 32 * 3 / 2;  // zerocheck fold buffers (double-buffered)
+  b += 3ull * N * 32;                   // inner sumcheck tables (eq, A, B)
+  b += 2ull * 2 * N * 32 * 2;           // WHIR g / w and their folds
+  b += 128ull * N * 4 + 2ull * N * 32;  // second commitment and its tree
+  b += 16ull << 20;                     // inputs, small tables, pool rounding
+  return b;
+}
+
+Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), budget_(hbm_budget) {
+  if (workers < 1) throw std::invalid_argument("a server needs at least one worker");
+  for (int i = 0; i < workers; i++) contexts_.push_back(std::make_unique<Context>(device, hbm_budget));
+  for (int i = 0; i < workers; i++) threads_.emplace_back([this, i] { worker_main(i); });
+}
+
+Server::~Server() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  cv_work_.notify_all();
+  for (auto& t : threads_) t.join();
+}
+
+uint64_t Server::submit(ServeJob job) {
+  const uint64_t fp = proof_footprint_bytes(job.log_n);
+  std::lock_guard<std::mutex> lk(mu_);
+  if (budget_ && fp > budget_) throw std::invalid_argument("proof footprint exceeds the HBM budget");
+  uint64_t t = next_ticket_++;
+  ServeResult r;
+  r.state = JOB_QUEUED;
+  r.submit_ms = steady_ms();
+  r.footprint = fp;
+  results_[t] = std::move(r);
+  jobs_[t] = std::move(job);
+  queue_.push_back(t);
+  cv_work_.notify_all();
+  return t;
+}
+
+JobState Server::poll(uint64_t ticket) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = results_.find(ticket);
+  if (it == results_.end()) throw std::invalid_argument("unknown ticket");
+  return it->second.state;
+}
+
+ServeResult Server::wait(uint64_t ticket, bool rel) {
+  std::unique_lock<std::mutex> lk(mu_);
+  if (results_.find(ticket) == results_.end()) throw std::invalid_argument("unknown ticket");
+  cv_done_.wait(lk, [&] {
+    JobState s = results_[ticket].state;
+    return s == JOB_DONE || s == JOB_FAILED;
+  });
+  ServeResult r = results_[ticket];
+  if (rel) results_.erase(ticket);
+  return r;
+}
+
+void Server::release(uint64_t ticket) {
+  std::lock_guard<std::mutex> lk(mu_);
+  results_.erase(ticket);
+}
+
+void Server::worker_main(int idx) {
+  Context& ctx = *contexts_[idx];
+  WL_CUDA(cudaSetDevice(device_));
+  for (;;) {
+    uint64_t ticket = 0;
+    ServeJob job;
+    uint64_t fp = 0;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      // FIFO admission: the head job starts once its footprint fits the remaining budget.
+      cv_work_.wait(lk, [&] {
+        if (stop_) return true;
+        if (queue_.empty()) return false;
+        uint64_t need = results_[queue_.front()].footprint;
+        return budget_ == 0 || in_use_ + need <= budget_ || running_ == 0;
+      });
+      if (stop_ && queue_.empty()) return;
+      if (stop_ && !queue_.empty()) {
+        // drain: keep serving until the queue is empty
+      }
+      ticket = queue_.front();
+      queue_.pop_front();
+      job = std::move(jobs_[ticket]);
+      jobs_.erase(ticket);
+      fp = results_[ticket].footprint;
+      in_use_ += fp;
+      running_++;
+      uint64_t cur = in_use_;
+      if (cur > peak_in_use_.load()) peak_in_use_.store(cur);
+      if (running_ > peak_running_.load()) peak_running_.store(running_);
+      results_[ticket].state = JOB_RUNNING;
+      results_[ticket].start_ms = steady_ms();
+    }
+    std::vector<uint32_t> proof;
+    std::string err;
+    bool ok = true;
+    try {
+      ProofJob pj;
+      pj.settings = job.settings;
+      pj.log_n = job.log_n;
+      pj.air = air_consts_from(job.constants.data());
+      pj.p16 = perm_consts_from<16>(job.constants.data() + N_AIR_CONSTS);
+      pj.p24 = perm_consts_from<24>(job.constants.data() + N_AIR_CONSTS + N_P16_CONSTS);
+      const size_t n_in = size_t(16) << job.log_n;
+      DBuf din(n_in * 4, ctx.stream);
+      WL_CUDA(cudaMemcpyAsync(din.as<void>(), job.inputs.data(), n_in * 4, cudaMemcpyHostToDevice, ctx.stream));
+      DBuf wit((size_t(AIR_W) << job.log_n) * 4, ctx.stream);
+      launch_trace_gen(din.as<uint32_t>(), pj.air, wit.as<uint32_t>(), job.log_n, ctx.stream);
+      din.reset();
+      proof = prove_air(ctx, pj, wit.as<uint32_t>(), nullptr);
+      wit.reset();
+      WL_CUDA(cudaStreamSynchronize(ctx.stream));
+    } catch (const std::exception& e) {
+      ok = false;
+      err = e.what();
+      cudaGetLastError();
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      in_use_ -= fp;
+      running_--;
+      ServeResult& r = results_[ticket];
+      r.end_ms = steady_ms();
+      r.state = ok ? JOB_DONE : JOB_FAILED;
+      r.proof = std::move(proof);
+      r.error = err;
+    }
+    cv_done_.notify_all();
+    cv_work_.notify_all();
+  }
+}
+
+}  // namespace wl
