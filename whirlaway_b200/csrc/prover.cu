@@ -563,7 +563,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   }
   // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
   // The zerocheck's returned challenges replace the eq challenges from here on
-  // (crates/air/src/prove.rs:109 rebinds zerocheck_challenges).
+  // (crates/air/src/prove.rs:114 rebinds zerocheck_challenges).
   std::vector<ef> inner_up(W), inner_down(W);
   const std::vector<ef> rtail(challenges.begin() + 1, challenges.end());
   DBuf eqt = eq_table_dev(ctx, rtail);
