@@ -35,6 +35,7 @@ typedef enum {
   WL_E_BUFFER_TOO_SMALL = 4,
   WL_E_INTERNAL = 5,
   WL_E_BUDGET = 6,
+  WL_E_SCRATCH_LIMIT = 7, /* problem larger than the fixed scratch of the allocation-free entry point */
   /* verifier outcomes, mirroring AirVerifError (crates/air/src/verify.rs:26-34) */
   WL_E_INVALID_PCS_COMMITMENT = 11,
   WL_E_INVALID_PCS_OPENING = 12,
@@ -120,6 +121,22 @@ wl_status wl_sumcheck_abc_prove(wl_ctx* ctx, const uint32_t* p16_constants, int3
 wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constants, int32_t log_n, int32_t skips,
                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                        uint32_t* proof_out, size_t* proof_len, float* round_ms);
+
+/* Allocation-free variant of wl_sumcheck_abc_prove_device; it has no counterpart in the
+ * reference. For callers that cannot allocate device memory (code running where cudaMalloc is
+ * not allowed, such as host callbacks, processes whose device memory another framework has
+ * already partitioned, or paths that must not touch an allocator): it makes no device, pinned
+ * or host-heap allocation. Its device scratch is a fixed 4 MiB array inside the library
+ * (present on every device that loads the library, until exit), which limits log_n to 14
+ * (WL_E_SCRATCH_LIMIT beyond). Inputs are canonical device arrays of 2^log_n values, left
+ * unchanged; the proof (host buffer, its exact length is returned with WL_E_BUFFER_TOO_SMALL
+ * when short) equals wl_sumcheck_abc_prove_device's. `stream` is a cudaStream_t (NULL: the
+ * default stream). All calls share the scratch array: calls that overlap on the GPU race and
+ * must be serialised. The first call on a device looks up the array's address; make it
+ * before any stream capture. */
+wl_status wl_sumcheck_abc_prove_noalloc(const uint32_t* p16_constants, int32_t log_n, int32_t skips,
+                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
+                                        uint32_t* proof_out, size_t* proof_len, void* stream);
 
 /* Serving and batching (no counterpart in the reference, which proves one instance at a time
  * in src/examples/poseidon2.rs:153-174). A server runs `workers` proofs concurrently on one

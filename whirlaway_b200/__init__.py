@@ -24,7 +24,7 @@ _sizep = ctypes.POINTER(ctypes.c_size_t)
 STATUS = {
     0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "OOM", 4: "BUFFER_TOO_SMALL", 5: "INTERNAL", 6: "BUDGET",
     11: "INVALID_PCS_COMMITMENT", 12: "INVALID_PCS_OPENING", 13: "FS", 14: "SUMCHECK", 15: "BOUNDARY",
-    16: "SUM_MISMATCH",
+    16: "SUM_MISMATCH", 7: "SCRATCH_LIMIT",
 }
 
 
@@ -96,6 +96,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                         _u32p, _sizep, ctypes.POINTER(ctypes.c_float)]),
         "wl_ctx_stream": (vp, [vp]),
         "wl_kernel_launch_count": (ctypes.c_uint64, []),
+        "wl_sumcheck_abc_prove_noalloc": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, _u32p,
+                                                         _sizep, vp]),
         "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
         "wl_server_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]),
         "wl_server_destroy": (None, [vp]),
@@ -301,6 +303,24 @@ def sumcheck_abc_prove(ctx: Context, p16_constants: np.ndarray, log_n: int, skip
                                        ctypes.byref(n), ms)
     ctx.check(st, "sumcheck_abc_prove")
     return out[: n.value].copy(), list(ms)
+
+
+def sumcheck_abc_prove_noalloc(p16_constants: np.ndarray, log_n: int, skips: int, a, b, c, stream: int = 0):
+    """Allocation-free zerocheck of eq(r, x) * (a*b - c) for callers that cannot allocate
+    device memory; a, b, c are CUDA tensors of canonical values (log_n <= 14)."""
+    lib = load_library()
+    n = ctypes.c_size_t(0)
+    p16 = np.ascontiguousarray(p16_constants, dtype=np.uint32)
+    ptrs = [ctypes.c_void_p(int(t.data_ptr())) for t in (a, b, c)]
+    st = lib.wl_sumcheck_abc_prove_noalloc(_ptr(p16), log_n, skips, *ptrs, None, ctypes.byref(n), ctypes.c_void_p(stream))
+    if st != 4:
+        raise ProverError(st, "sumcheck_abc_prove_noalloc (length query)")
+    out = np.zeros(n.value, np.uint32)
+    st = lib.wl_sumcheck_abc_prove_noalloc(_ptr(p16), log_n, skips, *ptrs, _ptr(out), ctypes.byref(n),
+                                           ctypes.c_void_p(stream))
+    if st:
+        raise ProverError(st, "sumcheck_abc_prove_noalloc")
+    return out[: n.value].copy()
 
 
 def proof_footprint_bytes(log_n: int) -> int:
