@@ -26,9 +26,10 @@ constexpr int NTT_THREADS = 512;
 __device__ __forceinline__ uint32_t sidx(uint32_t col, uint32_t i, int B) { return col * ((1u << B) + 1) + i; }
 
 // Per-block twiddle table: for local bit tl (global stage t = tl + 1 + lo_bits) the 2^tl
-// factors w_{2^t}^(lo_global + (m << lo_bits)), m < 2^tl, at offset 2^tl - 1.
-__device__ __forceinline__ void load_twiddles(uint32_t* tab, int B, int tl0, uint32_t lo_global, int lo_bits,
-                                              const uint32_t* __restrict__ tw) {
+// factors w_{2^t}^(lo_global + (m << lo_bits)), m < 2^tl, at offset 2^tl - 1, each as the
+// pair (canonical w, floor(w * 2^32 / p)) for Shoup multiplication.
+__device__ __forceinline__ void load_twiddles(uint2* tab, int B, int tl0, uint32_t lo_global, int lo_bits,
+                                              const uint2* __restrict__ tw) {
   for (uint32_t e = threadIdx.x; e < (1u << B) - 1; e += blockDim.x) {
     const int tl = 31 - __clz(e + 1);  // e + 1 in [2^tl, 2^(tl+1))
     if (tl < tl0) continue;
@@ -38,28 +39,37 @@ __device__ __forceinline__ void load_twiddles(uint32_t* tab, int B, int tl0, uin
   }
 }
 
-// Fused Moebius + DIT butterfly on (u, v) with twiddle w.
-__device__ __forceinline__ void bfly(uint32_t& u, uint32_t& v, uint32_t w) {
-  const uint32_t d = kb::mul(w, kb::sub(v, u));
+// x * w mod p for x < 2^32 and a canonical constant w with ws = floor(w 2^32 / p) (Shoup):
+// the quotient estimate is off by at most one, so x w - q p lies in [0, 2p). Montgomery form
+// of x is preserved (the product is linear in x).
+__device__ __forceinline__ uint32_t mul_shoup(uint32_t x, uint2 w) {
+  const uint32_t q = __umulhi(x, w.y);
+  const uint32_t r = x * w.x - q * kb::P;
+  return kb::umin(r, r - kb::P);
+}
+
+// Fused Moebius + DIT butterfly on (u, v): d = w (v - u), (u, v) <- (u + d, u - d).
+__device__ __forceinline__ void bfly(uint32_t& u, uint32_t& v, uint2 w) {
+  const uint32_t d = mul_shoup(v + kb::P - u, w);
   v = kb::sub(u, d);
   u = kb::add(u, d);
 }
 
 // Stages on local bits [tl0, tl1) of the 2^B points of CT columns in shared memory: two
 // bits per shared-memory round trip (radix 4), a final single bit if the count is odd.
-__device__ __forceinline__ void run_stages(uint32_t* sm, const uint32_t* tab, int B, int tl0, int tl1) {
+__device__ __forceinline__ void run_stages(uint32_t* sm, const uint2* tab, int B, int tl0, int tl1) {
   const uint32_t npts = 1u << B;
   int tl = tl0;
   for (; tl + 1 < tl1; tl += 2) {
     const uint32_t h = 1u << tl;
-    const uint32_t ngroups = npts >> 2;
+    const uint32_t ngroups = npts >> 2;  // 2^(B-2): shifts, not divisions
     for (uint32_t g = threadIdx.x; g < (uint32_t)CT * ngroups; g += blockDim.x) {
-      const uint32_t col = g / ngroups, q = g % ngroups;
+      const uint32_t col = g >> (B - 2), q = g & (ngroups - 1);
       const uint32_t r = q & (h - 1);
       const uint32_t a = ((q >> tl) << (tl + 2)) | r;
       uint32_t* base = sm + sidx(col, a, B);
       uint32_t x0 = base[0], x1 = base[h], x2 = base[2 * h], x3 = base[3 * h];
-      const uint32_t w1 = tab[h - 1 + r];
+      const uint2 w1 = tab[h - 1 + r];
       bfly(x0, x1, w1);
       bfly(x2, x3, w1);
       bfly(x0, x2, tab[2 * h - 1 + r]);
@@ -75,7 +85,7 @@ __device__ __forceinline__ void run_stages(uint32_t* sm, const uint32_t* tab, in
     const uint32_t h = 1u << tl;
     const uint32_t npairs = npts >> 1;
     for (uint32_t g = threadIdx.x; g < (uint32_t)CT * npairs; g += blockDim.x) {
-      const uint32_t col = g / npairs, m = g % npairs;
+      const uint32_t col = g >> (B - 1), m = g & (npairs - 1);
       const uint32_t r = m & (h - 1);
       const uint32_t a = ((m >> tl) << (tl + 1)) | r;
       uint32_t* base = sm + sidx(col, a, B);
@@ -90,9 +100,9 @@ __device__ __forceinline__ void run_stages(uint32_t* sm, const uint32_t* tab, in
 
 // First pass: points i of block blk (2^B of them) read source entry s = i >> rho, which
 // realises the zero-padded stages 1..rho as copies; then stages rho+1..B.
-__global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, const uint32_t* __restrict__ tw) {
-  extern __shared__ uint32_t sm[];
-  uint32_t* tab = sm + CT * ((1u << B) + 1);
+__global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, const uint2* __restrict__ tw) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint2* tab = reinterpret_cast<uint2*>(sm + ((CT * ((1u << B) + 1) + 1) & ~1u));
   const int tile = blockIdx.y;
   const size_t i0 = size_t(blockIdx.x) << B;
   const uint32_t npts = 1u << B;
@@ -100,11 +110,12 @@ __global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, con
   load_twiddles(tab, B, in.rho, 0, 0, tw);
   for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
     uint32_t col, il;
-    if (in.elem == 1) { il = idx % npts; col = idx / npts; }
+    if (in.elem == 1) { il = idx & (npts - 1); col = idx >> B; }
     else { col = idx % CT; il = idx / CT; }
     uint32_t gcol = tile * CT + col;
     size_t s = (i0 + il) >> in.rho;
-    size_t addr = (gcol / in.elem) * col_block + (gcol % in.elem) + s * in.elem;
+    const int le = in.elem == 8 ? 3 : 0;  // log2(elem)
+    size_t addr = size_t(gcol >> le) * col_block + (gcol & (in.elem - 1)) + (s << le);
     sm[sidx(col, il, B)] = (gcol < (uint32_t)in.n_cols && addr < in.src_len) ? in.src[addr] : 0u;
   }
   __syncthreads();
@@ -119,9 +130,9 @@ __global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, con
 // Later pass, in place: points i = lo + (j << B0) + (hi << (B0 + Bp)), stages B0+1..B0+Bp
 // (stages up to rho are copies and are skipped).
 __global__ void k_ntt_mid(uint32_t* __restrict__ data, int n_cols, int B0, int Bp, int rho,
-                          const uint32_t* __restrict__ tw) {
-  extern __shared__ uint32_t sm[];
-  uint32_t* tab = sm + CT * ((1u << Bp) + 1);
+                          const uint2* __restrict__ tw) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint2* tab = reinterpret_cast<uint2*>(sm + ((CT * ((1u << Bp) + 1) + 1) & ~1u));
   const int tile = blockIdx.y;
   const size_t g = blockIdx.x;
   const uint32_t lo = uint32_t(g & ((size_t(1) << B0) - 1));
@@ -153,13 +164,15 @@ __device__ uint32_t pow_dev(uint32_t a, uint32_t e) {
   }
   return r;
 }
-__global__ void k_twiddles(uint32_t* tw, uint32_t w24) {
+__global__ void k_twiddles(uint2* tw, uint32_t w24) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < (1u << 23)) tw[j] = pow_dev(w24, j);
+  if (j < (1u << 23)) {
+    const uint32_t w = kb::from_mont(pow_dev(w24, j));
+    tw[j] = make_uint2(w, uint32_t((uint64_t(w) << 32) / kb::P));
+  }
 }
 
 constexpr int LEAF_ROWS = 128;
-constexpr int LEAF_PAD = 129;
 constexpr int SUBTREE_LEVELS = 7;  // levels folded per pass (2^7 digests per block)
 
 // Tree layout: level l (2^(LL-l) digests of 8 words) starts at digest offset
@@ -198,46 +211,85 @@ __device__ __forceinline__ void subtree_reduce(uint32_t (*d)[8], int cnt, int le
   }
 }
 
-// Leaf digests of 128 rows per block (the row is Moebius-transformed over the position
-// bits of its column index first), then the first levels of the tree above them.
+// Adds (sign +1) or subtracts (sign -1) the 16 row entries of chunk `ch` (columns
+// 16 ch .. 16 ch + 15, zero at and beyond n_cols) into x, or loads them (sign 0).
+__device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ row, int n_cols, bool vec4, int ch, int sign,
+                                           uint32_t* x) {
+  const int c0 = ch * 16;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    uint32_t v[4];
+    const int c = c0 + 4 * q;
+    if (vec4) {
+      if (c < n_cols) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(row + c));
+        v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
+      } else {
+        v[0] = v[1] = v[2] = v[3] = 0u;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; e++) v[e] = c + e < n_cols ? __ldg(row + c + e) : 0u;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      uint32_t& d = x[4 * q + e];
+      d = sign == 0 ? v[e] : (sign > 0 ? kb::add(d, v[e]) : kb::sub(d, v[e]));
+    }
+  }
+}
+
+// Leaf digests of 128 rows per block, then the first levels of the tree above them.
+// Each thread hashes one row of 128 entries with the width-24 sponge (16 entries per
+// absorption), after the Moebius transform over the position bits [log_elem, 7) of the
+// column index: entry j becomes sum over i <= j (bitwise on those bits, equal elsewhere)
+// of (-1)^popcount(i ^ j) row[i]. Bits 4..6 select the 16-entry chunk, so chunk ch is the
+// signed sum of the chunks below it, and bits below 4 are transformed inside the chunk;
+// rows are read straight from global memory (no shared-memory staging, so occupancy
+// is bounded by registers).
 __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, size_t rows, int n_cols,
                                                          int log_elem, const __grid_constant__ kb::P24Consts c,
                                                          const __grid_constant__ kb::P16Consts c16,
                                                          uint32_t* __restrict__ tree, int LL, int levels) {
-  extern __shared__ uint32_t sm[];
+  __shared__ uint32_t d[LEAF_ROWS][8];
   const size_t row0 = size_t(blockIdx.x) * LEAF_ROWS;
   const int nrows = (rows - row0) < size_t(LEAF_ROWS) ? int(rows - row0) : LEAF_ROWS;
-  for (uint32_t idx = threadIdx.x; idx < LEAF_ROWS * 128; idx += blockDim.x) {
-    uint32_t r = idx / 128, col = idx % 128;
-    sm[r * LEAF_PAD + col] = (col < (uint32_t)n_cols && (int)r < nrows) ? lde[(row0 + r) * n_cols + col] : 0u;
-  }
-  __syncthreads();
   const int t = threadIdx.x;
   uint32_t st[24];
   if (t < nrows) {
-    uint32_t* r = sm + t * LEAF_PAD;
-    for (int b = log_elem; b < 7; b++) {
-      const int h = 1 << b;
-      for (int i = 0; i < 128; i++)
-        if (!(i & h)) r[i + h] = kb::sub(r[i + h], r[i]);
-    }
+    const uint32_t* row = lde + (row0 + t) * size_t(n_cols);
+    const bool vec4 = (n_cols & 3) == 0;
+    const int cmask = log_elem <= 4 ? 7 : (7 << (log_elem - 4)) & 7;  // chunk bits in the transform
 #pragma unroll
     for (int i = 0; i < 24; i++) st[i] = 0;
 #pragma unroll 1
     for (int ch = 0; ch < 8; ch++) {
+      leaf_chunk(row, n_cols, vec4, ch, 0, st);
+      const int m = ch & cmask;
+      if (m) {
+        // every proper subset of m, with the sign of the bits it drops
+        for (int sub = (m - 1) & m;; sub = (sub - 1) & m) {
+          const int sign = (__popc(m ^ sub) & 1) ? -1 : 1;
+          leaf_chunk(row, n_cols, vec4, (ch & ~m) | sub, sign, st);
+          if (!sub) break;
+        }
+      }
 #pragma unroll
-      for (int i = 0; i < 16; i++) st[i] = r[ch * 16 + i];
+      for (int b = 0; b < 4; b++) {
+        if (b < log_elem) continue;
+        const int h = 1 << b;
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+          if (!(i & h)) st[i + h] = kb::sub(st[i + h], st[i]);
+      }
       kb::p2_permute<24>(st, c);
     }
     uint32_t* o = tree + (row0 + t) * 8;
 #pragma unroll
-    for (int i = 0; i < 8; i++) o[i] = st[i];
-  }
-  __syncthreads();
-  uint32_t(*d)[8] = reinterpret_cast<uint32_t(*)[8]>(sm);
-  if (t < nrows) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) d[t][i] = st[i];
+    for (int i = 0; i < 8; i++) {
+      o[i] = st[i];
+      d[t][i] = st[i];
+    }
   }
   __syncthreads();
   subtree_reduce(d, nrows, levels, tree, LL, 0, row0, c16);
@@ -315,28 +367,28 @@ void launch_trace_gen(const uint32_t* inputs, const AirConsts& K, uint32_t* wit,
   WL_LAUNCH_CHECK();
 }
 
-void launch_twiddles(uint32_t* tw, cudaStream_t s) {
+void launch_twiddles(uint2* tw, cudaStream_t s) {
   k_twiddles<<<(1u << 23) / 256, 256, 0, s>>>(tw, kb::two_adic_gen_m(24));
   WL_LAUNCH_CHECK();
 }
 
-void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_t* tw, cudaStream_t s) {
+void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint2* tw, cudaStream_t s) {
   (void)tmp;
   const int T = in.L + in.rho;
   if (T > 2 * MAXB || T > 24) throw std::runtime_error("LDE size beyond two shared-memory passes");
   const int tiles = (in.n_cols + CT - 1) / CT;
   const int B0 = T <= MAXB ? T : (T + 1) / 2;
-  const size_t smem_max = (size_t(CT) * ((1u << MAXB) + 1) + (1u << MAXB)) * 4;
+  auto smem_for = [](int B) { return (((size_t(CT) * ((1u << B) + 1) + 1) & ~size_t(1)) + 2 * (size_t(1) << B)) * 4; };
+  const size_t smem_max = smem_for(MAXB);
   WL_CUDA(cudaFuncSetAttribute(k_ntt_first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
   WL_CUDA(cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
   dim3 g1((unsigned)(size_t(1) << (T - B0)), tiles);
-  k_ntt_first<<<g1, NTT_THREADS, (size_t(CT) * ((1u << B0) + 1) + (1u << B0)) * 4, s>>>(in, B0, out, tw);
+  k_ntt_first<<<g1, NTT_THREADS, smem_for(B0), s>>>(in, B0, out, tw);
   WL_LAUNCH_CHECK();
   if (B0 < T) {
     const int Bp = T - B0;
     dim3 g2((unsigned)(size_t(1) << (T - Bp)), tiles);
-    k_ntt_mid<<<g2, NTT_THREADS, (size_t(CT) * ((1u << Bp) + 1) + (1u << Bp)) * 4, s>>>(out, in.n_cols, B0, Bp, in.rho,
-                                                                                        tw);
+    k_ntt_mid<<<g2, NTT_THREADS, smem_for(Bp), s>>>(out, in.n_cols, B0, Bp, in.rho, tw);
     WL_LAUNCH_CHECK();
   }
 }
@@ -344,10 +396,8 @@ void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_
 void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s) {
   const int log_elem = elem == 8 ? 3 : 0;
-  const size_t smem = size_t(LEAF_ROWS) * LEAF_PAD * 4;
-  WL_CUDA(cudaFuncSetAttribute(k_leaf_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int first_levels = LL < SUBTREE_LEVELS ? LL : SUBTREE_LEVELS;
-  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, smem, s>>>(lde, rows, n_cols, log_elem, p24,
+  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, rows, n_cols, log_elem, p24,
                                                                                      p16, tree, LL, first_levels);
   WL_LAUNCH_CHECK();
   for (int l0 = first_levels; l0 < LL; l0 += SUBTREE_LEVELS) {

@@ -156,23 +156,28 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
   if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
 }
 
-// out[c * S + x] = sum_j sel[j] * up_c[j * S + x]
+// out[c * S + x] = sum_j sel[j] * up_c[j * S + x]  (the 2^k loads are issued before the
+// products, sel is zero-padded to 16)
 __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ sel_g,
                            ef* __restrict__ out) {
   __shared__ ef sel[16];
   const int nsk = 1 << k;
-  if (threadIdx.x < nsk) sel[threadIdx.x] = sel_g[threadIdx.x];
+  if (threadIdx.x < 16) sel[threadIdx.x] = threadIdx.x < (unsigned)nsk ? sel_g[threadIdx.x] : ef_zero();
   __syncthreads();
   const size_t N = size_t(1) << log_n, S = N >> k;
   const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
   if (x >= S) return;
   const uint32_t* col = wit + size_t(c) * N;
+  uint32_t v[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) v[j] = j < nsk ? col[up_row(size_t(j) * S + x, N)] : 0u;
   EfMacF m;
   m.init();
-  for (int j = 0; j < nsk; j++) {
-    m.mac(sel[j], col[up_row(size_t(j) * S + x, N)]);
-    if ((j & 3) == 3 || j == nsk - 1) m.flush();
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    m.mac(sel[j], v[j]);
+    if ((j & 3) == 3) m.flush();
   }
   out[size_t(c) * S + x] = m.acc;
 }
@@ -234,24 +239,33 @@ __device__ void internal_layer_smem_with0(const SmemState& S, const ef& x0) {
   for (int i = 1; i < 16; i++) S.set(i, ef_add(ef_diag16(i, S.get(i)), sum));
 }
 
-constexpr int ZCE_SEGMENTS = 9;
+constexpr int ZCE_FULL_SEGS = 7;  // full rounds evaluated without state
+constexpr int ZCE_SEGMENTS = ZCE_FULL_SEGS + 1;
 
-// Rounds >= 1. Block (x range, z, segment), z = 0, 2, 3 for blockIdx.y = 0, 1, 2. The 148
-// constraints split into 9 independent segments: the 4 beginning full rounds (each starts
-// from committed columns), the 20 partial rounds, and the 4 ending full rounds; the first
-// ending round starts from the state after the partial rounds, which is linear in the
-// committed columns (internal layers only). Each thread evaluates one segment at one
-// (x, z), so a point's work is spread over 9 threads; the per-segment sums add up in the
-// partial reduction. Loops stay rolled (small code) and the state lives in shared memory.
-__global__ void __launch_bounds__(ZCE_T) k_zc_eval_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
-                                                     const ef* __restrict__ alphas_g,
+// 4x4 block M4 = [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]] applied to a chunk.
+__device__ __forceinline__ void m4_ef(ef& x0, ef& x1, ef& x2, ef& x3) {
+  ef t01 = ef_add(x0, x1), t23 = ef_add(x2, x3), t0123 = ef_add(t01, t23);
+  ef t01123 = ef_add(t0123, x1), t01233 = ef_add(t0123, x3);
+  ef y3 = ef_add(t01233, ef_add(x0, x0));
+  ef y1 = ef_add(t01123, ef_add(x2, x2));
+  ef y0 = ef_add(t01123, t01);
+  ef y2 = ef_add(t01233, t23);
+  x0 = y0;
+  x1 = y1;
+  x2 = y2;
+  x3 = y3;
+}
+
+// Rounds >= 1, full rounds without state. For full round f with constraint weights
+// alpha_(c0 + i), sum_i alpha_(c0+i) (MDS(cubes)_i - post_i) = sum_j beta_(f,j) cube_j -
+// sum_i alpha_(c0+i) post_i, beta_f = MDS^T alpha (computed once on the host), and each
+// full round's input is committed: the previous round's post columns, or MDS(inputs) for
+// the first round (streamed: column sums of the M4 outputs, then chunk by chunk).
+// Block (x range, z, segment); segments 0..3 are the beginning rounds, 4..6 the ending
+// rounds 1..3. z = 0, 2, 3 for blockIdx.y = 0, 1, 2.
+__global__ void __launch_bounds__(ZCE_T, 4) k_zc_full_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
+                                                     const ef* __restrict__ alphas, const ef* __restrict__ betas,
                                                      const __grid_constant__ AirConsts K, ef* __restrict__ partial) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  ef* alphas = reinterpret_cast<ef*>(smraw);
-  uint4* planes = reinterpret_cast<uint4*>(smraw + sizeof(ef) * AIR_NC);
-  for (int i = threadIdx.x; i < AIR_NC; i += ZCE_T) alphas[i] = alphas_g[i];
-  const SmemState S{planes, planes + 16 * ZCE_T, (int)threadIdx.x};
-  __syncthreads();
   const size_t len = size_t(1) << m, half = len >> 1;
   const size_t x = size_t(blockIdx.x) * ZCE_T + threadIdx.x;
   const int zi = blockIdx.y, seg = blockIdx.z;
@@ -264,52 +278,41 @@ __global__ void __launch_bounds__(ZCE_T) k_zc_eval_ef(const ef* __restrict__ col
     ef v = ef_add(hi, d);               // z = 2: 2 hi - lo
     return zi == 1 ? v : ef_add(v, d);  // z = 3: 3 hi - 2 lo
   };
+  const int f = seg < 4 ? seg : seg + 1;  // full-round index 0..7 (4 = first ending round, not here)
+  const uint32_t* rc = seg < 4 ? K.begin[seg] : K.end[seg - 3];
+  const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
+  const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
+  const ef* beta = betas + 16 * f;
   ef acc = ef_zero();
-  if (seg == 4) {
+  if (seg == 0) {
+    ef S[4] = {ef_zero(), ef_zero(), ef_zero(), ef_zero()};
 #pragma unroll 1
-    for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
-#pragma unroll 1
-    for (int r = 0; r < 20; r++) {
-      const ef x0 = ef_cube(ef_add_f(S.get(0), K.partial[r]));
-      const ef p = get(81 + r);
-      acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(x0, p)));
-      internal_layer_smem_with0(S, p);
+    for (int q = 0; q < 4; q++) {
+      ef y0 = get(1 + 4 * q), y1 = get(2 + 4 * q), y2 = get(3 + 4 * q), y3 = get(4 + 4 * q);
+      m4_ef(y0, y1, y2, y3);
+      S[0] = ef_add(S[0], y0);
+      S[1] = ef_add(S[1], y1);
+      S[2] = ef_add(S[2], y2);
+      S[3] = ef_add(S[3], y3);
     }
-  } else {
-    const uint32_t* rc;
-    int post, cidx;
-    if (seg < 4) {
-      rc = K.begin[seg];
-      post = 17 + 16 * seg;
-      cidx = 16 * seg;
-      const int src = seg == 0 ? 1 : post - 16;
 #pragma unroll 1
-      for (int i = 0; i < 16; i++) S.set(i, get(src + i));
-      if (seg == 0) mds_light_smem(S);
-    } else {
-      const int e = seg - 5;
-      rc = K.end[e];
-      post = 101 + 16 * e;
-      cidx = 84 + 16 * e;
-      if (e == 0) {
-#pragma unroll 1
-        for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
-#pragma unroll 1
-        for (int r = 0; r < 20; r++) internal_layer_smem_with0(S, get(81 + r));
-      } else {
-#pragma unroll 1
-        for (int i = 0; i < 16; i++) S.set(i, get(post - 16 + i));
+    for (int q = 0; q < 4; q++) {
+      ef y[4] = {get(1 + 4 * q), get(2 + 4 * q), get(3 + 4 * q), get(4 + 4 * q)};
+      m4_ef(y[0], y[1], y[2], y[3]);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const int j = 4 * q + kk;
+        const ef in = ef_add(y[kk], S[kk]);
+        acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(in, rc[j]))));
       }
     }
+  } else {
+    const int src = post - 16;
 #pragma unroll 1
-    for (int i = 0; i < 16; i++) S.set(i, ef_cube(ef_add_f(S.get(i), rc[i])));
-    mds_light_smem(S);
-#pragma unroll 1
-    for (int i = 0; i < 16; i++) {
-      const ef p = get(post + i);
-      acc = ef_add(acc, ef_mul(alphas[cidx + i], ef_sub(S.get(i), p)));
-    }
+    for (int j = 0; j < 16; j++) acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(get(src + j), rc[j]))));
   }
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) acc = ef_sub(acc, ef_mul(alphas[c0 + i], get(post + i)));
   ef res = x < half ? ef_mul(acc, eq[x]) : ef_zero();
   res = warp_reduce_ef(res);
   __shared__ ef wsum[ZCE_T / 32];
@@ -318,72 +321,160 @@ __global__ void __launch_bounds__(ZCE_T) k_zc_eval_ef(const ef* __restrict__ col
   if (threadIdx.x == 0) {
     ef tot = wsum[0];
     for (int w = 1; w < ZCE_T / 32; w++) tot = ef_add(tot, wsum[w]);
-    partial[(size_t(blockIdx.x) * ZCE_SEGMENTS + seg) * 3 + zi] = tot;
+    partial[(size_t(blockIdx.x) * ZCE_FULL_SEGS + seg) * 3 + zi] = tot;
   }
 }
 
-__global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, const ef* __restrict__ r) {
+// Rounds >= 1, the partial rounds and the first ending round, which starts from the state
+// after the partial rounds: the 16-word state lives in shared memory, loops stay rolled.
+__global__ void __launch_bounds__(ZCE_T) k_zc_partial_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
+                                                        const ef* __restrict__ alphas_g,
+                                                        const ef* __restrict__ betas,
+                                                        const __grid_constant__ AirConsts K,
+                                                        ef* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  ef* alphas = reinterpret_cast<ef*>(smraw);
+  uint4* planes = reinterpret_cast<uint4*>(smraw + sizeof(ef) * AIR_NC);
+  for (int i = threadIdx.x; i < AIR_NC; i += ZCE_T) alphas[i] = alphas_g[i];
+  const SmemState S{planes, planes + 16 * ZCE_T, (int)threadIdx.x};
+  __syncthreads();
+  const size_t len = size_t(1) << m, half = len >> 1;
+  const size_t x = size_t(blockIdx.x) * ZCE_T + threadIdx.x;
+  const int zi = blockIdx.y;
+  const size_t xs = x < half ? x : 0;
+  auto get = [&](int c) -> ef {
+    const ef lo = cols[size_t(c) * len + xs];
+    if (zi == 0) return lo;
+    const ef hi = cols[size_t(c) * len + half + xs];
+    ef d = ef_sub(hi, lo);
+    ef v = ef_add(hi, d);
+    return zi == 1 ? v : ef_add(v, d);
+  };
+  ef acc = ef_zero();
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
+#pragma unroll 1
+  for (int r = 0; r < 20; r++) {
+    const ef x0 = ef_cube(ef_add_f(S.get(0), K.partial[r]));
+    const ef p = get(81 + r);
+    acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(x0, p)));
+    internal_layer_smem_with0(S, p);
+  }
+  const ef* beta = betas + 16 * 4;
+#pragma unroll 1
+  for (int j = 0; j < 16; j++) acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(S.get(j), K.end[0][j]))));
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) acc = ef_sub(acc, ef_mul(alphas[84 + i], get(101 + i)));
+  ef res = x < half ? ef_mul(acc, eq[x]) : ef_zero();
+  res = warp_reduce_ef(res);
+  __shared__ ef wsum[ZCE_T / 32];
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = res;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ef tot = wsum[0];
+    for (int w = 1; w < ZCE_T / 32; w++) tot = ef_add(tot, wsum[w]);
+    partial[size_t(blockIdx.x) * 3 + zi] = tot;
+  }
+}
+
+__global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, int ncols,
+                            const ef* __restrict__ r, const ef* __restrict__ eq_in, ef* __restrict__ eq_out,
+                            size_t eq_half) {
   const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
+  if (c == ncols) {
+    if (x < eq_half) eq_out[x] = ef_add(eq_in[x], eq_in[x + eq_half]);
+    return;
+  }
   if (x >= half) return;
   const ef* src = in + size_t(c) * 2 * half;
   out[size_t(c) * half + x] = ef_lerp(src[x], src[half + x], *r);
 }
 
-// partial[(c * 2^k + j)] = sum_x eqt[x] * up_c[j S + x] (and the same for down)
-__global__ void k_inner_sums(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ eqt,
-                             ef* __restrict__ pu, ef* __restrict__ pd) {
-  __shared__ ef scratch[32];
+// Per (column c, j < 2^k, x_hi): eq_hi[x_hi] * sum_{x_lo} eq_lo[x_lo] * up_c[j S + x] (and the
+// same for down), x = x_hi 2^ll + x_lo, with eq(tail, x) = eq_hi(x_hi) eq_lo(x_lo) factored so
+// every warp reads the same small eq_lo table. One warp per x_hi; 2^ll is a multiple of 32
+// or smaller than 32. Outputs pu/pd[(c * 2^k + j) * nhi + x_hi].
+constexpr int IS_WARPS = 8;
+__global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                              int ll, const ef* __restrict__ eq_hi,
+                                                              const ef* __restrict__ eq_lo, ef* __restrict__ pu,
+                                                              ef* __restrict__ pd) {
   const size_t N = size_t(1) << log_n, S = N >> k;
   const int c = blockIdx.x, j = blockIdx.y;
-  const uint32_t* col = wit + size_t(c) * N;
+  const uint32_t nhi = 1u << (log_n - k - ll);
+  const uint32_t xh = blockIdx.z * IS_WARPS + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (xh >= nhi) return;
+  const uint32_t nlo = 1u << ll;
+  const uint32_t* col = wit + size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+  const bool last = j == gridDim.y - 1 && xh == nhi - 1;  // holds the wrapped row N - 1
   EfMacF mu, md;
   mu.init();
   md.init();
-  int cnt = 0;
-  for (size_t x = threadIdx.x; x < S; x += blockDim.x) {
-    size_t i = size_t(j) * S + x;
-    const ef e = eqt[x];
-    mu.mac(e, col[up_row(i, N)]);
-    md.mac(e, col[down_row(i, N)]);
-    if (++cnt == 4) { mu.flush(); md.flush(); cnt = 0; }
+  uint32_t xl = lane;
+  for (; xl + 96 < nlo; xl += 128) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint32_t x = xl + 32 * q;
+      const ef e = eq_lo[x];
+      const bool wrap = last && x == nlo - 1;
+      mu.mac(e, col[wrap ? x - 1 : x]);
+      md.mac(e, col[wrap ? x : x + 1]);
+    }
+    mu.flush();
+    md.flush();
   }
-  mu.flush();
-  md.flush();
-  ef u = block_reduce_ef(mu.acc, scratch);
-  ef d = block_reduce_ef(md.acc, scratch);
-  if (threadIdx.x == 0) {
-    pu[size_t(c) * gridDim.y + j] = u;
-    pd[size_t(c) * gridDim.y + j] = d;
+  for (; xl < nlo; xl += 32) {
+    const ef e = eq_lo[xl];
+    const bool wrap = last && xl == nlo - 1;
+    mu.mac(e, col[wrap ? xl - 1 : xl]);
+    md.mac(e, col[wrap ? xl : xl + 1]);
+    mu.flush();
+    md.flush();
+  }
+  const ef su = warp_reduce_ef(mu.acc), sd = warp_reduce_ef(md.acc);
+  if (lane == 0) {
+    const size_t o = (size_t(c) * gridDim.y + j) * nhi + xh;
+    pu[o] = ef_mul(su, eq_hi[xh]);
+    pd[o] = ef_mul(sd, eq_hi[xh]);
   }
 }
 
-// out[c] = sum_j sel[j] * partial[c * nsk + j]
-__global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int ncols,
+// out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]
+__global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int nh, int ncols,
                               ef* __restrict__ out) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncols) return;
   ef acc = ef_zero();
-  for (int j = 0; j < nsk; j++) acc = ef_add(acc, ef_mul(sel[j], partial[size_t(c) * nsk + j]));
+  for (int j = 0; j < nsk; j++) {
+    ef s = ef_zero();
+    for (int h = 0; h < nh; h++) s = ef_add(s, partial[(size_t(c) * nsk + j) * nh + h]);
+    acc = ef_add(acc, ef_mul(sel[j], s));
+  }
   out[c] = acc;
 }
 
 // ------------------------------------------------------------------ inner phase
 __global__ void k_batch_cols(const uint32_t* __restrict__ wit, int log_n, const ef* __restrict__ eqc_g,
                              ef* __restrict__ out) {
-  __shared__ ef eqc[AIR_W];
-  for (int i = threadIdx.x; i < AIR_W; i += blockDim.x) eqc[i] = eqc_g[i];
+  __shared__ ef eqc[AIR_W + 3];
+  for (int i = threadIdx.x; i < AIR_W + 3; i += blockDim.x) eqc[i] = i < AIR_W ? eqc_g[i] : ef_zero();
   __syncthreads();
   const size_t N = size_t(1) << log_n;
   const size_t row = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (row >= N) return;
   EfMacF m;
   m.init();
-  for (int c = 0; c < AIR_W; c++) {
-    m.mac(eqc[c], wit[size_t(c) * N + row]);
-    if ((c & 3) == 3) m.flush();
+#pragma unroll 2
+  for (int c = 0; c < AIR_W; c += 4) {
+    uint32_t v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = c + q < AIR_W ? wit[size_t(c + q) * N + row] : 0u;
+#pragma unroll
+    for (int q = 0; q < 4; q++) m.mac(eqc[c + q], v[q]);
+    m.flush();
   }
-  m.flush();
   out[row] = m.acc;
 }
 
@@ -564,38 +655,43 @@ void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* o
   k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
-int zc_ef_blocks(int m) {  // partial sums per z (blocks x segments)
+int zc_ef_blocks(int m) {  // partial sums per z: (x blocks) x (7 full-round segments + 1)
   size_t half = size_t(1) << (m - 1);
   return (int)((half + ZCE_T - 1) / ZCE_T) * ZCE_SEGMENTS;
 }
-void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const AirConsts& K, ef* partial,
-                       cudaStream_t s) {
-  const size_t smem = sizeof(ef) * AIR_NC + sizeof(uint4) * 2 * 16 * ZCE_T;
-  WL_CUDA(cudaFuncSetAttribute(k_zc_eval_ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K,
+                       ef* partial, cudaStream_t s) {
   const unsigned xb = (unsigned)(zc_ef_blocks(m) / ZCE_SEGMENTS);
-  k_zc_eval_ef<<<dim3(xb, 3, ZCE_SEGMENTS), ZCE_T, smem, s>>>(cols, m, eq, alphas, K, partial);
+  k_zc_full_ef<<<dim3(xb, 3, ZCE_FULL_SEGS), ZCE_T, 0, s>>>(cols, m, eq, alphas, betas, K, partial);
+  WL_LAUNCH_CHECK();
+  const size_t smem = sizeof(ef) * AIR_NC + sizeof(uint4) * 2 * 16 * ZCE_T;
+  WL_CUDA(cudaFuncSetAttribute(k_zc_partial_ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_zc_partial_ef<<<dim3(xb, 3), ZCE_T, smem, s>>>(cols, m, eq, alphas, betas, K,
+                                                   partial + size_t(xb) * ZCE_FULL_SEGS * 3);
   WL_LAUNCH_CHECK();
 }
-void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s) {
-  dim3 grid((unsigned)((half + 255) / 256), ncols);
-  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, r);
+void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s, const ef* eq_in,
+                      ef* eq_out, size_t eq_half) {
+  const size_t width = eq_in && eq_half > half ? eq_half : half;
+  dim3 grid((unsigned)((width + 255) / 256), ncols + (eq_in ? 1 : 0));
+  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, ncols, r, eq_in, eq_out, eq_half);
   WL_LAUNCH_CHECK();
 }
-void launch_inner_sums(const uint32_t* wit, int log_n, int k, const ef* eqt, const ef* sel, ef* out_up,
-                       ef* out_down, cudaStream_t s) {
-  // out_up / out_down first hold the (column, j) partials (AIR_W * 2^k each) and then,
-  // at their start, the AIR_W combined values; the partials live past that prefix.
+void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
+                       const ef* sel, ef* out_up, ef* out_down, cudaStream_t s) {
+  // out_up / out_down hold AIR_W results followed by AIR_W * 2^k * 2^(log_n - k - ll) partials.
   const int nsk = 1 << k;
+  const int nh = 1 << (log_n - k - ll);
   ef* pu = out_up + AIR_W;
   ef* pd = out_down + AIR_W;
-  k_inner_sums<<<dim3(AIR_W, nsk), 256, 0, s>>>(wit, log_n, k, eqt, pu, pd);
+  k_inner_sums<<<dim3(AIR_W, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi,
+                                                                                         eq_lo, pu, pd);
   WL_LAUNCH_CHECK();
-  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pu, sel, nsk, AIR_W, out_up);
+  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pu, sel, nsk, nh, AIR_W, out_up);
   WL_LAUNCH_CHECK();
-  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pd, sel, nsk, AIR_W, out_down);
+  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pd, sel, nsk, nh, AIR_W, out_down);
   WL_LAUNCH_CHECK();
 }
-
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s) {
   size_t N = size_t(1) << log_n;
   k_batch_cols<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(wit, log_n, eqc, out);

@@ -13,7 +13,7 @@ namespace wl {
 namespace {
 using namespace kb;
 
-constexpr int MPB_SPLIT = 4;  // v_hi groups per column block
+constexpr int MPB_SPLIT = 16;  // v_hi groups per column block
 
 // out[(j * 2^lu + u) * MPB_SPLIT + g] = sum over v_hi in group g, v_lo of
 //   T[u * 2^lv + v] * hi_j[v_hi] * lo_j[v_lo]
@@ -21,6 +21,7 @@ template <int J>
 __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len, int lu, int lh, int ll,
                                    const ef* __restrict__ hi, const ef* __restrict__ lo, ef* __restrict__ out) {
   __shared__ ef scratch[32];
+  __shared__ ef hs[J][128];  // this block's slice of the hi tables
   const int u = blockIdx.x, g = blockIdx.y;
   const size_t lv = size_t(lh + ll);
   const size_t base = size_t(u) << lv;
@@ -28,6 +29,12 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
   const uint32_t nhi = 1u << lh;
   const uint32_t per = (nhi + MPB_SPLIT - 1) / MPB_SPLIT;
   const uint32_t h0 = g * per, h1 = min(nhi, h0 + per);
+  if (per <= 128) {
+    for (uint32_t i = threadIdx.x; i < per; i += blockDim.x)
+      for (int j = 0; j < J; j++) hs[j][i] = h0 + i < h1 ? hi[size_t(j) * nhi + h0 + i] : ef_zero();
+  }
+  __syncthreads();
+  auto hget = [&](int j, uint32_t vh) -> ef { return per <= 128 ? hs[j][vh - h0] : hi[size_t(j) * nhi + vh]; };
   ef res[J];
   for (int j = 0; j < J; j++) res[j] = ef_zero();
   if (base < t_len) {
@@ -45,7 +52,7 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
 #pragma unroll
         for (int q = 0; q < 4; q++)
 #pragma unroll
-          for (int j = 0; j < J; j++) m[j].mac(hi[size_t(j) * nhi + vh + q], t[q]);
+          for (int j = 0; j < J; j++) m[j].mac(hget(j, vh + q), t[q]);
 #pragma unroll
         for (int j = 0; j < J; j++) m[j].flush();
       }
@@ -54,7 +61,7 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
         uint32_t t = idx < t_len ? T[idx] : 0u;
 #pragma unroll
         for (int j = 0; j < J; j++) {
-          m[j].mac(hi[size_t(j) * nhi + vh], t);
+          m[j].mac(hget(j, vh), t);
           m[j].flush();
         }
       }
@@ -90,14 +97,18 @@ __global__ void k_whir_fold_T(const uint32_t* __restrict__ T, size_t t_len, int 
   if (v >= (size_t(1) << lv)) return;
   EfMacF m;
   m.init();
-  int cnt = 0;
-  for (int u = 0; u < nu; u++) {
-    size_t idx = (size_t(u) << lv) + v;
-    if (idx >= t_len) break;
-    m.mac(eqr[u], T[idx]);
-    if (++cnt == 4) { m.flush(); cnt = 0; }
+  for (int u0 = 0; u0 < nu; u0 += 4) {
+    if ((size_t(u0) << lv) + v >= t_len) break;  // the rest of the packed table is zero
+    uint32_t t[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const size_t idx = (size_t(u0 + q) << lv) + v;
+      t[q] = (u0 + q < nu && idx < t_len) ? T[idx] : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) m.mac(u0 + q < nu ? eqr[u0 + q] : ef_zero(), t[q]);
+    m.flush();
   }
-  m.flush();
   out[v] = m.acc;
 }
 

@@ -27,9 +27,9 @@ struct LdeSource {
   int rho;       // log2 of the rate expansion
   int n_cols;    // stored columns per row (leading columns; the rest are zero)
 };
-void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint32_t* twiddles, cudaStream_t s);
-// Twiddle table: tw[j] = w^j, w of order 2^24, j < 2^23.
-void launch_twiddles(uint32_t* tw, cudaStream_t s);
+void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint2* twiddles, cudaStream_t s);
+// Twiddle table: tw[j] = (w^j canonical, floor(w^j 2^32 / p)), w of order 2^24, j < 2^23.
+void launch_twiddles(uint2* tw, cudaStream_t s);
 // Merkle tree over the rows of an LDE matrix (rows of 128 values, the first `n_cols`
 // stored): leaf digests (each row Moebius-transformed over the bits [log2(elem), 7) of the
 // column index, then PaddingFreeSponge over Poseidon2-24) and 2-to-1 compressions
@@ -59,12 +59,18 @@ void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32
                      const ef* alphas, const AirConsts& K, ef* partial, cudaStream_t s);
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
 int zc_ef_blocks(int m);
-void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const AirConsts& K, ef* partial,
-                       cudaStream_t s);
-void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s);
-// Up/down evaluations of every column at (r0; tail): per (column, j) partial sums.
-void launch_inner_sums(const uint32_t* wit, int log_n, int k, const ef* eqt, const ef* sel, ef* out_up,
-                       ef* out_down, cudaStream_t s);
+// betas: the 8 full rounds' 16 weights beta_f = MDS^T (alpha_(c0(f)+i))_i, f = 0..7.
+void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K,
+                       ef* partial, cudaStream_t s);
+// Folds every column at r; with eq_in, also writes the next round's eq table
+// eq_out[x] = eq_in[x] + eq_in[x + eq_half].
+void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s,
+                      const ef* eq_in = nullptr, ef* eq_out = nullptr, size_t eq_half = 0);
+// Up/down evaluations of every column at (r0; tail), with eq(tail, .) factored as
+// eq_hi (2^(log_n-k-ll) entries) x eq_lo (2^ll entries). out_up / out_down must hold
+// AIR_W * (1 + 2^k * 2^(log_n-k-ll)) elements; the first AIR_W are the results.
+void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
+                       const ef* sel, ef* out_up, ef* out_down, cudaStream_t s);
 
 // --------------------------------------------------------------- inner phase
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s);

@@ -55,7 +55,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
   WL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-  WL_CUDA(cudaMalloc(&twiddles, sizeof(uint32_t) << 23));
+  WL_CUDA(cudaMalloc(&twiddles, sizeof(uint2) << 23));
   launch_twiddles(twiddles, stream);
   pinned_bytes = kUpBytes + kDownBytes;
   WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
@@ -459,7 +459,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   auto partial_eval = [&](const std::vector<ef>& pt) {
     std::vector<ef> pv(pt.begin() + lu, pt.end());
     EqPair e = eq_pair(ctx, pv, lh_v);
-    DBuf out(sizeof(ef) * (size_t(1) << lu) * 5, st);
+    DBuf out(sizeof(ef) * (size_t(1) << lu) * 17, st);  // results + 16 split partials
     { ProfScope _ps(ctx, "whir_partial_eval"); launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st); }
     std::vector<ef> h(size_t(1) << lu);
     ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * h.size());
@@ -486,6 +486,21 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   alphas[0] = kb::ef_one();
   for (int i = 1; i < AIR_NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
   DBuf d_alphas = upload(ctx, alphas);
+  // beta_f = MDS^T alpha_f for the 8 full rounds (constraints 16f.. for the beginning rounds,
+  // 84 + 16(f - 4).. for the ending rounds); MDS = circ(2 M4, M4, M4, M4).
+  std::vector<ef> betas(8 * 16, kb::ef_zero());
+  {
+    static const int M4[4][4] = {{2, 3, 1, 1}, {1, 2, 3, 1}, {1, 1, 2, 3}, {3, 1, 1, 2}};
+    for (int f = 0; f < 8; f++) {
+      const int c0 = f < 4 ? 16 * f : 84 + 16 * (f - 4);
+      for (int j = 0; j < 16; j++)
+        for (int i = 0; i < 16; i++) {
+          const int mij = M4[i % 4][j % 4] * (i / 4 == j / 4 ? 2 : 1);
+          betas[16 * f + j] = kb::ef_add(betas[16 * f + j], kb::ef_mul_f(alphas[c0 + i], fm(mij)));
+        }
+    }
+  }
+  DBuf d_betas = upload(ctx, betas);
   grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, n));
   std::vector<ef> zc(n + 1 - k);
   for (auto& x : zc) x = ts.sample_ext();
@@ -536,13 +551,19 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
   }
   const auto basis4 = lagrange_basis(4);
+  // eq table of round r (over zc[1+r..]) = eq table of round r-1 with its leading variable
+  // summed out; each fold below carries it along.
+  DBuf eqr;
+  if (n - k >= 1) {
+    eqr = DBuf(sizeof(ef) * (S / 2), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
+  }
   for (int round = 1; round <= n - k; round++) {
     const int m = n - k - round + 1;  // variables of the current columns
     const size_t half = size_t(1) << (m - 1);
-    DBuf eqr = eq_table_dev(ctx, std::vector<ef>(zc.begin() + 1 + round, zc.end()));
     const int nb = zc_ef_blocks(m);
     DBuf part(sizeof(ef) * size_t(nb) * 3, st);
-    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st); }
+    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part.as<ef>(), st); }
     std::vector<ef> s3 = reduce_to_host(ctx, part.as<ef>(), nb, 3);
     const ef& r = zc[round];
     ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
@@ -558,8 +579,11 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
                      mmf);
     DBuf nc(sizeof(ef) * size_t(W) * half, st);
     DBuf dc = scalar_dev(ctx, c);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st); }
+    DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st,
+                                                   half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
     cols = std::move(nc);
+    eqr = std::move(eqn);
   }
   // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
   // The zerocheck's returned challenges replace the eq challenges from here on
@@ -571,8 +595,11 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     std::vector<ef> selr(nsk);
     for (int i = 0; i < nsk; i++) selr[i] = upoly_eval(sel[i], challenges[0]);
     DBuf d_sel = upload(ctx, selr);
-    DBuf up(sizeof(ef) * size_t(W) * (1 + nsk), st), down(sizeof(ef) * size_t(W) * (1 + nsk), st);
-    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, eqt.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st); }
+    const int ll_t = std::min(12, n - k), lh_t = n - k - ll_t;
+    EqPair et = eq_pair(ctx, rtail, lh_t);
+    const size_t plen = size_t(W) * (1 + (size_t(nsk) << lh_t));
+    DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
+    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st); }
     ctx.to_host(inner_up.data(), up.as<ef>(), sizeof(ef) * W);
     ctx.to_host(inner_down.data(), down.as<ef>(), sizeof(ef) * W);
   }
@@ -783,16 +810,17 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     if (round_ms) round_ms->push_back(ms);
   };
   DBuf cols;
+  DBuf eq0;
   {
     tick();
     std::vector<uint32_t> lw(size_t(nz) * nsk);
     for (int zi = 0; zi < nz; zi++)
       for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
     DBuf d_lw = upload(ctx, lw);
-    DBuf eq = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1, r.end()));
+    eq0 = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1, r.end()));
     const int nb = abc0_blocks(n, k);
     DBuf part(sizeof(ef) * size_t(nb) * nz, st);
-    { ProfScope _ps(ctx, "abc0_eval"); launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq.as<ef>(), part.as<ef>(), st); }
+    { ProfScope _ps(ctx, "abc0_eval"); launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), part.as<ef>(), st); }
     std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
@@ -819,11 +847,15 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     tock();
   }
   const auto basis3 = lagrange_basis(3);
+  DBuf eqr;  // eq table of the current round, carried by the folds (see prove_air)
+  if (n - k >= 1) {
+    eqr = DBuf(sizeof(ef) * (S / 2), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
+  }
   for (int round = 1; round <= n - k; round++) {
     tick();
     const int m = n - k - round + 1;
     const size_t half = size_t(1) << (m - 1);
-    DBuf eqr = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1 + round, r.end()));
     const int nb = (int)((half + 31) / 32);
     DBuf part(sizeof(ef) * size_t(nb) * 2, st);
     { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part.as<ef>(), st); }
@@ -843,8 +875,11 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
                      mmf);
     DBuf nc(sizeof(ef) * 3 * half, st);
     DBuf dc = scalar_dev(ctx, cc);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st); }
+    DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st,
+                                                   half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
     cols = std::move(nc);
+    eqr = std::move(eqn);
     tock();
   }
   ef fin[3];
