@@ -3,14 +3,21 @@
 // and of the DuplexChallenger grinding behind pow_grinding).
 //
 // LDE. For one commitment every column of the codeword matrix is the evaluation, on the
-// subgroup of order 2^(L+rho), of a polynomial whose monomial coefficients are the Moebius
-// transform of a 2^L-long slice of the evaluation table, read in bit-reversed exponent
-// order. A radix-2 decimation-in-time NTT takes exactly that bit-reversed input, so the
-// Moebius step of the variable at stage t is fused into stage t's butterfly (v <- v - u
-// before u +- w v). Zero padding for the rate makes the first rho stages plain copies, so
-// the first pass replicates each input value 2^rho times and starts at stage rho + 1.
-// Stages run in shared-memory passes of up to 2^11 points over tiles of 8 columns; the
-// second pass works in place on the output, whose rows are the Merkle leaves.
+// subgroup of order 2^T (T = L + rho), of a polynomial whose monomial coefficients are the
+// Moebius transform of a 2^L-long slice of the evaluation table, read in bit-reversed
+// exponent order. A radix-2 decimation-in-time NTT takes exactly that bit-reversed input,
+// so the Moebius step of the variable at stage t is fused into stage t's butterfly
+// (v <- v - u before u +- w v). Zero padding for the rate makes stages 1..rho plain
+// copies: after them point i holds source entry i >> rho, so the work is stages
+// rho+1..T, split into passes of at most 8 stages.
+//
+// LDE layout in HBM (tile-major): columns in tiles of 8, word (tile, row, c) at
+// (tile * 2^T + row) * 8 + c, so 4 consecutive rows of a tile are one 128-byte line.
+// A pass over stages Bs+1..Bs+Bp works on lines of 2^Bp points i = lo + (j << Bs) +
+// (hi << (Bs + Bp)); a warp's 32 lanes are 8 columns x 4 (lo, hi) pairs of adjacent
+// rows, so every global access of a warp is one or two whole lines. Each thread keeps
+// 2^rb points of its line in registers for rb <= 4 stages, and a pass is two such
+// register rounds with one shared-memory exchange between them.
 #include <algorithm>
 
 #include "kernels.h"
@@ -18,26 +25,8 @@
 namespace wl {
 
 namespace {
-constexpr int CT = 8;         // columns per tile
-constexpr int MAXB = 11;      // log2 points per shared-memory pass
-constexpr int NTT_THREADS = 512;
-
-// Shared-memory tile: CT columns of 2^B points, column-major with one word of padding.
-__device__ __forceinline__ uint32_t sidx(uint32_t col, uint32_t i, int B) { return col * ((1u << B) + 1) + i; }
-
-// Per-block twiddle table: for local bit tl (global stage t = tl + 1 + lo_bits) the 2^tl
-// factors w_{2^t}^(lo_global + (m << lo_bits)), m < 2^tl, at offset 2^tl - 1, each as the
-// pair (canonical w, floor(w * 2^32 / p)) for Shoup multiplication.
-__device__ __forceinline__ void load_twiddles(uint2* tab, int B, int tl0, uint32_t lo_global, int lo_bits,
-                                              const uint2* __restrict__ tw) {
-  for (uint32_t e = threadIdx.x; e < (1u << B) - 1; e += blockDim.x) {
-    const int tl = 31 - __clz(e + 1);  // e + 1 in [2^tl, 2^(tl+1))
-    if (tl < tl0) continue;
-    const uint32_t m = e + 1 - (1u << tl);
-    const int t = tl + 1 + lo_bits;
-    tab[e] = tw[(lo_global + (m << lo_bits)) << (24 - t)];
-  }
-}
+constexpr int NTT_WARPS = 8;
+constexpr int NTT_MAX_BP = 8;  // stages per pass
 
 // x * w mod p for x < 2^32 and a canonical constant w with ws = floor(w 2^32 / p) (Shoup):
 // the quotient estimate is off by at most one, so x w - q p lies in [0, 2p). Montgomery form
@@ -55,104 +44,138 @@ __device__ __forceinline__ void bfly(uint32_t& u, uint32_t& v, uint2 w) {
   u = kb::add(u, d);
 }
 
-// Stages on local bits [tl0, tl1) of the 2^B points of CT columns in shared memory: two
-// bits per shared-memory round trip (radix 4), a final single bit if the count is odd.
-__device__ __forceinline__ void run_stages(uint32_t* sm, const uint2* tab, int B, int tl0, int tl1) {
-  const uint32_t npts = 1u << B;
-  int tl = tl0;
-  for (; tl + 1 < tl1; tl += 2) {
-    const uint32_t h = 1u << tl;
-    const uint32_t ngroups = npts >> 2;  // 2^(B-2): shifts, not divisions
-    for (uint32_t g = threadIdx.x; g < (uint32_t)CT * ngroups; g += blockDim.x) {
-      const uint32_t col = g >> (B - 2), q = g & (ngroups - 1);
-      const uint32_t r = q & (h - 1);
-      const uint32_t a = ((q >> tl) << (tl + 2)) | r;
-      uint32_t* base = sm + sidx(col, a, B);
-      uint32_t x0 = base[0], x1 = base[h], x2 = base[2 * h], x3 = base[3 * h];
-      const uint2 w1 = tab[h - 1 + r];
-      bfly(x0, x1, w1);
-      bfly(x2, x3, w1);
-      bfly(x0, x2, tab[2 * h - 1 + r]);
-      bfly(x1, x3, tab[2 * h - 1 + h + r]);
-      base[0] = x0;
-      base[h] = x1;
-      base[2 * h] = x2;
-      base[3 * h] = x3;
-    }
-    __syncthreads();
+// Where a round reads its points from and writes them to.
+enum NttIo { IO_SRC = 0, IO_GLOBAL = 1, IO_SMEM = 2 };
+
+struct NttLane {
+  const uint32_t* src;  // commitment source (IO_SRC)
+  size_t src_len;
+  size_t col_block;     // elem << L
+  int le;               // log2(elem)
+  uint32_t gcol;        // global column of this lane
+  bool col_ok;          // gcol < n_cols
+  uint32_t* data;       // LDE matrix
+  size_t row0;          // tile * 2^T + lo + (hi << (Bs + Bp)): row of j = 0 plus the tile base
+  int Bs, Bp;
+  size_t hi;            // source entry of j = 0 is hi << Bp
+  uint32_t* X;          // shared exchange buffer [2^Bp][32]
+  int lane;
+};
+
+template <int IO>
+__device__ __forceinline__ uint32_t ntt_load(const NttLane& ln, uint32_t j) {
+  if constexpr (IO == IO_SRC) {
+    const size_t s = size_t(j) + (ln.hi << ln.Bp);
+    const size_t addr = size_t(ln.gcol >> ln.le) * ln.col_block + (ln.gcol & ((1u << ln.le) - 1)) + (s << ln.le);
+    return (ln.col_ok && addr < ln.src_len) ? __ldg(ln.src + addr) : 0u;
+  } else if constexpr (IO == IO_GLOBAL) {
+    return ln.data[((ln.row0 + (size_t(j) << ln.Bs)) << 3) + (ln.gcol & 7)];
+  } else {
+    return ln.X[(j << 5) + ln.lane];
   }
-  if (tl < tl1) {
-    const uint32_t h = 1u << tl;
-    const uint32_t npairs = npts >> 1;
-    for (uint32_t g = threadIdx.x; g < (uint32_t)CT * npairs; g += blockDim.x) {
-      const uint32_t col = g >> (B - 1), m = g & (npairs - 1);
-      const uint32_t r = m & (h - 1);
-      const uint32_t a = ((m >> tl) << (tl + 1)) | r;
-      uint32_t* base = sm + sidx(col, a, B);
-      uint32_t x0 = base[0], x1 = base[h];
-      bfly(x0, x1, tab[h - 1 + r]);
-      base[0] = x0;
-      base[h] = x1;
-    }
-    __syncthreads();
+}
+template <int IO>
+__device__ __forceinline__ void ntt_store(const NttLane& ln, uint32_t j, uint32_t v) {
+  if constexpr (IO == IO_GLOBAL) {
+    ln.data[((ln.row0 + (size_t(j) << ln.Bs)) << 3) + (ln.gcol & 7)] = v;
+  } else {
+    ln.X[(j << 5) + ln.lane] = v;
   }
 }
 
-// First pass: points i of block blk (2^B of them) read source entry s = i >> rho, which
-// realises the zero-padded stages 1..rho as copies; then stages rho+1..B.
-__global__ void k_ntt_first(LdeSource in, int B, uint32_t* __restrict__ out, const uint2* __restrict__ tw) {
-  extern __shared__ __align__(16) uint32_t sm[];
-  uint2* tab = reinterpret_cast<uint2*>(sm + ((CT * ((1u << B) + 1) + 1) & ~1u));
-  const int tile = blockIdx.y;
-  const size_t i0 = size_t(blockIdx.x) << B;
-  const uint32_t npts = 1u << B;
-  const size_t col_block = size_t(in.elem) << in.L;
-  load_twiddles(tab, B, in.rho, 0, 0, tw);
-  for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
-    uint32_t col, il;
-    if (in.elem == 1) { il = idx & (npts - 1); col = idx >> B; }
-    else { col = idx % CT; il = idx / CT; }
-    uint32_t gcol = tile * CT + col;
-    size_t s = (i0 + il) >> in.rho;
-    const int le = in.elem == 8 ? 3 : 0;  // log2(elem)
-    size_t addr = size_t(gcol >> le) * col_block + (gcol & (in.elem - 1)) + (s << le);
-    sm[sidx(col, il, B)] = (gcol < (uint32_t)in.n_cols && addr < in.src_len) ? in.src[addr] : 0u;
-  }
-  __syncthreads();
-  if (in.rho < B) run_stages(sm, tab, B, in.rho, B);
-  for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
-    uint32_t col = idx % CT, il = idx / CT;
-    uint32_t gcol = tile * CT + col;
-    if (gcol < (uint32_t)in.n_cols) out[(i0 + il) * in.n_cols + gcol] = sm[sidx(col, il, B)];
+// One register round: stages b0..b0+RB-1 (local numbering) on the groups of 2^RB points
+// j = base + (k << b0) handled by this warp. `tws` is this lane's twiddle table: entry
+// 2^tl - 1 + r is the factor of local stage tl for j mod 2^tl = r.
+template <int RB, int IN, int OUT>
+__device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, int b0, int warp, bool active) {
+  constexpr int R = 1 << RB;
+  const uint32_t groups = 1u << (ln.Bp - RB);
+  for (uint32_t g = warp; g < groups; g += NTT_WARPS) {
+    const uint32_t base = (g & ((1u << b0) - 1)) | ((g >> b0) << (b0 + RB));
+    if (!active) continue;
+    uint32_t x[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) x[k] = ntt_load<IN>(ln, base + (uint32_t(k) << b0));
+    const uint32_t blo = base & ((1u << b0) - 1);
+#pragma unroll
+    for (int st = 0; st < RB; st++) {
+      const int tl = b0 + st;
+      const uint2* tt = tws + (1u << tl) - 1 + blo;
+      uint2 w[R > 1 ? R / 2 : 1];
+#pragma unroll
+      for (int m = 0; m < (1 << st); m++) w[m] = tt[uint32_t(m) << b0];
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+        if (k & (1 << st)) continue;
+        bfly(x[k], x[k + (1 << st)], w[k & ((1 << st) - 1)]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < R; k++) ntt_store<OUT>(ln, base + (uint32_t(k) << b0), x[k]);
   }
 }
 
-// Later pass, in place: points i = lo + (j << B0) + (hi << (B0 + Bp)), stages B0+1..B0+Bp
-// (stages up to rho are copies and are skipped).
-__global__ void k_ntt_mid(uint32_t* __restrict__ data, int n_cols, int B0, int Bp, int rho,
-                          const uint2* __restrict__ tw) {
+template <int IN, int OUT>
+__device__ __forceinline__ void ntt_round_rb(int rb, const NttLane& ln, const uint2* tws, int b0, int warp,
+                                             bool active) {
+  switch (rb) {
+    case 0: ntt_round<0, IN, OUT>(ln, tws, b0, warp, active); break;
+    case 1: ntt_round<1, IN, OUT>(ln, tws, b0, warp, active); break;
+    case 2: ntt_round<2, IN, OUT>(ln, tws, b0, warp, active); break;
+    case 3: ntt_round<3, IN, OUT>(ln, tws, b0, warp, active); break;
+    default: ntt_round<4, IN, OUT>(ln, tws, b0, warp, active); break;
+  }
+}
+
+// One pass over stages Bs+1..Bs+Bp (global numbering) for the lines of one tile.
+// blockIdx.x = (hi group << (Bs - lr_log)) | lo group; 2^lr_log lo values and 2^hg_log hi
+// values per block. The first pass (FROM_SRC, Bs = rho) reads the commitment source.
+template <bool FROM_SRC>
+__global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint32_t* __restrict__ data, int T,
+                                                            int Bs, int Bp, int rb1, int lr_log, int hg_log,
+                                                            const uint2* __restrict__ tw) {
   extern __shared__ __align__(16) uint32_t sm[];
-  uint2* tab = reinterpret_cast<uint2*>(sm + ((CT * ((1u << Bp) + 1) + 1) & ~1u));
-  const int tile = blockIdx.y;
-  const size_t g = blockIdx.x;
-  const uint32_t lo = uint32_t(g & ((size_t(1) << B0) - 1));
-  const size_t hi = g >> B0;
-  auto row_of = [&](uint32_t j) -> size_t { return lo + (size_t(j) << B0) + (hi << (B0 + Bp)); };
-  const int tl0 = rho > B0 ? rho - B0 : 0;
-  load_twiddles(tab, Bp, tl0, lo, B0, tw);
-  const uint32_t npts = 1u << Bp;
-  for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
-    uint32_t col = idx % CT, j = idx / CT;
-    uint32_t gcol = tile * CT + col;
-    sm[sidx(col, j, Bp)] = gcol < (uint32_t)n_cols ? data[row_of(j) * n_cols + gcol] : 0u;
+  const uint32_t npts = 1u << Bp, ntw = npts - 1;
+  const int LR = 1 << lr_log;
+  uint2* TW = reinterpret_cast<uint2*>(sm + (size_t(npts) << 5));  // [LR][2^Bp - 1]
+  const uint32_t lg = blockIdx.x & ((1u << (Bs - lr_log)) - 1);
+  const size_t hg = blockIdx.x >> (Bs - lr_log);
+  for (uint32_t idx = threadIdx.x; idx < (ntw << lr_log); idx += blockDim.x) {
+    const uint32_t l = idx & (LR - 1), e = idx >> lr_log;
+    const int tl = 31 - __clz(e + 1);  // e + 1 in [2^tl, 2^(tl+1))
+    const uint32_t r = e + 1 - (1u << tl);
+    const int t = Bs + tl + 1;
+    TW[l * ntw + e] = tw[((size_t(1) << (t - 1)) - 1) + (lg << lr_log) + l + (size_t(r) << Bs)];
   }
   __syncthreads();
-  if (tl0 < Bp) run_stages(sm, tab, Bp, tl0, Bp);
-  for (uint32_t idx = threadIdx.x; idx < (uint32_t)CT * npts; idx += blockDim.x) {
-    uint32_t col = idx % CT, j = idx / CT;
-    uint32_t gcol = tile * CT + col;
-    if (gcol < (uint32_t)n_cols) data[row_of(j) * n_cols + gcol] = sm[sidx(col, j, Bp)];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = lane & 7, l = (lane >> 3) & (LR - 1), h2 = lane >> (3 + lr_log);
+  const bool active = h2 < (1 << hg_log);
+  NttLane ln;
+  ln.src = in.src;
+  ln.src_len = in.src_len;
+  ln.le = in.elem == 8 ? 3 : 0;
+  ln.col_block = size_t(in.elem) << in.L;
+  ln.gcol = blockIdx.y * 8 + c;
+  ln.col_ok = ln.gcol < (uint32_t)in.n_cols;
+  ln.data = data;
+  ln.Bs = Bs;
+  ln.Bp = Bp;
+  ln.hi = (hg << hg_log) + h2;
+  ln.row0 = (size_t(blockIdx.y) << T) + (lg << lr_log) + l + (ln.hi << (Bs + Bp));
+  ln.X = sm;
+  ln.lane = lane;
+  const uint2* tws = TW + l * ntw;
+  const int rb2 = Bp - rb1;
+  if (rb2 == 0) {
+    if (FROM_SRC) ntt_round_rb<IO_SRC, IO_GLOBAL>(rb1, ln, tws, 0, warp, active);
+    else ntt_round_rb<IO_GLOBAL, IO_GLOBAL>(rb1, ln, tws, 0, warp, active);
+    return;
   }
+  if (FROM_SRC) ntt_round_rb<IO_SRC, IO_SMEM>(rb1, ln, tws, 0, warp, active);
+  else ntt_round_rb<IO_GLOBAL, IO_SMEM>(rb1, ln, tws, 0, warp, active);
+  __syncthreads();
+  ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb2, ln, tws, rb1, warp, active);
 }
 
 __device__ uint32_t pow_dev(uint32_t a, uint32_t e) {
@@ -164,16 +187,21 @@ __device__ uint32_t pow_dev(uint32_t a, uint32_t e) {
   }
   return r;
 }
+// Per-stage twiddles: stage t (1..24) holds w_{2^t}^x for x < 2^(t-1) at offset
+// 2^(t-1) - 1, each as (canonical w, floor(w 2^32 / p)) for Shoup multiplication.
 __global__ void k_twiddles(uint2* tw, uint32_t w24) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < (1u << 23)) {
-    const uint32_t w = kb::from_mont(pow_dev(w24, j));
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < (1u << 24) - 1) {
+    const int t = 32 - __clz(j + 1);
+    const uint32_t x = j + 1 - (1u << (t - 1));
+    const uint32_t w = kb::from_mont(pow_dev(w24, x << (24 - t)));
     tw[j] = make_uint2(w, uint32_t((uint64_t(w) << 32) / kb::P));
   }
 }
 
 constexpr int LEAF_ROWS = 128;
 constexpr int SUBTREE_LEVELS = 7;  // levels folded per pass (2^7 digests per block)
+constexpr int FLAT_LEVEL_MIN_LOG = 13;  // levels of at least 2^13 digests get their own launch
 
 // Tree layout: level l (2^(LL-l) digests of 8 words) starts at digest offset
 // 2^(LL+1) - 2^(LL+1-l).
@@ -211,25 +239,21 @@ __device__ __forceinline__ void subtree_reduce(uint32_t (*d)[8], int cnt, int le
   }
 }
 
-// Adds (sign +1) or subtracts (sign -1) the 16 row entries of chunk `ch` (columns
-// 16 ch .. 16 ch + 15, zero at and beyond n_cols) into x, or loads them (sign 0).
-__device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ row, int n_cols, bool vec4, int ch, int sign,
-                                           uint32_t* x) {
+// Adds (sign +1) or subtracts (sign -1) the 16 entries of chunk `ch` (columns 16 ch ..
+// 16 ch + 15, zero at and beyond n_cols) of LDE row `row` into x, or loads them (sign 0).
+// The LDE is tile-major with 2^T rows (n_cols a multiple of 8).
+__device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ lde, int T, size_t row, int n_cols, int ch,
+                                           int sign, uint32_t* x) {
   const int c0 = ch * 16;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     uint32_t v[4];
     const int c = c0 + 4 * q;
-    if (vec4) {
-      if (c < n_cols) {
-        const uint4 u = __ldg(reinterpret_cast<const uint4*>(row + c));
-        v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
-      } else {
-        v[0] = v[1] = v[2] = v[3] = 0u;
-      }
+    if (c < n_cols) {
+      const uint4 u = __ldg(reinterpret_cast<const uint4*>(lde + (((size_t(c >> 3) << T) + row) << 3) + (c & 7)));
+      v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
     } else {
-#pragma unroll
-      for (int e = 0; e < 4; e++) v[e] = c + e < n_cols ? __ldg(row + c + e) : 0u;
+      v[0] = v[1] = v[2] = v[3] = 0u;
     }
 #pragma unroll
     for (int e = 0; e < 4; e++) {
@@ -239,38 +263,35 @@ __device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ row, int
   }
 }
 
-// Leaf digests of 128 rows per block, then the first levels of the tree above them.
-// Each thread hashes one row of 128 entries with the width-24 sponge (16 entries per
+// Leaf digests (level 0 of the tree), one row per thread. Each thread hashes one row of 128 entries with the width-24 sponge (16 entries per
 // absorption), after the Moebius transform over the position bits [log_elem, 7) of the
 // column index: entry j becomes sum over i <= j (bitwise on those bits, equal elsewhere)
 // of (-1)^popcount(i ^ j) row[i]. Bits 4..6 select the 16-entry chunk, so chunk ch is the
 // signed sum of the chunks below it, and bits below 4 are transformed inside the chunk;
-// rows are read straight from global memory (no shared-memory staging, so occupancy
-// is bounded by registers).
-__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, size_t rows, int n_cols,
+// rows are read straight from the tile-major LDE (no shared-memory staging, so
+// occupancy is bounded by registers).
+__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, int T, int n_cols,
                                                          int log_elem, const __grid_constant__ kb::P24Consts c,
-                                                         const __grid_constant__ kb::P16Consts c16,
-                                                         uint32_t* __restrict__ tree, int LL, int levels) {
-  __shared__ uint32_t d[LEAF_ROWS][8];
+                                                         uint32_t* __restrict__ tree) {
   const size_t row0 = size_t(blockIdx.x) * LEAF_ROWS;
+  const size_t rows = size_t(1) << T;
   const int nrows = (rows - row0) < size_t(LEAF_ROWS) ? int(rows - row0) : LEAF_ROWS;
   const int t = threadIdx.x;
   uint32_t st[24];
   if (t < nrows) {
-    const uint32_t* row = lde + (row0 + t) * size_t(n_cols);
-    const bool vec4 = (n_cols & 3) == 0;
+    const size_t row = row0 + t;
     const int cmask = log_elem <= 4 ? 7 : (7 << (log_elem - 4)) & 7;  // chunk bits in the transform
 #pragma unroll
     for (int i = 0; i < 24; i++) st[i] = 0;
 #pragma unroll 1
     for (int ch = 0; ch < 8; ch++) {
-      leaf_chunk(row, n_cols, vec4, ch, 0, st);
+      leaf_chunk(lde, T, row, n_cols, ch, 0, st);
       const int m = ch & cmask;
       if (m) {
         // every proper subset of m, with the sign of the bits it drops
         for (int sub = (m - 1) & m;; sub = (sub - 1) & m) {
           const int sign = (__popc(m ^ sub) & 1) ? -1 : 1;
-          leaf_chunk(row, n_cols, vec4, (ch & ~m) | sub, sign, st);
+          leaf_chunk(lde, T, row, n_cols, (ch & ~m) | sub, sign, st);
           if (!sub) break;
         }
       }
@@ -284,15 +305,27 @@ __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restr
       }
       kb::p2_permute<24>(st, c);
     }
-    uint32_t* o = tree + (row0 + t) * 8;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      o[i] = st[i];
-      d[t][i] = st[i];
-    }
+    uint4* o = reinterpret_cast<uint4*>(tree + (row0 + t) * 8);
+    o[0] = make_uint4(st[0], st[1], st[2], st[3]);
+    o[1] = make_uint4(st[4], st[5], st[6], st[7]);
   }
-  __syncthreads();
-  subtree_reduce(d, nrows, levels, tree, LL, 0, row0, c16);
+}
+
+// Level l of the tree from level l - 1, one 2-to-1 compression per thread.
+__global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const __grid_constant__ kb::P16Consts c) {
+  const size_t m = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (m >= (size_t(1) << (LL - l))) return;
+  const uint4* src = reinterpret_cast<const uint4*>(tree + (tree_off(LL, l - 1) + 2 * m) * 8);
+  uint32_t st[16];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const uint4 u = src[q];
+    st[4 * q] = u.x, st[4 * q + 1] = u.y, st[4 * q + 2] = u.z, st[4 * q + 3] = u.w;
+  }
+  kb::p2_permute<16>(st, c);
+  uint4* o = reinterpret_cast<uint4*>(tree + (tree_off(LL, l) + m) * 8);
+  o[0] = make_uint4(st[0], st[1], st[2], st[3]);
+  o[1] = make_uint4(st[4], st[5], st[6], st[7]);
 }
 
 // Levels l0+1 .. l0+levels from 2^levels level-l0 digests per block.
@@ -305,6 +338,15 @@ __global__ void k_merkle_subtree(uint32_t* __restrict__ tree, int LL, int l0, in
   for (int i = threadIdx.x; i < cnt * 8; i += blockDim.x) d[i / 8][i % 8] = src[i];
   __syncthreads();
   subtree_reduce(d, cnt, levels, tree, LL, l0, first, c);
+}
+
+// Rows idx[q] of the tile-major LDE (2^T rows, n_cols columns) into out[q * n_cols + col].
+__global__ void k_gather_lde(const uint32_t* __restrict__ lde, int T, const uint64_t* __restrict__ idx, int n_cols,
+                             int n, uint32_t* __restrict__ out) {
+  const int q = blockIdx.x;
+  if (q >= n) return;
+  for (int c = threadIdx.x; c < n_cols; c += blockDim.x)
+    out[size_t(q) * n_cols + c] = lde[(((size_t(c >> 3) << T) + idx[q]) << 3) + (c & 7)];
 }
 
 __global__ void k_gather(const uint32_t* __restrict__ src, const uint64_t* __restrict__ idx, int width, int n,
@@ -368,44 +410,62 @@ void launch_trace_gen(const uint32_t* inputs, const AirConsts& K, uint32_t* wit,
 }
 
 void launch_twiddles(uint2* tw, cudaStream_t s) {
-  k_twiddles<<<(1u << 23) / 256, 256, 0, s>>>(tw, kb::two_adic_gen_m(24));
+  k_twiddles<<<(1u << 24) / 256, 256, 0, s>>>(tw, kb::two_adic_gen_m(24));
   WL_LAUNCH_CHECK();
 }
 
-void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint2* tw, cudaStream_t s) {
-  (void)tmp;
+void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s) {
   const int T = in.L + in.rho;
-  if (T > 2 * MAXB || T > 24) throw std::runtime_error("LDE size beyond two shared-memory passes");
-  const int tiles = (in.n_cols + CT - 1) / CT;
-  const int B0 = T <= MAXB ? T : (T + 1) / 2;
-  auto smem_for = [](int B) { return (((size_t(CT) * ((1u << B) + 1) + 1) & ~size_t(1)) + 2 * (size_t(1) << B)) * 4; };
-  const size_t smem_max = smem_for(MAXB);
-  WL_CUDA(cudaFuncSetAttribute(k_ntt_first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-  WL_CUDA(cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-  dim3 g1((unsigned)(size_t(1) << (T - B0)), tiles);
-  k_ntt_first<<<g1, NTT_THREADS, smem_for(B0), s>>>(in, B0, out, tw);
-  WL_LAUNCH_CHECK();
-  if (B0 < T) {
-    const int Bp = T - B0;
-    dim3 g2((unsigned)(size_t(1) << (T - Bp)), tiles);
-    k_ntt_mid<<<g2, NTT_THREADS, smem_for(Bp), s>>>(out, in.n_cols, B0, Bp, in.rho, tw);
+  if (T > 24) throw std::runtime_error("LDE beyond the two-adic subgroup of order 2^24");
+  if (in.n_cols % 8 || in.n_cols <= 0) throw std::runtime_error("LDE column count must be a multiple of 8");
+  const int tiles = in.n_cols / 8;
+  const int np = in.L <= NTT_MAX_BP ? 1 : (in.L + NTT_MAX_BP - 1) / NTT_MAX_BP;
+  int Bs = in.rho, left = in.L;
+  for (int p = 0; p < np; p++) {
+    const int Bp = (left + (np - p) - 1) / (np - p);
+    const int rb1 = (Bp + 1) / 2;
+    const int lr_log = Bs < 2 ? Bs : 2;
+    const int hi_bits = T - Bs - Bp;
+    const int hg_log = (2 - lr_log) < hi_bits ? (2 - lr_log) : hi_bits;
+    const unsigned gx = 1u << ((Bs - lr_log) + (hi_bits - hg_log));
+    const size_t smem = ((size_t(32) << Bp) + (size_t(2) << lr_log) * ((1u << Bp) - 1)) * 4;
+    if (p == 0) k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw);
+    else k_ntt_pass<false><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw);
     WL_LAUNCH_CHECK();
+    Bs += Bp;
+    left -= Bp;
   }
 }
 
 void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s) {
   const int log_elem = elem == 8 ? 3 : 0;
-  const int first_levels = LL < SUBTREE_LEVELS ? LL : SUBTREE_LEVELS;
-  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, rows, n_cols, log_elem, p24,
-                                                                                     p16, tree, LL, first_levels);
+  if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
+  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24,
+                                                                                     tree);
   WL_LAUNCH_CHECK();
-  for (int l0 = first_levels; l0 < LL; l0 += SUBTREE_LEVELS) {
+  // Wide levels one launch each (every SM busy); the narrow top of the tree in
+  // shared-memory subtrees of SUBTREE_LEVELS levels per launch.
+  int l0 = 0;
+  while (l0 < LL && LL - l0 - 1 >= FLAT_LEVEL_MIN_LOG) {
+    const size_t cnt = size_t(1) << (LL - l0 - 1);
+    k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16);
+    WL_LAUNCH_CHECK();
+    l0++;
+  }
+  for (; l0 < LL; l0 += SUBTREE_LEVELS) {
     const int lv = (LL - l0) < SUBTREE_LEVELS ? (LL - l0) : SUBTREE_LEVELS;
     const unsigned blocks = 1u << (LL - l0 - lv);
     k_merkle_subtree<<<blocks, 1 << (lv - 1), 0, s>>>(tree, LL, l0, lv, p16);
     WL_LAUNCH_CHECK();
   }
+}
+
+void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int n, uint32_t* out,
+                            cudaStream_t s) {
+  if (!n) return;
+  k_gather_lde<<<n, 128, 0, s>>>(lde, T, idx, n_cols, n, out);
+  WL_LAUNCH_CHECK();
 }
 
 void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s) {

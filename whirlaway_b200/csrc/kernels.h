@@ -27,17 +27,24 @@ struct LdeSource {
   int rho;       // log2 of the rate expansion
   int n_cols;    // stored columns per row (leading columns; the rest are zero)
 };
-void launch_lde(const LdeSource& in, uint32_t* tmp, uint32_t* out, const uint2* twiddles, cudaStream_t s);
-// Twiddle table: tw[j] = (w^j canonical, floor(w^j 2^32 / p)), w of order 2^24, j < 2^23.
+// Codeword matrix of 2^(L + rho) rows and n_cols (a multiple of 8) columns, tile-major:
+// word (tile, row, c) at (tile * 2^(L+rho) + row) * 8 + c.
+void launch_lde(const LdeSource& in, uint32_t* out, const uint2* twiddles, cudaStream_t s);
+// Per-stage twiddle table (2^24 - 1 entries): stage t = 1..24 holds (w canonical,
+// floor(w 2^32 / p)) for w = w_{2^t}^x, x < 2^(t-1), at offset 2^(t-1) - 1.
+constexpr size_t TWIDDLE_ENTRIES = (size_t(1) << 24) - 1;
 void launch_twiddles(uint2* tw, cudaStream_t s);
-// Merkle tree over the rows of an LDE matrix (rows of 128 values, the first `n_cols`
-// stored): leaf digests (each row Moebius-transformed over the bits [log2(elem), 7) of the
+// Merkle tree over the rows of a tile-major LDE matrix (rows of 128 values, the first
+// `n_cols` stored): leaf digests (each row Moebius-transformed over the bits [log2(elem), 7) of the
 // column index, then PaddingFreeSponge over Poseidon2-24) and 2-to-1 compressions
 // (Poseidon2-16), written level by level into `tree` (level l at digest offset
 // 2^(LL+1) - 2^(LL+1-l), LL = log2(rows)).
 void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s);
-// Gathers rows (raw, `n_cols` stored columns, zero padded to 128) and digests.
+// Gathers rows idx[q] of a tile-major LDE matrix (2^T rows) into out[q * n_cols + col].
+void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int n, uint32_t* out,
+                            cudaStream_t s);
+// Gathers rows of a row-major u32 matrix of the given width (Merkle digests: width 8).
 void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s);
 
 // --------------------------------------------------------------- PoW

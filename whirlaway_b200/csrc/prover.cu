@@ -55,7 +55,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
   WL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-  WL_CUDA(cudaMalloc(&twiddles, sizeof(uint2) << 23));
+  WL_CUDA(cudaMalloc(&twiddles, sizeof(uint2) * TWIDDLE_ENTRIES));
   launch_twiddles(twiddles, stream);
   pinned_bytes = kUpBytes + kDownBytes;
   WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
@@ -218,7 +218,7 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   if ((src.elem << fold) != 128) throw std::invalid_argument("leaf rows must hold 128 base-field values");
   const size_t rows = size_t(1) << c.log_leaves;
   c.lde = DBuf(rows * c.n_cols * sizeof(uint32_t), ctx.stream);
-  { ProfScope _ps(ctx, "lde"); launch_lde(src, nullptr, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
+  { ProfScope _ps(ctx, "lde"); launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
   const int LL = c.log_leaves;
   c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
   uint32_t* t = c.tree.as<uint32_t>();
@@ -246,7 +246,7 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   DBuf dr = upload(ctx, ridx), dd = upload(ctx, didx);
   DBuf rows(sizeof(uint32_t) * c.n_cols * std::max(nq, 1), ctx.stream);
   DBuf digs(sizeof(uint32_t) * 8 * std::max<size_t>(didx.size(), 1), ctx.stream);
-  { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.lde.as<uint32_t>(), dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream); }
+  { ProfScope _ps(ctx, "gather"); launch_gather_lde_rows(c.lde.as<uint32_t>(), LL, dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream); }
   { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream); }
   std::vector<uint32_t> hr(size_t(c.n_cols) * nq), hd(didx.size() * 8);
   if (nq) {

@@ -39,7 +39,7 @@ struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
   uint64_t hbm_budget = 0;
-  uint2* twiddles = nullptr;  // (w^j, floor(w^j 2^32 / p)) for w of order 2^24, j < 2^23
+  uint2* twiddles = nullptr;  // per-stage Shoup twiddles (launch_twiddles)
   void* pinned = nullptr;        // staging for small device-to-host reads
   size_t pinned_bytes = 0;
   std::string last_error;
