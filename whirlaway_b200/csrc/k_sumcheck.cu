@@ -182,67 +182,21 @@ __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, c
   out[size_t(c) * S + x] = m.acc;
 }
 
-constexpr int ZCE_T = 128;  // (x, z) points per block
+// ------------------------------------------------------------------ zerocheck rounds >= 1
+// One block per (x, z), x < 2^(m-1), z in {0, 2, 3}: the 148 batched constraints at the
+// point whose columns are lo + z (hi - lo) (lo, hi = the column at x and 2^(m-1) + x).
+//  * Warps 0-3: thread (seg, j), seg < 7, j < 16, one full-round constraint without state.
+//    For full round f with weights alpha_(c0+i), sum_i alpha_(c0+i) (MDS(cubes)_i - post_i)
+//    = sum_j beta_(f,j) cube_j - sum_i alpha_(c0+i) post_i with beta_f = MDS^T alpha (from
+//    the host); each round's input is committed: the previous round's post columns, or
+//    MDS(inputs) for the first round. seg 0..3 = beginning rounds, 4..6 = ending rounds 1..3.
+//  * Warp 4: the 20 partial rounds and ending round 0, whose input is the state after the
+//    partial rounds. Lane i < 16 holds state word i; the internal layer's sum is a shuffle
+//    reduction over the 16 lanes. The state continues from the committed partial post p_r,
+//    so the S-box of round r is off the chain: lane r keeps state word 0 of round r and the
+//    20 S-box constraints are evaluated in parallel after the loop.
+constexpr int ZCE_THREADS = 160;
 
-// The 16 extension-field state words of each thread live in shared memory as two planes
-// of uint4 (coordinates 0-3 and 4-7), so that a warp's 128-bit accesses are conflict-free.
-struct SmemState {
-  uint4* p0;
-  uint4* p1;
-  int t;
-  __device__ __forceinline__ ef get(int i) const {
-    uint4 a = p0[i * ZCE_T + t], b = p1[i * ZCE_T + t];
-    return ef{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
-  }
-  __device__ __forceinline__ void set(int i, const ef& v) const {
-    p0[i * ZCE_T + t] = make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]);
-    p1[i * ZCE_T + t] = make_uint4(v.c[4], v.c[5], v.c[6], v.c[7]);
-  }
-};
-
-__device__ __forceinline__ ef ef_diag16(int i, const ef& a) {
-  ef r;
-#pragma unroll
-  for (int k = 0; k < 8; k++) r.c[k] = p2_diag_mul<16>(i, a.c[k]);
-  return r;
-}
-
-__device__ void mds_light_smem(const SmemState& S) {
-#pragma unroll 1
-  for (int c = 0; c < 16; c += 4) {
-    ef x0 = S.get(c), x1 = S.get(c + 1), x2 = S.get(c + 2), x3 = S.get(c + 3);
-    ef t01 = ef_add(x0, x1), t23 = ef_add(x2, x3), t0123 = ef_add(t01, t23);
-    ef t01123 = ef_add(t0123, x1), t01233 = ef_add(t0123, x3);
-    S.set(c + 3, ef_add(t01233, ef_add(x0, x0)));
-    S.set(c + 1, ef_add(t01123, ef_add(x2, x2)));
-    S.set(c, ef_add(t01123, t01));
-    S.set(c + 2, ef_add(t01233, t23));
-  }
-#pragma unroll 1
-  for (int k = 0; k < 4; k++) {
-    ef a = S.get(k), b = S.get(4 + k), c = S.get(8 + k), d = S.get(12 + k);
-    ef sk = ef_add(ef_add(a, b), ef_add(c, d));
-    S.set(k, ef_add(a, sk));
-    S.set(4 + k, ef_add(b, sk));
-    S.set(8 + k, ef_add(c, sk));
-    S.set(12 + k, ef_add(d, sk));
-  }
-}
-
-// Internal layer with lane 0 replaced by x0.
-__device__ void internal_layer_smem_with0(const SmemState& S, const ef& x0) {
-  ef sum = x0;
-#pragma unroll 1
-  for (int i = 1; i < 16; i++) sum = ef_add(sum, S.get(i));
-  S.set(0, ef_add(ef_diag16(0, x0), sum));
-#pragma unroll 1
-  for (int i = 1; i < 16; i++) S.set(i, ef_add(ef_diag16(i, S.get(i)), sum));
-}
-
-constexpr int ZCE_FULL_SEGS = 7;  // full rounds evaluated without state
-constexpr int ZCE_SEGMENTS = ZCE_FULL_SEGS + 1;
-
-// 4x4 block M4 = [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]] applied to a chunk.
 __device__ __forceinline__ void m4_ef(ef& x0, ef& x1, ef& x2, ef& x3) {
   ef t01 = ef_add(x0, x1), t23 = ef_add(x2, x3), t0123 = ef_add(t01, t23);
   ef t01123 = ef_add(t0123, x1), t01233 = ef_add(t0123, x3);
@@ -256,125 +210,236 @@ __device__ __forceinline__ void m4_ef(ef& x0, ef& x1, ef& x2, ef& x3) {
   x3 = y3;
 }
 
-// Rounds >= 1, full rounds without state. For full round f with constraint weights
-// alpha_(c0 + i), sum_i alpha_(c0+i) (MDS(cubes)_i - post_i) = sum_j beta_(f,j) cube_j -
-// sum_i alpha_(c0+i) post_i, beta_f = MDS^T alpha (computed once on the host), and each
-// full round's input is committed: the previous round's post columns, or MDS(inputs) for
-// the first round (streamed: column sums of the M4 outputs, then chunk by chunk).
-// Block (x range, z, segment); segments 0..3 are the beginning rounds, 4..6 the ending
-// rounds 1..3. z = 0, 2, 3 for blockIdx.y = 0, 1, 2.
-__global__ void __launch_bounds__(ZCE_T, 4) k_zc_full_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
-                                                     const ef* __restrict__ alphas, const ef* __restrict__ betas,
-                                                     const __grid_constant__ AirConsts K, ef* __restrict__ partial) {
+__device__ __forceinline__ ef shfl_xor_ef(const ef& v, int d) {
+  ef r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.c[i] = __shfl_xor_sync(0xffffffffu, v.c[i], d);
+  return r;
+}
+__device__ __forceinline__ ef shfl_idx_ef(const ef& v, int src) {
+  ef r;
+#pragma unroll
+  for (int i = 0; i < 8; i++) r.c[i] = __shfl_sync(0xffffffffu, v.c[i], src);
+  return r;
+}
+
+__global__ void __launch_bounds__(ZCE_THREADS) k_zc_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
+                                                      const ef* __restrict__ alphas, const ef* __restrict__ betas,
+                                                      const __grid_constant__ AirConsts K, ef* __restrict__ partial) {
   const size_t len = size_t(1) << m, half = len >> 1;
-  const size_t x = size_t(blockIdx.x) * ZCE_T + threadIdx.x;
-  const int zi = blockIdx.y, seg = blockIdx.z;
-  const size_t xs = x < half ? x : 0;
+  const size_t x = blockIdx.x / 3;
+  const int zi = blockIdx.x - int(x) * 3;
   auto get = [&](int c) -> ef {
-    const ef lo = cols[size_t(c) * len + xs];
+    const ef lo = cols[size_t(c) * len + x];
     if (zi == 0) return lo;
-    const ef hi = cols[size_t(c) * len + half + xs];
+    const ef hi = cols[size_t(c) * len + half + x];
     ef d = ef_sub(hi, lo);
     ef v = ef_add(hi, d);               // z = 2: 2 hi - lo
     return zi == 1 ? v : ef_add(v, d);  // z = 3: 3 hi - 2 lo
   };
-  const int f = seg < 4 ? seg : seg + 1;  // full-round index 0..7 (4 = first ending round, not here)
-  const uint32_t* rc = seg < 4 ? K.begin[seg] : K.end[seg - 3];
-  const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
-  const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
-  const ef* beta = betas + 16 * f;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   ef acc = ef_zero();
-  if (seg == 0) {
-    ef S[4] = {ef_zero(), ef_zero(), ef_zero(), ef_zero()};
+  if (warp < 4) {
+    if (tid < 112) {
+      const int seg = tid >> 4, j = tid & 15;
+      const int f = seg < 4 ? seg : seg + 1;
+      const uint32_t rc = seg < 4 ? K.begin[seg][j] : K.end[seg - 3][j];
+      const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
+      const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
+      ef in;
+      if (seg == 0) {
+        // MDS(inputs)_j: the M4 output of chunk j / 4 plus the sum over chunks of position j % 4
+        const int q0 = j >> 2, k0 = j & 3;
+        ef S = ef_zero(), own = ef_zero();
 #pragma unroll 1
-    for (int q = 0; q < 4; q++) {
-      ef y0 = get(1 + 4 * q), y1 = get(2 + 4 * q), y2 = get(3 + 4 * q), y3 = get(4 + 4 * q);
-      m4_ef(y0, y1, y2, y3);
-      S[0] = ef_add(S[0], y0);
-      S[1] = ef_add(S[1], y1);
-      S[2] = ef_add(S[2], y2);
-      S[3] = ef_add(S[3], y3);
-    }
-#pragma unroll 1
-    for (int q = 0; q < 4; q++) {
-      ef y[4] = {get(1 + 4 * q), get(2 + 4 * q), get(3 + 4 * q), get(4 + 4 * q)};
-      m4_ef(y[0], y[1], y[2], y[3]);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const int j = 4 * q + kk;
-        const ef in = ef_add(y[kk], S[kk]);
-        acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(in, rc[j]))));
+        for (int q = 0; q < 4; q++) {
+          ef y[4] = {get(1 + 4 * q), get(2 + 4 * q), get(3 + 4 * q), get(4 + 4 * q)};
+          m4_ef(y[0], y[1], y[2], y[3]);
+          const ef yk = k0 == 0 ? y[0] : k0 == 1 ? y[1] : k0 == 2 ? y[2] : y[3];
+          S = ef_add(S, yk);
+          if (q == q0) own = yk;
+        }
+        in = ef_add(own, S);
+      } else {
+        in = get(post - 16 + j);
       }
+      acc = ef_sub(ef_mul(betas[16 * f + j], ef_cube(ef_add_f(in, rc))), ef_mul(alphas[c0 + j], get(post + j)));
     }
   } else {
-    const int src = post - 16;
+    const int i = lane & 15;
+    ef st = get(65 + i);                          // state after beginning round 3
+    const ef pr = lane < 20 ? get(81 + lane) : ef_zero();  // partial posts
+    const uint32_t dg = p2_diag<16>(i);
+    ef s0r = ef_zero();  // lane r: state word 0 at partial round r
 #pragma unroll 1
-    for (int j = 0; j < 16; j++) acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(get(src + j), rc[j]))));
+    for (int r = 0; r < 20; r++) {
+      const ef w0 = shfl_idx_ef(st, 0);
+      if (lane == r) s0r = w0;
+      const ef p = shfl_idx_ef(pr, r);
+      ef sp = i == 0 ? p : st;
+      ef sum = sp;
+#pragma unroll
+      for (int d = 8; d > 0; d >>= 1) sum = ef_add(sum, shfl_xor_ef(sum, d));
+      st = ef_add(ef_mul_f(sp, dg), sum);
+    }
+    if (lane < 20) {
+      const ef x0 = ef_cube(ef_add_f(s0r, K.partial[lane]));
+      acc = ef_mul(alphas[64 + lane], ef_sub(x0, pr));
+    }
+    if (lane < 16) {
+      const ef e = ef_sub(ef_mul(betas[16 * 4 + i], ef_cube(ef_add_f(st, K.end[0][i]))),
+                          ef_mul(alphas[84 + i], get(101 + i)));
+      acc = ef_add(acc, e);
+    }
   }
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) acc = ef_sub(acc, ef_mul(alphas[c0 + i], get(post + i)));
-  ef res = x < half ? ef_mul(acc, eq[x]) : ef_zero();
-  res = warp_reduce_ef(res);
-  __shared__ ef wsum[ZCE_T / 32];
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = res;
+  acc = warp_reduce_ef(acc);
+  __shared__ ef wsum[ZCE_THREADS / 32];
+  if (lane == 0) wsum[warp] = acc;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     ef tot = wsum[0];
-    for (int w = 1; w < ZCE_T / 32; w++) tot = ef_add(tot, wsum[w]);
-    partial[(size_t(blockIdx.x) * ZCE_FULL_SEGS + seg) * 3 + zi] = tot;
+#pragma unroll
+    for (int w = 1; w < ZCE_THREADS / 32; w++) tot = ef_add(tot, wsum[w]);
+    partial[blockIdx.x] = ef_mul(tot, eq[x]);
   }
 }
 
-// Rounds >= 1, the partial rounds and the first ending round, which starts from the state
-// after the partial rounds: the 16-word state lives in shared memory, loops stay rolled.
-__global__ void __launch_bounds__(ZCE_T) k_zc_partial_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq,
-                                                        const ef* __restrict__ alphas_g,
-                                                        const ef* __restrict__ betas,
-                                                        const __grid_constant__ AirConsts K,
-                                                        ef* __restrict__ partial) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  ef* alphas = reinterpret_cast<ef*>(smraw);
-  uint4* planes = reinterpret_cast<uint4*>(smraw + sizeof(ef) * AIR_NC);
-  for (int i = threadIdx.x; i < AIR_NC; i += ZCE_T) alphas[i] = alphas_g[i];
-  const SmemState S{planes, planes + 16 * ZCE_T, (int)threadIdx.x};
-  __syncthreads();
-  const size_t len = size_t(1) << m, half = len >> 1;
-  const size_t x = size_t(blockIdx.x) * ZCE_T + threadIdx.x;
-  const int zi = blockIdx.y;
-  const size_t xs = x < half ? x : 0;
-  auto get = [&](int c) -> ef {
-    const ef lo = cols[size_t(c) * len + xs];
-    if (zi == 0) return lo;
-    const ef hi = cols[size_t(c) * len + half + xs];
-    ef d = ef_sub(hi, lo);
-    ef v = ef_add(hi, d);
-    return zi == 1 ? v : ef_add(v, d);
-  };
-  ef acc = ef_zero();
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) S.set(i, get(65 + i));
-#pragma unroll 1
-  for (int r = 0; r < 20; r++) {
-    const ef x0 = ef_cube(ef_add_f(S.get(0), K.partial[r]));
-    const ef p = get(81 + r);
-    acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(x0, p)));
-    internal_layer_smem_with0(S, p);
-  }
-  const ef* beta = betas + 16 * 4;
-#pragma unroll 1
-  for (int j = 0; j < 16; j++) acc = ef_add(acc, ef_mul(beta[j], ef_cube(ef_add_f(S.get(j), K.end[0][j]))));
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) acc = ef_sub(acc, ef_mul(alphas[84 + i], get(101 + i)));
-  ef res = x < half ? ef_mul(acc, eq[x]) : ef_zero();
-  res = warp_reduce_ef(res);
-  __shared__ ef wsum[ZCE_T / 32];
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = res;
+// Dense forms of k_zc_ef for large rounds, in two kernels so that each keeps few
+// registers; both weight each point by eq[x] and write one partial sum per block and z
+// (blockIdx.y), first the full-round kernel's blocks, then the partial-round kernel's.
+//  * k_zc_full_dense: 16 lanes per point (2 points per warp); lane j evaluates constraint j
+//    of the 7 stateless full rounds. Beginning round 0 takes MDS(inputs): the lane's M4
+//    output plus the sum over the point's 4 chunks (two shuffles).
+//  * k_zc_partial_dense: 8 lanes per point (4 per warp); lane sub holds state words 2 sub,
+//    2 sub + 1 through the 20 partial rounds (the internal layer's sum is a local add plus
+//    three shuffles), keeps state word 0 of rounds r = sub (mod 8) for their S-box
+//    constraints, evaluated after the chain, and evaluates its two words of ending round 0.
+constexpr int ZCD_WARPS = 4;
+constexpr int ZCD_FULL_PTS = ZCD_WARPS * 2;     // points per block
+constexpr int ZCD_PARTIAL_PTS = ZCD_WARPS * 4;
+
+template <int PTS>
+__device__ __forceinline__ void zcd_block_store(ef v, ef* __restrict__ partial, size_t blk, int zi) {
+  __shared__ ef wsum[ZCD_WARPS];
+  v = warp_reduce_ef(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wsum[warp] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
-    ef tot = wsum[0];
-    for (int w = 1; w < ZCE_T / 32; w++) tot = ef_add(tot, wsum[w]);
-    partial[size_t(blockIdx.x) * 3 + zi] = tot;
+    ef t = wsum[0];
+#pragma unroll
+    for (int w = 1; w < ZCD_WARPS; w++) t = ef_add(t, wsum[w]);
+    partial[blk * 3 + zi] = t;
   }
+}
+
+#define ZCD_GET                                                            \
+  auto get = [&](int c) -> ef {                                             \
+    const ef lo = cols[size_t(c) * len + xs];                               \
+    if (zi == 0) return lo;                                                 \
+    const ef hi = cols[size_t(c) * len + half + xs];                        \
+    ef d = ef_sub(hi, lo);                                                  \
+    ef v = ef_add(hi, d);                                                   \
+    return zi == 1 ? v : ef_add(v, d);                                      \
+  }
+
+__global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_full_dense(const ef* __restrict__ cols, int m,
+                                                                 const ef* __restrict__ eq,
+                                                                 const ef* __restrict__ alphas,
+                                                                 const ef* __restrict__ betas,
+                                                                 const __grid_constant__ AirConsts K,
+                                                                 ef* __restrict__ partial) {
+  const size_t len = size_t(1) << m, half = len >> 1;
+  const int lane = threadIdx.x & 31, zi = blockIdx.y;
+  const int j = lane & 15;
+  const size_t x = size_t(blockIdx.x) * ZCD_FULL_PTS + (threadIdx.x >> 4);
+  const bool valid = x < half;
+  const size_t xs = valid ? x : 0;
+  ZCD_GET;
+  ef in;
+  {
+    const int q = j >> 2;
+    ef y0 = get(1 + 4 * q), y1 = get(2 + 4 * q), y2 = get(3 + 4 * q), y3 = get(4 + 4 * q);
+    m4_ef(y0, y1, y2, y3);
+    const int k0 = j & 3;
+    const ef y = k0 == 0 ? y0 : k0 == 1 ? y1 : k0 == 2 ? y2 : y3;
+    ef t = ef_add(y, shfl_xor_ef(y, 4));
+    t = ef_add(t, shfl_xor_ef(t, 8));
+    in = ef_add(y, t);
+  }
+  ef acc = ef_zero();
+#pragma unroll 1
+  for (int seg = 0; seg < 7; seg++) {
+    const int f = seg < 4 ? seg : seg + 1;
+    const uint32_t rc = seg < 4 ? K.begin[seg][j] : K.end[seg - 3][j];
+    const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
+    const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
+    if (seg > 0) in = get(post - 16 + j);
+    const ef pv = get(post + j);
+    acc = ef_add(acc, ef_sub(ef_mul(betas[16 * f + j], ef_cube(ef_add_f(in, rc))), ef_mul(alphas[c0 + j], pv)));
+  }
+  // fold the point's 16 lanes, weight by eq, then the block sum
+  ef pt = acc;
+#pragma unroll
+  for (int d = 8; d > 0; d >>= 1) pt = ef_add(pt, shfl_xor_ef(pt, d));
+  const ef res = (j == 0 && valid) ? ef_mul(pt, eq[xs]) : ef_zero();
+  zcd_block_store<ZCD_FULL_PTS>(res, partial, blockIdx.x, zi);
+}
+
+__global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* __restrict__ cols, int m,
+                                                                    const ef* __restrict__ eq,
+                                                                    const ef* __restrict__ alphas,
+                                                                    const ef* __restrict__ betas,
+                                                                    const __grid_constant__ AirConsts K,
+                                                                    ef* __restrict__ partial) {
+  const size_t len = size_t(1) << m, half = len >> 1;
+  const int lane = threadIdx.x & 31, zi = blockIdx.y;
+  const int sub = lane & 7, gbase = lane & ~7;
+  const size_t x = size_t(blockIdx.x) * ZCD_PARTIAL_PTS + (threadIdx.x >> 3);
+  const bool valid = x < half;
+  const size_t xs = valid ? x : 0;
+  ZCD_GET;
+  ef st[2], pslot[3], s0slot[3];
+  uint32_t dg[2];
+#pragma unroll
+  for (int kk = 0; kk < 2; kk++) {
+    st[kk] = get(65 + 2 * sub + kk);
+    dg[kk] = p2_diag<16>(2 * sub + kk);
+  }
+#pragma unroll
+  for (int t = 0; t < 3; t++) pslot[t] = (8 * t + sub < 20) ? get(81 + 8 * t + sub) : ef_zero();
+#pragma unroll
+  for (int r = 0; r < 20; r++) {
+    const int t = r >> 3, owner = r & 7;
+    const ef w0 = shfl_idx_ef(st[0], gbase);
+    if (sub == owner) s0slot[t] = w0;
+    const ef p = shfl_idx_ef(pslot[t], gbase | owner);
+    if (sub == 0) st[0] = p;
+    ef sum = ef_add(st[0], st[1]);
+    sum = ef_add(sum, shfl_xor_ef(sum, 1));
+    sum = ef_add(sum, shfl_xor_ef(sum, 2));
+    sum = ef_add(sum, shfl_xor_ef(sum, 4));
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) st[kk] = ef_add(ef_mul_f(st[kk], dg[kk]), sum);
+  }
+  ef acc = ef_zero();
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int r = 8 * t + sub;
+    if (r < 20)
+      acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(ef_cube(ef_add_f(s0slot[t], K.partial[r])), pslot[t])));
+  }
+#pragma unroll
+  for (int kk = 0; kk < 2; kk++) {
+    const int j = 2 * sub + kk;
+    acc = ef_add(acc, ef_sub(ef_mul(betas[16 * 4 + j], ef_cube(ef_add_f(st[kk], K.end[0][j]))),
+                             ef_mul(alphas[84 + j], get(101 + j))));
+  }
+  ef pt = acc;
+#pragma unroll
+  for (int d = 4; d > 0; d >>= 1) pt = ef_add(pt, shfl_xor_ef(pt, d));
+  const ef res = (sub == 0 && valid) ? ef_mul(pt, eq[xs]) : ef_zero();
+  zcd_block_store<ZCD_PARTIAL_PTS>(res, partial, blockIdx.x, zi);
 }
 
 __global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, int ncols,
@@ -655,19 +720,26 @@ void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* o
   k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
-int zc_ef_blocks(int m) {  // partial sums per z: (x blocks) x (7 full-round segments + 1)
-  size_t half = size_t(1) << (m - 1);
-  return (int)((half + ZCE_T - 1) / ZCE_T) * ZCE_SEGMENTS;
+// Rounds with at least ZC_DENSE_MIN_HALF points per z use the dense kernels.
+constexpr size_t ZC_DENSE_MIN_HALF = size_t(1) << 10;
+int zc_ef_blocks(int m) {  // partial sums per z
+  const size_t half = size_t(1) << (m - 1);
+  if (half < ZC_DENSE_MIN_HALF) return (int)half;
+  return (int)((half + ZCD_FULL_PTS - 1) / ZCD_FULL_PTS + (half + ZCD_PARTIAL_PTS - 1) / ZCD_PARTIAL_PTS);
 }
 void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K,
                        ef* partial, cudaStream_t s) {
-  const unsigned xb = (unsigned)(zc_ef_blocks(m) / ZCE_SEGMENTS);
-  k_zc_full_ef<<<dim3(xb, 3, ZCE_FULL_SEGS), ZCE_T, 0, s>>>(cols, m, eq, alphas, betas, K, partial);
-  WL_LAUNCH_CHECK();
-  const size_t smem = sizeof(ef) * AIR_NC + sizeof(uint4) * 2 * 16 * ZCE_T;
-  WL_CUDA(cudaFuncSetAttribute(k_zc_partial_ef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_zc_partial_ef<<<dim3(xb, 3), ZCE_T, smem, s>>>(cols, m, eq, alphas, betas, K,
-                                                   partial + size_t(xb) * ZCE_FULL_SEGS * 3);
+  const size_t half = size_t(1) << (m - 1);
+  if (half >= ZC_DENSE_MIN_HALF) {
+    const unsigned bf = (unsigned)((half + ZCD_FULL_PTS - 1) / ZCD_FULL_PTS);
+    const unsigned bp = (unsigned)((half + ZCD_PARTIAL_PTS - 1) / ZCD_PARTIAL_PTS);
+    k_zc_full_dense<<<dim3(bf, 3), ZCD_WARPS * 32, 0, s>>>(cols, m, eq, alphas, betas, K, partial);
+    WL_LAUNCH_CHECK();
+    k_zc_partial_dense<<<dim3(bp, 3), ZCD_WARPS * 32, 0, s>>>(cols, m, eq, alphas, betas, K,
+                                                              partial + size_t(bf) * 3);
+  } else {
+    k_zc_ef<<<(unsigned)(half * 3), ZCE_THREADS, 0, s>>>(cols, m, eq, alphas, betas, K, partial);
+  }
   WL_LAUNCH_CHECK();
 }
 void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s, const ef* eq_in,
