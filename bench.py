@@ -196,6 +196,9 @@ def run_reference(args, world, rank):
 
 
 # ----------------------------------------------------------------------------- GPU arm
+LEAF_EXTRA_DRAM_BYTES = 22.5  # measured DRAM bytes per leaf row beyond the row itself
+
+
 def whir_rows_hashed(log_n):
     """Leaf rows hashed per proof (all WHIR commitments) under the default parameters."""
     m = log_n + 8
@@ -226,8 +229,14 @@ def roofline(profile, log_n, modmul_peak, hbm_peak_gbs, launches_per_step, steps
         perms = (sum(rows) * 8 + sum(rows) * P16_MODMUL / P24_MODMUL) * steps
         byts = (rows[0] * (88 * 4 + 64) + sum(r * (128 * 4 + 64) for r in rows[1:])) * steps
         achieved = perms / (ms * 1e-3) / 1e9
+        # DRAM traffic per Merkle build: ncu's dram__bytes_read.sum + dram__bytes_write.sum of the
+        # leaf kernel at 2^17 rows was 374.5 B per 88-column row (the row once plus 22.5 B of digest
+        # and tree traffic); scaled by rows, with 128-column rows for the later commitments.
+        traffic = (rows[0] * (88 * 4 + LEAF_EXTRA_DRAM_BYTES)
+                   + sum(r * (128 * 4 + LEAF_EXTRA_DRAM_BYTES) for r in rows[1:])) * steps / max(launches, 1)
         out.update({"bound": "int", "achieved": achieved, "peak": p24_peak / 1e9, "unit": "G Poseidon2-24 perms/s",
-                    "frac": achieved * 1e9 / p24_peak, "traffic": None,
+                    "frac": achieved * 1e9 / p24_peak, "traffic": traffic,
+                    "traffic_source": "ncu capture at 2^17 rows scaled by rows (profiles/top_kernels_2p17_rows.md)",
                     "peak_source": "measured in this run: back-to-back Poseidon2-24 permutations from registers",
                     "modmul_view": {"achieved": perms * P24_MODMUL / (ms * 1e-3) / 1e9, "peak": modmul_peak / 1e9,
                                     "unit": "Gmodmul/s (standard count: 982 per Poseidon2-24)"},
