@@ -162,6 +162,15 @@ wl_status wl_server_wait(wl_server* server, uint64_t ticket, uint32_t* proof_out
                          double* times_ms);
 wl_status wl_server_stats(wl_server* server, uint64_t* peak_bytes_admitted, int32_t* peak_running);
 
+// Restricts the profiling of wl_profile_enable to one kernel class (NULL or "" = all), so
+// that a timed region can carry the events of its dominant kernel only. No reference
+// counterpart.
+wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class);
+
+// Number of host synchronisations of the context's stream so far (device-to-host reads
+// of challenges, sums and roots). Diagnostics; no reference counterpart.
+wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out);
+
 /* Instrumentation (no reference counterpart; the reference profiles with tracing spans,
  * src/examples/poseidon2.rs:91-100). With profiling on, every kernel class launched on the
  * context is bracketed by CUDA events on the context's stream; wl_profile_json writes

@@ -109,6 +109,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_server_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32)]),
         "wl_profile_enable": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
+        "wl_ctx_host_syncs": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "wl_profile_only": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double)]),
     }
@@ -170,8 +172,10 @@ class Context:
         """Raw cudaStream_t the library launches on (for torch.cuda.ExternalStream)."""
         return self._lib.wl_ctx_stream(self.handle) or 0
 
-    def profile(self, on: bool = True):
-        """Starts (or stops) per-kernel-class CUDA-event timing; totals restart."""
+    def profile(self, on: bool = True, only: str | None = None):
+        """Starts (or stops) per-kernel-class CUDA-event timing; totals restart. With `only`,
+        just that kernel class is timed."""
+        self.check(self._lib.wl_profile_only(self.handle, (only or "").encode()), "profile_only")
         self.check(self._lib.wl_profile_enable(self.handle, int(on)), "profile_enable")
 
     def profile_report(self) -> dict:
@@ -180,6 +184,13 @@ class Context:
         buf = ctypes.create_string_buffer(1 << 16)
         self.check(self._lib.wl_profile_json(self.handle, buf, len(buf)), "profile_json")
         return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
+
+    @property
+    def host_syncs(self) -> int:
+        """Host synchronisations of this context's stream so far."""
+        v = ctypes.c_uint64()
+        self.check(self._lib.wl_ctx_host_syncs(self.handle, ctypes.byref(v)), "host_syncs")
+        return v.value
 
     def probe_int_peaks(self, constants: np.ndarray):
         """Measured (Montgomery products/s, Poseidon2-24 permutations/s) from registers."""

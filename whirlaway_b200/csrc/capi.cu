@@ -309,6 +309,20 @@ wl_status wl_profile_enable(wl_ctx* ctx, int32_t on) {
   });
 }
 
+wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  return guarded(ctx, [&] {
+    ctx->c->profile_only = kernel_class ? kernel_class : "";
+    return WL_OK;
+  });
+}
+
+wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out) {
+  if (!ctx || !out) return WL_E_INVALID_ARG;
+  *out = ctx->c->host_syncs;
+  return WL_OK;
+}
+
 wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
   if (!ctx || !buf) return WL_E_INVALID_ARG;
   return guarded(ctx, [&] {

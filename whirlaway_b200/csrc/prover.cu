@@ -95,7 +95,7 @@ void Context::prof_flush() {
   pending.clear();
 }
 ProfScope::ProfScope(Context& ctx, const char* n) : c(ctx), name(n) {
-  if (!c.profile) return;
+  if (!c.profile || (!c.profile_only.empty() && c.profile_only != n)) return;
   a = c.take_event();
   WL_CUDA(cudaEventRecord(a, c.stream));
 }
@@ -111,27 +111,31 @@ ProfScope::~ProfScope() {
   c.pending.push_back({name, a, b});
 }
 
+void Context::wait_stream() {
+  WL_CUDA(cudaStreamSynchronize(stream));
+  host_syncs++;
+}
 void Context::to_host(void* dst, const void* src, size_t bytes) {
   char* down = static_cast<char*>(pinned) + kUpBytes;
   if (bytes <= kDownBytes) {
     WL_CUDA(cudaMemcpyAsync(down, src, bytes, cudaMemcpyDeviceToHost, stream));
-    WL_CUDA(cudaStreamSynchronize(stream));
+    wait_stream();
     memcpy(dst, down, bytes);
   } else {
     WL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
-    WL_CUDA(cudaStreamSynchronize(stream));
+    wait_stream();
   }
   g_up_off = 0;  // every earlier upload has completed
 }
 void Context::to_device(void* dst, const void* src, size_t bytes) {
   if (bytes > kUpBytes) {
     WL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
-    WL_CUDA(cudaStreamSynchronize(stream));
+    wait_stream();
     g_up_off = 0;
     return;
   }
   if (g_up_off + bytes > kUpBytes) {
-    WL_CUDA(cudaStreamSynchronize(stream));
+    wait_stream();
     g_up_off = 0;
   }
   char* up = static_cast<char*>(pinned) + g_up_off;

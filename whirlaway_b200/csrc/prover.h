@@ -43,13 +43,16 @@ struct Context {
   void* pinned = nullptr;        // staging for small device-to-host reads
   size_t pinned_bytes = 0;
   std::string last_error;
+  uint64_t host_syncs = 0;  // stream synchronisations made by the host (diagnostics)
   Context(int device, uint64_t budget);
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
+  void wait_stream();  // host synchronisation with `stream` (counted in host_syncs)
   void to_device(void* dst, const void* src, size_t bytes);
 
   // Optional per-kernel-class timing with CUDA events on `stream`.
   bool profile = false;
+  std::string profile_only;  // when set, only this kernel class is timed
   struct Pending {
     std::string name;
     cudaEvent_t a, b;
