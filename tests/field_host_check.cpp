@@ -27,6 +27,75 @@ int main() {
     uint32_t x = g() % P, xm = to_mont(x);
     for (int i = 0; i < 24; i++) if (p2_diag_mul<24>(i, xm) != mul(xm, p2_diag<24>(i))) b4++;
   }
-  printf("add %ld sub %ld mul %ld diag %ld halve %ld redc %ld\n", b1,b2,b3,b4,b5,b6);
-  return (b1 + b2 + b3 + b4 + b5 + b6) ? 1 : 0;
+  // cube (lazy inner square), the lazily reduced sums and whole permutations against plain
+  // modular arithmetic
+  long b7 = 0, b8 = 0;
+  for (int it = 0; it < 100000; it++) {
+    uint32_t v[23];
+    uint64_t ref = 0;
+    const bool top = it & 1;  // values at the top of the range
+    for (int i = 0; i < 23; i++) v[i] = top ? P - 1 - uint32_t(g() % 7) : uint32_t(g() % P), ref += v[i];
+    uint32_t x0 = top ? P - 1 : uint32_t(g() % P);
+    if (sum_mod<23>(v, x0) != uint32_t((ref + x0) % P)) b7++;
+    if (sum_mod<15>(v, x0) != uint32_t((ref - v[15] - v[16] - v[17] - v[18] - v[19] - v[20] - v[21] - v[22] + x0) % P)) b7++;
+  }
+  auto pm = [](uint64_t a, uint64_t b) { return uint32_t(a * b % P); };
+  for (int it = 0; it < 100000; it++) {
+    uint32_t x = g() % P;
+    if (from_mont(cube(to_mont(x))) != pm(pm(x, x), x)) b7++;
+  }
+  for (int w = 0; w < 2; w++) {
+    const int W = w ? 24 : 16, RP = w ? 23 : 20;
+    for (int it = 0; it < 300; it++) {
+      P16Consts c16;
+      P24Consts c24;
+      uint32_t* ei = w ? c24.ext_init : c16.ext_init;
+      uint32_t* et = w ? c24.ext_term : c16.ext_term;
+      uint32_t* in = w ? c24.internal : c16.internal;
+      for (int i = 0; i < 4 * W; i++) ei[i] = to_mont(g() % P), et[i] = to_mont(g() % P);
+      for (int i = 0; i < RP; i++) in[i] = to_mont(g() % P);
+      uint32_t s[24], r[24];
+      for (int i = 0; i < W; i++) s[i] = g() % P, r[i] = s[i];
+      // reference on canonical values: diag entries and constants through from_mont
+      auto mds = [&](uint32_t* v) {
+        uint32_t t[24];
+        for (int c = 0; c < W; c += 4)
+          for (int i = 0; i < 4; i++) {
+            static const int M4[4][4] = {{2, 3, 1, 1}, {1, 2, 3, 1}, {1, 1, 2, 3}, {3, 1, 1, 2}};
+            uint64_t a = 0;
+            for (int j = 0; j < 4; j++) a += uint64_t(M4[i][j]) * v[c + j];
+            t[c + i] = uint32_t(a % P);
+          }
+        for (int i = 0; i < W; i++) {
+          uint64_t a = t[i];
+          for (int c = 0; c < W; c += 4) a += t[c + (i & 3)];
+          v[i] = uint32_t(a % P);
+        }
+      };
+      auto cub = [&](uint32_t x) { return pm(pm(x, x), x); };
+      mds(r);
+      for (int rd = 0; rd < 4; rd++) {
+        for (int i = 0; i < W; i++) r[i] = cub(uint32_t((uint64_t(r[i]) + from_mont(ei[rd * W + i])) % P));
+        mds(r);
+      }
+      for (int rd = 0; rd < RP; rd++) {
+        r[0] = cub(uint32_t((uint64_t(r[0]) + from_mont(in[rd])) % P));
+        uint64_t sum = 0;
+        for (int i = 0; i < W; i++) sum += r[i];
+        for (int i = 0; i < W; i++) {
+          const uint32_t d = from_mont(w ? p2_diag<24>(i) : p2_diag<16>(i));
+          r[i] = uint32_t((uint64_t(pm(d, r[i])) + sum) % P);
+        }
+      }
+      for (int rd = 0; rd < 4; rd++) {
+        for (int i = 0; i < W; i++) r[i] = cub(uint32_t((uint64_t(r[i]) + from_mont(et[rd * W + i])) % P));
+        mds(r);
+      }
+      for (int i = 0; i < W; i++) s[i] = to_mont(s[i]);
+      if (w) p2_permute<24>(s, c24); else p2_permute<16>(s, c16);
+      for (int i = 0; i < W; i++) if (from_mont(s[i]) != r[i]) { b8++; break; }
+    }
+  }
+  printf("add %ld sub %ld mul %ld diag %ld halve %ld redc %ld cube %ld permute %ld\n", b1,b2,b3,b4,b5,b6,b7,b8);
+  return (b1 + b2 + b3 + b4 + b5 + b6 + b7 + b8) ? 1 : 0;
 }

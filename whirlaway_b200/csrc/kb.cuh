@@ -69,13 +69,13 @@ KB_HD uint32_t redc(uint64_t t) {
   r = hi < mh ? r + P : r;
   return umin(r, r - P);
 }
-// x * 2^-k for 1 <= k <= 31 (Montgomery form is preserved): REDC(x * 2^(32 - k)).
+// x * 2^-k for 1 <= k <= 31 (Montgomery form is preserved): REDC(x * 2^(32 - k)). The
+// low word of x * 2^(32 - k) times PINV is x times the constant PINV * 2^(32 - k) mod 2^32.
 KB_HD uint32_t mul_inv_pow2(uint32_t x, int k) {
-  uint64_t t = uint64_t(x) << (32 - k);
-  uint32_t lo = uint32_t(t), hi = uint32_t(t >> 32);
-  uint32_t m = lo * PINV;
-  uint32_t mh = umulhi(m, P);
-  uint32_t r = hi - mh;
+  const uint32_t hi = x >> k;
+  const uint32_t m = x * (PINV << (32 - k));
+  const uint32_t mh = umulhi(m, P);
+  const uint32_t r = hi - mh;
   return umin(r, r + P);
 }
 KB_HD uint32_t halve(uint32_t x) { return (x & 1) ? (x >> 1) + ((P + 1) >> 1) : (x >> 1); }
@@ -83,7 +83,16 @@ KB_HD uint64_t wmul(uint32_t a, uint32_t b) { return uint64_t(a) * b; }
 
 KB_HD uint32_t to_mont(uint32_t x) { return mul(x % P, R2_MOD_P); }
 KB_HD uint32_t from_mont(uint32_t x) { return mul(x, 1u); }
-KB_HD uint32_t cube(uint32_t x) { return mul(mul(x, x), x); }
+// Montgomery product left in (0, 2p) instead of [0, p): hi - mh lies in (-p, p/2) for
+// a, b < p, so adding p replaces the sign fix. Only for feeding another product.
+KB_HD uint32_t mul_lazy(uint32_t a, uint32_t b) {
+  uint32_t lo = a * b, hi = umulhi(a, b);
+  uint32_t m = lo * PINV;
+  uint32_t mh = umulhi(m, P);
+  return hi - mh + P;
+}
+// x^3 for x < p: (x^2 in (0, 2p)) * x < 2 p^2 keeps the second product's hi word below p.
+KB_HD uint32_t cube(uint32_t x) { return mul(mul_lazy(x, x), x); }
 
 inline uint32_t pow_m(uint32_t a, uint64_t e) {  // Montgomery in, Montgomery out
   uint32_t r = R_MOD_P;

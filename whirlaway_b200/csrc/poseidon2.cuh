@@ -83,20 +83,26 @@ KB_HD constexpr uint32_t p2_diag(int i) {
   }
 }
 
-// v * x for the diagonal entry v = V_i, using doublings, halvings and shifted reductions
-// instead of a general product; equal to mul(x, p2_diag<W>(i)).
+// Sign of the diagonal entry V_i.
 template <int W>
-KB_HD uint32_t p2_diag_mul(int i, uint32_t x) {
+KB_HD constexpr bool p2_diag_neg(int i) {
+  if (i == 0 || i == 6 || i == 7 || i == 8) return true;
+  return W == 16 ? i >= 12 : i >= 16;
+}
+
+// |V_i| * x using doublings, halvings and shifted reductions instead of a general product.
+template <int W>
+KB_HD uint32_t p2_diag_mag(int i, uint32_t x) {
   switch (i) {
-    case 0: return neg(dbl(x));
+    case 0: return dbl(x);
     case 1: return x;
     case 2: return dbl(x);
     case 3: return halve(x);
     case 4: return add(dbl(x), x);
     case 5: return dbl(dbl(x));
-    case 6: return neg(halve(x));
-    case 7: return neg(add(dbl(x), x));
-    case 8: return neg(dbl(dbl(x)));
+    case 6: return halve(x);
+    case 7: return add(dbl(x), x);
+    case 8: return dbl(dbl(x));
     case 9: return mul_inv_pow2(x, 8);
     default: break;
   }
@@ -104,10 +110,10 @@ KB_HD uint32_t p2_diag_mul(int i, uint32_t x) {
     switch (i) {
       case 10: return mul_inv_pow2(x, 3);
       case 11: return mul_inv_pow2(x, 24);
-      case 12: return neg(mul_inv_pow2(x, 8));
-      case 13: return neg(mul_inv_pow2(x, 3));
-      case 14: return neg(mul_inv_pow2(x, 4));
-      default: return neg(mul_inv_pow2(x, 24));
+      case 12: return mul_inv_pow2(x, 8);
+      case 13: return mul_inv_pow2(x, 3);
+      case 14: return mul_inv_pow2(x, 4);
+      default: return mul_inv_pow2(x, 24);
     }
   }
   switch (i) {
@@ -117,15 +123,29 @@ KB_HD uint32_t p2_diag_mul(int i, uint32_t x) {
     case 13: return mul_inv_pow2(x, 5);
     case 14: return mul_inv_pow2(x, 6);
     case 15: return mul_inv_pow2(x, 24);
-    case 16: return neg(mul_inv_pow2(x, 8));
-    case 17: return neg(mul_inv_pow2(x, 3));
-    case 18: return neg(mul_inv_pow2(x, 4));
-    case 19: return neg(mul_inv_pow2(x, 5));
-    case 20: return neg(mul_inv_pow2(x, 6));
-    case 21: return neg(mul_inv_pow2(x, 7));
-    case 22: return neg(mul_inv_pow2(x, 9));
-    default: return neg(mul_inv_pow2(x, 24));
+    case 16: return mul_inv_pow2(x, 8);
+    case 17: return mul_inv_pow2(x, 3);
+    case 18: return mul_inv_pow2(x, 4);
+    case 19: return mul_inv_pow2(x, 5);
+    case 20: return mul_inv_pow2(x, 6);
+    case 21: return mul_inv_pow2(x, 7);
+    case 22: return mul_inv_pow2(x, 9);
+    default: return mul_inv_pow2(x, 24);
   }
+}
+
+// V_i * x; equal to mul(x, p2_diag<W>(i)).
+template <int W>
+KB_HD uint32_t p2_diag_mul(int i, uint32_t x) {
+  const uint32_t m = p2_diag_mag<W>(i, x);
+  return p2_diag_neg<W>(i) ? neg(m) : m;
+}
+
+// V_i * x + sum, subtracting |V_i| x for the negative entries (no separate negation).
+template <int W>
+KB_HD uint32_t p2_diag_mul_add(int i, uint32_t x, uint32_t sum) {
+  const uint32_t m = p2_diag_mag<W>(i, x);
+  return p2_diag_neg<W>(i) ? sub(sum, m) : add(m, sum);
 }
 
 template <int W>
@@ -172,14 +192,28 @@ KB_HD void mds_light(uint32_t* s) {
   for (int i = 0; i < W; i++) s[i] = add(s[i], sums[i & 3]);
 }
 
+// (v[0] + ... + v[N-1] + x0) mod p for values < p: pairs are added without carry (each pair
+// is below 2^32), the pair sums in 64 bits (below 2^36), then the total is folded with
+// 2^32 = 2^25 - 2 and 2^31 = 2^24 - 1 (mod p) to below 2p and reduced once.
+template <int N>
+KB_HD uint32_t sum_mod(const uint32_t* v, uint32_t x0) {
+  uint64_t a = x0;
+#pragma unroll
+  for (int i = 0; i + 1 < N; i += 2) a += uint32_t(v[i] + v[i + 1]);
+  if (N & 1) a += v[N - 1];
+  const uint64_t b = uint64_t(uint32_t(a)) + uint64_t(uint32_t(a >> 32)) * ((1u << 25) - 2);  // < 2^33
+  const uint32_t c = (uint32_t(b) & 0x7fffffffu) + uint32_t(b >> 31) * ((1u << 24) - 1);        // < 2p
+  return umin(c, c - P);
+}
+
 // Internal layer applied to the state with s[0] replaced by x0 (the S-box output of a
 // partial round); the sum of the other lanes does not wait for the S-box.
 template <int W>
 KB_HD void internal_layer_with0(uint32_t* s, uint32_t x0) {
-  const uint32_t sum = add(tree_sum<W - 1>(s + 1), x0);
-  s[0] = add(p2_diag_mul<W>(0, x0), sum);
+  const uint32_t sum = sum_mod<W - 1>(s + 1, x0);
+  s[0] = p2_diag_mul_add<W>(0, x0, sum);
 #pragma unroll
-  for (int i = 1; i < W; i++) s[i] = add(p2_diag_mul<W>(i, s[i]), sum);
+  for (int i = 1; i < W; i++) s[i] = p2_diag_mul_add<W>(i, s[i], sum);
 }
 template <int W>
 KB_HD void internal_layer(uint32_t* s) {
