@@ -167,6 +167,12 @@ wl_status wl_server_stats(wl_server* server, uint64_t* peak_bytes_admitted, int3
 // counterpart.
 wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class);
 
+// How the prover waits for the device at each transcript round trip: 1 (the default for a
+// context) busy-polls an event, keeping the calling thread on its CPU so that no OS wake-up
+// delays the next round; 0 blocks in cudaStreamSynchronize (the default of server workers).
+// No reference counterpart.
+wl_status wl_ctx_set_spin_sync(wl_ctx* ctx, int32_t spin);
+
 // Number of host synchronisations of the context's stream so far (device-to-host reads
 // of challenges, sums and roots). Diagnostics; no reference counterpart.
 wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out);

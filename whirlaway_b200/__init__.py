@@ -110,6 +110,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_profile_enable": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "wl_ctx_host_syncs": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "wl_ctx_set_spin_sync": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_profile_only": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double)]),
@@ -184,6 +185,10 @@ class Context:
         buf = ctypes.create_string_buffer(1 << 16)
         self.check(self._lib.wl_profile_json(self.handle, buf, len(buf)), "profile_json")
         return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
+
+    def set_spin_sync(self, spin: bool = True):
+        """Busy-poll (True, the default) or block (False) at each host round trip."""
+        self.check(self._lib.wl_ctx_set_spin_sync(self.handle, int(spin)), "set_spin_sync")
 
     @property
     def host_syncs(self) -> int:

@@ -317,6 +317,12 @@ wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class) {
   });
 }
 
+wl_status wl_ctx_set_spin_sync(wl_ctx* ctx, int32_t spin) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  ctx->c->spin_sync = spin != 0;
+  return WL_OK;
+}
+
 wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out) {
   if (!ctx || !out) return WL_E_INVALID_ARG;
   *out = ctx->c->host_syncs;

@@ -200,43 +200,13 @@ __global__ void k_twiddles(uint2* tw, uint32_t w24) {
 }
 
 constexpr int LEAF_ROWS = 128;
-constexpr int SUBTREE_LEVELS = 7;  // levels folded per pass (2^7 digests per block)
+constexpr int TOP_LEVELS = 7;  // the last levels (<= 2^7 digests) run in one block
 constexpr int FLAT_LEVEL_MIN_LOG = 13;  // levels of at least 2^13 digests get their own launch
 
 // Tree layout: level l (2^(LL-l) digests of 8 words) starts at digest offset
 // 2^(LL+1) - 2^(LL+1-l).
 __device__ __forceinline__ size_t tree_off(int LL, int l) {
   return (size_t(1) << (LL + 1)) - (size_t(1) << (LL + 1 - l));
-}
-
-// `d` holds cnt digests of level l0 whose first global index is `first`; compresses
-// `levels` levels in shared memory and writes every new level to the tree.
-__device__ __forceinline__ void subtree_reduce(uint32_t (*d)[8], int cnt, int levels, uint32_t* __restrict__ tree,
-                                               int LL, int l0, size_t first, const kb::P16Consts& c) {
-  for (int lev = 1; lev <= levels; lev++) {
-    const int m = cnt >> lev;
-    const int t = threadIdx.x;
-    uint32_t st[16];
-    const bool act = t < m;
-    if (act) {
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        st[i] = d[2 * t][i];
-        st[8 + i] = d[2 * t + 1][i];
-      }
-      kb::p2_permute<16>(st, c);
-    }
-    __syncthreads();
-    if (act) {
-      uint32_t* o = tree + (tree_off(LL, l0 + lev) + (first >> lev) + t) * 8;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        d[t][i] = st[i];
-        o[i] = st[i];
-      }
-    }
-    __syncthreads();
-  }
 }
 
 // Adds (sign +1) or subtracts (sign -1) the 16 entries of chunk `ch` (columns 16 ch ..
@@ -328,16 +298,69 @@ __global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const
   o[1] = make_uint4(st[4], st[5], st[6], st[7]);
 }
 
-// Levels l0+1 .. l0+levels from 2^levels level-l0 digests per block.
-__global__ void k_merkle_subtree(uint32_t* __restrict__ tree, int LL, int l0, int levels,
-                                 const __grid_constant__ kb::P16Consts c) {
-  __shared__ uint32_t d[1 << SUBTREE_LEVELS][8];
-  const int cnt = 1 << levels;
-  const size_t first = size_t(blockIdx.x) * cnt;
-  const uint32_t* src = tree + (tree_off(LL, l0) + first) * 8;
-  for (int i = threadIdx.x; i < cnt * 8; i += blockDim.x) d[i / 8][i % 8] = src[i];
-  __syncthreads();
-  subtree_reduce(d, cnt, levels, tree, LL, l0, first, c);
+// Poseidon2-16 with the state spread over the 16 lanes of a half-warp (lane i holds word i),
+// for the narrow top of a Merkle tree where one thread per permutation leaves the device
+// idle and a single permutation's latency is the cost. Every lane of the warp calls it.
+// External layer: lane i's M4 row is 2 x_i + 3 x_(i+1) + x_(i+2) + x_(i+3) within its chunk
+// of 4, then the sum over the 4 chunks at the same position. Internal layer: lane 0 takes the
+// S-box, the sum is a 16-lane reduction, and each lane scales by its own diagonal entry.
+__device__ __forceinline__ uint32_t mds16_lanes(uint32_t a, int i) {
+  const int base = i & ~3;
+  const uint32_t b = __shfl_sync(0xffffffffu, a, base | ((i + 1) & 3), 16);
+  const uint32_t c = __shfl_sync(0xffffffffu, a, base | ((i + 2) & 3), 16);
+  const uint32_t d = __shfl_sync(0xffffffffu, a, base | ((i + 3) & 3), 16);
+  const uint32_t y = kb::add(kb::add(kb::add(a, b), kb::add(c, d)), kb::add(a, kb::dbl(b)));
+  uint32_t t = kb::add(y, __shfl_xor_sync(0xffffffffu, y, 4, 16));
+  t = kb::add(t, __shfl_xor_sync(0xffffffffu, t, 8, 16));
+  return kb::add(y, t);
+}
+__device__ uint32_t p2_permute16_lanes(uint32_t v, const kb::P16Consts& c) {
+  const int i = threadIdx.x & 15;
+  const uint32_t dg = kb::p2_diag<16>(i);
+  v = mds16_lanes(v, i);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube(kb::add(v, c.ext_init[r * 16 + i])), i);
+#pragma unroll 1
+  for (int r = 0; r < 20; r++) {
+    if (i == 0) v = kb::cube(kb::add(v, c.internal[r]));
+    uint32_t sum = v;
+#pragma unroll
+    for (int d = 8; d > 0; d >>= 1) sum = kb::add(sum, __shfl_xor_sync(0xffffffffu, sum, d, 16));
+    v = kb::add(kb::mul(v, dg), sum);
+  }
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube(kb::add(v, c.ext_term[r * 16 + i])), i);
+  return v;
+}
+
+// One level l of the tree, 16 lanes per compression (grid covers 16 * 2^(LL-l) threads).
+__global__ void k_merkle_level_lanes(uint32_t* __restrict__ tree, int LL, int l, const __grid_constant__ kb::P16Consts c) {
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t m = t >> 4;
+  const int i = threadIdx.x & 15;
+  const size_t cnt = size_t(1) << (LL - l);
+  const bool act = m < cnt;
+  const size_t warp_first = (t & ~size_t(31)) >> 4;
+  if (warp_first >= cnt) return;  // whole warp idle (uniform per warp)
+  uint32_t v = act ? tree[(tree_off(LL, l - 1) + 2 * m) * 8 + i] : 0u;
+  v = p2_permute16_lanes(v, c);
+  if (act && i < 8) tree[(tree_off(LL, l) + m) * 8 + i] = v;
+}
+
+// Levels l0+1 .. LL in one block of 1024 threads (at most 64 compressions per level).
+__global__ void __launch_bounds__(1024) k_merkle_top(uint32_t* __restrict__ tree, int LL, int l0,
+                                                     const __grid_constant__ kb::P16Consts c) {
+  const int g = threadIdx.x >> 4, i = threadIdx.x & 15;
+  for (int l = l0 + 1; l <= LL; l++) {
+    const int cnt = 1 << (LL - l);
+    if ((threadIdx.x >> 5) * 2 < cnt) {  // warps holding at least one live compression
+      const bool act = g < cnt;
+      uint32_t v = act ? tree[(tree_off(LL, l - 1) + 2 * size_t(g)) * 8 + i] : 0u;
+      v = p2_permute16_lanes(v, c);
+      if (act && i < 8) tree[(tree_off(LL, l) + g) * 8 + i] = v;
+    }
+    __syncthreads();
+  }
 }
 
 // Rows idx[q] of the tile-major LDE (2^T rows, n_cols columns) into out[q * n_cols + col].
@@ -444,8 +467,8 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
   k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24,
                                                                                      tree);
   WL_LAUNCH_CHECK();
-  // Wide levels one launch each (every SM busy); the narrow top of the tree in
-  // shared-memory subtrees of SUBTREE_LEVELS levels per launch.
+  // Wide levels: one launch each, one compression per thread. Narrower levels: 16 lanes per
+  // compression. The last levels (at most 128 digests) in one block.
   int l0 = 0;
   while (l0 < LL && LL - l0 - 1 >= FLAT_LEVEL_MIN_LOG) {
     const size_t cnt = size_t(1) << (LL - l0 - 1);
@@ -453,10 +476,14 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
     WL_LAUNCH_CHECK();
     l0++;
   }
-  for (; l0 < LL; l0 += SUBTREE_LEVELS) {
-    const int lv = (LL - l0) < SUBTREE_LEVELS ? (LL - l0) : SUBTREE_LEVELS;
-    const unsigned blocks = 1u << (LL - l0 - lv);
-    k_merkle_subtree<<<blocks, 1 << (lv - 1), 0, s>>>(tree, LL, l0, lv, p16);
+  while (l0 < LL && LL - l0 > TOP_LEVELS) {
+    const size_t threads = size_t(16) << (LL - l0 - 1);
+    k_merkle_level_lanes<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(tree, LL, l0 + 1, p16);
+    WL_LAUNCH_CHECK();
+    l0++;
+  }
+  if (l0 < LL) {
+    k_merkle_top<<<1, 1024, 0, s>>>(tree, LL, l0, p16);
     WL_LAUNCH_CHECK();
   }
 }

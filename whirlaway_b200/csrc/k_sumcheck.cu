@@ -20,28 +20,31 @@ __device__ __forceinline__ size_t down_row(size_t i, size_t N) { return i == N -
 
 // ------------------------------------------------------------------ eq tables
 // out[x] = prod_i (x_i ? r_i : 1 - r_i), x_1 = most significant bit of x.
+// eq(pt, x) for x < 2^nvars, x's leading bit pairing with pt[0]. The point and its
+// complements are staged in shared memory; block b holds the 2^nlo entries with high part b.
+constexpr int EQ_MAX_VARS = 32;
 __global__ void k_eq_table(const ef* __restrict__ pt, int nvars, ef* __restrict__ out) {
+  __shared__ ef r1[EQ_MAX_VARS], r0[EQ_MAX_VARS];
   __shared__ ef hi_val;
   const int nlo = nvars < 10 ? nvars : 10;
   const int nhi = nvars - nlo;
+  for (int i = threadIdx.x; i < nvars; i += blockDim.x) {
+    const ef r = pt[i];
+    r1[i] = r;
+    r0[i] = ef_sub(ef_one(), r);
+  }
+  __syncthreads();
   const size_t xhi = blockIdx.x;
   if (threadIdx.x == 0) {
     ef h = ef_one();
-    for (int i = 0; i < nhi; i++) {
-      bool bit = (xhi >> (nhi - 1 - i)) & 1;
-      h = ef_mul(h, bit ? pt[i] : ef_sub(ef_one(), pt[i]));
-    }
+    for (int i = 0; i < nhi; i++) h = ef_mul(h, ((xhi >> (nhi - 1 - i)) & 1) ? r1[i] : r0[i]);
     hi_val = h;
   }
   __syncthreads();
   const uint32_t xlo = threadIdx.x;
   if (xlo >= (1u << nlo)) return;
   ef v = hi_val;
-  for (int i = 0; i < nlo; i++) {
-    bool bit = (xlo >> (nlo - 1 - i)) & 1;
-    const ef& r = pt[nhi + i];
-    v = ef_mul(v, bit ? r : ef_sub(ef_one(), r));
-  }
+  for (int i = 0; i < nlo; i++) v = ef_mul(v, ((xlo >> (nlo - 1 - i)) & 1) ? r1[nhi + i] : r0[nhi + i]);
   out[(xhi << nlo) + xlo] = v;
 }
 
@@ -507,40 +510,48 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
 }
 
 // out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]
+// out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]; one warp per column.
 __global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int nh, int ncols,
                               ef* __restrict__ out) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (c >= ncols) return;
   ef acc = ef_zero();
-  for (int j = 0; j < nsk; j++) {
-    ef s = ef_zero();
-    for (int h = 0; h < nh; h++) s = ef_add(s, partial[(size_t(c) * nsk + j) * nh + h]);
-    acc = ef_add(acc, ef_mul(sel[j], s));
-  }
-  out[c] = acc;
+  for (int idx = lane; idx < nsk * nh; idx += 32)
+    acc = ef_add(acc, ef_mul(sel[idx / nh], partial[size_t(c) * nsk * nh + idx]));
+  acc = warp_reduce_ef(acc);
+  if (lane == 0) out[c] = acc;
 }
 
 // ------------------------------------------------------------------ inner phase
+// out[row] = sum_c eqc[c] * wit[c][row]; two adjacent rows per thread (8-byte loads).
 __global__ void k_batch_cols(const uint32_t* __restrict__ wit, int log_n, const ef* __restrict__ eqc_g,
                              ef* __restrict__ out) {
   __shared__ ef eqc[AIR_W + 3];
   for (int i = threadIdx.x; i < AIR_W + 3; i += blockDim.x) eqc[i] = i < AIR_W ? eqc_g[i] : ef_zero();
   __syncthreads();
   const size_t N = size_t(1) << log_n;
-  const size_t row = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t row = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
   if (row >= N) return;
-  EfMacF m;
-  m.init();
+  EfMacF m0, m1;
+  m0.init();
+  m1.init();
 #pragma unroll 2
   for (int c = 0; c < AIR_W; c += 4) {
-    uint32_t v[4];
+    uint2 v[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) v[q] = c + q < AIR_W ? wit[size_t(c + q) * N + row] : 0u;
+    for (int q = 0; q < 4; q++)
+      v[q] = c + q < AIR_W ? __ldg(reinterpret_cast<const uint2*>(wit + size_t(c + q) * N + row)) : make_uint2(0, 0);
 #pragma unroll
-    for (int q = 0; q < 4; q++) m.mac(eqc[c + q], v[q]);
-    m.flush();
+    for (int q = 0; q < 4; q++) {
+      m0.mac(eqc[c + q], v[q].x);
+      m1.mac(eqc[c + q], v[q].y);
+    }
+    m0.flush();
+    m1.flush();
   }
-  out[row] = m.acc;
+  out[row] = m0.acc;
+  out[row + 1] = m1.acc;
 }
 
 constexpr int SUB_THREADS = 256, SUB_PER_THREAD = 16;
@@ -586,13 +597,17 @@ __global__ void k_inner_mle(const ef* __restrict__ e, int log_n, const ef* __res
   out[y] = ef_add(mu, ef_mul(*alpha2, md));
 }
 
-constexpr int PROD_THREADS = 256, PROD_PER_THREAD = 8;
+constexpr int PROD_THREADS = 256;
+// points per thread: 8 for large tables, fewer for small ones so that latency, not a
+// serial loop, bounds the small rounds
+int prod_per_thread(size_t half) { return half >= (size_t(1) << 19) ? 8 : half >= (size_t(1) << 16) ? 2 : 1; }
 
-__global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, size_t half, ef* __restrict__ partial) {
+__global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, size_t half, int per,
+                            ef* __restrict__ partial) {
   __shared__ ef scratch[32];
   ef s0 = ef_zero(), s2 = ef_zero();
-  for (int q = 0; q < PROD_PER_THREAD; q++) {
-    size_t x = (size_t(blockIdx.x) * PROD_PER_THREAD + q) * PROD_THREADS + threadIdx.x;
+  for (int q = 0; q < per; q++) {
+    size_t x = (size_t(blockIdx.x) * per + q) * PROD_THREADS + threadIdx.x;
     if (x < half) {
       ef al = a[x], ah = a[x + half], bl = b[x], bh = b[x + half];
       s0 = ef_add(s0, ef_mul(al, bl));
@@ -689,6 +704,7 @@ __global__ void k_abc_eval_ef(const ef* __restrict__ cols, int m, const ef* __re
 
 // ------------------------------------------------------------------ launchers
 void launch_eq_table(const ef* point, int nvars, ef* out, cudaStream_t s) {
+  if (nvars > EQ_MAX_VARS) throw std::invalid_argument("eq table: too many variables");
   int nlo = nvars < 10 ? nvars : 10;
   k_eq_table<<<(unsigned)(size_t(1) << (nvars - nlo)), 1u << nlo, 0, s>>>(point, nvars, out);
   WL_LAUNCH_CHECK();
@@ -759,14 +775,15 @@ void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* 
   k_inner_sums<<<dim3(AIR_W, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi,
                                                                                          eq_lo, pu, pd);
   WL_LAUNCH_CHECK();
-  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pu, sel, nsk, nh, AIR_W, out_up);
+  k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pu, sel, nsk, nh, AIR_W, out_up);
   WL_LAUNCH_CHECK();
-  k_combine_sel<<<(AIR_W + 127) / 128, 128, 0, s>>>(pd, sel, nsk, nh, AIR_W, out_down);
+  k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pd, sel, nsk, nh, AIR_W, out_down);
   WL_LAUNCH_CHECK();
 }
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s) {
+  if (log_n < 1) throw std::invalid_argument("batch_cols: at least 2 rows");
   size_t N = size_t(1) << log_n;
-  k_batch_cols<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(wit, log_n, eqc, out);
+  k_batch_cols<<<(unsigned)((N / 2 + 255) / 256), 256, 0, s>>>(wit, log_n, eqc, out);
   WL_LAUNCH_CHECK();
 }
 int sub_eval_blocks(int log_n, int k) {
@@ -786,11 +803,11 @@ void launch_inner_mle(const ef* e, int log_n, const ef* alpha2, ef* out, cudaStr
   WL_LAUNCH_CHECK();
 }
 int prod_blocks(size_t half) {
-  size_t per = size_t(PROD_THREADS) * PROD_PER_THREAD;
+  size_t per = size_t(PROD_THREADS) * prod_per_thread(half);
   return (int)((half + per - 1) / per);
 }
 void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s) {
-  k_prod_eval<<<prod_blocks(half), PROD_THREADS, 0, s>>>(a, b, half, partial);
+  k_prod_eval<<<prod_blocks(half), PROD_THREADS, 0, s>>>(a, b, half, prod_per_thread(half), partial);
   WL_LAUNCH_CHECK();
 }
 void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s) {

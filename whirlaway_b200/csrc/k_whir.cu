@@ -147,14 +147,16 @@ __global__ void k_add_eq_terms_ef(ef* __restrict__ w, int lh, int ll, int npts, 
   w[v] = acc;
 }
 
-constexpr int WSC_THREADS = 256, WSC_PER_THREAD = 8;
+constexpr int WSC_THREADS = 256;
+// points per thread: 8 for large tables, fewer for small ones (latency-bound rounds)
+int wsc_per_thread(size_t half) { return half >= (size_t(1) << 19) ? 8 : half >= (size_t(1) << 16) ? 2 : 1; }
 
-__global__ void k_whir_sc_eval(const ef* __restrict__ g, const ef* __restrict__ w, size_t half,
+__global__ void k_whir_sc_eval(const ef* __restrict__ g, const ef* __restrict__ w, size_t half, int per,
                                ef* __restrict__ partial) {
   __shared__ ef scratch[32];
   ef s0 = ef_zero(), s1 = ef_zero(), s2 = ef_zero();
-  for (int q = 0; q < WSC_PER_THREAD; q++) {
-    size_t x = (size_t(blockIdx.x) * WSC_PER_THREAD + q) * WSC_THREADS + threadIdx.x;
+  for (int q = 0; q < per; q++) {
+    size_t x = (size_t(blockIdx.x) * per + q) * WSC_THREADS + threadIdx.x;
     if (x < half) {
       ef gl = g[x], gh = g[x + half], wl_ = w[x], wh = w[x + half];
       s0 = ef_add(s0, ef_mul(gl, wl_));
@@ -223,11 +225,11 @@ void launch_add_eq_terms_ef(ef* w, int lh, int ll, int npts, const ef* hi, const
   WL_LAUNCH_CHECK();
 }
 int whir_sc_blocks(size_t half) {
-  size_t per = size_t(WSC_THREADS) * WSC_PER_THREAD;
+  size_t per = size_t(WSC_THREADS) * wsc_per_thread(half);
   return (int)((half + per - 1) / per);
 }
 void launch_whir_sc_eval(const ef* g, const ef* w, size_t half, ef* partial, cudaStream_t s) {
-  k_whir_sc_eval<<<whir_sc_blocks(half), WSC_THREADS, 0, s>>>(g, w, half, partial);
+  k_whir_sc_eval<<<whir_sc_blocks(half), WSC_THREADS, 0, s>>>(g, w, half, wsc_per_thread(half), partial);
   WL_LAUNCH_CHECK();
 }
 int mle_ef_blocks(int lh) { return 1 << lh; }

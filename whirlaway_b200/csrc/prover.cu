@@ -66,6 +66,7 @@ Context::~Context() {
   cudaStreamSynchronize(stream);
   for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : event_pool) cudaEventDestroy(e);
+  if (sync_event) cudaEventDestroy(sync_event);
   cudaFree(twiddles);
   cudaFreeHost(pinned);
   cudaStreamDestroy(stream);
@@ -112,7 +113,16 @@ ProfScope::~ProfScope() {
 }
 
 void Context::wait_stream() {
-  WL_CUDA(cudaStreamSynchronize(stream));
+  if (spin_sync) {
+    if (!sync_event) WL_CUDA(cudaEventCreateWithFlags(&sync_event, cudaEventDisableTiming));
+    WL_CUDA(cudaEventRecord(sync_event, stream));
+    cudaError_t e;
+    while ((e = cudaEventQuery(sync_event)) == cudaErrorNotReady) {
+    }
+    WL_CUDA(e);
+  } else {
+    WL_CUDA(cudaStreamSynchronize(stream));
+  }
   host_syncs++;
 }
 void Context::to_host(void* dst, const void* src, size_t bytes) {

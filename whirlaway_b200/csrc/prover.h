@@ -48,6 +48,12 @@ struct Context {
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
   void wait_stream();  // host synchronisation with `stream` (counted in host_syncs)
+  // How wait_stream waits: true (default) = the host thread polls an event without sleeping,
+  // so the OS never has to wake it at the end of a round (blocking waits measured up to
+  // ~20 ms of wake-up stalls per proof); false = blocking cudaStreamSynchronize (server
+  // workers, which would otherwise occupy one CPU each).
+  bool spin_sync = true;
+  cudaEvent_t sync_event = nullptr;
   void to_device(void* dst, const void* src, size_t bytes);
 
   // Optional per-kernel-class timing with CUDA events on `stream`.

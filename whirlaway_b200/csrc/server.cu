@@ -27,7 +27,10 @@ uint64_t proof_footprint_bytes(int log_n) {
 
 Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), budget_(hbm_budget) {
   if (workers < 1) throw std::invalid_argument("a server needs at least one worker");
-  for (int i = 0; i < workers; i++) contexts_.push_back(std::make_unique<Context>(device, hbm_budget));
+  for (int i = 0; i < workers; i++) {
+    contexts_.push_back(std::make_unique<Context>(device, hbm_budget));
+    contexts_.back()->spin_sync = false;  // workers block: the other workers' proofs fill the device
+  }
   for (int i = 0; i < workers; i++) threads_.emplace_back([this, i] { worker_main(i); });
 }
 
