@@ -74,7 +74,8 @@ __global__ void k_reduce_partials(const ef* __restrict__ partial, int nblk, int 
 
 // ------------------------------------------------------------------ AIR zerocheck
 constexpr int ZC0_X = 32, ZC0_Z = 15;
-constexpr int ZC0_STAGES = 4;   // columns in flight
+constexpr int ZC0_STAGES = 4;   // column groups in flight
+constexpr int ZC0_GROUP = 4;    // columns per staged group (one block barrier per group)
 constexpr int ZC0_PAD = 20;     // words per x in a staged column tile (16 values + padding)
 
 __device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
@@ -88,8 +89,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Thread (x, z): the up columns are extended from their values at j * 2^(n-k) + x, j < 2^k,
 // to the point z by the Lagrange weights L_j(z); the batched constraint over those values is
 // weighted by eq[x]. A warp holds 32 consecutive x for one z. The 2^k x 32 values of each
-// column are staged in shared memory by a cp.async pipeline (the constraint reads columns
-// 1..164 in increasing order, each exactly once), so the extension reads shared memory only.
+// column are staged in shared memory by a cp.async pipeline, ZC0_GROUP columns per stage (the
+// constraint reads columns 1..164 in increasing order, each exactly once, so one block
+// barrier per group suffices), and the extension reads shared memory only.
 __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* __restrict__ wit, int log_n, int k,
                                                                int nz, const uint32_t* __restrict__ lw,
                                                                const ef* __restrict__ eq,
@@ -97,7 +99,7 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
                                                                const __grid_constant__ AirConsts K,
                                                                ef* __restrict__ partial) {
   __shared__ ef alphas[AIR_NC];
-  __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_X * ZC0_PAD];
+  __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_GROUP][ZC0_X * ZC0_PAD];
   const int tid = threadIdx.y * ZC0_X + threadIdx.x;
   constexpr int NT = ZC0_X * ZC0_Z;
   for (int i = tid; i < AIR_NC; i += NT) alphas[i] = alphas_g[i];
@@ -111,10 +113,13 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
 #pragma unroll
   for (int j = 0; j < 16; j++) w[j] = (zi < nz && j < nsk) ? lw[zi * nsk + j] : 0u;
 
-  // producer: column c's tile -> slot, tile[slot][xl * PAD + j] = up_c[j * S + x0 + xl]
-  auto issue = [&](int c) {
-    if (c < AIR_W) {
-      uint32_t* dst = tile[c % ZC0_STAGES];
+  // producer: group g (columns 1 + G g ..) -> its slot, tile[slot][cc][xl * PAD + j] =
+  // up_c[j * S + x0 + xl] for c = 1 + G g + cc
+  auto issue = [&](int g) {
+    for (int cc = 0; cc < ZC0_GROUP; cc++) {
+      const int c = 1 + ZC0_GROUP * g + cc;
+      if (c >= AIR_W) break;
+      uint32_t* dst = tile[g % ZC0_STAGES][cc];
       const uint32_t* col = wit + size_t(c) * N;
       for (int idx = tid; idx < 16 * ZC0_X; idx += NT) {
         const int j = idx / ZC0_X, xl = idx % ZC0_X;
@@ -127,13 +132,16 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
     }
     cp_async_commit();
   };
-  for (int c = 1; c < 1 + ZC0_STAGES - 1; c++) issue(c);
-  int next = ZC0_STAGES;  // next column to prefetch
+  for (int g = 0; g < ZC0_STAGES - 1; g++) issue(g);
+  int next = ZC0_STAGES - 1;  // next group to prefetch
   auto get = [&](int c) -> uint32_t {
-    cp_async_wait<ZC0_STAGES - 2>();
-    __syncthreads();
-    issue(next++);
-    const uint4* row = reinterpret_cast<const uint4*>(tile[c % ZC0_STAGES] + threadIdx.x * ZC0_PAD);
+    const int g = (c - 1) / ZC0_GROUP, cc = (c - 1) % ZC0_GROUP;
+    if (cc == 0) {
+      cp_async_wait<ZC0_STAGES - 2>();
+      __syncthreads();
+      issue(next++);
+    }
+    const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
     uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
