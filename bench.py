@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--batch-size", type=int, default=64)
-    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests per arrival rate (the full serving configuration uses 2000)")
     return ap.parse_args()

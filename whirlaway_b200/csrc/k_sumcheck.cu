@@ -20,32 +20,49 @@ __device__ __forceinline__ size_t down_row(size_t i, size_t N) { return i == N -
 
 // ------------------------------------------------------------------ eq tables
 // out[x] = prod_i (x_i ? r_i : 1 - r_i), x_1 = most significant bit of x.
-// eq(pt, x) for x < 2^nvars, x's leading bit pairing with pt[0]. The point and its
-// complements are staged in shared memory; block b holds the 2^nlo entries with high part b.
+// eq(pt, x) for x < 2^nvars, x's leading bit pairing with pt[0]. A block writes 2^EQ_BLK_BITS
+// consecutive entries: x = (block << nbits) + (a << nb) + b, eq = H * A[a] * B[b], where A and
+// B are tables over the block's two groups of low variables (<= 16 entries each, built in
+// shared memory) and H is the product over the block's high variables (a product tree).
 constexpr int EQ_MAX_VARS = 32;
-__global__ void k_eq_table(const ef* __restrict__ pt, int nvars, ef* __restrict__ out) {
-  __shared__ ef r1[EQ_MAX_VARS], r0[EQ_MAX_VARS];
-  __shared__ ef hi_val;
-  const int nlo = nvars < 10 ? nvars : 10;
-  const int nhi = nvars - nlo;
-  for (int i = threadIdx.x; i < nvars; i += blockDim.x) {
+constexpr int EQ_BLK_BITS = 8;
+constexpr int EQ_THREADS = 1 << EQ_BLK_BITS;
+__global__ void __launch_bounds__(EQ_THREADS) k_eq_table(const ef* __restrict__ pt, int nvars, ef* __restrict__ out) {
+  __shared__ ef r1[EQ_MAX_VARS], r0[EQ_MAX_VARS], fac[EQ_MAX_VARS], A[16], B[16];
+  const int nbits = nvars < EQ_BLK_BITS ? nvars : EQ_BLK_BITS;
+  const int nhi = nvars - nbits, na = nbits / 2, nb = nbits - na;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < nvars; i += blockDim.x) {
     const ef r = pt[i];
     r1[i] = r;
     r0[i] = ef_sub(ef_one(), r);
   }
   __syncthreads();
   const size_t xhi = blockIdx.x;
-  if (threadIdx.x == 0) {
-    ef h = ef_one();
-    for (int i = 0; i < nhi; i++) h = ef_mul(h, ((xhi >> (nhi - 1 - i)) & 1) ? r1[i] : r0[i]);
-    hi_val = h;
+  if (tid < nhi) fac[tid] = ((xhi >> (nhi - 1 - tid)) & 1) ? r1[tid] : r0[tid];
+  if (tid >= 64 && tid - 64 < (1 << na)) {
+    const int a = tid - 64;
+    ef v = ef_one();
+    for (int i = 0; i < na; i++) v = ef_mul(v, ((a >> (na - 1 - i)) & 1) ? r1[nhi + i] : r0[nhi + i]);
+    A[a] = v;
+  }
+  if (tid >= 96 && tid - 96 < (1 << nb)) {
+    const int b = tid - 96;
+    ef v = ef_one();
+    for (int i = 0; i < nb; i++) v = ef_mul(v, ((b >> (nb - 1 - i)) & 1) ? r1[nhi + na + i] : r0[nhi + na + i]);
+    B[b] = v;
   }
   __syncthreads();
-  const uint32_t xlo = threadIdx.x;
-  if (xlo >= (1u << nlo)) return;
-  ef v = hi_val;
-  for (int i = 0; i < nlo; i++) v = ef_mul(v, ((xlo >> (nlo - 1 - i)) & 1) ? r1[nhi + i] : r0[nhi + i]);
-  out[(xhi << nlo) + xlo] = v;
+  for (int len = nhi; len > 1;) {
+    const int m = (len + 1) >> 1;
+    if (tid < len - m) fac[tid] = ef_mul(fac[tid], fac[tid + m]);
+    __syncthreads();
+    len = m;
+  }
+  if (tid < (1 << nbits)) {
+    const ef h = nhi ? fac[0] : ef_one();
+    out[(xhi << nbits) + tid] = ef_mul(ef_mul(h, A[tid >> nb]), B[tid & ((1 << nb) - 1)]);
+  }
 }
 
 __global__ void k_eq_table_f(const uint32_t* __restrict__ pts, int npts, int nvars, uint32_t* __restrict__ out) {
@@ -713,8 +730,8 @@ __global__ void k_abc_eval_ef(const ef* __restrict__ cols, int m, const ef* __re
 // ------------------------------------------------------------------ launchers
 void launch_eq_table(const ef* point, int nvars, ef* out, cudaStream_t s) {
   if (nvars > EQ_MAX_VARS) throw std::invalid_argument("eq table: too many variables");
-  int nlo = nvars < 10 ? nvars : 10;
-  k_eq_table<<<(unsigned)(size_t(1) << (nvars - nlo)), 1u << nlo, 0, s>>>(point, nvars, out);
+  const int nbits = nvars < EQ_BLK_BITS ? nvars : EQ_BLK_BITS;
+  k_eq_table<<<(unsigned)(size_t(1) << (nvars - nbits)), EQ_THREADS, 0, s>>>(point, nvars, out);
   WL_LAUNCH_CHECK();
 }
 void launch_eq_table_f(const uint32_t* pts, int npts, int nvars, uint32_t* out, cudaStream_t s) {
