@@ -66,15 +66,22 @@ __device__ __forceinline__ ef block_reduce_ef(ef v, ef* scratch) {
   return v;
 }
 
-// Lazy extension-field multiply-accumulate by base-field scalars: at most four products
-// per coordinate are summed in 64 bits before a Montgomery reduction.
+// Lazy extension-field multiply-accumulate by base-field scalars. Each coordinate is a 64-bit
+// running sum; flush() folds it with 2^32 = 2^25 - 2 (mod p) into hi * (2^25 - 2) + lo, one
+// wide multiply-add, leaving it below 2^57 + 2^32, so that at most four more products (each
+// below p^2, 4 p^2 = 2^64 - 2^58 + ...) keep it below 2^64. value() folds once more and
+// makes the single Montgomery reduction (its input is below 4 p^2).
 struct EfMacF {
+  static constexpr uint32_t C32 = (1u << 25) - 2;  // 2^32 mod p
   uint64_t s[8];
-  ef acc;
   __device__ __forceinline__ void init() {
 #pragma unroll
     for (int i = 0; i < 8; i++) s[i] = 0;
-    acc = kb::ef_zero();
+  }
+  // starts from v (Montgomery form): v * 2^32 reduces to v, and is stored folded
+  __device__ __forceinline__ void init_with(const ef& v) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) s[i] = uint64_t(v.c[i]) * C32;
   }
   __device__ __forceinline__ void mac(const ef& a, uint32_t f) {
 #pragma unroll
@@ -82,10 +89,14 @@ struct EfMacF {
   }
   __device__ __forceinline__ void flush() {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      acc.c[i] = kb::add(acc.c[i], kb::redc(s[i]));
-      s[i] = 0;
-    }
+    for (int i = 0; i < 8; i++) s[i] = uint64_t(uint32_t(s[i] >> 32)) * C32 + uint32_t(s[i]);
+  }
+  __device__ __forceinline__ ef value() {
+    flush();
+    ef r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.c[i] = kb::redc(s[i]);
+    return r;
   }
 };
 #endif

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
       K, get, [&](uint32_t h, int i) { m.mac(alphas[i], h); }, [&]() { m.flush(); });
   cp_async_wait<0>();
   const bool active = zi < nz && x < S;
-  ef res = active ? ef_mul(m.acc, eq[x]) : ef_zero();
+  ef res = active ? ef_mul(m.value(), eq[x]) : ef_zero();
   res = warp_reduce_ef(res);
   if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
 }
@@ -207,7 +207,7 @@ __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, c
     m.mac(sel[j], v[j]);
     if ((j & 3) == 3) m.flush();
   }
-  out[size_t(c) * S + x] = m.acc;
+  out[size_t(c) * S + x] = m.value();
 }
 
 // ------------------------------------------------------------------ zerocheck rounds >= 1
@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
     mu.flush();
     md.flush();
   }
-  const ef su = warp_reduce_ef(mu.acc), sd = warp_reduce_ef(md.acc);
+  const ef su = warp_reduce_ef(mu.value()), sd = warp_reduce_ef(md.value());
   if (lane == 0) {
     const size_t o = (size_t(c) * gridDim.y + j) * nhi + xh;
     pu[o] = ef_mul(su, eq_hi[xh]);
@@ -575,8 +575,8 @@ __global__ void k_batch_cols(const uint32_t* __restrict__ wit, int log_n, const 
     m0.flush();
     m1.flush();
   }
-  out[row] = m0.acc;
-  out[row + 1] = m1.acc;
+  out[row] = m0.value();
+  out[row + 1] = m1.value();
 }
 
 constexpr int SUB_THREADS = 256, SUB_PER_THREAD = 16;
@@ -706,7 +706,7 @@ __global__ void k_abc0_fold(const uint32_t* __restrict__ a, const uint32_t* __re
     m.mac(sel[j], src[size_t(j) * S + x]);
     if ((j & 3) == 3 || j == nsk - 1) m.flush();
   }
-  out[size_t(blockIdx.y) * S + x] = m.acc;
+  out[size_t(blockIdx.y) * S + x] = m.value();
 }
 
 __global__ void k_abc_eval_ef(const ef* __restrict__ cols, int m, const ef* __restrict__ eq, ef* __restrict__ partial) {

@@ -68,7 +68,7 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
 #pragma unroll
       for (int j = 0; j < J; j++) {
         m[j].flush();
-        res[j] = ef_add(res[j], ef_mul(m[j].acc, lo[size_t(j) * nlo + vlo]));
+        res[j] = ef_add(res[j], ef_mul(m[j].value(), lo[size_t(j) * nlo + vlo]));
       }
     }
   }
@@ -109,7 +109,7 @@ __global__ void k_whir_fold_T(const uint32_t* __restrict__ T, size_t t_len, int 
     for (int q = 0; q < 4; q++) m.mac(u0 + q < nu ? eqr[u0 + q] : ef_zero(), t[q]);
     m.flush();
   }
-  out[v] = m.acc;
+  out[v] = m.value();
 }
 
 // w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (base-field points)
@@ -123,8 +123,7 @@ __global__ void k_add_eq_terms_f(ef* __restrict__ w, int lh, int ll, int npts, c
   const size_t vh = v >> ll, vl = v & ((size_t(1) << ll) - 1);
   const size_t nhi = size_t(1) << lh, nlo = size_t(1) << ll;
   EfMacF m;
-  m.init();
-  m.acc = w[v];
+  m.init_with(w[v]);
   int cnt = 0;
   for (int t = 0; t < npts; t++) {
     uint32_t e = mul(hi[t * nhi + vh], lo[t * nlo + vl]);
@@ -132,7 +131,7 @@ __global__ void k_add_eq_terms_f(ef* __restrict__ w, int lh, int ll, int npts, c
     if (++cnt == 4) { m.flush(); cnt = 0; }
   }
   m.flush();
-  w[v] = m.acc;
+  w[v] = m.value();
 }
 
 // w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (extension-field points)
