@@ -47,45 +47,22 @@ __device__ __forceinline__ void bfly(uint32_t& u, uint32_t& v, uint2 w) {
 // Where a round reads its points from and writes them to.
 enum NttIo { IO_SRC = 0, IO_GLOBAL = 1, IO_SMEM = 2 };
 
+// Per-lane addressing of a pass: point j of this lane's line lives at base[j << step] for
+// each of the three places a round reads or writes.
 struct NttLane {
-  const uint32_t* src;  // commitment source (IO_SRC)
-  size_t src_len;
-  size_t col_block;     // elem << L
-  int le;               // log2(elem)
-  uint32_t gcol;        // global column of this lane
-  bool col_ok;          // gcol < n_cols
-  uint32_t* data;       // LDE matrix
-  size_t row0;          // tile * 2^T + lo + (hi << (Bs + Bp)): row of j = 0 plus the tile base
-  int Bs, Bp;
-  size_t hi;            // source entry of j = 0 is hi << Bp
-  uint32_t* X;          // shared exchange buffer [2^Bp][32]
-  int lane;
+  const uint32_t* src;      // commitment source at j = 0 (nullptr: column beyond n_cols)
+  const uint32_t* src_end;  // one past the source (entries beyond it read as zero)
+  int src_step;             // log2(elem)
+  uint32_t* data;           // LDE word of row j = 0, this lane's column
+  int data_step;            // Bs + 3 (rows are 8 words apart within a tile)
+  uint32_t* X;              // exchange buffer [2^Bp][32], this lane's column
+  int Bp;
 };
-
-template <int IO>
-__device__ __forceinline__ uint32_t ntt_load(const NttLane& ln, uint32_t j) {
-  if constexpr (IO == IO_SRC) {
-    const size_t s = size_t(j) + (ln.hi << ln.Bp);
-    const size_t addr = size_t(ln.gcol >> ln.le) * ln.col_block + (ln.gcol & ((1u << ln.le) - 1)) + (s << ln.le);
-    return (ln.col_ok && addr < ln.src_len) ? __ldg(ln.src + addr) : 0u;
-  } else if constexpr (IO == IO_GLOBAL) {
-    return ln.data[((ln.row0 + (size_t(j) << ln.Bs)) << 3) + (ln.gcol & 7)];
-  } else {
-    return ln.X[(j << 5) + ln.lane];
-  }
-}
-template <int IO>
-__device__ __forceinline__ void ntt_store(const NttLane& ln, uint32_t j, uint32_t v) {
-  if constexpr (IO == IO_GLOBAL) {
-    ln.data[((ln.row0 + (size_t(j) << ln.Bs)) << 3) + (ln.gcol & 7)] = v;
-  } else {
-    ln.X[(j << 5) + ln.lane] = v;
-  }
-}
 
 // One register round: stages b0..b0+RB-1 (local numbering) on the groups of 2^RB points
 // j = base + (k << b0) handled by this warp. `tws` is this lane's twiddle table: entry
-// 2^tl - 1 + r is the factor of local stage tl for j mod 2^tl = r.
+// 2^tl - 1 + r is the factor of local stage tl for j mod 2^tl = r. Addresses are formed
+// once per group (a base pointer and a stride); the source range is checked once per group.
 template <int RB, int IN, int OUT>
 __device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, int b0, int warp, bool active) {
   constexpr int R = 1 << RB;
@@ -94,8 +71,26 @@ __device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, i
     const uint32_t base = (g & ((1u << b0) - 1)) | ((g >> b0) << (b0 + RB));
     if (!active) continue;
     uint32_t x[R];
+    if constexpr (IN == IO_SRC) {
+      const uint32_t* p0 = ln.src + (size_t(base) << ln.src_step);
+      const size_t stride = size_t(1) << (b0 + ln.src_step);
+      if (ln.src && p0 + (R - 1) * stride < ln.src_end) {
 #pragma unroll
-    for (int k = 0; k < R; k++) x[k] = ntt_load<IN>(ln, base + (uint32_t(k) << b0));
+        for (int k = 0; k < R; k++) x[k] = __ldg(p0 + k * stride);
+      } else {
+#pragma unroll
+        for (int k = 0; k < R; k++) x[k] = (ln.src && p0 + k * stride < ln.src_end) ? __ldg(p0 + k * stride) : 0u;
+      }
+    } else if constexpr (IN == IO_GLOBAL) {
+      const uint32_t* p0 = ln.data + (size_t(base) << ln.data_step);
+      const size_t stride = size_t(1) << (b0 + ln.data_step);
+#pragma unroll
+      for (int k = 0; k < R; k++) x[k] = p0[k * stride];
+    } else {
+      const uint32_t* p0 = ln.X + (base << 5);
+#pragma unroll
+      for (int k = 0; k < R; k++) x[k] = p0[(uint32_t(k) << b0) << 5];
+    }
     const uint32_t blo = base & ((1u << b0) - 1);
 #pragma unroll
     for (int st = 0; st < RB; st++) {
@@ -110,8 +105,16 @@ __device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, i
         bfly(x[k], x[k + (1 << st)], w[k & ((1 << st) - 1)]);
       }
     }
+    if constexpr (OUT == IO_GLOBAL) {
+      uint32_t* p0 = ln.data + (size_t(base) << ln.data_step);
+      const size_t stride = size_t(1) << (b0 + ln.data_step);
 #pragma unroll
-    for (int k = 0; k < R; k++) ntt_store<OUT>(ln, base + (uint32_t(k) << b0), x[k]);
+      for (int k = 0; k < R; k++) p0[k * stride] = x[k];
+    } else {
+      uint32_t* p0 = ln.X + (base << 5);
+#pragma unroll
+      for (int k = 0; k < R; k++) p0[(uint32_t(k) << b0) << 5] = x[k];
+    }
   }
 }
 
@@ -152,19 +155,20 @@ __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint3
   const int c = lane & 7, l = (lane >> 3) & (LR - 1), h2 = lane >> (3 + lr_log);
   const bool active = h2 < (1 << hg_log);
   NttLane ln;
-  ln.src = in.src;
-  ln.src_len = in.src_len;
-  ln.le = in.elem == 8 ? 3 : 0;
-  ln.col_block = size_t(in.elem) << in.L;
-  ln.gcol = blockIdx.y * 8 + c;
-  ln.col_ok = ln.gcol < (uint32_t)in.n_cols;
-  ln.data = data;
-  ln.Bs = Bs;
+  const int le = in.elem == 8 ? 3 : 0;
+  const uint32_t gcol = blockIdx.y * 8 + c;
+  const size_t hi = (hg << hg_log) + h2;
+  const size_t row0 = (size_t(blockIdx.y) << T) + (lg << lr_log) + l + (hi << (Bs + Bp));
+  ln.src = nullptr;
+  ln.src_end = in.src + in.src_len;
+  if (FROM_SRC && gcol < (uint32_t)in.n_cols)
+    ln.src = in.src + size_t(gcol >> le) * (size_t(in.elem) << in.L) + (gcol & ((1u << le) - 1)) +
+             ((hi << Bp) << le);
+  ln.src_step = le;
+  ln.data = data + (row0 << 3) + c;
+  ln.data_step = Bs + 3;
+  ln.X = sm + lane;
   ln.Bp = Bp;
-  ln.hi = (hg << hg_log) + h2;
-  ln.row0 = (size_t(blockIdx.y) << T) + (lg << lr_log) + l + (ln.hi << (Bs + Bp));
-  ln.X = sm;
-  ln.lane = lane;
   const uint2* tws = TW + l * ntw;
   const int rb2 = Bp - rb1;
   if (rb2 == 0) {
