@@ -470,8 +470,10 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
   zcd_block_store<ZCD_PARTIAL_PTS>(res, partial, blockIdx.x, zi);
 }
 
+// Folds every column at the challenge (*r, or rv when r is null) and, in the extra column
+// slot, sums the next round's eq table out of the current one.
 __global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, size_t half, int ncols,
-                            const ef* __restrict__ r, const ef* __restrict__ eq_in, ef* __restrict__ eq_out,
+                            const ef* __restrict__ r, ef rv, const ef* __restrict__ eq_in, ef* __restrict__ eq_out,
                             size_t eq_half) {
   const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
@@ -481,7 +483,7 @@ __global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, siz
   }
   if (x >= half) return;
   const ef* src = in + size_t(c) * 2 * half;
-  out[size_t(c) * half + x] = ef_lerp(src[x], src[half + x], *r);
+  out[size_t(c) * half + x] = ef_lerp(src[x], src[half + x], r ? *r : rv);
 }
 
 // Per (column c, j < 2^k, x_hi): eq_hi[x_hi] * sum_{x_lo} eq_lo[x_lo] * up_c[j S + x] (and the
@@ -649,10 +651,10 @@ __global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, 
 }
 
 __global__ void k_fold2(const ef* __restrict__ a, const ef* __restrict__ b, ef* __restrict__ oa, ef* __restrict__ ob,
-                        size_t half, const ef* __restrict__ r) {
+                        size_t half, const ef* __restrict__ r, ef rv) {
   const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (x >= half) return;
-  const ef rr = *r;
+  const ef rr = r ? *r : rv;
   oa[x] = ef_lerp(a[x], a[x + half], rr);
   ob[x] = ef_lerp(b[x], b[x + half], rr);
 }
@@ -787,7 +789,14 @@ void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r
                       ef* eq_out, size_t eq_half) {
   const size_t width = eq_in && eq_half > half ? eq_half : half;
   dim3 grid((unsigned)((width + 255) / 256), ncols + (eq_in ? 1 : 0));
-  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, ncols, r, eq_in, eq_out, eq_half);
+  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, ncols, r, ef_zero(), eq_in, eq_out, eq_half);
+  WL_LAUNCH_CHECK();
+}
+void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef& r, cudaStream_t s, const ef* eq_in,
+                         ef* eq_out, size_t eq_half) {
+  const size_t width = eq_in && eq_half > half ? eq_half : half;
+  dim3 grid((unsigned)((width + 255) / 256), ncols + (eq_in ? 1 : 0));
+  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, ncols, nullptr, r, eq_in, eq_out, eq_half);
   WL_LAUNCH_CHECK();
 }
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
@@ -836,7 +845,11 @@ void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaSt
   WL_LAUNCH_CHECK();
 }
 void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s) {
-  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, r);
+  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, r, ef_zero());
+  WL_LAUNCH_CHECK();
+}
+void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s) {
+  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, nullptr, r);
   WL_LAUNCH_CHECK();
 }
 

@@ -73,6 +73,9 @@ void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, co
 // eq_out[x] = eq_in[x] + eq_in[x + eq_half].
 void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r, cudaStream_t s,
                       const ef* eq_in = nullptr, ef* eq_out = nullptr, size_t eq_half = 0);
+// The same with the challenge passed by value (no device copy of it).
+void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef& r, cudaStream_t s,
+                         const ef* eq_in = nullptr, ef* eq_out = nullptr, size_t eq_half = 0);
 // Up/down evaluations of every column at (r0; tail), with eq(tail, .) factored as
 // eq_hi (2^(log_n-k-ll) entries) x eq_lo (2^ll entries). out_up / out_down must hold
 // AIR_W * (1 + 2^k * 2^(log_n-k-ll)) elements; the first AIR_W are the results.
@@ -88,6 +91,8 @@ void launch_inner_mle(const ef* eqp, int log_n, const ef* alpha2, ef* out, cudaS
 int prod_blocks(size_t half);
 void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s);
 void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s);
+// The same with the challenge passed by value (no device copy of it).
+void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s);
 
 // --------------------------------------------------------------- a*b - c zerocheck
 void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,

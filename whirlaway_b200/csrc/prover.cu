@@ -59,6 +59,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   launch_twiddles(twiddles, stream);
   pinned_bytes = kUpBytes + kDownBytes;
   WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
+  WL_CUDA(cudaHostGetDevicePointer(&pinned_dev, pinned, 0));
   WL_CUDA(cudaStreamSynchronize(stream));
 }
 Context::~Context() {
@@ -68,6 +69,7 @@ Context::~Context() {
   for (auto e : event_pool) cudaEventDestroy(e);
   if (sync_event) cudaEventDestroy(sync_event);
   cudaFree(twiddles);
+  if (part_buf) cudaFree(part_buf);
   cudaFreeHost(pinned);
   cudaStreamDestroy(stream);
 }
@@ -125,6 +127,16 @@ void Context::wait_stream() {
   }
   host_syncs++;
 }
+ef* Context::partials(size_t n) {
+  if (n > part_cap) {
+    if (part_buf) WL_CUDA(cudaFreeAsync(part_buf, stream));
+    part_buf = nullptr;
+    const size_t cap = std::max<size_t>(n, size_t(1) << 16);
+    WL_CUDA(cudaMallocAsync(&part_buf, sizeof(ef) * cap, stream));
+    part_cap = cap;
+  }
+  return static_cast<ef*>(part_buf);
+}
 void Context::to_host(void* dst, const void* src, size_t bytes) {
   char* down = static_cast<char*>(pinned) + kUpBytes;
   if (bytes <= kDownBytes) {
@@ -167,11 +179,16 @@ DBuf upload(Context& ctx, const std::vector<T>& v) {
   return b;
 }
 
+// The reduction writes its k sums straight into the mapped download staging.
 std::vector<ef> reduce_to_host(Context& ctx, const ef* partial, int nblk, int k) {
-  DBuf out(sizeof(ef) * k, ctx.stream);
-  { ProfScope _ps(ctx, "reduce"); launch_reduce_partials(partial, nblk, k, out.as<ef>(), ctx.stream); }
+  if (sizeof(ef) * size_t(k) > kDownBytes) throw std::invalid_argument("reduce_to_host: too many sums");
+  char* down = static_cast<char*>(ctx.pinned) + kUpBytes;
+  ef* down_dev = reinterpret_cast<ef*>(static_cast<char*>(ctx.pinned_dev) + kUpBytes);
+  { ProfScope _ps(ctx, "reduce"); launch_reduce_partials(partial, nblk, k, down_dev, ctx.stream); }
+  ctx.wait_stream();
+  g_up_off = 0;  // every earlier upload has completed
   std::vector<ef> h(k);
-  ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * k);
+  memcpy(h.data(), down, sizeof(ef) * k);
   return h;
 }
 
@@ -357,9 +374,9 @@ ef mle_eval_dev(Context& ctx, const ef* g, int m, const std::vector<ef>& pt) {
   int lh, ll;
   split_vars(m, lh, ll);
   EqPair e = eq_pair(ctx, pt, lh);
-  DBuf part(sizeof(ef) << lh, ctx.stream);
-  { ProfScope _ps(ctx, "mle_eval"); launch_mle_eval_ef(g, lh, ll, e.hi.as<ef>(), e.lo.as<ef>(), part.as<ef>(), ctx.stream); }
-  return reduce_to_host(ctx, part.as<ef>(), 1 << lh, 1)[0];
+  ef* part = ctx.partials(size_t(1) << lh);
+  { ProfScope _ps(ctx, "mle_eval"); launch_mle_eval_ef(g, lh, ll, e.hi.as<ef>(), e.lo.as<ef>(), part, ctx.stream); }
+  return reduce_to_host(ctx, part, 1 << lh, 1)[0];
 }
 
 // k rounds of the WHIR sumcheck on device tables (g, w), both of size 2^m on entry.
@@ -368,17 +385,16 @@ void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, e
   for (int t = 0; t < rounds; t++) {
     size_t half = size_t(1) << (m - 1);
     int nb = whir_sc_blocks(half);
-    DBuf part(sizeof(ef) * 3 * nb, ctx.stream);
-    { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part.as<ef>(), ctx.stream); }
-    std::vector<ef> h = reduce_to_host(ctx, part.as<ef>(), nb, 3);
+    ef* part = ctx.partials(size_t(3) * nb);
+    { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream); }
+    std::vector<ef> h = reduce_to_host(ctx, part, nb, 3);
     ts.add_ext(h.data(), 3);
     grind(ctx, ts, p16, pow_bits);
     ef r = ts.sample_ext();
     rnd.push_back(r);
     sigma = quad_eval(h.data(), r);
     DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
-    DBuf dr = scalar_dev(ctx, r);
-    { ProfScope _ps(ctx, "fold"); launch_fold2(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, dr.as<ef>(), ctx.stream); }
+    { ProfScope _ps(ctx, "fold"); launch_fold2_at(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, r, ctx.stream); }
     g = std::move(ng);
     w = std::move(nw);
     m--;
@@ -539,9 +555,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
     DBuf d_lw = upload(ctx, lw);
     const int nb = zc0_blocks(n, k);
-    DBuf part(sizeof(ef) * size_t(nb) * nz, st);
-    { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part.as<ef>(), st); }
-    std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
+    ef* part = ctx.partials(size_t(nb) * nz);
+    { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part, st); }
+    std::vector<ef> sums = reduce_to_host(ctx, part, nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
     std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
@@ -577,9 +593,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     const int m = n - k - round + 1;  // variables of the current columns
     const size_t half = size_t(1) << (m - 1);
     const int nb = zc_ef_blocks(m);
-    DBuf part(sizeof(ef) * size_t(nb) * 3, st);
-    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part.as<ef>(), st); }
-    std::vector<ef> s3 = reduce_to_host(ctx, part.as<ef>(), nb, 3);
+    ef* part = ctx.partials(size_t(nb) * 3);
+    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+    std::vector<ef> s3 = reduce_to_host(ctx, part, nb, 3);
     const ef& r = zc[round];
     ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
     ef e1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(e0, kb::ef_sub(kb::ef_one(), r))), kb::ef_inv(r));
@@ -593,9 +609,8 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
                      mmf);
     DBuf nc(sizeof(ef) * size_t(W) * half, st);
-    DBuf dc = scalar_dev(ctx, c);
     DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), W, half, dc.as<ef>(), st,
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), W, half, c, st,
                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
     cols = std::move(nc);
     eqr = std::move(eqn);
@@ -636,9 +651,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   std::vector<ef> sub(nsk);
   {
     const int nb = sub_eval_blocks(n, k);
-    DBuf part(sizeof(ef) * size_t(nb) * nsk * 2, st);
-    { ProfScope _ps(ctx, "sub_evals"); launch_sub_evals(B.as<ef>(), n, k, nullptr, eqt.as<ef>(), part.as<ef>(), st); }
-    std::vector<ef> ud = reduce_to_host(ctx, part.as<ef>(), nb, nsk * 2);
+    ef* part = ctx.partials(size_t(nb) * nsk * 2);
+    { ProfScope _ps(ctx, "sub_evals"); launch_sub_evals(B.as<ef>(), n, k, nullptr, eqt.as<ef>(), part, st); }
+    std::vector<ef> ud = reduce_to_host(ctx, part, nb, nsk * 2);
     for (int j = 0; j < nsk; j++) sub[j] = kb::ef_add(ud[2 * j], kb::ef_mul(alpha2, ud[2 * j + 1]));
   }
   ts.add_ext(sub.data(), sub.size());
@@ -662,9 +677,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   for (int round = 0; round < n; round++) {
     const size_t half = N >> (round + 1);
     const int nb = prod_blocks(half);
-    DBuf part(sizeof(ef) * size_t(nb) * 2, st);
-    { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part.as<ef>(), st); }
-    std::vector<ef> s02 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
+    ef* part = ctx.partials(size_t(nb) * 2);
+    { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st); }
+    std::vector<ef> s02 = reduce_to_host(ctx, part, nb, 2);
     ef s1 = kb::ef_sub(inner_sum, s02[0]);
     std::vector<ef> p = interpolate(basis3, {s02[0], s1, s02[1]});
     ts.add_ext(p.data(), p.size());
@@ -673,8 +688,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     inner_sum = poly_eval(p, c);
     grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 2));
     DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
-    DBuf dc = scalar_dev(ctx, c);
-    { ProfScope _ps(ctx, "fold"); launch_fold2(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, dc.as<ef>(), st); }
+    { ProfScope _ps(ctx, "fold"); launch_fold2_at(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, c, st); }
     A = std::move(na);
     B = std::move(nbuf);
   }
@@ -834,9 +848,9 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     DBuf d_lw = upload(ctx, lw);
     eq0 = eq_table_dev(ctx, std::vector<ef>(r.begin() + 1, r.end()));
     const int nb = abc0_blocks(n, k);
-    DBuf part(sizeof(ef) * size_t(nb) * nz, st);
-    { ProfScope _ps(ctx, "abc0_eval"); launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), part.as<ef>(), st); }
-    std::vector<ef> sums = reduce_to_host(ctx, part.as<ef>(), nb, nz);
+    ef* part = ctx.partials(size_t(nb) * nz);
+    { ProfScope _ps(ctx, "abc0_eval"); launch_abc0_eval(a, b, c, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), part, st); }
+    std::vector<ef> sums = reduce_to_host(ctx, part, nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
     std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
@@ -872,9 +886,9 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     const int m = n - k - round + 1;
     const size_t half = size_t(1) << (m - 1);
     const int nb = (int)((half + 31) / 32);
-    DBuf part(sizeof(ef) * size_t(nb) * 2, st);
-    { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part.as<ef>(), st); }
-    std::vector<ef> s2 = reduce_to_host(ctx, part.as<ef>(), nb, 2);
+    ef* part = ctx.partials(size_t(nb) * 2);
+    { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st); }
+    std::vector<ef> s2 = reduce_to_host(ctx, part, nb, 2);
     const ef& rr = r[round];
     ef v0 = kb::ef_mul(s2[0], mmf), v2 = kb::ef_mul(s2[1], mmf);
     ef v1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(v0, kb::ef_sub(kb::ef_one(), rr))), kb::ef_inv(rr));
@@ -889,9 +903,8 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
                                 kb::ef_mul(rr, cc)),
                      mmf);
     DBuf nc(sizeof(ef) * 3 * half, st);
-    DBuf dc = scalar_dev(ctx, cc);
     DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols(cols.as<ef>(), nc.as<ef>(), 3, half, dc.as<ef>(), st,
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), 3, half, cc, st,
                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
     cols = std::move(nc);
     eqr = std::move(eqn);

@@ -42,6 +42,11 @@ struct Context {
   uint2* twiddles = nullptr;  // per-stage Shoup twiddles (launch_twiddles)
   void* pinned = nullptr;        // staging for small device-to-host reads
   size_t pinned_bytes = 0;
+  void* pinned_dev = nullptr;    // the same staging as seen by kernels (mapped host memory)
+  // Reused device buffer for per-round partial sums (grown on demand, kept by the context).
+  void* part_buf = nullptr;
+  size_t part_cap = 0;
+  ef* partials(size_t n);
   std::string last_error;
   uint64_t host_syncs = 0;  // stream synchronisations made by the host (diagnostics)
   Context(int device, uint64_t budget);
