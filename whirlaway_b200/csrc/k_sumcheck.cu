@@ -184,8 +184,9 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
   if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
 }
 
-// out[c * S + x] = sum_j sel[j] * up_c[j * S + x]  (the 2^k loads are issued before the
-// products, sel is zero-padded to 16)
+// out[c * S + x] = sum_j sel[j] * up_c[j * S + x] for two adjacent x per thread (8-byte
+// loads; the 2^k loads are issued before the products, sel is zero-padded to 16). The up
+// row of 2^k S - 1 is 2^k S - 2, patched for the last pair.
 __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ sel_g,
                            ef* __restrict__ out) {
   __shared__ ef sel[16];
@@ -193,21 +194,33 @@ __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, c
   if (threadIdx.x < 16) sel[threadIdx.x] = threadIdx.x < (unsigned)nsk ? sel_g[threadIdx.x] : ef_zero();
   __syncthreads();
   const size_t N = size_t(1) << log_n, S = N >> k;
-  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t x = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
   const int c = blockIdx.y;
   if (x >= S) return;
   const uint32_t* col = wit + size_t(c) * N;
-  uint32_t v[16];
+  uint2 v[16];
 #pragma unroll
-  for (int j = 0; j < 16; j++) v[j] = j < nsk ? col[up_row(size_t(j) * S + x, N)] : 0u;
-  EfMacF m;
-  m.init();
+  for (int j = 0; j < 16; j++)
+    v[j] = j < nsk ? __ldg(reinterpret_cast<const uint2*>(col + size_t(j) * S + x)) : make_uint2(0, 0);
+  if (x + 2 == S) {
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if (j == nsk - 1) v[j].y = col[N - 2];
+  }
+  EfMacF m0, m1;
+  m0.init();
+  m1.init();
 #pragma unroll
   for (int j = 0; j < 16; j++) {
-    m.mac(sel[j], v[j]);
-    if ((j & 3) == 3) m.flush();
+    m0.mac(sel[j], v[j].x);
+    m1.mac(sel[j], v[j].y);
+    if ((j & 3) == 3) {
+      m0.flush();
+      m1.flush();
+    }
   }
-  out[size_t(c) * S + x] = m.value();
+  out[size_t(c) * S + x] = m0.value();
+  out[size_t(c) * S + x + 1] = m1.value();
 }
 
 // ------------------------------------------------------------------ zerocheck rounds >= 1
@@ -495,18 +508,23 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
                                                               int ll, const ef* __restrict__ eq_hi,
                                                               const ef* __restrict__ eq_lo, ef* __restrict__ pu,
                                                               ef* __restrict__ pd) {
+  // columns c0 and c0 + 1 (when it exists) share each eq_lo load
   const size_t N = size_t(1) << log_n, S = N >> k;
-  const int c = blockIdx.x, j = blockIdx.y;
+  const int c0 = 2 * blockIdx.x, j = blockIdx.y;
+  const bool two = c0 + 1 < AIR_W;
   const uint32_t nhi = 1u << (log_n - k - ll);
   const uint32_t xh = blockIdx.z * IS_WARPS + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (xh >= nhi) return;
   const uint32_t nlo = 1u << ll;
-  const uint32_t* col = wit + size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+  const uint32_t* col0 = wit + size_t(c0) * N + size_t(j) * S + (size_t(xh) << ll);
+  const uint32_t* col1 = two ? col0 + N : col0;
   const bool last = j == gridDim.y - 1 && xh == nhi - 1;  // holds the wrapped row N - 1
-  EfMacF mu, md;
-  mu.init();
-  md.init();
+  EfMacF u0, d0, u1, d1;
+  u0.init();
+  d0.init();
+  u1.init();
+  d1.init();
   uint32_t xl = lane;
   for (; xl + 96 < nlo; xl += 128) {
 #pragma unroll
@@ -514,29 +532,45 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
       const uint32_t x = xl + 32 * q;
       const ef e = eq_lo[x];
       const bool wrap = last && x == nlo - 1;
-      mu.mac(e, col[wrap ? x - 1 : x]);
-      md.mac(e, col[wrap ? x : x + 1]);
+      const uint32_t xu = wrap ? x - 1 : x, xd = wrap ? x : x + 1;
+      u0.mac(e, col0[xu]);
+      d0.mac(e, col0[xd]);
+      u1.mac(e, col1[xu]);
+      d1.mac(e, col1[xd]);
     }
-    mu.flush();
-    md.flush();
+    u0.flush();
+    d0.flush();
+    u1.flush();
+    d1.flush();
   }
   for (; xl < nlo; xl += 32) {
     const ef e = eq_lo[xl];
     const bool wrap = last && xl == nlo - 1;
-    mu.mac(e, col[wrap ? xl - 1 : xl]);
-    md.mac(e, col[wrap ? xl : xl + 1]);
-    mu.flush();
-    md.flush();
+    const uint32_t xu = wrap ? xl - 1 : xl, xd = wrap ? xl : xl + 1;
+    u0.mac(e, col0[xu]);
+    d0.mac(e, col0[xd]);
+    u1.mac(e, col1[xu]);
+    d1.mac(e, col1[xd]);
+    u0.flush();
+    d0.flush();
+    u1.flush();
+    d1.flush();
   }
-  const ef su = warp_reduce_ef(mu.value()), sd = warp_reduce_ef(md.value());
+  const ef su0 = warp_reduce_ef(u0.value()), sd0 = warp_reduce_ef(d0.value());
+  const ef su1 = warp_reduce_ef(u1.value()), sd1 = warp_reduce_ef(d1.value());
   if (lane == 0) {
-    const size_t o = (size_t(c) * gridDim.y + j) * nhi + xh;
-    pu[o] = ef_mul(su, eq_hi[xh]);
-    pd[o] = ef_mul(sd, eq_hi[xh]);
+    const ef h = eq_hi[xh];
+    size_t o = (size_t(c0) * gridDim.y + j) * nhi + xh;
+    pu[o] = ef_mul(su0, h);
+    pd[o] = ef_mul(sd0, h);
+    if (two) {
+      o = (size_t(c0 + 1) * gridDim.y + j) * nhi + xh;
+      pu[o] = ef_mul(su1, h);
+      pd[o] = ef_mul(sd1, h);
+    }
   }
 }
 
-// out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]
 // out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]; one warp per column.
 __global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int nh, int ncols,
                               ef* __restrict__ out) {
@@ -759,7 +793,8 @@ void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32
 }
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {
   size_t S = size_t(1) << (log_n - k);
-  dim3 grid((unsigned)((S + 255) / 256), AIR_W);
+  if (S < 2) throw std::invalid_argument("zc0_fold: at least 2 points per skip block");
+  dim3 grid((unsigned)((S / 2 + 255) / 256), AIR_W);
   k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
@@ -806,8 +841,8 @@ void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* 
   const int nh = 1 << (log_n - k - ll);
   ef* pu = out_up + AIR_W;
   ef* pd = out_down + AIR_W;
-  k_inner_sums<<<dim3(AIR_W, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi,
-                                                                                         eq_lo, pu, pd);
+  k_inner_sums<<<dim3((AIR_W + 1) / 2, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(
+      wit, log_n, k, ll, eq_hi, eq_lo, pu, pd);
   WL_LAUNCH_CHECK();
   k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pu, sel, nsk, nh, AIR_W, out_up);
   WL_LAUNCH_CHECK();

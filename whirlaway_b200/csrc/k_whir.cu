@@ -42,17 +42,30 @@ __global__ void k_mle_partial_base(const uint32_t* __restrict__ T, size_t t_len,
       EfMacF m[J];
       for (int j = 0; j < J; j++) m[j].init();
       uint32_t vh = h0;
+      const bool inside = base + (size_t(h1) << ll) <= t_len;  // no entry of this block is past the table
       for (; vh + 4 <= h1; vh += 4) {  // four loads in flight per thread
         uint32_t t[4];
+        if (inside) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          size_t idx = base + (size_t(vh + q) << ll) + vlo;
-          t[q] = idx < t_len ? T[idx] : 0u;
+          for (int q = 0; q < 4; q++) t[q] = __ldg(T + base + (size_t(vh + q) << ll) + vlo);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            size_t idx = base + (size_t(vh + q) << ll) + vlo;
+            t[q] = idx < t_len ? T[idx] : 0u;
+          }
         }
+        if (per <= 128) {
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+          for (int q = 0; q < 4; q++)
 #pragma unroll
-          for (int j = 0; j < J; j++) m[j].mac(hget(j, vh + q), t[q]);
+            for (int j = 0; j < J; j++) m[j].mac(hs[j][vh + q - h0], t[q]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int j = 0; j < J; j++) m[j].mac(hi[size_t(j) * nhi + vh + q], t[q]);
+        }
 #pragma unroll
         for (int j = 0; j < J; j++) m[j].flush();
       }
@@ -86,51 +99,74 @@ __global__ void k_sum_split(const ef* __restrict__ in, size_t n, ef* __restrict_
   out[i] = acc;
 }
 
-// out[v] = sum_u eqr[u] * T[u * 2^lv + v]
+// out[v] = sum_u eqr[u] * T[u * 2^lv + v]; two adjacent v per thread (8-byte loads).
 __global__ void k_whir_fold_T(const uint32_t* __restrict__ T, size_t t_len, int lu, int lv,
                               const ef* __restrict__ eqr_g, ef* __restrict__ out) {
   extern __shared__ ef eqr[];
   const int nu = 1 << lu;
   for (int i = threadIdx.x; i < nu; i += blockDim.x) eqr[i] = eqr_g[i];
   __syncthreads();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t v = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
   if (v >= (size_t(1) << lv)) return;
-  EfMacF m;
-  m.init();
+  EfMacF m0, m1;
+  m0.init();
+  m1.init();
+  const size_t row = size_t(1) << lv;
   for (int u0 = 0; u0 < nu; u0 += 4) {
-    if ((size_t(u0) << lv) + v >= t_len) break;  // the rest of the packed table is zero
-    uint32_t t[4];
+    const size_t base = (size_t(u0) << lv) + v;
+    if (base >= t_len) break;  // the rest of the packed table is zero
+    uint2 t[4];
+    ef e[4];
+    if (u0 + 3 < nu && base + 3 * row + 1 < t_len) {  // the whole group is in range
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const size_t idx = (size_t(u0 + q) << lv) + v;
-      t[q] = (u0 + q < nu && idx < t_len) ? T[idx] : 0u;
+      for (int q = 0; q < 4; q++) {
+        t[q] = __ldg(reinterpret_cast<const uint2*>(T + base + q * row));
+        e[q] = eqr[u0 + q];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const size_t idx = base + q * row;
+        const bool in_u = u0 + q < nu;
+        t[q] = make_uint2(in_u && idx < t_len ? T[idx] : 0u, in_u && idx + 1 < t_len ? T[idx + 1] : 0u);
+        e[q] = in_u ? eqr[u0 + q] : ef_zero();
+      }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) m.mac(u0 + q < nu ? eqr[u0 + q] : ef_zero(), t[q]);
-    m.flush();
+    for (int q = 0; q < 4; q++) {
+      m0.mac(e[q], t[q].x);
+      m1.mac(e[q], t[q].y);
+    }
+    m0.flush();
+    m1.flush();
   }
-  out[v] = m.value();
+  out[v] = m0.value();
+  out[v + 1] = m1.value();
 }
 
-// w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (base-field points)
+// w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (base-field points). When a block's
+// entries share v_hi (2^ll >= blockDim), a_t = coefs[t] * hi_t[v_hi] is formed once per block
+// and each entry accumulates a_t * lo_t[v_lo]; otherwise each term multiplies hi and lo.
 __global__ void k_add_eq_terms_f(ef* __restrict__ w, int lh, int ll, int npts, const uint32_t* __restrict__ hi,
                                  const uint32_t* __restrict__ lo, const ef* __restrict__ coefs_g) {
   extern __shared__ ef coefs[];
-  for (int i = threadIdx.x; i < npts; i += blockDim.x) coefs[i] = coefs_g[i];
+  const size_t nhi = size_t(1) << lh, nlo = size_t(1) << ll;
+  const bool shared_hi = nlo >= blockDim.x;
+  const size_t vh_blk = (size_t(blockIdx.x) * blockDim.x) >> ll;
+  for (int i = threadIdx.x; i < npts; i += blockDim.x)
+    coefs[i] = shared_hi ? ef_mul_f(coefs_g[i], hi[i * nhi + vh_blk]) : coefs_g[i];
   __syncthreads();
   const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= (size_t(1) << (lh + ll))) return;
-  const size_t vh = v >> ll, vl = v & ((size_t(1) << ll) - 1);
-  const size_t nhi = size_t(1) << lh, nlo = size_t(1) << ll;
+  const size_t vh = v >> ll, vl = v & (nlo - 1);
   EfMacF m;
   m.init_with(w[v]);
   int cnt = 0;
   for (int t = 0; t < npts; t++) {
-    uint32_t e = mul(hi[t * nhi + vh], lo[t * nlo + vl]);
-    m.mac(coefs[t], e);
+    const uint32_t l = lo[t * nlo + vl];
+    m.mac(coefs[t], shared_hi ? l : mul(hi[t * nhi + vh], l));
     if (++cnt == 4) { m.flush(); cnt = 0; }
   }
-  m.flush();
   w[v] = m.value();
 }
 
@@ -205,7 +241,8 @@ void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, in
 
 void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s) {
   size_t n = size_t(1) << lv;
-  k_whir_fold_T<<<(unsigned)((n + 255) / 256), 256, sizeof(ef) << lu, s>>>(T, t_len, lu, lv, eqr, out);
+  if (lv < 1) throw std::invalid_argument("whir_fold_T: at least 2 entries");
+  k_whir_fold_T<<<(unsigned)((n / 2 + 255) / 256), 256, sizeof(ef) << lu, s>>>(T, t_len, lu, lv, eqr, out);
   WL_LAUNCH_CHECK();
 }
 
