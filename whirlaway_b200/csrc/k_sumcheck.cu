@@ -159,18 +159,23 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
       issue(next++);
     }
     const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
-    uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    // two chains of (up to) 8 products, folded with 2^32 = 2^25 - 2 (mod p) after every 4
+    // (a folded sum stays below 2^57 + 2^32, so 4 more products fit in 64 bits), then one
+    // Montgomery reduction of their sum (below 2^59 < 4 p^2)
+    uint64_t sa = 0, sb = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (4 * q < nsk) {
-        uint4 v = row[q];
-        s0 += wmul(w[4 * q], v.x);
-        s1 += wmul(w[4 * q + 1], v.y);
-        s2 += wmul(w[4 * q + 2], v.z);
-        s3 += wmul(w[4 * q + 3], v.w);
+        const uint4 v = row[q];
+        uint64_t& acc = (q & 1) ? sb : sa;
+        acc += wmul(w[4 * q], v.x);
+        acc += wmul(w[4 * q + 1], v.y);
+        acc += wmul(w[4 * q + 2], v.z);
+        acc += wmul(w[4 * q + 3], v.w);
+        acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
       }
     }
-    return add(add(redc(s0), redc(s1)), add(redc(s2), redc(s3)));
+    return redc(sa + sb);
   };
   __syncthreads();  // alphas
   EfMacF m;
@@ -440,35 +445,38 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
   const bool valid = x < half;
   const size_t xs = valid ? x : 0;
   ZCD_GET;
-  ef st[2], pslot[3], s0slot[3];
+  ef st[2];
   uint32_t dg[2];
 #pragma unroll
   for (int kk = 0; kk < 2; kk++) {
     st[kk] = get(65 + 2 * sub + kk);
     dg[kk] = p2_diag<16>(2 * sub + kk);
   }
-#pragma unroll
-  for (int t = 0; t < 3; t++) pslot[t] = (8 * t + sub < 20) ? get(81 + 8 * t + sub) : ef_zero();
-#pragma unroll
-  for (int r = 0; r < 20; r++) {
-    const int t = r >> 3, owner = r & 7;
-    const ef w0 = shfl_idx_ef(st[0], gbase);
-    if (sub == owner) s0slot[t] = w0;
-    const ef p = shfl_idx_ef(pslot[t], gbase | owner);
-    if (sub == 0) st[0] = p;
-    ef sum = ef_add(st[0], st[1]);
-    sum = ef_add(sum, shfl_xor_ef(sum, 1));
-    sum = ef_add(sum, shfl_xor_ef(sum, 2));
-    sum = ef_add(sum, shfl_xor_ef(sum, 4));
-#pragma unroll
-    for (int kk = 0; kk < 2; kk++) st[kk] = ef_add(ef_mul_f(st[kk], dg[kk]), sum);
-  }
+  // rounds in groups of 8 (a rolled loop keeps the code small): in group t, lane sub holds
+  // the partial post p_(8t+sub), records state word 0 of round 8t + sub, and evaluates that
+  // round's S-box constraint once the group is done
   ef acc = ef_zero();
-#pragma unroll
+  ef p_cur = get(81 + sub);
+#pragma unroll 1
   for (int t = 0; t < 3; t++) {
+    ef s0_cur = ef_zero();
+#pragma unroll
+    for (int o = 0; o < 8; o++) {
+      if (8 * t + o >= 20) break;
+      const ef w0 = shfl_idx_ef(st[0], gbase);
+      if (sub == o) s0_cur = w0;
+      const ef p = shfl_idx_ef(p_cur, gbase | o);
+      if (sub == 0) st[0] = p;
+      ef sum = ef_add(st[0], st[1]);
+      sum = ef_add(sum, shfl_xor_ef(sum, 1));
+      sum = ef_add(sum, shfl_xor_ef(sum, 2));
+      sum = ef_add(sum, shfl_xor_ef(sum, 4));
+#pragma unroll
+      for (int kk = 0; kk < 2; kk++) st[kk] = ef_add(ef_mul_f(st[kk], dg[kk]), sum);
+    }
     const int r = 8 * t + sub;
-    if (r < 20)
-      acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(ef_cube(ef_add_f(s0slot[t], K.partial[r])), pslot[t])));
+    if (r < 20) acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(ef_cube(ef_add_f(s0_cur, K.partial[r])), p_cur)));
+    if (t < 2) p_cur = (r + 8 < 20) ? get(81 + r + 8) : ef_zero();
   }
 #pragma unroll
   for (int kk = 0; kk < 2; kk++) {
