@@ -5,6 +5,9 @@
 #include <cstdio>
 #include <random>
 #include "poseidon2.cuh"
+namespace wl {
+void host_p16_permute(uint32_t* s, const kb::P16Consts& c);
+}
 using namespace kb;
 int main() {
   std::mt19937_64 g(1);
@@ -92,8 +95,14 @@ int main() {
         mds(r);
       }
       for (int i = 0; i < W; i++) s[i] = to_mont(s[i]);
+      uint32_t sv[16];
+      for (int i = 0; i < 16; i++) sv[i] = s[i];
       if (w) p2_permute<24>(s, c24); else p2_permute<16>(s, c16);
       for (int i = 0; i < W; i++) if (from_mont(s[i]) != r[i]) { b8++; break; }
+      if (!w) {  // the transcript's host permutation (vector when the CPU has AVX-512)
+        wl::host_p16_permute(sv, c16);
+        for (int i = 0; i < 16; i++) if (sv[i] != s[i]) { b8++; break; }
+      }
     }
   }
   printf("add %ld sub %ld mul %ld diag %ld halve %ld redc %ld cube %ld permute %ld\n", b1,b2,b3,b4,b5,b6,b7,b8);

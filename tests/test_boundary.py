@@ -46,6 +46,7 @@ def test_host_entry_points_without_gpu(wl, oracle):
 def test_device_field_arithmetic_on_host(tmp_path):
     exe = tmp_path / "field_check"
     subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "whirlaway_b200", "csrc"),
-                    os.path.join(ROOT, "tests", "field_host_check.cpp"), "-o", str(exe)], check=True)
+                    os.path.join(ROOT, "tests", "field_host_check.cpp"),
+                    os.path.join(ROOT, "whirlaway_b200", "csrc", "host_perm.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr

@@ -11,7 +11,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libwhirlaway_b200.so")
-SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_probe.cu", "prover.cu", "server.cu", "noalloc.cu", "capi.cu"]
+SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_probe.cu", "prover.cu", "server.cu", "noalloc.cu", "capi.cu",
+           "host_perm.cpp"]
+CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC"]  # host-only sources (g++; CPU features dispatched at run time)
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -34,17 +36,20 @@ def build(verbose=False, jobs=None):
     objs, procs = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
+        o = os.path.join(OUT_DIR, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if _stale(o, [s] + headers):
-            cmd = ["nvcc"] + NVCC_FLAGS + ["-c", s, "-o", o]
+            if src.endswith(".cpp"):
+                cmd = ["g++"] + CXX_FLAGS + ["-c", s, "-o", o]
+            else:
+                cmd = ["nvcc"] + NVCC_FLAGS + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
             procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
     for src, p in procs:
         out, _ = p.communicate()
         if p.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{out.decode()}")
+            raise RuntimeError(f"compiler failed on {src}:\n{out.decode()}")
     if _stale(LIB, objs):
         cmd = ["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-ccbin", "g++", "-o", LIB] + objs
         subprocess.run(cmd, check=True)

@@ -31,6 +31,9 @@ struct Settings {
 // ------------------------------------------------------------------ transcript
 // DuplexChallenger<F, Poseidon16, 16, 8>: observations overwrite the rate part of the
 // sponge once eight are buffered; samples pop from the end of the last squeeze.
+// Poseidon2-16 on the host (host_perm.cpp): AVX-512 when the CPU has it, else scalar.
+void host_p16_permute(uint32_t* s, const kb::P16Consts& c);
+
 struct HostChallenger {
   const kb::P16Consts* perm = nullptr;
   uint32_t state[16] = {0};
@@ -41,7 +44,7 @@ struct HostChallenger {
   void duplex() {
     for (int i = 0; i < in_len; i++) state[i] = in[i];
     in_len = 0;
-    kb::p2_permute<16>(state, *perm);
+    host_p16_permute(state, *perm);
     for (int i = 0; i < 8; i++) out[i] = state[i];
     out_len = 8;
   }
