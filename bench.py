@@ -388,7 +388,7 @@ def run_ours(args, world, rank, local):
     dominant = max(breakdown.items(), key=lambda kv: kv[1][0])[0]
     sampler = ClockSampler(local)
     ctx.profile(True, only=dominant)
-    syncs0 = ctx.host_syncs
+    syncs0, wait0 = ctx.host_syncs, ctx.host_wait_ms
     barrier(world)
     torch.cuda.synchronize()
     launches0 = wl.kernel_launch_count()
@@ -407,6 +407,7 @@ def run_ours(args, world, rank, local):
     profile = ctx.profile_report()
     ctx.profile(False)
     host_syncs = (ctx.host_syncs - syncs0) / args.steps
+    host_wait = (ctx.host_wait_ms - wait0) / args.steps
     value = args.steps * (1 << log_n) * world / (elapsed_ms * 1e-3)
 
     # end to end through the C ABI with a pinned host witness
@@ -461,6 +462,7 @@ def run_ours(args, world, rank, local):
         "int_peaks": {"modmul_per_s": modmul_peak, "p24_perms_per_s": p24_peak},
         "phases_ms": table.last_timings_ms,
         "host_syncs_per_step": host_syncs,
+        "host_wait_ms_per_step": host_wait,
         "kernel_profile_ms": {k: round(v[0], 4) for k, v in sorted(breakdown.items(), key=lambda kv: -kv[1][0])},
         "kernel_profile_source": "CUDA events per kernel class over the last warm-up proof",
         "proof_len": int(proof.size),

@@ -177,6 +177,10 @@ wl_status wl_ctx_set_spin_sync(wl_ctx* ctx, int32_t spin);
 // of challenges, sums and roots). Diagnostics; no reference counterpart.
 wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out);
 
+// Total milliseconds the host has spent waiting in those synchronisations (the rest of a
+// proof's wall time is host work and launches). Diagnostics; no reference counterpart.
+wl_status wl_ctx_host_wait_ms(wl_ctx* ctx, double* out);
+
 /* Instrumentation (no reference counterpart; the reference profiles with tracing spans,
  * src/examples/poseidon2.rs:91-100). With profiling on, every kernel class launched on the
  * context is bracketed by CUDA events on the context's stream; wl_profile_json writes

@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "wl_ctx_host_syncs": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "wl_ctx_set_spin_sync": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_ctx_host_wait_ms": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "wl_profile_only": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double)]),
@@ -195,6 +196,13 @@ class Context:
         """Host synchronisations of this context's stream so far."""
         v = ctypes.c_uint64()
         self.check(self._lib.wl_ctx_host_syncs(self.handle, ctypes.byref(v)), "host_syncs")
+        return v.value
+
+    @property
+    def host_wait_ms(self) -> float:
+        """Milliseconds the host has spent waiting for this context's stream."""
+        v = ctypes.c_double()
+        self.check(self._lib.wl_ctx_host_wait_ms(self.handle, ctypes.byref(v)), "host_wait_ms")
         return v.value
 
     def probe_int_peaks(self, constants: np.ndarray):

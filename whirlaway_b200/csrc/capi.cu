@@ -329,6 +329,12 @@ wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out) {
   return WL_OK;
 }
 
+wl_status wl_ctx_host_wait_ms(wl_ctx* ctx, double* out) {
+  if (!ctx || !out) return WL_E_INVALID_ARG;
+  *out = ctx->c->host_wait_ms;
+  return WL_OK;
+}
+
 wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
   if (!ctx || !buf) return WL_E_INVALID_ARG;
   return guarded(ctx, [&] {

@@ -115,6 +115,7 @@ ProfScope::~ProfScope() {
 }
 
 void Context::wait_stream() {
+  const auto w0 = std::chrono::steady_clock::now();
   if (spin_sync) {
     if (!sync_event) WL_CUDA(cudaEventCreateWithFlags(&sync_event, cudaEventDisableTiming));
     WL_CUDA(cudaEventRecord(sync_event, stream));
@@ -126,6 +127,7 @@ void Context::wait_stream() {
     WL_CUDA(cudaStreamSynchronize(stream));
   }
   host_syncs++;
+  host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
 }
 ef* Context::partials(size_t n) {
   if (n > part_cap) {

@@ -49,6 +49,7 @@ struct Context {
   ef* partials(size_t n);
   std::string last_error;
   uint64_t host_syncs = 0;  // stream synchronisations made by the host (diagnostics)
+  double host_wait_ms = 0;  // time the host spent in them
   Context(int device, uint64_t budget);
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
