@@ -99,6 +99,43 @@ struct EfMacF {
     return r;
   }
 };
+
+// Lazy extension x extension multiply-accumulate: acc += a * b in F[X]/(X^8 - 3). Coefficient
+// k of a * b is sum_t a_t * b'_(k-t), b'_i = b_i for i >= 0 and 3 b_(i+8) for the wrapped
+// terms; its 8 products go into the 64-bit running sum in two groups of four, each followed
+// by the fold of EfMacF (so the sum stays below 2^64), and value() reduces once. Against a
+// full product and an addition this saves the 16 reductions of every term.
+struct EfMacE {
+  uint64_t s[8];
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int i = 0; i < 8; i++) s[i] = 0;
+  }
+  __device__ __forceinline__ static uint64_t fold(uint64_t v) {
+    return uint64_t(uint32_t(v >> 32)) * EfMacF::C32 + uint32_t(v);
+  }
+  __device__ __forceinline__ void mac(const ef& a, const ef& b) {
+    uint32_t b3[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) b3[j] = kb::add(kb::dbl(b.c[j]), b.c[j]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      uint64_t v = s[k];
+#pragma unroll
+      for (int t = 0; t < 4; t++) v += kb::wmul(a.c[t], t <= k ? b.c[k - t] : b3[k + 8 - t]);
+      v = fold(v);
+#pragma unroll
+      for (int t = 4; t < 8; t++) v += kb::wmul(a.c[t], t <= k ? b.c[k - t] : b3[k + 8 - t]);
+      s[k] = fold(v);
+    }
+  }
+  __device__ __forceinline__ ef value() const {
+    ef r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.c[i] = kb::redc(fold(s[i]));
+    return r;
+  }
+};
 #endif
 
 }  // namespace wl

@@ -413,17 +413,28 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_full_dense(const ef* __re
     t = ef_add(t, shfl_xor_ef(t, 8));
     in = ef_add(y, t);
   }
-  ef acc = ef_zero();
+  EfMacE pos, neg;  // beta * cube terms, alpha * post terms
+  pos.init();
+  neg.init();
+  // A round's input is the previous round's post, which this lane already holds, except for
+  // ending round 1 (segment 4), whose input is ending round 0's post. The next segment's
+  // post (and that one input) are loaded a segment ahead.
+  auto post_of = [](int seg) { return seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3); };
+  ef pv = get(post_of(0) + j);
+  ef in4 = ef_zero();
 #pragma unroll 1
   for (int seg = 0; seg < 7; seg++) {
     const int f = seg < 4 ? seg : seg + 1;
     const uint32_t rc = seg < 4 ? K.begin[seg][j] : K.end[seg - 3][j];
-    const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
     const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
-    if (seg > 0) in = get(post - 16 + j);
-    const ef pv = get(post + j);
-    acc = ef_add(acc, ef_sub(ef_mul(betas[16 * f + j], ef_cube(ef_add_f(in, rc))), ef_mul(alphas[c0 + j], pv)));
+    const ef pv_next = seg < 6 ? get(post_of(seg + 1) + j) : ef_zero();
+    if (seg == 3) in4 = get(101 + j);
+    pos.mac(betas[16 * f + j], ef_cube(ef_add_f(in, rc)));
+    neg.mac(alphas[c0 + j], pv);
+    in = seg == 3 ? in4 : pv;
+    pv = pv_next;
   }
+  const ef acc = ef_sub(pos.value(), neg.value());
   // fold the point's 16 lanes, weight by eq, then the block sum
   ef pt = acc;
 #pragma unroll
@@ -455,7 +466,9 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
   // rounds in groups of 8 (a rolled loop keeps the code small): in group t, lane sub holds
   // the partial post p_(8t+sub), records state word 0 of round 8t + sub, and evaluates that
   // round's S-box constraint once the group is done
-  ef acc = ef_zero();
+  EfMacE pos, neg;  // S-box / cube terms, committed-post terms
+  pos.init();
+  neg.init();
   ef p_cur = get(81 + sub);
 #pragma unroll 1
   for (int t = 0; t < 3; t++) {
@@ -475,16 +488,19 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
       for (int kk = 0; kk < 2; kk++) st[kk] = ef_add(ef_mul_f(st[kk], dg[kk]), sum);
     }
     const int r = 8 * t + sub;
-    if (r < 20) acc = ef_add(acc, ef_mul(alphas[64 + r], ef_sub(ef_cube(ef_add_f(s0_cur, K.partial[r])), p_cur)));
+    if (r < 20) {
+      pos.mac(alphas[64 + r], ef_cube(ef_add_f(s0_cur, K.partial[r])));
+      neg.mac(alphas[64 + r], p_cur);
+    }
     if (t < 2) p_cur = (r + 8 < 20) ? get(81 + r + 8) : ef_zero();
   }
 #pragma unroll
   for (int kk = 0; kk < 2; kk++) {
     const int j = 2 * sub + kk;
-    acc = ef_add(acc, ef_sub(ef_mul(betas[16 * 4 + j], ef_cube(ef_add_f(st[kk], K.end[0][j]))),
-                             ef_mul(alphas[84 + j], get(101 + j))));
+    pos.mac(betas[16 * 4 + j], ef_cube(ef_add_f(st[kk], K.end[0][j])));
+    neg.mac(alphas[84 + j], get(101 + j));
   }
-  ef pt = acc;
+  ef pt = ef_sub(pos.value(), neg.value());
 #pragma unroll
   for (int d = 4; d > 0; d >>= 1) pt = ef_add(pt, shfl_xor_ef(pt, d));
   const ef res = (sub == 0 && valid) ? ef_mul(pt, eq[xs]) : ef_zero();
