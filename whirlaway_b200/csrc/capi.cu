@@ -243,12 +243,16 @@ wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* consta
   if (!ctx) return WL_E_INVALID_ARG;
   std::string why;
   if (!settings_ok(s, log_n, why)) return fail(ctx, WL_E_INVALID_ARG, why);
-  wl_witness* w = nullptr;
-  wl_status st = wl_witness_upload(ctx, log_n, witness, &w);
-  if (st != WL_OK) return st;
-  st = wl_prove_witness(ctx, s, constants, w, proof_out, proof_len, timings_ms);
-  wl_witness_free(ctx, w);
-  return st;
+  if (!witness || !constants || !proof_len) return fail(ctx, WL_E_INVALID_ARG, "NULL argument");
+  if (log_n < 2 || log_n > 22) return fail(ctx, WL_E_INVALID_ARG, "log_n out of range");
+  // the witness goes up in tiles of 16 columns while the first commitment encodes
+  return guarded(ctx, [&] {
+    wl::ProofJob job = make_job(s, constants, log_n);
+    wl::Timings t;
+    std::vector<uint32_t> pr = wl::prove_air_host(*ctx->c, job, witness, &t);
+    store_timings(t, timings_ms);
+    return emit_proof(ctx, pr, proof_out, proof_len);
+  });
 }
 
 wl_status wl_prove_batch(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, int32_t n,

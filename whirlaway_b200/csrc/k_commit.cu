@@ -136,7 +136,8 @@ __device__ __forceinline__ void ntt_round_rb(int rb, const NttLane& ln, const ui
 template <bool FROM_SRC>
 __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint32_t* __restrict__ data, int T,
                                                             int Bs, int Bp, int rb1, int lr_log, int hg_log,
-                                                            const uint2* __restrict__ tw) {
+                                                            const uint2* __restrict__ tw, int tile0) {
+  const int tile = tile0 + blockIdx.y;
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t npts = 1u << Bp, ntw = npts - 1;
   const int LR = 1 << lr_log;
@@ -156,9 +157,9 @@ __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint3
   const bool active = h2 < (1 << hg_log);
   NttLane ln;
   const int le = in.elem == 8 ? 3 : 0;
-  const uint32_t gcol = blockIdx.y * 8 + c;
+  const uint32_t gcol = tile * 8 + c;
   const size_t hi = (hg << hg_log) + h2;
-  const size_t row0 = (size_t(blockIdx.y) << T) + (lg << lr_log) + l + (hi << (Bs + Bp));
+  const size_t row0 = (size_t(tile) << T) + (lg << lr_log) + l + (hi << (Bs + Bp));
   ln.src = nullptr;
   ln.src_end = in.src + in.src_len;
   if (FROM_SRC && gcol < (uint32_t)in.n_cols)
@@ -441,11 +442,13 @@ void launch_twiddles(uint2* tw, cudaStream_t s) {
   WL_LAUNCH_CHECK();
 }
 
-void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s) {
+void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s, int tile_begin, int tile_end) {
   const int T = in.L + in.rho;
   if (T > 24) throw std::runtime_error("LDE beyond the two-adic subgroup of order 2^24");
   if (in.n_cols % 8 || in.n_cols <= 0) throw std::runtime_error("LDE column count must be a multiple of 8");
-  const int tiles = in.n_cols / 8;
+  if (tile_end < 0) tile_end = in.n_cols / 8;
+  if (tile_begin < 0 || tile_begin >= tile_end || tile_end > in.n_cols / 8) throw std::runtime_error("LDE tile range");
+  const int tiles = tile_end - tile_begin;
   const int np = in.L <= NTT_MAX_BP ? 1 : (in.L + NTT_MAX_BP - 1) / NTT_MAX_BP;
   int Bs = in.rho, left = in.L;
   for (int p = 0; p < np; p++) {
@@ -456,8 +459,12 @@ void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_
     const int hg_log = (2 - lr_log) < hi_bits ? (2 - lr_log) : hi_bits;
     const unsigned gx = 1u << ((Bs - lr_log) + (hi_bits - hg_log));
     const size_t smem = ((size_t(32) << Bp) + (size_t(2) << lr_log) * ((1u << Bp) - 1)) * 4;
-    if (p == 0) k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw);
-    else k_ntt_pass<false><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw);
+    if (p == 0)
+      k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
+                                                                      tile_begin);
+    else
+      k_ntt_pass<false><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
+                                                                       tile_begin);
     WL_LAUNCH_CHECK();
     Bs += Bp;
     left -= Bp;

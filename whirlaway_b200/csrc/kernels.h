@@ -29,7 +29,9 @@ struct LdeSource {
 };
 // Codeword matrix of 2^(L + rho) rows and n_cols (a multiple of 8) columns, tile-major:
 // word (tile, row, c) at (tile * 2^(L+rho) + row) * 8 + c.
-void launch_lde(const LdeSource& in, uint32_t* out, const uint2* twiddles, cudaStream_t s);
+// Tiles [tile_begin, tile_end) of 8 columns only (default: all); tiles are independent.
+void launch_lde(const LdeSource& in, uint32_t* out, const uint2* twiddles, cudaStream_t s, int tile_begin = 0,
+                int tile_end = -1);
 // Per-stage twiddle table (2^24 - 1 entries): stage t = 1..24 holds (w canonical,
 // floor(w 2^32 / p)) for w = w_{2^t}^x, x < 2^(t-1), at offset 2^(t-1) - 1.
 constexpr size_t TWIDDLE_ENTRIES = (size_t(1) << 24) - 1;

@@ -51,6 +51,7 @@ thread_local size_t g_up_off = 0;
 Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaSetDevice(dev));
   WL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  WL_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
   cudaMemPool_t pool;
   WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
@@ -71,6 +72,8 @@ Context::~Context() {
   cudaFree(twiddles);
   if (part_buf) cudaFree(part_buf);
   cudaFreeHost(pinned);
+  cudaStreamSynchronize(copy_stream);
+  cudaStreamDestroy(copy_stream);
   cudaStreamDestroy(stream);
 }
 cudaEvent_t Context::take_event() {
@@ -242,7 +245,7 @@ struct Commitment {
 size_t level_offset(int LL, int l) { return (size_t(1) << (LL + 1)) - (size_t(1) << (LL + 1 - l)); }
 
 Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, const kb::P24Consts& p24,
-                  const kb::P16Consts& p16) {
+                  const kb::P16Consts& p16, const std::vector<cudaEvent_t>* tile_ready = nullptr) {
   Commitment c;
   c.num_vars = num_vars;
   c.fold = fold;
@@ -252,7 +255,18 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   if ((src.elem << fold) != 128) throw std::invalid_argument("leaf rows must hold 128 base-field values");
   const size_t rows = size_t(1) << c.log_leaves;
   c.lde = DBuf(rows * c.n_cols * sizeof(uint32_t), ctx.stream);
-  { ProfScope _ps(ctx, "lde"); launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
+  if (tile_ready) {
+    // tile t's source columns arrive behind event t
+    for (int t = 0; t < c.n_cols / 8; t++) {
+      if (t < (int)tile_ready->size()) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[t], 0));
+      ProfScope _ps(ctx, "lde");
+      launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, t, t + 1);
+    }
+    for (size_t t = c.n_cols / 8; t < tile_ready->size(); t++) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[t], 0));
+  } else {
+    ProfScope _ps(ctx, "lde");
+    launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream);
+  }
   const int LL = c.log_leaves;
   c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
   uint32_t* t = c.tree.as<uint32_t>();
@@ -463,7 +477,8 @@ size_t proof_len_bound(const Settings& s, int log_n) {
   return n;
 }
 
-std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit, Timings* tm) {
+std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit, Timings* tm,
+                                const std::vector<cudaEvent_t>* tile_ready) {
   const Settings& s = job.settings;
   const int n = job.log_n, k = s.univariate_skips, W = AIR_W;
   if (k >= n) throw std::invalid_argument("univariate_skips must be smaller than log_n_rows");
@@ -483,7 +498,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   split_vars(lv, lh_v, ll_v);
   LdeSource src0{wit, t_len, 1, lv, ws.c[0].log_inv_rate, 0};
   src0.n_cols = (int)(((t_len + (size_t(1) << lv) - 1) >> lv) + 7) / 8 * 8;
-  Commitment c0 = commit(ctx, src0, m0, ws.c[0].fold, job.p24, job.p16);
+  Commitment c0 = commit(ctx, src0, m0, ws.c[0].fold, job.p24, job.p16, tile_ready);
   ts.add_base(c0.root, 8);
   // Commitment OOD: F_0[u] = sum_v T[u, v] eq(pt_v, v), answer = sum_u eq(pt_u, u) F_0[u].
   std::vector<std::vector<ef>> ood_pts;
@@ -813,6 +828,40 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     tm->total_ms = t4 - t0;
   }
   return to_canonical(ts.proof);
+}
+
+std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const uint32_t* wit_host, Timings* tm) {
+  const size_t N = size_t(1) << job.log_n;
+  DBuf wit(sizeof(uint32_t) * N * AIR_W, ctx.stream);
+  // the copy stream must not start before the allocation is usable
+  cudaEvent_t alloc_done;
+  WL_CUDA(cudaEventCreateWithFlags(&alloc_done, cudaEventDisableTiming));
+  WL_CUDA(cudaEventRecord(alloc_done, ctx.stream));
+  WL_CUDA(cudaStreamWaitEvent(ctx.copy_stream, alloc_done, 0));
+  std::vector<cudaEvent_t> ready;
+  for (int c0 = 0; c0 < AIR_W; c0 += 16) {
+    const size_t cols = std::min(16, AIR_W - c0);
+    uint32_t* dst = wit.as<uint32_t>() + size_t(c0) * N;
+    cudaEvent_t e;
+    WL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ready.push_back(e);
+    WL_CUDA(cudaMemcpyAsync(dst, wit_host + size_t(c0) * N, sizeof(uint32_t) * cols * N, cudaMemcpyHostToDevice,
+                            ctx.copy_stream));
+    launch_to_mont(dst, cols * N, ctx.copy_stream);
+    WL_CUDA(cudaEventRecord(e, ctx.copy_stream));
+  }
+  std::vector<uint32_t> proof;
+  try {
+    proof = prove_air(ctx, job, wit.as<uint32_t>(), tm, &ready);
+  } catch (...) {
+    cudaStreamSynchronize(ctx.copy_stream);
+    for (auto e : ready) cudaEventDestroy(e);
+    cudaEventDestroy(alloc_done);
+    throw;
+  }
+  for (auto e : ready) cudaEventDestroy(e);
+  cudaEventDestroy(alloc_done);
+  return proof;
 }
 
 // ------------------------------------------------------------------ a*b - c zerocheck

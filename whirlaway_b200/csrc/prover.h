@@ -38,6 +38,7 @@ class DBuf {
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host-to-device witness tiles, overlapped with the LDE
   uint64_t hbm_budget = 0;
   uint2* twiddles = nullptr;  // per-stage Shoup twiddles (launch_twiddles)
   void* pinned = nullptr;        // staging for small device-to-host reads
@@ -99,7 +100,15 @@ struct ProofJob {
 
 // Proves with a device-resident, Montgomery-form, column-major witness (165 columns of
 // 2^log_n values). Returns the proof in canonical form.
-std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit_dev, Timings* t);
+// With `tile_ready`, event t signals that witness columns 16 t .. 16 t + 15 are on the device;
+// the first commitment's LDE waits for each tile just before encoding it.
+std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit_dev, Timings* t,
+                                const std::vector<cudaEvent_t>* tile_ready = nullptr);
+
+// Proves from a host witness (canonical, column-major): the witness is copied in tiles of 16
+// columns on the context's copy stream while the first commitment encodes the tiles already
+// present. Same proof as uploading first.
+std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const uint32_t* wit_host, Timings* t);
 
 // Standalone zerocheck of eq(r, x) * (a * b - c) with a univariate skip; a, b, c device
 // Montgomery arrays of 2^log_n. Returns the proof (canonical) and per-round device times.
