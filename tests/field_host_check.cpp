@@ -30,6 +30,17 @@ int main() {
     uint32_t x = g() % P, xm = to_mont(x);
     for (int i = 0; i < 24; i++) if (p2_diag_mul<24>(i, xm) != mul(xm, p2_diag<24>(i))) b4++;
   }
+  // x * 2^-k at the ends of the range and with all low bits set
+  for (int k = 1; k <= 24; k++) {
+    const uint32_t inv = detail::cm_inv2(k, false);
+    const uint32_t lowk = (1u << k) - 1;
+    const uint32_t edge[] = {0u, 1u, P - 1, P - 2, lowk, P - 1 - lowk, (P - 1) & ~lowk, ((P - 1) & ~lowk) - 1};
+    for (uint32_t x : edge) if (mul_inv_pow2(x, k) != mul(x, inv)) b4++;
+    for (int it = 0; it < 20000; it++) {
+      const uint32_t x = g() % P;
+      if (mul_inv_pow2(x, k) != mul(x, inv)) b4++;
+    }
+  }
   // cube (lazy inner square), the lazily reduced sums and whole permutations against plain
   // modular arithmetic
   long b7 = 0, b8 = 0;

@@ -103,23 +103,130 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Thread (x, z): the up columns are extended from their values at j * 2^(n-k) + x, j < 2^k,
-// to the point z by the Lagrange weights L_j(z); the batched constraint over those values is
+// The batched constraint sum_i alpha_i C_i is rewritten as
+//   sum_i gamma_i cube(u_i) - sum_i alpha_i col_(17+i),
+// since constraint i is (a linear map of an S-box layer) minus its committed column 17 + i:
+// the full rounds' linear map moves onto the weights (gamma = MDS^T alpha, the host's betas)
+// and the partial rounds' weight is alpha itself. Each cube input u_i is an affine function
+// of the row: a committed column plus a round constant (the inputs of beginning and ending
+// rounds 1..3), or, for the 52 others, MDS of the inputs (beginning round 0), the partial
+// chain's state word 0 (the 20 partial rounds) and the state after the chain (ending round
+// 0). The extension to a point z is linear and keeps constants (the Lagrange weights sum to
+// one), so k_zc0_rows computes those 52 inputs once per row, and the committed-column term,
+// which is linear, once per row as well (weighted by L_j(z) after its sum over x); per
+// point z only the 148 cube inputs are extended, cubed and weighted.
+
+// Source of cube input i: computed input q[qcol] (round constant included), or committed
+// column 1 + i (qcol < 0) plus the round constant zc0_rc.
+__device__ __forceinline__ int zc0_qcol(int i) {
+  if (i < 16) return i;             // beginning round 0
+  if (i < 64) return -1;            // beginning rounds 1..3: columns 17..64
+  if (i < 100) return i - 48;       // partial rounds (q 16..35), ending round 0 (q 36..51)
+  return -1;                        // ending rounds 1..3: columns 101..148
+}
+__device__ __forceinline__ uint32_t zc0_rc(const AirConsts& K, int i) {
+  if (i >= 16 && i < 64) return K.begin[(i - 16) / 16 + 1][i & 15];
+  if (i >= 100) return K.end[(i - 100) / 16 + 1][(i - 100) & 15];
+  return 0u;
+}
+
+// One thread per row r = j S + x, reading the row's up row. Writes q[c * N + r]:
+//   c < 16       MDS(inputs)_c + rc_begin[0][c]
+//   16 <= c < 36 state word 0 before partial round c - 16, plus its round constant
+//   36 <= c < 52 state after the 20 partial rounds, plus rc_end[0]
+// and the committed-column term -L_j(z) sum_r eq[x] sum_i alpha_i col_(17+i) of the block's
+// rows as partial[blockIdx.x * nz + z].
+constexpr int ZC0R_THREADS = 256;
+__global__ void __launch_bounds__(ZC0R_THREADS) k_zc0_rows(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                           int nz, const uint32_t* __restrict__ lw,
+                                                           const ef* __restrict__ eq,
+                                                           const ef* __restrict__ alphas_g,
+                                                           const __grid_constant__ AirConsts K,
+                                                           uint32_t* __restrict__ q, ef* __restrict__ partial) {
+  __shared__ ef alphas[AIR_NC];
+  __shared__ ef scratch[32];
+  __shared__ ef total;
+  for (int i = threadIdx.x; i < AIR_NC; i += blockDim.x) alphas[i] = alphas_g[i];
+  __syncthreads();
+  const int lS = log_n - k;
+  const size_t N = size_t(1) << log_n;
+  const size_t rb = size_t(blockIdx.x) * ZC0R_THREADS;
+  const size_t r = rb + threadIdx.x;
+  ef c = ef_zero();
+  if (r < N) {
+    const uint32_t* row = wit + up_row(r, N);
+    EfMacF m;
+    m.init();
+#pragma unroll 1
+    for (int i = 0; i < AIR_NC; i += 4) {
+      uint32_t v[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) v[e] = __ldg(row + size_t(17 + i + e) * N);
+#pragma unroll
+      for (int e = 0; e < 4; e++) m.mac(alphas[i + e], v[e]);
+      m.flush();
+    }
+    uint32_t s[16];
+#pragma unroll
+    for (int t = 0; t < 16; t++) s[t] = __ldg(row + size_t(1 + t) * N);
+    mds_light<16>(s);
+    uint32_t* qr = q + r;
+#pragma unroll
+    for (int t = 0; t < 16; t++) qr[size_t(t) * N] = add(s[t], K.begin[0][t]);
+#pragma unroll
+    for (int t = 0; t < 16; t++) s[t] = __ldg(row + size_t(65 + t) * N);
+#pragma unroll 1
+    for (int pr = 0; pr < 20; pr++) {
+      qr[size_t(16 + pr) * N] = add(s[0], K.partial[pr]);
+      internal_layer_with0<16>(s, __ldg(row + size_t(81 + pr) * N));
+    }
+#pragma unroll
+    for (int t = 0; t < 16; t++) qr[size_t(36 + t) * N] = add(s[t], K.end[0][t]);
+    c = ef_mul(m.value(), eq[r & ((size_t(1) << lS) - 1)]);
+  }
+  const size_t last = (rb + ZC0R_THREADS <= N ? rb + ZC0R_THREADS : N) - 1;
+  const int nsk = 1 << k;
+  if ((rb >> lS) == (last >> lS)) {  // one skip index j in the block: reduce, then weight
+    const ef tot = block_reduce_ef(c, scratch);
+    if (threadIdx.x == 0) total = tot;
+    __syncthreads();
+    const int j = int(rb >> lS);
+    for (int z = threadIdx.x; z < nz; z += blockDim.x)
+      partial[size_t(blockIdx.x) * nz + z] = ef_sub(ef_zero(), ef_mul_f(total, lw[size_t(z) * nsk + j]));
+  } else {  // small tables: weight per row, reduce per point
+    const int j = r < N ? int(r >> lS) : 0;
+    for (int z = 0; z < nz; z++) {
+      const ef v = block_reduce_ef(ef_mul_f(c, lw[size_t(z) * nsk + j]), scratch);
+      if (threadIdx.x == 0) partial[size_t(blockIdx.x) * nz + z] = ef_sub(ef_zero(), v);
+    }
+  }
+}
+
+// Thread (x, z): the 148 cube inputs are extended from their values at rows j S + x, j < 2^k,
+// to the point z by the Lagrange weights L_j(z), cubed and weighted by gamma; the sum is
 // weighted by eq[x]. A warp holds 32 consecutive x for one z. The 2^k x 32 values of each
-// column are staged in shared memory by a cp.async pipeline, ZC0_GROUP columns per stage (the
-// constraint reads columns 1..164 in increasing order, each exactly once, so one block
-// barrier per group suffices), and the extension reads shared memory only.
-__global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* __restrict__ wit, int log_n, int k,
+// input are staged in shared memory by a cp.async pipeline, ZC0_GROUP inputs per stage (one
+// block barrier per group), and the extension reads shared memory only. Every thread stages
+// the same (j, x) entries of every input, so their offsets are formed once; the weights of
+// j >= 2^k are zero, so the extension always takes 16 products (the unstaged entries are
+// multiplied by zero).
+__global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* __restrict__ wit,
+                                                               const uint32_t* __restrict__ q, int log_n, int k,
                                                                int nz, const uint32_t* __restrict__ lw,
                                                                const ef* __restrict__ eq,
                                                                const ef* __restrict__ alphas_g,
+                                                               const ef* __restrict__ betas_g,
                                                                const __grid_constant__ AirConsts K,
                                                                ef* __restrict__ partial) {
-  __shared__ ef alphas[AIR_NC];
+  __shared__ ef gam[AIR_NC];
+  __shared__ uint32_t rcs[AIR_NC];
   __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_GROUP][ZC0_X * ZC0_PAD];
   const int tid = threadIdx.y * ZC0_X + threadIdx.x;
   constexpr int NT = ZC0_X * ZC0_Z;
-  for (int i = tid; i < AIR_NC; i += NT) alphas[i] = alphas_g[i];
+  for (int i = tid; i < AIR_NC; i += NT) {
+    gam[i] = i < 64 ? betas_g[i] : (i < 84 ? alphas_g[i] : betas_g[i - 20]);
+    rcs[i] = zc0_rc(K, i);
+  }
   const int zi = blockIdx.y * ZC0_Z + threadIdx.y;
   const int nsk = 1 << k;
   const size_t N = size_t(1) << log_n;
@@ -130,58 +237,70 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 1) k_zc0_eval(const uint32_t* _
 #pragma unroll
   for (int j = 0; j < 16; j++) w[j] = (zi < nz && j < nsk) ? lw[zi * nsk + j] : 0u;
 
-  // producer: group g (columns 1 + G g ..) -> its slot, tile[slot][cc][xl * PAD + j] =
-  // up_c[j * S + x0 + xl] for c = 1 + G g + cc
+  // staged entries of this thread: e = tid, tid + NT of the 16 x 32 (j, x) grid; source row
+  // j S + x (the up row for committed columns differs only at row N - 1)
+  constexpr int NE = (16 * ZC0_X + NT - 1) / NT;
+  uint32_t srow[NE], sdst[NE];
+  bool sval[NE], slast[NE];
+#pragma unroll
+  for (int e = 0; e < NE; e++) {
+    const int idx = tid + e * NT;
+    const int j = idx / ZC0_X, xl = idx % ZC0_X;
+    size_t xx = x0 + xl;
+    if (xx >= S) xx = 0;
+    sval[e] = idx < 16 * ZC0_X && j < nsk;
+    srow[e] = uint32_t(size_t(j) * S + xx);
+    slast[e] = size_t(j) * S + xx == N - 1;
+    sdst[e] = uint32_t(xl * ZC0_PAD + j);
+  }
   auto issue = [&](int g) {
+#pragma unroll
     for (int cc = 0; cc < ZC0_GROUP; cc++) {
-      const int c = 1 + ZC0_GROUP * g + cc;
-      if (c >= AIR_W) break;
-      uint32_t* dst = tile[g % ZC0_STAGES][cc];
-      const uint32_t* col = wit + size_t(c) * N;
-      for (int idx = tid; idx < 16 * ZC0_X; idx += NT) {
-        const int j = idx / ZC0_X, xl = idx % ZC0_X;
-        if (j < nsk) {
-          size_t xx = x0 + xl;
-          if (xx >= S) xx = 0;
-          cp_async4(dst + xl * ZC0_PAD + j, col + up_row(size_t(j) * S + xx, N));
-        }
+      const int i = ZC0_GROUP * g + cc;
+      if (i < AIR_NC) {
+        const int qc = zc0_qcol(i);
+        const uint32_t* col = qc >= 0 ? q + size_t(qc) * N : wit + size_t(1 + i) * N;
+        uint32_t* dst = tile[g % ZC0_STAGES][cc];
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+          if (sval[e]) cp_async4(dst + sdst[e], col + (srow[e] - uint32_t(slast[e] && qc < 0)));
       }
     }
     cp_async_commit();
   };
   for (int g = 0; g < ZC0_STAGES - 1; g++) issue(g);
-  int next = ZC0_STAGES - 1;  // next group to prefetch
-  auto get = [&](int c) -> uint32_t {
-    const int g = (c - 1) / ZC0_GROUP, cc = (c - 1) % ZC0_GROUP;
-    if (cc == 0) {
-      cp_async_wait<ZC0_STAGES - 2>();
-      __syncthreads();
-      issue(next++);
-    }
-    const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
-    // two chains of (up to) 8 products, folded with 2^32 = 2^25 - 2 (mod p) after every 4
-    // (a folded sum stays below 2^57 + 2^32, so 4 more products fit in 64 bits), then one
-    // Montgomery reduction of their sum (below 2^59 < 4 p^2)
-    uint64_t sa = 0, sb = 0;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      if (4 * q < nsk) {
-        const uint4 v = row[q];
-        uint64_t& acc = (q & 1) ? sb : sa;
-        acc += wmul(w[4 * q], v.x);
-        acc += wmul(w[4 * q + 1], v.y);
-        acc += wmul(w[4 * q + 2], v.z);
-        acc += wmul(w[4 * q + 3], v.w);
-        acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
-      }
-    }
-    return redc(sa + sb);
-  };
-  __syncthreads();  // alphas
   EfMacF m;
   m.init();
-  air_eval_f(
-      K, get, [&](uint32_t h, int i) { m.mac(alphas[i], h); }, [&]() { m.flush(); });
+  constexpr int NG = AIR_NC / ZC0_GROUP;
+  static_assert(NG * ZC0_GROUP == AIR_NC, "whole groups");
+#pragma unroll 1
+  for (int g = 0; g < NG; g++) {
+    cp_async_wait<ZC0_STAGES - 2>();
+    __syncthreads();  // group g landed for every thread; the slot of group g - 1 is free
+    issue(g + ZC0_STAGES - 1);
+#pragma unroll
+    for (int cc = 0; cc < ZC0_GROUP; cc++) {
+      const int i = ZC0_GROUP * g + cc;
+      const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
+      // two chains of 8 products, folded with 2^32 = 2^25 - 2 (mod p) after every 4 (below
+      // 2^57 + 2^32 each); the round constant enters the high word (rc 2^32 reduces to rc),
+      // and one Montgomery reduction of the total (below 2^63 < 4 p^2) follows
+      uint64_t sa = 0, sb = 0;
+#pragma unroll
+      for (int qq = 0; qq < 4; qq++) {
+        const uint4 v = row[qq];
+        uint64_t& acc = (qq & 1) ? sb : sa;
+        acc += wmul(w[4 * qq], v.x);
+        acc += wmul(w[4 * qq + 1], v.y);
+        acc += wmul(w[4 * qq + 2], v.z);
+        acc += wmul(w[4 * qq + 3], v.w);
+        acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
+      }
+      const uint32_t u = redc(sa + sb + (uint64_t(rcs[i]) << 32));
+      m.mac(gam[i], cube(u));
+    }
+    m.flush();
+  }
   cp_async_wait<0>();
   const bool active = zi < nz && x < S;
   ef res = active ? ef_mul(m.value(), eq[x]) : ef_zero();
@@ -809,10 +928,17 @@ int zc0_blocks(int log_n, int k) {
   size_t S = size_t(1) << (log_n - k);
   return (int)((S + ZC0_X - 1) / ZC0_X);
 }
-void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
-                     const ef* alphas, const AirConsts& K, ef* partial, cudaStream_t s) {
+int zc0_row_blocks(int log_n) { return (int)(((size_t(1) << log_n) + ZC0R_THREADS - 1) / ZC0R_THREADS); }
+void launch_zc0_rows(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
+                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, cudaStream_t s) {
+  k_zc0_rows<<<zc0_row_blocks(log_n), ZC0R_THREADS, 0, s>>>(wit, log_n, k, nz, lw, eq, alphas, K, q, partial);
+  WL_LAUNCH_CHECK();
+}
+void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, int nz, const uint32_t* lw,
+                     const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K, ef* partial,
+                     cudaStream_t s) {
   dim3 grid(zc0_blocks(log_n, k), (nz + ZC0_Z - 1) / ZC0_Z), block(ZC0_X, ZC0_Z);
-  k_zc0_eval<<<grid, block, 0, s>>>(wit, log_n, k, nz, lw, eq, alphas, K, partial);
+  k_zc0_eval<<<grid, block, 0, s>>>(wit, q, log_n, k, nz, lw, eq, alphas, betas, K, partial);
   WL_LAUNCH_CHECK();
 }
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {

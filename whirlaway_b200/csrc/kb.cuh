@@ -69,13 +69,12 @@ KB_HD uint32_t redc(uint64_t t) {
   r = hi < mh ? r + P : r;
   return umin(r, r - P);
 }
-// x * 2^-k for 1 <= k <= 31 (Montgomery form is preserved): REDC(x * 2^(32 - k)). The
-// low word of x * 2^(32 - k) times PINV is x times the constant PINV * 2^(32 - k) mod 2^32.
+// x * 2^-k for 1 <= k <= 24, x < p (linear, so Montgomery form is preserved). With
+// x = hi 2^k + lo and 2^24 | p - 1, 2^-k = -(p - 1) / 2^k (mod p), so the product is
+// hi - lo (p - 1) / 2^k, which lies in (-(p - 1), 2^(31 - k)): one low-word multiply and a
+// sign fix, no high-word product.
 KB_HD uint32_t mul_inv_pow2(uint32_t x, int k) {
-  const uint32_t hi = x >> k;
-  const uint32_t m = x * (PINV << (32 - k));
-  const uint32_t mh = umulhi(m, P);
-  const uint32_t r = hi - mh;
+  const uint32_t r = (x >> k) - (x & ((1u << k) - 1)) * ((P - 1) >> k);
   return umin(r, r + P);
 }
 KB_HD uint32_t halve(uint32_t x) { return (x & 1) ? (x >> 1) + ((P + 1) >> 1) : (x >> 1); }

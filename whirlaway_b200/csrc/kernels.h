@@ -60,12 +60,20 @@ void launch_eq_table_f(const uint32_t* points, int npts, int nvars, uint32_t* ou
 void launch_reduce_partials(const ef* partial, int nblk, int k, ef* out, cudaStream_t s);
 
 // --------------------------------------------------------------- AIR zerocheck
-// Round 0 with univariate skip over the top k variables: partial[blk * nz + z] sums, for
-// the nz points z_0.. given by their Lagrange weights lw[z * 2^k + j], the eq-weighted
-// batched constraint over the up columns.
+// Round 0 with univariate skip over the top k variables: for the nz points z_0.. given by
+// their Lagrange weights lw[z * 2^k + j], the eq-weighted batched constraint over the up
+// columns, as partial sums partial[blk * nz + z] of two kernels. launch_zc0_rows writes the
+// ZC0_NQ computed cube inputs of every row to q (ZC0_NQ * 2^log_n words) and its
+// zc0_row_blocks partial sums (the committed-column term); launch_zc0_eval reads q and writes
+// zc0_blocks partial sums (the S-box term). The point sums are the sums over both.
+constexpr int ZC0_NQ = 52;
 int zc0_blocks(int log_n, int k);
-void launch_zc0_eval(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
-                     const ef* alphas, const AirConsts& K, ef* partial, cudaStream_t s);
+int zc0_row_blocks(int log_n);
+void launch_zc0_rows(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
+                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, cudaStream_t s);
+void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, int nz, const uint32_t* lw,
+                     const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K, ef* partial,
+                     cudaStream_t s);
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
 int zc_ef_blocks(int m);
 // betas: the 8 full rounds' 16 weights beta_f = MDS^T (alpha_(c0(f)+i))_i, f = 0..7.

@@ -571,10 +571,14 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     for (int zi = 0; zi < nz; zi++)
       for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
     DBuf d_lw = upload(ctx, lw);
-    const int nb = zc0_blocks(n, k);
-    ef* part = ctx.partials(size_t(nb) * nz);
-    { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, part, st); }
-    std::vector<ef> sums = reduce_to_host(ctx, part, nb, nz);
+    const int nb = zc0_blocks(n, k), nbr = zc0_row_blocks(n);
+    ef* part = ctx.partials(size_t(nb + nbr) * nz);
+    {
+      DBuf q(sizeof(uint32_t) * ZC0_NQ * N, st);
+      { ProfScope _ps(ctx, "zc0_rows"); launch_zc0_rows(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, q.as<uint32_t>(), part + size_t(nb) * nz, st); }
+      { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, q.as<uint32_t>(), n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+    }
+    std::vector<ef> sums = reduce_to_host(ctx, part, nb + nbr, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
     std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
