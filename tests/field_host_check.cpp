@@ -1,6 +1,7 @@
 // Host-side check of the product's field arithmetic (whirlaway_b200/csrc/kb.cuh and
 // poseidon2.cuh compile for the host too): Montgomery products, lazy reductions, the
-// unsigned-min additions and the shortcut multiplications of the Poseidon2 internal layer,
+// unsigned-min additions, the shortcut multiplications of the Poseidon2 internal layer and the
+// canonical-domain S-box with fp64 quotients,
 // each against a plain modular reference. Built and run by tests/test_boundary.py.
 #include <cstdio>
 #include <random>
@@ -58,6 +59,16 @@ int main() {
     uint32_t x = g() % P;
     if (from_mont(cube(to_mont(x))) != pm(pm(x, x), x)) b7++;
   }
+  // canonical-domain S-box with fp64 quotients, on unreduced inputs below 2p
+  {
+    const uint32_t edge[] = {0u, 1u, 2u, P - 2, P - 1, P, P + 1, 2 * P - 2, 2 * P - 1, 46341u, 65535u, 65536u,
+                             1u << 30, (1u << 31) - 1, 1u << 31, 0xfe000000u, 0xfe000001u};
+    for (uint32_t u : edge) if (cube_fq(u) != pm(pm(u % P, u % P), u % P)) b7++;
+    for (int it = 0; it < 2000000; it++) {
+      const uint32_t u = uint32_t(g() % (2ull * P));
+      if (cube_fq(u) != pm(pm(u % P, u % P), u % P)) b7++;
+    }
+  }
   for (int w = 0; w < 2; w++) {
     const int W = w ? 24 : 16, RP = w ? 23 : 20;
     for (int it = 0; it < 300; it++) {
@@ -105,6 +116,10 @@ int main() {
         for (int i = 0; i < W; i++) r[i] = cub(uint32_t((uint64_t(r[i]) + from_mont(et[rd * W + i])) % P));
         mds(r);
       }
+      uint32_t sc[24];  // the canonical-domain permutation of the Merkle hashes
+      for (int i = 0; i < W; i++) sc[i] = s[i];
+      if (w) p2_permute_fq<24>(sc, p2_consts_canonical(c24)); else p2_permute_fq<16>(sc, p2_consts_canonical(c16));
+      for (int i = 0; i < W; i++) if (sc[i] != r[i]) { b8++; break; }
       for (int i = 0; i < W; i++) s[i] = to_mont(s[i]);
       uint32_t sv[16];
       for (int i = 0; i < 16; i++) sv[i] = s[i];

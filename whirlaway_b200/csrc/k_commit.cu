@@ -238,6 +238,10 @@ __device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ lde, int
   }
 }
 
+// The tree holds canonical digests: the permutations run in the canonical domain (see
+// p2_permute_fq), the absorbed LDE entries are converted from Montgomery form, and the host
+// converts the root and the opened digests back.
+//
 // Leaf digests (level 0 of the tree), one row per thread. Each thread hashes one row of 128 entries with the width-24 sponge (16 entries per
 // absorption), after the Moebius transform over the position bits [log_elem, 7) of the
 // column index: entry j becomes sum over i <= j (bitwise on those bits, equal elsewhere)
@@ -278,7 +282,9 @@ __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restr
         for (int i = 0; i < 16; i++)
           if (!(i & h)) st[i + h] = kb::sub(st[i + h], st[i]);
       }
-      kb::p2_permute<24>(st, c);
+#pragma unroll
+      for (int i = 0; i < 16; i++) st[i] = kb::from_mont(st[i]);
+      kb::p2_permute_fq<24>(st, c);
     }
     uint4* o = reinterpret_cast<uint4*>(tree + (row0 + t) * 8);
     o[0] = make_uint4(st[0], st[1], st[2], st[3]);
@@ -297,13 +303,15 @@ __global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const
     const uint4 u = src[q];
     st[4 * q] = u.x, st[4 * q + 1] = u.y, st[4 * q + 2] = u.z, st[4 * q + 3] = u.w;
   }
-  kb::p2_permute<16>(st, c);
+  kb::p2_permute_fq<16>(st, c);
   uint4* o = reinterpret_cast<uint4*>(tree + (tree_off(LL, l) + m) * 8);
   o[0] = make_uint4(st[0], st[1], st[2], st[3]);
   o[1] = make_uint4(st[4], st[5], st[6], st[7]);
 }
 
-// Poseidon2-16 with the state spread over the 16 lanes of a half-warp (lane i holds word i),
+// Poseidon2-16 (canonical domain, canonical constants; the internal diagonal is applied by
+// Montgomery products with its Montgomery form, which is the same linear map) with the state
+// spread over the 16 lanes of a half-warp (lane i holds word i),
 // for the narrow top of a Merkle tree where one thread per permutation leaves the device
 // idle and a single permutation's latency is the cost. Every lane of the warp calls it.
 // External layer: lane i's M4 row is 2 x_i + 3 x_(i+1) + x_(i+2) + x_(i+3) within its chunk
@@ -324,17 +332,17 @@ __device__ uint32_t p2_permute16_lanes(uint32_t v, const kb::P16Consts& c) {
   const uint32_t dg = kb::p2_diag<16>(i);
   v = mds16_lanes(v, i);
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube(kb::add(v, c.ext_init[r * 16 + i])), i);
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + c.ext_init[r * 16 + i]), i);
 #pragma unroll 1
   for (int r = 0; r < 20; r++) {
-    if (i == 0) v = kb::cube(kb::add(v, c.internal[r]));
+    if (i == 0) v = kb::cube_fq(v + c.internal[r]);
     uint32_t sum = v;
 #pragma unroll
     for (int d = 8; d > 0; d >>= 1) sum = kb::add(sum, __shfl_xor_sync(0xffffffffu, sum, d, 16));
     v = kb::add(kb::mul(v, dg), sum);
   }
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube(kb::add(v, c.ext_term[r * 16 + i])), i);
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + c.ext_term[r * 16 + i]), i);
   return v;
 }
 
@@ -475,7 +483,9 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s) {
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
-  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24,
+  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
+  const kb::P16Consts p16c = kb::p2_consts_canonical(p16);
+  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24c,
                                                                                      tree);
   WL_LAUNCH_CHECK();
   // Wide levels: one launch each, one compression per thread. Narrower levels: 16 lanes per
@@ -483,18 +493,18 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
   int l0 = 0;
   while (l0 < LL && LL - l0 - 1 >= FLAT_LEVEL_MIN_LOG) {
     const size_t cnt = size_t(1) << (LL - l0 - 1);
-    k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16);
+    k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16c);
     WL_LAUNCH_CHECK();
     l0++;
   }
   while (l0 < LL && LL - l0 > TOP_LEVELS) {
     const size_t threads = size_t(16) << (LL - l0 - 1);
-    k_merkle_level_lanes<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(tree, LL, l0 + 1, p16);
+    k_merkle_level_lanes<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(tree, LL, l0 + 1, p16c);
     WL_LAUNCH_CHECK();
     l0++;
   }
   if (l0 < LL) {
-    k_merkle_top<<<1, 1024, 0, s>>>(tree, LL, l0, p16);
+    k_merkle_top<<<1, 1024, 0, s>>>(tree, LL, l0, p16c);
     WL_LAUNCH_CHECK();
   }
 }

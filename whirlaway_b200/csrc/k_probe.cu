@@ -1,6 +1,7 @@
 // Throughput probes: the integer-pipe ceilings the kernels are measured against. Both run
 // from registers only (no memory traffic besides one store per thread): independent chains
-// of Montgomery products, and back-to-back Poseidon2-24 permutations.
+// of Montgomery products, and back-to-back Poseidon2-24 permutations (the canonical-domain
+// form the Merkle leaves use).
 #include "prover.h"
 
 namespace wl {
@@ -31,7 +32,7 @@ __global__ void k_probe_p24(const __grid_constant__ kb::P24Consts c, int iters, 
   uint32_t s[24];
 #pragma unroll
   for (int i = 0; i < 24; i++) s[i] = (tid * 24u + i) % kb::P;
-  for (int it = 0; it < iters; it++) kb::p2_permute<24>(s, c);
+  for (int it = 0; it < iters; it++) kb::p2_permute_fq<24>(s, c);
   uint32_t x = 0;
 #pragma unroll
   for (int i = 0; i < 24; i++) x ^= s[i];
@@ -77,8 +78,9 @@ double bench_modmul_per_s(Context& ctx) {
 double bench_p24_per_s(Context& ctx, const kb::P24Consts& c) {
   const int blocks = sm_count(ctx.device) * 8, threads = 128, iters = 32;
   DBuf out(sizeof(uint32_t) * blocks * threads, ctx.stream);
+  const kb::P24Consts cc = kb::p2_consts_canonical(c);
   double ms = time_best(ctx, [&] {
-    k_probe_p24<<<blocks, threads, 0, ctx.stream>>>(c, iters, out.as<uint32_t>());
+    k_probe_p24<<<blocks, threads, 0, ctx.stream>>>(cc, iters, out.as<uint32_t>());
     WL_LAUNCH_CHECK();
   }, 5);
   return double(blocks) * threads * iters / (ms * 1e-3);

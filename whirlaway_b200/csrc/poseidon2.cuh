@@ -8,6 +8,9 @@
 // Round constants are runtime data (drawn from the workload's StdRng stream) and are
 // kept in Montgomery form.
 #pragma once
+#include <cmath>
+#include <cstring>
+
 #include "kb.cuh"
 
 namespace kb {
@@ -237,6 +240,81 @@ KB_HD void p2_permute(uint32_t* s, const P2Consts<W>& c) {
     for (int i = 0; i < W; i++) s[i] = cube(add(s[i], c.ext_term[r * W + i]));
     mds_light<W>(s);
   }
+}
+
+// ---------------------------------------------------------------- canonical-domain S-box
+// The Merkle hashes run in the canonical (non-Montgomery) domain with an S-box whose two
+// products take their quotients by p from the fp64 pipe, which the integer kernels leave
+// idle, instead of two Montgomery reductions (four high-word integer products) on the
+// integer multiply pipe. For a product t = a b with |a|, |b| < 2^32 and |t| < 2^64, the
+// fp64 product fl(a b) is within 2^11 of t and fl(1/p) within 2^-84 of 1/p, so
+// fl(a b) fl(1/p) is within 2^-19 of t / p; one fused multiply-add that also adds
+// 1.5 * 2^52 rounds it to an integer held in the low mantissa bits: q = floor(t / p) or one
+// more. t - q p, formed exactly in 32-bit arithmetic (only its low word is needed), lies in
+// [-p, p). The linear layers are the same in either domain.
+constexpr double FQ_INV_P = 1.0 / 2130706433.0;
+constexpr double FQ_ROUND = 6755399441055744.0;  // 1.5 * 2^52
+
+// u as an fp64 value (exact).
+KB_HD double fq_from_u32(uint32_t u) {
+#ifdef __CUDA_ARCH__
+  return __hiloint2double(0x43300000, int(u)) - 4503599627370496.0;  // (2^52 + u) - 2^52
+#else
+  return double(u);
+#endif
+}
+// r read as a signed 32-bit value, as an fp64 value (exact).
+KB_HD double fq_from_i32(uint32_t r) {
+#ifdef __CUDA_ARCH__
+  return __hiloint2double(0x43300000, int(r ^ 0x80000000u)) - 4503601774854144.0;  // - (2^52 + 2^31)
+#else
+  return double(int32_t(r));
+#endif
+}
+// Low word of the rounded quotient prod / p (|prod / p| < 2^51).
+KB_HD uint32_t fq_quot(double prod) {
+#ifdef __CUDA_ARCH__
+  return uint32_t(__double2loint(fma(prod, FQ_INV_P, FQ_ROUND)));
+#else
+  const double y = std::fma(prod, FQ_INV_P, FQ_ROUND);
+  uint64_t bits;
+  std::memcpy(&bits, &y, sizeof bits);
+  return uint32_t(bits);
+#endif
+}
+// u^3 mod p for u < 2p (an unreduced sum of two canonical values), canonical.
+KB_HD uint32_t cube_fq(uint32_t u) {
+  const double du = fq_from_u32(u);
+  const uint32_t r = u * u - fq_quot(du * du) * P;               // u^2 mod p, in [-p, p)
+  const uint32_t r3 = r * u - fq_quot(fq_from_i32(r) * du) * P;  // |r u| < 2 p^2
+  return umin(r3, r3 + P);
+}
+
+// The permutation on canonical values with canonical round constants (p2_consts_canonical).
+template <int W>
+KB_HD void p2_permute_fq(uint32_t* s, const P2Consts<W>& c) {
+  mds_light<W>(s);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) s[i] = cube_fq(s[i] + c.ext_init[r * W + i]);
+    mds_light<W>(s);
+  }
+#pragma unroll 1
+  for (int r = 0; r < P2Consts<W>::RP; r++) internal_layer_with0<W>(s, cube_fq(s[0] + c.internal[r]));
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) s[i] = cube_fq(s[i] + c.ext_term[r * W + i]);
+    mds_light<W>(s);
+  }
+}
+template <int W>
+inline P2Consts<W> p2_consts_canonical(const P2Consts<W>& m) {
+  P2Consts<W> c;
+  for (int i = 0; i < 4 * W; i++) c.ext_init[i] = from_mont(m.ext_init[i]), c.ext_term[i] = from_mont(m.ext_term[i]);
+  for (int i = 0; i < P2Consts<W>::RP; i++) c.internal[i] = from_mont(m.internal[i]);
+  return c;
 }
 
 // Extension-field versions of the linear layers (constraint evaluation over EF).

@@ -272,6 +272,7 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   uint32_t* t = c.tree.as<uint32_t>();
   { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_tree(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, p16, t, LL, ctx.stream); }
   ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
+  for (uint32_t& w : c.root) w = kb::to_mont(w);  // the tree holds canonical digests
   return c;
 }
 
@@ -300,6 +301,7 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   if (nq) {
     ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
     ctx.to_host(hd.data(), digs.as<uint32_t>(), hd.size() * 4);
+    for (uint32_t& w : hd) w = kb::to_mont(w);  // canonical digests
   }
   const int log_elem = c.elem == 8 ? 3 : 0;
   std::vector<std::vector<uint32_t>> out;
