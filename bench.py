@@ -385,6 +385,8 @@ def run_ours(args, world, rank, local):
     ctx.profile(True)
     table.prove_witness(wit)
     breakdown = ctx.profile_report()
+    host_profile = {k[5:]: round(v[0], 4) for k, v in breakdown.items() if k.startswith("host:")}
+    breakdown = {k: v for k, v in breakdown.items() if not k.startswith("host:")}
     dominant = max(breakdown.items(), key=lambda kv: kv[1][0])[0]
     sampler = ClockSampler(local)
     ctx.profile(True, only=dominant)
@@ -404,7 +406,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     launches = wl.kernel_launch_count() - launches0
     elapsed_ms = dist_max(e0.elapsed_time(e1), world)
-    profile = ctx.profile_report()
+    profile = {k: v for k, v in ctx.profile_report().items() if not k.startswith("host:")}
     ctx.profile(False)
     host_syncs = (ctx.host_syncs - syncs0) / args.steps
     host_wait = (ctx.host_wait_ms - wait0) / args.steps
@@ -465,6 +467,7 @@ def run_ours(args, world, rank, local):
         "host_wait_ms_per_step": host_wait,
         "kernel_profile_ms": {k: round(v[0], 4) for k, v in sorted(breakdown.items(), key=lambda kv: -kv[1][0])},
         "kernel_profile_source": "CUDA events per kernel class over the last warm-up proof",
+        "host_profile_ms": host_profile,
         "proof_len": int(proof.size),
         "batched": batched,
         "serving": serving,

@@ -309,6 +309,11 @@ wl_status wl_profile_enable(wl_ctx* ctx, int32_t on) {
     ctx->c->prof_flush();
     ctx->c->prof_totals.clear();
     ctx->c->profile = on != 0;
+    wl::host_clock() = wl::HostClock{};
+    wl::host_clock().on = on != 0;
+    ctx->c->prof_t0_ms = wl::host_now_ms();
+    ctx->c->prof_wait0_ms = ctx->c->host_wait_ms;
+    ctx->c->prof_syncs0 = ctx->c->host_syncs;
     return WL_OK;
   });
 }
@@ -349,6 +354,19 @@ wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
       if (!first) js += ", ";
       first = false;
       js += "\"" + kv.first + "\": [" + std::to_string(kv.second.first) + ", " + std::to_string(kv.second.second) + "]";
+    }
+    const wl::HostClock& hc = wl::host_clock();
+    if (hc.on) {
+      const std::pair<const char*, std::pair<double, long>> host[] = {
+          {"host:transcript_perm", {hc.perm_ms, hc.perms}}, {"host:alloc", {hc.alloc_ms, hc.allocs}},
+          {"host:launch", {hc.launch_ms, hc.launches}}, {"host:upload", {hc.upload_ms, hc.uploads}},
+          {"host:wait", {ctx->c->host_wait_ms - ctx->c->prof_wait0_ms, long(ctx->c->host_syncs - ctx->c->prof_syncs0)}},
+          {"host:elapsed", {wl::host_now_ms() - ctx->c->prof_t0_ms, 1L}}};
+      for (auto& h : host) {
+        if (!first) js += ", ";
+        first = false;
+        js += "\"" + std::string(h.first) + "\": [" + std::to_string(h.second.first) + ", " + std::to_string(h.second.second) + "]";
+      }
     }
     js += "}";
     if (js.size() + 1 > cap) return fail(ctx, WL_E_BUFFER_TOO_SMALL, "profile buffer too small");

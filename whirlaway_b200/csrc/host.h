@@ -5,6 +5,7 @@
 // are Montgomery form unless a name says otherwise.
 #pragma once
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <stdexcept>
 #include <vector>
@@ -28,6 +29,22 @@ struct Settings {
   int whir_pow_bits = 16;
 };
 
+// ------------------------------------------------------------------ host time accounting
+// Per-thread totals of the host work between device waits (profiling diagnostics: only
+// counted while the thread's context profiles).
+struct HostClock {
+  bool on = false;
+  double perm_ms = 0, alloc_ms = 0, launch_ms = 0, upload_ms = 0;
+  long perms = 0, allocs = 0, launches = 0, uploads = 0;
+};
+inline HostClock& host_clock() {
+  thread_local HostClock c;
+  return c;
+}
+inline double host_now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // ------------------------------------------------------------------ transcript
 // DuplexChallenger<F, Poseidon16, 16, 8>: observations overwrite the rate part of the
 // sponge once eight are buffered; samples pop from the end of the last squeeze.
@@ -44,7 +61,10 @@ struct HostChallenger {
   void duplex() {
     for (int i = 0; i < in_len; i++) state[i] = in[i];
     in_len = 0;
+    HostClock& hc = host_clock();
+    const double t0 = hc.on ? host_now_ms() : 0;
     host_p16_permute(state, *perm);
+    if (hc.on) hc.perm_ms += host_now_ms() - t0, hc.perms++;
     for (int i = 0; i < 8; i++) out[i] = state[i];
     out_len = 8;
   }

@@ -7,26 +7,104 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <map>
+#include <mutex>
 
 #include "prover.h"
 
 namespace wl {
 
 // ------------------------------------------------------------------ memory
+// Per-stream cache of freed device buffers, reused for requests of exactly the same size on
+// the same stream (stream order makes the reuse safe). Proofs of one size request the same
+// buffers every time; without the cache, some of those requests made the stream-ordered
+// allocator map new memory, at 0.3-100 ms of host time per request while the device idled.
+// Bounded per stream: the oldest entries are freed beyond the limit.
+namespace {
+struct StreamCache {
+  size_t limit = 0, bytes = 0;
+  std::deque<std::pair<size_t, void*>> entries;  // oldest first
+};
+std::mutex g_cache_mu;
+std::map<cudaStream_t, StreamCache> g_caches;
+
+bool cache_take(cudaStream_t s, size_t bytes, void** p) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_caches.find(s);
+  if (it == g_caches.end()) return false;
+  auto& es = it->second.entries;
+  for (auto e = es.rbegin(); e != es.rend(); ++e) {
+    if (e->first == bytes) {
+      *p = e->second;
+      it->second.bytes -= bytes;
+      es.erase(std::next(e).base());
+      return true;
+    }
+  }
+  return false;
+}
+bool cache_put(cudaStream_t s, size_t bytes, void* p) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_caches.find(s);
+  if (it == g_caches.end() || bytes > it->second.limit) return false;
+  StreamCache& c = it->second;
+  c.entries.emplace_back(bytes, p);
+  c.bytes += bytes;
+  while (c.bytes > c.limit) {
+    cudaFreeAsync(c.entries.front().second, s);
+    c.bytes -= c.entries.front().first;
+    c.entries.pop_front();
+  }
+  return true;
+}
+// Frees every cached buffer of stream s (and with remove, stops caching for it).
+void cache_flush(cudaStream_t s, bool remove) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_caches.find(s);
+  if (it == g_caches.end()) return;
+  for (auto& e : it->second.entries) cudaFreeAsync(e.second, s);
+  it->second.entries.clear();
+  it->second.bytes = 0;
+  if (remove) g_caches.erase(it);
+}
+}  // namespace
+
+void stream_cache_enable(cudaStream_t s, size_t limit) {
+  cache_flush(s, false);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  g_caches[s].limit = limit;
+}
+void Context::set_cache_limit(size_t bytes) { stream_cache_enable(stream, bytes); }
+
 DBuf::DBuf(size_t bytes, cudaStream_t s) : bytes_(bytes), s_(s) {
   if (bytes) {
-    cudaError_t e = cudaMallocAsync(&p_, bytes, s);
-    if (e != cudaSuccess) {
-      p_ = nullptr;
-      bytes_ = 0;
-      cudaGetLastError();
-      throw CudaError(e, "cudaMallocAsync(" + std::to_string(bytes) + " bytes)");
+    HostClock& hc = host_clock();
+    const double t0 = hc.on ? host_now_ms() : 0;
+    if (!cache_take(s, bytes, &p_)) {
+      cudaError_t e = cudaMallocAsync(&p_, bytes, s);
+      if (e == cudaErrorMemoryAllocation) {  // cached buffers of other sizes go back to the pool first
+        cudaGetLastError();
+        cache_flush(s, false);
+        e = cudaMallocAsync(&p_, bytes, s);
+      }
+      if (e != cudaSuccess) {
+        p_ = nullptr;
+        bytes_ = 0;
+        cudaGetLastError();
+        throw CudaError(e, "cudaMallocAsync(" + std::to_string(bytes) + " bytes)");
+      }
     }
+    if (hc.on) hc.alloc_ms += host_now_ms() - t0, hc.allocs++;
   }
 }
 DBuf::~DBuf() { reset(); }
 void DBuf::reset() {
-  if (p_) cudaFreeAsync(p_, s_);
+  if (p_) {
+    HostClock& hc = host_clock();
+    const double t0 = hc.on ? host_now_ms() : 0;
+    if (!cache_put(s_, bytes_, p_)) cudaFreeAsync(p_, s_);
+    if (hc.on) hc.alloc_ms += host_now_ms() - t0;
+  }
   p_ = nullptr;
   bytes_ = 0;
 }
@@ -43,6 +121,7 @@ DBuf& DBuf::operator=(DBuf&& o) noexcept {
 }
 
 namespace {
+constexpr size_t kCacheBytes = size_t(8) << 30;  // device buffer cache per context stream
 constexpr size_t kUpBytes = 4 << 20;    // pinned upload ring
 constexpr size_t kDownBytes = 4 << 20;  // pinned download staging
 thread_local size_t g_up_off = 0;
@@ -52,6 +131,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaSetDevice(dev));
   WL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   WL_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+  stream_cache_enable(stream, kCacheBytes);
   cudaMemPool_t pool;
   WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
@@ -65,6 +145,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
 }
 Context::~Context() {
   cudaSetDevice(device);
+  cache_flush(stream, true);
   cudaStreamSynchronize(stream);
   for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : event_pool) cudaEventDestroy(e);
@@ -101,11 +182,14 @@ void Context::prof_flush() {
   pending.clear();
 }
 ProfScope::ProfScope(Context& ctx, const char* n) : c(ctx), name(n) {
+  if (host_clock().on) t_host = host_now_ms();
   if (!c.profile || (!c.profile_only.empty() && c.profile_only != n)) return;
   a = c.take_event();
   WL_CUDA(cudaEventRecord(a, c.stream));
 }
 ProfScope::~ProfScope() {
+  HostClock& hc = host_clock();
+  if (hc.on && t_host > 0) hc.launch_ms += host_now_ms() - t_host, hc.launches++;
   if (!c.profile || !a) return;
   cudaEvent_t b = nullptr;
   try {
@@ -155,6 +239,12 @@ void Context::to_host(void* dst, const void* src, size_t bytes) {
   g_up_off = 0;  // every earlier upload has completed
 }
 void Context::to_device(void* dst, const void* src, size_t bytes) {
+  HostClock& hc = host_clock();
+  const double t0 = hc.on ? host_now_ms() : 0;
+  to_device_impl(dst, src, bytes);
+  if (hc.on) hc.upload_ms += host_now_ms() - t0, hc.uploads++;
+}
+void Context::to_device_impl(void* dst, const void* src, size_t bytes) {
   if (bytes > kUpBytes) {
     WL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
     wait_stream();

@@ -51,6 +51,8 @@ struct Context {
   std::string last_error;
   uint64_t host_syncs = 0;  // stream synchronisations made by the host (diagnostics)
   double host_wait_ms = 0;  // time the host spent in them
+  double prof_t0_ms = 0, prof_wait0_ms = 0;  // host clock and host_wait_ms when profiling began
+  uint64_t prof_syncs0 = 0;
   Context(int device, uint64_t budget);
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
@@ -62,6 +64,10 @@ struct Context {
   bool spin_sync = true;
   cudaEvent_t sync_event = nullptr;
   void to_device(void* dst, const void* src, size_t bytes);
+  void to_device_impl(void* dst, const void* src, size_t bytes);
+  // Freed device buffers of `stream` are kept for reuse by later requests of the same size,
+  // up to this many bytes (8 GiB by default; 0 disables the cache).
+  void set_cache_limit(size_t bytes);
 
   // Optional per-kernel-class timing with CUDA events on `stream`.
   bool profile = false;
@@ -82,6 +88,7 @@ struct ProfScope {
   Context& c;
   const char* name;
   cudaEvent_t a = nullptr;
+  double t_host = 0;  // host time of the scope (the launches), when the thread's HostClock is on
   ProfScope(Context& ctx, const char* n);
   ~ProfScope();
 };

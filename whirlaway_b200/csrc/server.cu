@@ -30,6 +30,7 @@ Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), 
   for (int i = 0; i < workers; i++) {
     contexts_.push_back(std::make_unique<Context>(device, hbm_budget));
     contexts_.back()->spin_sync = false;  // workers block: the other workers' proofs fill the device
+    contexts_.back()->set_cache_limit(0);  // admission counts running proofs only: no cached buffers
   }
   for (int i = 0; i < workers; i++) threads_.emplace_back([this, i] { worker_main(i); });
 }
