@@ -129,6 +129,8 @@ inline std::vector<std::vector<uint32_t>> lagrange_basis(int n) {
   }
   return basis;
 }
+// The same bases, computed once per n and process.
+const std::vector<std::vector<uint32_t>>& lagrange_basis_cached(int n);
 inline std::vector<ef> interpolate(const std::vector<std::vector<uint32_t>>& basis, const std::vector<ef>& ys) {
   size_t n = ys.size();
   std::vector<ef> out(n, kb::ef_zero());

@@ -408,19 +408,54 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   return out;
 }
 
-// Coefficient-form multilinear evaluation of a (transformed) row at r (row MSB <-> r_1).
-ef fold_row(const std::vector<uint32_t>& row, int fold, int elem, const std::vector<ef>& r) {
-  std::vector<ef> v(size_t(1) << fold);
-  for (size_t p = 0; p < v.size(); p++) {
-    v[p] = kb::ef_zero();
-    for (int e = 0; e < elem; e++) v[p].c[e] = row[p * elem + e];
+}  // namespace
+
+const std::vector<std::vector<uint32_t>>& lagrange_basis_cached(int n) {
+  static std::mutex mu;
+  static std::map<int, std::vector<std::vector<uint32_t>>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(n);
+  if (it == cache.end()) it = cache.emplace(n, lagrange_basis(n)).first;
+  return it->second;
+}
+
+namespace {
+
+// Coefficient-form multilinear evaluation of a (transformed) row at r (row MSB <-> r_1):
+// folding the row by v[q] + r_i v[q + h], MSB first, gives sum_p v_p m_p with the monomial
+// m_p = prod of r_i over the set bits of p (bit fold-1-i <-> r_i). The monomials depend on r
+// only, so one table serves every query of a round.
+std::vector<ef> fold_monomials(int fold, const std::vector<ef>& r) {
+  std::vector<ef> m(size_t(1) << fold);
+  m[0] = kb::ef_one();
+  for (int b = 0; b < fold; b++) {
+    const size_t w = size_t(1) << b;
+    for (size_t p = 0; p < w; p++) m[p + w] = kb::ef_mul(m[p], r[fold - 1 - b]);
   }
-  for (int i = 0; i < fold; i++) {
-    size_t h = v.size() / 2;
-    for (size_t q = 0; q < h; q++) v[q] = kb::ef_add(v[q], kb::ef_mul(r[i], v[q + h]));
-    v.resize(h);
+  return m;
+}
+ef fold_row(const std::vector<uint32_t>& row, int elem, const std::vector<ef>& mono) {
+  if (elem != 1) {
+    ef acc = kb::ef_zero();
+    for (size_t p = 0; p < mono.size(); p++) {
+      ef v;
+      for (int e = 0; e < 8; e++) v.c[e] = e < elem ? row[p * elem + e] : 0u;
+      acc = kb::ef_add(acc, kb::ef_mul(v, mono[p]));
+    }
+    return acc;
   }
-  return v[0];
+  // base-field row: lazy sums of products, folded with 2^32 = 2^25 - 2 (mod p) after every 4
+  // (below 2^57 + 2^32, so 4 more products of values below p fit in 64 bits)
+  constexpr uint64_t C32 = (1u << 25) - 2;
+  uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (size_t p = 0; p < mono.size(); p++) {
+    for (int k = 0; k < 8; k++) acc[k] += kb::wmul(row[p], mono[p].c[k]);
+    if ((p & 3) == 3)
+      for (int k = 0; k < 8; k++) acc[k] = (acc[k] >> 32) * C32 + uint32_t(acc[k]);
+  }
+  ef r;
+  for (int k = 0; k < 8; k++) r.c[k] = kb::redc((acc[k] >> 32) * C32 + uint32_t(acc[k]));
+  return r;
 }
 
 void split_vars(int lv, int& lh, int& ll) {
@@ -648,7 +683,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   // ---------------------------------------------------------------- 3) zerocheck
   const int nsk = 1 << k;
   const auto sel = [&] {
-    auto b = lagrange_basis(nsk);
+    auto b = lagrange_basis_cached(nsk);
     return b;
   }();  // L_i on {0..2^k-1}
   const int nz = 3 * (nsk - 1) - nsk + 1;
@@ -673,7 +708,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     std::vector<ef> sums = reduce_to_host(ctx, part, nb + nbr, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
-    std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
+    std::vector<ef> p = interpolate(lagrange_basis_cached((int)ys.size()), ys);
     std::vector<ef> qv(nsk);
     for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], zc[0]);
     p = poly_mul(p, interpolate(sel, qv));
@@ -694,7 +729,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     cols = DBuf(sizeof(ef) * size_t(W) * S, st);
     { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
   }
-  const auto basis4 = lagrange_basis(4);
+  const auto basis4 = lagrange_basis_cached(4);
   // eq table of round r (over zc[1+r..]) = eq table of round r-1 with its leading variable
   // summed out; each fold below carries it along.
   DBuf eqr;
@@ -785,7 +820,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     std::vector<ef> ee = eq_table_host(eps);
     for (int j = 0; j < nsk; j++) inner_sum = kb::ef_add(inner_sum, kb::ef_mul(ee[j], sub[j]));
   }
-  const auto basis3 = lagrange_basis(3);
+  const auto basis3 = lagrange_basis_cached(3);
   std::vector<ef> inner_ch;
   for (int round = 0; round < n; round++) {
     const size_t half = N >> (round + 1);
@@ -876,12 +911,13 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       const uint32_t gen = kb::two_adic_gen_m(prev->log_leaves);
       std::vector<std::vector<uint32_t>> stir_pts;
       std::vector<ef> stir_vals;
+      const std::vector<ef> mono = fold_monomials(prev->fold, last_r);
       for (size_t t = 0; t < q.size(); t++) {
         uint32_t y = kb::pow_m(gen, q[t]);
         std::vector<uint32_t> pt(m);
         for (int b = 0; b < m; b++) { pt[b] = y; y = kb::mul(y, y); }
         stir_pts.push_back(pt);
-        stir_vals.push_back(fold_row(rows[t], prev->fold, prev->elem, last_r));
+        stir_vals.push_back(fold_row(rows[t], prev->elem, mono));
       }
       ef gm = ts.sample_ext();
       std::vector<ef> coef_ef, coef_f;
@@ -970,7 +1006,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
   const size_t S = size_t(1) << (n - k);
   std::vector<ef> r(n + 1 - k);
   for (auto& x : r) x = ts.sample_ext();
-  auto sel = lagrange_basis(nsk);
+  auto sel = lagrange_basis_cached(nsk);
   const int nz = 2 * (nsk - 1) - nsk + 1;
   ef sum = kb::ef_zero(), mmf;
   std::vector<ef> ch;
@@ -1000,7 +1036,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     std::vector<ef> sums = reduce_to_host(ctx, part, nb, nz);
     std::vector<ef> ys(nsk, kb::ef_zero());
     ys.insert(ys.end(), sums.begin(), sums.end());
-    std::vector<ef> p = interpolate(lagrange_basis((int)ys.size()), ys);
+    std::vector<ef> p = interpolate(lagrange_basis_cached((int)ys.size()), ys);
     std::vector<ef> qv(nsk);
     for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], r[0]);
     p = poly_mul(p, interpolate(sel, qv));
@@ -1022,7 +1058,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     { ProfScope _ps(ctx, "abc0_fold"); launch_abc0_fold(a, b, c, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
     tock();
   }
-  const auto basis3 = lagrange_basis(3);
+  const auto basis3 = lagrange_basis_cached(3);
   DBuf eqr;  // eq table of the current round, carried by the folds (see prove_air)
   if (n - k >= 1) {
     eqr = DBuf(sizeof(ef) * (S / 2), st);
