@@ -242,13 +242,42 @@ __device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ lde, int
 // p2_permute_fq), the absorbed LDE entries are converted from Montgomery form, and the host
 // converts the root and the opened digests back.
 //
-// Leaf digests (level 0 of the tree), one row per thread. Each thread hashes one row of 128 entries with the width-24 sponge (16 entries per
-// absorption), after the Moebius transform over the position bits [log_elem, 7) of the
-// column index: entry j becomes sum over i <= j (bitwise on those bits, equal elsewhere)
-// of (-1)^popcount(i ^ j) row[i]. Bits 4..6 select the 16-entry chunk, so chunk ch is the
-// signed sum of the chunks below it, and bits below 4 are transformed inside the chunk;
-// rows are read straight from the tile-major LDE (no shared-memory staging, so
-// occupancy is bounded by registers).
+// Absorbs chunk ch of LDE row `row` into the sponge state st (the chunk overwrites the rate
+// st[0..15]; st[16..23] is the capacity): the Moebius transform over the position bits
+// [log_elem, 7) of the column index makes entry j the sum over i <= j (bitwise on those bits,
+// equal elsewhere) of (-1)^popcount(i ^ j) row[i]. Bits 4..6 select the 16-entry chunk, so
+// chunk ch is the signed sum of the chunks below it, and bits below 4 are transformed inside
+// the chunk. Then the permutation.
+__device__ __forceinline__ void leaf_absorb(const uint32_t* __restrict__ lde, int T, size_t row, int n_cols,
+                                            int log_elem, int ch, const kb::P24Consts& c, uint32_t* st) {
+  const int cmask = log_elem <= 4 ? 7 : (7 << (log_elem - 4)) & 7;  // chunk bits in the transform
+  leaf_chunk(lde, T, row, n_cols, ch, 0, st);
+  const int m = ch & cmask;
+  if (m) {
+    // every proper subset of m, with the sign of the bits it drops
+    for (int sub = (m - 1) & m;; sub = (sub - 1) & m) {
+      const int sign = (__popc(m ^ sub) & 1) ? -1 : 1;
+      leaf_chunk(lde, T, row, n_cols, (ch & ~m) | sub, sign, st);
+      if (!sub) break;
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    if (b < log_elem) continue;
+    const int h = 1 << b;
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+      if (!(i & h)) st[i + h] = kb::sub(st[i + h], st[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) st[i] = kb::from_mont(st[i]);
+  kb::p2_permute_fq<24>(st, c);
+}
+
+// Leaf digests (level 0 of the tree), one row per thread: each thread hashes one row of 128
+// entries with the width-24 sponge (16 entries per absorption, 8 absorptions). Rows are read
+// straight from the tile-major LDE (no shared-memory staging, so occupancy is bounded by
+// registers).
 __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, int T, int n_cols,
                                                          int log_elem, const __grid_constant__ kb::P24Consts c,
                                                          uint32_t* __restrict__ tree) {
@@ -259,36 +288,42 @@ __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restr
   uint32_t st[24];
   if (t < nrows) {
     const size_t row = row0 + t;
-    const int cmask = log_elem <= 4 ? 7 : (7 << (log_elem - 4)) & 7;  // chunk bits in the transform
 #pragma unroll
     for (int i = 0; i < 24; i++) st[i] = 0;
 #pragma unroll 1
-    for (int ch = 0; ch < 8; ch++) {
-      leaf_chunk(lde, T, row, n_cols, ch, 0, st);
-      const int m = ch & cmask;
-      if (m) {
-        // every proper subset of m, with the sign of the bits it drops
-        for (int sub = (m - 1) & m;; sub = (sub - 1) & m) {
-          const int sign = (__popc(m ^ sub) & 1) ? -1 : 1;
-          leaf_chunk(lde, T, row, n_cols, (ch & ~m) | sub, sign, st);
-          if (!sub) break;
-        }
-      }
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        if (b < log_elem) continue;
-        const int h = 1 << b;
-#pragma unroll
-        for (int i = 0; i < 16; i++)
-          if (!(i & h)) st[i + h] = kb::sub(st[i + h], st[i]);
-      }
-#pragma unroll
-      for (int i = 0; i < 16; i++) st[i] = kb::from_mont(st[i]);
-      kb::p2_permute_fq<24>(st, c);
-    }
+    for (int ch = 0; ch < 8; ch++) leaf_absorb(lde, T, row, n_cols, log_elem, ch, c, st);
     uint4* o = reinterpret_cast<uint4*>(tree + (row0 + t) * 8);
     o[0] = make_uint4(st[0], st[1], st[2], st[3]);
     o[1] = make_uint4(st[4], st[5], st[6], st[7]);
+  }
+}
+
+// One absorption (chunk ch) for every row, the capacity carried between launches in cap
+// (8 words per row): the sponge of k_leaf_hash split by chunk, so that chunk ch can be hashed
+// as soon as the LDE tiles it reads exist. The last chunk writes the digests.
+__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_absorb(const uint32_t* __restrict__ lde, int T, int n_cols,
+                                                           int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                           int ch, uint32_t* __restrict__ cap,
+                                                           uint32_t* __restrict__ tree) {
+  const size_t row = size_t(blockIdx.x) * LEAF_ROWS + threadIdx.x;
+  if (row >= (size_t(1) << T)) return;
+  uint32_t st[24];
+  if (ch == 0) {
+#pragma unroll
+    for (int i = 16; i < 24; i++) st[i] = 0;
+  } else {
+    const uint4* in = reinterpret_cast<const uint4*>(cap + row * 8);
+    const uint4 a = in[0], b = in[1];
+    st[16] = a.x, st[17] = a.y, st[18] = a.z, st[19] = a.w, st[20] = b.x, st[21] = b.y, st[22] = b.z, st[23] = b.w;
+  }
+  leaf_absorb(lde, T, row, n_cols, log_elem, ch, c, st);
+  uint4* o = reinterpret_cast<uint4*>(ch == 7 ? tree + row * 8 : cap + row * 8);
+  if (ch == 7) {
+    o[0] = make_uint4(st[0], st[1], st[2], st[3]);
+    o[1] = make_uint4(st[4], st[5], st[6], st[7]);
+  } else {
+    o[0] = make_uint4(st[16], st[17], st[18], st[19]);
+    o[1] = make_uint4(st[20], st[21], st[22], st[23]);
   }
 }
 
@@ -484,10 +519,25 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
   const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
-  const kb::P16Consts p16c = kb::p2_consts_canonical(p16);
   k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24c,
                                                                                      tree);
   WL_LAUNCH_CHECK();
+  launch_merkle_levels(tree, LL, p16, s);
+}
+
+void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24, int ch,
+                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s) {
+  const int log_elem = elem == 8 ? 3 : 0;
+  if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
+  if (ch < 0 || ch > 7) throw std::invalid_argument("leaf chunk out of range");
+  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
+  k_leaf_absorb<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24c,
+                                                                                       ch, cap, tree);
+  WL_LAUNCH_CHECK();
+}
+
+void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s) {
+  const kb::P16Consts p16c = kb::p2_consts_canonical(p16);
   // Wide levels: one launch each, one compression per thread. Narrower levels: 16 lanes per
   // compression. The last levels (at most 128 digests) in one block.
   int l0 = 0;

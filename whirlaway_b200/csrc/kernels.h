@@ -43,6 +43,13 @@ void launch_twiddles(uint2* tw, cudaStream_t s);
 // 2^(LL+1) - 2^(LL+1-l), LL = log2(rows)).
 void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s);
+// The same leaves one absorption at a time: chunk ch (0..7) reads LDE tiles 2ch and 2ch + 1
+// (and, through the Moebius transform, those of the chunks below it); the 8 capacity words of
+// every row are carried in cap (8 * rows words) and chunk 7 writes the digests. Then
+// launch_merkle_levels builds the compressions.
+void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24, int ch,
+                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s);
+void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s);
 // Gathers rows idx[q] of a tile-major LDE matrix (2^T rows) into out[q * n_cols + col].
 void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int n, uint32_t* out,
                             cudaStream_t s);

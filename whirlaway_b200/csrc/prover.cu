@@ -345,22 +345,31 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
   if ((src.elem << fold) != 128) throw std::invalid_argument("leaf rows must hold 128 base-field values");
   const size_t rows = size_t(1) << c.log_leaves;
   c.lde = DBuf(rows * c.n_cols * sizeof(uint32_t), ctx.stream);
-  if (tile_ready) {
-    // tile t's source columns arrive behind event t
-    for (int t = 0; t < c.n_cols / 8; t++) {
-      if (t < (int)tile_ready->size()) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[t], 0));
-      ProfScope _ps(ctx, "lde");
-      launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, t, t + 1);
-    }
-    for (size_t t = c.n_cols / 8; t < tile_ready->size(); t++) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[t], 0));
-  } else {
-    ProfScope _ps(ctx, "lde");
-    launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream);
-  }
   const int LL = c.log_leaves;
   c.tree = DBuf(((size_t(2) << LL) - 1) * 8 * sizeof(uint32_t), ctx.stream);
   uint32_t* t = c.tree.as<uint32_t>();
-  { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_tree(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, p16, t, LL, ctx.stream); }
+  if (tile_ready) {
+    // Tile t's source columns arrive behind event t. The leaf sponges run one absorption at
+    // a time: chunk ch reads LDE tiles up to 2ch + 1, so it is hashed as soon as those tiles
+    // are encoded, and the hashing overlaps the rest of the upload too.
+    DBuf cap(sizeof(uint32_t) * 8 * rows, ctx.stream);
+    const int ntiles = c.n_cols / 8;
+    int next = 0;
+    for (int ch = 0; ch < 8; ch++) {
+      for (; next < std::min(ntiles, 2 * ch + 2); next++) {
+        if (next < (int)tile_ready->size()) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[next], 0));
+        ProfScope _ps(ctx, "lde");
+        launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, next, next + 1);
+      }
+      ProfScope _ps(ctx, "merkle_tree");
+      launch_leaf_absorb(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, ch, cap.as<uint32_t>(), t, LL, ctx.stream);
+    }
+    for (size_t e = ntiles; e < tile_ready->size(); e++) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[e], 0));
+    { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_levels(t, LL, p16, ctx.stream); }
+  } else {
+    { ProfScope _ps(ctx, "lde"); launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
+    { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_tree(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, p16, t, LL, ctx.stream); }
+  }
   ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
   for (uint32_t& w : c.root) w = kb::to_mont(w);  // the tree holds canonical digests
   return c;
