@@ -131,6 +131,9 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaSetDevice(dev));
   WL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   WL_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+  int prio_lo = 0, prio_hi = 0;  // conversions first: the encoding of a tile waits for them
+  WL_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  WL_CUDA(cudaStreamCreateWithPriority(&conv_stream, cudaStreamNonBlocking, prio_hi));
   stream_cache_enable(stream, kCacheBytes);
   cudaMemPool_t pool;
   WL_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
@@ -155,6 +158,8 @@ Context::~Context() {
   cudaFreeHost(pinned);
   cudaStreamSynchronize(copy_stream);
   cudaStreamDestroy(copy_stream);
+  cudaStreamSynchronize(conv_stream);
+  cudaStreamDestroy(conv_stream);
   cudaStreamDestroy(stream);
 }
 cudaEvent_t Context::take_event() {
@@ -979,29 +984,40 @@ std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const ui
   WL_CUDA(cudaEventCreateWithFlags(&alloc_done, cudaEventDisableTiming));
   WL_CUDA(cudaEventRecord(alloc_done, ctx.stream));
   WL_CUDA(cudaStreamWaitEvent(ctx.copy_stream, alloc_done, 0));
-  std::vector<cudaEvent_t> ready;
+  // The copy stream only copies (back to back, so the copy engine never waits for a kernel);
+  // the conversion stream converts each tile to Montgomery form once its copy has landed.
+  WL_CUDA(cudaStreamWaitEvent(ctx.conv_stream, alloc_done, 0));
+  std::vector<cudaEvent_t> copied, ready;
+  auto destroy = [&] {
+    for (auto e : copied) cudaEventDestroy(e);
+    for (auto e : ready) cudaEventDestroy(e);
+    cudaEventDestroy(alloc_done);
+  };
   for (int c0 = 0; c0 < AIR_W; c0 += 16) {
     const size_t cols = std::min(16, AIR_W - c0);
     uint32_t* dst = wit.as<uint32_t>() + size_t(c0) * N;
-    cudaEvent_t e;
-    WL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    ready.push_back(e);
+    cudaEvent_t ec, er;
+    WL_CUDA(cudaEventCreateWithFlags(&ec, cudaEventDisableTiming));
+    copied.push_back(ec);
+    WL_CUDA(cudaEventCreateWithFlags(&er, cudaEventDisableTiming));
+    ready.push_back(er);
     WL_CUDA(cudaMemcpyAsync(dst, wit_host + size_t(c0) * N, sizeof(uint32_t) * cols * N, cudaMemcpyHostToDevice,
                             ctx.copy_stream));
-    launch_to_mont(dst, cols * N, ctx.copy_stream);
-    WL_CUDA(cudaEventRecord(e, ctx.copy_stream));
+    WL_CUDA(cudaEventRecord(ec, ctx.copy_stream));
+    WL_CUDA(cudaStreamWaitEvent(ctx.conv_stream, ec, 0));
+    launch_to_mont(dst, cols * N, ctx.conv_stream);
+    WL_CUDA(cudaEventRecord(er, ctx.conv_stream));
   }
   std::vector<uint32_t> proof;
   try {
     proof = prove_air(ctx, job, wit.as<uint32_t>(), tm, &ready);
   } catch (...) {
     cudaStreamSynchronize(ctx.copy_stream);
-    for (auto e : ready) cudaEventDestroy(e);
-    cudaEventDestroy(alloc_done);
+    cudaStreamSynchronize(ctx.conv_stream);
+    destroy();
     throw;
   }
-  for (auto e : ready) cudaEventDestroy(e);
-  cudaEventDestroy(alloc_done);
+  destroy();
   return proof;
 }
 

@@ -39,6 +39,7 @@ struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // host-to-device witness tiles, overlapped with the LDE
+  cudaStream_t conv_stream = nullptr;  // Montgomery conversion of the copied tiles
   uint64_t hbm_budget = 0;
   uint2* twiddles = nullptr;  // per-stage Shoup twiddles (launch_twiddles)
   void* pinned = nullptr;        // staging for small device-to-host reads
