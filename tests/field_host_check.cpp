@@ -5,6 +5,7 @@
 // each against a plain modular reference. Built and run by tests/test_boundary.py.
 #include <cstdio>
 #include <random>
+#include <type_traits>
 #include "poseidon2.cuh"
 namespace wl {
 void host_p16_permute(uint32_t* s, const kb::P16Consts& c);
@@ -68,6 +69,31 @@ int main() {
       const uint32_t u = uint32_t(g() % (2ull * P));
       if (cube_fq(u) != pm(pm(u % P, u % P), u % P)) b7++;
     }
+  }
+  // internal layer with lazily reduced words 9.. (any value below 2^32) against the canonical one
+  {
+    auto lazy_check = [&](auto wtag) {
+      constexpr int W = decltype(wtag)::value;
+      for (int it = 0; it < 200000; it++) {
+        uint32_t s[W], r[W];
+        const uint32_t x0 = (it % 7 == 0) ? P - 1 : uint32_t(g() % P);
+        for (int i = 0; i < W; i++) {
+          if (i < 9) s[i] = (it % 5 == 0) ? P - 1 - uint32_t(g() % 3) : uint32_t(g() % P);
+          else s[i] = (it % 3 == 0) ? 0xffffffffu - uint32_t(g() % 5) : uint32_t(g());
+          r[i] = s[i] % P;
+        }
+        internal_layer_lazy_with0<W>(s, x0);
+        internal_layer_with0<W>(r, x0);
+        for (int i = 0; i < W; i++) {
+          if (i < 9 && s[i] >= P) { b4++; break; }
+          if (s[i] % P != r[i]) { b4++; break; }
+        }
+        internal_lazy_finish<W>(s);
+        for (int i = 0; i < W; i++) if (s[i] != r[i]) { b4++; break; }
+      }
+    };
+    lazy_check(std::integral_constant<int, 16>{});
+    lazy_check(std::integral_constant<int, 24>{});
   }
   for (int w = 0; w < 2; w++) {
     const int W = w ? 24 : 16, RP = w ? 23 : 20;

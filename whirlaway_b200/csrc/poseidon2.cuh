@@ -290,6 +290,57 @@ KB_HD uint32_t cube_fq(uint32_t u) {
   return umin(r3, r3 + P);
 }
 
+// k of the diagonal entries +-2^-k (entries 9.., both widths).
+template <int W>
+KB_HD constexpr int p2_diag_k(int i) {
+  constexpr int k16[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 8, 3, 24, 8, 3, 4, 24};
+  constexpr int k24[24] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 8, 2, 3, 4, 5, 6, 24, 8, 3, 4, 5, 6, 7, 9, 24};
+  return W == 16 ? k16[i] : k24[i];
+}
+
+// Internal layer with lazily reduced words. Words 0..8 (multipliers -2, 1, 2, 1/2, 3, 4, -1/2,
+// -3, -4, applied by doublings and halvings) are canonical on entry and exit. Words 9.. (the
+// multipliers +-2^-k, 2 <= k <= 24) may enter with any value below 2^32 and leave below 2^32:
+// x 2^-k = (x >> k) - (x mod 2^k)(p - 1)/2^k (mod p) holds for every x, and its canonical
+// form is umin(r, r + p) because r < 2^(32-k) <= p. The sum is reduced once, from 64 bits.
+//  * positive, k >= 8: hi + sum + p - lo c in (0, 2p + 2^24), no reduction at all;
+//  * positive, k < 8: r + sum in [0, 2p);  negative: sum + p - r in (0, 2p).
+template <int W>
+KB_HD void internal_layer_lazy_with0(uint32_t* s, uint32_t x0) {
+  // canonical words pair up without carry (each pair below 2p < 2^32)
+  uint64_t a = uint64_t(x0 + s[1]) + uint32_t(s[2] + s[3]) + uint32_t(s[4] + s[5]) + uint32_t(s[6] + s[7]) + s[8];
+#pragma unroll
+  for (int i = 9; i < W; i++) a += s[i];  // below 2^37
+  const uint64_t b = uint64_t(uint32_t(a)) + uint64_t(uint32_t(a >> 32)) * ((1u << 25) - 2);  // < 2^33
+  uint32_t sum = (uint32_t(b) & 0x7fffffffu) + uint32_t(b >> 31) * ((1u << 24) - 1);         // < 2p
+  sum = umin(sum, sum - P);
+  s[0] = p2_diag_mul_add<W>(0, x0, sum);
+#pragma unroll
+  for (int i = 1; i < 9; i++) s[i] = p2_diag_mul_add<W>(i, s[i], sum);
+#pragma unroll
+  for (int i = 9; i < W; i++) {
+    const int k = p2_diag_k<W>(i);
+    const uint32_t x = s[i], hi = x >> k, lo = x & ((1u << k) - 1), cst = (P - 1) >> k;
+    if (!p2_diag_neg<W>(i) && k >= 8) {
+      s[i] = hi + sum + P - lo * cst;
+    } else {
+      uint32_t r = hi - lo * cst;
+      r = umin(r, r + P);
+      s[i] = p2_diag_neg<W>(i) ? sum + P - r : sum + r;
+    }
+  }
+}
+// Canonical form of the lazy words after the last internal round (below 2p + 2^24).
+template <int W>
+KB_HD void internal_lazy_finish(uint32_t* s) {
+#pragma unroll
+  for (int i = 9; i < W; i++) {
+    uint32_t x = umin(s[i], s[i] - P);
+    if (!p2_diag_neg<W>(i) && p2_diag_k<W>(i) >= 8) x = umin(x, x - P);
+    s[i] = x;
+  }
+}
+
 // The permutation on canonical values with canonical round constants (p2_consts_canonical).
 template <int W>
 KB_HD void p2_permute_fq(uint32_t* s, const P2Consts<W>& c) {
@@ -301,7 +352,8 @@ KB_HD void p2_permute_fq(uint32_t* s, const P2Consts<W>& c) {
     mds_light<W>(s);
   }
 #pragma unroll 1
-  for (int r = 0; r < P2Consts<W>::RP; r++) internal_layer_with0<W>(s, cube_fq(s[0] + c.internal[r]));
+  for (int r = 0; r < P2Consts<W>::RP; r++) internal_layer_lazy_with0<W>(s, cube_fq(s[0] + c.internal[r]));
+  internal_lazy_finish<W>(s);
 #pragma unroll 1
   for (int r = 0; r < 4; r++) {
 #pragma unroll
