@@ -19,6 +19,8 @@
 // 2^rb points of its line in registers for rb <= 4 stages, and a pass is two such
 // register rounds with one shared-memory exchange between them.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "kernels.h"
 
@@ -181,6 +183,99 @@ __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint3
   else ntt_round_rb<IO_GLOBAL, IO_SMEM>(rb1, ln, tws, 0, warp, active);
   __syncthreads();
   ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb2, ln, tws, rb1, warp, active);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit16() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait16() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Passes after the first (Bs >= 2, so a block's 4 lo values are 4 consecutive rows and point
+// j of a line is one contiguous 128-byte piece of the tile: 4 rows x 8 columns). Persistent
+// blocks walk a contiguous range of lines (lo group outermost, then tile, then hi) and copy
+// the next line into the second of two shared-memory buffers with cp.async while the current
+// one is transformed: the first register round reads and writes shared memory in place, the
+// second writes the codeword. Twiddles are reloaded when the lo group changes.
+constexpr int NTT_ASYNC_BLOCKS_PER_SM = 4;
+__global__ void __launch_bounds__(NTT_WARPS * 32, NTT_ASYNC_BLOCKS_PER_SM) k_ntt_pass_async(uint32_t* __restrict__ data, int T, int Bs, int Bp,
+                                                                  int rb1, const uint2* __restrict__ tw, int tile0,
+                                                                  int tiles, uint32_t nlines, uint32_t per_block) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  const uint32_t npts = 1u << Bp, ntw = npts - 1;
+  uint2* TW = reinterpret_cast<uint2*>(sm + (npts << 6));  // [4][2^Bp - 1]
+  const uint32_t nhi = 1u << (T - Bs - Bp);
+  const uint32_t first = blockIdx.x * per_block;
+  const uint32_t last = first + per_block < nlines ? first + per_block : nlines;
+  if (first >= last) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = lane & 7, l = lane >> 3;
+  auto coords = [&](uint32_t id, uint32_t& lg, int& tile, uint32_t& hi) {
+    hi = id % nhi;
+    const uint32_t r = id / nhi;
+    tile = tile0 + int(r % uint32_t(tiles));
+    lg = r / uint32_t(tiles);
+  };
+  auto row_base = [&](uint32_t lg, int tile, uint32_t hi) {
+    return (size_t(tile) << T) + (size_t(lg) << 2) + (size_t(hi) << (Bs + Bp));
+  };
+  auto prefetch = [&](uint32_t id, uint32_t* X) {
+    uint32_t lg, hi;
+    int tile;
+    coords(id, lg, tile, hi);
+    const uint32_t* g = data + (row_base(lg, tile, hi) << 3);
+    for (uint32_t idx = threadIdx.x; idx < (npts << 3); idx += blockDim.x) {
+      const uint32_t j = idx >> 3, q = idx & 7;
+      cp_async16(X + (j << 5) + 4 * q, g + ((size_t(j) << Bs) << 3) + 4 * q);
+    }
+    cp_async_commit16();
+  };
+  const int rb2 = Bp - rb1;
+  uint32_t cur_lg = ~0u;
+  prefetch(first, sm);
+  for (uint32_t id = first, it = 0; id < last; id++, it++) {
+    uint32_t* X = sm + ((it & 1) << (Bp + 5));
+    if (id + 1 < last) {
+      prefetch(id + 1, sm + (((it + 1) & 1) << (Bp + 5)));
+      cp_async_wait16<1>();
+    } else {
+      cp_async_wait16<0>();
+    }
+    __syncthreads();  // line id is in X for every thread
+    uint32_t lg, hi;
+    int tile;
+    coords(id, lg, tile, hi);
+    if (lg != cur_lg) {
+      for (uint32_t idx = threadIdx.x; idx < (ntw << 2); idx += blockDim.x) {
+        const uint32_t ll = idx & 3, e = idx >> 2;
+        const int tl = 31 - __clz(e + 1);  // e + 1 in [2^tl, 2^(tl+1))
+        const uint32_t r = e + 1 - (1u << tl);
+        const int t = Bs + tl + 1;
+        TW[ll * ntw + e] = tw[((size_t(1) << (t - 1)) - 1) + (size_t(lg) << 2) + ll + (size_t(r) << Bs)];
+      }
+      cur_lg = lg;
+      __syncthreads();
+    }
+    NttLane ln;
+    ln.src = nullptr;
+    ln.src_end = nullptr;
+    ln.src_step = 0;
+    ln.data = data + ((row_base(lg, tile, hi) + l) << 3) + c;
+    ln.data_step = Bs + 3;
+    ln.X = X + lane;
+    ln.Bp = Bp;
+    const uint2* tws = TW + l * ntw;
+    if (rb2 == 0) {
+      ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb1, ln, tws, 0, warp, true);
+    } else {
+      ntt_round_rb<IO_SMEM, IO_SMEM>(rb1, ln, tws, 0, warp, true);
+      __syncthreads();
+      ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb2, ln, tws, rb1, warp, true);
+    }
+    __syncthreads();  // X is free for the prefetch two lines ahead
+  }
 }
 
 __device__ uint32_t pow_dev(uint32_t a, uint32_t e) {
@@ -485,6 +580,28 @@ void launch_twiddles(uint2* tw, cudaStream_t s) {
   WL_LAUNCH_CHECK();
 }
 
+namespace {
+int ntt_sm_count() {
+  int dev = 0, n = 0;
+  WL_CUDA(cudaGetDevice(&dev));
+  WL_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  return n;
+}
+// Opts the double-buffered pass into more than 48 KB of dynamic shared memory (once per
+// device and size).
+void ntt_async_smem_limit(size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static std::mutex mu;
+  static std::map<int, size_t> done;
+  int dev = 0;
+  WL_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev] >= bytes) return;
+  WL_CUDA(cudaFuncSetAttribute(k_ntt_pass_async, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  done[dev] = bytes;
+}
+}  // namespace
+
 void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s, int tile_begin, int tile_end) {
   const int T = in.L + in.rho;
   if (T > 24) throw std::runtime_error("LDE beyond the two-adic subgroup of order 2^24");
@@ -502,12 +619,23 @@ void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_
     const int hg_log = (2 - lr_log) < hi_bits ? (2 - lr_log) : hi_bits;
     const unsigned gx = 1u << ((Bs - lr_log) + (hi_bits - hg_log));
     const size_t smem = ((size_t(32) << Bp) + (size_t(2) << lr_log) * ((1u << Bp) - 1)) * 4;
-    if (p == 0)
+    const uint32_t nlines = gx * uint32_t(tiles);
+    const size_t smem2 = ((size_t(64) << Bp) + size_t(8) * ((1u << Bp) - 1)) * 4;
+    const uint32_t per_sm = std::min<uint32_t>(NTT_ASYNC_BLOCKS_PER_SM, uint32_t((227 * 1024) / (smem2 + 1024)));
+    const uint32_t nblk = uint32_t(ntt_sm_count()) * std::max<uint32_t>(per_sm, 1);
+    if (p == 0) {
       k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
                                                                       tile_begin);
-    else
+    } else if (lr_log == 2 && hg_log == 0 && nlines >= 4 * nblk) {
+      // enough lines for every block to pipeline several: the double-buffered kernel
+      const uint32_t per = (nlines + nblk - 1) / nblk;
+      ntt_async_smem_limit(smem2);
+      k_ntt_pass_async<<<(nlines + per - 1) / per, NTT_WARPS * 32, smem2, s>>>(out, T, Bs, Bp, rb1, tw, tile_begin,
+                                                                               tiles, nlines, per);
+    } else {
       k_ntt_pass<false><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
                                                                        tile_begin);
+    }
     WL_LAUNCH_CHECK();
     Bs += Bp;
     left -= Bp;
