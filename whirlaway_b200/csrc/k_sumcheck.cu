@@ -135,14 +135,16 @@ __device__ __forceinline__ uint32_t zc0_rc(const AirConsts& K, int i) {
 //   16 <= c < 36 state word 0 before partial round c - 16, plus its round constant
 //   36 <= c < 52 state after the 20 partial rounds, plus rc_end[0]
 // and the committed-column term -L_j(z) sum_r eq[x] sum_i alpha_i col_(17+i) of the block's
-// rows as partial[blockIdx.x * nz + z].
+// rows as partial[blockIdx.x * nz + z]; arow[r] = sum_i alpha_i col_(17+i) (the later rounds
+// carry its fold as one more column).
 constexpr int ZC0R_THREADS = 256;
 __global__ void __launch_bounds__(ZC0R_THREADS) k_zc0_rows(const uint32_t* __restrict__ wit, int log_n, int k,
                                                            int nz, const uint32_t* __restrict__ lw,
                                                            const ef* __restrict__ eq,
                                                            const ef* __restrict__ alphas_g,
                                                            const __grid_constant__ AirConsts K,
-                                                           uint32_t* __restrict__ q, ef* __restrict__ partial) {
+                                                           uint32_t* __restrict__ q, ef* __restrict__ partial,
+                                                           ef* __restrict__ arow) {
   __shared__ ef alphas[AIR_NC];
   __shared__ ef scratch[32];
   __shared__ ef total;
@@ -182,7 +184,9 @@ __global__ void __launch_bounds__(ZC0R_THREADS) k_zc0_rows(const uint32_t* __res
     }
 #pragma unroll
     for (int t = 0; t < 16; t++) qr[size_t(36 + t) * N] = add(s[t], K.end[0][t]);
-    c = ef_mul(m.value(), eq[r & ((size_t(1) << lS) - 1)]);
+    const ef a = m.value();
+    arow[r] = a;
+    c = ef_mul(a, eq[r & ((size_t(1) << lS) - 1)]);
   }
   const size_t last = (rb + ZC0R_THREADS <= N ? rb + ZC0R_THREADS : N) - 1;
   const int nsk = 1 << k;
@@ -347,6 +351,19 @@ __global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, c
   out[size_t(c) * S + x + 1] = m1.value();
 }
 
+// out[x] = sum_j sel[j] * a[j * S + x] for an extension-field table a that is already read at
+// up rows (the committed-column combination of k_zc0_rows).
+__global__ void k_zc0_fold_ef(const ef* __restrict__ a, int log_n, int k, const ef* __restrict__ sel,
+                              ef* __restrict__ out) {
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (x >= S) return;
+  EfMacE m;
+  m.init();
+  for (int j = 0; j < (1 << k); j++) m.mac(sel[j], a[size_t(j) * S + x]);
+  out[x] = m.value();
+}
+
 // ------------------------------------------------------------------ zerocheck rounds >= 1
 // One block per (x, z), x < 2^(m-1), z in {0, 2, 3}: the 148 batched constraints at the
 // point whose columns are lo + z (hi - lo) (lo, hi = the column at x and 2^(m-1) + x).
@@ -410,7 +427,6 @@ __global__ void __launch_bounds__(ZCE_THREADS) k_zc_ef(const ef* __restrict__ co
       const int f = seg < 4 ? seg : seg + 1;
       const uint32_t rc = seg < 4 ? K.begin[seg][j] : K.end[seg - 3][j];
       const int post = seg < 4 ? 17 + 16 * seg : 101 + 16 * (seg - 3);
-      const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
       ef in;
       if (seg == 0) {
         // MDS(inputs)_j: the M4 output of chunk j / 4 plus the sum over chunks of position j % 4
@@ -428,7 +444,7 @@ __global__ void __launch_bounds__(ZCE_THREADS) k_zc_ef(const ef* __restrict__ co
       } else {
         in = get(post - 16 + j);
       }
-      acc = ef_sub(ef_mul(betas[16 * f + j], ef_cube(ef_add_f(in, rc))), ef_mul(alphas[c0 + j], get(post + j)));
+      acc = ef_mul(betas[16 * f + j], ef_cube(ef_add_f(in, rc)));
     }
   } else {
     const int i = lane & 15;
@@ -449,12 +465,10 @@ __global__ void __launch_bounds__(ZCE_THREADS) k_zc_ef(const ef* __restrict__ co
     }
     if (lane < 20) {
       const ef x0 = ef_cube(ef_add_f(s0r, K.partial[lane]));
-      acc = ef_mul(alphas[64 + lane], ef_sub(x0, pr));
+      acc = ef_mul(alphas[64 + lane], x0);
     }
     if (lane < 16) {
-      const ef e = ef_sub(ef_mul(betas[16 * 4 + i], ef_cube(ef_add_f(st, K.end[0][i]))),
-                          ef_mul(alphas[84 + i], get(101 + i)));
-      acc = ef_add(acc, e);
+      acc = ef_add(acc, ef_mul(betas[16 * 4 + i], ef_cube(ef_add_f(st, K.end[0][i]))));
     }
   }
   acc = warp_reduce_ef(acc);
@@ -465,7 +479,8 @@ __global__ void __launch_bounds__(ZCE_THREADS) k_zc_ef(const ef* __restrict__ co
     ef tot = wsum[0];
 #pragma unroll
     for (int w = 1; w < ZCE_THREADS / 32; w++) tot = ef_add(tot, wsum[w]);
-    partial[blockIdx.x] = ef_mul(tot, eq[x]);
+    // the committed-post terms of all 148 constraints: the carried column
+    partial[blockIdx.x] = ef_mul(ef_sub(tot, get(AIR_W)), eq[x]);
   }
 }
 
@@ -532,9 +547,8 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_full_dense(const ef* __re
     t = ef_add(t, shfl_xor_ef(t, 8));
     in = ef_add(y, t);
   }
-  EfMacE pos, neg;  // beta * cube terms, alpha * post terms
+  EfMacE pos;  // beta * cube terms
   pos.init();
-  neg.init();
   // A round's input is the previous round's post, which this lane already holds, except for
   // ending round 1 (segment 4), whose input is ending round 0's post. The next segment's
   // post (and that one input) are loaded a segment ahead.
@@ -545,15 +559,15 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_full_dense(const ef* __re
   for (int seg = 0; seg < 7; seg++) {
     const int f = seg < 4 ? seg : seg + 1;
     const uint32_t rc = seg < 4 ? K.begin[seg][j] : K.end[seg - 3][j];
-    const int c0 = seg < 4 ? 16 * seg : 84 + 16 * (seg - 3);
-    const ef pv_next = seg < 6 ? get(post_of(seg + 1) + j) : ef_zero();
+    const ef pv_next = seg < 5 ? get(post_of(seg + 1) + j) : ef_zero();
     if (seg == 3) in4 = get(101 + j);
     pos.mac(betas[16 * f + j], ef_cube(ef_add_f(in, rc)));
-    neg.mac(alphas[c0 + j], pv);
     in = seg == 3 ? in4 : pv;
     pv = pv_next;
   }
-  const ef acc = ef_sub(pos.value(), neg.value());
+  // the committed-post terms of all 148 constraints are the carried column sum_i alpha_i
+  // col_(17+i), subtracted once per point
+  const ef acc = j == 0 ? ef_sub(pos.value(), get(AIR_W)) : pos.value();
   // fold the point's 16 lanes, weight by eq, then the block sum
   ef pt = acc;
 #pragma unroll
@@ -585,9 +599,8 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
   // rounds in groups of 8 (a rolled loop keeps the code small): in group t, lane sub holds
   // the partial post p_(8t+sub), records state word 0 of round 8t + sub, and evaluates that
   // round's S-box constraint once the group is done
-  EfMacE pos, neg;  // S-box / cube terms, committed-post terms
+  EfMacE pos;  // S-box / cube terms (the committed-post terms are in k_zc_full_dense)
   pos.init();
-  neg.init();
   ef p_cur = get(81 + sub);
 #pragma unroll 1
   for (int t = 0; t < 3; t++) {
@@ -609,7 +622,6 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
     const int r = 8 * t + sub;
     if (r < 20) {
       pos.mac(alphas[64 + r], ef_cube(ef_add_f(s0_cur, K.partial[r])));
-      neg.mac(alphas[64 + r], p_cur);
     }
     if (t < 2) p_cur = (r + 8 < 20) ? get(81 + r + 8) : ef_zero();
   }
@@ -617,9 +629,8 @@ __global__ void __launch_bounds__(ZCD_WARPS * 32) k_zc_partial_dense(const ef* _
   for (int kk = 0; kk < 2; kk++) {
     const int j = 2 * sub + kk;
     pos.mac(betas[16 * 4 + j], ef_cube(ef_add_f(st[kk], K.end[0][j])));
-    neg.mac(alphas[84 + j], get(101 + j));
   }
-  ef pt = ef_sub(pos.value(), neg.value());
+  ef pt = pos.value();
 #pragma unroll
   for (int d = 4; d > 0; d >>= 1) pt = ef_add(pt, shfl_xor_ef(pt, d));
   const ef res = (sub == 0 && valid) ? ef_mul(pt, eq[xs]) : ef_zero();
@@ -930,8 +941,14 @@ int zc0_blocks(int log_n, int k) {
 }
 int zc0_row_blocks(int log_n) { return (int)(((size_t(1) << log_n) + ZC0R_THREADS - 1) / ZC0R_THREADS); }
 void launch_zc0_rows(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
-                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, cudaStream_t s) {
-  k_zc0_rows<<<zc0_row_blocks(log_n), ZC0R_THREADS, 0, s>>>(wit, log_n, k, nz, lw, eq, alphas, K, q, partial);
+                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, ef* arow, cudaStream_t s) {
+  k_zc0_rows<<<zc0_row_blocks(log_n), ZC0R_THREADS, 0, s>>>(wit, log_n, k, nz, lw, eq, alphas, K, q, partial,
+                                                            arow);
+  WL_LAUNCH_CHECK();
+}
+void launch_zc0_fold_ef(const ef* a, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {
+  const size_t S = size_t(1) << (log_n - k);
+  k_zc0_fold_ef<<<(unsigned)((S + 255) / 256), 256, 0, s>>>(a, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
 void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, int nz, const uint32_t* lw,

@@ -77,12 +77,17 @@ constexpr int ZC0_NQ = 52;
 int zc0_blocks(int log_n, int k);
 int zc0_row_blocks(int log_n);
 void launch_zc0_rows(const uint32_t* wit, int log_n, int k, int nz, const uint32_t* lw, const ef* eq,
-                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, cudaStream_t s);
+                     const ef* alphas, const AirConsts& K, uint32_t* q, ef* partial, ef* arow, cudaStream_t s);
+// Round-0 fold of the committed-column combination arow (2^log_n EF, one per row): out[x] =
+// sum_j sel[j] arow[j 2^(log_n-k) + x]. The rounds >= 1 carry it as column AIR_W of their
+// folded columns: the committed-post terms of every constraint, summed once per point.
+void launch_zc0_fold_ef(const ef* arow, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
 void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, int nz, const uint32_t* lw,
                      const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K, ef* partial,
                      cudaStream_t s);
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
 int zc_ef_blocks(int m);
+// cols: AIR_W + 1 folded columns (the last one the committed-column combination).
 // betas: the 8 full rounds' 16 weights beta_f = MDS^T (alpha_(c0(f)+i))_i, f = 0..7.
 void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K,
                        ef* partial, cudaStream_t s);

@@ -707,6 +707,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   ef sum = kb::ef_zero();
   ef mmf = kb::ef_one();
   DBuf cols;
+  // the committed-column combination sum_i alpha_i col_(17+i) of every row; folded, it is the
+  // last of the W + 1 columns of the rounds >= 1
+  DBuf arow(sizeof(ef) * N, st);
   {
     std::vector<uint32_t> lw(size_t(nz) * nsk);
     for (int zi = 0; zi < nz; zi++)
@@ -716,7 +719,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     ef* part = ctx.partials(size_t(nb + nbr) * nz);
     {
       DBuf q(sizeof(uint32_t) * ZC0_NQ * N, st);
-      { ProfScope _ps(ctx, "zc0_rows"); launch_zc0_rows(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, q.as<uint32_t>(), part + size_t(nb) * nz, st); }
+      { ProfScope _ps(ctx, "zc0_rows"); launch_zc0_rows(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, q.as<uint32_t>(), part + size_t(nb) * nz, arow.as<ef>(), st); }
       { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, q.as<uint32_t>(), n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
     }
     std::vector<ef> sums = reduce_to_host(ctx, part, nb + nbr, nz);
@@ -740,8 +743,10 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
     }
     DBuf d_sel = upload(ctx, selr);
-    cols = DBuf(sizeof(ef) * size_t(W) * S, st);
+    cols = DBuf(sizeof(ef) * size_t(W + 1) * S, st);
     { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
+    { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold_ef(arow.as<ef>(), n, k, d_sel.as<ef>(), cols.as<ef>() + size_t(W) * S, st); }
+    arow.reset();
   }
   const auto basis4 = lagrange_basis_cached(4);
   // eq table of round r (over zc[1+r..]) = eq table of round r-1 with its leading variable
@@ -770,9 +775,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 4));
     mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
                      mmf);
-    DBuf nc(sizeof(ef) * size_t(W) * half, st);
+    DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
     DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), W, half, c, st,
+    { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), W + 1, half, c, st,
                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
     cols = std::move(nc);
     eqr = std::move(eqn);

@@ -17,7 +17,8 @@ uint64_t proof_footprint_bytes(int log_n) {
   b += uint64_t(AIR_W) * N * 4;         // witness
   b += 88ull * 4 * N * 4;               // first commitment: LDE (88 stored columns, rate 1/2, fold 2^7)
   b += 2ull * 4 * N * 32;               // its Merkle tree
-  b += uint64_t(AIR_W) * (N / 16) * 32 * 3 / 2;  // zerocheck fold buffers (double-buffered)
+  b += uint64_t(AIR_W + 1) * (N / 16) * 32 * 3 / 2;  // zerocheck fold buffers (double-buffered)
+  b += 32ull * N + 4ull * ZC0_NQ * N;                 // round 0: per-row combination and cube inputs
   b += 3ull * N * 32;                   // inner sumcheck tables (eq, A, B)
   b += 2ull * 2 * N * 32 * 2;           // WHIR g / w and their folds
   b += 128ull * N * 4 + 2ull * N * 32;  // second commitment and its tree
