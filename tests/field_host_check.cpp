@@ -32,6 +32,12 @@ int main() {
     uint32_t x = g() % P, xm = to_mont(x);
     for (int i = 0; i < 24; i++) if (p2_diag_mul<24>(i, xm) != mul(xm, p2_diag<24>(i))) b4++;
   }
+  // extension-field square (distinct products only) against the general product
+  for (int it = 0; it < 200000; it++) {
+    ef a;
+    for (int i = 0; i < 8; i++) a.c[i] = (it % 4 == 0) ? P - 1 - uint32_t(g() % 3) : uint32_t(g() % P);
+    if (!ef_eq(ef_sqr(a), ef_mul(a, a))) b3++;
+  }
   // x * 2^-k at the ends of the range and with all low bits set
   for (int k = 1; k <= 24; k++) {
     const uint32_t inv = detail::cm_inv2(k, false);

@@ -91,8 +91,8 @@ __global__ void k_reduce_partials(const ef* __restrict__ partial, int nblk, int 
 
 // ------------------------------------------------------------------ AIR zerocheck
 constexpr int ZC0_X = 32, ZC0_Z = 15;
-constexpr int ZC0_STAGES = 4;   // column groups in flight
-constexpr int ZC0_GROUP = 4;    // columns per staged group (one block barrier per group)
+constexpr int ZC0_STAGES = 2;   // input groups in flight
+constexpr int ZC0_GROUP = 8;    // inputs per staged group (one block barrier per group)
 constexpr int ZC0_PAD = 20;     // words per x in a staged column tile (16 values + padding)
 
 __device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
@@ -275,16 +275,17 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* _
   for (int g = 0; g < ZC0_STAGES - 1; g++) issue(g);
   EfMacF m;
   m.init();
-  constexpr int NG = AIR_NC / ZC0_GROUP;
-  static_assert(NG * ZC0_GROUP == AIR_NC, "whole groups");
+  constexpr int NG = (AIR_NC + ZC0_GROUP - 1) / ZC0_GROUP;
+  static_assert(ZC0_GROUP % 4 == 0 && AIR_NC % 4 == 0, "flushes after every 4 products");
 #pragma unroll 1
   for (int g = 0; g < NG; g++) {
     cp_async_wait<ZC0_STAGES - 2>();
     __syncthreads();  // group g landed for every thread; the slot of group g - 1 is free
     issue(g + ZC0_STAGES - 1);
-#pragma unroll
+#pragma unroll 4
     for (int cc = 0; cc < ZC0_GROUP; cc++) {
       const int i = ZC0_GROUP * g + cc;
+      if (i >= AIR_NC) break;  // the last group is partial
       const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
       // two chains of 8 products, folded with 2^32 = 2^25 - 2 (mod p) after every 4 (below
       // 2^57 + 2^32 each); the round constant enters the high word (rc 2^32 reduces to rc),
@@ -302,8 +303,8 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* _
       }
       const uint32_t u = redc(sa + sb + (uint64_t(rcs[i]) << 32));
       m.mac(gam[i], cube(u));
+      if ((cc & 3) == 3) m.flush();
     }
-    m.flush();
   }
   cp_async_wait<0>();
   const bool active = zi < nz && x < S;

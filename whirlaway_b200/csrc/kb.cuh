@@ -178,8 +178,38 @@ KB_HD ef ef_mul(const ef& a, const ef& b) {
   }
   return r;
 }
-KB_HD ef ef_sqr(const ef& a) { return ef_mul(a, a); }
-KB_HD ef ef_cube(const ef& a) { return ef_mul(ef_mul(a, a), a); }
+// Square with the 36 distinct products: coefficient k sums a_i a_j over i <= j with
+// i + j = k (cross terms by 2 a_i) and, times 3, over i + j = k + 8 (cross terms by 6 a_i);
+// the doubled and tripled operands are formed once. At most five products per coefficient,
+// folded with 2^32 = 2^25 - 2 (mod p) after the fourth, then one Montgomery reduction.
+KB_HD ef ef_sqr(const ef& a) {
+  uint32_t d[8], t[8], s[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    d[i] = dbl(a.c[i]);
+    t[i] = add(d[i], a.c[i]);
+    s[i] = dbl(t[i]);
+  }
+  ef r;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    uint64_t acc = 0;
+    int n = 0;
+#pragma unroll
+    for (int i = 0; i <= k / 2; i++) {
+      acc += wmul(i == k - i ? a.c[i] : d[i], a.c[k - i]);
+      if (++n == 4) acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
+    }
+#pragma unroll
+    for (int i = k + 1; i <= (k + 8) / 2; i++) {
+      acc += wmul(i == k + 8 - i ? t[i] : s[i], a.c[k + 8 - i]);
+      if (++n == 4) acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
+    }
+    r.c[k] = redc(acc);
+  }
+  return r;
+}
+KB_HD ef ef_cube(const ef& a) { return ef_mul(ef_sqr(a), a); }
 
 // a + r * (b - a)
 KB_HD ef ef_lerp(const ef& a, const ef& b, const ef& r) { return ef_add(a, ef_mul(r, ef_sub(b, a))); }
