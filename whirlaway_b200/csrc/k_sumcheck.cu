@@ -726,6 +726,158 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
   }
 }
 
+// ---- inner sums on the tensor cores
+// A sum of products of 31-bit values is exact in integer matrix products over byte limbs:
+// with x = sum_a 2^(8a) x_a and e = sum_b 2^(8b) e_b (bytes), sum_k x e = sum_(a,b) 2^(8(a+b))
+// sum_k x_a e_b, and each inner sum of 4096 byte products stays below 2^28. The witness
+// segments of 2^ll rows are the rows of A (u32 values, split into 4 byte matrices in
+// registers), the eq_lo weights the columns of B: 16 columns, the 8 coefficients of eq_lo[x]
+// (up sums) and of eq_lo[x - 1] (down sums, shifted by one row), as 4 byte matrices
+// prepared once (k_eq_limbs). Each m16n8k32 u8 product adds 16 x 8 x 32 byte products into
+// s32 accumulators; warp b of a block holds the 4 x 2 tiles of B limb b for a 16-row tile.
+// The limb products are recombined by diagonal (a + b = d, below 2^30), weighted by
+// 2^(8d) mod p (7 wide products, below 4 p^2) and reduced once: the Montgomery values give
+// the Montgomery product. The row boundary terms (the down sum's element past the segment,
+// the wrapped last row) are added on the CUDA cores.
+__device__ __forceinline__ void mma_u8_16832(int (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// Byte a of four consecutive values, packed (limb a of a k-quad of the A fragment).
+__device__ __forceinline__ void byte_transpose4(const uint4 q, uint32_t (&r)[4]) {
+  const uint32_t p01l = __byte_perm(q.x, q.y, 0x5140), p01h = __byte_perm(q.x, q.y, 0x7362);
+  const uint32_t p23l = __byte_perm(q.z, q.w, 0x5140), p23h = __byte_perm(q.z, q.w, 0x7362);
+  r[0] = __byte_perm(p01l, p23l, 0x5410);
+  r[1] = __byte_perm(p01l, p23l, 0x7632);
+  r[2] = __byte_perm(p01h, p23h, 0x5410);
+  r[3] = __byte_perm(p01h, p23h, 0x7632);
+}
+// limbs[(b * 16 + n) * nlo + x] = byte b of column n of B at row x: n < 8 coefficient n of
+// eq_lo[x], n >= 8 coefficient n - 8 of eq_lo[x - 1] (zero at x = 0).
+__global__ void k_eq_limbs(const ef* __restrict__ eq_lo, int nlo, uint8_t* __restrict__ limbs) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 16 * nlo) return;
+  const int n = idx / nlo, x = idx - n * nlo;
+  uint32_t v = 0;
+  if (n < 8) v = eq_lo[x].c[n];
+  else if (x > 0) v = eq_lo[x - 1].c[n - 8];
+#pragma unroll
+  for (int b = 0; b < 4; b++) limbs[(size_t(b) * 16 + n) * nlo + x] = uint8_t(v >> (8 * b));
+}
+constexpr int ISM_WARPS = 4;  // one per B limb
+__global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                                  int ll, const ef* __restrict__ eq_hi,
+                                                                  const ef* __restrict__ eq_lo,
+                                                                  const uint8_t* __restrict__ limbs,
+                                                                  ef* __restrict__ pu, ef* __restrict__ pd) {
+  __shared__ int cs[4][4][16][17];  // [a][b][row][col], padded
+  __shared__ ef up_s[16], dn_s[16];
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const uint32_t nsk = 1u << k, nhi = 1u << (log_n - k - ll), nlo = 1u << ll;
+  const uint32_t M = uint32_t(AIR_W) * nsk * nhi;
+  const uint32_t m0 = blockIdx.x * 16;
+  const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  auto row_base = [&](uint32_t m) -> size_t {
+    const uint32_t xh = m % nhi, cj = m / nhi, j = cj % nsk, c = cj / nsk;
+    return size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+  };
+  const uint32_t ra = m0 + g, rb = m0 + g + 8;
+  const bool va = ra < M, vb = rb < M;
+  const uint32_t* pa = wit + (va ? row_base(ra) : 0) + 4 * t;
+  const uint32_t* pb = wit + (vb ? row_base(rb) : 0) + 4 * t;
+  const uint32_t* lb = reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo);
+  const uint32_t lstride = nlo >> 2;  // u32 per limb row
+  int acc[4][2][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
+  const uint4 zero4 = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+  for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
+    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
+    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
+    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
+    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
+    uint32_t l0[4], l1[4], l2[4], l3[4];
+    byte_transpose4(q0, l0);
+    byte_transpose4(q1, l1);
+    byte_transpose4(q2, l2);
+    byte_transpose4(q3, l3);
+    uint32_t bf[2][2];
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+      const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (k0 >> 2) + t;
+      bf[nt][0] = __ldg(col);
+      bf[nt][1] = __ldg(col + 4);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+      cs[a][b][g][nt * 8 + 2 * t] = acc[a][nt][0];
+      cs[a][b][g][nt * 8 + 2 * t + 1] = acc[a][nt][1];
+      cs[a][b][g + 8][nt * 8 + 2 * t] = acc[a][nt][2];
+      cs[a][b][g + 8][nt * 8 + 2 * t + 1] = acc[a][nt][3];
+    }
+  __syncthreads();
+  // recombination: 256 (row, column) values, two per thread
+  for (int e = threadIdx.x; e < 256; e += ISM_WARPS * 32) {
+    const int row = e >> 4, col = e & 15;
+    constexpr uint32_t W8[7] = {uint32_t(kb::detail::cpow(2, 0)),  uint32_t(kb::detail::cpow(2, 8)),
+                                uint32_t(kb::detail::cpow(2, 16)), uint32_t(kb::detail::cpow(2, 24)),
+                                uint32_t(kb::detail::cpow(2, 32)), uint32_t(kb::detail::cpow(2, 40)),
+                                uint32_t(kb::detail::cpow(2, 48))};  // 2^(8d) mod p
+    uint64_t v = 0;
+#pragma unroll
+    for (int d = 0; d < 7; d++) {
+      uint32_t dd = 0;  // below 4 * 2^12 * 255^2 < 2^31
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+        if (d - a >= 0 && d - a < 4) dd += uint32_t(cs[a][d - a][row][col]);
+      v += kb::wmul(dd, W8[d]);
+    }
+    const uint32_t r = kb::redc(v);
+    if (col < 8) up_s[row].c[col] = r;
+    else dn_s[row].c[col - 8] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    const uint32_t m = m0 + threadIdx.x;
+    if (m < M) {
+      const uint32_t xh = m % nhi, cj = m / nhi, j = cj % nsk, c = cj / nsk;
+      const size_t base = size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+      const uint32_t* col = wit + size_t(c) * N;
+      const bool last = j == nsk - 1 && xh == nhi - 1;  // the segment holding row N - 1
+      const ef el = eq_lo[nlo - 1];
+      ef up = up_s[threadIdx.x], dn = dn_s[threadIdx.x];
+      if (last) {
+        // up row of N - 1 is N - 2; down row of N - 1 is N - 1
+        up = ef_add(up, ef_mul_f(el, kb::sub(col[N - 2], col[N - 1])));
+        dn = ef_add(dn, ef_mul_f(el, col[N - 1]));
+      } else {
+        dn = ef_add(dn, ef_mul_f(el, wit[base + nlo]));
+      }
+      const ef h = eq_hi[xh];
+      pu[m] = ef_mul(up, h);
+      pd[m] = ef_mul(dn, h);
+    }
+  }
+}
+
 // out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]; one warp per column.
 __global__ void k_combine_sel(const ef* __restrict__ partial, const ef* __restrict__ sel, int nsk, int nh, int ncols,
                               ef* __restrict__ out) {
@@ -1003,14 +1155,22 @@ void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef
   WL_LAUNCH_CHECK();
 }
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
-                       const ef* sel, ef* out_up, ef* out_down, cudaStream_t s) {
+                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s) {
   // out_up / out_down hold AIR_W results followed by AIR_W * 2^k * 2^(log_n - k - ll) partials.
   const int nsk = 1 << k;
   const int nh = 1 << (log_n - k - ll);
   ef* pu = out_up + AIR_W;
   ef* pd = out_down + AIR_W;
-  k_inner_sums<<<dim3((AIR_W + 1) / 2, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(
-      wit, log_n, k, ll, eq_hi, eq_lo, pu, pd);
+  if (limbs && ll >= INNER_MMA_MIN_LL && ll <= 12) {  // 2^12 byte products per s32 sum
+    const int nlo = 1 << ll;
+    k_eq_limbs<<<(16 * nlo + 255) / 256, 256, 0, s>>>(eq_lo, nlo, limbs);
+    WL_LAUNCH_CHECK();
+    const uint32_t M = uint32_t(AIR_W) * nsk * nh;
+    k_inner_sums_mma<<<(M + 15) / 16, ISM_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi, eq_lo, limbs, pu, pd);
+  } else {
+    k_inner_sums<<<dim3((AIR_W + 1) / 2, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(
+        wit, log_n, k, ll, eq_hi, eq_lo, pu, pd);
+  }
   WL_LAUNCH_CHECK();
   k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pu, sel, nsk, nh, AIR_W, out_up);
   WL_LAUNCH_CHECK();

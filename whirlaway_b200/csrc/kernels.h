@@ -101,8 +101,11 @@ void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef
 // Up/down evaluations of every column at (r0; tail), with eq(tail, .) factored as
 // eq_hi (2^(log_n-k-ll) entries) x eq_lo (2^ll entries). out_up / out_down must hold
 // AIR_W * (1 + 2^k * 2^(log_n-k-ll)) elements; the first AIR_W are the results.
+// With limbs (64 * 2^ll bytes of scratch) and ll >= INNER_MMA_MIN_LL, the segment sums run
+// as byte-limb integer matrix products on the tensor cores.
+constexpr int INNER_MMA_MIN_LL = 5;
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
-                       const ef* sel, ef* out_up, ef* out_down, cudaStream_t s);
+                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s);
 
 // --------------------------------------------------------------- inner phase
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s);

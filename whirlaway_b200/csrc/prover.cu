@@ -796,7 +796,8 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     EqPair et = eq_pair(ctx, rtail, lh_t);
     const size_t plen = size_t(W) * (1 + (size_t(nsk) << lh_t));
     DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
-    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), st); }
+    DBuf limbs(size_t(64) << ll_t, st);
+    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), limbs.as<uint8_t>(), st); }
     ctx.to_host(inner_up.data(), up.as<ef>(), sizeof(ef) * W);
     ctx.to_host(inner_down.data(), down.as<ef>(), sizeof(ef) * W);
   }
