@@ -768,6 +768,80 @@ __global__ void k_eq_limbs(const ef* __restrict__ eq_lo, int nlo, uint8_t* __res
   for (int b = 0; b < 4; b++) limbs[(size_t(b) * 16 + n) * nlo + x] = uint8_t(v >> (8 * b));
 }
 constexpr int ISM_WARPS = 4;  // one per B limb
+
+// The 16-row tile product of a warp: rows g and g + 8 of the tile read nlo consecutive values
+// from pa / pb (zero rows when va / vb is false), B limb b from lb (NT column tiles of 8, each
+// column nlo bytes, lstride u32 apart); acc[a][nt] accumulates A limb a times B limb b.
+template <int NT>
+__device__ __forceinline__ void limb_tile_mma(const uint32_t* pa, const uint32_t* pb, bool va, bool vb,
+                                              const uint32_t* lb, uint32_t lstride, uint32_t nlo, int g, int t,
+                                              int (&acc)[4][NT][4]) {
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
+  const uint4 zero4 = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+  for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
+    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
+    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
+    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
+    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
+    uint32_t l0[4], l1[4], l2[4], l3[4];
+    byte_transpose4(q0, l0);
+    byte_transpose4(q1, l1);
+    byte_transpose4(q2, l2);
+    byte_transpose4(q3, l3);
+    uint32_t bf[NT][2];
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (k0 >> 2) + t;
+      bf[nt][0] = __ldg(col);
+      bf[nt][1] = __ldg(col + 4);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
+#pragma unroll
+      for (int nt = 0; nt < NT; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
+    }
+  }
+}
+// Sum over the limb pairs of column value (row, col), from the per-pair accumulators
+// cs[a][b][row][col]: diagonals a + b = d (below 4 * 2^12 * 255^2 < 2^31) weighted by
+// 2^(8d) mod p, then one Montgomery reduction (the sum stays below 4 p^2).
+template <int C>
+__device__ __forceinline__ uint32_t limb_recombine(const int (&cs)[4][4][16][C], int row, int col) {
+  constexpr uint32_t W8[7] = {uint32_t(kb::detail::cpow(2, 0)),  uint32_t(kb::detail::cpow(2, 8)),
+                              uint32_t(kb::detail::cpow(2, 16)), uint32_t(kb::detail::cpow(2, 24)),
+                              uint32_t(kb::detail::cpow(2, 32)), uint32_t(kb::detail::cpow(2, 40)),
+                              uint32_t(kb::detail::cpow(2, 48))};  // 2^(8d) mod p
+  uint64_t v = 0;
+#pragma unroll
+  for (int d = 0; d < 7; d++) {
+    uint32_t dd = 0;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+      if (d - a >= 0 && d - a < 4) dd += uint32_t(cs[a][d - a][row][col]);
+    v += kb::wmul(dd, W8[d]);
+  }
+  return kb::redc(v);
+}
+template <int NT, int C>
+__device__ __forceinline__ void limb_store(int (&cs)[4][4][16][C], const int (&acc)[4][NT][4], int b, int g, int t) {
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      cs[a][b][g][nt * 8 + 2 * t] = acc[a][nt][0];
+      cs[a][b][g][nt * 8 + 2 * t + 1] = acc[a][nt][1];
+      cs[a][b][g + 8][nt * 8 + 2 * t] = acc[a][nt][2];
+      cs[a][b][g + 8][nt * 8 + 2 * t + 1] = acc[a][nt][3];
+    }
+}
+
 __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_t* __restrict__ wit, int log_n, int k,
                                                                   int ll, const ef* __restrict__ eq_hi,
                                                                   const ef* __restrict__ eq_lo,
@@ -787,70 +861,15 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
   };
   const uint32_t ra = m0 + g, rb = m0 + g + 8;
   const bool va = ra < M, vb = rb < M;
-  const uint32_t* pa = wit + (va ? row_base(ra) : 0) + 4 * t;
-  const uint32_t* pb = wit + (vb ? row_base(rb) : 0) + 4 * t;
-  const uint32_t* lb = reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo);
-  const uint32_t lstride = nlo >> 2;  // u32 per limb row
   int acc[4][2][4];
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
-  const uint4 zero4 = make_uint4(0, 0, 0, 0);
-#pragma unroll 1
-  for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
-    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
-    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
-    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
-    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
-    uint32_t l0[4], l1[4], l2[4], l3[4];
-    byte_transpose4(q0, l0);
-    byte_transpose4(q1, l1);
-    byte_transpose4(q2, l2);
-    byte_transpose4(q3, l3);
-    uint32_t bf[2][2];
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++) {
-      const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (k0 >> 2) + t;
-      bf[nt][0] = __ldg(col);
-      bf[nt][1] = __ldg(col + 4);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
-#pragma unroll
-      for (int nt = 0; nt < 2; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++) {
-      cs[a][b][g][nt * 8 + 2 * t] = acc[a][nt][0];
-      cs[a][b][g][nt * 8 + 2 * t + 1] = acc[a][nt][1];
-      cs[a][b][g + 8][nt * 8 + 2 * t] = acc[a][nt][2];
-      cs[a][b][g + 8][nt * 8 + 2 * t + 1] = acc[a][nt][3];
-    }
+  limb_tile_mma<2>(wit + (va ? row_base(ra) : 0) + 4 * t, wit + (vb ? row_base(rb) : 0) + 4 * t, va, vb,
+                   reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo), nlo >> 2, nlo, g, t, acc);
+  limb_store<2>(cs, acc, b, g, t);
   __syncthreads();
   // recombination: 256 (row, column) values, two per thread
   for (int e = threadIdx.x; e < 256; e += ISM_WARPS * 32) {
     const int row = e >> 4, col = e & 15;
-    constexpr uint32_t W8[7] = {uint32_t(kb::detail::cpow(2, 0)),  uint32_t(kb::detail::cpow(2, 8)),
-                                uint32_t(kb::detail::cpow(2, 16)), uint32_t(kb::detail::cpow(2, 24)),
-                                uint32_t(kb::detail::cpow(2, 32)), uint32_t(kb::detail::cpow(2, 40)),
-                                uint32_t(kb::detail::cpow(2, 48))};  // 2^(8d) mod p
-    uint64_t v = 0;
-#pragma unroll
-    for (int d = 0; d < 7; d++) {
-      uint32_t dd = 0;  // below 4 * 2^12 * 255^2 < 2^31
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-        if (d - a >= 0 && d - a < 4) dd += uint32_t(cs[a][d - a][row][col]);
-      v += kb::wmul(dd, W8[d]);
-    }
-    const uint32_t r = kb::redc(v);
+    const uint32_t r = limb_recombine(cs, row, col);
     if (col < 8) up_s[row].c[col] = r;
     else dn_s[row].c[col - 8] = r;
   }
@@ -876,6 +895,50 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
       pd[m] = ef_mul(dn, h);
     }
   }
+}
+
+// WHIR partial evaluation on the tensor cores: rows m = (u, v_hi) are the segments
+// T[m 2^ll .. m 2^ll + 2^ll) of the packed table (zero past t_len), B the 8 coefficients of
+// lo (limbs[(b * 8 + n) * nlo + x]); each row's dot product times hi[v_hi], summed over the
+// block's 16 rows, is partial[(v_hi / 16) * 2^lu + u].
+__global__ void __launch_bounds__(ISM_WARPS * 32) k_mle_partial_mma(const uint32_t* __restrict__ T, size_t t_len,
+                                                                   int lu, int lh, int ll,
+                                                                   const ef* __restrict__ hi,
+                                                                   const uint8_t* __restrict__ limbs,
+                                                                   ef* __restrict__ partial) {
+  __shared__ int cs[4][4][16][9];
+  __shared__ ef rows_s[16];
+  const uint32_t nhi = 1u << lh, nlo = 1u << ll;
+  const uint32_t m0 = blockIdx.x * 16;  // 16 rows of one u (16 divides nhi)
+  const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const size_t ba = size_t(m0 + g) << ll, bb = size_t(m0 + g + 8) << ll;
+  const bool va = ba < t_len, vb = bb < t_len;  // t_len is a multiple of 2^ll
+  int acc[4][1][4];
+  limb_tile_mma<1>(T + (va ? ba : 0) + 4 * t, T + (vb ? bb : 0) + 4 * t, va, vb,
+                   reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 8 * nlo), nlo >> 2, nlo, g, t, acc);
+  limb_store<1>(cs, acc, b, g, t);
+  __syncthreads();
+  {
+    const int row = threadIdx.x >> 3, col = threadIdx.x & 7;
+    rows_s[row].c[col] = limb_recombine(cs, row, col);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const uint32_t u = m0 >> lh, vh0 = m0 & (nhi - 1);
+    ef v = threadIdx.x < 16 ? ef_mul(rows_s[threadIdx.x], hi[vh0 + threadIdx.x]) : ef_zero();
+    v = warp_reduce_ef(v);
+    if (threadIdx.x == 0) partial[size_t(vh0 >> 4) * (size_t(1) << lu) + u] = v;
+  }
+}
+// limbs[(b * 8 + n) * nlo + x] = byte b of coefficient n of lo[x].
+__global__ void k_lo_limbs(const ef* __restrict__ lo, int nlo, uint8_t* __restrict__ limbs) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 8 * nlo) return;
+  const int n = idx / nlo, x = idx - n * nlo;
+  const uint32_t v = lo[x].c[n];
+#pragma unroll
+  for (int b = 0; b < 4; b++) limbs[(size_t(b) * 8 + n) * nlo + x] = uint8_t(v >> (8 * b));
 }
 
 // out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]; one warp per column.
@@ -1176,6 +1239,23 @@ void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* 
   WL_LAUNCH_CHECK();
   k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pd, sel, nsk, nh, AIR_W, out_down);
   WL_LAUNCH_CHECK();
+}
+size_t mle_partial_scratch_bytes(int lu, int lh, int ll) {
+  if (ll < INNER_MMA_MIN_LL || ll > 12 || lh < 4) return 0;
+  return (sizeof(ef) << (lu + lh - 4)) + (size_t(32) << ll);
+}
+bool launch_mle_partial_mma(const uint32_t* T, size_t t_len, int lu, int lh, int ll, const ef* hi, const ef* lo,
+                            ef* out, void* scratch, cudaStream_t s) {
+  if (!scratch || !mle_partial_scratch_bytes(lu, lh, ll) || t_len % (size_t(1) << ll)) return false;
+  ef* partial = static_cast<ef*>(scratch);
+  uint8_t* limbs = reinterpret_cast<uint8_t*>(partial + (size_t(1) << (lu + lh - 4)));
+  const int nlo = 1 << ll;
+  k_lo_limbs<<<(8 * nlo + 255) / 256, 256, 0, s>>>(lo, nlo, limbs);
+  WL_LAUNCH_CHECK();
+  k_mle_partial_mma<<<1u << (lu + lh - 4), ISM_WARPS * 32, 0, s>>>(T, t_len, lu, lh, ll, hi, limbs, partial);
+  WL_LAUNCH_CHECK();
+  launch_reduce_partials(partial, 1 << (lh - 4), 1 << lu, out, s);
+  return true;
 }
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s) {
   if (log_n < 1) throw std::invalid_argument("batch_cols: at least 2 rows");

@@ -133,6 +133,12 @@ void launch_abc_eval_ef(const ef* cols, int m, const ef* eq, ef* partial, cudaSt
 // witness of `t_len` values. out[j * 2^lu + u].
 void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, int ll, int J, const ef* hi,
                              const ef* lo, ef* out, cudaStream_t s);
+// The same for one point on the tensor cores (byte-limb matrix products, as for the inner
+// sums), writing out[u] for u < 2^lu. Needs mle_partial_scratch_bytes (0: not available for
+// these sizes) of scratch; returns false, launching nothing, when it does not apply.
+size_t mle_partial_scratch_bytes(int lu, int lh, int ll);
+bool launch_mle_partial_mma(const uint32_t* T, size_t t_len, int lu, int lh, int ll, const ef* hi, const ef* lo,
+                            ef* out, void* scratch, cudaStream_t s);
 void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s);
 void launch_add_eq_terms_f(ef* w, int lh, int ll, int npts, const uint32_t* hi, const uint32_t* lo, const ef* coefs,
                            cudaStream_t s);

@@ -649,7 +649,13 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     std::vector<ef> pv(pt.begin() + lu, pt.end());
     EqPair e = eq_pair(ctx, pv, lh_v);
     DBuf out(sizeof(ef) * (size_t(1) << lu) * 17, st);  // results + 16 split partials
-    { ProfScope _ps(ctx, "whir_partial_eval"); launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st); }
+    const size_t scratch_bytes = mle_partial_scratch_bytes(lu, lh_v, ll_v);
+    DBuf scratch(scratch_bytes, st);
+    {
+      ProfScope _ps(ctx, "whir_partial_eval");
+      if (!launch_mle_partial_mma(wit, t_len, lu, lh_v, ll_v, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), scratch.as<void>(), st))
+        launch_mle_partial_base(wit, t_len, lu, lh_v, ll_v, 1, e.hi.as<ef>(), e.lo.as<ef>(), out.as<ef>(), st);
+    }
     std::vector<ef> h(size_t(1) << lu);
     ctx.to_host(h.data(), out.as<ef>(), sizeof(ef) * h.size());
     return h;
