@@ -768,6 +768,7 @@ __global__ void k_eq_limbs(const ef* __restrict__ eq_lo, int nlo, uint8_t* __res
   for (int b = 0; b < 4; b++) limbs[(size_t(b) * 16 + n) * nlo + x] = uint8_t(v >> (8 * b));
 }
 constexpr int ISM_WARPS = 4;  // one per B limb
+constexpr int CS_WARPS = 4;   // warps of the kernels whose warps own whole tiles
 
 // The 16-row tile product of a warp: rows g and g + 8 of the tile read nlo consecutive values
 // from pa / pb (zero rows when va / vb is false), B limb b from lb (NT column tiles of 8, each
@@ -899,37 +900,75 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
 
 // WHIR partial evaluation on the tensor cores: rows m = (u, v_hi) are the segments
 // T[m 2^ll .. m 2^ll + 2^ll) of the packed table (zero past t_len), B the 8 coefficients of
-// lo (limbs[(b * 8 + n) * nlo + x]); each row's dot product times hi[v_hi], summed over the
-// block's 16 rows, is partial[(v_hi / 16) * 2^lu + u].
-__global__ void __launch_bounds__(ISM_WARPS * 32) k_mle_partial_mma(const uint32_t* __restrict__ T, size_t t_len,
-                                                                   int lu, int lh, int ll,
-                                                                   const ef* __restrict__ hi,
-                                                                   const uint8_t* __restrict__ limbs,
-                                                                   ef* __restrict__ partial) {
-  __shared__ int cs[4][4][16][9];
-  __shared__ ef rows_s[16];
+// lo (limbs[(b * 8 + n) * nlo + x]). Each warp owns a 16-row tile (16 consecutive v_hi of one
+// u) and all 4 x 4 limb pairs, so every segment value is loaded and split into limbs once;
+// its rows' dot products times hi[v_hi], summed, are partial[(v_hi / 16) * 2^lu + u].
+__global__ void __launch_bounds__(CS_WARPS * 32) k_mle_partial_mma(const uint32_t* __restrict__ T, size_t t_len,
+                                                                  int lu, int lh, int ll,
+                                                                  const ef* __restrict__ hi,
+                                                                  const uint8_t* __restrict__ limbs,
+                                                                  ef* __restrict__ partial) {
+  __shared__ int cs_all[CS_WARPS][4][4][16][9];
+  __shared__ ef rows_all[CS_WARPS][16];
   const uint32_t nhi = 1u << lh, nlo = 1u << ll;
-  const uint32_t m0 = blockIdx.x * 16;  // 16 rows of one u (16 divides nhi)
-  const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
+  int(&cs)[4][4][16][9] = cs_all[warp];
+  const uint32_t m0 = (blockIdx.x * CS_WARPS + warp) * 16;  // 16 rows of one u (16 divides nhi)
+  if (m0 >= (1u << (lu + lh))) return;  // whole warp (no block barrier below)
   const size_t ba = size_t(m0 + g) << ll, bb = size_t(m0 + g + 8) << ll;
   const bool va = ba < t_len, vb = bb < t_len;  // t_len is a multiple of 2^ll
-  int acc[4][1][4];
-  limb_tile_mma<1>(T + (va ? ba : 0) + 4 * t, T + (vb ? bb : 0) + 4 * t, va, vb,
-                   reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 8 * nlo), nlo >> 2, nlo, g, t, acc);
-  limb_store<1>(cs, acc, b, g, t);
-  __syncthreads();
-  {
-    const int row = threadIdx.x >> 3, col = threadIdx.x & 7;
-    rows_s[row].c[col] = limb_recombine(cs, row, col);
+  const uint32_t* pa = T + (va ? ba : 0) + 4 * t;
+  const uint32_t* pb = T + (vb ? bb : 0) + 4 * t;
+  const uint32_t* lw = reinterpret_cast<const uint32_t*>(limbs);
+  const uint32_t lstride = nlo >> 2;
+  int acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
+  const uint4 zero4 = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+  for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
+    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
+    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
+    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
+    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
+    uint32_t l0[4], l1[4], l2[4], l3[4];
+    byte_transpose4(q0, l0);
+    byte_transpose4(q1, l1);
+    byte_transpose4(q2, l2);
+    byte_transpose4(q3, l3);
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const uint32_t* col = lw + size_t(b * 8 + g) * lstride + (k0 >> 2) + t;
+      const uint32_t b0 = __ldg(col), b1 = __ldg(col + 4);
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
+        mma_u8_16832(acc[a][b], af, b0, b1);
+      }
+    }
   }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const uint32_t u = m0 >> lh, vh0 = m0 & (nhi - 1);
-    ef v = threadIdx.x < 16 ? ef_mul(rows_s[threadIdx.x], hi[vh0 + threadIdx.x]) : ef_zero();
-    v = warp_reduce_ef(v);
-    if (threadIdx.x == 0) partial[size_t(vh0 >> 4) * (size_t(1) << lu) + u] = v;
-  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      cs[a][b][g][2 * t] = acc[a][b][0];
+      cs[a][b][g][2 * t + 1] = acc[a][b][1];
+      cs[a][b][g + 8][2 * t] = acc[a][b][2];
+      cs[a][b][g + 8][2 * t + 1] = acc[a][b][3];
+    }
+  __syncwarp();
+#pragma unroll
+  for (int e = lane; e < 128; e += 32) rows_all[warp][e >> 3].c[e & 7] = limb_recombine(cs, e >> 3, e & 7);
+  __syncwarp();
+  const uint32_t u = m0 >> lh, vh0 = m0 & (nhi - 1);
+  ef v = lane < 16 ? ef_mul(rows_all[warp][lane], hi[vh0 + lane]) : ef_zero();
+  v = warp_reduce_ef(v);
+  if (lane == 0) partial[size_t(vh0 >> 4) * (size_t(1) << lu) + u] = v;
 }
 // limbs[(b * 8 + n) * nlo + x] = byte b of coefficient n of lo[x].
 __global__ void k_lo_limbs(const ef* __restrict__ lo, int nlo, uint8_t* __restrict__ limbs) {
@@ -939,6 +978,90 @@ __global__ void k_lo_limbs(const ef* __restrict__ lo, int nlo, uint8_t* __restri
   const uint32_t v = lo[x].c[n];
 #pragma unroll
   for (int b = 0; b < 4; b++) limbs[(size_t(b) * 8 + n) * nlo + x] = uint8_t(v >> (8 * b));
+}
+
+// Weighted column sums on the tensor cores: out[m] = sum_(k < K) w[k] A[m][k] for extension
+// weights w and base-field A, by byte-limb matrix products (as the inner sums) with the rows
+// m on the M side and the short K (<= 192) in chunks of 32. A[m][k] sits at
+// src[k * kstride + m] (consecutive rows are consecutive words, so every load of a warp reads
+// whole sectors). Used for the batched column (the witness columns, kstride N). The same form
+// was measured slower than the CUDA-core kernels for the WHIR table g (K = 128) and for the
+// round-0 fold (K = 2^k <= 16, padded to 32): their loads dominate, and the CUDA-core
+// kernels read two rows per load.
+// Each warp owns a 16-row tile and all 4 x 4 limb pairs; limbs[(b * 8 + n) * Kp + k] holds
+// byte b of coefficient n of w[k] (zero for k >= K).
+__global__ void __launch_bounds__(CS_WARPS * 32) k_colsum_mma(const uint32_t* __restrict__ src, size_t M, int K,
+                                                             int Kp, size_t kstride,
+                                                             const uint8_t* __restrict__ limbs, ef* __restrict__ out) {
+  __shared__ int cs_all[CS_WARPS][4][4][16][9];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  int(&cs)[4][4][16][9] = cs_all[warp];
+  const size_t m0 = (size_t(blockIdx.x) * CS_WARPS + warp) * 16;
+  if (m0 >= M) return;  // whole warp (no block barrier below)
+  const size_t ra = m0 + g, rb = m0 + g + 8;
+  const bool va = ra < M, vb = rb < M;
+  auto load = [&](size_t m, bool vm, int kk) -> uint32_t {
+    return (vm && kk < K) ? __ldg(src + size_t(kk) * kstride + m) : 0u;
+  };
+  int acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
+  const uint32_t* lw = reinterpret_cast<const uint32_t*>(limbs);
+  const int lstride = Kp >> 2;
+#pragma unroll 1
+  for (int k0 = 0; k0 < Kp; k0 += 32) {
+    uint4 q[4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int kb0 = k0 + 16 * h + 4 * t;
+      q[2 * h] = make_uint4(load(ra, va, kb0), load(ra, va, kb0 + 1), load(ra, va, kb0 + 2), load(ra, va, kb0 + 3));
+      q[2 * h + 1] =
+          make_uint4(load(rb, vb, kb0), load(rb, vb, kb0 + 1), load(rb, vb, kb0 + 2), load(rb, vb, kb0 + 3));
+    }
+    uint32_t l[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) byte_transpose4(q[i], l[i]);
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const uint32_t* col = lw + size_t(b * 8 + g) * lstride + (k0 >> 2) + t;
+      const uint32_t b0 = __ldg(col), b1 = __ldg(col + 4);
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const uint32_t af[4] = {l[0][a], l[1][a], l[2][a], l[3][a]};
+        mma_u8_16832(acc[a][b], af, b0, b1);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      cs[a][b][g][2 * t] = acc[a][b][0];
+      cs[a][b][g][2 * t + 1] = acc[a][b][1];
+      cs[a][b][g + 8][2 * t] = acc[a][b][2];
+      cs[a][b][g + 8][2 * t + 1] = acc[a][b][3];
+    }
+  __syncwarp();
+  uint32_t* o = reinterpret_cast<uint32_t*>(out);
+#pragma unroll
+  for (int e = lane; e < 128; e += 32) {
+    const int row = e >> 3, col = e & 7;
+    if (m0 + row < M) o[(m0 + row) * 8 + col] = limb_recombine(cs, row, col);
+  }
+}
+// limbs[(b * 8 + n) * Kp + k] = byte b of coefficient n of w[k] (zero for k >= K).
+__global__ void k_w_limbs(const ef* __restrict__ w, int K, int Kp, uint8_t* __restrict__ limbs) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 8 * Kp) return;
+  const int n = idx / Kp, x = idx - n * Kp;
+  const uint32_t v = x < K ? w[x].c[n] : 0u;
+#pragma unroll
+  for (int b = 0; b < 4; b++) limbs[(size_t(b) * 8 + n) * Kp + x] = uint8_t(v >> (8 * b));
 }
 
 // out[c] = sum_j sel[j] * sum_h partial[(c * nsk + j) * nh + h]; one warp per column.
@@ -1240,6 +1363,16 @@ void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* 
   k_combine_sel<<<(AIR_W + 7) / 8, 256, 0, s>>>(pd, sel, nsk, nh, AIR_W, out_down);
   WL_LAUNCH_CHECK();
 }
+size_t colsum_limb_bytes(int K) { return K > 192 ? 0 : size_t(32) * ((K + 31) / 32 * 32); }
+void launch_batch_cols_mma(const uint32_t* wit, int log_n, const ef* eqc, ef* out, uint8_t* limbs, cudaStream_t s) {
+  const size_t N = size_t(1) << log_n;
+  const int K = AIR_W, Kp = (K + 31) / 32 * 32;
+  k_w_limbs<<<(8 * Kp + 255) / 256, 256, 0, s>>>(eqc, K, Kp, limbs);
+  WL_LAUNCH_CHECK();
+  const size_t tiles = (N + 15) / 16;
+  k_colsum_mma<<<(unsigned)((tiles + CS_WARPS - 1) / CS_WARPS), CS_WARPS * 32, 0, s>>>(wit, N, K, Kp, N, limbs, out);
+  WL_LAUNCH_CHECK();
+}
 size_t mle_partial_scratch_bytes(int lu, int lh, int ll) {
   if (ll < INNER_MMA_MIN_LL || ll > 12 || lh < 4) return 0;
   return (sizeof(ef) << (lu + lh - 4)) + (size_t(32) << ll);
@@ -1252,7 +1385,9 @@ bool launch_mle_partial_mma(const uint32_t* T, size_t t_len, int lu, int lh, int
   const int nlo = 1 << ll;
   k_lo_limbs<<<(8 * nlo + 255) / 256, 256, 0, s>>>(lo, nlo, limbs);
   WL_LAUNCH_CHECK();
-  k_mle_partial_mma<<<1u << (lu + lh - 4), ISM_WARPS * 32, 0, s>>>(T, t_len, lu, lh, ll, hi, limbs, partial);
+  const uint32_t tiles = 1u << (lu + lh - 4);
+  k_mle_partial_mma<<<(tiles + CS_WARPS - 1) / CS_WARPS, CS_WARPS * 32, 0, s>>>(T, t_len, lu, lh, ll, hi, limbs,
+                                                                               partial);
   WL_LAUNCH_CHECK();
   launch_reduce_partials(partial, 1 << (lh - 4), 1 << lu, out, s);
   return true;

@@ -137,6 +137,10 @@ void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, in
 // sums), writing out[u] for u < 2^lu. Needs mle_partial_scratch_bytes (0: not available for
 // these sizes) of scratch; returns false, launching nothing, when it does not apply.
 size_t mle_partial_scratch_bytes(int lu, int lh, int ll);
+// The batched column (launch_batch_cols) on the tensor cores (byte-limb matrix products),
+// with colsum_limb_bytes(AIR_W) bytes of scratch for the limbs of the weights.
+size_t colsum_limb_bytes(int K);
+void launch_batch_cols_mma(const uint32_t* wit, int log_n, const ef* eqc, ef* out, uint8_t* limbs, cudaStream_t s);
 bool launch_mle_partial_mma(const uint32_t* T, size_t t_len, int lu, int lh, int ll, const ef* hi, const ef* lo,
                             ef* out, void* scratch, cudaStream_t s);
 void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s);

@@ -820,7 +820,11 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   eqc.resize(W);
   DBuf d_eqc = upload(ctx, eqc);
   DBuf B(sizeof(ef) * N, st);
-  { ProfScope _ps(ctx, "batch_cols"); launch_batch_cols(wit, n, d_eqc.as<ef>(), B.as<ef>(), st); }
+  {
+    DBuf limbs(colsum_limb_bytes(W), st);
+    ProfScope _ps(ctx, "batch_cols");
+    launch_batch_cols_mma(wit, n, d_eqc.as<ef>(), B.as<ef>(), limbs.as<uint8_t>(), st);
+  }
   ef alpha2 = ts.sample_ext();
   std::vector<ef> sub(nsk);
   {
