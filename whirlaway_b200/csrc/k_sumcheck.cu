@@ -9,6 +9,7 @@
 // row and repeat the last (crates/air/src/utils.rs:140-160); neither is materialised.
 // Folded columns are extension-field arrays, column c at cols + c * len.
 #include "kernels.h"
+#include "limb_mma.cuh"
 
 namespace wl {
 
@@ -739,22 +740,6 @@ __global__ void __launch_bounds__(IS_WARPS * 32) k_inner_sums(const uint32_t* __
 // 2^(8d) mod p (7 wide products, below 4 p^2) and reduced once: the Montgomery values give
 // the Montgomery product. The row boundary terms (the down sum's element past the segment,
 // the wrapped last row) are added on the CUDA cores.
-__device__ __forceinline__ void mma_u8_16832(int (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-// Byte a of four consecutive values, packed (limb a of a k-quad of the A fragment).
-__device__ __forceinline__ void byte_transpose4(const uint4 q, uint32_t (&r)[4]) {
-  const uint32_t p01l = __byte_perm(q.x, q.y, 0x5140), p01h = __byte_perm(q.x, q.y, 0x7362);
-  const uint32_t p23l = __byte_perm(q.z, q.w, 0x5140), p23h = __byte_perm(q.z, q.w, 0x7362);
-  r[0] = __byte_perm(p01l, p23l, 0x5410);
-  r[1] = __byte_perm(p01l, p23l, 0x7632);
-  r[2] = __byte_perm(p01h, p23h, 0x5410);
-  r[3] = __byte_perm(p01h, p23h, 0x7632);
-}
 // limbs[(b * 16 + n) * nlo + x] = byte b of column n of B at row x: n < 8 coefficient n of
 // eq_lo[x], n >= 8 coefficient n - 8 of eq_lo[x - 1] (zero at x = 0).
 __global__ void k_eq_limbs(const ef* __restrict__ eq_lo, int nlo, uint8_t* __restrict__ limbs) {

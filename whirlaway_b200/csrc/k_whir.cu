@@ -7,6 +7,7 @@
 // Equality polynomials over m variables are factored as eq(pt, v) = hi(v_hi) * lo(v_lo)
 // with v_lo the low ll bits, so a table of 2^m entries costs 2^lh + 2^ll to build.
 #include "kernels.h"
+#include "limb_mma.cuh"
 
 namespace wl {
 
@@ -170,6 +171,73 @@ __global__ void k_add_eq_terms_f(ef* __restrict__ w, int lh, int ll, int npts, c
   w[v] = m.value();
 }
 
+// The same on the tensor cores (byte-limb matrix products): the block's rows share v_hi,
+// so B[t][n] = coefficient n of coefs[t] hi_t[v_hi] (its limbs in shared memory,
+// bs[(b * 8 + n) * Kp + t]); each warp's 16 rows v_lo read lo_t[v_lo] (consecutive rows are
+// consecutive words) and own all 16 limb pairs, so every accumulator position is recombined
+// by the lane that holds it.
+constexpr int AEQ_WARPS = 8;
+constexpr int AEQ_MAX_K = 1024;
+__global__ void __launch_bounds__(AEQ_WARPS * 32) k_add_eq_terms_f_mma(ef* __restrict__ w, int lh, int ll, int npts,
+                                                                      int Kp, const uint32_t* __restrict__ hi,
+                                                                      const uint32_t* __restrict__ lo,
+                                                                      const ef* __restrict__ coefs) {
+  extern __shared__ __align__(16) uint8_t bs[];
+  const uint32_t nhi = 1u << lh, nlo = 1u << ll;
+  const uint32_t rows = nlo < AEQ_WARPS * 16 ? nlo : AEQ_WARPS * 16;  // one 16-row tile per warp
+  const uint32_t per_vh = nlo / rows;
+  const uint32_t vh = blockIdx.x / per_vh, xl0 = (blockIdx.x % per_vh) * rows;
+  for (int idx = threadIdx.x; idx < 8 * Kp; idx += blockDim.x) {
+    const int n = idx / Kp, t = idx - n * Kp;
+    const uint32_t v = t < npts ? mul(coefs[t].c[n], hi[size_t(t) * nhi + vh]) : 0u;
+#pragma unroll
+    for (int b = 0; b < 4; b++) bs[(b * 8 + n) * Kp + t] = uint8_t(v >> (8 * b));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  for (uint32_t x0 = xl0 + uint32_t(warp) * 16; x0 < xl0 + rows; x0 += AEQ_WARPS * 16) {  // no barrier in here
+    const uint32_t xa = x0 + g, xb = xa + 8;
+    int acc[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
+    auto ld = [&](int k, uint32_t x) -> uint32_t { return k < npts ? __ldg(lo + size_t(k) * nlo + x) : 0u; };
+#pragma unroll 1
+    for (int k0 = 0; k0 < Kp; k0 += 32) {
+      uint4 q[4];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int kb0 = k0 + 16 * h + 4 * t;
+        q[2 * h] = make_uint4(ld(kb0, xa), ld(kb0 + 1, xa), ld(kb0 + 2, xa), ld(kb0 + 3, xa));
+        q[2 * h + 1] = make_uint4(ld(kb0, xb), ld(kb0 + 1, xb), ld(kb0 + 2, xb), ld(kb0 + 3, xb));
+      }
+      uint32_t l[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) byte_transpose4(q[i], l[i]);
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const uint32_t* col = reinterpret_cast<const uint32_t*>(bs + (b * 8 + g) * Kp + k0) + t;
+        const uint32_t b0 = col[0], b1 = col[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          const uint32_t af[4] = {l[0][a], l[1][a], l[2][a], l[3][a]};
+          mma_u8_16832(acc[a][b], af, b0, b1);
+        }
+      }
+    }
+    // lane (g, t) holds coefficients 2t, 2t + 1 of rows xa (q = 0, 1) and xb (q = 2, 3)
+    uint2* pa = reinterpret_cast<uint2*>(w + (size_t(vh) << ll) + xa) + t;
+    uint2* pb = reinterpret_cast<uint2*>(w + (size_t(vh) << ll) + xb) + t;
+    const uint2 oa = *pa, ob = *pb;
+    *pa = make_uint2(add(oa.x, limb_recombine_lane(acc, 0)), add(oa.y, limb_recombine_lane(acc, 1)));
+    *pb = make_uint2(add(ob.x, limb_recombine_lane(acc, 2)), add(ob.y, limb_recombine_lane(acc, 3)));
+  }
+}
+
 // w[v] += sum_t coefs[t] * hi_t[v_hi] * lo_t[v_lo]   (extension-field points)
 __global__ void k_add_eq_terms_ef(ef* __restrict__ w, int lh, int ll, int npts, const ef* __restrict__ hi,
                                   const ef* __restrict__ lo, const ef* __restrict__ coefs) {
@@ -250,6 +318,14 @@ void launch_add_eq_terms_f(ef* w, int lh, int ll, int npts, const uint32_t* hi, 
                            cudaStream_t s) {
   if (!npts) return;
   size_t n = size_t(1) << (lh + ll);
+  const int Kp = (npts + 31) / 32 * 32;
+  if (ll >= 4 && Kp <= AEQ_MAX_K) {
+    const uint32_t rows = (1u << ll) < AEQ_WARPS * 16 ? (1u << ll) : AEQ_WARPS * 16;
+    k_add_eq_terms_f_mma<<<(unsigned)(n / rows), AEQ_WARPS * 32, size_t(32) * Kp, s>>>(w, lh, ll, npts, Kp, hi, lo,
+                                                                                       coefs);
+    WL_LAUNCH_CHECK();
+    return;
+  }
   k_add_eq_terms_f<<<(unsigned)((n + 255) / 256), 256, sizeof(ef) * npts, s>>>(w, lh, ll, npts, hi, lo, coefs);
   WL_LAUNCH_CHECK();
 }
