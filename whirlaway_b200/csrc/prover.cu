@@ -153,6 +153,7 @@ Context::~Context() {
   for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : event_pool) cudaEventDestroy(e);
   if (sync_event) cudaEventDestroy(sync_event);
+  if (block_event) cudaEventDestroy(block_event);
   cudaFree(twiddles);
   if (part_buf) cudaFree(part_buf);
   cudaFreeHost(pinned);
@@ -216,7 +217,17 @@ void Context::wait_stream() {
     }
     WL_CUDA(e);
   } else {
-    WL_CUDA(cudaStreamSynchronize(stream));
+    // polls for at most block_after_us, then sleeps on an event with blocking sync (a plain
+    // stream synchronisation may spin, and many spinning workers starve the host work of the
+    // others; sleeping at once costs a wake-up on every short wait)
+    if (!block_event) WL_CUDA(cudaEventCreateWithFlags(&block_event, cudaEventDisableTiming | cudaEventBlockingSync));
+    WL_CUDA(cudaEventRecord(block_event, stream));
+    const auto until = w0 + std::chrono::microseconds(block_after_us);
+    cudaError_t e;
+    while ((e = cudaEventQuery(block_event)) == cudaErrorNotReady && std::chrono::steady_clock::now() < until) {
+    }
+    if (e == cudaErrorNotReady) e = cudaEventSynchronize(block_event);
+    WL_CUDA(e);
   }
   host_syncs++;
   host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();

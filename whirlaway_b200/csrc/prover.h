@@ -60,10 +60,11 @@ struct Context {
   void wait_stream();  // host synchronisation with `stream` (counted in host_syncs)
   // How wait_stream waits: true (default) = the host thread polls an event without sleeping,
   // so the OS never has to wake it at the end of a round (blocking waits measured up to
-  // ~20 ms of wake-up stalls per proof); false = blocking cudaStreamSynchronize (server
-  // workers, which would otherwise occupy one CPU each).
+  // ~20 ms of wake-up stalls per proof); false = the thread polls for block_after_us, then
+  // sleeps on a blocking-sync event (server workers, which would otherwise occupy one CPU each).
   bool spin_sync = true;
-  cudaEvent_t sync_event = nullptr;
+  int block_after_us = 500;
+  cudaEvent_t sync_event = nullptr, block_event = nullptr;
   void to_device(void* dst, const void* src, size_t bytes);
   void to_device_impl(void* dst, const void* src, size_t bytes);
   // Freed device buffers of `stream` are kept for reuse by later requests of the same size,

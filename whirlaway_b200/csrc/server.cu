@@ -1,5 +1,6 @@
 // Batched / served proving (see server.h).
 #include <chrono>
+#include <cstdlib>
 
 #include "server.h"
 
@@ -31,6 +32,7 @@ Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), 
   for (int i = 0; i < workers; i++) {
     contexts_.push_back(std::make_unique<Context>(device, hbm_budget));
     contexts_.back()->spin_sync = false;  // workers block: the other workers' proofs fill the device
+    if (const char* v = std::getenv("WL_WORKER_POLL_US")) contexts_.back()->block_after_us = std::atoi(v);
     contexts_.back()->set_cache_limit(0);  // admission counts running proofs only: no cached buffers
   }
   for (int i = 0; i < workers; i++) threads_.emplace_back([this, i] { worker_main(i); });
@@ -136,7 +138,7 @@ void Server::worker_main(int idx) {
       din.reset();
       proof = prove_air(ctx, pj, wit.as<uint32_t>(), nullptr);
       wit.reset();
-      WL_CUDA(cudaStreamSynchronize(ctx.stream));
+      ctx.wait_stream();
     } catch (const std::exception& e) {
       ok = false;
       err = e.what();
