@@ -769,12 +769,20 @@ __device__ __forceinline__ void limb_tile_mma(const uint32_t* pa, const uint32_t
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
   const uint4 zero4 = make_uint4(0, 0, 0, 0);
+  // the next step's values are requested before this step's products (two steps in flight)
+  uint4 n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa)) : zero4;
+  uint4 n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb)) : zero4;
+  uint4 n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + 16)) : zero4;
+  uint4 n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + 16)) : zero4;
 #pragma unroll 1
   for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
-    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
-    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
-    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
-    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
+    const uint4 q0 = n0, q1 = n1, q2 = n2, q3 = n3;
+    if (k0 + 32 < nlo) {
+      n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 32)) : zero4;
+      n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 32)) : zero4;
+      n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 48)) : zero4;
+      n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 48)) : zero4;
+    }
     uint32_t l0[4], l1[4], l2[4], l3[4];
     byte_transpose4(q0, l0);
     byte_transpose4(q1, l1);
@@ -915,12 +923,20 @@ __global__ void __launch_bounds__(CS_WARPS * 32) k_mle_partial_mma(const uint32_
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
   const uint4 zero4 = make_uint4(0, 0, 0, 0);
+  // the next step's values are requested before this step's products (two steps in flight)
+  uint4 n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa)) : zero4;
+  uint4 n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb)) : zero4;
+  uint4 n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + 16)) : zero4;
+  uint4 n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + 16)) : zero4;
 #pragma unroll 1
   for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
-    const uint4 q0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0)) : zero4;
-    const uint4 q1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0)) : zero4;
-    const uint4 q2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 16)) : zero4;
-    const uint4 q3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 16)) : zero4;
+    const uint4 q0 = n0, q1 = n1, q2 = n2, q3 = n3;
+    if (k0 + 32 < nlo) {
+      n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 32)) : zero4;
+      n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 32)) : zero4;
+      n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 48)) : zero4;
+      n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 48)) : zero4;
+    }
     uint32_t l0[4], l1[4], l2[4], l3[4];
     byte_transpose4(q0, l0);
     byte_transpose4(q1, l1);
@@ -998,9 +1014,8 @@ __global__ void __launch_bounds__(CS_WARPS * 32) k_colsum_mma(const uint32_t* __
       for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
   const uint32_t* lw = reinterpret_cast<const uint32_t*>(limbs);
   const int lstride = Kp >> 2;
-#pragma unroll 1
-  for (int k0 = 0; k0 < Kp; k0 += 32) {
-    uint4 q[4];
+  // the next step's values are requested before this step's products (two steps in flight)
+  auto load_step = [&](int k0, uint4 (&q)[4]) {
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const int kb0 = k0 + 16 * h + 4 * t;
@@ -1008,6 +1023,15 @@ __global__ void __launch_bounds__(CS_WARPS * 32) k_colsum_mma(const uint32_t* __
       q[2 * h + 1] =
           make_uint4(load(rb, vb, kb0), load(rb, vb, kb0 + 1), load(rb, vb, kb0 + 2), load(rb, vb, kb0 + 3));
     }
+  };
+  uint4 nq[4];
+  load_step(0, nq);
+#pragma unroll 1
+  for (int k0 = 0; k0 < Kp; k0 += 32) {
+    uint4 q[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) q[i] = nq[i];
+    if (k0 + 32 < Kp) load_step(k0 + 32, nq);
     uint32_t l[4][4];
 #pragma unroll
     for (int i = 0; i < 4; i++) byte_transpose4(q[i], l[i]);

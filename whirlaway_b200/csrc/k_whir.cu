@@ -206,15 +206,23 @@ __global__ void __launch_bounds__(AEQ_WARPS * 32) k_add_eq_terms_f_mma(ef* __res
 #pragma unroll
         for (int q = 0; q < 4; q++) acc[a][b][q] = 0;
     auto ld = [&](int k, uint32_t x) -> uint32_t { return k < npts ? __ldg(lo + size_t(k) * nlo + x) : 0u; };
-#pragma unroll 1
-    for (int k0 = 0; k0 < Kp; k0 += 32) {
-      uint4 q[4];
+    // the next step's values are requested before this step's products (two steps in flight)
+    auto load_step = [&](int k0, uint4 (&q)[4]) {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int kb0 = k0 + 16 * h + 4 * t;
         q[2 * h] = make_uint4(ld(kb0, xa), ld(kb0 + 1, xa), ld(kb0 + 2, xa), ld(kb0 + 3, xa));
         q[2 * h + 1] = make_uint4(ld(kb0, xb), ld(kb0 + 1, xb), ld(kb0 + 2, xb), ld(kb0 + 3, xb));
       }
+    };
+    uint4 nq[4];
+    load_step(0, nq);
+#pragma unroll 1
+    for (int k0 = 0; k0 < Kp; k0 += 32) {
+      uint4 q[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) q[i] = nq[i];
+      if (k0 + 32 < Kp) load_step(k0 + 32, nq);
       uint32_t l[4][4];
 #pragma unroll
       for (int i = 0; i < 4; i++) byte_transpose4(q[i], l[i]);

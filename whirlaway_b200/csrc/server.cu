@@ -1,4 +1,5 @@
 // Batched / served proving (see server.h).
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 
@@ -34,6 +35,24 @@ Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), 
     contexts_.back()->spin_sync = false;  // workers block: the other workers' proofs fill the device
     if (const char* v = std::getenv("WL_WORKER_POLL_US")) contexts_.back()->block_after_us = std::atoi(v);
     contexts_.back()->set_cache_limit(0);  // admission counts running proofs only: no cached buffers
+  }
+  // The budget is reserved in the stream-ordered pool up front (one allocation, freed at once;
+  // the pool keeps it and carves the workers' buffers from it). Growing the pool while proofs
+  // run maps new memory under the driver's lock, which stalled every running proof for
+  // 0.3-2.5 s each time the concurrency reached a new peak.
+  if (hbm_budget) {
+    size_t free_b = 0, total_b = 0;
+    WL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = size_t(2) << 30;
+    const size_t want = std::min<uint64_t>(hbm_budget, free_b > margin ? free_b - margin : 0);
+    cudaStream_t s = contexts_[0]->stream;
+    void* p = nullptr;
+    if (want && cudaMallocAsync(&p, want, s) == cudaSuccess) {
+      WL_CUDA(cudaFreeAsync(p, s));
+      WL_CUDA(cudaStreamSynchronize(s));
+    } else {
+      cudaGetLastError();  // not reserved: the pool grows on demand
+    }
   }
   for (int i = 0; i < workers; i++) threads_.emplace_back([this, i] { worker_main(i); });
 }
