@@ -122,6 +122,20 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                        uint32_t* proof_out, size_t* proof_len, float* round_ms);
 
+/* AirTable::verify (crates/air/src/verify.rs:55-249) on the host CPU: no context, no device.
+ * Checks proof_data (canonical u32 words) against the settings, the constants blob and log_n.
+ * WL_OK when the proof is accepted; otherwise the AirVerifError outcome of the first failed
+ * check (WL_E_INVALID_PCS_COMMITMENT, WL_E_INVALID_PCS_OPENING, WL_E_FS, WL_E_SUMCHECK,
+ * WL_E_SUM_MISMATCH), or WL_E_INVALID_ARG for bad arguments or a word that is not a
+ * canonical field element. */
+wl_status wl_verify(const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
+                    const uint32_t* proof, size_t proof_len);
+/* sumcheck::verify_with_univariate_skip (crates/sumcheck/src/verify.rs:44-69) of a proof from
+ * wl_sumcheck_abc_prove: the round polynomials, the zero claim and the final values a(r),
+ * b(r), c(r) against eq(r, .) * (a * b - c). Host CPU only. */
+wl_status wl_sumcheck_abc_verify(const uint32_t* p16_constants, int32_t log_n, int32_t skips, const uint32_t* proof,
+                                 size_t proof_len);
+
 /* Allocation-free variant of wl_sumcheck_abc_prove_device; it has no counterpart in the
  * reference. For callers that cannot allocate device memory (code running where cudaMalloc is
  * not allowed, such as host callbacks, processes whose device memory another framework has

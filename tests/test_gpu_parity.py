@@ -38,6 +38,7 @@ def test_prove_matches_oracle(oracle, wl, ctx, log_n):
     got = wl.AirTable(ctx, consts, log_n).prove(wit)
     assert got.size == ref.size and np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
     assert oracle.verify(log_n, consts, got) == 0
+    assert wl.verify(consts, log_n, got) == 0  # the product's host verifier
 
 
 def test_prove_device_witness_matches_host_path(oracle, wl, ctx):
@@ -65,4 +66,5 @@ def test_sumcheck_abc_matches_oracle(oracle, wl, ctx, log_n, skips):
     got, ms = wl.sumcheck_abc_prove(ctx, p16, log_n, skips, a, b, c)
     assert np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
     assert oracle.verify_abc(p16, log_n, skips, got) == 0
+    assert wl.sumcheck_abc_verify(p16, log_n, skips, got) == 0
     assert len(ms) == log_n - skips + 1

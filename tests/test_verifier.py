@@ -1,0 +1,104 @@
+"""The product's host verifier (wl_verify, wl_sumcheck_abc_verify) on CPU, against proofs the
+oracle prover makes: honest proofs are accepted, corrupted ones rejected with the
+AirVerifError outcome of crates/air/src/verify.rs, and the oracle's own verifier agrees on
+acceptance."""
+import numpy as np
+import pytest
+
+P = 0x7F000001
+OK, COMMITMENT, OPENING, FS, SUMCHECK, SUM_MISMATCH = 0, 11, 12, 13, 14, 16
+
+
+def honest(oracle, log_n, settings=None):
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    proof, _ = oracle.prove(log_n, consts, wit, settings)
+    return consts, wit, proof
+
+
+@pytest.mark.parametrize("log_n", [5, 7, 9])
+def test_accepts_honest_proofs(wl, oracle, log_n):
+    consts, _, proof = honest(oracle, log_n)
+    assert oracle.verify(log_n, consts, proof) == 0
+    assert wl.verify(consts, log_n, proof) == OK
+
+
+def test_settings_and_sizes_must_match(wl, oracle):
+    log_n = 6
+    consts, _, proof = honest(oracle, log_n)
+    assert wl.verify(consts, log_n, proof) == OK
+    assert wl.verify(consts, log_n + 1, proof) != OK              # other height
+    assert wl.verify(consts, log_n, proof, wl.AirSettings(univariate_skips=3)) != OK
+    other = consts.copy()
+    other[200] = (int(other[200]) + 1) % P                        # other Poseidon16 constant
+    assert wl.verify(other, log_n, proof) != OK
+    other = consts.copy()
+    other[5] = (int(other[5]) + 1) % P                            # other AIR round constant
+    assert wl.verify(other, log_n, proof) != OK
+
+
+def test_rejects_corrupted_words(wl, oracle):
+    log_n = 6
+    consts, _, proof = honest(oracle, log_n)
+    rng = np.random.default_rng(3)
+    positions = sorted(set([0, 3, 8, 20, 200, 1000, proof.size // 2, proof.size - 5, proof.size - 1]
+                           + list(rng.integers(0, proof.size, 24))))
+    for pos in positions:
+        bad = proof.copy()
+        bad[pos] = (int(bad[pos]) + 1) % P
+        got = wl.verify(consts, log_n, bad)
+        assert got != OK, pos
+        assert (oracle.verify(log_n, consts, bad) != 0), pos
+    # the root and the OOD answers belong to the commitment; the transcript changes after them
+    bad = proof.copy()
+    bad[0] = (int(bad[0]) + 1) % P
+    assert wl.verify(consts, log_n, bad) in (SUMCHECK, SUM_MISMATCH, FS, OPENING)
+
+
+def test_rejects_truncated_and_padded_proofs(wl, oracle):
+    log_n = 5
+    consts, _, proof = honest(oracle, log_n)
+    assert wl.verify(consts, log_n, proof[:-1]) == OPENING         # the last Merkle path is short
+    assert wl.verify(consts, log_n, proof[:4]) == COMMITMENT       # the root is incomplete
+    assert wl.verify(consts, log_n, np.concatenate([proof, np.zeros(1, np.uint32)])) == FS
+    assert wl.verify(consts, log_n, np.zeros(0, np.uint32)) == COMMITMENT
+
+
+def test_rejects_non_canonical_words(wl, oracle):
+    log_n = 5
+    consts, _, proof = honest(oracle, log_n)
+    bad = proof.copy()
+    bad[10] = P + int(bad[10]) % 7  # same residue class, not canonical
+    assert wl.verify(consts, log_n, bad) == 1
+
+
+def test_rejects_proof_of_invalid_trace(wl, oracle):
+    log_n = 6
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    wit[(20 << log_n) + 7] ^= 1  # break one post-round state
+    proof, _ = oracle.prove(log_n, consts, wit)
+    assert oracle.verify(log_n, consts, proof) != 0
+    assert wl.verify(consts, log_n, proof) == SUM_MISMATCH
+
+
+def test_abc_verifier(wl, oracle):
+    rng = np.random.default_rng(4)
+    consts, _ = oracle.workload(2)
+    p16 = consts[148:296]
+    for log_n, skips in ((8, 3), (10, 4), (6, 1)):
+        a = rng.integers(0, P, 1 << log_n, dtype=np.uint64)
+        b = rng.integers(0, P, 1 << log_n, dtype=np.uint64)
+        c = (a * b) % P
+        a, b, c = (x.astype(np.uint32) for x in (a, b, c))
+        proof = oracle.prove_abc(p16, log_n, skips, a, b, c)
+        assert wl.sumcheck_abc_verify(p16, log_n, skips, proof) == OK
+        bad = proof.copy()
+        bad[9] = (int(bad[9]) + 1) % P
+        assert wl.sumcheck_abc_verify(p16, log_n, skips, bad) != OK
+        bad = proof.copy()
+        bad[-1] = (int(bad[-1]) + 1) % P  # a final value
+        assert wl.sumcheck_abc_verify(p16, log_n, skips, bad) == SUM_MISMATCH
+        c2 = c.copy()
+        c2[5] ^= 1
+        assert wl.sumcheck_abc_verify(p16, log_n, skips, oracle.prove_abc(p16, log_n, skips, a, b, c2)) != OK

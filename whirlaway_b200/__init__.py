@@ -99,6 +99,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_sumcheck_abc_prove_noalloc": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, _u32p,
                                                          _sizep, vp]),
         "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
+        "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
+        "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_server_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]),
         "wl_server_destroy": (None, [vp]),
         "wl_server_last_error": (ctypes.c_char_p, [vp]),
@@ -345,6 +347,22 @@ def sumcheck_abc_prove_noalloc(p16_constants: np.ndarray, log_n: int, skips: int
     if st:
         raise ProverError(st, "sumcheck_abc_prove_noalloc")
     return out[: n.value].copy()
+
+
+def verify(constants: np.ndarray, log_n: int, proof: np.ndarray, settings: AirSettings = AirSettings()) -> int:
+    """AirTable::verify on the host CPU (no device): 0 when the proof is accepted, else the
+    verifier status (11 commitment, 12 opening, 13 Fiat-Shamir, 14 sumcheck, 16 sum mismatch;
+    1 for bad arguments)."""
+    c = np.ascontiguousarray(constants, dtype=np.uint32)
+    pr = np.ascontiguousarray(proof, dtype=np.uint32)
+    return load_library().wl_verify(ctypes.byref(settings._c()), _ptr(c), log_n, _ptr(pr), pr.size)
+
+
+def sumcheck_abc_verify(p16_constants: np.ndarray, log_n: int, skips: int, proof: np.ndarray) -> int:
+    """Verifies a sumcheck_abc_prove proof on the host CPU; 0 when accepted."""
+    c = np.ascontiguousarray(p16_constants, dtype=np.uint32)
+    pr = np.ascontiguousarray(proof, dtype=np.uint32)
+    return load_library().wl_sumcheck_abc_verify(_ptr(c), log_n, skips, _ptr(pr), pr.size)
 
 
 def proof_footprint_bytes(log_n: int) -> int:

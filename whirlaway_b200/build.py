@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libwhirlaway_b200.so")
-SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_probe.cu", "prover.cu", "server.cu", "noalloc.cu", "capi.cu",
+SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_probe.cu", "prover.cu", "server.cu", "noalloc.cu", "verifier.cu", "capi.cu",
            "host_perm.cpp"]
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC"]  # host-only sources (g++; CPU features dispatched at run time)
 NVCC_FLAGS = [

@@ -114,9 +114,10 @@ __device__ __forceinline__ void air_eval_f(const AirConsts& K, Get&& get, Acc&& 
   }
 }
 
-// Extension-field constraint evaluation: returns sum_i alpha^i * h_i.
+// Extension-field constraint evaluation: returns sum_i alpha^i * h_i (device kernels and the
+// host verifier).
 template <class Get>
-__device__ __forceinline__ kb::ef air_eval_ef(const AirConsts& K, const kb::ef* alphas, Get&& get) {
+__host__ __device__ __forceinline__ kb::ef air_eval_ef(const AirConsts& K, const kb::ef* alphas, Get&& get) {
   using namespace kb;
   ef s[16];
 #pragma unroll

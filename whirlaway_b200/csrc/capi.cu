@@ -7,6 +7,7 @@
 #include "../../include/whirlaway_b200.h"
 #include "prover.h"
 #include "server.h"
+#include "verifier.h"
 
 struct wl_ctx {
   std::unique_ptr<wl::Context> c;
@@ -301,6 +302,31 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16c, int32_
                                        const uint32_t* a, const uint32_t* b, const uint32_t* c, uint32_t* proof_out,
                                        size_t* proof_len, float* round_ms) {
   return abc_common(ctx, p16c, log_n, skips, a, b, c, true, proof_out, proof_len, round_ms);
+}
+
+// Host-only verifiers: no context, no device.
+wl_status wl_verify(const wl_air_settings* s, const uint32_t* constants, int32_t log_n, const uint32_t* proof,
+                    size_t proof_len) {
+  std::string why;
+  if (!constants || (!proof && proof_len) || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
+  for (size_t i = 0; i < proof_len; i++)
+    if (proof[i] >= kb::P) return WL_E_INVALID_ARG;  // not a canonical field element
+  return guarded(nullptr, [&] {
+    wl::ProofJob job = make_job(s, constants, log_n);
+    return wl_status(wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len));
+  });
+}
+
+wl_status wl_sumcheck_abc_verify(const uint32_t* p16c, int32_t log_n, int32_t skips, const uint32_t* proof,
+                                 size_t proof_len) {
+  if (!p16c || (!proof && proof_len) || log_n < 2 || log_n > 26 || skips < 1 || skips > 4 || skips >= log_n)
+    return WL_E_INVALID_ARG;
+  for (size_t i = 0; i < proof_len; i++)
+    if (proof[i] >= kb::P) return WL_E_INVALID_ARG;
+  return guarded(nullptr, [&] {
+    const kb::P16Consts p16 = wl::perm_consts_from<16>(p16c);
+    return wl_status(wl::verify_abc_proof(p16, log_n, skips, proof, proof_len));
+  });
 }
 
 wl_status wl_profile_enable(wl_ctx* ctx, int32_t on) {

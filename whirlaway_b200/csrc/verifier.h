@@ -1,0 +1,26 @@
+// Host-side verifiers of the AIR proof and of the a*b - c zerocheck proof (verifier.cu).
+#pragma once
+#include <array>
+#include <cstddef>
+#include <cstdint>
+
+#include "host.h"
+
+namespace wl {
+
+// Outcomes, valued as the C ABI's verifier statuses (AirVerifError, crates/air/src/verify.rs:26-34).
+enum VerifyOutcome : int {
+  VERIFY_OK = 0,
+  VERIFY_PCS_COMMITMENT = 11,
+  VERIFY_PCS_OPENING = 12,
+  VERIFY_FS = 13,
+  VERIFY_SUMCHECK = 14,
+  VERIFY_SUM_MISMATCH = 16,
+};
+
+// proof: proof_data as canonical u32 words; constants in Montgomery form.
+int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
+                     int log_n, const uint32_t* proof, size_t proof_len);
+int verify_abc_proof(const kb::P16Consts& p16, int log_n, int skips, const uint32_t* proof, size_t proof_len);
+
+}  // namespace wl
