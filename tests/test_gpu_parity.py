@@ -41,6 +41,18 @@ def test_prove_matches_oracle(oracle, wl, ctx, log_n):
     assert wl.verify(consts, log_n, got) == 0  # the product's host verifier
 
 
+@pytest.mark.parametrize("log_n,skips", [(8, 1), (8, 2), (9, 3), (6, 3)])
+def test_prove_other_skips_matches_oracle(oracle, wl, ctx, log_n, skips):
+    """Univariate skips below 4: fewer round-0 points (2, 6, 14) than the 30 of the default."""
+    settings = wl.AirSettings(univariate_skips=skips)
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    ref, _ = oracle.prove(log_n, consts, wit, settings.as_array())
+    got = wl.AirTable(ctx, consts, log_n, settings).prove(wit)
+    assert got.size == ref.size and np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
+    assert wl.verify(consts, log_n, got, settings) == 0
+
+
 def test_prove_device_witness_matches_host_path(oracle, wl, ctx):
     log_n = 9
     consts, inputs = oracle.workload(log_n, 3)

@@ -91,7 +91,7 @@ __global__ void k_reduce_partials(const ef* __restrict__ partial, int nblk, int 
 }
 
 // ------------------------------------------------------------------ AIR zerocheck
-constexpr int ZC0_X = 32, ZC0_Z = 15;
+constexpr int ZC0_X = 32;
 constexpr int ZC0_STAGES = 2;   // input groups in flight
 constexpr int ZC0_GROUP = 8;    // inputs per staged group (one block barrier per group)
 constexpr int ZC0_PAD = 20;     // words per x in a staged column tile (16 values + padding)
@@ -207,40 +207,67 @@ __global__ void __launch_bounds__(ZC0R_THREADS) k_zc0_rows(const uint32_t* __res
   }
 }
 
-// Thread (x, z): the 148 cube inputs are extended from their values at rows j S + x, j < 2^k,
-// to the point z by the Lagrange weights L_j(z), cubed and weighted by gamma; the sum is
-// weighted by eq[x]. A warp holds 32 consecutive x for one z. The 2^k x 32 values of each
-// input are staged in shared memory by a cp.async pipeline, ZC0_GROUP inputs per stage (one
-// block barrier per group), and the extension reads shared memory only. Every thread stages
-// the same (j, x) entries of every input, so their offsets are formed once; the weights of
-// j >= 2^k are zero, so the extension always takes 16 products (the unstaged entries are
-// multiplied by zero).
-__global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* __restrict__ wit,
-                                                               const uint32_t* __restrict__ q, int log_n, int k,
-                                                               int nz, const uint32_t* __restrict__ lw,
-                                                               const ef* __restrict__ eq,
-                                                               const ef* __restrict__ alphas_g,
-                                                               const ef* __restrict__ betas_g,
-                                                               const __grid_constant__ AirConsts K,
-                                                               ef* __restrict__ partial) {
+// The 148 cube inputs of every row x are extended from their values at rows j S + x, j < 2^k,
+// to the points z by the Lagrange weights L_j(z), cubed, weighted by gamma and summed, weighted
+// by eq[x]. The extension runs on the tensor cores: sum_j L_j(z) v_j(x) is an exact modular
+// dot product over j, computed as a byte-limb integer matrix product whose rows are x, whose
+// reduction index is (j, a) for the 16 points j and the 4 bytes a of v_j(x), and whose
+// columns are (z, b) for the 4 bytes b of M(j, z, a) = the Montgomery form of L_j(z) 2^(8a).
+// The reduction index needs no byte shuffling: the staged words [x][j] are the A operand as
+// they lie (byte a of word j is k = 4j + a). With acc_b = sum_(j,a) v_(j,a) M_b(j, z, a) below
+// 2^22, v = sum_b acc_b 2^(8b) < 2^46 is congruent to (sum_j v_j L_j(z)) R^2, so one Montgomery
+// reduction (with the round constant in the high word) gives the cube input in Montgomery form.
+// A block holds 32 x (two 16-row tiles) and the z-octets of all points; warp (tile, octet)
+// issues 4 n8 tiles (b = 0..3) per k32 step, so each lane ends with all limbs of 4 (x, z)
+// sums, and the B fragments (16 words per lane) depend on z only. The 16 x 32 values of each
+// input are staged in shared memory by a cp.async pipeline, ZC0_GROUP inputs per stage; the
+// weights of j >= 2^k are zero, so unstaged entries contribute nothing.
+constexpr int ZC0M_WARPS = 8;  // 2 x-tiles x 4 z-octets (30 points)
+__global__ void __launch_bounds__(ZC0M_WARPS * 32, 2) k_zc0_eval_mma(const uint32_t* __restrict__ wit,
+                                                                    const uint32_t* __restrict__ q, int log_n,
+                                                                    int k, int nz, const uint32_t* __restrict__ lw,
+                                                                    const ef* __restrict__ eq,
+                                                                    const ef* __restrict__ alphas_g,
+                                                                    const ef* __restrict__ betas_g,
+                                                                    const __grid_constant__ AirConsts K,
+                                                                    ef* __restrict__ partial) {
   __shared__ ef gam[AIR_NC];
   __shared__ uint32_t rcs[AIR_NC];
   __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_GROUP][ZC0_X * ZC0_PAD];
-  const int tid = threadIdx.y * ZC0_X + threadIdx.x;
-  constexpr int NT = ZC0_X * ZC0_Z;
+  __shared__ ef red[4][8];  // per z-octet and point: the sum over the second x-tile
+  constexpr int NT = ZC0M_WARPS * 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3, mt = warp & 1, zo = warp >> 1;
   for (int i = tid; i < AIR_NC; i += NT) {
     gam[i] = i < 64 ? betas_g[i] : (i < 84 ? alphas_g[i] : betas_g[i - 20]);
     rcs[i] = zc0_rc(K, i);
   }
-  const int zi = blockIdx.y * ZC0_Z + threadIdx.y;
   const int nsk = 1 << k;
   const size_t N = size_t(1) << log_n;
   const size_t S = N >> k;
   const size_t x0 = size_t(blockIdx.x) * ZC0_X;
-  const size_t x = x0 + threadIdx.x;
-  uint32_t w[16];
+  const bool zwarp = zo * 8 < nz;  // warps of octets past the last point only stage
+
+  // B fragments: bf[b][kk][h] packs, in byte a, byte b of M(j, z, a) for j = 8 kk + 4 h + t
+  // and z = 8 zo + g (the lane's B column)
+  uint32_t bf[4][2][2];
+  {
+    const int z = zo * 8 + g;
 #pragma unroll
-  for (int j = 0; j < 16; j++) w[j] = (zi < nz && j < nsk) ? lw[zi * nsk + j] : 0u;
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = 8 * kk + 4 * h + t;
+        const uint32_t L = (z < nz && j < nsk) ? lw[z * nsk + j] : 0u;
+        uint32_t m[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) m[a] = kb::mul(L, uint32_t(kb::detail::cpow(2, 8 * a + 32)));
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+          bf[b][kk][h] = ((m[0] >> (8 * b)) & 0xffu) | (((m[1] >> (8 * b)) & 0xffu) << 8) |
+                         (((m[2] >> (8 * b)) & 0xffu) << 16) | (((m[3] >> (8 * b)) & 0xffu) << 24);
+      }
+  }
 
   // staged entries of this thread: e = tid, tid + NT of the 16 x 32 (j, x) grid; source row
   // j S + x (the up row for committed columns differs only at row N - 1)
@@ -258,14 +285,14 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* _
     slast[e] = size_t(j) * S + xx == N - 1;
     sdst[e] = uint32_t(xl * ZC0_PAD + j);
   }
-  auto issue = [&](int g) {
+  auto issue = [&](int grp) {
 #pragma unroll
     for (int cc = 0; cc < ZC0_GROUP; cc++) {
-      const int i = ZC0_GROUP * g + cc;
+      const int i = ZC0_GROUP * grp + cc;
       if (i < AIR_NC) {
         const int qc = zc0_qcol(i);
         const uint32_t* col = qc >= 0 ? q + size_t(qc) * N : wit + size_t(1 + i) * N;
-        uint32_t* dst = tile[g % ZC0_STAGES][cc];
+        uint32_t* dst = tile[grp % ZC0_STAGES][cc];
 #pragma unroll
         for (int e = 0; e < NE; e++)
           if (sval[e]) cp_async4(dst + sdst[e], col + (srow[e] - uint32_t(slast[e] && qc < 0)));
@@ -273,45 +300,84 @@ __global__ void __launch_bounds__(ZC0_X * ZC0_Z, 2) k_zc0_eval(const uint32_t* _
     }
     cp_async_commit();
   };
-  for (int g = 0; g < ZC0_STAGES - 1; g++) issue(g);
-  EfMacF m;
-  m.init();
+  for (int grp = 0; grp < ZC0_STAGES - 1; grp++) issue(grp);
+  EfMacF m[4];  // (x, z) = (g, 2t), (g, 2t + 1), (g + 8, 2t), (g + 8, 2t + 1) of the warp's tile
+#pragma unroll
+  for (int o = 0; o < 4; o++) m[o].init();
   constexpr int NG = (AIR_NC + ZC0_GROUP - 1) / ZC0_GROUP;
   static_assert(ZC0_GROUP % 4 == 0 && AIR_NC % 4 == 0, "flushes after every 4 products");
 #pragma unroll 1
-  for (int g = 0; g < NG; g++) {
+  for (int grp = 0; grp < NG; grp++) {
     cp_async_wait<ZC0_STAGES - 2>();
-    __syncthreads();  // group g landed for every thread; the slot of group g - 1 is free
-    issue(g + ZC0_STAGES - 1);
-#pragma unroll 4
-    for (int cc = 0; cc < ZC0_GROUP; cc++) {
-      const int i = ZC0_GROUP * g + cc;
-      if (i >= AIR_NC) break;  // the last group is partial
-      const uint4* row = reinterpret_cast<const uint4*>(tile[g % ZC0_STAGES][cc] + threadIdx.x * ZC0_PAD);
-      // two chains of 8 products, folded with 2^32 = 2^25 - 2 (mod p) after every 4 (below
-      // 2^57 + 2^32 each); the round constant enters the high word (rc 2^32 reduces to rc),
-      // and one Montgomery reduction of the total (below 2^63 < 4 p^2) follows
-      uint64_t sa = 0, sb = 0;
+    __syncthreads();  // group grp landed for every thread; the slot of group grp - 1 is free
+    issue(grp + ZC0_STAGES - 1);
+    if (zwarp) {
+#pragma unroll 2
+      for (int cc = 0; cc < ZC0_GROUP; cc++) {
+        const int i = ZC0_GROUP * grp + cc;
+        if (i >= AIR_NC) break;  // the last group is partial
+        const uint32_t* r0 = tile[grp % ZC0_STAGES][cc] + (16 * mt + g) * ZC0_PAD;
+        const uint32_t* r1 = r0 + 8 * ZC0_PAD;
+        int acc[4][4];
 #pragma unroll
-      for (int qq = 0; qq < 4; qq++) {
-        const uint4 v = row[qq];
-        uint64_t& acc = (qq & 1) ? sb : sa;
-        acc += wmul(w[4 * qq], v.x);
-        acc += wmul(w[4 * qq + 1], v.y);
-        acc += wmul(w[4 * qq + 2], v.z);
-        acc += wmul(w[4 * qq + 3], v.w);
-        acc = uint64_t(uint32_t(acc >> 32)) * ((1u << 25) - 2) + uint32_t(acc);
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int o = 0; o < 4; o++) acc[b][o] = 0;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++) {
+          const uint32_t af[4] = {r0[8 * kk + t], r1[8 * kk + t], r0[8 * kk + t + 4], r1[8 * kk + t + 4]};
+#pragma unroll
+          for (int b = 0; b < 4; b++) mma_u8_16832(acc[b], af, bf[b][kk][0], bf[b][kk][1]);
+        }
+        const uint64_t rc_hi = uint64_t(rcs[i]) << 32;
+        const ef& gm = gam[i];
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+          const uint32_t lo = uint32_t(acc[0][o]) + (uint32_t(acc[1][o]) << 8);  // < 2^31
+          const uint32_t hi = uint32_t(acc[2][o]) + (uint32_t(acc[3][o]) << 8);  // < 2^31
+          const uint32_t u = kb::redc(uint64_t(lo) + (uint64_t(hi) << 16) + rc_hi);
+          m[o].mac(gm, kb::cube(u));
+        }
+        if ((cc & 3) == 3) {
+#pragma unroll
+          for (int o = 0; o < 4; o++) m[o].flush();
+        }
       }
-      const uint32_t u = redc(sa + sb + (uint64_t(rcs[i]) << 32));
-      m.mac(gam[i], cube(u));
-      if ((cc & 3) == 3) m.flush();
     }
   }
   cp_async_wait<0>();
-  const bool active = zi < nz && x < S;
-  ef res = active ? ef_mul(m.value(), eq[x]) : ef_zero();
-  res = warp_reduce_ef(res);
-  if (threadIdx.x == 0 && zi < nz) partial[size_t(blockIdx.x) * nz + zi] = res;
+  // weight by eq[x], sum over the 16 x of the tile (lanes of equal t), then over the two tiles
+  ef sz[2];
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    ef acc = ef_zero();
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const size_t x = x0 + 16 * mt + g + 8 * hh;
+      const ef v = m[2 * hh + c].value();
+      if (zwarp && x < S) acc = ef_add(acc, ef_mul(v, eq[x]));
+    }
+#pragma unroll
+    for (int d = 4; d < 32; d <<= 1) {
+      ef o;
+#pragma unroll
+      for (int w = 0; w < 8; w++) o.c[w] = __shfl_xor_sync(0xffffffffu, acc.c[w], d);
+      acc = ef_add(acc, o);
+    }
+    sz[c] = acc;
+  }
+  if (mt == 1 && g == 0) {
+    red[zo][2 * t] = sz[0];
+    red[zo][2 * t + 1] = sz[1];
+  }
+  __syncthreads();
+  if (mt == 0 && g == 0) {
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const int z = zo * 8 + 2 * t + c;
+      if (z < nz) partial[size_t(blockIdx.x) * nz + z] = ef_add(sz[c], red[zo][2 * t + c]);
+    }
+  }
 }
 
 // out[c * S + x] = sum_j sel[j] * up_c[j * S + x] for two adjacent x per thread (8-byte
@@ -1302,8 +1368,9 @@ void launch_zc0_fold_ef(const ef* a, int log_n, int k, const ef* sel, ef* out, c
 void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, int nz, const uint32_t* lw,
                      const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K, ef* partial,
                      cudaStream_t s) {
-  dim3 grid(zc0_blocks(log_n, k), (nz + ZC0_Z - 1) / ZC0_Z), block(ZC0_X, ZC0_Z);
-  k_zc0_eval<<<grid, block, 0, s>>>(wit, q, log_n, k, nz, lw, eq, alphas, betas, K, partial);
+  if (nz > 32) throw std::invalid_argument("zc0_eval: at most 32 points");
+  k_zc0_eval_mma<<<zc0_blocks(log_n, k), ZC0M_WARPS * 32, 0, s>>>(wit, q, log_n, k, nz, lw, eq, alphas, betas, K,
+                                                                  partial);
   WL_LAUNCH_CHECK();
 }
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {
