@@ -380,43 +380,107 @@ __global__ void __launch_bounds__(ZC0M_WARPS * 32, 2) k_zc0_eval_mma(const uint3
   }
 }
 
-// out[c * S + x] = sum_j sel[j] * up_c[j * S + x] for two adjacent x per thread (8-byte
-// loads; the 2^k loads are issued before the products, sel is zero-padded to 16). The up
-// row of 2^k S - 1 is 2^k S - 2, patched for the last pair.
-__global__ void k_zc0_fold(const uint32_t* __restrict__ wit, int log_n, int k, const ef* __restrict__ sel_g,
-                           ef* __restrict__ out) {
-  __shared__ ef sel[16];
+// out[c * S + x] = sum_j sel[j] * up_c[j * S + x] for every column c, on the tensor cores as
+// in k_zc0_eval_mma: rows x, reduction index (j, a) over the 16 points and the 4 bytes of
+// up_c[j S + x] (the staged [x][j] words as they lie), columns (n, b) for the 8 coefficients n
+// of sel[j] and the 4 bytes b of the Montgomery form of sel[j]_n 2^(8a). Each lane ends with
+// all limbs of coefficients 2t, 2t + 1 of rows g, g + 8; one Montgomery reduction each. A
+// block holds 32 x and walks the columns in staged groups of ZC0_GROUP; warp (tile, slot)
+// takes columns slot and slot + 4 of each group. The up row of row N - 1 is N - 2.
+__global__ void __launch_bounds__(ZC0M_WARPS * 32) k_zc0_fold_mma(const uint32_t* __restrict__ wit, int log_n,
+                                                                 int k, const ef* __restrict__ sel,
+                                                                 ef* __restrict__ out) {
+  __shared__ __align__(16) uint32_t tile[ZC0_STAGES][ZC0_GROUP][ZC0_X * ZC0_PAD];
+  constexpr int NT = ZC0M_WARPS * 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3, mt = warp & 1, slot = warp >> 1;
   const int nsk = 1 << k;
-  if (threadIdx.x < 16) sel[threadIdx.x] = threadIdx.x < (unsigned)nsk ? sel_g[threadIdx.x] : ef_zero();
-  __syncthreads();
-  const size_t N = size_t(1) << log_n, S = N >> k;
-  const size_t x = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
-  const int c = blockIdx.y;
-  if (x >= S) return;
-  const uint32_t* col = wit + size_t(c) * N;
-  uint2 v[16];
+  const size_t N = size_t(1) << log_n;
+  const size_t S = N >> k;
+  const size_t x0 = size_t(blockIdx.x) * ZC0_X;
+  // B fragments: bf[b][kk][h] packs, in byte a, byte b of the Montgomery form of
+  // sel[j]_n 2^(8a) for j = 8 kk + 4 h + t and coefficient n = g (the lane's B column)
+  uint32_t bf[4][2][2];
 #pragma unroll
-  for (int j = 0; j < 16; j++)
-    v[j] = j < nsk ? __ldg(reinterpret_cast<const uint2*>(col + size_t(j) * S + x)) : make_uint2(0, 0);
-  if (x + 2 == S) {
+  for (int kk = 0; kk < 2; kk++)
 #pragma unroll
-    for (int j = 0; j < 16; j++)
-      if (j == nsk - 1) v[j].y = col[N - 2];
+    for (int h = 0; h < 2; h++) {
+      const int j = 8 * kk + 4 * h + t;
+      const uint32_t v = j < nsk ? sel[j].c[g] : 0u;
+      uint32_t m[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) m[a] = kb::mul(v, uint32_t(kb::detail::cpow(2, 8 * a + 32)));
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+        bf[b][kk][h] = ((m[0] >> (8 * b)) & 0xffu) | (((m[1] >> (8 * b)) & 0xffu) << 8) |
+                       (((m[2] >> (8 * b)) & 0xffu) << 16) | (((m[3] >> (8 * b)) & 0xffu) << 24);
+    }
+  constexpr int NE = (16 * ZC0_X + NT - 1) / NT;
+  uint32_t srow[NE], sdst[NE];
+  bool sval[NE];
+#pragma unroll
+  for (int e = 0; e < NE; e++) {
+    const int idx = tid + e * NT;
+    const int j = idx / ZC0_X, xl = idx % ZC0_X;
+    size_t xx = x0 + xl;
+    if (xx >= S) xx = 0;
+    sval[e] = idx < 16 * ZC0_X && j < nsk;
+    const size_t row = size_t(j) * S + xx;
+    srow[e] = uint32_t(row == N - 1 ? N - 2 : row);
+    sdst[e] = uint32_t(xl * ZC0_PAD + j);
   }
-  EfMacF m0, m1;
-  m0.init();
-  m1.init();
+  auto issue = [&](int grp) {
 #pragma unroll
-  for (int j = 0; j < 16; j++) {
-    m0.mac(sel[j], v[j].x);
-    m1.mac(sel[j], v[j].y);
-    if ((j & 3) == 3) {
-      m0.flush();
-      m1.flush();
+    for (int cc = 0; cc < ZC0_GROUP; cc++) {
+      const int c = ZC0_GROUP * grp + cc;
+      if (c < AIR_W) {
+        const uint32_t* col = wit + size_t(c) * N;
+        uint32_t* dst = tile[grp % ZC0_STAGES][cc];
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+          if (sval[e]) cp_async4(dst + sdst[e], col + srow[e]);
+      }
+    }
+    cp_async_commit();
+  };
+  for (int grp = 0; grp < ZC0_STAGES - 1; grp++) issue(grp);
+  constexpr int NG = (AIR_W + ZC0_GROUP - 1) / ZC0_GROUP;
+  const size_t xa = x0 + 16 * mt + g, xb = xa + 8;
+#pragma unroll 1
+  for (int grp = 0; grp < NG; grp++) {
+    cp_async_wait<ZC0_STAGES - 2>();
+    __syncthreads();  // group grp landed for every thread; the slot of group grp - 1 is free
+    issue(grp + ZC0_STAGES - 1);
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int cc = slot + 4 * r;
+      const int c = ZC0_GROUP * grp + cc;
+      if (c >= AIR_W) break;
+      const uint32_t* r0 = tile[grp % ZC0_STAGES][cc] + (16 * mt + g) * ZC0_PAD;
+      const uint32_t* r1 = r0 + 8 * ZC0_PAD;
+      int acc[4][4];
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int o = 0; o < 4; o++) acc[b][o] = 0;
+#pragma unroll
+      for (int kk = 0; kk < 2; kk++) {
+        const uint32_t af[4] = {r0[8 * kk + t], r1[8 * kk + t], r0[8 * kk + t + 4], r1[8 * kk + t + 4]};
+#pragma unroll
+        for (int b = 0; b < 4; b++) mma_u8_16832(acc[b], af, bf[b][kk][0], bf[b][kk][1]);
+      }
+      uint32_t res[4];
+#pragma unroll
+      for (int o = 0; o < 4; o++) {
+        const uint32_t lo = uint32_t(acc[0][o]) + (uint32_t(acc[1][o]) << 8);  // < 2^31
+        const uint32_t hi = uint32_t(acc[2][o]) + (uint32_t(acc[3][o]) << 8);  // < 2^31
+        res[o] = kb::redc(uint64_t(lo) + (uint64_t(hi) << 16));
+      }
+      if (xa < S) reinterpret_cast<uint2*>(out + size_t(c) * S + xa)[t] = make_uint2(res[0], res[1]);
+      if (xb < S) reinterpret_cast<uint2*>(out + size_t(c) * S + xb)[t] = make_uint2(res[2], res[3]);
     }
   }
-  out[size_t(c) * S + x] = m0.value();
-  out[size_t(c) * S + x + 1] = m1.value();
+  cp_async_wait<0>();
 }
 
 // out[x] = sum_j sel[j] * a[j * S + x] for an extension-field table a that is already read at
@@ -1376,8 +1440,7 @@ void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, i
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s) {
   size_t S = size_t(1) << (log_n - k);
   if (S < 2) throw std::invalid_argument("zc0_fold: at least 2 points per skip block");
-  dim3 grid((unsigned)((S / 2 + 255) / 256), AIR_W);
-  k_zc0_fold<<<grid, 256, 0, s>>>(wit, log_n, k, sel, out);
+  k_zc0_fold_mma<<<zc0_blocks(log_n, k), ZC0M_WARPS * 32, 0, s>>>(wit, log_n, k, sel, out);
   WL_LAUNCH_CHECK();
 }
 // Rounds with at least ZC_DENSE_MIN_HALF points per z use the dense kernels.
