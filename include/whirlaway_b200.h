@@ -130,6 +130,22 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
  * canonical field element. */
 wl_status wl_verify(const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
                     const uint32_t* proof, size_t proof_len);
+/* Per-phase transcript dumps, for diffing against another implementation of the protocol (a
+ * build of the reference with the same parameters): JSON text
+ *   {"proof_len": L, "events": [{"kind", "phase", "offset", "values"}, ...]}
+ * with one "phase" event where each phase (commit, batching, zerocheck, inner_sums,
+ * inner_sumcheck, whir, whir_round_i, whir_final) starts in proof_data, and every "challenge"
+ * (8 canonical words), "queries" batch (sorted distinct indices) and "grinding" witness, each
+ * with the proof_data offset at which it is drawn. *len is the buffer capacity on entry and the
+ * bytes needed (with the terminating NUL) on return; WL_E_BUFFER_TOO_SMALL when short.
+ * wl_ctx_set_transcript_dump(ctx, 1) makes every later proof on ctx record its dump;
+ * wl_transcript_dump returns the last one. wl_verify_transcript runs wl_verify and returns the
+ * transcript as the verifier reads it (up to the first failed check) with the verify status. */
+wl_status wl_ctx_set_transcript_dump(wl_ctx* ctx, int32_t on);
+wl_status wl_transcript_dump(wl_ctx* ctx, char* buf, size_t* len);
+wl_status wl_verify_transcript(const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
+                               const uint32_t* proof, size_t proof_len, char* buf, size_t* len);
+
 /* sumcheck::verify_with_univariate_skip (crates/sumcheck/src/verify.rs:44-69) of a proof from
  * wl_sumcheck_abc_prove: the round polynomials, the zero claim and the final values a(r),
  * b(r), c(r) against eq(r, .) * (a * b - c). Host CPU only. */

@@ -53,6 +53,20 @@ def test_prove_other_skips_matches_oracle(oracle, wl, ctx, log_n, skips):
     assert wl.verify(consts, log_n, got, settings) == 0
 
 
+def test_transcript_dump_prover_equals_verifier(oracle, wl):
+    """The GPU prover's per-phase transcript dump equals the host verifier's reading of its proof."""
+    log_n = 8
+    consts, inputs = oracle.workload(log_n)
+    with wl.Context(0) as c:
+        c.set_transcript_dump(True)
+        proof = wl.AirTable(c, consts, log_n).prove(oracle.trace(log_n, consts, inputs))
+        dump = c.transcript_dump()
+    st, vdump = wl.verify_transcript(consts, log_n, proof)
+    assert st == 0
+    assert dump["proof_len"] == proof.size
+    assert dump == vdump
+
+
 def test_prove_device_witness_matches_host_path(oracle, wl, ctx):
     log_n = 9
     consts, inputs = oracle.workload(log_n, 3)

@@ -102,3 +102,35 @@ def test_abc_verifier(wl, oracle):
         c2 = c.copy()
         c2[5] ^= 1
         assert wl.sumcheck_abc_verify(p16, log_n, skips, oracle.prove_abc(p16, log_n, skips, a, b, c2)) != OK
+
+
+def test_verifier_transcript_dump(wl, oracle):
+    log_n, k = 7, 4
+    consts, _, proof = honest(oracle, log_n)
+    st, dump = wl.verify_transcript(consts, log_n, proof)
+    assert st == OK and dump["proof_len"] == proof.size
+    ev = dump["events"]
+    phases = [e for e in ev if e["kind"] == "phase"]
+    names = [e["phase"] for e in phases]
+    assert names[:6] == ["commit", "batching", "zerocheck", "inner_sums", "inner_sumcheck", "whir"]
+    assert names[-1] == "whir_final" and all(n.startswith("whir_round_") for n in names[6:-1])
+    offs = [e["offset"] for e in ev]
+    assert offs == sorted(offs) and offs[-1] <= proof.size
+    count = lambda ph, kind: sum(1 for e in ev if e["phase"] == ph and e["kind"] == kind)
+    assert count("batching", "challenge") == 1 + (log_n - k + 1)   # alpha, zerocheck challenges
+    assert count("zerocheck", "challenge") == log_n - k + 1           # one per round
+    assert count("inner_sums", "challenge") == 8 + 1 + k              # column batching, alpha', epsilons
+    assert count("inner_sumcheck", "challenge") == log_n
+    for e in ev:
+        if e["kind"] == "challenge":
+            assert len(e["values"]) == 8 and all(0 <= v < P for v in e["values"])
+        if e["kind"] == "queries":
+            assert e["values"] == sorted(set(e["values"]))
+    # the commitment root is the first 8 words; the first challenge (OOD) follows it
+    first = next(e for e in ev if e["kind"] == "challenge")
+    assert first["phase"] == "commit" and first["offset"] == 8
+    # a corrupted proof is read up to the failed check
+    bad = proof.copy()
+    bad[proof.size // 2] = (int(bad[proof.size // 2]) + 1) % P
+    st2, dump2 = wl.verify_transcript(consts, log_n, bad)
+    assert st2 != OK and len(dump2["events"]) <= len(ev)

@@ -101,6 +101,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
         "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
+        "wl_ctx_set_transcript_dump": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_transcript_dump": (ctypes.c_int, [vp, ctypes.c_char_p, _sizep]),
+        "wl_verify_transcript": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p,
+                                                ctypes.c_size_t, ctypes.c_char_p, _sizep]),
         "wl_server_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]),
         "wl_server_destroy": (None, [vp]),
         "wl_server_last_error": (ctypes.c_char_p, [vp]),
@@ -192,6 +196,17 @@ class Context:
     def set_spin_sync(self, spin: bool = True):
         """Busy-poll (True, the default) or block (False) at each host round trip."""
         self.check(self._lib.wl_ctx_set_spin_sync(self.handle, int(spin)), "set_spin_sync")
+
+    def set_transcript_dump(self, on: bool = True):
+        """Records a per-phase transcript dump of every later proof on this context."""
+        self.check(self._lib.wl_ctx_set_transcript_dump(self.handle, int(on)), "set_transcript_dump")
+
+    def transcript_dump(self) -> dict:
+        """The dump of the last proof (after set_transcript_dump(True))."""
+        import json
+        st, text = _text_call(self._lib.wl_transcript_dump, self.handle)
+        self.check(st, "transcript_dump")
+        return json.loads(text)
 
     @property
     def host_syncs(self) -> int:
@@ -356,6 +371,26 @@ def verify(constants: np.ndarray, log_n: int, proof: np.ndarray, settings: AirSe
     c = np.ascontiguousarray(constants, dtype=np.uint32)
     pr = np.ascontiguousarray(proof, dtype=np.uint32)
     return load_library().wl_verify(ctypes.byref(settings._c()), _ptr(c), log_n, _ptr(pr), pr.size)
+
+
+def _text_call(fn, *args):
+    n = ctypes.c_size_t(1 << 20)
+    for _ in range(2):
+        buf = ctypes.create_string_buffer(n.value)
+        st = fn(*args, buf, ctypes.byref(n))
+        if st != 4:  # not WL_E_BUFFER_TOO_SMALL
+            return st, buf.value.decode()
+    raise ProverError(st, "transcript dump")
+
+
+def verify_transcript(constants: np.ndarray, log_n: int, proof: np.ndarray, settings: AirSettings = AirSettings()):
+    """Runs the host verifier and returns (status, transcript dump as read by the verifier)."""
+    import json
+    c = np.ascontiguousarray(constants, dtype=np.uint32)
+    pr = np.ascontiguousarray(proof, dtype=np.uint32)
+    st, text = _text_call(load_library().wl_verify_transcript, ctypes.byref(settings._c()), _ptr(c), log_n,
+                          _ptr(pr), pr.size)
+    return st, json.loads(text)
 
 
 def sumcheck_abc_verify(p16_constants: np.ndarray, log_n: int, skips: int, proof: np.ndarray) -> int:

@@ -317,6 +317,47 @@ wl_status wl_verify(const wl_air_settings* s, const uint32_t* constants, int32_t
   });
 }
 
+namespace {
+wl_status emit_text(const std::string& text, char* buf, size_t* len) {
+  const size_t need = text.size() + 1;
+  if (!buf || *len < need) {
+    *len = need;
+    return WL_E_BUFFER_TOO_SMALL;
+  }
+  memcpy(buf, text.c_str(), need);
+  *len = need;
+  return WL_OK;
+}
+}  // namespace
+
+wl_status wl_ctx_set_transcript_dump(wl_ctx* ctx, int32_t on) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  ctx->c->dump_transcript = on != 0;
+  if (!on) ctx->c->last_dump.clear();
+  return WL_OK;
+}
+
+wl_status wl_transcript_dump(wl_ctx* ctx, char* buf, size_t* len) {
+  if (!ctx || !len) return WL_E_INVALID_ARG;
+  if (ctx->c->last_dump.empty()) return fail(ctx, WL_E_INVALID_ARG, "no transcript recorded (enable it, then prove)");
+  return emit_text(ctx->c->last_dump, buf, len);
+}
+
+wl_status wl_verify_transcript(const wl_air_settings* s, const uint32_t* constants, int32_t log_n,
+                               const uint32_t* proof, size_t proof_len, char* buf, size_t* len) {
+  std::string why;
+  if (!constants || !len || (!proof && proof_len) || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
+  for (size_t i = 0; i < proof_len; i++)
+    if (proof[i] >= kb::P) return WL_E_INVALID_ARG;
+  return guarded(nullptr, [&] {
+    wl::ProofJob job = make_job(s, constants, log_n);
+    wl::TranscriptLog log;
+    const int st = wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len, &log);
+    const wl_status out = emit_text(log.json(proof_len), buf, len);
+    return out != WL_OK ? out : wl_status(st);
+  });
+}
+
 wl_status wl_sumcheck_abc_verify(const uint32_t* p16c, int32_t log_n, int32_t skips, const uint32_t* proof,
                                  size_t proof_len) {
   if (!p16c || (!proof && proof_len) || log_n < 2 || log_n > 26 || skips < 1 || skips > 4 || skips >= log_n)

@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cstdint>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "air.cuh"
@@ -80,9 +81,44 @@ struct HostChallenger {
   uint32_t sample_bits(int bits) { return kb::from_mont(sample()) & ((1u << bits) - 1); }
 };
 
+// Per-phase record of a transcript, for diffing one implementation against another: where
+// each phase starts in proof_data, and every challenge, query batch and grinding witness with
+// the proof offset at which it was drawn (values canonical).
+struct TranscriptLog {
+  struct Event {
+    std::string kind;   // "phase", "challenge", "queries", "grinding"
+    std::string phase;  // the phase it belongs to
+    size_t offset = 0;  // words of proof_data before it
+    std::vector<uint32_t> values;
+  };
+  std::vector<Event> events;
+  std::string phase;
+  void begin(const char* name, size_t offset) {
+    phase = name;
+    events.push_back({"phase", phase, offset, {}});
+  }
+  void add(const char* kind, size_t offset, const uint32_t* v, size_t n, bool mont) {
+    Event e{kind, phase, offset, {}};
+    for (size_t i = 0; i < n; i++) e.values.push_back(mont ? kb::from_mont(v[i]) : v[i]);
+    events.push_back(std::move(e));
+  }
+  std::string json(size_t proof_len) const {
+    std::string o = "{\"proof_len\": " + std::to_string(proof_len) + ", \"events\": [";
+    for (size_t i = 0; i < events.size(); i++) {
+      const Event& e = events[i];
+      o += (i ? ", " : "") + std::string("{\"kind\": \"") + e.kind + "\", \"phase\": \"" + e.phase +
+           "\", \"offset\": " + std::to_string(e.offset) + ", \"values\": [";
+      for (size_t k = 0; k < e.values.size(); k++) o += (k ? ", " : "") + std::to_string(e.values[k]);
+      o += "]}";
+    }
+    return o + "]}";
+  }
+};
+
 struct Transcript {
   HostChallenger ch;
   std::vector<uint32_t> proof;  // Montgomery form
+  TranscriptLog* log = nullptr;
   explicit Transcript(const kb::P16Consts* p) { ch.perm = p; }
   void add_base(const uint32_t* v, size_t n) {
     for (size_t i = 0; i < n; i++) { proof.push_back(v[i]); ch.observe(v[i]); }
@@ -94,7 +130,11 @@ struct Transcript {
   ef sample_ext() {
     ef e;
     for (int i = 0; i < 8; i++) e.c[i] = ch.sample();
+    if (log) log->add("challenge", proof.size(), e.c, 8, true);
     return e;
+  }
+  void phase(const char* name) {
+    if (log) log->begin(name, proof.size());
   }
 };
 

@@ -335,6 +335,7 @@ void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
       uint32_t w = kb::to_mont(r);
       ts.ch.observe(w);
       if (ts.ch.sample_bits(bits) != 0) throw std::runtime_error("grinding witness failed on the host");
+      if (ts.log) ts.log->add("grinding", ts.proof.size(), &w, 1, true);
       ts.proof.push_back(w);
       return;
     }
@@ -396,6 +397,7 @@ std::vector<uint32_t> sample_queries(Transcript& ts, int log_leaves, int count) 
   for (auto& x : q) x = ts.ch.sample_bits(log_leaves);
   std::sort(q.begin(), q.end());
   q.erase(std::unique(q.begin(), q.end()), q.end());
+  if (ts.log) ts.log->add("queries", ts.proof.size(), q.data(), q.size(), false);
   return q;
 }
 
@@ -640,8 +642,11 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   const WhirSchedule ws = WhirSchedule::build(m0, s);
   cudaStream_t st = ctx.stream;
   Transcript ts(&job.p16);
+  TranscriptLog tlog;
+  if (ctx.dump_transcript) ts.log = &tlog;
   for (uint32_t x : ws.domain_separator()) ts.ch.observe(kb::to_mont(x));
   const double t0 = now_ms();
+  ts.phase("commit");
 
   // ---------------------------------------------------------------- 1) commit
   const size_t t_len = size_t(W) * N;
@@ -686,6 +691,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   const double t1 = now_ms();
 
   // ---------------------------------------------------------------- 2) challenges
+  ts.phase("batching");
   grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, log2_up(AIR_NC)));
   ef alpha = ts.sample_ext();
   std::vector<ef> alphas(AIR_NC);
@@ -712,6 +718,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   for (auto& x : zc) x = ts.sample_ext();
 
   // ---------------------------------------------------------------- 3) zerocheck
+  ts.phase("zerocheck");
   const int nsk = 1 << k;
   const auto sel = [&] {
     auto b = lagrange_basis_cached(nsk);
@@ -822,6 +829,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   const double t2 = now_ms();
 
   // ---------------------------------------------------------------- 4) inner sumcheck
+  ts.phase("inner_sums");
   ts.add_ext(inner_up.data(), W);
   ts.add_ext(inner_down.data(), W);
   grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, AIR_LOG_W));
@@ -863,6 +871,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   }
   const auto basis3 = lagrange_basis_cached(3);
   std::vector<ef> inner_ch;
+  ts.phase("inner_sumcheck");
   for (int round = 0; round < n; round++) {
     const size_t half = N >> (round + 1);
     const int nb = prod_blocks(half);
@@ -890,6 +899,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   const double t3 = now_ms();
 
   // ---------------------------------------------------------------- 5) WHIR opening
+  ts.phase("whir");
   {
     // initial constraints: the commitment OOD points, then the statement
     std::vector<std::vector<ef>> pts = ood_pts;
@@ -932,6 +942,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     for (int i = 0; i < ws.num_rounds; i++) {
       const WhirRound& ci = ws.c[i];
       const WhirRound& cn = ws.c[i + 1];
+      ts.phase(("whir_round_" + std::to_string(i + 1)).c_str());
       LdeSource src{g.as<uint32_t>(), size_t(8) << m, 8, m - cn.fold, cn.log_inv_rate, 128};
       commits.push_back(commit(ctx, src, m, cn.fold, job.p24, job.p16));
       const Commitment& cd = commits.back();
@@ -980,6 +991,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       prev = &cd;
     }
     // final round
+    ts.phase("whir_final");
     std::vector<ef> gf(size_t(1) << m), wf(size_t(1) << m);
     ctx.to_host(gf.data(), g.as<ef>(), sizeof(ef) << m);
     ctx.to_host(wf.data(), w.as<ef>(), sizeof(ef) << m);
@@ -1000,6 +1012,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     tm->whir_ms = t4 - t3;
     tm->total_ms = t4 - t0;
   }
+  if (ts.log) ctx.last_dump = tlog.json(ts.proof.size());
   return to_canonical(ts.proof);
 }
 

@@ -63,6 +63,9 @@ struct Context {
   // ~20 ms of wake-up stalls per proof); false = the thread polls for block_after_us, then
   // sleeps on a blocking-sync event (server workers, which would otherwise occupy one CPU each).
   bool spin_sync = true;
+  // When set, prove_air records a per-phase transcript log of each proof into last_dump (JSON).
+  bool dump_transcript = false;
+  std::string last_dump;
   int block_after_us = 500;
   cudaEvent_t sync_event = nullptr, block_event = nullptr;
   void to_device(void* dst, const void* src, size_t bytes);

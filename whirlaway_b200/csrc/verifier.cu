@@ -10,6 +10,7 @@
 // sumcheck (short proof, grinding, a round sum) is a sumcheck error, anything inside the WHIR
 // opening an opening error.
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "verifier.h"
@@ -25,7 +26,14 @@ struct ProofReader {
   HostChallenger ch;
   const uint32_t* words;
   size_t len, pos = 0;
-  ProofReader(const kb::P16Consts* p16, const uint32_t* w, size_t n) : words(w), len(n) { ch.perm = p16; }
+  TranscriptLog* log = nullptr;
+  ProofReader(const kb::P16Consts* p16, const uint32_t* w, size_t n, TranscriptLog* lg = nullptr)
+      : words(w), len(n), log(lg) {
+    ch.perm = p16;
+  }
+  void phase(const char* name) {
+    if (log) log->begin(name, pos);
+  }
   bool base(uint32_t* v, size_t n) {
     if (len - pos < n) return false;
     for (size_t i = 0; i < n; i++) {
@@ -47,14 +55,17 @@ struct ProofReader {
   ef sample() {
     ef e;
     for (int i = 0; i < 8; i++) e.c[i] = ch.sample();
+    if (log) log->add("challenge", pos, e.c, 8, true);
     return e;
   }
   // check_pow_grinding: the witness is observed, then `bits` sampled bits must be zero (no
   // witness at all for 0 bits)
   bool pow(int bits) {
     if (bits <= 0) return true;
+    const size_t at = pos;
     uint32_t w;
     if (!base(&w, 1)) return false;
+    if (log) log->add("grinding", at, &w, 1, true);
     return ch.sample_bits(bits) == 0;
   }
 };
@@ -178,6 +189,7 @@ class WhirVerifier {
   }
 
   bool verify(const Digest& root0, std::vector<std::vector<ef>> pts, std::vector<ef> vals) {
+    rd_.phase("whir");
     ef sigma = kb::ef_zero();
     add_group(0, pts, vals, rd_.sample(), sigma);
     if (!fold_block(ws_.c[0].fold, sigma)) return false;
@@ -185,6 +197,7 @@ class WhirVerifier {
     for (int i = 0; i < ws_.num_rounds; i++) {
       const WhirRound& ci = ws_.c[i];
       const WhirRound& cn = ws_.c[i + 1];
+      rd_.phase(("whir_round_" + std::to_string(i + 1)).c_str());
       Digest root;
       if (!rd_.base(root.data(), 8)) return false;
       std::vector<std::vector<ef>> npts;
@@ -211,6 +224,7 @@ class WhirVerifier {
       prev_root = root;
     }
     // final polynomial, its queries, the last sumcheck
+    rd_.phase("whir_final");
     std::vector<ef> gfin(size_t(1) << ws_.final_vars);
     if (!rd_.ext(gfin.data(), gfin.size())) return false;
     const WhirRound& cl = ws_.c[ws_.num_rounds];
@@ -270,6 +284,7 @@ class WhirVerifier {
     for (auto& x : q) x = rd_.ch.sample_bits(ll);
     std::sort(q.begin(), q.end());
     q.erase(std::unique(q.begin(), q.end()), q.end());
+    if (rd_.log) rd_.log->add("queries", rd_.pos, q.data(), q.size(), false);
     const std::vector<ef>& r = blocks_.back();
     for (uint32_t idx : q) {
       std::vector<uint32_t> row(128), path(size_t(8) * ll);
@@ -308,17 +323,19 @@ class WhirVerifier {
 }  // namespace
 
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
-                     int n, const uint32_t* proof, size_t proof_len) {
+                     int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log) {
   const int k = s.univariate_skips, W = AIR_W, nsk = 1 << k;
   const WhirSchedule ws = WhirSchedule::build(n + AIR_LOG_W, s);
-  ProofReader rd(&p16, proof, proof_len);
+  ProofReader rd(&p16, proof, proof_len, log);
   for (uint32_t x : ws.domain_separator()) rd.ch.observe(kb::to_mont(x));
+  rd.phase("commit");
   WhirVerifier whir(ws, p16, p24, rd);
   Digest root;
   std::vector<std::vector<ef>> ood_pts;
   std::vector<ef> ood_vals;
   if (!whir.parse_commitment(root, ood_pts, ood_vals)) return VERIFY_PCS_COMMITMENT;
 
+  rd.phase("batching");
   if (!rd.pow(batching_pow_bits(s.security_bits, log2_up(AIR_NC)))) return VERIFY_FS;
   const ef alpha = rd.sample();
   if (!rd.pow(batching_pow_bits(s.security_bits, n))) return VERIFY_FS;
@@ -329,10 +346,12 @@ int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Const
   std::vector<int> deg{4 * (nsk - 1)}, set{nsk};
   for (int i = 0; i < n - k; i++) deg.push_back(4), set.push_back(2);
   Claim outer;
+  rd.phase("zerocheck");
   if (!sumcheck_rounds(rd, deg, set, s.security_bits, outer)) return VERIFY_SUMCHECK;
   if (!kb::ef_is_zero(outer.sum)) return VERIFY_SUM_MISMATCH;
 
   std::vector<ef> up(W), down(W);
+  rd.phase("inner_sums");
   if (!rd.ext(up.data(), W) || !rd.ext(down.data(), W)) return VERIFY_FS;
   const auto& sel = lagrange_basis_cached(nsk);
   std::vector<ef> outer_sel(nsk);
@@ -369,6 +388,7 @@ int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Const
 
   // inner product sumcheck over the n row variables, degree 2
   Claim inner;
+  rd.phase("inner_sumcheck");
   if (!sumcheck_rounds(rd, std::vector<int>(n, 2), std::vector<int>(n, 2), s.security_bits, inner))
     return VERIFY_SUMCHECK;
   if (!kb::ef_eq(inner.sum, mle_eval(sub, eps))) return VERIFY_SUM_MISMATCH;
