@@ -130,6 +130,13 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
  * canonical field element. */
 wl_status wl_verify(const wl_air_settings* settings, const uint32_t* constants, int32_t log_n,
                     const uint32_t* proof, size_t proof_len);
+/* wl_verify over n proofs on `threads` host threads (<= 0: all hardware threads); proof i has
+ * log_ns[i] rows and its outcome goes to statuses[i]. Returns WL_OK when every proof was
+ * checked (whatever the outcomes), else the argument error. */
+wl_status wl_verify_batch(const wl_air_settings* settings, const uint32_t* constants, int32_t n,
+                          const int32_t* log_ns, const uint32_t* const* proofs, const size_t* proof_lens,
+                          int32_t threads, int32_t* statuses);
+
 /* Per-phase transcript dumps, for diffing against another implementation of the protocol (a
  * build of the reference with the same parameters): JSON text
  *   {"proof_len": L, "events": [{"kind", "phase", "offset", "values"}, ...]}

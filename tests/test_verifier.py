@@ -134,3 +134,21 @@ def test_verifier_transcript_dump(wl, oracle):
     bad[proof.size // 2] = (int(bad[proof.size // 2]) + 1) % P
     st2, dump2 = wl.verify_transcript(consts, log_n, bad)
     assert st2 != OK and len(dump2["events"]) <= len(ev)
+
+
+def test_verify_batch_threads(wl, oracle):
+    consts, _ = oracle.workload(5, 1)
+    jobs = []
+    for k, log_n in enumerate((5, 6, 7, 6, 5)):
+        c, i = oracle.workload(log_n, 10 + k)  # own inputs; the constants skip the input draws
+        assert np.array_equal(c, consts)
+        proof, _ = oracle.prove(log_n, c, oracle.trace(log_n, c, i))
+        jobs.append((log_n, proof))
+    bad = jobs[2][1].copy()
+    bad[100] = (int(bad[100]) + 1) % P
+    jobs.append((7, bad))
+    jobs.append((6, jobs[0][1]))  # wrong height for that proof
+    for threads in (1, 4, 0):
+        st = wl.verify_batch(consts, jobs, threads=threads)
+        assert st[:5] == [OK] * 5 and st[5] != OK and st[6] != OK
+        assert st == [wl.verify(consts, l, p) for l, p in jobs]

@@ -101,6 +101,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
         "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
+        "wl_verify_batch": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_u32p), _sizep,
+                                           ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
         "wl_ctx_set_transcript_dump": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_transcript_dump": (ctypes.c_int, [vp, ctypes.c_char_p, _sizep]),
         "wl_verify_transcript": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p,
@@ -371,6 +374,21 @@ def verify(constants: np.ndarray, log_n: int, proof: np.ndarray, settings: AirSe
     c = np.ascontiguousarray(constants, dtype=np.uint32)
     pr = np.ascontiguousarray(proof, dtype=np.uint32)
     return load_library().wl_verify(ctypes.byref(settings._c()), _ptr(c), log_n, _ptr(pr), pr.size)
+
+
+def verify_batch(constants: np.ndarray, jobs, settings: AirSettings = AirSettings(), threads: int = 0):
+    """wl_verify over [(log_n, proof), ...] on host threads; returns the list of statuses."""
+    c = np.ascontiguousarray(constants, dtype=np.uint32)
+    prs = [np.ascontiguousarray(p, dtype=np.uint32) for _, p in jobs]
+    n = len(jobs)
+    log_ns = (ctypes.c_int32 * n)(*[int(l) for l, _ in jobs])
+    ptrs = (_u32p * n)(*[_ptr(p) for p in prs])
+    lens = (ctypes.c_size_t * n)(*[p.size for p in prs])
+    out = (ctypes.c_int32 * n)()
+    st = load_library().wl_verify_batch(ctypes.byref(settings._c()), _ptr(c), n, log_ns, ptrs, lens, threads, out)
+    if st:
+        raise ProverError(st, "verify_batch")
+    return list(out)
 
 
 def _text_call(fn, *args):

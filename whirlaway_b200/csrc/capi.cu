@@ -1,5 +1,9 @@
 // C ABI (include/whirlaway_b200.h): argument checks, error mapping, witness handles.
 #include <cstring>
+#include <algorithm>
+#include <vector>
+#include <thread>
+#include <atomic>
 #include <exception>
 #include <memory>
 #include <new>
@@ -355,6 +359,27 @@ wl_status wl_verify_transcript(const wl_air_settings* s, const uint32_t* constan
     const int st = wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len, &log);
     const wl_status out = emit_text(log.json(proof_len), buf, len);
     return out != WL_OK ? out : wl_status(st);
+  });
+}
+
+wl_status wl_verify_batch(const wl_air_settings* s, const uint32_t* constants, int32_t n, const int32_t* log_ns,
+                          const uint32_t* const* proofs, const size_t* proof_lens, int32_t threads,
+                          int32_t* statuses) {
+  if (!s || !constants || n < 0 || (n && (!log_ns || !proofs || !proof_lens || !statuses)))
+    return WL_E_INVALID_ARG;
+  return guarded(nullptr, [&] {
+    unsigned hw = std::thread::hardware_concurrency();
+    int T = threads > 0 ? threads : int(hw ? hw : 1);
+    T = std::max(1, std::min(T, n));
+    std::atomic<int> next{0};
+    auto work = [&] {
+      for (int i = next++; i < n; i = next++) statuses[i] = wl_verify(s, constants, log_ns[i], proofs[i], proof_lens[i]);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    return WL_OK;
   });
 }
 
