@@ -459,6 +459,7 @@ wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
         first = false;
         js += "\"" + std::string(h.first) + "\": [" + std::to_string(h.second.first) + ", " + std::to_string(h.second.second) + "]";
       }
+      for (auto& b : hc.busy) js += ", \"host:busy:" + b.first + "\": [" + std::to_string(b.second) + ", 1]";
     }
     js += "}";
     if (js.size() + 1 > cap) return fail(ctx, WL_E_BUFFER_TOO_SMALL, "profile buffer too small");

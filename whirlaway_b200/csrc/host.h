@@ -37,6 +37,15 @@ struct HostClock {
   bool on = false;
   double perm_ms = 0, alloc_ms = 0, launch_ms = 0, upload_ms = 0;
   long perms = 0, allocs = 0, launches = 0, uploads = 0;
+  // host time between device waits, by proof phase (the phase current when the wait begins)
+  const char* phase = "setup";
+  double last_wait_end = 0;
+  std::vector<std::pair<std::string, double>> busy;
+  void add_busy(double ms) {
+    for (auto& b : busy)
+      if (b.first == phase) { b.second += ms; return; }
+    busy.emplace_back(phase, ms);
+  }
 };
 inline HostClock& host_clock() {
   thread_local HostClock c;
@@ -135,7 +144,9 @@ struct Transcript {
   }
   void phase(const char* name) {
     if (log) log->begin(name, proof.size());
+    host_clock_phase(name);
   }
+  static void host_clock_phase(const char* name);
 };
 
 // ------------------------------------------------------------------ small polynomials

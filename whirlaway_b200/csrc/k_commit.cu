@@ -507,12 +507,24 @@ __global__ void __launch_bounds__(1024) k_merkle_top(uint32_t* __restrict__ tree
 }
 
 // Rows idx[q] of the tile-major LDE (2^T rows, n_cols columns) into out[q * n_cols + col].
-__global__ void k_gather_lde(const uint32_t* __restrict__ lde, int T, const uint64_t* __restrict__ idx, int n_cols,
-                             int n, uint32_t* __restrict__ out) {
-  const int q = blockIdx.x;
-  if (q >= n) return;
-  for (int c = threadIdx.x; c < n_cols; c += blockDim.x)
-    out[size_t(q) * n_cols + c] = lde[(((size_t(c >> 3) << T) + idx[q]) << 3) + (c & 7)];
+// Row idx[q] of the tile-major LDE (128 threads, one per position; positions >= n_cols are
+// zero), Moebius-transformed over the position bits [log_elem, 7) as the leaf hash absorbs it:
+// for each bit b, v[i | 2^b] -= v[i]. Writes out[q * 128 + i].
+__global__ void __launch_bounds__(128) k_gather_lde(const uint32_t* __restrict__ lde, int T,
+                                                    const uint64_t* __restrict__ idx, int n_cols, int log_elem,
+                                                    int n, uint32_t* __restrict__ out) {
+  __shared__ uint32_t v[128];
+  const int q = blockIdx.x, i = threadIdx.x;
+  if (q >= n) return;  // whole block
+  v[i] = i < n_cols ? lde[(((size_t(i >> 3) << T) + idx[q]) << 3) + (i & 7)] : 0u;
+  __syncthreads();
+  for (int b = log_elem; b < 7; b++) {
+    const uint32_t lo = v[i & ~(1 << b)];
+    __syncthreads();
+    if (i & (1 << b)) v[i] = kb::sub(v[i], lo);
+    __syncthreads();
+  }
+  out[size_t(q) * 128 + i] = v[i];
 }
 
 __global__ void k_gather(const uint32_t* __restrict__ src, const uint64_t* __restrict__ idx, int width, int n,
@@ -687,10 +699,11 @@ void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cuda
   }
 }
 
-void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int n, uint32_t* out,
-                            cudaStream_t s) {
+void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int log_elem, int n,
+                            uint32_t* out, cudaStream_t s) {
+  if (n_cols > 128 || log_elem < 0 || log_elem > 7) throw std::invalid_argument("gather: rows of at most 128 values");
   if (!n) return;
-  k_gather_lde<<<n, 128, 0, s>>>(lde, T, idx, n_cols, n, out);
+  k_gather_lde<<<n, 128, 0, s>>>(lde, T, idx, n_cols, log_elem, n, out);
   WL_LAUNCH_CHECK();
 }
 

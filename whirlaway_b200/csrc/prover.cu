@@ -207,8 +207,25 @@ ProfScope::~ProfScope() {
   c.pending.push_back({name, a, b});
 }
 
+void Transcript::host_clock_phase(const char* name) {
+  HostClock& hc = host_clock();
+  if (hc.on) {
+    static thread_local std::string names[16];
+    static thread_local int next = 0;
+    for (auto& n : names)
+      if (n == name) { hc.phase = n.c_str(); return; }
+    names[next % 16] = name;
+    hc.phase = names[next++ % 16].c_str();
+  }
+}
+
 void Context::wait_stream() {
   const auto w0 = std::chrono::steady_clock::now();
+  HostClock& hclk = host_clock();
+  if (hclk.on) {
+    const double t = host_now_ms();
+    if (hclk.last_wait_end > 0) hclk.add_busy(t - hclk.last_wait_end);
+  }
   if (spin_sync) {
     if (!sync_event) WL_CUDA(cudaEventCreateWithFlags(&sync_event, cudaEventDisableTiming));
     WL_CUDA(cudaEventRecord(sync_event, stream));
@@ -231,6 +248,7 @@ void Context::wait_stream() {
   }
   host_syncs++;
   host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+  if (hclk.on) hclk.last_wait_end = host_now_ms();
 }
 ef* Context::partials(size_t n) {
   if (n > part_cap) {
@@ -410,27 +428,23 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   for (uint32_t i : idx)
     for (int l = 0; l < LL; l++) didx.push_back(level_offset(LL, l) + ((i >> l) ^ 1u));
   DBuf dr = upload(ctx, ridx), dd = upload(ctx, didx);
-  DBuf rows(sizeof(uint32_t) * c.n_cols * std::max(nq, 1), ctx.stream);
+  const int log_elem = c.elem == 8 ? 3 : 0;
+  DBuf rows(sizeof(uint32_t) * 128 * std::max(nq, 1), ctx.stream);
   DBuf digs(sizeof(uint32_t) * 8 * std::max<size_t>(didx.size(), 1), ctx.stream);
-  { ProfScope _ps(ctx, "gather"); launch_gather_lde_rows(c.lde.as<uint32_t>(), LL, dr.as<uint64_t>(), c.n_cols, nq, rows.as<uint32_t>(), ctx.stream); }
+  { ProfScope _ps(ctx, "gather"); launch_gather_lde_rows(c.lde.as<uint32_t>(), LL, dr.as<uint64_t>(), c.n_cols, log_elem, nq, rows.as<uint32_t>(), ctx.stream); }
   { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream); }
-  std::vector<uint32_t> hr(size_t(c.n_cols) * nq), hd(didx.size() * 8);
+  std::vector<uint32_t> hr(size_t(128) * nq), hd(didx.size() * 8);
   if (nq) {
     ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
     ctx.to_host(hd.data(), digs.as<uint32_t>(), hd.size() * 4);
     for (uint32_t& w : hd) w = kb::to_mont(w);  // canonical digests
   }
-  const int log_elem = c.elem == 8 ? 3 : 0;
   std::vector<std::vector<uint32_t>> out;
   for (int q = 0; q < nq; q++) {
-    std::vector<uint32_t> row(128, 0);
-    for (int i = 0; i < c.n_cols; i++) row[i] = hr[size_t(q) * c.n_cols + i];
-    for (int b = log_elem; b < 7; b++)
-      for (int i = 0; i < 128; i++)
-        if (!(i & (1 << b))) row[i + (1 << b)] = kb::sub(row[i + (1 << b)], row[i]);
-    ts.hint(row.data(), 128);
+    const uint32_t* row = &hr[size_t(q) * 128];  // Moebius-transformed on the device, as hashed
+    ts.hint(row, 128);
     ts.hint(&hd[size_t(q) * LL * 8], size_t(LL) * 8);
-    out.push_back(row);
+    out.emplace_back(row, row + 128);
   }
   return out;
 }
