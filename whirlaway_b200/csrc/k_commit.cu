@@ -509,11 +509,15 @@ __global__ void __launch_bounds__(1024) k_merkle_top(uint32_t* __restrict__ tree
 // Rows idx[q] of the tile-major LDE (2^T rows, n_cols columns) into out[q * n_cols + col].
 // Row idx[q] of the tile-major LDE (128 threads, one per position; positions >= n_cols are
 // zero), Moebius-transformed over the position bits [log_elem, 7) as the leaf hash absorbs it:
-// for each bit b, v[i | 2^b] -= v[i]. Writes out[q * 128 + i].
+// for each bit b, v[i | 2^b] -= v[i]. Writes out[q * 128 + i]. With mono, also the row's
+// folded value folded[q] = sum_p v_p mono[p] over its 128 >> log_elem elements (base-field
+// values, or extension elements of 8 consecutive words).
 __global__ void __launch_bounds__(128) k_gather_lde(const uint32_t* __restrict__ lde, int T,
                                                     const uint64_t* __restrict__ idx, int n_cols, int log_elem,
-                                                    int n, uint32_t* __restrict__ out) {
+                                                    int n, uint32_t* __restrict__ out, const kb::ef* __restrict__ mono,
+                                                    kb::ef* __restrict__ folded) {
   __shared__ uint32_t v[128];
+  __shared__ kb::ef scratch[32];
   const int q = blockIdx.x, i = threadIdx.x;
   if (q >= n) return;  // whole block
   v[i] = i < n_cols ? lde[(((size_t(i >> 3) << T) + idx[q]) << 3) + (i & 7)] : 0u;
@@ -525,6 +529,18 @@ __global__ void __launch_bounds__(128) k_gather_lde(const uint32_t* __restrict__
     __syncthreads();
   }
   out[size_t(q) * 128 + i] = v[i];
+  if (mono) {
+    kb::ef c = kb::ef_zero();
+    if (log_elem == 0) {
+      c = kb::ef_mul_f(mono[i], v[i]);
+    } else if (i < (128 >> log_elem)) {
+      kb::ef e = kb::ef_zero();
+      for (int k = 0; k < (1 << log_elem); k++) e.c[k] = v[(i << log_elem) + k];
+      c = kb::ef_mul(e, mono[i]);
+    }
+    c = block_reduce_ef(c, scratch);
+    if (i == 0) folded[q] = c;
+  }
 }
 
 __global__ void k_gather(const uint32_t* __restrict__ src, const uint64_t* __restrict__ idx, int width, int n,
@@ -700,10 +716,10 @@ void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cuda
 }
 
 void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int log_elem, int n,
-                            uint32_t* out, cudaStream_t s) {
+                            uint32_t* out, const ef* mono, ef* folded, cudaStream_t s) {
   if (n_cols > 128 || log_elem < 0 || log_elem > 7) throw std::invalid_argument("gather: rows of at most 128 values");
   if (!n) return;
-  k_gather_lde<<<n, 128, 0, s>>>(lde, T, idx, n_cols, log_elem, n, out);
+  k_gather_lde<<<n, 128, 0, s>>>(lde, T, idx, n_cols, log_elem, n, out, mono, folded);
   WL_LAUNCH_CHECK();
 }
 

@@ -52,9 +52,11 @@ void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, 
 void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s);
 // Gathers rows idx[q] of a tile-major LDE matrix (2^T rows, n_cols <= 128 stored columns) as
 // the leaves hash them: 128 values per row (zero beyond n_cols), Moebius-transformed over the
-// position bits [log_elem, 7), into out[q * 128 + i].
+// position bits [log_elem, 7), into out[q * 128 + i]. With mono (128 >> log_elem entries),
+// also folded[q] = sum_p row_p mono[p] over the row's base-field values (log_elem 0) or
+// extension elements (log_elem 3).
 void launch_gather_lde_rows(const uint32_t* lde, int T, const uint64_t* idx, int n_cols, int log_elem, int n,
-                            uint32_t* out, cudaStream_t s);
+                            uint32_t* out, const ef* mono, ef* folded, cudaStream_t s);
 // Gathers rows of a row-major u32 matrix of the given width (Merkle digests: width 8).
 void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int n, uint32_t* out, cudaStream_t s);
 

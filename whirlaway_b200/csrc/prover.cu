@@ -420,9 +420,10 @@ std::vector<uint32_t> sample_queries(Transcript& ts, int log_leaves, int count) 
 }
 
 // Appends rows (Moebius-transformed over the position bits, as hashed) and
-// authentication paths as hints; returns the rows.
-std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const std::vector<uint32_t>& idx,
-                                        Transcript& ts) {
+// authentication paths as hints. With mono (the folding monomials of the commitment's fold
+// randomness), returns each opened row's folded value (its STIR answer).
+std::vector<ef> open(Context& ctx, const Commitment& c, const std::vector<uint32_t>& idx, Transcript& ts,
+                     const std::vector<ef>* mono = nullptr) {
   const int LL = c.log_leaves, nq = (int)idx.size();
   std::vector<uint64_t> ridx(idx.begin(), idx.end()), didx;
   for (uint32_t i : idx)
@@ -431,22 +432,23 @@ std::vector<std::vector<uint32_t>> open(Context& ctx, const Commitment& c, const
   const int log_elem = c.elem == 8 ? 3 : 0;
   DBuf rows(sizeof(uint32_t) * 128 * std::max(nq, 1), ctx.stream);
   DBuf digs(sizeof(uint32_t) * 8 * std::max<size_t>(didx.size(), 1), ctx.stream);
-  { ProfScope _ps(ctx, "gather"); launch_gather_lde_rows(c.lde.as<uint32_t>(), LL, dr.as<uint64_t>(), c.n_cols, log_elem, nq, rows.as<uint32_t>(), ctx.stream); }
+  DBuf dmono = mono ? upload(ctx, *mono) : DBuf();
+  DBuf dfold(mono ? sizeof(ef) * std::max(nq, 1) : 0, ctx.stream);
+  { ProfScope _ps(ctx, "gather"); launch_gather_lde_rows(c.lde.as<uint32_t>(), LL, dr.as<uint64_t>(), c.n_cols, log_elem, nq, rows.as<uint32_t>(), mono ? dmono.as<ef>() : nullptr, mono ? dfold.as<ef>() : nullptr, ctx.stream); }
   { ProfScope _ps(ctx, "gather"); launch_gather_u32(c.tree.as<uint32_t>(), dd.as<uint64_t>(), 8, (int)didx.size(), digs.as<uint32_t>(), ctx.stream); }
   std::vector<uint32_t> hr(size_t(128) * nq), hd(didx.size() * 8);
+  std::vector<ef> folded(mono ? nq : 0);
   if (nq) {
     ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
     ctx.to_host(hd.data(), digs.as<uint32_t>(), hd.size() * 4);
+    if (mono) ctx.to_host(folded.data(), dfold.as<ef>(), sizeof(ef) * nq);
     for (uint32_t& w : hd) w = kb::to_mont(w);  // canonical digests
   }
-  std::vector<std::vector<uint32_t>> out;
   for (int q = 0; q < nq; q++) {
-    const uint32_t* row = &hr[size_t(q) * 128];  // Moebius-transformed on the device, as hashed
-    ts.hint(row, 128);
+    ts.hint(&hr[size_t(q) * 128], 128);  // Moebius-transformed on the device, as hashed
     ts.hint(&hd[size_t(q) * LL * 8], size_t(LL) * 8);
-    out.emplace_back(row, row + 128);
   }
-  return out;
+  return folded;
 }
 
 }  // namespace
@@ -465,7 +467,7 @@ namespace {
 // Coefficient-form multilinear evaluation of a (transformed) row at r (row MSB <-> r_1):
 // folding the row by v[q] + r_i v[q + h], MSB first, gives sum_p v_p m_p with the monomial
 // m_p = prod of r_i over the set bits of p (bit fold-1-i <-> r_i). The monomials depend on r
-// only, so one table serves every query of a round.
+// only, so one table serves every query of a round (the dot products run in the row gather).
 std::vector<ef> fold_monomials(int fold, const std::vector<ef>& r) {
   std::vector<ef> m(size_t(1) << fold);
   m[0] = kb::ef_one();
@@ -475,30 +477,6 @@ std::vector<ef> fold_monomials(int fold, const std::vector<ef>& r) {
   }
   return m;
 }
-ef fold_row(const std::vector<uint32_t>& row, int elem, const std::vector<ef>& mono) {
-  if (elem != 1) {
-    ef acc = kb::ef_zero();
-    for (size_t p = 0; p < mono.size(); p++) {
-      ef v;
-      for (int e = 0; e < 8; e++) v.c[e] = e < elem ? row[p * elem + e] : 0u;
-      acc = kb::ef_add(acc, kb::ef_mul(v, mono[p]));
-    }
-    return acc;
-  }
-  // base-field row: lazy sums of products, folded with 2^32 = 2^25 - 2 (mod p) after every 4
-  // (below 2^57 + 2^32, so 4 more products of values below p fit in 64 bits)
-  constexpr uint64_t C32 = (1u << 25) - 2;
-  uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (size_t p = 0; p < mono.size(); p++) {
-    for (int k = 0; k < 8; k++) acc[k] += kb::wmul(row[p], mono[p].c[k]);
-    if ((p & 3) == 3)
-      for (int k = 0; k < 8; k++) acc[k] = (acc[k] >> 32) * C32 + uint32_t(acc[k]);
-  }
-  ef r;
-  for (int k = 0; k < 8; k++) r.c[k] = kb::redc((acc[k] >> 32) * C32 + uint32_t(acc[k]));
-  return r;
-}
-
 void split_vars(int lv, int& lh, int& ll) {
   ll = std::min(10, lv);
   lh = lv - ll;
@@ -973,17 +951,15 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       }
       grind(ctx, ts, job.p16, ci.pow_bits);
       std::vector<uint32_t> q = sample_queries(ts, prev->log_leaves, ci.queries);
-      auto rows = open(ctx, *prev, q, ts);
+      const std::vector<ef> mono = fold_monomials(prev->fold, last_r);
+      const std::vector<ef> stir_vals = open(ctx, *prev, q, ts, &mono);
       const uint32_t gen = kb::two_adic_gen_m(prev->log_leaves);
       std::vector<std::vector<uint32_t>> stir_pts;
-      std::vector<ef> stir_vals;
-      const std::vector<ef> mono = fold_monomials(prev->fold, last_r);
       for (size_t t = 0; t < q.size(); t++) {
         uint32_t y = kb::pow_m(gen, q[t]);
         std::vector<uint32_t> pt(m);
         for (int b = 0; b < m; b++) { pt[b] = y; y = kb::mul(y, y); }
         stir_pts.push_back(pt);
-        stir_vals.push_back(fold_row(rows[t], prev->elem, mono));
       }
       ef gm = ts.sample_ext();
       std::vector<ef> coef_ef, coef_f;
