@@ -6,6 +6,8 @@
 //
 // Equality polynomials over m variables are factored as eq(pt, v) = hi(v_hi) * lo(v_lo)
 // with v_lo the low ll bits, so a table of 2^m entries costs 2^lh + 2^ll to build.
+#include <algorithm>
+
 #include "kernels.h"
 #include "limb_mma.cuh"
 
@@ -101,6 +103,67 @@ __global__ void k_sum_split(const ef* __restrict__ in, size_t n, ef* __restrict_
 }
 
 // out[v] = sum_u eqr[u] * T[u * 2^lv + v]; two adjacent v per thread (8-byte loads).
+// The same fold on the tensor cores (byte-limb form whose reduction index carries the value's
+// limbs): rows v, reduction index (u, a) over the nonzero rows u < U of T and the 4 bytes a of
+// T[u, v], columns (n, b) for the 8 coefficients n and the 4 bytes b of M(u, n, a) = the
+// Montgomery form of eqr[u]_n 2^(8a). The B fragments come from a table built once per launch
+// (k_fold_T_limbs, bfrag[((kk * 4 + b) * 2 + h) * 32 + lane]); A fragments are loaded straight
+// from T (lanes of equal t read 8 consecutive v: whole 32-byte sectors). Each warp owns 16 rows
+// and all 4 n8 tiles; acc_b < 4U 255^2 < 2^25, sum_b acc_b 2^(8b) < 2^50, one Montgomery
+// reduction per coefficient.
+constexpr int FT_WARPS = 4;
+__global__ void k_fold_T_limbs(const ef* __restrict__ eqr, int U, int Up, uint32_t* __restrict__ bfrag) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // (kk, b, h, lane)
+  if (idx >= Up / 8 * 256) return;
+  const int lane = idx & 31, h = (idx >> 5) & 1, b = (idx >> 6) & 3, kk = idx >> 8;
+  const int g = lane >> 2, t = lane & 3;
+  const int u = 8 * kk + 4 * h + t;
+  const uint32_t w = u < U ? eqr[u].c[g] : 0u;
+  uint32_t word = 0;
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const uint32_t m = mul(w, uint32_t(detail::cpow(2, 8 * a + 32)));
+    word |= ((m >> (8 * b)) & 0xffu) << (8 * a);
+  }
+  bfrag[idx] = word;
+}
+__global__ void __launch_bounds__(FT_WARPS * 32) k_whir_fold_T_mma(const uint32_t* __restrict__ T, size_t t_len,
+                                                                   int lv, int U, int Up,
+                                                                   const uint32_t* __restrict__ bfrag,
+                                                                   ef* __restrict__ out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const size_t nv = size_t(1) << lv;
+  const size_t v0 = (size_t(blockIdx.x) * FT_WARPS + warp) * 16;
+  if (v0 >= nv) return;  // whole warp
+  const size_t va = v0 + g, vb = va + 8;
+  auto ld = [&](int u, size_t v) -> uint32_t {
+    const size_t i = (size_t(u) << lv) + v;
+    return (u < U && v < nv && i < t_len) ? __ldg(T + i) : 0u;
+  };
+  int acc[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; b++)
+#pragma unroll
+    for (int o = 0; o < 4; o++) acc[b][o] = 0;
+#pragma unroll 1
+  for (int kk = 0; kk < Up / 8; kk++) {
+    const int u0 = 8 * kk + t;
+    const uint32_t af[4] = {ld(u0, va), ld(u0, vb), ld(u0 + 4, va), ld(u0 + 4, vb)};
+    const uint32_t* bp = bfrag + size_t(kk) * 256 + lane;
+#pragma unroll
+    for (int b = 0; b < 4; b++) mma_u8_16832(acc[b], af, __ldg(bp + (2 * b) * 32), __ldg(bp + (2 * b + 1) * 32));
+  }
+  uint32_t r[4];
+#pragma unroll
+  for (int o = 0; o < 4; o++)
+    r[o] = redc(uint64_t(uint32_t(acc[0][o])) + (uint64_t(uint32_t(acc[1][o])) << 8) +
+                (uint64_t(uint32_t(acc[2][o])) << 16) + (uint64_t(uint32_t(acc[3][o])) << 24));
+  // lane (g, t) holds coefficients 2t, 2t + 1 of rows va and vb
+  if (va < nv) reinterpret_cast<uint2*>(out + va)[t] = make_uint2(r[0], r[1]);
+  if (vb < nv) reinterpret_cast<uint2*>(out + vb)[t] = make_uint2(r[2], r[3]);
+}
+
 __global__ void k_whir_fold_T(const uint32_t* __restrict__ T, size_t t_len, int lu, int lv,
                               const ef* __restrict__ eqr_g, ef* __restrict__ out) {
   extern __shared__ ef eqr[];
@@ -315,9 +378,24 @@ void launch_mle_partial_base(const uint32_t* T, size_t t_len, int lu, int lh, in
   WL_LAUNCH_CHECK();
 }
 
-void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s) {
+size_t whir_fold_T_scratch_bytes(int lu) { return size_t(4) * (((size_t(1) << lu) + 7) / 8) * 256; }
+void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s,
+                        uint32_t* scratch) {
   size_t n = size_t(1) << lv;
   if (lv < 1) throw std::invalid_argument("whir_fold_T: at least 2 entries");
+  if (scratch && lv >= 4) {
+    const size_t rows_nz = (t_len + n - 1) >> lv;  // rows u of T with a nonzero entry
+    const int U = int(std::min<size_t>(size_t(1) << lu, rows_nz)), Up = (U + 7) / 8 * 8;
+    if (U > 0) {
+      k_fold_T_limbs<<<(Up / 8 * 256 + 255) / 256, 256, 0, s>>>(eqr, U, Up, scratch);
+      WL_LAUNCH_CHECK();
+      const size_t tiles = n / 16;
+      k_whir_fold_T_mma<<<(unsigned)((tiles + FT_WARPS - 1) / FT_WARPS), FT_WARPS * 32, 0, s>>>(T, t_len, lv, U, Up,
+                                                                                              scratch, out);
+      WL_LAUNCH_CHECK();
+      return;
+    }
+  }
   k_whir_fold_T<<<(unsigned)((n / 2 + 255) / 256), 256, sizeof(ef) << lu, s>>>(T, t_len, lu, lv, eqr, out);
   WL_LAUNCH_CHECK();
 }

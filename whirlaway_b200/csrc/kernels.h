@@ -147,7 +147,11 @@ size_t colsum_limb_bytes(int K);
 void launch_batch_cols_mma(const uint32_t* wit, int log_n, const ef* eqc, ef* out, uint8_t* limbs, cudaStream_t s);
 bool launch_mle_partial_mma(const uint32_t* T, size_t t_len, int lu, int lh, int ll, const ef* hi, const ef* lo,
                             ef* out, void* scratch, cudaStream_t s);
-void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s);
+// out[v] = sum_u eqr[u] T[u 2^lv + v] (zero past t_len); with scratch
+// (whir_fold_T_scratch_bytes(lu)) on the tensor cores.
+size_t whir_fold_T_scratch_bytes(int lu);
+void launch_whir_fold_T(const uint32_t* T, size_t t_len, int lu, int lv, const ef* eqr, ef* out, cudaStream_t s,
+                        uint32_t* scratch = nullptr);
 void launch_add_eq_terms_f(ef* w, int lh, int ll, int npts, const uint32_t* hi, const uint32_t* lo, const ef* coefs,
                            cudaStream_t s);
 void launch_add_eq_terms_ef(ef* w, int lh, int ll, int npts, const ef* hi, const ef* lo, const ef* coefs,

@@ -918,7 +918,8 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     DBuf g(sizeof(ef) << m, st), w(sizeof(ef) << m, st);
     {
       DBuf er = upload(ctx, eq_table_host(r0));
-      { ProfScope _ps(ctx, "whir_fold_T"); launch_whir_fold_T(wit, t_len, lu, m, er.as<ef>(), g.as<ef>(), st); }
+      DBuf fscratch(whir_fold_T_scratch_bytes(lu), st);
+      { ProfScope _ps(ctx, "whir_fold_T"); launch_whir_fold_T(wit, t_len, lu, m, er.as<ef>(), g.as<ef>(), st, fscratch.as<uint32_t>()); }
       WL_CUDA(cudaMemsetAsync(w.as<void>(), 0, sizeof(ef) << m, st));
       std::vector<std::vector<ef>> pv;
       std::vector<ef> cv;
