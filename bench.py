@@ -186,6 +186,18 @@ def cpu_prove_rate(log_n, steps, warmup, threads=None):
     return steps * (1 << log_n) / dt, cores, dt / steps
 
 
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo), for the baseline record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -198,7 +210,8 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear Montgomery)", "data": "synthetic",
         "config": workload_config(args.log_n),
-        "cpu_baseline": {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port", "sample": sample,
+                         "cpu_model": cpu_model(), "nproc": os.cpu_count()},
         "e2e": {"value": rate, "unit": "perms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -448,7 +461,8 @@ def run_ours(args, world, rank, local):
         cl = min(args.cpu_sample_log_n, log_n)
         rate, cores, sec = cpu_prove_rate(cl, 1, 0)
         cpu = {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port",
-               "sample": f"one CPU-oracle proof of 2^{cl} rows ({sec:.2f} s), all host threads"}
+               "sample": f"one CPU-oracle proof of 2^{cl} rows ({sec:.2f} s), all host threads",
+               "cpu_model": cpu_model(), "nproc": os.cpu_count()}
     batched = serving = None
     if world == 1 and not args.no_batched:
         batched = batched_run(wl, args)
