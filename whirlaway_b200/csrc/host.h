@@ -38,7 +38,7 @@ struct HostClock {
   double perm_ms = 0, alloc_ms = 0, launch_ms = 0, upload_ms = 0;
   long perms = 0, allocs = 0, launches = 0, uploads = 0;
   // host time between device waits, by proof phase (the phase current when the wait begins)
-  const char* phase = "setup";
+  std::string phase = "setup";
   double last_wait_end = 0;
   std::vector<std::pair<std::string, double>> busy;
   void add_busy(double ms) {

@@ -209,14 +209,7 @@ ProfScope::~ProfScope() {
 
 void Transcript::host_clock_phase(const char* name) {
   HostClock& hc = host_clock();
-  if (hc.on) {
-    static thread_local std::string names[16];
-    static thread_local int next = 0;
-    for (auto& n : names)
-      if (n == name) { hc.phase = n.c_str(); return; }
-    names[next % 16] = name;
-    hc.phase = names[next++ % 16].c_str();
-  }
+  if (hc.on) hc.phase = name;
 }
 
 void Context::wait_stream() {
