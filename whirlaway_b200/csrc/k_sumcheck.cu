@@ -883,56 +883,10 @@ __global__ void k_eq_limbs(const ef* __restrict__ eq_lo, int nlo, uint8_t* __res
   for (int b = 0; b < 4; b++) limbs[(size_t(b) * 16 + n) * nlo + x] = uint8_t(v >> (8 * b));
 }
 constexpr int ISM_WARPS = 4;  // one per B limb
+constexpr int ISM_STAGES = 4;  // chunks of 32 values in flight per tile
+constexpr int ISM_ROW = 48;    // words per staged row (32 + 16: conflict-free 16-byte fragment reads)
 constexpr int CS_WARPS = 4;   // warps of the kernels whose warps own whole tiles
 
-// The 16-row tile product of a warp: rows g and g + 8 of the tile read nlo consecutive values
-// from pa / pb (zero rows when va / vb is false), B limb b from lb (NT column tiles of 8, each
-// column nlo bytes, lstride u32 apart); acc[a][nt] accumulates A limb a times B limb b.
-template <int NT>
-__device__ __forceinline__ void limb_tile_mma(const uint32_t* pa, const uint32_t* pb, bool va, bool vb,
-                                              const uint32_t* lb, uint32_t lstride, uint32_t nlo, int g, int t,
-                                              int (&acc)[4][NT][4]) {
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int nt = 0; nt < NT; nt++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
-  const uint4 zero4 = make_uint4(0, 0, 0, 0);
-  // the next step's values are requested before this step's products (two steps in flight)
-  uint4 n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa)) : zero4;
-  uint4 n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb)) : zero4;
-  uint4 n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + 16)) : zero4;
-  uint4 n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + 16)) : zero4;
-#pragma unroll 1
-  for (uint32_t k0 = 0; k0 < nlo; k0 += 32) {
-    const uint4 q0 = n0, q1 = n1, q2 = n2, q3 = n3;
-    if (k0 + 32 < nlo) {
-      n0 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 32)) : zero4;
-      n1 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 32)) : zero4;
-      n2 = va ? __ldg(reinterpret_cast<const uint4*>(pa + k0 + 48)) : zero4;
-      n3 = vb ? __ldg(reinterpret_cast<const uint4*>(pb + k0 + 48)) : zero4;
-    }
-    uint32_t l0[4], l1[4], l2[4], l3[4];
-    byte_transpose4(q0, l0);
-    byte_transpose4(q1, l1);
-    byte_transpose4(q2, l2);
-    byte_transpose4(q3, l3);
-    uint32_t bf[NT][2];
-#pragma unroll
-    for (int nt = 0; nt < NT; nt++) {
-      const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (k0 >> 2) + t;
-      bf[nt][0] = __ldg(col);
-      bf[nt][1] = __ldg(col + 4);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
-#pragma unroll
-      for (int nt = 0; nt < NT; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
-    }
-  }
-}
 // Sum over the limb pairs of column value (row, col), from the per-pair accumulators
 // cs[a][b][row][col]: diagonals a + b = d (below 4 * 2^12 * 255^2 < 2^31) weighted by
 // 2^(8d) mod p, then one Montgomery reduction (the sum stays below 4 p^2).
@@ -973,6 +927,7 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
                                                                   ef* __restrict__ pu, ef* __restrict__ pd) {
   __shared__ int cs[4][4][16][17];  // [a][b][row][col], padded
   __shared__ ef up_s[16], dn_s[16];
+  __shared__ __align__(16) uint32_t ism_a[ISM_STAGES][16][ISM_ROW];
   const size_t N = size_t(1) << log_n, S = N >> k;
   const uint32_t nsk = 1u << k, nhi = 1u << (log_n - k - ll), nlo = 1u << ll;
   const uint32_t M = uint32_t(AIR_W) * nsk * nhi;
@@ -983,12 +938,66 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
     const uint32_t xh = m % nhi, cj = m / nhi, j = cj % nsk, c = cj / nsk;
     return size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
   };
-  const uint32_t ra = m0 + g, rb = m0 + g + 8;
-  const bool va = ra < M, vb = rb < M;
-  int acc[4][2][4];
-  limb_tile_mma<2>(wit + (va ? row_base(ra) : 0) + 4 * t, wit + (vb ? row_base(rb) : 0) + 4 * t, va, vb,
-                   reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo), nlo >> 2, nlo, g, t, acc);
-  limb_store<2>(cs, acc, b, g, t);
+  // The tile's 16 segments stream through shared memory in chunks of 32 values (one 16-byte
+  // cp.async per thread and chunk, ISM_STAGES chunks in flight), so the four warps (one per
+  // limb of B) read each value from HBM once; rows past M are zero-filled.
+  {
+    const int crow = threadIdx.x >> 3, cpiece = threadIdx.x & 7;  // 16 rows x 8 pieces
+    const uint32_t mr = m0 + crow;
+    const bool cval = mr < M;
+    const uint32_t* csrc = wit + (cval ? row_base(mr) : 0) + 4 * cpiece;
+    const unsigned cdst0 = (unsigned)__cvta_generic_to_shared(&ism_a[0][crow][4 * cpiece]);
+    const unsigned cstage = sizeof(ism_a[0]);
+    const uint32_t nch = nlo >> 5;
+    auto issue = [&](uint32_t c) {
+      if (c < nch) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(cdst0 + (c % ISM_STAGES) * cstage),
+                     "l"(csrc + 32 * c), "r"(cval ? 16 : 0));
+      }
+      asm volatile("cp.async.commit_group;\n" ::);
+    };
+    for (int c = 0; c < ISM_STAGES - 1; c++) issue(c);
+    int acc[4][2][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
+    const uint32_t* lb = reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo);
+    const uint32_t lstride = nlo >> 2;
+#pragma unroll 1
+    for (uint32_t c = 0; c < nch; c++) {
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(ISM_STAGES - 2));
+      __syncthreads();  // chunk c landed for every thread; the slot of chunk c - 1 is free
+      issue(c + ISM_STAGES - 1);
+      const uint32_t(&X)[16][ISM_ROW] = ism_a[c % ISM_STAGES];
+      const uint4 q0 = *reinterpret_cast<const uint4*>(&X[g][4 * t]);
+      const uint4 q1 = *reinterpret_cast<const uint4*>(&X[g + 8][4 * t]);
+      const uint4 q2 = *reinterpret_cast<const uint4*>(&X[g][16 + 4 * t]);
+      const uint4 q3 = *reinterpret_cast<const uint4*>(&X[g + 8][16 + 4 * t]);
+      uint32_t l0[4], l1[4], l2[4], l3[4];
+      byte_transpose4(q0, l0);
+      byte_transpose4(q1, l1);
+      byte_transpose4(q2, l2);
+      byte_transpose4(q3, l3);
+      uint32_t bf[2][2];
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++) {
+        const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (c << 3) + t;
+        bf[nt][0] = __ldg(col);
+        bf[nt][1] = __ldg(col + 4);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
+      }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    limb_store<2>(cs, acc, b, g, t);
+  }
   __syncthreads();
   // recombination: 256 (row, column) values, two per thread
   for (int e = threadIdx.x; e < 256; e += ISM_WARPS * 32) {
