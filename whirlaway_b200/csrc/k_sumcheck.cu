@@ -8,6 +8,7 @@
 // "up" columns replace the last row by the one before it and "down" columns shift by one
 // row and repeat the last (crates/air/src/utils.rs:140-160); neither is materialised.
 // Folded columns are extension-field arrays, column c at cols + c * len.
+#include <algorithm>
 #include "kernels.h"
 #include "limb_mma.cuh"
 
@@ -785,6 +786,88 @@ __global__ void k_fold_cols(const ef* __restrict__ in, ef* __restrict__ out, siz
   out[size_t(c) * half + x] = ef_lerp(src[x], src[half + x], r ? *r : rv);
 }
 
+// lo + r (hi - lo) for the 16 values of a warp's tile on the tensor cores (byte-limb value
+// form): r d = sum_e d_e (X^e r), so the product is a matrix product with rows = values,
+// reduction index = (coefficient e of d, byte a), columns = (n, b) for the 8 coefficients n and
+// 4 bytes b of the Montgomery form of (X^e r)_n 2^(8a) (the lane's B fragments, fold_frag).
+// One k32 step: four mma per 16 values; acc_b < 32 255^2, one reduction per coefficient.
+__device__ __forceinline__ void fold_frag(const ef& r, int g, int t, uint32_t (&bf)[4][2]) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int e = t + 4 * h;
+    // (X^e r)_g = r_(g - e), times 3 where X^8 = 3 wraps it
+    const uint32_t w = g >= e ? r.c[g - e] : kb::add(kb::dbl(r.c[g - e + 8]), r.c[g - e + 8]);
+    uint32_t m[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) m[a] = kb::mul(w, uint32_t(kb::detail::cpow(2, 8 * a + 32)));
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      bf[b][h] = ((m[0] >> (8 * b)) & 0xffu) | (((m[1] >> (8 * b)) & 0xffu) << 8) |
+                 (((m[2] >> (8 * b)) & 0xffu) << 16) | (((m[3] >> (8 * b)) & 0xffu) << 24);
+  }
+}
+__device__ __forceinline__ void lerp16_mma(const ef* __restrict__ lo, const ef* __restrict__ hi, ef* __restrict__ out,
+                                           uint32_t nv, const uint32_t (&bf)[4][2], int g, int t) {
+  const uint32_t* l32 = reinterpret_cast<const uint32_t*>(lo);
+  const uint32_t* h32 = reinterpret_cast<const uint32_t*>(hi);
+  const bool va = uint32_t(g) < nv, vb = uint32_t(g + 8) < nv;
+  auto dw = [&](int row, int e, bool v) -> uint32_t { return v ? kb::sub(h32[row * 8 + e], l32[row * 8 + e]) : 0u; };
+  const uint32_t af[4] = {dw(g, t, va), dw(g + 8, t, vb), dw(g, t + 4, va), dw(g + 8, t + 4, vb)};
+  int acc[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+#pragma unroll
+    for (int o = 0; o < 4; o++) acc[b][o] = 0;
+    mma_u8_16832(acc[b], af, bf[b][0], bf[b][1]);
+  }
+  auto prod = [&](int o) {
+    return kb::redc(uint64_t(uint32_t(acc[0][o])) + (uint64_t(uint32_t(acc[1][o])) << 8) +
+                    (uint64_t(uint32_t(acc[2][o])) << 16) + (uint64_t(uint32_t(acc[3][o])) << 24));
+  };
+  // lane (g, t) holds coefficients 2t, 2t + 1 of rows g and g + 8
+  if (va) {
+    const uint2 l = reinterpret_cast<const uint2*>(lo + g)[t];
+    reinterpret_cast<uint2*>(out + g)[t] = make_uint2(kb::add(l.x, prod(0)), kb::add(l.y, prod(1)));
+  }
+  if (vb) {
+    const uint2 l = reinterpret_cast<const uint2*>(lo + g + 8)[t];
+    reinterpret_cast<uint2*>(out + g + 8)[t] = make_uint2(kb::add(l.x, prod(2)), kb::add(l.y, prod(3)));
+  }
+}
+// k_fold_cols with the challenge by value, 16 values per warp on the tensor cores; the extra
+// column slot (blockIdx.y == ncols) sums the next eq table as k_fold_cols does.
+__global__ void __launch_bounds__(256) k_fold_cols_mma(const ef* __restrict__ in, ef* __restrict__ out, size_t half,
+                                                      int ncols, ef rv, const ef* __restrict__ eq_in,
+                                                      ef* __restrict__ eq_out, size_t eq_half) {
+  const int c = blockIdx.y;
+  if (c == ncols) {
+    const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x < eq_half) eq_out[x] = ef_add(eq_in[x], eq_in[x + eq_half]);
+    return;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const size_t x0 = (size_t(blockIdx.x) * 8 + warp) * 16;
+  if (x0 >= half) return;  // whole warp
+  uint32_t bf[4][2];
+  fold_frag(rv, g, t, bf);
+  const ef* src = in + size_t(c) * 2 * half;
+  const uint32_t nv = half - x0 < 16 ? uint32_t(half - x0) : 16u;
+  lerp16_mma(src + x0, src + half + x0, out + size_t(c) * half + x0, nv, bf, g, t);
+}
+// k_fold2 with the challenge by value: blockIdx.y selects (a, oa) or (b, ob).
+__global__ void __launch_bounds__(256) k_fold2_mma(const ef* __restrict__ a, const ef* __restrict__ b,
+                                                  ef* __restrict__ oa, ef* __restrict__ ob, size_t half, ef rv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  const size_t x0 = (size_t(blockIdx.x) * 8 + warp) * 16;
+  if (x0 >= half) return;  // whole warp
+  uint32_t bf[4][2];
+  fold_frag(rv, g, t, bf);
+  const ef* src = blockIdx.y ? b : a;
+  ef* dst = blockIdx.y ? ob : oa;
+  const uint32_t nv = half - x0 < 16 ? uint32_t(half - x0) : 16u;
+  lerp16_mma(src + x0, src + half + x0, dst + x0, nv, bf, g, t);
+}
+
 // Per (column c, j < 2^k, x_hi): eq_hi[x_hi] * sum_{x_lo} eq_lo[x_lo] * up_c[j S + x] (and the
 // same for down), x = x_hi 2^ll + x_lo, with eq(tail, x) = eq_hi(x_hi) eq_lo(x_lo) factored so
 // every warp reads the same small eq_lo table. One warp per x_hi; 2^ll is a multiple of 32
@@ -1325,14 +1408,6 @@ __global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, 
   }
 }
 
-__global__ void k_fold2(const ef* __restrict__ a, const ef* __restrict__ b, ef* __restrict__ oa, ef* __restrict__ ob,
-                        size_t half, const ef* __restrict__ r, ef rv) {
-  const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (x >= half) return;
-  const ef rr = r ? *r : rv;
-  oa[x] = ef_lerp(a[x], a[x + half], rr);
-  ob[x] = ef_lerp(b[x], b[x + half], rr);
-}
 
 // ------------------------------------------------------------------ a*b - c
 constexpr int ABC_X = 32;
@@ -1483,9 +1558,10 @@ void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r
 }
 void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef& r, cudaStream_t s, const ef* eq_in,
                          ef* eq_out, size_t eq_half) {
-  const size_t width = eq_in && eq_half > half ? eq_half : half;
-  dim3 grid((unsigned)((width + 255) / 256), ncols + (eq_in ? 1 : 0));
-  k_fold_cols<<<grid, 256, 0, s>>>(in, out, half, ncols, nullptr, r, eq_in, eq_out, eq_half);
+  // 128 values per block for the columns, 256 for the eq table
+  const size_t bx = std::max((half + 127) / 128, eq_in ? (eq_half + 255) / 256 : size_t(0));
+  dim3 grid((unsigned)std::max<size_t>(bx, 1), ncols + (eq_in ? 1 : 0));
+  k_fold_cols_mma<<<grid, 256, 0, s>>>(in, out, half, ncols, r, eq_in, eq_out, eq_half);
   WL_LAUNCH_CHECK();
 }
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
@@ -1570,12 +1646,8 @@ void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaSt
   k_prod_eval<<<prod_blocks(half), PROD_THREADS, 0, s>>>(a, b, half, prod_per_thread(half), partial);
   WL_LAUNCH_CHECK();
 }
-void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s) {
-  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, r, ef_zero());
-  WL_LAUNCH_CHECK();
-}
 void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s) {
-  k_fold2<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(a, b, oa, ob, half, nullptr, r);
+  k_fold2_mma<<<dim3((unsigned)((half + 127) / 128), 2), 256, 0, s>>>(a, b, oa, ob, half, r);
   WL_LAUNCH_CHECK();
 }
 

@@ -119,8 +119,7 @@ void launch_sub_evals(const ef* batched, int log_n, int k, const ef* alpha2, con
 void launch_inner_mle(const ef* eqp, int log_n, const ef* alpha2, ef* out, cudaStream_t s);
 int prod_blocks(size_t half);
 void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s);
-void launch_fold2(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r, cudaStream_t s);
-// The same with the challenge passed by value (no device copy of it).
+// Folds the tables a and b at the challenge r (lo + r (hi - lo)).
 void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s);
 
 // --------------------------------------------------------------- a*b - c zerocheck
