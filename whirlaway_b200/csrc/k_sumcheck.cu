@@ -854,7 +854,7 @@ __global__ void __launch_bounds__(256) k_fold_cols_mma(const ef* __restrict__ in
   const uint32_t nv = half - x0 < 16 ? uint32_t(half - x0) : 16u;
   lerp16_mma(src + x0, src + half + x0, out + size_t(c) * half + x0, nv, bf, g, t);
 }
-// k_fold2 with the challenge by value: blockIdx.y selects (a, oa) or (b, ob).
+// lo + r (hi - lo) for two tables with the challenge by value: blockIdx.y selects (a, oa) or (b, ob).
 __global__ void __launch_bounds__(256) k_fold2_mma(const ef* __restrict__ a, const ef* __restrict__ b,
                                                   ef* __restrict__ oa, ef* __restrict__ ob, size_t half, ef rv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
