@@ -53,6 +53,29 @@ def test_extension_field_identities(oracle):
     assert np.array_equal(x8, np.array([3, 0, 0, 0, 0, 0, 0, 0], np.uint32))
 
 
+def test_two_adic_generator_and_frobenius_order(oracle):
+    """3^127 has multiplicative order 2^24 (p - 1 = 2^24 * 127, 3 generates F_p^*), and the
+    Frobenius a -> a^p of the degree-8 extension has order 8 on a generic element."""
+    w = pow(3, 127, P)
+    assert pow(w, 1 << 24, P) == 1 and pow(w, 1 << 23, P) != 1
+    assert pow(3, (P - 1) // 2, P) != 1 and pow(3, (P - 1) // 127, P) != 1  # 3 is a generator
+
+    def ef_pow(a, e):
+        r = np.array([1, 0, 0, 0, 0, 0, 0, 0], np.uint32)
+        while e:
+            if e & 1:
+                r = oracle.ef_mul(r, a)
+            a = oracle.ef_mul(a, a)
+            e >>= 1
+        return r
+
+    a = _ef_rand(np.random.default_rng(7))
+    x = a
+    for k in range(1, 9):
+        x = ef_pow(x, P)
+        assert np.array_equal(x, a) == (k == 8), k
+
+
 def test_ntt_matches_naive_dft(oracle):
     rng = np.random.default_rng(2)
     for log_size in (1, 3, 6):
