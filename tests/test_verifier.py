@@ -152,3 +152,18 @@ def test_verify_batch_threads(wl, oracle):
         st = wl.verify_batch(consts, jobs, threads=threads)
         assert st[:5] == [OK] * 5 and st[5] != OK and st[6] != OK
         assert st == [wl.verify(consts, l, p) for l, p in jobs]
+
+
+@pytest.mark.parametrize("kw", [dict(univariate_skips=2), dict(log_inv_rate=2), dict(security_bits=100),
+                                dict(rs_domain_initial_reduction=3), dict(whir_pow_bits=10)])
+def test_other_settings_roundtrip(wl, oracle, kw):
+    """The product's WHIR schedule and verifier agree with the oracle prover on non-default
+    settings (the schedule drives the transcript layout, so any mismatch rejects)."""
+    log_n = 7
+    s = wl.AirSettings(**kw)
+    consts, _, proof = honest(oracle, log_n, s.as_array())
+    assert oracle.verify(log_n, consts, proof, s.as_array()) == 0
+    assert wl.verify(consts, log_n, proof, s) == OK
+    assert proof.size <= wl.proof_len_bound(s, log_n)
+    if kw != dict(whir_pow_bits=10):
+        assert wl.verify(consts, log_n, proof) != OK  # the default settings read it differently
