@@ -53,6 +53,20 @@ def test_prove_other_skips_matches_oracle(oracle, wl, ctx, log_n, skips):
     assert wl.verify(consts, log_n, got, settings) == 0
 
 
+@pytest.mark.parametrize("kw", [dict(log_inv_rate=2), dict(security_bits=100), dict(rs_domain_initial_reduction=3),
+                                dict(whir_pow_bits=10), dict(log_inv_rate=3, univariate_skips=3)])
+@pytest.mark.parametrize("log_n", [7, 10])
+def test_prove_other_settings_matches_oracle(oracle, wl, ctx, kw, log_n):
+    """Non-default AirSettings: rate, security level, RS domain reduction, PoW bits."""
+    settings = wl.AirSettings(**kw)
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    ref, _ = oracle.prove(log_n, consts, wit, settings.as_array())
+    got = wl.AirTable(ctx, consts, log_n, settings).prove(wit)
+    assert got.size == ref.size and np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
+    assert wl.verify(consts, log_n, got, settings) == 0
+
+
 def test_transcript_dump_prover_equals_verifier(oracle, wl):
     """The GPU prover's per-phase transcript dump equals the host verifier's reading of its proof."""
     log_n = 8
