@@ -122,7 +122,8 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16_constant
                                        const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                        uint32_t* proof_out, size_t* proof_len, float* round_ms);
 
-/* AirTable::verify (crates/air/src/verify.rs:55-249) on the host CPU: no context, no device.
+/* AirTable::verify (crates/air/src/verify.rs:55-249) on the host CPU: no context, no device
+ * (the Merkle paths of each round's queries are checked on up to 16 host threads).
  * Checks proof_data (canonical u32 words) against the settings, the constants blob and log_n.
  * WL_OK when the proof is accepted; otherwise the AirVerifError outcome of the first failed
  * check (WL_E_INVALID_PCS_COMMITMENT, WL_E_INVALID_PCS_OPENING, WL_E_FS, WL_E_SUMCHECK,

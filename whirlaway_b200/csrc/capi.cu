@@ -309,16 +309,24 @@ wl_status wl_sumcheck_abc_prove_device(wl_ctx* ctx, const uint32_t* p16c, int32_
 }
 
 // Host-only verifiers: no context, no device.
-wl_status wl_verify(const wl_air_settings* s, const uint32_t* constants, int32_t log_n, const uint32_t* proof,
-                    size_t proof_len) {
+namespace {
+wl_status verify_with(const wl_air_settings* s, const uint32_t* constants, int32_t log_n, const uint32_t* proof,
+                      size_t proof_len, int threads) {
   std::string why;
   if (!constants || (!proof && proof_len) || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
   for (size_t i = 0; i < proof_len; i++)
     if (proof[i] >= kb::P) return WL_E_INVALID_ARG;  // not a canonical field element
   return guarded(nullptr, [&] {
     wl::ProofJob job = make_job(s, constants, log_n);
-    return wl_status(wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len));
+    return wl_status(
+        wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len, nullptr, threads));
   });
+}
+}  // namespace
+
+wl_status wl_verify(const wl_air_settings* s, const uint32_t* constants, int32_t log_n, const uint32_t* proof,
+                    size_t proof_len) {
+  return verify_with(s, constants, log_n, proof, proof_len, 0);
 }
 
 namespace {
@@ -373,7 +381,8 @@ wl_status wl_verify_batch(const wl_air_settings* s, const uint32_t* constants, i
     T = std::max(1, std::min(T, n));
     std::atomic<int> next{0};
     auto work = [&] {
-      for (int i = next++; i < n; i = next++) statuses[i] = wl_verify(s, constants, log_ns[i], proofs[i], proof_lens[i]);
+      for (int i = next++; i < n; i = next++)
+        statuses[i] = verify_with(s, constants, log_ns[i], proofs[i], proof_lens[i], 1);  // one thread per proof
     };
     std::vector<std::thread> pool;
     for (int t = 1; t < T; t++) pool.emplace_back(work);

@@ -10,6 +10,8 @@
 // sumcheck (short proof, grinding, a round sum) is a sumcheck error, anything inside the WHIR
 // opening an opening error.
 #include <algorithm>
+#include <thread>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -172,8 +174,9 @@ struct Group {
 
 class WhirVerifier {
  public:
-  WhirVerifier(const WhirSchedule& ws, const kb::P16Consts& p16, const kb::P24Consts& p24, ProofReader& rd)
-      : ws_(ws), p16_(p16), p24_(p24), rd_(rd) {}
+  WhirVerifier(const WhirSchedule& ws, const kb::P16Consts& p16, const kb::P24Consts& p24, ProofReader& rd,
+               int threads)
+      : ws_(ws), p16_(p16), p24_(p24), rd_(rd), threads_(threads) {}
 
   // Commitment: the root, then one answer per OOD sample z at the point (z, z^2, z^4, ...).
   bool parse_commitment(Digest& root, std::vector<std::vector<ef>>& pts, std::vector<ef>& vals) {
@@ -285,30 +288,56 @@ class WhirVerifier {
     std::sort(q.begin(), q.end());
     q.erase(std::unique(q.begin(), q.end()), q.end());
     if (rd_.log) rd_.log->add("queries", rd_.pos, q.data(), q.size(), false);
+    // the hints are read in order; the paths are then checked and the rows folded in parallel
+    // (each query is independent: one leaf sponge, ll compressions, one fold)
+    const size_t nq = q.size(), rl = 128, pl = size_t(8) * ll;
+    std::vector<uint32_t> rows(nq * rl), paths(nq * pl);
+    for (size_t i = 0; i < nq; i++)
+      if (!rd_.hint(&rows[i * rl], rl) || !rd_.hint(&paths[i * pl], pl)) return false;
     const std::vector<ef>& r = blocks_.back();
-    for (uint32_t idx : q) {
-      std::vector<uint32_t> row(128), path(size_t(8) * ll);
-      if (!rd_.hint(row.data(), row.size()) || !rd_.hint(path.data(), path.size())) return false;
-      Digest cur = leaf_digest(row.data(), p24_);
+    folded.assign(nq, kb::ef_zero());
+    std::vector<char> good(nq, 0);
+    auto check = [&](size_t i) {
+      const uint32_t* row = &rows[i * rl];
+      const uint32_t* path = &paths[i * pl];
+      Digest cur = leaf_digest(row, p24_);
       for (int l = 0; l < ll; l++) {
         Digest sib;
         for (int e = 0; e < 8; e++) sib[e] = path[size_t(l) * 8 + e];
-        cur = ((idx >> l) & 1) ? compress(sib, cur, p16_) : compress(cur, sib, p16_);
+        cur = ((q[i] >> l) & 1) ? compress(sib, cur, p16_) : compress(cur, sib, p16_);
       }
-      if (cur != root) return false;
+      if (cur != root) return;
       const int k = rc.fold;
       std::vector<ef> v(size_t(1) << k);
       for (size_t p = 0; p < v.size(); p++) {
         v[p] = kb::ef_zero();
         for (int e = 0; e < elem; e++) v[p].c[e] = row[p * elem + e];
       }
-      for (int i = 0; i < k; i++) {
+      for (int j = 0; j < k; j++) {
         const size_t h = v.size() / 2;
-        for (size_t p = 0; p < h; p++) v[p] = kb::ef_add(v[p], kb::ef_mul(r[i], v[p + h]));
+        for (size_t p = 0; p < h; p++) v[p] = kb::ef_add(v[p], kb::ef_mul(r[j], v[p + h]));
         v.resize(h);
       }
-      folded.push_back(v[0]);
+      folded[i] = v[0];
+      good[i] = 1;
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t cap = threads_ > 0 ? size_t(threads_) : std::min<size_t>(hw ? hw : 1, 16);
+    const size_t T = std::min<size_t>(cap, (nq + 7) / 8);
+    if (T <= 1) {
+      for (size_t i = 0; i < nq; i++) check(i);
+    } else {
+      std::atomic<size_t> next{0};
+      auto work = [&] {
+        for (size_t i = next++; i < nq; i = next++) check(i);
+      };
+      std::vector<std::thread> pool;
+      for (size_t t = 1; t < T; t++) pool.emplace_back(work);
+      work();
+      for (auto& th : pool) th.join();
     }
+    for (size_t i = 0; i < nq; i++)
+      if (!good[i]) return false;
     return true;
   }
 
@@ -316,6 +345,7 @@ class WhirVerifier {
   const kb::P16Consts& p16_;
   const kb::P24Consts& p24_;
   ProofReader& rd_;
+  int threads_;                          // host threads for the query checks (0: up to 16)
   std::vector<std::vector<ef>> blocks_;  // folding randomness of each sumcheck block
   std::vector<Group> groups_;
 };
@@ -323,13 +353,13 @@ class WhirVerifier {
 }  // namespace
 
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
-                     int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log) {
+                     int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log, int threads) {
   const int k = s.univariate_skips, W = AIR_W, nsk = 1 << k;
   const WhirSchedule ws = WhirSchedule::build(n + AIR_LOG_W, s);
   ProofReader rd(&p16, proof, proof_len, log);
   for (uint32_t x : ws.domain_separator()) rd.ch.observe(kb::to_mont(x));
   rd.phase("commit");
-  WhirVerifier whir(ws, p16, p24, rd);
+  WhirVerifier whir(ws, p16, p24, rd, threads);
   Digest root;
   std::vector<std::vector<ef>> ood_pts;
   std::vector<ef> ood_vals;

@@ -20,9 +20,11 @@ enum VerifyOutcome : int {
 
 // proof: proof_data as canonical u32 words; constants in Montgomery form.
 // With log, the transcript as read (phases, challenges, queries, grinding witnesses) is recorded
-// in the same form as the prover's (Transcript::log), up to the first failed check.
+// in the same form as the prover's (Transcript::log), up to the first failed check. The Merkle
+// paths of each round's queries are checked on `threads` host threads (0: up to 16).
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
-                     int log_n, const uint32_t* proof, size_t proof_len, TranscriptLog* log = nullptr);
+                     int log_n, const uint32_t* proof, size_t proof_len, TranscriptLog* log = nullptr,
+                     int threads = 0);
 int verify_abc_proof(const kb::P16Consts& p16, int log_n, int skips, const uint32_t* proof, size_t proof_len);
 
 }  // namespace wl
