@@ -41,7 +41,7 @@ def test_prove_matches_oracle(oracle, wl, ctx, log_n):
     assert wl.verify(consts, log_n, got) == 0  # the product's host verifier
 
 
-@pytest.mark.parametrize("log_n,skips", [(8, 1), (8, 2), (9, 3), (6, 3)])
+@pytest.mark.parametrize("log_n,skips", [(8, 1), (8, 2), (9, 3), (6, 3), (2, 1), (3, 2), (4, 3), (4, 1)])
 def test_prove_other_skips_matches_oracle(oracle, wl, ctx, log_n, skips):
     """Univariate skips below 4: fewer round-0 points (2, 6, 14) than the 30 of the default."""
     settings = wl.AirSettings(univariate_skips=skips)

@@ -167,3 +167,14 @@ def test_other_settings_roundtrip(wl, oracle, kw):
     assert proof.size <= wl.proof_len_bound(s, log_n)
     if kw != dict(whir_pow_bits=10):
         assert wl.verify(consts, log_n, proof) != OK  # the default settings read it differently
+
+
+@pytest.mark.parametrize("log_n,skips", [(2, 1), (3, 2), (4, 3), (5, 4)])
+def test_tiny_tables(wl, oracle, log_n, skips):
+    """The smallest tables the settings allow (no WHIR folding round before the final one)."""
+    s = wl.AirSettings(univariate_skips=skips)
+    consts, _, proof = honest(oracle, log_n, s.as_array())
+    assert wl.verify(consts, log_n, proof, s) == OK
+    bad = proof.copy()
+    bad[proof.size // 3] = (int(bad[proof.size // 3]) + 1) % P
+    assert wl.verify(consts, log_n, bad, s) != OK
