@@ -153,11 +153,12 @@ Digest leaf_digest(const uint32_t* row, const kb::P24Consts& p24) {
   for (int i = 0; i < 8; i++) d[i] = s[i];
   return d;
 }
-// 2-to-1 compression: the first 8 words of Poseidon2-16(left || right).
+// 2-to-1 compression: the first 8 words of Poseidon2-16(left || right) (the transcript's host
+// permutation: AVX-512 when the CPU has it).
 Digest compress(const Digest& l, const Digest& r, const kb::P16Consts& p16) {
   uint32_t s[16];
   for (int i = 0; i < 8; i++) s[i] = l[i], s[8 + i] = r[i];
-  kb::p2_permute<16>(s, p16);
+  host_p16_permute(s, p16);
   Digest d;
   for (int i = 0; i < 8; i++) d[i] = s[i];
   return d;
