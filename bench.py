@@ -51,8 +51,12 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--batch-size", type=int, default=64)
     ap.add_argument("--workers", type=int, default=16)
-    ap.add_argument("--serving-requests", type=int, default=200,
-                    help="requests per arrival rate (the full serving configuration uses 2000)")
+    ap.add_argument("--no-sumcheck", action="store_true")
+    ap.add_argument("--sumcheck-log-n", type=int, default=24)
+    ap.add_argument("--sumcheck-reps", type=int, default=3)
+    ap.add_argument("--serving-requests", type=int, default=2000, help="requests per arrival rate")
+    ap.add_argument("--serving-rates", type=str, default="1,4",
+                    help="offered load as multiples of the plain path's capacity on the mix")
     return ap.parse_args()
 
 
@@ -326,21 +330,99 @@ def batched_run(wl, args):
             "timing": "host wall clock around submit-all/wait-all, inputs on the host (trace generated on the GPU)"}
 
 
-def serving_run(wl, args, plain_rate_hint):
+def sumcheck_run(wl, ctx, args):
+    """Sumcheck + folding microbench: the zerocheck of eq(r, x) * (a(x) b(x) - c(x)) over three
+    columns of 2^24 base-field values (a, b uniform from a seed, c = a * b so that the
+    constraint vanishes), with the first round univariate-skipping 3 variables; per-round times
+    (CUDA events on the library's stream, from the round's first launch to its fold, host
+    transcript work between them included) and each round's algorithmic HBM bytes."""
+    import numpy as np
+    import torch
+    log_n, k = args.sumcheck_log_n, 3
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    p = 0x7F000001
+    a = torch.randint(0, p, (1 << log_n,), generator=gen, device="cuda", dtype=torch.int64)
+    b = torch.randint(0, p, (1 << log_n,), generator=gen, device="cuda", dtype=torch.int64)
+    c = (a * b) % p
+    a, b, c = (x.to(torch.int32) for x in (a, b, c))
+    consts, _ = wl.generate_workload(2)
+    p16 = consts[148:296]
+    for _ in range(2):
+        proof, _ = wl.sumcheck_abc_prove(ctx, p16, log_n, k, a, b, c, device=True)
+    runs = [wl.sumcheck_abc_prove(ctx, p16, log_n, k, a, b, c, device=True)[1] for _ in range(args.sumcheck_reps)]
+    rounds = [float(np.median([r[i] for r in runs])) for i in range(len(runs[0]))]
+    assert wl.sumcheck_abc_verify(p16, log_n, k, proof) == 0
+    S = 1 << (log_n - k)
+    # round 0 reads a, b, c (4 B each) and writes the three folded columns (32 B extension
+    # values); round i >= 1 reads 3 columns of 2^(n-k-i+1) values and the eq table, and writes
+    # the halves
+    byts = [3 * (1 << log_n) * 4 + 3 * S * 32 + (S // 2) * 32]
+    m = log_n - k
+    for i in range(1, m + 1):
+        ln = 1 << (m - i + 1)
+        byts.append(3 * ln * 32 + (ln // 2) * 32 + 3 * (ln // 2) * 32 + (ln // 4) * 32)
+    total = sum(rounds)
+    return {"workload": f"zerocheck of eq * (a*b - c), three columns of 2^{log_n} base-field values, "
+                        f"univariate skip {k}, {len(rounds)} rounds",
+            "round_ms": [round(x, 4) for x in rounds], "total_ms": total,
+            "round_hbm_gbs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(byts, rounds)],
+            "round0_hbm_frac": byts[0] / (rounds[0] * 1e-3) / 1e9 / args.hbm_peak,
+            "algorithmic_bytes": sum(byts), "reps": args.sumcheck_reps, "verified": True,
+            "timing": "median over reps of CUDA-event time per round on the prover's stream"}
+
+
+def sumcheck_cpu_baseline(args):
+    """The oracle's a*b - c zerocheck on the same microbench size, all host threads."""
+    import numpy as np
+    from tests import oracle_lib
+    oracle = oracle_lib.load()
+    log_n, k = args.sumcheck_log_n, 3
+    rng = np.random.default_rng(7)
+    p = 0x7F000001
+    a = rng.integers(0, p, 1 << log_n, dtype=np.uint64)
+    b = rng.integers(0, p, 1 << log_n, dtype=np.uint64)
+    c = (a * b) % p
+    a, b, c = (x.astype(np.uint32) for x in (a, b, c))
+    consts, _ = oracle.workload(2)
+    t0 = time.perf_counter()
+    oracle.prove_abc(consts[148:296], log_n, k, a, b, c)
+    dt = time.perf_counter() - t0
+    return {"total_ms": dt * 1e3, "cores": oracle.lib.wlo_max_threads(), "kind": "port",
+            "sample": f"one oracle proof of the full microbench (2^{log_n} rows, skip {k})"}
+
+
+def serving_run(wl, args):
     """Serving configuration: Poisson arrivals of requests with log2 rows log-uniform on
-    [12, 20] (rounded), admitted by HBM footprint against a 160 GB budget."""
+    [12, 20] (rounded), admitted by HBM footprint against a 160 GB budget. Offered loads are
+    multiples of the plain path's capacity on this mix (proofs one at a time on one stream,
+    measured on the first requests). Inputs come from a pool of four seeded instances per
+    size (each request still has its own transcript and proof)."""
     import threading
     import numpy as np
     rng = np.random.default_rng(1)
     R = args.serving_requests
     sizes = [int(round(x)) for x in rng.uniform(12, 20, R)]
-    inputs = [wl.generate_workload(n, 5000 + k) for k, n in enumerate(sizes)]
+    pool = {n: [wl.generate_workload(n, 5000 + 16 * n + j) for j in range(4)] for n in sorted(set(sizes))}
+    inputs = [pool[n][k % 4] for k, n in enumerate(sizes)]
     mean_rows = float(np.mean([1 << n for n in sizes]))
-    base = plain_rate_hint / mean_rows  # requests/s the plain path sustains on this mix
+    # the plain path's rate on this mix, from its first requests proved one at a time
+    sample = list(zip(inputs, sizes))[:48]
+    with wl.Context(0) as ctx:
+        for (c, i), n in sample[:2]:
+            w = wl.Witness.generate(ctx, c, i, n)
+            wl.AirTable(ctx, c, n).prove_witness(w)
+            w.free()
+        t0 = time.perf_counter()
+        for (c, i), n in sample:
+            w = wl.Witness.generate(ctx, c, i, n)
+            wl.AirTable(ctx, c, n).prove_witness(w)
+            w.free()
+        plain_rate = sum(1 << n for _, n in sample) / (time.perf_counter() - t0)
+    base = plain_rate / mean_rows  # requests/s the plain path sustains on this mix
     out = []
     with wl.Server(0, workers=args.workers, hbm_budget_bytes=160 << 30) as srv:
         wl.batch_prove(srv, [(c, i, n) for (c, i), n in list(zip(inputs, sizes))[:args.workers]])
-        for mult in (0.5, 1.0, 2.0, 4.0):
+        for mult in [float(x) for x in args.serving_rates.split(",")]:
             lam = base * mult
             gaps = rng.exponential(1.0 / lam, R)
             tickets = [None] * R
@@ -369,14 +451,15 @@ def serving_run(wl, args, plain_rate_hint):
             th.join()
             wall = done_t - t0
             lat = np.array(lat)
+            sustained = sum(1 << n for n in sizes) / wall
             out.append({"offered_requests_per_s": lam, "offered_x_plain_capacity": mult,
-                        "sustained_perms_per_s": sum(1 << n for n in sizes) / wall,
+                        "sustained_perms_per_s": sustained, "sustained_x_plain": sustained / plain_rate,
                         "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99))})
         stats = srv.stats()
     return {"requests_per_rate": R, "log_n_rows": "log-uniform on [12, 20], rounded, seed 1",
             "hbm_budget_bytes": 160 << 30, "workers": args.workers, "peak_running": stats["peak_running"],
-            "peak_bytes_admitted": stats["peak_bytes_admitted"], "rates": out,
-            "timing": "host wall clock; latency = submission to proof ready"}
+            "peak_bytes_admitted": stats["peak_bytes_admitted"], "plain_one_at_a_time_perms_per_s": plain_rate,
+            "rates": out, "timing": "host wall clock; latency = submission to proof ready"}
 
 
 def run_ours(args, world, rank, local):
@@ -449,6 +532,9 @@ def run_ours(args, world, rank, local):
                "h2d_bytes_per_step": int(host_np.nbytes), "d2h_bytes_per_step": int(p2.nbytes),
                "ms_per_step": e2e_ms / args.steps}
 
+    # the timed proof is checked by the library's host verifier (AirTable::verify), as the
+    # reference verifies the proof it times (src/examples/poseidon2.rs:177-189)
+    verified = wl.verify(consts, log_n, proof) == 0
     if rank != 0:
         return
     try:
@@ -463,17 +549,21 @@ def run_ours(args, world, rank, local):
         cpu = {"value": rate, "unit": "perms/s", "cores": cores, "kind": "port",
                "sample": f"one CPU-oracle proof of 2^{cl} rows ({sec:.2f} s), all host threads",
                "cpu_model": cpu_model(), "nproc": os.cpu_count()}
-    batched = serving = None
+    args.hbm_peak = hbm_peak
+    batched = serving = sumcheck = None
+    if world == 1 and not args.no_sumcheck:
+        sumcheck = sumcheck_run(wl, ctx, args)
+        if not args.no_cpu_baseline:
+            sumcheck["cpu_baseline"] = sumcheck_cpu_baseline(args)
     if world == 1 and not args.no_batched:
         batched = batched_run(wl, args)
     if world == 1 and not args.no_serving:
-        hint = batched["plain_one_at_a_time_perms_per_s"] if batched else value
-        serving = serving_run(wl, args, hint)
+        serving = serving_run(wl, args)
     line = {
         "metric": METRIC, "value": value, "unit": "perms/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear Montgomery; exact modular integer)",
-        "data": "synthetic", "config": workload_config(log_n),
+        "data": "synthetic", "config": workload_config(log_n), "verified": bool(verified),
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "roofline": roofline(profile, breakdown, log_n, modmul_peak, hbm_peak, args.steps, p24_peak),
         "cpu_baseline": cpu,
@@ -485,6 +575,7 @@ def run_ours(args, world, rank, local):
         "kernel_profile_source": "CUDA events per kernel class over the last warm-up proof",
         "host_profile_ms": host_profile,
         "proof_len": int(proof.size),
+        "sumcheck_microbench": sumcheck,
         "batched": batched,
         "serving": serving,
     }

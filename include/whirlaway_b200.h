@@ -161,17 +161,20 @@ wl_status wl_sumcheck_abc_verify(const uint32_t* p16_constants, int32_t log_n, i
                                  size_t proof_len);
 
 /* Allocation-free variant of wl_sumcheck_abc_prove_device; it has no counterpart in the
- * reference. For callers that cannot allocate device memory (code running where cudaMalloc is
- * not allowed, such as host callbacks, processes whose device memory another framework has
- * already partitioned, or paths that must not touch an allocator): it makes no device, pinned
- * or host-heap allocation. Its device scratch is a fixed 4 MiB array inside the library
+ * reference. For callers that cannot allocate device memory: processes whose device memory
+ * another framework owns and has already partitioned, and latency paths that must not enter
+ * an allocator (an allocation can map new memory and stall the device). It makes no device,
+ * pinned or host-heap allocation. Its device scratch is a fixed 4 MiB array inside the library
  * (present on every device that loads the library, until exit), which limits log_n to 14
  * (WL_E_SCRATCH_LIMIT beyond). Inputs are canonical device arrays of 2^log_n values, left
  * unchanged; the proof (host buffer, its exact length is returned with WL_E_BUFFER_TOO_SMALL
  * when short) equals wl_sumcheck_abc_prove_device's. `stream` is a cudaStream_t (NULL: the
  * default stream). All calls share the scratch array: calls that overlap on the GPU race and
- * must be serialised. The first call on a device looks up the array's address; make it
- * before any stream capture. */
+ * must be serialised. The call copies between host and device and waits for its stream
+ * between rounds, so it must not be called from a stream callback or host function (where
+ * CUDA calls are not permitted) and rejects a stream under graph capture (WL_E_INVALID_ARG).
+ * The first call on a device looks up the array's address (a failed lookup is retried by the
+ * next call). */
 wl_status wl_sumcheck_abc_prove_noalloc(const uint32_t* p16_constants, int32_t log_n, int32_t skips,
                                         const uint32_t* a_dev, const uint32_t* b_dev, const uint32_t* c_dev,
                                         uint32_t* proof_out, size_t* proof_len, void* stream);
@@ -186,7 +189,9 @@ wl_status wl_sumcheck_abc_prove_noalloc(const uint32_t* p16_constants, int32_t l
  * witness. Tickets are thread-safe to submit, poll and wait on. */
 typedef struct wl_server wl_server;
 typedef enum { WL_JOB_QUEUED = 0, WL_JOB_RUNNING = 1, WL_JOB_DONE = 2, WL_JOB_FAILED = 3 } wl_job_state;
-uint64_t wl_proof_footprint_bytes(int32_t log_n);
+/* Upper bound of the device memory one proof of 2^log_n rows takes under `settings` (NULL: the
+ * defaults), by phase from the prover's buffer sizes; 0 for invalid arguments. */
+uint64_t wl_proof_footprint_bytes(const wl_air_settings* settings, int32_t log_n);
 wl_status wl_server_create(int32_t device, int32_t workers, uint64_t hbm_budget_bytes, wl_server** out);
 void wl_server_destroy(wl_server* server); /* finishes queued and running jobs first */
 const char* wl_server_last_error(const wl_server* server);

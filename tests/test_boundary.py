@@ -41,6 +41,9 @@ def test_host_entry_points_without_gpu(wl, oracle):
     with pytest.raises(wl.ProverError):
         wl.proof_len_bound(wl.AirSettings(univariate_skips=4), 4)  # skips must be < log_n
     assert wl.proof_footprint_bytes(20) > 3 << 30
+    # rate 1/8 quadruples the first commitment; invalid settings give 0
+    assert wl.proof_footprint_bytes(20, wl.AirSettings(log_inv_rate=3)) > 2 * wl.proof_footprint_bytes(20)
+    assert wl.proof_footprint_bytes(3, wl.AirSettings(univariate_skips=4)) == 0
 
 
 def test_device_field_arithmetic_on_host(tmp_path):

@@ -108,3 +108,63 @@ def test_sumcheck_abc_matches_oracle(oracle, wl, ctx, log_n, skips):
     assert oracle.verify_abc(p16, log_n, skips, got) == 0
     assert wl.sumcheck_abc_verify(p16, log_n, skips, got) == 0
     assert len(ms) == log_n - skips + 1
+
+
+# Production-size parity. The kernels that switch on only for large tables run here:
+#  - zerocheck rounds >= 1 with at least 2^10 points per z use k_zc_full_dense and
+#    k_zc_partial_dense (log_n - skips - 1 >= 10, i.e. log_n >= 15 at 4 skips);
+#  - LDE passes after the first use the persistent double-buffered k_ntt_pass_async when a
+#    pass has at least 4 lines per resident block (2^(n+2)-row codeword of 88 columns: 11,264
+#    lines at log_n 15 and 16 against 2,368 blocks' worth);
+#  - Merkle levels of at least 2^13 digests get one launch per level (5 levels at log_n 16).
+# The oracle proves 2^16 rows in 10-20 s on the host threads; each proof is computed once.
+_big_cache = {}
+
+
+def _oracle_big(oracle, log_n, skips):
+    key = (log_n, skips)
+    if key not in _big_cache:
+        settings = np.array([128, 1, 7, 4, skips, 5, 16], np.int32)
+        consts, inputs = oracle.workload(log_n)
+        wit = oracle.trace(log_n, consts, inputs)
+        ref, _ = oracle.prove(log_n, consts, wit, settings)
+        _big_cache[key] = (consts, inputs, wit, ref)
+    return _big_cache[key]
+
+
+@pytest.mark.parametrize("log_n,skips,path", [(15, 4, "device"), (16, 4, "device"), (16, 4, "host"),
+                                              (16, 3, "device")])
+def test_prove_production_sizes_match_oracle(oracle, wl, ctx, log_n, skips, path):
+    consts, inputs, wit, ref = _oracle_big(oracle, log_n, skips)
+    settings = wl.AirSettings(univariate_skips=skips)
+    table = wl.AirTable(ctx, consts, log_n, settings)
+    ctx.profile(True)
+    if path == "device":
+        w = wl.Witness.generate(ctx, consts, inputs, log_n)
+        got = table.prove_witness(w)
+        w.free()
+    else:
+        got = table.prove(wit)
+    classes = ctx.profile_report()
+    ctx.profile(False)
+    assert "zc_eval_dense" in classes, "the dense zerocheck kernels did not run"
+    assert got.size == ref.size and np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
+    assert wl.verify(consts, log_n, got, settings) == 0
+
+
+@pytest.mark.parametrize("log_n,skips", [(16, 3), (18, 3), (24, 3)])
+def test_sumcheck_abc_large_matches_oracle(oracle, wl, ctx, log_n, skips):
+    """The a*b - c zerocheck of the sumcheck microbench at larger tables, up to its full size
+    (three columns of 2^24, univariate skip 3)."""
+    rng = np.random.default_rng(log_n * 10 + skips)
+    p = 0x7F000001
+    a = rng.integers(0, p, 1 << log_n, dtype=np.uint64)
+    b = rng.integers(0, p, 1 << log_n, dtype=np.uint64)
+    c = (a * b) % p
+    a, b, c = (x.astype(np.uint32) for x in (a, b, c))
+    consts, _ = oracle.workload(2)
+    p16 = consts[148:296]
+    ref = oracle.prove_abc(p16, log_n, skips, a, b, c)
+    got, ms = wl.sumcheck_abc_prove(ctx, p16, log_n, skips, a, b, c)
+    assert np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
+    assert wl.sumcheck_abc_verify(p16, log_n, skips, got) == 0

@@ -54,3 +54,70 @@ def test_server_rejects_oversized_job(wl):
         with pytest.raises(wl.ProverError) as e:
             srv.submit(c, i, 10)
         assert e.value.status == 6  # WL_E_BUDGET
+
+
+def _pool():
+    """The device's default stream-ordered pool (where the prover's buffers are carved)."""
+    from cuda.bindings import driver as drv
+    assert drv.cuInit(0)[0] == drv.CUresult.CUDA_SUCCESS
+    err, dev = drv.cuDeviceGet(0)
+    assert err == drv.CUresult.CUDA_SUCCESS
+    err, pool = drv.cuDeviceGetDefaultMemPool(dev)
+    assert err == drv.CUresult.CUDA_SUCCESS
+    return drv, pool
+
+
+def _pool_used(drv, pool, attr):
+    err, v = drv.cuMemPoolGetAttribute(pool, attr)
+    assert err == drv.CUresult.CUDA_SUCCESS
+    return int(v)
+
+
+def _pool_reset_high(drv, pool):
+    err, = drv.cuMemPoolSetAttribute(pool, drv.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH,
+                                      drv.cuuint64_t(0))
+    assert err == drv.CUresult.CUDA_SUCCESS
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(log_inv_rate=3), dict(univariate_skips=2), dict(rs_domain_initial_reduction=3)])
+def test_footprint_bounds_measured_device_memory(wl, kw):
+    """The admission estimate (wl_proof_footprint_bytes) bounds the device memory a proof
+    really takes: the pool's high-water mark over one served proof, at several sizes and
+    settings (the rate scales the first commitment, the skips the zerocheck tables)."""
+    import torch
+    drv, pool = _pool()
+    A = drv.CUmemPool_attribute
+    settings = wl.AirSettings(**kw)
+    with wl.Server(0, workers=1) as srv:
+        for n in (10, 14, 16):
+            c, i = wl.generate_workload(n, 40 + n)
+            torch.cuda.synchronize()
+            base = _pool_used(drv, pool, A.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+            _pool_reset_high(drv, pool)
+            srv.wait(srv.submit(c, i, n, settings), n, settings)
+            high = _pool_used(drv, pool, A.CU_MEMPOOL_ATTR_USED_MEM_HIGH) - base
+            est = wl.proof_footprint_bytes(n, settings)
+            assert high <= est, (n, kw, high, est)
+            if n == 16:
+                assert high >= est // 3, (n, kw, high, est)  # the bound is not vacuous
+
+
+def test_served_mix_device_memory_within_admitted(wl):
+    """During a served mix the pool's high-water mark stays within the bytes the server
+    admitted (its peak of summed footprints of running proofs)."""
+    import torch
+    drv, pool = _pool()
+    A = drv.CUmemPool_attribute
+    sizes = [14, 12, 15, 13, 14, 11, 15, 12, 13, 14]
+    jobs = _jobs(wl, sizes, 900)
+    with wl.Server(0, workers=4) as srv:
+        torch.cuda.synchronize()
+        base = _pool_used(drv, pool, A.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+        _pool_reset_high(drv, pool)
+        tickets = [srv.submit(c, i, n) for c, i, n in jobs]
+        for t, (_, _, n) in zip(tickets, jobs):
+            srv.wait(t, n)
+        high = _pool_used(drv, pool, A.CU_MEMPOOL_ATTR_USED_MEM_HIGH) - base
+        stats = srv.stats()
+    assert stats["peak_running"] >= 2
+    assert high <= stats["peak_bytes_admitted"], (high, stats)

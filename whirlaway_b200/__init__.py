@@ -98,7 +98,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_kernel_launch_count": (ctypes.c_uint64, []),
         "wl_sumcheck_abc_prove_noalloc": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, _u32p,
                                                          _sizep, vp]),
-        "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.c_int32]),
+        "wl_proof_footprint_bytes": (ctypes.c_uint64, [vp, ctypes.c_int32]),
         "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_verify_batch": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
@@ -418,9 +418,9 @@ def sumcheck_abc_verify(p16_constants: np.ndarray, log_n: int, skips: int, proof
     return load_library().wl_sumcheck_abc_verify(_ptr(c), log_n, skips, _ptr(pr), pr.size)
 
 
-def proof_footprint_bytes(log_n: int) -> int:
-    """Device bytes the server reserves for one proof of 2^log_n rows."""
-    return load_library().wl_proof_footprint_bytes(log_n)
+def proof_footprint_bytes(log_n: int, settings: AirSettings = AirSettings()) -> int:
+    """Device bytes the server reserves for one proof of 2^log_n rows under `settings`."""
+    return load_library().wl_proof_footprint_bytes(ctypes.byref(settings._c()), log_n)
 
 
 class Server:

@@ -384,10 +384,7 @@ wl_status wl_verify_batch(const wl_air_settings* s, const uint32_t* constants, i
       for (int i = next++; i < n; i = next++)
         statuses[i] = verify_with(s, constants, log_ns[i], proofs[i], proof_lens[i], 1);  // one thread per proof
     };
-    std::vector<std::thread> pool;
-    for (int t = 1; t < T; t++) pool.emplace_back(work);
-    work();
-    for (auto& th : pool) th.join();
+    wl::run_on_threads(size_t(T), work);
     return WL_OK;
   });
 }
@@ -488,7 +485,16 @@ wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* mod
   });
 }
 
-uint64_t wl_proof_footprint_bytes(int32_t log_n) { return wl::proof_footprint_bytes(log_n); }
+uint64_t wl_proof_footprint_bytes(const wl_air_settings* s, int32_t log_n) {
+  wl_air_settings d;
+  if (!s) {
+    wl_default_settings(&d);
+    s = &d;
+  }
+  std::string why;
+  if (!settings_ok(s, log_n, why)) return 0;
+  return wl::proof_footprint_bytes(to_settings(s), log_n);
+}
 
 wl_status wl_server_create(int32_t device, int32_t workers, uint64_t budget, wl_server** out) {
   if (!out || workers < 1 || workers > 64) return WL_E_INVALID_ARG;

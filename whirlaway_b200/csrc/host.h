@@ -7,8 +7,12 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdint>
+#include <exception>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "air.cuh"
@@ -405,6 +409,33 @@ inline kb::P2Consts<W> perm_consts_from(const uint32_t* c) {
   for (int k = 0; k < 4 * W; k++) p.ext_term[k] = kb::to_mont(c[i++]);
   for (int k = 0; k < kb::P2Consts<W>::RP; k++) p.internal[k] = kb::to_mont(c[i++]);
   return p;
+}
+
+
+// Runs `work` on the calling thread and on up to T - 1 more host threads, then joins them.
+// A thread that cannot be started (the process is at its thread limit) leaves the work to the
+// threads already running; an exception thrown by `work` on any thread is rethrown here after
+// every thread has been joined, so nothing terminates the process.
+template <class Work>
+void run_on_threads(size_t T, Work&& work) {
+  std::exception_ptr first;
+  std::mutex mu;
+  auto guarded = [&] {
+    try {
+      work();
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!first) first = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  try {
+    for (size_t t = 1; t < T; t++) pool.emplace_back(guarded);
+  } catch (const std::system_error&) {
+  }
+  guarded();
+  for (auto& th : pool) th.join();
+  if (first) std::rethrow_exception(first);
 }
 
 }  // namespace wl

@@ -1529,6 +1529,7 @@ void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* o
 }
 // Rounds with at least ZC_DENSE_MIN_HALF points per z use the dense kernels.
 constexpr size_t ZC_DENSE_MIN_HALF = size_t(1) << 10;
+bool zc_eval_is_dense(int m) { return (size_t(1) << (m - 1)) >= ZC_DENSE_MIN_HALF; }
 int zc_ef_blocks(int m) {  // partial sums per z
   const size_t half = size_t(1) << (m - 1);
   if (half < ZC_DENSE_MIN_HALF) return (int)half;

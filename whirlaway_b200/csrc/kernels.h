@@ -91,6 +91,9 @@ void launch_zc0_eval(const uint32_t* wit, const uint32_t* q, int log_n, int k, i
                      cudaStream_t s);
 void launch_zc0_fold(const uint32_t* wit, int log_n, int k, const ef* sel, ef* out, cudaStream_t s);
 int zc_ef_blocks(int m);
+// True when the round over m variables runs on the dense kernels (k_zc_full_dense,
+// k_zc_partial_dense) rather than one block per point (k_zc_ef).
+bool zc_eval_is_dense(int m);
 // cols: AIR_W + 1 folded columns (the last one the committed-column combination).
 // betas: the 8 full rounds' 16 weights beta_f = MDS^T (alpha_(c0(f)+i))_i, f = 0..7.
 void launch_zc_eval_ef(const ef* cols, int m, const ef* eq, const ef* alphas, const ef* betas, const AirConsts& K,

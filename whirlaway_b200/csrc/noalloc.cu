@@ -1,12 +1,12 @@
 // Allocation-free variant of the standalone a*b - c zerocheck prover.
 //
-// For callers that cannot allocate device memory: code that runs where cudaMalloc is not
-// allowed or not wanted (for example inside a host callback, in a process whose device
-// memory is owned and pre-partitioned by another framework, or on a latency path that must
-// not touch the allocator). Every device buffer this prover needs lives in one file-scope
-// device array of fixed size, and host-side state is kept in fixed-capacity arrays; the call
-// makes no cudaMalloc / cudaMallocAsync / cudaMallocHost / cudaFree call and no host heap
-// allocation of its own.
+// For callers that cannot allocate device memory: a process whose device memory is owned and
+// pre-partitioned by another framework (which would see any allocation of ours as memory it
+// no longer has), or a latency path that must not enter an allocator (whose calls can map new
+// memory and stall the device for milliseconds). Every device buffer this prover needs lives
+// in one file-scope device array of fixed size, and host-side state is kept in fixed-capacity
+// arrays; the call makes no cudaMalloc / cudaMallocAsync / cudaMallocHost / cudaFree call and
+// no host heap allocation of its own.
 //
 // Limits and sharing:
 //  * log_n <= 14 (and 1 <= skips <= 4, skips < log_n); larger sizes are rejected with
@@ -15,8 +15,12 @@
 //    exits) is shared by all calls and keeps the last call's contents; every buffer the prover
 //    reads is written earlier in the same call. Calls that overlap on the GPU (on different
 //    streams or from different threads) race on it and must be serialised by the caller.
+//  * The call copies to and from the host and waits for its stream between sumcheck rounds.
+//    It must not be called from a stream callback or a host function (cudaLaunchHostFunc),
+//    where CUDA calls are not permitted, and it cannot run on a stream that is being captured
+//    into a graph: a capturing stream is rejected with WL_E_INVALID_ARG.
 //  * The first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//    with that device current); make that first call before any stream capture.
+//    with that device current); a failed lookup is not kept, the next call retries it.
 #include <cstring>
 #include <mutex>
 
@@ -33,21 +37,28 @@ constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-std::once_flag g_once[MAX_DEVICES];
+std::mutex g_scratch_mu;
 void* g_scratch_ptr[MAX_DEVICES];
-cudaError_t g_scratch_err[MAX_DEVICES];
 
-// Device address of the scratch array for the current device (looked up once per device).
+// Device address of the scratch array for the current device. Looked up once per device and
+// kept only on success, so that a transient failure is retried by the next call.
 cudaError_t scratch_base(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-  std::call_once(g_once[dev], [&] {
-    g_scratch_err[dev] = cudaGetSymbolAddress(&g_scratch_ptr[dev], g_noalloc_scratch);
-  });
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return e;
+    }
+    g_scratch_ptr[dev] = p;
+  }
   *out = g_scratch_ptr[dev];
-  return g_scratch_err[dev];
+  return cudaSuccess;
 }
 
 // Bump allocation inside the scratch array (256-byte aligned).
@@ -314,6 +325,12 @@ extern "C" wl_status wl_sumcheck_abc_prove_noalloc(const uint32_t* p16_constants
     return WL_E_BUFFER_TOO_SMALL;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return WL_E_INVALID_ARG;
+  }
+  if (cap != cudaStreamCaptureStatusNone) return WL_E_INVALID_ARG;  // host round trips cannot be captured
   try {
     void* base = nullptr;
     if (wl::scratch_base(&base) != cudaSuccess || !base) return WL_E_CUDA;

@@ -771,7 +771,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     const size_t half = size_t(1) << (m - 1);
     const int nb = zc_ef_blocks(m);
     ef* part = ctx.partials(size_t(nb) * 3);
-    { ProfScope _ps(ctx, "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+    { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
     std::vector<ef> s3 = reduce_to_host(ctx, part, nb, 3);
     const ef& r = zc[round];
     ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);

@@ -13,19 +13,41 @@ double steady_ms() {
 }
 }  // namespace
 
-uint64_t proof_footprint_bytes(int log_n) {
+// Upper bound of the device memory one proof takes from the stream-ordered pool, by phase,
+// from the buffer sizes of prove_air (N = 2^log_n rows, W = 165 columns, 32-byte extension
+// values). The witness (W N words) lives throughout, and so do the commitments: the first one
+// (2^(n+1+rho) rows of 88 stored columns and its Merkle tree), and in the WHIR rounds the later
+// ones (128 columns; the first of them 2^(n+4+rho-d) rows for an RS domain reduction d, each
+// next one half as many).
+//  * zerocheck: round 0 holds the per-row combination (N values), then either the 52 computed
+//    cube inputs per row or the W + 1 folded columns (N / 2^k values each); round 1 holds the
+//    folded columns and their halves, with the eq tables.
+//  * inner sumcheck: two tables of N values and their halves.
+//  * WHIR: g and the weights (2N values each), their halves, the later commitments.
+// A margin covers the small tables (eq tables, partial sums, query rows, OOD work) and the
+// pool's rounding.
+uint64_t proof_footprint_bytes(const Settings& s, int log_n) {
   const uint64_t N = uint64_t(1) << log_n;
-  uint64_t b = 0;
-  b += uint64_t(AIR_W) * N * 4;         // witness
-  b += 88ull * 4 * N * 4;               // first commitment: LDE (88 stored columns, rate 1/2, fold 2^7)
-  b += 2ull * 4 * N * 32;               // its Merkle tree
-  b += uint64_t(AIR_W + 1) * (N / 16) * 32 * 3 / 2;  // zerocheck fold buffers (double-buffered)
-  b += 32ull * N + 4ull * ZC0_NQ * N;                 // round 0: per-row combination and cube inputs
-  b += 3ull * N * 32;                   // inner sumcheck tables (eq, A, B)
-  b += 2ull * 2 * N * 32 * 2;           // WHIR g / w and their folds
-  b += 128ull * N * 4 + 2ull * N * 32;  // second commitment and its tree
-  b += 16ull << 20;                     // inputs, small tables, pool rounding
-  return b;
+  const int rho = s.log_inv_rate, k = s.univariate_skips;
+  const uint64_t E = 32;  // bytes per extension value
+  const uint64_t wit = uint64_t(AIR_W) * N * 4;
+  const uint64_t rows0 = N << (1 + rho);
+  const uint64_t c0 = rows0 * 88 * 4 + rows0 * 2 * 32;
+  const uint64_t S = N >> k;
+  const uint64_t zc0 = E * N + std::max<uint64_t>(4ull * ZC0_NQ * N, uint64_t(AIR_W + 1) * S * E) + E * S;
+  const uint64_t zc1 = uint64_t(AIR_W + 1) * S * E * 3 / 2 + E * S * 3 / 2;
+  const uint64_t zc = std::max(zc0, zc1);
+  const uint64_t inner = E * (S + 3 * N);
+  // later commitments: 2^(n+4+rho-d) rows of 128 columns and a tree (d the RS domain
+  // reduction of the first round; 2^(n+rho-1) at the defaults), then halving (a geometric
+  // series below twice the first)
+  const int lr1 = log_n + 4 + rho - s.rs_reduction;
+  const uint64_t rows1 = lr1 >= 0 ? uint64_t(1) << lr1 : 1;
+  const uint64_t c1 = 2 * (rows1 * 128 * 4 + rows1 * 2 * 32);
+  const uint64_t whir = 2 * (2 * N * E) * 3 / 2 + c1 + (2 * N * E) / 8;
+  const uint64_t phase = std::max(std::max(zc, inner), whir);
+  const uint64_t margin = (uint64_t(64) << 20) + (wit + c0 + phase) / 32;
+  return wit + c0 + phase + margin;
 }
 
 Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), budget_(hbm_budget) {
@@ -67,7 +89,7 @@ Server::~Server() {
 }
 
 uint64_t Server::submit(ServeJob job) {
-  const uint64_t fp = proof_footprint_bytes(job.log_n);
+  const uint64_t fp = proof_footprint_bytes(job.settings, job.log_n);
   std::lock_guard<std::mutex> lk(mu_);
   if (budget_ && fp > budget_) throw std::invalid_argument("proof footprint exceeds the HBM budget");
   uint64_t t = next_ticket_++;
@@ -108,7 +130,13 @@ void Server::release(uint64_t ticket) {
 
 void Server::worker_main(int idx) {
   Context& ctx = *contexts_[idx];
-  WL_CUDA(cudaSetDevice(device_));
+  // A worker thread must never throw: a failed device selection fails every job it takes.
+  std::string setup_err;
+  const cudaError_t se = cudaSetDevice(device_);
+  if (se != cudaSuccess) {
+    setup_err = std::string("cudaSetDevice: ") + cudaGetErrorString(se);
+    cudaGetLastError();
+  }
   for (;;) {
     uint64_t ticket = 0;
     ServeJob job;
@@ -143,6 +171,7 @@ void Server::worker_main(int idx) {
     std::string err;
     bool ok = true;
     try {
+      if (!setup_err.empty()) throw std::runtime_error(setup_err);
       ProofJob pj;
       pj.settings = job.settings;
       pj.log_n = job.log_n;

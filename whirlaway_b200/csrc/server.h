@@ -44,7 +44,7 @@ struct ServeResult {
 // Device bytes one proof of 2^log_n rows may hold at its peak (witness, LDE and Merkle tree
 // of the first commitment, zerocheck and inner-sumcheck tables, WHIR tables and later
 // commitments), with slack for pool rounding.
-uint64_t proof_footprint_bytes(int log_n);
+uint64_t proof_footprint_bytes(const Settings& s, int log_n);
 
 class Server {
  public:

@@ -332,10 +332,7 @@ class WhirVerifier {
       auto work = [&] {
         for (size_t i = next++; i < nq; i = next++) check(i);
       };
-      std::vector<std::thread> pool;
-      for (size_t t = 1; t < T; t++) pool.emplace_back(work);
-      work();
-      for (auto& th : pool) th.join();
+      run_on_threads(T, work);
     }
     for (size_t i = 0; i < nq; i++)
       if (!good[i]) return false;
