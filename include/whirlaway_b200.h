@@ -230,9 +230,6 @@ wl_status wl_ctx_host_wait_ms(wl_ctx* ctx, double* out);
  * {"class": [total_ms, launches], ...} for everything since the last enable. */
 wl_status wl_profile_enable(wl_ctx* ctx, int32_t on);
 wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap);
-/* Measured integer-pipe ceilings on the context's device: Montgomery products per second and
- * Poseidon2-24 permutations per second (p24 constants from a constants blob). */
-wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* modmul_per_s, double* p24_per_s);
 /* The context's CUDA stream (a cudaStream_t), for callers that time work with their own
  * events, and the number of kernels the library has launched in this process. */
 void* wl_ctx_stream(wl_ctx* ctx);

@@ -122,8 +122,6 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_ctx_set_spin_sync": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_ctx_host_wait_ms": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "wl_profile_only": (ctypes.c_int, [vp, ctypes.c_char_p]),
-        "wl_probe_int_peaks": (ctypes.c_int, [vp, _u32p, ctypes.POINTER(ctypes.c_double),
-                                              ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -224,13 +222,6 @@ class Context:
         v = ctypes.c_double()
         self.check(self._lib.wl_ctx_host_wait_ms(self.handle, ctypes.byref(v)), "host_wait_ms")
         return v.value
-
-    def probe_int_peaks(self, constants: np.ndarray):
-        """Measured (Montgomery products/s, Poseidon2-24 permutations/s) from registers."""
-        a, b = ctypes.c_double(), ctypes.c_double()
-        c = np.ascontiguousarray(constants, dtype=np.uint32)
-        self.check(self._lib.wl_probe_int_peaks(self.handle, _ptr(c), ctypes.byref(a), ctypes.byref(b)), "probe")
-        return a.value, b.value
 
     def close(self):
         if getattr(self, "handle", None):

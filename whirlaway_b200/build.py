@@ -11,8 +11,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libwhirlaway_b200.so")
-SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_probe.cu", "prover.cu", "server.cu", "noalloc.cu", "verifier.cu", "capi.cu",
+SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "prover.cu", "server.cu", "noalloc.cu", "verifier.cu", "capi.cu",
            "host_perm.cpp"]
+# Integer-pipe throughput probes: a separate library that only the benchmark loads.
+PROBE_SRC = os.path.join("probe", "int_peaks.cu")
+PROBE_LIB = os.path.join(OUT_DIR, "libwl_probe.so")
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC"]  # host-only sources (g++; CPU features dispatched at run time)
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
@@ -52,6 +55,12 @@ def build(verbose=False, jobs=None):
             raise RuntimeError(f"compiler failed on {src}:\n{out.decode()}")
     if _stale(LIB, objs):
         cmd = ["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-ccbin", "g++", "-o", LIB] + objs
+        subprocess.run(cmd, check=True)
+    probe = os.path.join(CSRC, PROBE_SRC)
+    if _stale(PROBE_LIB, [probe] + headers):
+        cmd = ["nvcc"] + NVCC_FLAGS + ["-shared", probe, "-o", PROBE_LIB]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
     return LIB
 

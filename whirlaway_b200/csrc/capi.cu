@@ -474,17 +474,6 @@ wl_status wl_profile_json(wl_ctx* ctx, char* buf, size_t cap) {
   });
 }
 
-wl_status wl_probe_int_peaks(wl_ctx* ctx, const uint32_t* constants, double* modmul_per_s, double* p24_per_s) {
-  if (!ctx || !constants) return WL_E_INVALID_ARG;
-  return guarded(ctx, [&] {
-    if (modmul_per_s) *modmul_per_s = wl::bench_modmul_per_s(*ctx->c);
-    if (p24_per_s)
-      *p24_per_s = wl::bench_p24_per_s(*ctx->c,
-                                       wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS));
-    return WL_OK;
-  });
-}
-
 uint64_t wl_proof_footprint_bytes(const wl_air_settings* s, int32_t log_n) {
   wl_air_settings d;
   if (!s) {

@@ -129,9 +129,4 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int log_
 
 size_t proof_len_bound(const Settings& s, int log_n);
 
-// Throughput probes used as measured compute peaks: Montgomery products per second and
-// Poseidon2-24 permutations per second, both from registers (no memory traffic).
-double bench_modmul_per_s(Context& ctx);
-double bench_p24_per_s(Context& ctx, const kb::P24Consts& c);
-
 }  // namespace wl
