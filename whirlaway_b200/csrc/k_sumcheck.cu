@@ -836,9 +836,12 @@ __device__ __forceinline__ void lerp16_mma(const ef* __restrict__ lo, const ef* 
 }
 // k_fold_cols with the challenge by value, 16 values per warp on the tensor cores; the extra
 // column slot (blockIdx.y == ncols) sums the next eq table as k_fold_cols does.
+// The challenge comes by value (rv) or, when rptr is set, from device memory (a challenge
+// sampled on the device by the round-finishing kernel).
 __global__ void __launch_bounds__(256) k_fold_cols_mma(const ef* __restrict__ in, ef* __restrict__ out, size_t half,
-                                                      int ncols, ef rv, const ef* __restrict__ eq_in,
-                                                      ef* __restrict__ eq_out, size_t eq_half) {
+                                                      int ncols, ef rv, const ef* __restrict__ rptr,
+                                                      const ef* __restrict__ eq_in, ef* __restrict__ eq_out,
+                                                      size_t eq_half) {
   const int c = blockIdx.y;
   if (c == ncols) {
     const size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -849,19 +852,20 @@ __global__ void __launch_bounds__(256) k_fold_cols_mma(const ef* __restrict__ in
   const size_t x0 = (size_t(blockIdx.x) * 8 + warp) * 16;
   if (x0 >= half) return;  // whole warp
   uint32_t bf[4][2];
-  fold_frag(rv, g, t, bf);
+  fold_frag(rptr ? *rptr : rv, g, t, bf);
   const ef* src = in + size_t(c) * 2 * half;
   const uint32_t nv = half - x0 < 16 ? uint32_t(half - x0) : 16u;
   lerp16_mma(src + x0, src + half + x0, out + size_t(c) * half + x0, nv, bf, g, t);
 }
 // lo + r (hi - lo) for two tables with the challenge by value: blockIdx.y selects (a, oa) or (b, ob).
 __global__ void __launch_bounds__(256) k_fold2_mma(const ef* __restrict__ a, const ef* __restrict__ b,
-                                                  ef* __restrict__ oa, ef* __restrict__ ob, size_t half, ef rv) {
+                                                  ef* __restrict__ oa, ef* __restrict__ ob, size_t half, ef rv,
+                                                  const ef* __restrict__ rptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
   const size_t x0 = (size_t(blockIdx.x) * 8 + warp) * 16;
   if (x0 >= half) return;  // whole warp
   uint32_t bf[4][2];
-  fold_frag(rv, g, t, bf);
+  fold_frag(rptr ? *rptr : rv, g, t, bf);
   const ef* src = blockIdx.y ? b : a;
   ef* dst = blockIdx.y ? ob : oa;
   const uint32_t nv = half - x0 < 16 ? uint32_t(half - x0) : 16u;
@@ -1562,7 +1566,14 @@ void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef
   // 128 values per block for the columns, 256 for the eq table
   const size_t bx = std::max((half + 127) / 128, eq_in ? (eq_half + 255) / 256 : size_t(0));
   dim3 grid((unsigned)std::max<size_t>(bx, 1), ncols + (eq_in ? 1 : 0));
-  k_fold_cols_mma<<<grid, 256, 0, s>>>(in, out, half, ncols, r, eq_in, eq_out, eq_half);
+  k_fold_cols_mma<<<grid, 256, 0, s>>>(in, out, half, ncols, r, nullptr, eq_in, eq_out, eq_half);
+  WL_LAUNCH_CHECK();
+}
+void launch_fold_cols_dev(const ef* in, ef* out, int ncols, size_t half, const ef* r_dev, cudaStream_t s,
+                          const ef* eq_in, ef* eq_out, size_t eq_half) {
+  const size_t bx = std::max((half + 127) / 128, eq_in ? (eq_half + 255) / 256 : size_t(0));
+  dim3 grid((unsigned)std::max<size_t>(bx, 1), ncols + (eq_in ? 1 : 0));
+  k_fold_cols_mma<<<grid, 256, 0, s>>>(in, out, half, ncols, ef_zero(), r_dev, eq_in, eq_out, eq_half);
   WL_LAUNCH_CHECK();
 }
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
@@ -1648,7 +1659,11 @@ void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaSt
   WL_LAUNCH_CHECK();
 }
 void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s) {
-  k_fold2_mma<<<dim3((unsigned)((half + 127) / 128), 2), 256, 0, s>>>(a, b, oa, ob, half, r);
+  k_fold2_mma<<<dim3((unsigned)((half + 127) / 128), 2), 256, 0, s>>>(a, b, oa, ob, half, r, nullptr);
+  WL_LAUNCH_CHECK();
+}
+void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r_dev, cudaStream_t s) {
+  k_fold2_mma<<<dim3((unsigned)((half + 127) / 128), 2), 256, 0, s>>>(a, b, oa, ob, half, ef_zero(), r_dev);
   WL_LAUNCH_CHECK();
 }
 

@@ -1,0 +1,194 @@
+// Device-side Fiat-Shamir for the sumcheck rounds.
+//
+// A sumcheck round ends with a few extension-field sums (the round polynomial at a handful of
+// points), which the prover interpolates, writes to the proof, absorbs into the
+// DuplexChallenger<F, Poseidon16, 16, 8> and answers with a sampled challenge that the next
+// fold uses (crates/sumcheck/src/prove.rs:190-222 for the zerocheck and product sumchecks;
+// the WHIR folding sumcheck sends its three values directly). Done on the host, every round is
+// a device-to-host round trip during which the device idles. Here one single-block kernel per
+// round reduces the partial sums, finishes the round exactly as the host would (same
+// challenger semantics as HostChallenger: observations fill the rate and duplex at eight,
+// samples pop from the end of the last squeeze) and leaves the challenge in device memory for
+// the fold, so the host enqueues a whole phase of rounds without waiting and reads the
+// appended proof words, the challenges and the challenger state back once at its end.
+#include "kernels.h"
+
+namespace wl {
+
+namespace {
+
+constexpr int FIN_THREADS = 384;  // up to three sums, 128 threads each
+
+// The permutation runs on a register copy of the state (the challenger itself, indexed by its
+// buffer lengths, lives in local memory).
+__device__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p) {
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = (i < 8 && i < c.in_len) ? c.in[i] : c.state[i];
+  c.in_len = 0;
+  kb::p2_permute<16>(s, p);
+#pragma unroll
+  for (int i = 0; i < 16; i++) c.state[i] = s[i];
+#pragma unroll
+  for (int i = 0; i < 8; i++) c.out[i] = s[i];
+  c.out_len = 8;
+}
+__device__ void dch_observe(DevChallenger& c, uint32_t x, const kb::P16Consts& p) {
+  c.out_len = 0;
+  c.in[c.in_len++] = x;
+  if (c.in_len == 8) dch_duplex(c, p);
+}
+__device__ uint32_t dch_sample(DevChallenger& c, const kb::P16Consts& p) {
+  if (c.in_len || !c.out_len) dch_duplex(c, p);
+  return c.out[--c.out_len];
+}
+// Writes v to the proof and absorbs it (Transcript::add_ext).
+__device__ void dts_add_ext(DevRound& st, uint32_t* proof, const ef& v, const kb::P16Consts& p) {
+#pragma unroll 1
+  for (int i = 0; i < 8; i++) {
+    proof[st.proof_len++] = v.c[i];
+    dch_observe(st.ch, v.c[i], p);
+  }
+}
+__device__ ef dts_sample_ext(DevRound& st, const kb::P16Consts& p) {
+  ef e;
+#pragma unroll 1
+  for (int i = 0; i < 8; i++) e.c[i] = dch_sample(st.ch, p);
+  return e;
+}
+
+// Sums of `nsum` interleaved partials (partial[b * nsum + z]) into red[z]; every thread of the
+// block takes part, the result is valid after the final barrier.
+__device__ void reduce_sums(const ef* __restrict__ partial, int nb, int nsum, ef* red, ef* scratch) {
+  const int z = threadIdx.x >> 7, t = threadIdx.x & 127;
+  ef acc = kb::ef_zero();
+  if (z < nsum)
+    for (int b = t; b < nb; b += 128) acc = kb::ef_add(acc, partial[size_t(b) * nsum + z]);
+  acc = warp_reduce_ef(acc);
+  if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (t == 0 && z < nsum) {
+    ef s = scratch[z * 4];
+    for (int w = 1; w < 4; w++) s = kb::ef_add(s, scratch[z * 4 + w]);
+    red[z] = s;
+  }
+  __syncthreads();
+}
+
+__device__ ef poly_eval_dev(const ef* c, int n, const ef& x) {
+  ef r = kb::ef_zero();
+  for (int i = n - 1; i >= 0; i--) r = kb::ef_add(kb::ef_mul(r, x), c[i]);
+  return r;
+}
+
+// Round of a sumcheck with an eq factor (the zerocheck's rounds >= 1 and those of the a*b - c
+// zerocheck): the computed sums are at z = 0, 2, .., NPTS - 1 (NPTS - 1 of them), weighted by
+// the factor mmf of the variables already folded; the value at 1 follows from the claim,
+// e1 = (sum - e0 (1 - r)) / r. The round polynomial is the interpolation on 0..NPTS-1 times the
+// eq factor of the current variable, (1 - r) + (2r - 1) X: NPTS + 1 coefficients.
+template <int NPTS>
+__global__ void __launch_bounds__(FIN_THREADS) k_eqsc_round_finish(const ef* __restrict__ partial, int nb, ef r,
+                                                                   ef rinv, const __grid_constant__ FinishConsts fc,
+                                                                   DevRound* __restrict__ stp,
+                                                                   uint32_t* __restrict__ proof,
+                                                                   ef* __restrict__ ch_out) {
+  __shared__ ef red[3], scratch[12];
+  reduce_sums(partial, nb, NPTS - 1, red, scratch);
+  if (threadIdx.x) return;
+  DevRound st = *stp;
+  ef e[NPTS];
+  e[0] = kb::ef_mul(red[0], st.mmf);
+  for (int i = 2; i < NPTS; i++) e[i] = kb::ef_mul(red[i - 1], st.mmf);
+  const ef one = kb::ef_one();
+  const ef omr = kb::ef_sub(one, r);
+  e[1] = kb::ef_mul(kb::ef_sub(st.sum, kb::ef_mul(e[0], omr)), rinv);
+  ef q[NPTS];
+  for (int k = 0; k < NPTS; k++) q[k] = kb::ef_zero();
+  for (int i = 0; i < NPTS; i++)
+    for (int k = 0; k < NPTS; k++) q[k] = kb::ef_add(q[k], kb::ef_mul_f(e[i], fc.basis[NPTS - 3][i][k]));
+  const ef lin = kb::ef_sub(kb::ef_add(r, r), one);  // (1 - r) + lin X
+  ef p[NPTS + 1];
+  for (int k = 0; k <= NPTS; k++) p[k] = kb::ef_zero();
+  for (int k = 0; k < NPTS; k++) {
+    p[k] = kb::ef_add(p[k], kb::ef_mul(q[k], omr));
+    p[k + 1] = kb::ef_add(p[k + 1], kb::ef_mul(q[k], lin));
+  }
+  for (int k = 0; k <= NPTS; k++) dts_add_ext(st, proof, p[k], fc.p16);
+  const ef c = dts_sample_ext(st, fc.p16);
+  st.sum = poly_eval_dev(p, NPTS + 1, c);
+  st.mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(omr, kb::ef_sub(one, c)), kb::ef_mul(r, c)), st.mmf);
+  ch_out[st.round++] = c;
+  *stp = st;
+}
+
+// Round of the product sumcheck (the inner sumcheck): sums at 0 and 2, the value at 1 from the
+// claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
+__global__ void __launch_bounds__(FIN_THREADS) k_prod_round_finish(const ef* __restrict__ partial, int nb,
+                                                                   const __grid_constant__ FinishConsts fc,
+                                                                   DevRound* __restrict__ stp,
+                                                                   uint32_t* __restrict__ proof,
+                                                                   ef* __restrict__ ch_out) {
+  __shared__ ef red[3], scratch[12];
+  reduce_sums(partial, nb, 2, red, scratch);
+  if (threadIdx.x) return;
+  DevRound st = *stp;
+  const ef y[3] = {red[0], kb::ef_sub(st.sum, red[0]), red[1]};
+  ef p[3];
+  for (int k = 0; k < 3; k++) {
+    p[k] = kb::ef_zero();
+    for (int i = 0; i < 3; i++) p[k] = kb::ef_add(p[k], kb::ef_mul_f(y[i], fc.basis[0][i][k]));
+  }
+  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, p[k], fc.p16);
+  const ef c = dts_sample_ext(st, fc.p16);
+  st.sum = poly_eval_dev(p, 3, c);
+  ch_out[st.round++] = c;
+  *stp = st;
+}
+
+// Round of the WHIR folding sumcheck: the three values h(0), h(1), h(2) go to the proof as
+// they are; the next claim is h(r) by quadratic interpolation on 0, 1, 2.
+__global__ void __launch_bounds__(FIN_THREADS) k_whir_round_finish(const ef* __restrict__ partial, int nb,
+                                                                   const __grid_constant__ FinishConsts fc,
+                                                                   DevRound* __restrict__ stp,
+                                                                   uint32_t* __restrict__ proof,
+                                                                   ef* __restrict__ ch_out) {
+  __shared__ ef red[3], scratch[12];
+  reduce_sums(partial, nb, 3, red, scratch);
+  if (threadIdx.x) return;
+  DevRound st = *stp;
+  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, red[k], fc.p16);
+  const ef r = dts_sample_ext(st, fc.p16);
+  // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2
+  const ef rm1 = kb::ef_sub_f(r, fc.one), rm2 = kb::ef_sub_f(r, fc.two);
+  const ef a = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[0], rm1), rm2), fc.inv2);
+  const ef b = kb::ef_mul(kb::ef_mul(red[1], r), rm2);
+  const ef c = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[2], r), rm1), fc.inv2);
+  st.sum = kb::ef_add(kb::ef_sub(a, b), c);
+  ch_out[st.round++] = r;
+  *stp = st;
+}
+
+}  // namespace
+
+void launch_eqsc_round_finish(int npts, const ef* partial, int nb, const ef& r, const ef& rinv,
+                              const FinishConsts& fc, DevRound* st, uint32_t* proof, ef* ch_out, cudaStream_t s) {
+  if (npts == 4)
+    k_eqsc_round_finish<4><<<1, FIN_THREADS, 0, s>>>(partial, nb, r, rinv, fc, st, proof, ch_out);
+  else if (npts == 3)
+    k_eqsc_round_finish<3><<<1, FIN_THREADS, 0, s>>>(partial, nb, r, rinv, fc, st, proof, ch_out);
+  else
+    throw std::invalid_argument("eq-factor sumcheck rounds of 3 or 4 points");
+  WL_LAUNCH_CHECK();
+}
+void launch_prod_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
+                              ef* ch_out, cudaStream_t s) {
+  k_prod_round_finish<<<1, FIN_THREADS, 0, s>>>(partial, nb, fc, st, proof, ch_out);
+  WL_LAUNCH_CHECK();
+}
+void launch_whir_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
+                              ef* ch_out, cudaStream_t s) {
+  k_whir_round_finish<<<1, FIN_THREADS, 0, s>>>(partial, nb, fc, st, proof, ch_out);
+  WL_LAUNCH_CHECK();
+}
+
+}  // namespace wl

@@ -105,6 +105,9 @@ void launch_fold_cols(const ef* in, ef* out, int ncols, size_t half, const ef* r
 // The same with the challenge passed by value (no device copy of it).
 void launch_fold_cols_at(const ef* in, ef* out, int ncols, size_t half, const ef& r, cudaStream_t s,
                          const ef* eq_in = nullptr, ef* eq_out = nullptr, size_t eq_half = 0);
+// The same with the challenge in device memory (sampled by a round-finishing kernel).
+void launch_fold_cols_dev(const ef* in, ef* out, int ncols, size_t half, const ef* r_dev, cudaStream_t s,
+                          const ef* eq_in = nullptr, ef* eq_out = nullptr, size_t eq_half = 0);
 // Up/down evaluations of every column at (r0; tail), with eq(tail, .) factored as
 // eq_hi (2^(log_n-k-ll) entries) x eq_lo (2^ll entries). out_up / out_down must hold
 // AIR_W * (1 + 2^k * 2^(log_n-k-ll)) elements; the first AIR_W are the results.
@@ -124,6 +127,7 @@ int prod_blocks(size_t half);
 void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaStream_t s);
 // Folds the tables a and b at the challenge r (lo + r (hi - lo)).
 void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s);
+void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r_dev, cudaStream_t s);
 
 // --------------------------------------------------------------- a*b - c zerocheck
 void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
@@ -162,5 +166,43 @@ int whir_sc_blocks(size_t half);
 void launch_whir_sc_eval(const ef* g, const ef* w, size_t half, ef* partial, cudaStream_t s);
 int mle_ef_blocks(int lh);
 void launch_mle_eval_ef(const ef* g, int lh, int ll, const ef* hi, const ef* lo, ef* partial, cudaStream_t s);
+
+// --------------------------------------------------------------- device-side transcript
+// The DuplexChallenger<F, Poseidon16, 16, 8> state (Montgomery form), as HostChallenger holds it.
+struct DevChallenger {
+  uint32_t state[16];
+  uint32_t in[8];
+  uint32_t out[8];
+  int32_t in_len, out_len;
+};
+// State of a phase of sumcheck rounds run on the device: the challenger, the current claim,
+// the zerocheck's eq weight of the folded variables, the proof words appended so far and the
+// number of rounds finished (index of the next challenge).
+struct DevRound {
+  DevChallenger ch;
+  ef sum;
+  ef mmf;
+  uint32_t proof_len;
+  int32_t round;
+};
+// Constants of the round-finishing kernels: Poseidon2-16 (Montgomery), the Lagrange bases on
+// the nodes 0..2 and 0..3 (basis[0][i][k], basis[1][i][k]: coefficient k of basis polynomial i)
+// and the Montgomery forms of 1, 2 and 1/2.
+struct FinishConsts {
+  kb::P16Consts p16;
+  uint32_t basis[2][4][4];
+  uint32_t one, two, inv2;
+};
+// One round's finish on the device (one block): reduces `nb` interleaved partial sums, writes
+// the round polynomial to proof[st->proof_len..], absorbs it, samples the challenge into
+// ch_out[st->round] and updates st. Eq-factor rounds (npts 4: the AIR zerocheck, 3: the a*b - c
+// zerocheck) take the current variable's eq challenge r and its inverse; the product
+// sumcheck (inner sumcheck) and the WHIR folding sumcheck need no more.
+void launch_eqsc_round_finish(int npts, const ef* partial, int nb, const ef& r, const ef& rinv,
+                              const FinishConsts& fc, DevRound* st, uint32_t* proof, ef* ch_out, cudaStream_t s);
+void launch_prod_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
+                              ef* ch_out, cudaStream_t s);
+void launch_whir_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
+                              ef* ch_out, cudaStream_t s);
 
 }  // namespace wl

@@ -265,6 +265,27 @@ void Context::to_host(void* dst, const void* src, size_t bytes) {
   }
   g_up_off = 0;  // every earlier upload has completed
 }
+void Context::to_host_many(const std::vector<HostCopy>& copies) {
+  char* down = static_cast<char*>(pinned) + kUpBytes;
+  size_t off = 0;
+  for (const HostCopy& c : copies) off += (c.bytes + 255) & ~size_t(255);
+  if (off > kDownBytes) {  // too large for the staging: one copy (and wait) each
+    for (const HostCopy& c : copies) to_host(c.dst, c.src, c.bytes);
+    return;
+  }
+  off = 0;
+  for (const HostCopy& c : copies) {
+    if (c.bytes) WL_CUDA(cudaMemcpyAsync(down + off, c.src, c.bytes, cudaMemcpyDeviceToHost, stream));
+    off += (c.bytes + 255) & ~size_t(255);
+  }
+  wait_stream();
+  off = 0;
+  for (const HostCopy& c : copies) {
+    if (c.bytes) memcpy(c.dst, down + off, c.bytes);
+    off += (c.bytes + 255) & ~size_t(255);
+  }
+  g_up_off = 0;  // every earlier upload has completed
+}
 void Context::to_device(void* dst, const void* src, size_t bytes) {
   HostClock& hc = host_clock();
   const double t0 = hc.on ? host_now_ms() : 0;
@@ -327,6 +348,80 @@ DBuf eq_table_dev(Context& ctx, const std::vector<ef>& pt) {
 }
 
 DBuf scalar_dev(Context& ctx, const ef& v) { return upload(ctx, std::vector<ef>{v}); }
+
+// Constants of the round-finishing kernels for one proof.
+FinishConsts finish_consts(const kb::P16Consts& p16) {
+  FinishConsts fc;
+  fc.p16 = p16;
+  for (int b = 0; b < 2; b++) {
+    const auto& basis = lagrange_basis_cached(3 + b);
+    for (int i = 0; i < 4; i++)
+      for (int k = 0; k < 4; k++) fc.basis[b][i][k] = (i < 3 + b && k < 3 + b) ? basis[i][k] : 0u;
+  }
+  fc.one = fm(1);
+  fc.two = fm(2);
+  fc.inv2 = kb::inv_m(fm(2));
+  return fc;
+}
+
+// A phase of sumcheck rounds whose transcript runs on the device (k_transcript.cu). The
+// challenger state and the claim go to the device at the start; the host then enqueues every
+// round (its sums, the finishing kernel, the fold at the sampled challenge) without waiting,
+// and finish() reads the state, the appended proof words and the challenges back in one copy,
+// leaving the host transcript exactly where the host-driven rounds would have left it.
+struct DevPhase {
+  Context& ctx;
+  Transcript& ts;
+  int rounds;
+  size_t words_per_round;
+  DBuf buf;  // [DevRound][challenges: rounds][proof words: rounds * words_per_round]
+  DevRound* st = nullptr;
+  ef* chs = nullptr;
+  uint32_t* words = nullptr;
+  DevPhase(Context& c, Transcript& t, int nrounds, size_t wpr, const ef& sum, const ef& mmf)
+      : ctx(c), ts(t), rounds(nrounds), words_per_round(wpr) {
+    buf = DBuf(bytes(), ctx.stream);
+    st = buf.as<DevRound>();
+    chs = reinterpret_cast<ef*>(buf.as<char>() + sizeof(DevRound));
+    words = reinterpret_cast<uint32_t*>(chs + rounds);
+    DevRound h{};
+    memcpy(h.ch.state, ts.ch.state, sizeof(h.ch.state));
+    memcpy(h.ch.in, ts.ch.in, sizeof(h.ch.in));
+    memcpy(h.ch.out, ts.ch.out, sizeof(h.ch.out));
+    h.ch.in_len = ts.ch.in_len;
+    h.ch.out_len = ts.ch.out_len;
+    h.sum = sum;
+    h.mmf = mmf;
+    h.proof_len = 0;
+    h.round = 0;
+    ctx.to_device(st, &h, sizeof(h));
+  }
+  size_t bytes() const { return sizeof(DevRound) + sizeof(ef) * rounds + sizeof(uint32_t) * rounds * words_per_round; }
+  // Returns the challenges; *sum (and *mmf) receive the final claim (and eq weight).
+  std::vector<ef> finish(ef* sum, ef* mmf) {
+    std::vector<char> h(bytes());
+    ctx.to_host(h.data(), buf.as<void>(), h.size());
+    DevRound d;
+    memcpy(&d, h.data(), sizeof(d));
+    if (d.round != rounds || d.proof_len != rounds * words_per_round)
+      throw std::runtime_error("device sumcheck phase: round count mismatch");
+    memcpy(ts.ch.state, d.ch.state, sizeof(d.ch.state));
+    memcpy(ts.ch.in, d.ch.in, sizeof(d.ch.in));
+    memcpy(ts.ch.out, d.ch.out, sizeof(d.ch.out));
+    ts.ch.in_len = d.ch.in_len;
+    ts.ch.out_len = d.ch.out_len;
+    std::vector<ef> ch(rounds);
+    memcpy(ch.data(), h.data() + sizeof(DevRound), sizeof(ef) * rounds);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(h.data() + sizeof(DevRound) + sizeof(ef) * rounds);
+    for (int r = 0; r < rounds; r++) {
+      ts.proof.insert(ts.proof.end(), w + r * words_per_round, w + (r + 1) * words_per_round);
+      if (ts.log) ts.log->add("challenge", ts.proof.size(), ch[r].c, 8, true);
+    }
+    if (sum) *sum = d.sum;
+    if (mmf) *mmf = d.mmf;
+    return ch;
+  }
+};
 
 // Grinding: the smallest witness (searched on the device in batches), then the host
 // challenger replays observe(w) + sample_bits exactly as check_witness does.
@@ -433,9 +528,9 @@ std::vector<ef> open(Context& ctx, const Commitment& c, const std::vector<uint32
   std::vector<uint32_t> hr(size_t(128) * nq), hd(didx.size() * 8);
   std::vector<ef> folded(mono ? nq : 0);
   if (nq) {
-    ctx.to_host(hr.data(), rows.as<uint32_t>(), hr.size() * 4);
-    ctx.to_host(hd.data(), digs.as<uint32_t>(), hd.size() * 4);
-    if (mono) ctx.to_host(folded.data(), dfold.as<ef>(), sizeof(ef) * nq);
+    ctx.to_host_many({{hr.data(), rows.as<uint32_t>(), hr.size() * 4},
+                      {hd.data(), digs.as<uint32_t>(), hd.size() * 4},
+                      {folded.data(), dfold.as<ef>(), mono ? sizeof(ef) * nq : 0}});
     for (uint32_t& w : hd) w = kb::to_mont(w);  // canonical digests
   }
   for (int q = 0; q < nq; q++) {
@@ -535,9 +630,29 @@ ef mle_eval_dev(Context& ctx, const ef* g, int m, const std::vector<ef>& pt) {
   return reduce_to_host(ctx, part, 1 << lh, 1)[0];
 }
 
-// k rounds of the WHIR sumcheck on device tables (g, w), both of size 2^m on entry.
+// k rounds of the WHIR sumcheck on device tables (g, w), both of size 2^m on entry. Without
+// grinding the transcript runs on the device (one host wait for the whole block of rounds).
 void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, ef& sigma, int rounds, int pow_bits,
                        const kb::P16Consts& p16, std::vector<ef>& rnd) {
+  if (pow_bits == 0 && rounds > 0) {
+    const FinishConsts fc = finish_consts(p16);
+    DevPhase ph(ctx, ts, rounds, 24, sigma, kb::ef_one());
+    for (int t = 0; t < rounds; t++) {
+      const size_t half = size_t(1) << (m - 1);
+      const int nb = whir_sc_blocks(half);
+      ef* part = ctx.partials(size_t(3) * nb);
+      { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream); }
+      { ProfScope _ps(ctx, "round_finish"); launch_whir_round_finish(part, nb, fc, ph.st, ph.words, ph.chs, ctx.stream); }
+      DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
+      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, ph.chs + t, ctx.stream); }
+      g = std::move(ng);
+      w = std::move(nw);
+      m--;
+    }
+    const std::vector<ef> r = ph.finish(&sigma, nullptr);
+    rnd.insert(rnd.end(), r.begin(), r.end());
+    return;
+  }
   for (int t = 0; t < rounds; t++) {
     size_t half = size_t(1) << (m - 1);
     int nb = whir_sc_blocks(half);
@@ -766,7 +881,31 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     eqr = DBuf(sizeof(ef) * (S / 2), st);
     { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
   }
-  for (int round = 1; round <= n - k; round++) {
+  const bool zc_on_device = sumcheck_pow_bits(s.security_bits, 4) == 0;
+  if (zc_on_device && n - k >= 1) {
+    // every round's transcript on the device: the sums, the finishing kernel (interpolation,
+    // absorption, challenge) and the fold at the device-sampled challenge, one host wait
+    const FinishConsts fc = finish_consts(job.p16);
+    DevPhase ph(ctx, ts, n - k, 40, sum, mmf);
+    for (int round = 1; round <= n - k; round++) {
+      const int m = n - k - round + 1;
+      const size_t half = size_t(1) << (m - 1);
+      const int nb = zc_ef_blocks(m);
+      ef* part = ctx.partials(size_t(nb) * 3);
+      { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+      const ef& r = zc[round];
+      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(4, part, nb, r, kb::ef_inv(r), fc, ph.st, ph.words, ph.chs, st); }
+      DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
+      DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+      { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), W + 1, half, ph.chs + (round - 1), st,
+                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
+      cols = std::move(nc);
+      eqr = std::move(eqn);
+    }
+    const std::vector<ef> ch = ph.finish(&sum, &mmf);
+    challenges.insert(challenges.end(), ch.begin(), ch.end());
+  }
+  for (int round = 1; !zc_on_device && round <= n - k; round++) {
     const int m = n - k - round + 1;  // variables of the current columns
     const size_t half = size_t(1) << (m - 1);
     const int nb = zc_ef_blocks(m);
@@ -808,8 +947,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
     DBuf limbs(size_t(64) << ll_t, st);
     { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), limbs.as<uint8_t>(), st); }
-    ctx.to_host(inner_up.data(), up.as<ef>(), sizeof(ef) * W);
-    ctx.to_host(inner_down.data(), down.as<ef>(), sizeof(ef) * W);
+    ctx.to_host_many({{inner_up.data(), up.as<ef>(), sizeof(ef) * W}, {inner_down.data(), down.as<ef>(), sizeof(ef) * W}});
   }
   cols.reset();
   const double t2 = now_ms();
@@ -858,7 +996,24 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   const auto basis3 = lagrange_basis_cached(3);
   std::vector<ef> inner_ch;
   ts.phase("inner_sumcheck");
-  for (int round = 0; round < n; round++) {
+  const bool inner_on_device = sumcheck_pow_bits(s.security_bits, 2) == 0;
+  if (inner_on_device) {
+    const FinishConsts fc = finish_consts(job.p16);
+    DevPhase ph(ctx, ts, n, 24, inner_sum, kb::ef_one());
+    for (int round = 0; round < n; round++) {
+      const size_t half = N >> (round + 1);
+      const int nb = prod_blocks(half);
+      ef* part = ctx.partials(size_t(nb) * 2);
+      { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st); }
+      { ProfScope _ps(ctx, "round_finish"); launch_prod_round_finish(part, nb, fc, ph.st, ph.words, ph.chs, st); }
+      DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
+      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, ph.chs + round, st); }
+      A = std::move(na);
+      B = std::move(nbuf);
+    }
+    inner_ch = ph.finish(&inner_sum, nullptr);
+  }
+  for (int round = 0; !inner_on_device && round < n; round++) {
     const size_t half = N >> (round + 1);
     const int nb = prod_blocks(half);
     ef* part = ctx.partials(size_t(nb) * 2);
@@ -978,8 +1133,7 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     // final round
     ts.phase("whir_final");
     std::vector<ef> gf(size_t(1) << m), wf(size_t(1) << m);
-    ctx.to_host(gf.data(), g.as<ef>(), sizeof(ef) << m);
-    ctx.to_host(wf.data(), w.as<ef>(), sizeof(ef) << m);
+    ctx.to_host_many({{gf.data(), g.as<ef>(), sizeof(ef) << m}, {wf.data(), w.as<ef>(), sizeof(ef) << m}});
     ts.add_ext(gf.data(), gf.size());
     const WhirRound& cl = ws.c[ws.num_rounds];
     grind(ctx, ts, job.p16, cl.pow_bits);
@@ -1114,7 +1268,39 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     eqr = DBuf(sizeof(ef) * (S / 2), st);
     { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
   }
-  for (int round = 1; round <= n - k; round++) {
+  if (n - k >= 1 && sumcheck_pow_bits(128, 3) == 0) {
+    // rounds >= 1 with the transcript on the device; per-round times from events recorded at
+    // the round boundaries, read after the phase
+    const FinishConsts fc = finish_consts(p16);
+    DevPhase ph(ctx, ts, n - k, 32, sum, mmf);
+    std::vector<cudaEvent_t> ev(n - k + 1);
+    for (auto& e : ev) WL_CUDA(cudaEventCreate(&e));
+    WL_CUDA(cudaEventRecord(ev[0], st));
+    for (int round = 1; round <= n - k; round++) {
+      const int m = n - k - round + 1;
+      const size_t half = size_t(1) << (m - 1);
+      const int nb = (int)((half + 31) / 32);
+      ef* part = ctx.partials(size_t(nb) * 2);
+      { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st); }
+      const ef& rr = r[round];
+      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(3, part, nb, rr, kb::ef_inv(rr), fc, ph.st, ph.words, ph.chs, st); }
+      DBuf nc(sizeof(ef) * 3 * half, st);
+      DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+      { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 3, half, ph.chs + (round - 1), st,
+                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
+      cols = std::move(nc);
+      eqr = std::move(eqn);
+      WL_CUDA(cudaEventRecord(ev[round], st));
+    }
+    ph.finish(&sum, &mmf);
+    for (int round = 1; round <= n - k; round++) {
+      float ms = 0;
+      WL_CUDA(cudaEventElapsedTime(&ms, ev[round - 1], ev[round]));
+      if (round_ms) round_ms->push_back(ms);
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+  for (int round = 1; sumcheck_pow_bits(128, 3) != 0 && round <= n - k; round++) {
     tick();
     const int m = n - k - round + 1;
     const size_t half = size_t(1) << (m - 1);

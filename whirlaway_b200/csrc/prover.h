@@ -57,6 +57,13 @@ struct Context {
   Context(int device, uint64_t budget);
   ~Context();
   void to_host(void* dst, const void* src, size_t bytes);
+  // Several device-to-host copies behind one wait.
+  struct HostCopy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  };
+  void to_host_many(const std::vector<HostCopy>& copies);
   void wait_stream();  // host synchronisation with `stream` (counted in host_syncs)
   // How wait_stream waits: true (default) = the host thread polls an event without sleeping,
   // so the OS never has to wake it at the end of a round (blocking waits measured up to
