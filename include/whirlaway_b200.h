@@ -216,6 +216,20 @@ wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class);
 // No reference counterpart.
 wl_status wl_ctx_set_spin_sync(wl_ctx* ctx, int32_t spin);
 
+/* Autotuning of the commitment's launch plans (no reference counterpart; the reference has
+ * no GPU kernels). The LDE's stage split and persistent-pass occupancy ("lde", 6 plans), the
+ * leaf sponges' rows per block ("leaf", 3 plans) and the Merkle level schedule ("merkle",
+ * 3 plans) each have plans that write the same result at different speeds. A context that
+ * tunes (the default for wl_ctx_create; server workers do not) runs every plan the first time
+ * it meets a table shape, timed with CUDA events, and keeps the fastest per device and shape
+ * for every context of the process. wl_tune_force pins a family to one plan (-1: back to
+ * tuning); wl_tune_report writes the kept plans and their timings as JSON (same length
+ * convention as wl_transcript_dump); wl_tune_clear forgets them. */
+wl_status wl_ctx_set_autotune(wl_ctx* ctx, int32_t on);
+wl_status wl_tune_force(const char* family, int32_t plan);
+wl_status wl_tune_report(char* buf, size_t* len);
+wl_status wl_tune_clear(void);
+
 // Number of host synchronisations of the context's stream so far (device-to-host reads
 // of challenges, sums and roots). Diagnostics; no reference counterpart.
 wl_status wl_ctx_host_syncs(wl_ctx* ctx, uint64_t* out);

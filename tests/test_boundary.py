@@ -53,3 +53,15 @@ def test_device_field_arithmetic_on_host(tmp_path):
                     os.path.join(ROOT, "whirlaway_b200", "csrc", "host_perm.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_tuner_interface_without_device(wl):
+    """The autotuner's process-wide controls work without a GPU: families by name, plans in
+    range, an empty report before any proof."""
+    rep = wl.tune_report()
+    assert set(rep) == {"lde", "leaf", "merkle"}
+    wl.tune_force("lde", 5)
+    wl.tune_force("lde", -1)
+    for fam, plan in (("lde", 6), ("leaf", 3), ("nope", 0)):
+        with pytest.raises(wl.ProverError):
+            wl.tune_force(fam, plan)

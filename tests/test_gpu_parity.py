@@ -168,3 +168,50 @@ def test_sumcheck_abc_large_matches_oracle(oracle, wl, ctx, log_n, skips):
     got, ms = wl.sumcheck_abc_prove(ctx, p16, log_n, skips, a, b, c)
     assert np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
     assert wl.sumcheck_abc_verify(p16, log_n, skips, got) == 0
+
+
+@pytest.mark.parametrize("family,plan", [("lde", p) for p in range(6)] + [("leaf", p) for p in range(3)] +
+                         [("merkle", p) for p in range(3)])
+def test_every_tuned_plan_matches_oracle(oracle, wl, ctx, family, plan):
+    """Every launch plan the autotuner can pick writes the same commitment: a proof with the
+    plan forced equals the oracle's (2^13 rows: three NTT passes, 2^15 leaves so that the
+    Merkle schedules differ)."""
+    log_n = 13
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    ref, _ = oracle.prove(log_n, consts, wit)
+    wl.tune_force(family, plan)
+    try:
+        w = wl.Witness.generate(ctx, consts, inputs, log_n)
+        got = wl.AirTable(ctx, consts, log_n).prove_witness(w)
+        w.free()
+        got_host = wl.AirTable(ctx, consts, log_n).prove(wit)  # the tile-pipelined commitment
+    finally:
+        wl.tune_force(family, -1)
+    assert np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
+    assert np.array_equal(got_host, ref), f"first difference at {first_diff(got_host, ref)}"
+
+
+def test_autotuner_keeps_a_plan_per_shape(oracle, wl):
+    """A tuning context times every plan on the first proof of a shape and keeps the fastest;
+    the proof is still the oracle's, and a second proof of the shape reuses the kept plans."""
+    log_n = 11
+    consts, inputs = oracle.workload(log_n)
+    wit = oracle.trace(log_n, consts, inputs)
+    ref, _ = oracle.prove(log_n, consts, wit)
+    wl.tune_clear()
+    with wl.Context(0) as c:
+        c.set_autotune(True)
+        w = wl.Witness.generate(c, consts, inputs, log_n)
+        table = wl.AirTable(c, consts, log_n)
+        p1 = table.prove_witness(w)
+        rep = wl.tune_report()
+        p2 = table.prove_witness(w)
+        w.free()
+    assert np.array_equal(p1, ref) and np.array_equal(p2, ref)
+    for fam, n in (("lde", 6), ("leaf", 3), ("merkle", 3)):
+        assert rep[fam], fam
+        for e in rep[fam]:
+            assert len(e["ms"]) == n and 0 <= e["plan"] < n
+            assert e["ms"][e["plan"]] == min(e["ms"])
+    assert wl.tune_report() == rep  # nothing re-tuned by the second proof

@@ -120,6 +120,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_profile_json": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "wl_ctx_host_syncs": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "wl_ctx_set_spin_sync": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_ctx_set_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_tune_force": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32]),
+        "wl_tune_report": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]),
+        "wl_tune_clear": (ctypes.c_int, []),
         "wl_ctx_host_wait_ms": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "wl_profile_only": (ctypes.c_int, [vp, ctypes.c_char_p]),
     }
@@ -197,6 +201,10 @@ class Context:
     def set_spin_sync(self, spin: bool = True):
         """Busy-poll (True, the default) or block (False) at each host round trip."""
         self.check(self._lib.wl_ctx_set_spin_sync(self.handle, int(spin)), "set_spin_sync")
+
+    def set_autotune(self, on: bool = True):
+        """Tunes the commitment's launch plans on the first proof of each table shape."""
+        self.check(self._lib.wl_ctx_set_autotune(self.handle, int(on)), "set_autotune")
 
     def set_transcript_dump(self, on: bool = True):
         """Records a per-phase transcript dump of every later proof on this context."""
@@ -407,6 +415,30 @@ def sumcheck_abc_verify(p16_constants: np.ndarray, log_n: int, skips: int, proof
     c = np.ascontiguousarray(p16_constants, dtype=np.uint32)
     pr = np.ascontiguousarray(proof, dtype=np.uint32)
     return load_library().wl_sumcheck_abc_verify(_ptr(c), log_n, skips, _ptr(pr), pr.size)
+
+
+def tune_force(family: str, plan: int):
+    """Pins an autotuned family ("lde", "leaf", "merkle") to one plan (-1: tune again)."""
+    st = load_library().wl_tune_force(family.encode(), plan)
+    if st:
+        raise ProverError(st, "tune_force")
+
+
+def tune_report() -> dict:
+    """The autotuner's kept plans: {family: [{device, key, plan, ms}, ...]}."""
+    import json
+    lib = load_library()
+    n = ctypes.c_size_t(0)
+    lib.wl_tune_report(None, ctypes.byref(n))
+    buf = ctypes.create_string_buffer(n.value)
+    st = lib.wl_tune_report(buf, ctypes.byref(n))
+    if st:
+        raise ProverError(st, "tune_report")
+    return json.loads(buf.value.decode())
+
+
+def tune_clear():
+    load_library().wl_tune_clear()
 
 
 def proof_footprint_bytes(log_n: int, settings: AirSettings = AirSettings()) -> int:

@@ -12,6 +12,7 @@
 #include "prover.h"
 #include "server.h"
 #include "verifier.h"
+#include "tuner.h"
 
 struct wl_ctx {
   std::unique_ptr<wl::Context> c;
@@ -427,6 +428,29 @@ wl_status wl_profile_only(wl_ctx* ctx, const char* kernel_class) {
 wl_status wl_ctx_set_spin_sync(wl_ctx* ctx, int32_t spin) {
   if (!ctx) return WL_E_INVALID_ARG;
   ctx->c->spin_sync = spin != 0;
+  return WL_OK;
+}
+
+wl_status wl_ctx_set_autotune(wl_ctx* ctx, int32_t on) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  ctx->c->autotune = on != 0;
+  return WL_OK;
+}
+
+wl_status wl_tune_force(const char* family, int32_t plan) {
+  const int f = wl::tune_family_from_name(family);
+  if (f < 0 || plan < -1 || plan >= wl::tune_plan_count(f)) return WL_E_INVALID_ARG;
+  wl::tune_force(f, plan);
+  return WL_OK;
+}
+
+wl_status wl_tune_report(char* buf, size_t* len) {
+  if (!len) return WL_E_INVALID_ARG;
+  return emit_text(wl::tune_json(), buf, len);
+}
+
+wl_status wl_tune_clear(void) {
+  wl::tune_clear();
   return WL_OK;
 }
 

@@ -299,7 +299,7 @@ __global__ void k_twiddles(uint2* tw, uint32_t w24) {
   }
 }
 
-constexpr int LEAF_ROWS = 128;
+// Leaf rows per block: 64, 128 (default) or 256, the autotuner's pick (LEAF_PLANS).
 constexpr int TOP_LEVELS = 7;  // the last levels (<= 2^7 digests) run in one block
 constexpr int FLAT_LEVEL_MIN_LOG = 13;  // levels of at least 2^13 digests get their own launch
 
@@ -373,12 +373,13 @@ __device__ __forceinline__ void leaf_absorb(const uint32_t* __restrict__ lde, in
 // entries with the width-24 sponge (16 entries per absorption, 8 absorptions). Rows are read
 // straight from the tile-major LDE (no shared-memory staging, so occupancy is bounded by
 // registers).
-__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, int T, int n_cols,
-                                                         int log_elem, const __grid_constant__ kb::P24Consts c,
-                                                         uint32_t* __restrict__ tree) {
-  const size_t row0 = size_t(blockIdx.x) * LEAF_ROWS;
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, int T, int n_cols,
+                                                    int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                    uint32_t* __restrict__ tree) {
+  const size_t row0 = size_t(blockIdx.x) * ROWS;
   const size_t rows = size_t(1) << T;
-  const int nrows = (rows - row0) < size_t(LEAF_ROWS) ? int(rows - row0) : LEAF_ROWS;
+  const int nrows = (rows - row0) < size_t(ROWS) ? int(rows - row0) : ROWS;
   const int t = threadIdx.x;
   uint32_t st[24];
   if (t < nrows) {
@@ -396,11 +397,12 @@ __global__ void __launch_bounds__(LEAF_ROWS) k_leaf_hash(const uint32_t* __restr
 // One absorption (chunk ch) for every row, the capacity carried between launches in cap
 // (8 words per row): the sponge of k_leaf_hash split by chunk, so that chunk ch can be hashed
 // as soon as the LDE tiles it reads exist. The last chunk writes the digests.
-__global__ void __launch_bounds__(LEAF_ROWS) k_leaf_absorb(const uint32_t* __restrict__ lde, int T, int n_cols,
-                                                           int log_elem, const __grid_constant__ kb::P24Consts c,
-                                                           int ch, uint32_t* __restrict__ cap,
-                                                           uint32_t* __restrict__ tree) {
-  const size_t row = size_t(blockIdx.x) * LEAF_ROWS + threadIdx.x;
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS) k_leaf_absorb(const uint32_t* __restrict__ lde, int T, int n_cols,
+                                                      int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                      int ch, uint32_t* __restrict__ cap,
+                                                      uint32_t* __restrict__ tree) {
+  const size_t row = size_t(blockIdx.x) * ROWS + threadIdx.x;
   if (row >= (size_t(1) << T)) return;
   uint32_t st[24];
   if (ch == 0) {
@@ -630,14 +632,19 @@ void ntt_async_smem_limit(size_t bytes) {
 }
 }  // namespace
 
-void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s, int tile_begin, int tile_end) {
+void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_t s, int tile_begin, int tile_end,
+                int plan) {
   const int T = in.L + in.rho;
   if (T > 24) throw std::runtime_error("LDE beyond the two-adic subgroup of order 2^24");
   if (in.n_cols % 8 || in.n_cols <= 0) throw std::runtime_error("LDE column count must be a multiple of 8");
   if (tile_end < 0) tile_end = in.n_cols / 8;
   if (tile_begin < 0 || tile_begin >= tile_end || tile_end > in.n_cols / 8) throw std::runtime_error("LDE tile range");
+  if (plan < 0 || plan >= LDE_PLANS) plan = LDE_PLAN_DEFAULT;
   const int tiles = tile_end - tile_begin;
-  const int np = in.L <= NTT_MAX_BP ? 1 : (in.L + NTT_MAX_BP - 1) / NTT_MAX_BP;
+  // plan: the fewest passes of at most NTT_MAX_BP stages (plans 0-2) or one pass more (3-5),
+  // with 2, 3 or 4 persistent blocks per SM for the double-buffered passes
+  const int np = (in.L <= NTT_MAX_BP ? 1 : (in.L + NTT_MAX_BP - 1) / NTT_MAX_BP) + (plan >= 3 && in.L >= 2 ? 1 : 0);
+  const uint32_t async_per_sm = 2 + uint32_t(plan % 3);
   int Bs = in.rho, left = in.L;
   for (int p = 0; p < np; p++) {
     const int Bp = (left + (np - p) - 1) / (np - p);
@@ -649,7 +656,7 @@ void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_
     const size_t smem = ((size_t(32) << Bp) + (size_t(2) << lr_log) * ((1u << Bp) - 1)) * 4;
     const uint32_t nlines = gx * uint32_t(tiles);
     const size_t smem2 = ((size_t(64) << Bp) + size_t(8) * ((1u << Bp) - 1)) * 4;
-    const uint32_t per_sm = std::min<uint32_t>(NTT_ASYNC_BLOCKS_PER_SM, uint32_t((227 * 1024) / (smem2 + 1024)));
+    const uint32_t per_sm = std::min<uint32_t>(async_per_sm, uint32_t((227 * 1024) / (smem2 + 1024)));
     const uint32_t nblk = uint32_t(ntt_sm_count()) * std::max<uint32_t>(per_sm, 1);
     if (p == 0) {
       k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
@@ -674,30 +681,46 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
                         const kb::P16Consts& p16, uint32_t* tree, int LL, cudaStream_t s) {
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
-  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
-  k_leaf_hash<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24c,
-                                                                                     tree);
-  WL_LAUNCH_CHECK();
+  (void)log_elem;
+  launch_leaf_hash(lde, rows, n_cols, elem, p24, tree, LL, s, LEAF_PLAN_DEFAULT);
   launch_merkle_levels(tree, LL, p16, s);
 }
 
+void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
+                      uint32_t* tree, int LL, cudaStream_t s, int rows_choice) {
+  const int log_elem = elem == 8 ? 3 : 0;
+  if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
+  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
+  switch (rows_choice) {
+    case 0: k_leaf_hash<64><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(lde, LL, n_cols, log_elem, p24c, tree); break;
+    case 2: k_leaf_hash<256><<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(lde, LL, n_cols, log_elem, p24c, tree); break;
+    default: k_leaf_hash<128><<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(lde, LL, n_cols, log_elem, p24c, tree); break;
+  }
+  WL_LAUNCH_CHECK();
+}
+
 void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24, int ch,
-                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s) {
+                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s, int rows_choice) {
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
   if (ch < 0 || ch > 7) throw std::invalid_argument("leaf chunk out of range");
   const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
-  k_leaf_absorb<<<(unsigned)((rows + LEAF_ROWS - 1) / LEAF_ROWS), LEAF_ROWS, 0, s>>>(lde, LL, n_cols, log_elem, p24c,
-                                                                                       ch, cap, tree);
+  switch (rows_choice) {
+    case 0: k_leaf_absorb<64><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(lde, LL, n_cols, log_elem, p24c, ch, cap, tree); break;
+    case 2: k_leaf_absorb<256><<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(lde, LL, n_cols, log_elem, p24c, ch, cap, tree); break;
+    default: k_leaf_absorb<128><<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(lde, LL, n_cols, log_elem, p24c, ch, cap, tree); break;
+  }
   WL_LAUNCH_CHECK();
 }
 
-void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s) {
+void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s, int plan) {
   const kb::P16Consts p16c = kb::p2_consts_canonical(p16);
   // Wide levels: one launch each, one compression per thread. Narrower levels: 16 lanes per
-  // compression. The last levels (at most 128 digests) in one block.
+  // compression. The last levels (at most 128 digests) in one block. The plan sets the width
+  // from which a level runs one compression per thread: 2^11, 2^13 (default) or 2^15 digests.
+  const int flat_min = plan == 0 ? 11 : plan == 2 ? 15 : FLAT_LEVEL_MIN_LOG;
   int l0 = 0;
-  while (l0 < LL && LL - l0 - 1 >= FLAT_LEVEL_MIN_LOG) {
+  while (l0 < LL && LL - l0 - 1 >= flat_min) {
     const size_t cnt = size_t(1) << (LL - l0 - 1);
     k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16c);
     WL_LAUNCH_CHECK();

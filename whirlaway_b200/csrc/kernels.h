@@ -30,8 +30,11 @@ struct LdeSource {
 // Codeword matrix of 2^(L + rho) rows and n_cols (a multiple of 8) columns, tile-major:
 // word (tile, row, c) at (tile * 2^(L+rho) + row) * 8 + c.
 // Tiles [tile_begin, tile_end) of 8 columns only (default: all); tiles are independent.
+// plan (0 .. LDE_PLANS - 1, chosen by the autotuner): the pass split and the persistent
+// passes' blocks per SM; every plan writes the same codeword.
+constexpr int LDE_PLANS = 6, LDE_PLAN_DEFAULT = 2;
 void launch_lde(const LdeSource& in, uint32_t* out, const uint2* twiddles, cudaStream_t s, int tile_begin = 0,
-                int tile_end = -1);
+                int tile_end = -1, int plan = LDE_PLAN_DEFAULT);
 // Per-stage twiddle table (2^24 - 1 entries): stage t = 1..24 holds (w canonical,
 // floor(w 2^32 / p)) for w = w_{2^t}^x, x < 2^(t-1), at offset 2^(t-1) - 1.
 constexpr size_t TWIDDLE_ENTRIES = (size_t(1) << 24) - 1;
@@ -47,9 +50,16 @@ void launch_merkle_tree(const uint32_t* lde, size_t rows, int n_cols, int elem, 
 // (and, through the Moebius transform, those of the chunks below it); the 8 capacity words of
 // every row are carried in cap (8 * rows words) and chunk 7 writes the digests. Then
 // launch_merkle_levels builds the compressions.
+// rows_choice / plan: the autotuner's pick (leaf rows per block 64, 128 (default) or 256; the
+// level width from which compressions run one per thread 2^11, 2^13 (default) or 2^15).
+constexpr int LEAF_PLANS = 3, LEAF_PLAN_DEFAULT = 1, MERKLE_PLANS = 3, MERKLE_PLAN_DEFAULT = 1;
 void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24, int ch,
-                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s);
-void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s);
+                        uint32_t* cap, uint32_t* tree, int LL, cudaStream_t s, int rows_choice = LEAF_PLAN_DEFAULT);
+// Level 0 of the tree (the leaf digests) only.
+void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, const kb::P24Consts& p24,
+                      uint32_t* tree, int LL, cudaStream_t s, int rows_choice = LEAF_PLAN_DEFAULT);
+void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s,
+                          int plan = MERKLE_PLAN_DEFAULT);
 // Gathers rows idx[q] of a tile-major LDE matrix (2^T rows, n_cols <= 128 stored columns) as
 // the leaves hash them: 128 values per row (zero beyond n_cols), Moebius-transformed over the
 // position bits [log_elem, 7), into out[q * 128 + i]. With mono (128 >> log_elem entries),

@@ -11,6 +11,7 @@
 #include <mutex>
 
 #include "prover.h"
+#include "tuner.h"
 
 namespace wl {
 
@@ -458,6 +459,49 @@ struct Commitment {
 };
 size_t level_offset(int LL, int l) { return (size_t(1) << (LL + 1)) - (size_t(1) << (LL + 1 - l)); }
 
+// Runs launch(plan) with the autotuner's plan for (family, key): a forced plan, else the kept
+// one, else (on a tuning context) every plan in turn, each timed twice with CUDA events on the
+// context's stream, keeping the fastest (all plans write the same result, so the data is
+// right whichever ran last); a context that does not tune uses the default plan.
+template <class Launch>
+void tuned(Context& ctx, int family, uint64_t key, Launch&& launch) {
+  int plan = tune_forced(family);
+  if (plan < 0) plan = tune_lookup(ctx.device, family, key);
+  if (plan >= 0 || !ctx.autotune) {
+    launch(plan >= 0 ? plan : tune_default_plan(family));
+    return;
+  }
+  const int n = tune_plan_count(family);
+  std::vector<float> ms(n, 1e30f);
+  cudaEvent_t a = ctx.take_event(), b = ctx.take_event();
+  for (int rep = 0; rep < 2; rep++)
+    for (int c = 0; c < n; c++) {
+      WL_CUDA(cudaEventRecord(a, ctx.stream));
+      launch(c);
+      WL_CUDA(cudaEventRecord(b, ctx.stream));
+      WL_CUDA(cudaEventSynchronize(b));
+      float t = 0;
+      WL_CUDA(cudaEventElapsedTime(&t, a, b));
+      ms[c] = std::min(ms[c], t);
+    }
+  ctx.event_pool.push_back(a);
+  ctx.event_pool.push_back(b);
+  int best = 0;
+  for (int c = 1; c < n; c++)
+    if (ms[c] < ms[best]) best = c;
+  tune_store(ctx.device, family, key, best, ms);
+}
+// The kept (or forced) plan without tuning: the tile-pipelined commitment cannot re-run its
+// launches, it uses what a device-witness proof of the same shape has tuned.
+int tuned_plan(Context& ctx, int family, uint64_t key) {
+  int plan = tune_forced(family);
+  if (plan < 0) plan = tune_lookup(ctx.device, family, key);
+  return plan >= 0 ? plan : tune_default_plan(family);
+}
+uint64_t lde_key(const LdeSource& src) {
+  return uint64_t(src.L) | uint64_t(src.rho) << 8 | uint64_t(src.n_cols) << 16 | uint64_t(src.elem) << 32;
+}
+
 Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, const kb::P24Consts& p24,
                   const kb::P16Consts& p16, const std::vector<cudaEvent_t>* tile_ready = nullptr) {
   Commitment c;
@@ -478,21 +522,33 @@ Commitment commit(Context& ctx, const LdeSource& src, int num_vars, int fold, co
     // are encoded, and the hashing overlaps the rest of the upload too.
     DBuf cap(sizeof(uint32_t) * 8 * rows, ctx.stream);
     const int ntiles = c.n_cols / 8;
+    const int lde_plan = tuned_plan(ctx, TUNE_LDE, lde_key(src));
+    const int leaf_plan = tuned_plan(ctx, TUNE_LEAF, lde_key(src));
     int next = 0;
     for (int ch = 0; ch < 8; ch++) {
       for (; next < std::min(ntiles, 2 * ch + 2); next++) {
         if (next < (int)tile_ready->size()) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[next], 0));
         ProfScope _ps(ctx, "lde");
-        launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, next, next + 1);
+        launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, next, next + 1, lde_plan);
       }
       ProfScope _ps(ctx, "merkle_tree");
-      launch_leaf_absorb(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, ch, cap.as<uint32_t>(), t, LL, ctx.stream);
+      launch_leaf_absorb(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, ch, cap.as<uint32_t>(), t, LL, ctx.stream,
+                         leaf_plan);
     }
     for (size_t e = ntiles; e < tile_ready->size(); e++) WL_CUDA(cudaStreamWaitEvent(ctx.stream, (*tile_ready)[e], 0));
-    { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_levels(t, LL, p16, ctx.stream); }
+    { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_levels(t, LL, p16, ctx.stream, tuned_plan(ctx, TUNE_MERKLE, LL)); }
   } else {
-    { ProfScope _ps(ctx, "lde"); launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream); }
-    { ProfScope _ps(ctx, "merkle_tree"); launch_merkle_tree(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, p16, t, LL, ctx.stream); }
+    {
+      ProfScope _ps(ctx, "lde");
+      tuned(ctx, TUNE_LDE, lde_key(src), [&](int plan) {
+        launch_lde(src, c.lde.as<uint32_t>(), ctx.twiddles, ctx.stream, 0, -1, plan);
+      });
+    }
+    ProfScope _ps(ctx, "merkle_tree");
+    tuned(ctx, TUNE_LEAF, lde_key(src), [&](int plan) {
+      launch_leaf_hash(c.lde.as<uint32_t>(), rows, c.n_cols, c.elem, p24, t, LL, ctx.stream, plan);
+    });
+    tuned(ctx, TUNE_MERKLE, LL, [&](int plan) { launch_merkle_levels(t, LL, p16, ctx.stream, plan); });
   }
   ctx.to_host(c.root, t + level_offset(LL, LL) * 8, 32);
   for (uint32_t& w : c.root) w = kb::to_mont(w);  // the tree holds canonical digests

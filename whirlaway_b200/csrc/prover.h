@@ -70,6 +70,9 @@ struct Context {
   // ~20 ms of wake-up stalls per proof); false = the thread polls for block_after_us, then
   // sleeps on a blocking-sync event (server workers, which would otherwise occupy one CPU each).
   bool spin_sync = true;
+  // When set, the first proof of each table shape tunes the commitment's launch plans (see
+  // tuner.h); server workers leave it off and use the plans a tuning context has kept.
+  bool autotune = true;
   // When set, prove_air records a per-phase transcript log of each proof into last_dump (JSON).
   bool dump_transcript = false;
   std::string last_dump;

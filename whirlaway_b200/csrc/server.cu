@@ -57,6 +57,7 @@ Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), 
     contexts_.back()->spin_sync = false;  // workers block: the other workers' proofs fill the device
     if (const char* v = std::getenv("WL_WORKER_POLL_US")) contexts_.back()->block_after_us = std::atoi(v);
     contexts_.back()->set_cache_limit(0);  // admission counts running proofs only: no cached buffers
+    contexts_.back()->autotune = false;    // concurrent proofs would disturb the timings
   }
   // The budget is reserved in the stream-ordered pool up front (one allocation, freed at once;
   // the pool keeps it and carves the workers' buffers from it). Growing the pool while proofs
