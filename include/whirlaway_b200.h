@@ -138,6 +138,17 @@ wl_status wl_verify_batch(const wl_air_settings* settings, const uint32_t* const
                           const int32_t* log_ns, const uint32_t* const* proofs, const size_t* proof_lens,
                           int32_t threads, int32_t* statuses);
 
+/* wl_verify_batch with the Merkle paths checked on the context's GPU: each proof's transcript
+ * is replayed on host threads (one proof per thread, `threads` as for wl_verify_batch) with its
+ * Merkle openings listed instead of hashed, then every opening of every proof (the leaf sponge
+ * over the opened row and one compression per level of its path) is checked by one kernel.
+ * statuses[i] equals wl_verify's outcome for proof i: a failed opening is an opening error
+ * (every listed opening precedes the check that ended the replay). Same arguments as
+ * wl_verify_batch plus the context; WL_OK when every proof was checked. */
+wl_status wl_verify_batch_device(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants, int32_t n,
+                                 const int32_t* log_ns, const uint32_t* const* proofs, const size_t* proof_lens,
+                                 int32_t threads, int32_t* statuses);
+
 /* Per-phase transcript dumps, for diffing against another implementation of the protocol (a
  * build of the reference with the same parameters): JSON text
  *   {"proof_len": L, "events": [{"kind", "phase", "offset", "values"}, ...]}

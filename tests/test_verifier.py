@@ -178,3 +178,46 @@ def test_tiny_tables(wl, oracle, log_n, skips):
     bad = proof.copy()
     bad[proof.size // 3] = (int(bad[proof.size // 3]) + 1) % P
     assert wl.verify(consts, log_n, bad, s) != OK
+
+
+@pytest.mark.gpu
+def test_verify_batch_device_matches_host(oracle, wl, ctx):
+    """The GPU-checked batch verifier gives every proof the host verifier's outcome: honest
+    proofs of several sizes are accepted; a corrupted opened row, path digest or commitment
+    root is an opening error (11 for a root the commitment phase already reads), and a corrupted
+    sumcheck word fails before the openings with the host's outcome."""
+    consts, _ = oracle.workload(2)
+    jobs = []
+    for log_n in (6, 8, 9):
+        c, inputs = oracle.workload(log_n)
+        assert np.array_equal(c, consts)
+        jobs.append((log_n, oracle.prove(log_n, consts, oracle.trace(log_n, consts, inputs))[0]))
+    dump_n, dump_p = jobs[1]
+    _, tr = wl.verify_transcript(consts, dump_n, dump_p)
+    phases = {e["phase"]: e["offset"] for e in tr["events"] if e["kind"] == "phase"}
+    # opened rows and paths follow each "queries" event (hints, not absorbed)
+    qoffs = [e["offset"] for e in tr["events"] if e["kind"] == "queries"]
+    assert len(qoffs) >= 2
+    bad = []
+    p = dump_p.copy()
+    p[qoffs[0] + 5] = (int(p[qoffs[0] + 5]) + 1) % 0x7F000001  # a word of the first opened row
+    bad.append((dump_n, p))
+    p = dump_p.copy()
+    p[qoffs[-1] + 128 + 3] = (int(p[qoffs[-1] + 128 + 3]) + 1) % 0x7F000001  # a digest of a path
+    bad.append((dump_n, p))
+    p = dump_p.copy()
+    p[phases["whir_round_1"] + 3] = (int(p[phases["whir_round_1"] + 3]) + 1) % 0x7F000001  # a later root
+    bad.append((dump_n, p))
+    p = dump_p.copy()
+    p[phases["zerocheck"] + 9] = (int(p[phases["zerocheck"] + 9]) + 1) % 0x7F000001
+    bad.append((dump_n, p))
+    p = dump_p.copy()
+    p[0] = (int(p[0]) + 1) % 0x7F000001  # the first commitment's root
+    bad.append((dump_n, p))
+    allj = jobs + bad
+    host = wl.verify_batch(consts, allj)
+    dev = wl.verify_batch_device(ctx, consts, allj)
+    assert host[:3] == [0, 0, 0]
+    assert all(h != 0 for h in host[3:])
+    assert host[3] == OPENING and host[4] == OPENING
+    assert dev == host

@@ -98,7 +98,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_kernel_launch_count": (ctypes.c_uint64, []),
         "wl_sumcheck_abc_prove_noalloc": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, _u32p,
                                                          _sizep, vp]),
-        "wl_proof_footprint_bytes": (ctypes.c_uint64, [vp, ctypes.c_int32]),
+        "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.POINTER(_Settings), ctypes.c_int32]),
         "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_verify_batch": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
@@ -121,6 +121,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wl_ctx_host_syncs": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "wl_ctx_set_spin_sync": (ctypes.c_int, [vp, ctypes.c_int32]),
         "wl_ctx_set_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "wl_verify_batch_device": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
+                                                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_u32p), _sizep,
+                                                  ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
         "wl_tune_force": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32]),
         "wl_tune_report": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]),
         "wl_tune_clear": (ctypes.c_int, []),
@@ -398,6 +401,21 @@ def _text_call(fn, *args):
         if st != 4:  # not WL_E_BUFFER_TOO_SMALL
             return st, buf.value.decode()
     raise ProverError(st, "transcript dump")
+
+
+def verify_batch_device(ctx, constants: np.ndarray, jobs, settings: AirSettings = AirSettings(), threads: int = 0):
+    """wl_verify_batch with the Merkle paths of all proofs checked in one GPU kernel on `ctx`'s
+    device (the transcripts replay on host threads); returns the list of statuses."""
+    c = np.ascontiguousarray(constants, dtype=np.uint32)
+    prs = [np.ascontiguousarray(p, dtype=np.uint32) for _, p in jobs]
+    n = len(jobs)
+    log_ns = (ctypes.c_int32 * n)(*[int(l) for l, _ in jobs])
+    ptrs = (_u32p * n)(*[_ptr(p) for p in prs])
+    lens = (ctypes.c_size_t * n)(*[p.size for p in prs])
+    out = (ctypes.c_int32 * n)()
+    ctx.check(ctx._lib.wl_verify_batch_device(ctx.handle, ctypes.byref(settings._c()), _ptr(c), n, log_ns, ptrs, lens,
+                                              threads, out), "verify_batch_device")
+    return list(out)
 
 
 def verify_transcript(constants: np.ndarray, log_n: int, proof: np.ndarray, settings: AirSettings = AirSettings()):

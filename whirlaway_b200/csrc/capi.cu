@@ -390,6 +390,71 @@ wl_status wl_verify_batch(const wl_air_settings* s, const uint32_t* constants, i
   });
 }
 
+wl_status wl_verify_batch_device(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, int32_t n,
+                                 const int32_t* log_ns, const uint32_t* const* proofs, const size_t* proof_lens,
+                                 int32_t threads, int32_t* statuses) {
+  if (!ctx || !s || !constants || n < 0 || (n && (!log_ns || !proofs || !proof_lens || !statuses)))
+    return WL_E_INVALID_ARG;
+  return guarded(ctx, [&] {
+    // 1) every transcript on host threads, one proof per thread, Merkle openings listed
+    std::vector<std::vector<wl::MerkleOpening>> open(n);
+    unsigned hw = std::thread::hardware_concurrency();
+    int T = threads > 0 ? threads : int(hw ? hw : 1);
+    T = std::max(1, std::min(T, std::max(n, 1)));
+    std::atomic<int> next{0};
+    auto work = [&] {
+      for (int i = next++; i < n; i = next++) {
+        std::string why;
+        const uint32_t* pr = proofs[i];
+        const size_t len = proof_lens[i];
+        bool canonical = pr || !len;
+        for (size_t k = 0; canonical && k < len; k++) canonical = pr[k] < kb::P;
+        if (!canonical || !settings_ok(s, log_ns[i], why)) {
+          statuses[i] = WL_E_INVALID_ARG;
+          continue;
+        }
+        wl::ProofJob job = make_job(s, constants, log_ns[i]);
+        statuses[i] = wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_ns[i], pr, len, nullptr, 1,
+                                           &open[i]);
+      }
+    };
+    wl::run_on_threads(size_t(T), work);
+    // 2) all openings in one kernel over the concatenated proofs
+    std::vector<size_t> base(n + 1, 0);
+    for (int i = 0; i < n; i++) base[i + 1] = base[i] + (open[i].empty() ? 0 : proof_lens[i]);
+    std::vector<wl::OpeningCheck> ops;
+    std::vector<int> owner;
+    for (int i = 0; i < n; i++)
+      for (const wl::MerkleOpening& o : open[i]) {
+        ops.push_back({base[i] + o.row, base[i] + o.path, base[i] + o.root, o.q, o.ll});
+        owner.push_back(i);
+      }
+    if (ops.empty()) return WL_OK;
+    wl::Context& c = *ctx->c;
+    wl::DBuf words(sizeof(uint32_t) * base[n], c.stream), dops(sizeof(wl::OpeningCheck) * ops.size(), c.stream),
+        dok(ops.size(), c.stream);
+    for (int i = 0; i < n; i++)
+      if (!open[i].empty())
+        WL_CUDA(cudaMemcpyAsync(words.as<uint32_t>() + base[i], proofs[i], sizeof(uint32_t) * proof_lens[i],
+                                cudaMemcpyHostToDevice, c.stream));
+    WL_CUDA(cudaMemcpyAsync(dops.as<void>(), ops.data(), sizeof(wl::OpeningCheck) * ops.size(), cudaMemcpyHostToDevice,
+                            c.stream));
+    const wl::ProofJob job = make_job(s, constants, log_ns[0]);
+    {
+      wl::ProfScope _ps(c, "check_openings");
+      wl::launch_check_openings(words.as<uint32_t>(), dops.as<wl::OpeningCheck>(), int(ops.size()), job.p24, job.p16,
+                                dok.as<uint8_t>(), c.stream);
+    }
+    std::vector<uint8_t> ok(ops.size());
+    WL_CUDA(cudaMemcpyAsync(ok.data(), dok.as<void>(), ok.size(), cudaMemcpyDeviceToHost, c.stream));
+    c.wait_stream();
+    // 3) a failed opening comes before whatever ended the replay: an opening error
+    for (size_t j = 0; j < ok.size(); j++)
+      if (!ok[j]) statuses[owner[j]] = WL_E_INVALID_PCS_OPENING;
+    return WL_OK;
+  });
+}
+
 wl_status wl_sumcheck_abc_verify(const uint32_t* p16c, int32_t log_n, int32_t skips, const uint32_t* proof,
                                  size_t proof_len) {
   if (!p16c || (!proof && proof_len) || log_n < 2 || log_n > 26 || skips < 1 || skips > 4 || skips >= log_n)

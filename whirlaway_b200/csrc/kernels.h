@@ -215,4 +215,17 @@ void launch_prod_round_finish(const ef* partial, int nb, const FinishConsts& fc,
 void launch_whir_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
                               ef* ch_out, cudaStream_t s);
 
+// --------------------------------------------------------------- batched Merkle-path checks
+// One opening to check: word offsets (into the concatenated canonical proofs) of its row (128
+// values), its path (ll digests, leaf level first) and its root; q is the leaf index.
+struct OpeningCheck {
+  uint64_t row, path, root;
+  uint32_t q;
+  int32_t ll;
+};
+// ok[i] = 1 when opening i's row hashes, through its path, to its root (p24, p16: Montgomery
+// constants as in a constants blob).
+void launch_check_openings(const uint32_t* words, const OpeningCheck* ops, int n, const kb::P24Consts& p24,
+                           const kb::P16Consts& p16, uint8_t* ok, cudaStream_t s);
+
 }  // namespace wl

@@ -176,11 +176,12 @@ struct Group {
 class WhirVerifier {
  public:
   WhirVerifier(const WhirSchedule& ws, const kb::P16Consts& p16, const kb::P24Consts& p24, ProofReader& rd,
-               int threads)
-      : ws_(ws), p16_(p16), p24_(p24), rd_(rd), threads_(threads) {}
+               int threads, std::vector<MerkleOpening>* defer)
+      : ws_(ws), p16_(p16), p24_(p24), rd_(rd), threads_(threads), defer_(defer) {}
 
   // Commitment: the root, then one answer per OOD sample z at the point (z, z^2, z^4, ...).
   bool parse_commitment(Digest& root, std::vector<std::vector<ef>>& pts, std::vector<ef>& vals) {
+    root0_off_ = rd_.pos;
     if (!rd_.base(root.data(), 8)) return false;
     for (int q = 0; q < ws_.c[0].ood; q++) {
       const ef z = rd_.sample();
@@ -198,11 +199,13 @@ class WhirVerifier {
     add_group(0, pts, vals, rd_.sample(), sigma);
     if (!fold_block(ws_.c[0].fold, sigma)) return false;
     Digest prev_root = root0;
+    size_t prev_root_off = root0_off_;
     for (int i = 0; i < ws_.num_rounds; i++) {
       const WhirRound& ci = ws_.c[i];
       const WhirRound& cn = ws_.c[i + 1];
       rd_.phase(("whir_round_" + std::to_string(i + 1)).c_str());
       Digest root;
+      const size_t root_off = rd_.pos;
       if (!rd_.base(root.data(), 8)) return false;
       std::vector<std::vector<ef>> npts;
       std::vector<ef> nvals;
@@ -217,7 +220,7 @@ class WhirVerifier {
       // STIR queries on the previous commitment: the folded value of each opened row
       std::vector<uint32_t> q;
       std::vector<ef> folded;
-      if (!open(ci, i == 0 ? 1 : 8, prev_root, q, folded)) return false;
+      if (!open(ci, i == 0 ? 1 : 8, prev_root, prev_root_off, q, folded)) return false;
       const uint32_t gen = kb::two_adic_gen_m(ci.log_leaves());
       for (size_t t = 0; t < q.size(); t++) {
         npts.push_back(pow_point(kb::ef_from(kb::pow_m(gen, q[t])), cn.num_vars));
@@ -226,6 +229,7 @@ class WhirVerifier {
       add_group(blocks_.size(), npts, nvals, rd_.sample(), sigma);
       if (!fold_block(cn.fold, sigma)) return false;
       prev_root = root;
+      prev_root_off = root_off;
     }
     // final polynomial, its queries, the last sumcheck
     rd_.phase("whir_final");
@@ -235,7 +239,7 @@ class WhirVerifier {
     if (!rd_.pow(cl.pow_bits)) return false;
     std::vector<uint32_t> q;
     std::vector<ef> folded;
-    if (!open(cl, ws_.num_rounds == 0 ? 1 : 8, prev_root, q, folded)) return false;
+    if (!open(cl, ws_.num_rounds == 0 ? 1 : 8, prev_root, prev_root_off, q, folded)) return false;
     const uint32_t gen = kb::two_adic_gen_m(cl.log_leaves());
     for (size_t t = 0; t < q.size(); t++)
       if (!kb::ef_eq(folded[t], mle_eval(gfin, pow_point(kb::ef_from(kb::pow_m(gen, q[t])), ws_.final_vars))))
@@ -282,7 +286,11 @@ class WhirVerifier {
   // Samples the queries of round `rc` on the commitment with `root`, checks each opened row
   // (128 values, Moebius-transformed as hashed) against it and folds it with the last block's
   // randomness (coefficient form, the row's most significant position bit first).
-  bool open(const WhirRound& rc, int elem, const Digest& root, std::vector<uint32_t>& q, std::vector<ef>& folded) {
+  // With a deferral list, the paths are not hashed here: each opening (offsets of its row, path
+  // and root in proof_data) is appended to the list for a batched check, and the rows are
+  // folded as if their paths held.
+  bool open(const WhirRound& rc, int elem, const Digest& root, size_t root_off, std::vector<uint32_t>& q,
+            std::vector<ef>& folded) {
     const int ll = rc.log_leaves();
     q.resize(rc.queries);
     for (auto& x : q) x = rd_.ch.sample_bits(ll);
@@ -293,21 +301,28 @@ class WhirVerifier {
     // (each query is independent: one leaf sponge, ll compressions, one fold)
     const size_t nq = q.size(), rl = 128, pl = size_t(8) * ll;
     std::vector<uint32_t> rows(nq * rl), paths(nq * pl);
-    for (size_t i = 0; i < nq; i++)
-      if (!rd_.hint(&rows[i * rl], rl) || !rd_.hint(&paths[i * pl], pl)) return false;
+    for (size_t i = 0; i < nq; i++) {
+      const size_t row_off = rd_.pos;
+      if (!rd_.hint(&rows[i * rl], rl)) return false;
+      const size_t path_off = rd_.pos;
+      if (!rd_.hint(&paths[i * pl], pl)) return false;
+      if (defer_) defer_->push_back({row_off, path_off, root_off, q[i], ll});
+    }
     const std::vector<ef>& r = blocks_.back();
     folded.assign(nq, kb::ef_zero());
     std::vector<char> good(nq, 0);
     auto check = [&](size_t i) {
       const uint32_t* row = &rows[i * rl];
       const uint32_t* path = &paths[i * pl];
-      Digest cur = leaf_digest(row, p24_);
-      for (int l = 0; l < ll; l++) {
-        Digest sib;
-        for (int e = 0; e < 8; e++) sib[e] = path[size_t(l) * 8 + e];
-        cur = ((q[i] >> l) & 1) ? compress(sib, cur, p16_) : compress(cur, sib, p16_);
+      if (!defer_) {
+        Digest cur = leaf_digest(row, p24_);
+        for (int l = 0; l < ll; l++) {
+          Digest sib;
+          for (int e = 0; e < 8; e++) sib[e] = path[size_t(l) * 8 + e];
+          cur = ((q[i] >> l) & 1) ? compress(sib, cur, p16_) : compress(cur, sib, p16_);
+        }
+        if (cur != root) return;
       }
-      if (cur != root) return;
       const int k = rc.fold;
       std::vector<ef> v(size_t(1) << k);
       for (size_t p = 0; p < v.size(); p++) {
@@ -344,6 +359,8 @@ class WhirVerifier {
   const kb::P24Consts& p24_;
   ProofReader& rd_;
   int threads_;                          // host threads for the query checks (0: up to 16)
+  std::vector<MerkleOpening>* defer_;    // when set, openings are listed instead of checked
+  size_t root0_off_ = 0;
   std::vector<std::vector<ef>> blocks_;  // folding randomness of each sumcheck block
   std::vector<Group> groups_;
 };
@@ -351,13 +368,14 @@ class WhirVerifier {
 }  // namespace
 
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
-                     int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log, int threads) {
+                     int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log, int threads,
+                     std::vector<MerkleOpening>* defer) {
   const int k = s.univariate_skips, W = AIR_W, nsk = 1 << k;
   const WhirSchedule ws = WhirSchedule::build(n + AIR_LOG_W, s);
   ProofReader rd(&p16, proof, proof_len, log);
   for (uint32_t x : ws.domain_separator()) rd.ch.observe(kb::to_mont(x));
   rd.phase("commit");
-  WhirVerifier whir(ws, p16, p24, rd, threads);
+  WhirVerifier whir(ws, p16, p24, rd, threads, defer);
   Digest root;
   std::vector<std::vector<ef>> ood_pts;
   std::vector<ef> ood_vals;
