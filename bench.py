@@ -375,6 +375,10 @@ def sumcheck_run(wl, ctx, args):
     for _ in range(2):
         proof, _ = wl.sumcheck_abc_prove(ctx, p16, log_n, k, a, b, c, device=True)
     runs = [wl.sumcheck_abc_prove(ctx, p16, log_n, k, a, b, c, device=True)[1] for _ in range(args.sumcheck_reps)]
+    ctx.profile(True)  # one more run with every kernel class timed (not part of round_ms)
+    wl.sumcheck_abc_prove(ctx, p16, log_n, k, a, b, c, device=True)
+    prof = {n: round(v[0], 4) for n, v in ctx.profile_report().items() if not n.startswith("host:")}
+    ctx.profile(False)
     rounds = [float(np.median([r[i] for r in runs])) for i in range(len(runs[0]))]
     assert wl.sumcheck_abc_verify(p16, log_n, k, proof) == 0
     S = 1 << (log_n - k)
@@ -393,6 +397,7 @@ def sumcheck_run(wl, ctx, args):
             "round_hbm_gbs": [round(b / (t * 1e-3) / 1e9, 1) for b, t in zip(byts, rounds)],
             "round0_hbm_frac": byts[0] / (rounds[0] * 1e-3) / 1e9 / args.hbm_peak,
             "algorithmic_bytes": sum(byts), "reps": args.sumcheck_reps, "verified": True,
+            "kernel_profile_ms": prof,
             "timing": "median over reps of CUDA-event time per round on the prover's stream"}
 
 
