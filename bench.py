@@ -607,6 +607,7 @@ def run_ours(args, world, rank, local):
         "kernel_profile_source": "CUDA events per kernel class over the last warm-up proof",
         "host_profile_ms": host_profile,
         "proof_len": int(proof.size),
+        "autotune": wl.tune_report(),
         "sumcheck_microbench": sumcheck,
         "batched": batched,
         "serving": serving,

@@ -215,3 +215,16 @@ def test_autotuner_keeps_a_plan_per_shape(oracle, wl):
             assert len(e["ms"]) == n and 0 <= e["plan"] < n
             assert e["ms"][e["plan"]] == min(e["ms"])
     assert wl.tune_report() == rep  # nothing re-tuned by the second proof
+
+
+def test_prove_bench_size_matches_oracle(oracle, wl, ctx):
+    """The benchmark's own workload, 2^20 rows with the reference's defaults, proved on the GPU
+    and by the oracle (two to three minutes of the host's threads): the proofs are identical."""
+    log_n = 20
+    consts, inputs = wl.generate_workload(log_n)
+    w = wl.Witness.generate(ctx, consts, inputs, log_n)
+    got = wl.AirTable(ctx, consts, log_n).prove_witness(w)
+    wit = w.download()
+    w.free()
+    ref, _ = oracle.prove(log_n, consts, wit)
+    assert got.size == ref.size and np.array_equal(got, ref), f"first difference at {first_diff(got, ref)}"
