@@ -11,6 +11,8 @@
 // samples pop from the end of the last squeeze) and leaves the challenge in device memory for
 // the fold, so the host enqueues a whole phase of rounds without waiting and reads the
 // appended proof words, the challenges and the challenger state back once at its end.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace wl {
@@ -168,7 +170,40 @@ __global__ void __launch_bounds__(FIN_THREADS) k_whir_round_finish(const ef* __r
   *stp = st;
 }
 
+// First level of the reduction of nb interleaved rows of k partial sums (partial[row * k + z]):
+// block b sums a contiguous range of rows into out[b * k + z]. Thread t takes sum z = t % k on
+// rows t / k, t / k + tpz, ... (tpz = 256 / k threads per sum), so a warp reads consecutive
+// extension elements.
+constexpr int WIDE_THREADS = 256;
+__global__ void __launch_bounds__(WIDE_THREADS) k_reduce_wide(const ef* __restrict__ partial, int nb, int k,
+                                                              ef* __restrict__ out) {
+  __shared__ ef red[WIDE_THREADS];
+  const int tpz = WIDE_THREADS / k, t = threadIdx.x;
+  const int per = (nb + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(nb, r0 + per);
+  ef acc = kb::ef_zero();
+  if (t < tpz * k) {
+    const int z = t % k;
+    for (int r = r0 + t / k; r < r1; r += tpz) acc = kb::ef_add(acc, partial[size_t(r) * k + z]);
+  }
+  red[t] = acc;
+  __syncthreads();
+  if (t < k) {
+    ef s = kb::ef_zero();
+    for (int i = 0; i < tpz; i++) s = kb::ef_add(s, red[i * k + t]);
+    out[size_t(blockIdx.x) * k + t] = s;
+  }
+}
+
 }  // namespace
+
+int launch_reduce_wide(const ef* partial, int nb, int k, ef* out, int max_blocks, cudaStream_t s) {
+  if (k < 1 || k > 32) throw std::invalid_argument("wide reduction of 1..32 sums");
+  const int blocks = std::max(1, std::min(max_blocks, (nb + 63) / 64));
+  k_reduce_wide<<<blocks, WIDE_THREADS, 0, s>>>(partial, nb, k, out);
+  WL_LAUNCH_CHECK();
+  return blocks;
+}
 
 void launch_eqsc_round_finish(int npts, const ef* partial, int nb, const ef& r, const ef& rinv,
                               const FinishConsts& fc, DevRound* st, uint32_t* proof, ef* ch_out, cudaStream_t s) {

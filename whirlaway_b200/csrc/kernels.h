@@ -208,6 +208,10 @@ struct FinishConsts {
 // ch_out[st->round] and updates st. Eq-factor rounds (npts 4: the AIR zerocheck, 3: the a*b - c
 // zerocheck) take the current variable's eq challenge r and its inverse; the product
 // sumcheck (inner sumcheck) and the WHIR folding sumcheck need no more.
+// First level of a reduction of nb interleaved rows of k <= 32 partial sums
+// (partial[row * k + z]) into at most max_blocks rows in out (coalesced reads, many blocks);
+// returns the number of rows written. The finishing kernels (and the host reads) then sum those.
+int launch_reduce_wide(const ef* partial, int nb, int k, ef* out, int max_blocks, cudaStream_t s);
 void launch_eqsc_round_finish(int npts, const ef* partial, int nb, const ef& r, const ef& rinv,
                               const FinishConsts& fc, DevRound* st, uint32_t* proof, ef* ch_out, cudaStream_t s);
 void launch_prod_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,

@@ -141,6 +141,7 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   uint64_t thr = UINT64_MAX;
   WL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
   WL_CUDA(cudaMalloc(&twiddles, sizeof(uint2) * TWIDDLE_ENTRIES));
+  WL_CUDA(cudaMalloc(&part2, sizeof(ef) * kWideBlocks * 32));
   launch_twiddles(twiddles, stream);
   pinned_bytes = kUpBytes + kDownBytes;
   WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
@@ -157,6 +158,7 @@ Context::~Context() {
   if (block_event) cudaEventDestroy(block_event);
   cudaFree(twiddles);
   if (part_buf) cudaFree(part_buf);
+  if (part2) cudaFree(part2);
   cudaFreeHost(pinned);
   cudaStreamSynchronize(copy_stream);
   cudaStreamDestroy(copy_stream);
@@ -244,6 +246,14 @@ void Context::wait_stream() {
   host_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
   if (hclk.on) hclk.last_wait_end = host_now_ms();
 }
+const ef* Context::reduce_wide(const ef* partial, int& nb, int k) {
+  if (nb <= 2 * kWideBlocks || k > 32) return partial;
+  {
+    ProfScope _ps(*this, "reduce");
+    nb = launch_reduce_wide(partial, nb, k, part2, kWideBlocks, stream);
+  }
+  return part2;
+}
 ef* Context::partials(size_t n) {
   if (n > part_cap) {
     if (part_buf) WL_CUDA(cudaFreeAsync(part_buf, stream));
@@ -328,6 +338,7 @@ std::vector<ef> reduce_to_host(Context& ctx, const ef* partial, int nblk, int k)
   if (sizeof(ef) * size_t(k) > kDownBytes) throw std::invalid_argument("reduce_to_host: too many sums");
   char* down = static_cast<char*>(ctx.pinned) + kUpBytes;
   ef* down_dev = reinterpret_cast<ef*>(static_cast<char*>(ctx.pinned_dev) + kUpBytes);
+  partial = ctx.reduce_wide(partial, nblk, k);
   { ProfScope _ps(ctx, "reduce"); launch_reduce_partials(partial, nblk, k, down_dev, ctx.stream); }
   ctx.wait_stream();
   g_up_off = 0;  // every earlier upload has completed
@@ -698,7 +709,9 @@ void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, e
       const int nb = whir_sc_blocks(half);
       ef* part = ctx.partials(size_t(3) * nb);
       { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream); }
-      { ProfScope _ps(ctx, "round_finish"); launch_whir_round_finish(part, nb, fc, ph.st, ph.words, ph.chs, ctx.stream); }
+      int nr = nb;
+      const ef* red = ctx.reduce_wide(part, nr, 3);
+      { ProfScope _ps(ctx, "round_finish"); launch_whir_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, ctx.stream); }
       DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
       { ProfScope _ps(ctx, "fold"); launch_fold2_dev(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, ph.chs + t, ctx.stream); }
       g = std::move(ng);
@@ -950,7 +963,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       ef* part = ctx.partials(size_t(nb) * 3);
       { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
       const ef& r = zc[round];
-      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(4, part, nb, r, kb::ef_inv(r), fc, ph.st, ph.words, ph.chs, st); }
+      int nr = nb;
+      const ef* red = ctx.reduce_wide(part, nr, 3);
+      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(4, red, nr, r, kb::ef_inv(r), fc, ph.st, ph.words, ph.chs, st); }
       DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
       DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
       { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), W + 1, half, ph.chs + (round - 1), st,
@@ -1061,7 +1076,9 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
       const int nb = prod_blocks(half);
       ef* part = ctx.partials(size_t(nb) * 2);
       { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st); }
-      { ProfScope _ps(ctx, "round_finish"); launch_prod_round_finish(part, nb, fc, ph.st, ph.words, ph.chs, st); }
+      int nr = nb;
+      const ef* red = ctx.reduce_wide(part, nr, 2);
+      { ProfScope _ps(ctx, "round_finish"); launch_prod_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, st); }
       DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
       { ProfScope _ps(ctx, "fold"); launch_fold2_dev(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, ph.chs + round, st); }
       A = std::move(na);
@@ -1339,7 +1356,9 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
       ef* part = ctx.partials(size_t(nb) * 2);
       { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st); }
       const ef& rr = r[round];
-      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(3, part, nb, rr, kb::ef_inv(rr), fc, ph.st, ph.words, ph.chs, st); }
+      int nr = nb;
+      const ef* red = ctx.reduce_wide(part, nr, 2);
+      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(3, red, nr, rr, kb::ef_inv(rr), fc, ph.st, ph.words, ph.chs, st); }
       DBuf nc(sizeof(ef) * 3 * half, st);
       DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
       { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 3, half, ph.chs + (round - 1), st,

@@ -49,6 +49,12 @@ struct Context {
   void* part_buf = nullptr;
   size_t part_cap = 0;
   ef* partials(size_t n);
+  // Second-level partial sums (launch_reduce_wide's output), fixed capacity.
+  static constexpr int kWideBlocks = 512;
+  ef* part2 = nullptr;
+  // Reduces nb interleaved rows of k partial sums to a few rows in part2 when nb is large
+  // (returns part2 and sets nb to its row count), else returns partial unchanged.
+  const ef* reduce_wide(const ef* partial, int& nb, int k);
   std::string last_error;
   uint64_t host_syncs = 0;  // stream synchronisations made by the host (diagnostics)
   double host_wait_ms = 0;  // time the host spent in them
