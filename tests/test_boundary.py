@@ -59,9 +59,9 @@ def test_tuner_interface_without_device(wl):
     """The autotuner's process-wide controls work without a GPU: families by name, plans in
     range, an empty report before any proof."""
     rep = wl.tune_report()
-    assert set(rep) == {"lde", "leaf", "merkle"}
+    assert set(rep) == {"lde", "leaf", "merkle", "inner"}
     wl.tune_force("lde", 5)
     wl.tune_force("lde", -1)
-    for fam, plan in (("lde", 6), ("leaf", 3), ("nope", 0)):
+    for fam, plan in (("lde", 6), ("leaf", 3), ("inner", 2), ("nope", 0)):
         with pytest.raises(wl.ProverError):
             wl.tune_force(fam, plan)

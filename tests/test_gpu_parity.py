@@ -171,11 +171,11 @@ def test_sumcheck_abc_large_matches_oracle(oracle, wl, ctx, log_n, skips):
 
 
 @pytest.mark.parametrize("family,plan", [("lde", p) for p in range(6)] + [("leaf", p) for p in range(3)] +
-                         [("merkle", p) for p in range(3)])
+                         [("merkle", p) for p in range(3)] + [("inner", p) for p in range(2)])
 def test_every_tuned_plan_matches_oracle(oracle, wl, ctx, family, plan):
-    """Every launch plan the autotuner can pick writes the same commitment: a proof with the
-    plan forced equals the oracle's (2^13 rows: three NTT passes, 2^15 leaves so that the
-    Merkle schedules differ)."""
+    """Every launch plan the autotuner can pick gives the same proof: with the plan forced the
+    proof equals the oracle's (2^13 rows: three NTT passes, 2^15 leaves so that the Merkle
+    schedules differ, 2^5-row inner-sum segments for both stagings)."""
     log_n = 13
     consts, inputs = oracle.workload(log_n)
     wit = oracle.trace(log_n, consts, inputs)
@@ -209,7 +209,7 @@ def test_autotuner_keeps_a_plan_per_shape(oracle, wl):
         p2 = table.prove_witness(w)
         w.free()
     assert np.array_equal(p1, ref) and np.array_equal(p2, ref)
-    for fam, n in (("lde", 6), ("leaf", 3), ("merkle", 3)):
+    for fam, n in (("lde", 6), ("leaf", 3), ("merkle", 3), ("inner", 2)):
         assert rep[fam], fam
         for e in rep[fam]:
             assert len(e["ms"]) == n and 0 <= e["plan"] < n

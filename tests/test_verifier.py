@@ -186,10 +186,10 @@ def test_verify_batch_device_matches_host(oracle, wl, ctx):
     proofs of several sizes are accepted; a corrupted opened row, path digest or commitment
     root is an opening error (11 for a root the commitment phase already reads), and a corrupted
     sumcheck word fails before the openings with the host's outcome."""
-    consts, _ = oracle.workload(2)
+    consts, _ = oracle.workload(2, 1)  # with an input seed the constants do not depend on log_n
     jobs = []
     for log_n in (6, 8, 9):
-        c, inputs = oracle.workload(log_n)
+        c, inputs = oracle.workload(log_n, 10 + log_n)
         assert np.array_equal(c, consts)
         jobs.append((log_n, oracle.prove(log_n, consts, oracle.trace(log_n, consts, inputs))[0]))
     dump_n, dump_p = jobs[1]

@@ -1117,6 +1117,167 @@ __global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_mma(const uint32_
   }
 }
 
+// The same inner sums with the tile staged by the bulk-copy (TMA) engine: one thread issues,
+// per chunk, one cp.async.bulk of 128 bytes for each of the 16 segments, completing on the
+// chunk's mbarrier (expected bytes set by the same thread); all threads wait on the mbarrier's
+// phase before reading the chunk. ISB_STAGES chunks are in flight. Every wait is bounded: a
+// wait that runs out counts a pipeline timeout (the host checks the counter after the inner
+// sums and fails the proof) and the kernel stops consuming. Rows past M copy segment m0's data
+// (their results are never stored). The B fragments of the next chunk are loaded from L2
+// while the current chunk is multiplied.
+constexpr int ISB_STAGES = 6;
+constexpr uint32_t PIPE_WAIT_LIMIT = 1u << 20;  // try_wait rounds (each a bounded hardware wait)
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < PIPE_WAIT_LIMIT; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(ISM_WARPS * 32) k_inner_sums_bulk(const uint32_t* __restrict__ wit, int log_n, int k,
+                                                                   int ll, const ef* __restrict__ eq_hi,
+                                                                   const ef* __restrict__ eq_lo,
+                                                                   const uint8_t* __restrict__ limbs,
+                                                                   ef* __restrict__ pu, ef* __restrict__ pd,
+                                                                   unsigned* __restrict__ timeouts) {
+  __shared__ int cs[4][4][16][17];  // [a][b][row][col], padded
+  __shared__ ef up_s[16], dn_s[16];
+  __shared__ __align__(128) uint32_t isb_a[ISB_STAGES][16][ISM_ROW];
+  __shared__ __align__(8) uint64_t bars[ISB_STAGES];
+  __shared__ int stop;
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  const uint32_t nsk = 1u << k, nhi = 1u << (log_n - k - ll), nlo = 1u << ll;
+  const uint32_t M = uint32_t(AIR_W) * nsk * nhi;
+  const uint32_t m0 = blockIdx.x * 16;
+  const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  auto row_base = [&](uint32_t m) -> size_t {
+    const uint32_t xh = m % nhi, cj = m / nhi, j = cj % nsk, c = cj / nsk;
+    return size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+  };
+  const uint32_t nch = nlo >> 5;
+  const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&bars[0]);
+  const unsigned dst0 = (unsigned)__cvta_generic_to_shared(&isb_a[0][0][0]);
+  if (threadIdx.x == 0) {
+    stop = 0;
+    for (int st = 0; st < ISB_STAGES; st++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8 * st));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  // issued by thread 0 only: chunk c into slot c % ISB_STAGES
+  auto issue = [&](uint32_t c) {
+    if (c >= nch) return;
+    const uint32_t slot = c % ISB_STAGES;
+    const unsigned bar = bar0 + 8 * slot;
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of the slot come first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(16u * 128u) : "memory");
+    for (int row = 0; row < 16; row++) {
+      const uint32_t m = m0 + row < M ? m0 + row : m0;
+      const uint32_t* src = wit + row_base(m) + 32 * size_t(c);
+      const unsigned dst = dst0 + ((slot * 16 + row) * ISM_ROW) * 4;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];\n" ::"r"(dst),
+          "l"(src), "r"(bar)
+          : "memory");
+    }
+  };
+  if (threadIdx.x == 0)
+    for (int c = 0; c < ISB_STAGES - 1; c++) issue(c);
+  int acc[4][2][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[a][nt][q] = 0;
+  const uint32_t* lb = reinterpret_cast<const uint32_t*>(limbs + size_t(b) * 16 * nlo);
+  const uint32_t lstride = nlo >> 2;
+  uint32_t bf[2][2], bfn[2][2];
+  auto load_b = [&](uint32_t c, uint32_t (&f)[2][2]) {
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+      const uint32_t* col = lb + size_t(nt * 8 + g) * lstride + (c << 3) + t;
+      f[nt][0] = __ldg(col);
+      f[nt][1] = __ldg(col + 4);
+    }
+  };
+  load_b(0, bf);
+  uint32_t consumed = 0;
+#pragma unroll 1
+  for (uint32_t c = 0; c < nch; c++) {
+    if (!mbar_wait_bounded(bar0 + 8 * (c % ISB_STAGES), (c / ISB_STAGES) & 1)) {
+      atomicAdd(timeouts, 1u);
+      stop = 1;
+    }
+    __syncthreads();  // chunk c landed; every thread is done with the slot of chunk c - 1
+    if (stop) break;
+    if (threadIdx.x == 0) issue(c + ISB_STAGES - 1);
+    if (c + 1 < nch) load_b(c + 1, bfn);
+    const uint32_t(&X)[16][ISM_ROW] = isb_a[c % ISB_STAGES];
+    const uint4 q0 = *reinterpret_cast<const uint4*>(&X[g][4 * t]);
+    const uint4 q1 = *reinterpret_cast<const uint4*>(&X[g + 8][4 * t]);
+    const uint4 q2 = *reinterpret_cast<const uint4*>(&X[g][16 + 4 * t]);
+    const uint4 q3 = *reinterpret_cast<const uint4*>(&X[g + 8][16 + 4 * t]);
+    uint32_t l0[4], l1[4], l2[4], l3[4];
+    byte_transpose4(q0, l0);
+    byte_transpose4(q1, l1);
+    byte_transpose4(q2, l2);
+    byte_transpose4(q3, l3);
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const uint32_t af[4] = {l0[a], l1[a], l2[a], l3[a]};
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++) mma_u8_16832(acc[a][nt], af, bf[nt][0], bf[nt][1]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) bf[nt][0] = bfn[nt][0], bf[nt][1] = bfn[nt][1];
+    consumed = c + 1;
+  }
+  if (consumed < nch) {
+    // a wait ran out: let the copies already issued land (bounded) before the block exits
+    const uint32_t issued = min(nch, consumed + ISB_STAGES - 1);
+    for (uint32_t c = consumed; c < issued; c++) mbar_wait_bounded(bar0 + 8 * (c % ISB_STAGES), (c / ISB_STAGES) & 1);
+    return;
+  }
+  limb_store<2>(cs, acc, b, g, t);
+  __syncthreads();
+  for (int e = threadIdx.x; e < 256; e += ISM_WARPS * 32) {
+    const int row = e >> 4, col = e & 15;
+    const uint32_t r = limb_recombine(cs, row, col);
+    if (col < 8) up_s[row].c[col] = r;
+    else dn_s[row].c[col - 8] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    const uint32_t m = m0 + threadIdx.x;
+    if (m < M) {
+      const uint32_t xh = m % nhi, cj = m / nhi, j = cj % nsk, c = cj / nsk;
+      const size_t base = size_t(c) * N + size_t(j) * S + (size_t(xh) << ll);
+      const uint32_t* col = wit + size_t(c) * N;
+      const bool last = j == nsk - 1 && xh == nhi - 1;  // the segment holding row N - 1
+      const ef el = eq_lo[nlo - 1];
+      ef up = up_s[threadIdx.x], dn = dn_s[threadIdx.x];
+      if (last) {
+        up = ef_add(up, ef_mul_f(el, kb::sub(col[N - 2], col[N - 1])));
+        dn = ef_add(dn, ef_mul_f(el, col[N - 1]));
+      } else {
+        dn = ef_add(dn, ef_mul_f(el, wit[base + nlo]));
+      }
+      const ef h = eq_hi[xh];
+      pu[m] = ef_mul(up, h);
+      pd[m] = ef_mul(dn, h);
+    }
+  }
+}
+
 // WHIR partial evaluation on the tensor cores: rows m = (u, v_hi) are the segments
 // T[m 2^ll .. m 2^ll + 2^ll) of the packed table (zero past t_len), B the 8 coefficients of
 // lo (limbs[(b * 8 + n) * nlo + x]). Each warp owns a 16-row tile (16 consecutive v_hi of one
@@ -1577,7 +1738,8 @@ void launch_fold_cols_dev(const ef* in, ef* out, int ncols, size_t half, const e
   WL_LAUNCH_CHECK();
 }
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
-                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s) {
+                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s, int plan,
+                       unsigned* timeouts) {
   // out_up / out_down hold AIR_W results followed by AIR_W * 2^k * 2^(log_n - k - ll) partials.
   const int nsk = 1 << k;
   const int nh = 1 << (log_n - k - ll);
@@ -1588,7 +1750,11 @@ void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* 
     k_eq_limbs<<<(16 * nlo + 255) / 256, 256, 0, s>>>(eq_lo, nlo, limbs);
     WL_LAUNCH_CHECK();
     const uint32_t M = uint32_t(AIR_W) * nsk * nh;
-    k_inner_sums_mma<<<(M + 15) / 16, ISM_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi, eq_lo, limbs, pu, pd);
+    if (plan == 1 && timeouts)
+      k_inner_sums_bulk<<<(M + 15) / 16, ISM_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi, eq_lo, limbs, pu, pd,
+                                                                 timeouts);
+    else
+      k_inner_sums_mma<<<(M + 15) / 16, ISM_WARPS * 32, 0, s>>>(wit, log_n, k, ll, eq_hi, eq_lo, limbs, pu, pd);
   } else {
     k_inner_sums<<<dim3((AIR_W + 1) / 2, nsk, (nh + IS_WARPS - 1) / IS_WARPS), IS_WARPS * 32, 0, s>>>(
         wit, log_n, k, ll, eq_hi, eq_lo, pu, pd);

@@ -21,6 +21,27 @@ namespace {
 
 constexpr int FIN_THREADS = 384;  // up to three sums, 128 threads each
 
+// Poseidon2-16 in Montgomery form, the operations of kb::p2_permute<16> with every round
+// unrolled: one thread runs the transcript, so the permutation's latency is the cost, and with
+// constant indices the round constants are instruction operands instead of indexed loads.
+__device__ __forceinline__ void p16_unrolled(uint32_t* s, const kb::P16Consts& c) {
+  kb::mds_light<16>(s);
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) s[i] = kb::cube(kb::add(s[i], c.ext_init[r * 16 + i]));
+    kb::mds_light<16>(s);
+  }
+#pragma unroll
+  for (int r = 0; r < kb::P16Consts::RP; r++) kb::internal_layer_with0<16>(s, kb::cube(kb::add(s[0], c.internal[r])));
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) s[i] = kb::cube(kb::add(s[i], c.ext_term[r * 16 + i]));
+    kb::mds_light<16>(s);
+  }
+}
+
 // The permutation runs on a register copy of the state (the challenger itself, indexed by its
 // buffer lengths, lives in local memory).
 __device__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p) {
@@ -28,7 +49,7 @@ __device__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p) {
 #pragma unroll
   for (int i = 0; i < 16; i++) s[i] = (i < 8 && i < c.in_len) ? c.in[i] : c.state[i];
   c.in_len = 0;
-  kb::p2_permute<16>(s, p);
+  p16_unrolled(s, p);
 #pragma unroll
   for (int i = 0; i < 16; i++) c.state[i] = s[i];
 #pragma unroll
@@ -64,8 +85,15 @@ __device__ ef dts_sample_ext(DevRound& st, const kb::P16Consts& p) {
 __device__ void reduce_sums(const ef* __restrict__ partial, int nb, int nsum, ef* red, ef* scratch) {
   const int z = threadIdx.x >> 7, t = threadIdx.x & 127;
   ef acc = kb::ef_zero();
-  if (z < nsum)
-    for (int b = t; b < nb; b += 128) acc = kb::ef_add(acc, partial[size_t(b) * nsum + z]);
+  if (z < nsum) {
+    int b = t;
+    for (; b + 384 < nb; b += 512) {  // four loads in flight
+      const ef v0 = partial[size_t(b) * nsum + z], v1 = partial[size_t(b + 128) * nsum + z];
+      const ef v2 = partial[size_t(b + 256) * nsum + z], v3 = partial[size_t(b + 384) * nsum + z];
+      acc = kb::ef_add(acc, kb::ef_add(kb::ef_add(v0, v1), kb::ef_add(v2, v3)));
+    }
+    for (; b < nb; b += 128) acc = kb::ef_add(acc, partial[size_t(b) * nsum + z]);
+  }
   acc = warp_reduce_ef(acc);
   if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = acc;
   __syncthreads();

@@ -124,8 +124,13 @@ void launch_fold_cols_dev(const ef* in, ef* out, int ncols, size_t half, const e
 // With limbs (64 * 2^ll bytes of scratch) and ll >= INNER_MMA_MIN_LL, the segment sums run
 // as byte-limb integer matrix products on the tensor cores.
 constexpr int INNER_MMA_MIN_LL = 5;
+// plan 0 stages the witness tiles with cp.async per thread, plan 1 with bulk copies (the TMA
+// engine) completing on mbarriers; plan 1 needs `timeouts`, a device counter of pipeline waits
+// that ran out (each wait is bounded; the caller fails the proof when it is not zero).
+constexpr int INNER_PLANS = 2;
 void launch_inner_sums(const uint32_t* wit, int log_n, int k, int ll, const ef* eq_hi, const ef* eq_lo,
-                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s);
+                       const ef* sel, ef* out_up, ef* out_down, uint8_t* limbs, cudaStream_t s, int plan = 0,
+                       unsigned* timeouts = nullptr);
 
 // --------------------------------------------------------------- inner phase
 void launch_batch_cols(const uint32_t* wit, int log_n, const ef* eqc, ef* out, cudaStream_t s);

@@ -142,6 +142,8 @@ Context::Context(int dev, uint64_t budget) : device(dev), hbm_budget(budget) {
   WL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
   WL_CUDA(cudaMalloc(&twiddles, sizeof(uint2) * TWIDDLE_ENTRIES));
   WL_CUDA(cudaMalloc(&part2, sizeof(ef) * kWideBlocks * 32));
+  WL_CUDA(cudaMalloc(&pipe_timeouts, sizeof(unsigned)));
+  WL_CUDA(cudaMemsetAsync(pipe_timeouts, 0, sizeof(unsigned), stream));
   launch_twiddles(twiddles, stream);
   pinned_bytes = kUpBytes + kDownBytes;
   WL_CUDA(cudaMallocHost(&pinned, pinned_bytes));
@@ -159,6 +161,7 @@ Context::~Context() {
   cudaFree(twiddles);
   if (part_buf) cudaFree(part_buf);
   if (part2) cudaFree(part2);
+  if (pipe_timeouts) cudaFree(pipe_timeouts);
   cudaFreeHost(pinned);
   cudaStreamSynchronize(copy_stream);
   cudaStreamDestroy(copy_stream);
@@ -1017,8 +1020,17 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
     const size_t plen = size_t(W) * (1 + (size_t(nsk) << lh_t));
     DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
     DBuf limbs(size_t(64) << ll_t, st);
-    { ProfScope _ps(ctx, "inner_sums"); launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(), limbs.as<uint8_t>(), st); }
-    ctx.to_host_many({{inner_up.data(), up.as<ef>(), sizeof(ef) * W}, {inner_down.data(), down.as<ef>(), sizeof(ef) * W}});
+    {
+      ProfScope _ps(ctx, "inner_sums");
+      tuned(ctx, TUNE_INNER, uint64_t(n) | uint64_t(k) << 8, [&](int plan) {
+        launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(),
+                          limbs.as<uint8_t>(), st, plan, ctx.pipe_timeouts);
+      });
+    }
+    unsigned timeouts = 0;
+    ctx.to_host_many({{inner_up.data(), up.as<ef>(), sizeof(ef) * W}, {inner_down.data(), down.as<ef>(), sizeof(ef) * W},
+                      {&timeouts, ctx.pipe_timeouts, sizeof(unsigned)}});
+    if (timeouts) throw std::runtime_error("inner sums: a bounded pipeline wait ran out on the device");
   }
   cols.reset();
   const double t2 = now_ms();

@@ -51,6 +51,9 @@ struct Context {
   ef* partials(size_t n);
   // Second-level partial sums (launch_reduce_wide's output), fixed capacity.
   static constexpr int kWideBlocks = 512;
+  // Device counter of bounded pipeline waits that ran out (kernels with mbarrier pipelines);
+  // zero on a healthy device, checked after each such kernel's results are read.
+  unsigned* pipe_timeouts = nullptr;
   ef* part2 = nullptr;
   // Reduces nb interleaved rows of k partial sums to a few rows in part2 when nb is large
   // (returns part2 and sets nb to its row count), else returns partial unchanged.

@@ -14,10 +14,10 @@ struct Entry {
 };
 std::mutex g_mu;
 std::map<std::tuple<int, int, uint64_t>, Entry> g_table;
-int g_forced[TUNE_FAMILIES] = {-1, -1, -1};
-const char* const kNames[TUNE_FAMILIES] = {"lde", "leaf", "merkle"};
-const int kPlans[TUNE_FAMILIES] = {6, 3, 3};
-const int kDefaults[TUNE_FAMILIES] = {2, 1, 1};
+int g_forced[TUNE_FAMILIES] = {-1, -1, -1, -1};
+const char* const kNames[TUNE_FAMILIES] = {"lde", "leaf", "merkle", "inner"};
+const int kPlans[TUNE_FAMILIES] = {6, 3, 3, 2};
+const int kDefaults[TUNE_FAMILIES] = {2, 1, 1, 0};
 }  // namespace
 
 const char* tune_family_name(int f) { return f >= 0 && f < TUNE_FAMILIES ? kNames[f] : "?"; }

@@ -1,7 +1,9 @@
 // Autotuner of kernel launch plans. Several kernels of the commitment have launch plans that
 // compute the same result with different shapes: the LDE's split of its stages into passes and
 // the persistent passes' blocks per SM, the leaf sponges' rows per block, and the width from
-// which a Merkle level runs one compression per thread. Which plan is fastest depends on the
+// which a Merkle level runs one compression per thread; and the inner sums' staging of the
+// witness (cp.async per thread, or bulk copies by the TMA engine on an mbarrier pipeline).
+// Which plan is fastest depends on the
 // table's shape (rows, columns, element size). The first time a tuning context meets a shape it
 // runs every plan on the real data (each writes the same output), times them with CUDA events
 // and keeps the fastest for that device and shape; later proofs of the shape, on any context
@@ -13,12 +15,12 @@
 
 namespace wl {
 
-enum TuneFamily { TUNE_LDE = 0, TUNE_LEAF = 1, TUNE_MERKLE = 2, TUNE_FAMILIES = 3 };
+enum TuneFamily { TUNE_LDE = 0, TUNE_LEAF = 1, TUNE_MERKLE = 2, TUNE_INNER = 3, TUNE_FAMILIES = 4 };
 
 const char* tune_family_name(int family);
 int tune_plan_count(int family);
 int tune_default_plan(int family);
-// Family by name ("lde", "leaf", "merkle"), -1 if unknown.
+// Family by name ("lde", "leaf", "merkle", "inner"), -1 if unknown.
 int tune_family_from_name(const char* name);
 // A plan forced for every shape of a family (-1: none), process-wide; for tests and sweeps.
 void tune_force(int family, int plan);
