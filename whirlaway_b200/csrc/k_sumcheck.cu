@@ -1575,9 +1575,63 @@ __global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, 
 
 
 // ------------------------------------------------------------------ a*b - c
-constexpr int ABC_X = 32;
 
-__global__ void k_abc0_eval(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+// Round 0 of the a*b - c zerocheck: for every point z of the skipped variables' extension and
+// every x, v_z(x) = A_z(x) B_z(x) - C_z(x) with A_z(x) = sum_j L_j(z) a[j S + x] (and B, C the
+// same), weighted by eq(x). Grid-stride over x, one thread per x at a time, all nz points per
+// thread: each value is read once (a, b, c and eq(x) coalesced), the points' products stay in
+// registers, and each thread keeps nz extension accumulators that one block reduction sums at
+// the end (one partial per block and point).
+constexpr int ABC_X = 32;
+constexpr int ABC0_THREADS = 256;
+constexpr int ABC0_MAX_Z = 7;  // 2 (2^k - 1) - 2^k + 1 points for k <= 3
+__global__ void __launch_bounds__(ABC0_THREADS, 2) k_abc0_eval(const uint32_t* __restrict__ a,
+                                                           const uint32_t* __restrict__ b,
+                                                           const uint32_t* __restrict__ c, int log_n, int k, int nz,
+                                                           const uint32_t* __restrict__ lw,
+                                                           const ef* __restrict__ eq, ef* __restrict__ partial) {
+  __shared__ uint32_t w_s[ABC0_MAX_Z * 8];
+  __shared__ ef scratch[32];
+  const int nsk = 1 << k;
+  for (int i = threadIdx.x; i < nz * nsk; i += blockDim.x) w_s[i] = lw[i];
+  __syncthreads();
+  const size_t N = size_t(1) << log_n, S = N >> k;
+  ef acc[ABC0_MAX_Z];
+#pragma unroll
+  for (int z = 0; z < ABC0_MAX_Z; z++) acc[z] = ef_zero();
+  for (size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < S; x += size_t(gridDim.x) * blockDim.x) {
+    uint32_t va[8], vb[8], vc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      if (j < nsk) va[j] = a[size_t(j) * S + x], vb[j] = b[size_t(j) * S + x], vc[j] = c[size_t(j) * S + x];
+    const ef e = eq[x];
+#pragma unroll
+    for (int z = 0; z < ABC0_MAX_Z; z++) {
+      if (z >= nz) break;
+      const uint32_t* wz = w_s + z * nsk;
+      uint64_t sa = 0, sb = 0, sc = 0, ta = 0, tb = 0, tc = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (j >= nsk) break;
+        if (j < 4) sa += wmul(wz[j], va[j]), sb += wmul(wz[j], vb[j]), sc += wmul(wz[j], vc[j]);
+        else ta += wmul(wz[j], va[j]), tb += wmul(wz[j], vb[j]), tc += wmul(wz[j], vc[j]);
+      }
+      const uint32_t A = add(redc(sa), redc(ta)), B = add(redc(sb), redc(tb)), C = add(redc(sc), redc(tc));
+      acc[z] = ef_add(acc[z], ef_mul_f(e, sub(mul(A, B), C)));
+    }
+  }
+#pragma unroll
+  for (int z = 0; z < ABC0_MAX_Z; z++) {
+    if (z >= nz) break;
+    const ef t = block_reduce_ef(acc[z], scratch);
+    if (threadIdx.x == 0) partial[size_t(blockIdx.x) * nz + z] = t;
+    __syncthreads();  // scratch is reused by the next point
+  }
+}
+
+// One thread per (x, point) with the block spanning the points: the form for 4 skipped
+// variables (15 points, too many to keep per thread).
+__global__ void k_abc0_eval_points(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                             const uint32_t* __restrict__ c, int log_n, int k, int nz, const uint32_t* __restrict__ lw,
                             const ef* __restrict__ eq, ef* __restrict__ partial) {
   __shared__ uint32_t w_s[32 * 16];
@@ -1834,13 +1888,22 @@ void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, con
 }
 
 int abc0_blocks(int log_n, int k) {
-  size_t S = size_t(1) << (log_n - k);
-  return (int)((S + ABC_X - 1) / ABC_X);
+  const size_t S = size_t(1) << (log_n - k);
+  if (k > 3) return (int)((S + ABC_X - 1) / ABC_X);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::max<size_t>(1, std::min<size_t>((S + ABC0_THREADS - 1) / ABC0_THREADS, size_t(sms) * 2));
 }
 void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
                       const uint32_t* lw, const ef* eq, ef* partial, cudaStream_t s) {
-  if (nz > 32 || k > 4) throw std::runtime_error("abc round 0: too many points");
-  k_abc0_eval<<<abc0_blocks(log_n, k), dim3(ABC_X, nz), 0, s>>>(a, b, c, log_n, k, nz, lw, eq, partial);
+  if (k > 3) {
+    if (nz > 32 || k > 4) throw std::runtime_error("abc round 0: too many points");
+    k_abc0_eval_points<<<abc0_blocks(log_n, k), dim3(ABC_X, nz), 0, s>>>(a, b, c, log_n, k, nz, lw, eq, partial);
+  } else {
+    if (nz > ABC0_MAX_Z) throw std::runtime_error("abc round 0: too many points");
+    k_abc0_eval<<<abc0_blocks(log_n, k), ABC0_THREADS, 0, s>>>(a, b, c, log_n, k, nz, lw, eq, partial);
+  }
   WL_LAUNCH_CHECK();
 }
 void launch_abc0_fold(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, const ef* sel,
