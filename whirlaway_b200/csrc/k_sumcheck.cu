@@ -1574,6 +1574,84 @@ __global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, 
 }
 
 
+// ------------------------------------------------------------------ fold fused with the next round
+// The fold of the previous round at its challenge (lo + r (hi - lo), the challenge read from
+// device memory where the round-finishing kernel left it) fused with this round's sums, so
+// every table is read once per round: thread x of this round (x < h, the tables' new length
+// being 2h) reads old entries x, x + h, x + 2h, x + 3h, writes the two folded entries x and
+// x + h, and accumulates the round polynomial's values. Grid-stride; one partial per block.
+constexpr int FE_THREADS = 256;
+__device__ __forceinline__ ef fe_lerp(const ef* t, size_t i, size_t L, const ef& r) {
+  const ef lo = t[i];
+  return ef_add(lo, ef_mul(r, ef_sub(t[i + L], lo)));
+}
+// Product sumcheck (NS = 2: values at 0 and 2; the inner sumcheck) and WHIR folding sumcheck
+// (NS = 3: values at 0, 1, 2) on the pair of tables (a, b).
+template <int NS>
+__global__ void __launch_bounds__(FE_THREADS) k_pair_fold_eval(const ef* __restrict__ a, const ef* __restrict__ b,
+                                                               const ef* __restrict__ rptr, ef* __restrict__ na,
+                                                               ef* __restrict__ nb, size_t h,
+                                                               ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  const ef r = *rptr;
+  const size_t L = 2 * h;
+  ef s0 = ef_zero(), s1 = ef_zero(), s2 = ef_zero();
+  for (size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < h; x += size_t(gridDim.x) * blockDim.x) {
+    const ef al = fe_lerp(a, x, L, r), ah = fe_lerp(a, x + h, L, r);
+    const ef bl = fe_lerp(b, x, L, r), bh = fe_lerp(b, x + h, L, r);
+    na[x] = al;
+    na[x + h] = ah;
+    nb[x] = bl;
+    nb[x + h] = bh;
+    s0 = ef_add(s0, ef_mul(al, bl));
+    if (NS == 3) s1 = ef_add(s1, ef_mul(ah, bh));
+    s2 = ef_add(s2, ef_mul(ef_sub(ef_add(ah, ah), al), ef_sub(ef_add(bh, bh), bl)));
+  }
+  s0 = block_reduce_ef(s0, scratch);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * NS] = s0;
+  __syncthreads();
+  if (NS == 3) {
+    s1 = block_reduce_ef(s1, scratch);
+    if (threadIdx.x == 0) partial[size_t(blockIdx.x) * NS + 1] = s1;
+    __syncthreads();
+  }
+  s2 = block_reduce_ef(s2, scratch);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * NS + NS - 1] = s2;
+}
+// The a*b - c zerocheck's rounds >= 2: three columns (column q of old length 4h at q 4h, of new
+// length 2h at q 2h) and the eq table (old length 2h, the leading variable summed out into the
+// new table of length h); values at z = 0 and 2 of (A B - C) eq.
+__global__ void __launch_bounds__(FE_THREADS) k_abc_fold_eval(const ef* __restrict__ cols, const ef* __restrict__ rptr,
+                                                              const ef* __restrict__ eq_prev, ef* __restrict__ nc,
+                                                              ef* __restrict__ eq_new, size_t h,
+                                                              ef* __restrict__ partial) {
+  __shared__ ef scratch[32];
+  const ef r = *rptr;
+  const size_t L = 2 * h;
+  ef s0 = ef_zero(), s2 = ef_zero();
+  for (size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < h; x += size_t(gridDim.x) * blockDim.x) {
+    ef lo[3], t[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const ef* col = cols + size_t(q) * 2 * L;
+      lo[q] = fe_lerp(col, x, L, r);
+      const ef hi = fe_lerp(col, x + h, L, r);
+      nc[size_t(q) * L + x] = lo[q];
+      nc[size_t(q) * L + x + h] = hi;
+      t[q] = ef_sub(ef_add(hi, hi), lo[q]);
+    }
+    const ef e = ef_add(eq_prev[x], eq_prev[x + h]);
+    eq_new[x] = e;
+    s0 = ef_add(s0, ef_mul(ef_sub(ef_mul(lo[0], lo[1]), lo[2]), e));
+    s2 = ef_add(s2, ef_mul(ef_sub(ef_mul(t[0], t[1]), t[2]), e));
+  }
+  s0 = block_reduce_ef(s0, scratch);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 2] = s0;
+  __syncthreads();
+  s2 = block_reduce_ef(s2, scratch);
+  if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 2 + 1] = s2;
+}
+
 // ------------------------------------------------------------------ a*b - c
 
 // Round 0 of the a*b - c zerocheck: for every point z of the skipped variables' extension and
@@ -1884,6 +1962,29 @@ void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, cons
 }
 void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r_dev, cudaStream_t s) {
   k_fold2_mma<<<dim3((unsigned)((half + 127) / 128), 2), 256, 0, s>>>(a, b, oa, ob, half, ef_zero(), r_dev);
+  WL_LAUNCH_CHECK();
+}
+
+int fold_eval_blocks(size_t h) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::max<size_t>(1, std::min<size_t>((h + FE_THREADS - 1) / FE_THREADS, size_t(sms) * 4));
+}
+void launch_pair_fold_eval(int nsums, const ef* a, const ef* b, const ef* r_dev, ef* na, ef* nb, size_t h,
+                           ef* partial, cudaStream_t s) {
+  const int g = fold_eval_blocks(h);
+  if (nsums == 2)
+    k_pair_fold_eval<2><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial);
+  else if (nsums == 3)
+    k_pair_fold_eval<3><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial);
+  else
+    throw std::invalid_argument("fold-evaluate: 2 or 3 sums");
+  WL_LAUNCH_CHECK();
+}
+void launch_abc_fold_eval(const ef* cols, const ef* r_dev, const ef* eq_prev, ef* nc, ef* eq_new, size_t h, ef* partial,
+                          cudaStream_t s) {
+  k_abc_fold_eval<<<fold_eval_blocks(h), FE_THREADS, 0, s>>>(cols, r_dev, eq_prev, nc, eq_new, h, partial);
   WL_LAUNCH_CHECK();
 }
 

@@ -144,6 +144,19 @@ void launch_prod_eval(const ef* a, const ef* b, size_t half, ef* partial, cudaSt
 void launch_fold2_at(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef& r, cudaStream_t s);
 void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, const ef* r_dev, cudaStream_t s);
 
+// --------------------------------------------------------------- fold fused with the next round
+// The previous round's fold at its device challenge r_dev fused with this round's sums (each
+// table read once per round). Pair form: tables a, b of length 4h fold into na, nb of length
+// 2h, and block partials of sum_x na_lo nb_lo (and na_hi nb_hi with 3 sums) and of
+// (2 na_hi - na_lo)(2 nb_hi - nb_lo) over x < h go to partial[blk * nsums + z]. The a*b - c
+// form folds three columns (4h -> 2h) and the eq table (2h -> h: the leading variable summed
+// out) and sums (A B - C) eq at z = 0 and 2. fold_eval_blocks(h) partial rows.
+int fold_eval_blocks(size_t h);
+void launch_pair_fold_eval(int nsums, const ef* a, const ef* b, const ef* r_dev, ef* na, ef* nb, size_t h,
+                           ef* partial, cudaStream_t s);
+void launch_abc_fold_eval(const ef* cols, const ef* r_dev, const ef* eq_prev, ef* nc, ef* eq_new, size_t h, ef* partial,
+                          cudaStream_t s);
+
 // --------------------------------------------------------------- a*b - c zerocheck
 void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
                       const uint32_t* lw, const ef* eq, ef* partial, cudaStream_t s);

@@ -707,19 +707,40 @@ void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, e
   if (pow_bits == 0 && rounds > 0) {
     const FinishConsts fc = finish_consts(p16);
     DevPhase ph(ctx, ts, rounds, 24, sigma, kb::ef_one());
+    // round 0 evaluates the tables as they are; round t >= 1 folds at challenge t - 1 and
+    // evaluates in one pass; the last challenge's fold closes the block
     for (int t = 0; t < rounds; t++) {
-      const size_t half = size_t(1) << (m - 1);
-      const int nb = whir_sc_blocks(half);
-      ef* part = ctx.partials(size_t(3) * nb);
-      { ProfScope _ps(ctx, "whir_sc_eval"); launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream); }
+      const size_t half = size_t(1) << (m - 1 - t);
+      int nb;
+      ef* part;
+      if (t == 0) {
+        nb = whir_sc_blocks(half);
+        part = ctx.partials(size_t(3) * nb);
+        ProfScope _ps(ctx, "whir_sc_eval");
+        launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream);
+      } else {
+        nb = fold_eval_blocks(half);
+        part = ctx.partials(size_t(3) * nb);
+        DBuf ng(sizeof(ef) * 2 * half, ctx.stream), nw(sizeof(ef) * 2 * half, ctx.stream);
+        {
+          ProfScope _ps(ctx, "fold_eval");
+          launch_pair_fold_eval(3, g.as<ef>(), w.as<ef>(), ph.chs + (t - 1), ng.as<ef>(), nw.as<ef>(), half, part,
+                                ctx.stream);
+        }
+        g = std::move(ng);
+        w = std::move(nw);
+      }
       int nr = nb;
       const ef* red = ctx.reduce_wide(part, nr, 3);
       { ProfScope _ps(ctx, "round_finish"); launch_whir_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, ctx.stream); }
+    }
+    {
+      const size_t half = size_t(1) << (m - rounds);
       DBuf ng(sizeof(ef) * half, ctx.stream), nw(sizeof(ef) * half, ctx.stream);
-      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, ph.chs + t, ctx.stream); }
+      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(g.as<ef>(), w.as<ef>(), ng.as<ef>(), nw.as<ef>(), half, ph.chs + (rounds - 1), ctx.stream); }
       g = std::move(ng);
       w = std::move(nw);
-      m--;
+      m -= rounds;
     }
     const std::vector<ef> r = ph.finish(&sigma, nullptr);
     rnd.insert(rnd.end(), r.begin(), r.end());
@@ -1083,16 +1104,36 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   if (inner_on_device) {
     const FinishConsts fc = finish_consts(job.p16);
     DevPhase ph(ctx, ts, n, 24, inner_sum, kb::ef_one());
+    // round 0 evaluates A and B as they are, round r >= 1 folds them at challenge r - 1 and
+    // evaluates in one pass; the last challenge's fold leaves the final values
     for (int round = 0; round < n; round++) {
       const size_t half = N >> (round + 1);
-      const int nb = prod_blocks(half);
-      ef* part = ctx.partials(size_t(nb) * 2);
-      { ProfScope _ps(ctx, "prod_eval"); launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st); }
+      int nb;
+      ef* part;
+      if (round == 0) {
+        nb = prod_blocks(half);
+        part = ctx.partials(size_t(nb) * 2);
+        ProfScope _ps(ctx, "prod_eval");
+        launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st);
+      } else {
+        nb = fold_eval_blocks(half);
+        part = ctx.partials(size_t(nb) * 2);
+        DBuf na(sizeof(ef) * 2 * half, st), nbuf(sizeof(ef) * 2 * half, st);
+        {
+          ProfScope _ps(ctx, "fold_eval");
+          launch_pair_fold_eval(2, A.as<ef>(), B.as<ef>(), ph.chs + (round - 1), na.as<ef>(), nbuf.as<ef>(), half, part,
+                                st);
+        }
+        A = std::move(na);
+        B = std::move(nbuf);
+      }
       int nr = nb;
       const ef* red = ctx.reduce_wide(part, nr, 2);
       { ProfScope _ps(ctx, "round_finish"); launch_prod_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, st); }
-      DBuf na(sizeof(ef) * half, st), nbuf(sizeof(ef) * half, st);
-      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), half, ph.chs + round, st); }
+    }
+    {
+      DBuf na(sizeof(ef), st), nbuf(sizeof(ef), st);
+      { ProfScope _ps(ctx, "fold"); launch_fold2_dev(A.as<ef>(), B.as<ef>(), na.as<ef>(), nbuf.as<ef>(), 1, ph.chs + (n - 1), st); }
       A = std::move(na);
       B = std::move(nbuf);
     }
@@ -1361,22 +1402,40 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     std::vector<cudaEvent_t> ev(n - k + 1);
     for (auto& e : ev) WL_CUDA(cudaEventCreate(&e));
     WL_CUDA(cudaEventRecord(ev[0], st));
+    // round 1 evaluates the round-0 fold as it is; round r >= 2 folds the columns (and sums the
+    // eq table's leading variable out) at challenge r - 1 and evaluates in one pass; the last
+    // challenge's fold leaves the three final values
     for (int round = 1; round <= n - k; round++) {
       const int m = n - k - round + 1;
       const size_t half = size_t(1) << (m - 1);
-      const int nb = (int)((half + 31) / 32);
-      ef* part = ctx.partials(size_t(nb) * 2);
-      { ProfScope _ps(ctx, "abc_eval_ef"); launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st); }
+      int nb;
+      ef* part;
+      if (round == 1) {
+        nb = (int)((half + 31) / 32);
+        part = ctx.partials(size_t(nb) * 2);
+        ProfScope _ps(ctx, "abc_eval_ef");
+        launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st);
+      } else {
+        nb = fold_eval_blocks(half);
+        part = ctx.partials(size_t(nb) * 2);
+        DBuf nc(sizeof(ef) * 3 * 2 * half, st), eqn(sizeof(ef) * half, st);
+        {
+          ProfScope _ps(ctx, "fold_eval");
+          launch_abc_fold_eval(cols.as<ef>(), ph.chs + (round - 2), eqr.as<ef>(), nc.as<ef>(), eqn.as<ef>(), half, part,
+                               st);
+        }
+        cols = std::move(nc);
+        eqr = std::move(eqn);
+      }
       const ef& rr = r[round];
       int nr = nb;
       const ef* red = ctx.reduce_wide(part, nr, 2);
       { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(3, red, nr, rr, kb::ef_inv(rr), fc, ph.st, ph.words, ph.chs, st); }
-      DBuf nc(sizeof(ef) * 3 * half, st);
-      DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-      { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 3, half, ph.chs + (round - 1), st,
-                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
-      cols = std::move(nc);
-      eqr = std::move(eqn);
+      if (round == n - k) {
+        DBuf nc(sizeof(ef) * 3, st);
+        { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 3, 1, ph.chs + (round - 1), st); }
+        cols = std::move(nc);
+      }
       WL_CUDA(cudaEventRecord(ev[round], st));
     }
     ph.finish(&sum, &mmf);
