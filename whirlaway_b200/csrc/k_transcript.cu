@@ -21,35 +21,54 @@ namespace {
 
 constexpr int FIN_THREADS = 384;  // up to three sums, 128 threads each
 
-// Poseidon2-16 in Montgomery form, the operations of kb::p2_permute<16> with every round
-// unrolled: one thread runs the transcript, so the permutation's latency is the cost, and with
-// constant indices the round constants are instruction operands instead of indexed loads.
-__device__ __forceinline__ void p16_unrolled(uint32_t* s, const kb::P16Consts& c) {
-  kb::mds_light<16>(s);
+// Poseidon2-16 in Montgomery form for one warp whose 32 lanes all hold the same state (the
+// transcript runs redundantly on every lane of warp 0, so every lane has every value). The
+// full rounds spread the state over 16 lanes (lane i, and its mirror i + 16, holds word i):
+// the S-boxes run side by side and the external layer is three in-chunk shuffles and two
+// cross-chunk shuffle sums. The partial rounds run on the whole state in every lane (only word
+// 0 takes the S-box, the other words' updates are independent of each other). The field values
+// are those of kb::p2_permute<16>: the same linear maps and S-box, evaluated in another order.
+__device__ __forceinline__ uint32_t m4_lanes(uint32_t a, int i) {
+  const int base = i & ~3;
+  const uint32_t b = __shfl_sync(0xffffffffu, a, base | ((i + 1) & 3), 16);
+  const uint32_t c = __shfl_sync(0xffffffffu, a, base | ((i + 2) & 3), 16);
+  const uint32_t d = __shfl_sync(0xffffffffu, a, base | ((i + 3) & 3), 16);
+  // row i of circ(2, 3, 1, 1) within the chunk: 2a + 3b + c + d
+  const uint32_t y = kb::add(kb::add(kb::add(a, b), kb::add(c, d)), kb::add(a, kb::dbl(b)));
+  uint32_t t = kb::add(y, __shfl_xor_sync(0xffffffffu, y, 4, 16));
+  t = kb::add(t, __shfl_xor_sync(0xffffffffu, t, 8, 16));
+  return kb::add(y, t);
+}
+__device__ __forceinline__ uint32_t lane_word(const uint32_t (&s)[16], int i) {
+  uint32_t v = s[0];
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
+  for (int j = 1; j < 16; j++) v = i == j ? s[j] : v;
+  return v;
+}
+__device__ __forceinline__ void p16_warp(uint32_t (&s)[16], const kb::P16Consts& c) {
+  const int i = threadIdx.x & 15;
+  uint32_t v = m4_lanes(lane_word(s, i), i);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, c.ext_init[r * 16 + i])), i);
 #pragma unroll
-    for (int i = 0; i < 16; i++) s[i] = kb::cube(kb::add(s[i], c.ext_init[r * 16 + i]));
-    kb::mds_light<16>(s);
-  }
-#pragma unroll
+  for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
+#pragma unroll 4
   for (int r = 0; r < kb::P16Consts::RP; r++) kb::internal_layer_with0<16>(s, kb::cube(kb::add(s[0], c.internal[r])));
+  v = lane_word(s, i);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, c.ext_term[r * 16 + i])), i);
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
-#pragma unroll
-    for (int i = 0; i < 16; i++) s[i] = kb::cube(kb::add(s[i], c.ext_term[r * 16 + i]));
-    kb::mds_light<16>(s);
-  }
+  for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
 }
 
 // The permutation runs on a register copy of the state (the challenger itself, indexed by its
-// buffer lengths, lives in local memory).
+// buffer lengths, lives in local memory). Every lane of the calling warp takes part.
 __device__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p) {
   uint32_t s[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) s[i] = (i < 8 && i < c.in_len) ? c.in[i] : c.state[i];
   c.in_len = 0;
-  p16_unrolled(s, p);
+  p16_warp(s, p);
 #pragma unroll
   for (int i = 0; i < 16; i++) c.state[i] = s[i];
 #pragma unroll
@@ -69,7 +88,8 @@ __device__ uint32_t dch_sample(DevChallenger& c, const kb::P16Consts& p) {
 __device__ void dts_add_ext(DevRound& st, uint32_t* proof, const ef& v, const kb::P16Consts& p) {
 #pragma unroll 1
   for (int i = 0; i < 8; i++) {
-    proof[st.proof_len++] = v.c[i];
+    if ((threadIdx.x & 31) == 0) proof[st.proof_len] = v.c[i];
+    st.proof_len++;
     dch_observe(st.ch, v.c[i], p);
   }
 }
@@ -117,14 +137,14 @@ __device__ ef poly_eval_dev(const ef* c, int n, const ef& x) {
 // e1 = (sum - e0 (1 - r)) / r. The round polynomial is the interpolation on 0..NPTS-1 times the
 // eq factor of the current variable, (1 - r) + (2r - 1) X: NPTS + 1 coefficients.
 template <int NPTS>
-__global__ void __launch_bounds__(FIN_THREADS) k_eqsc_round_finish(const ef* __restrict__ partial, int nb, ef r,
+__global__ void __launch_bounds__(FIN_THREADS, 1) k_eqsc_round_finish(const ef* __restrict__ partial, int nb, ef r,
                                                                    ef rinv, const __grid_constant__ FinishConsts fc,
                                                                    DevRound* __restrict__ stp,
                                                                    uint32_t* __restrict__ proof,
                                                                    ef* __restrict__ ch_out) {
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, NPTS - 1, red, scratch);
-  if (threadIdx.x) return;
+  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
   DevRound st = *stp;
   ef e[NPTS];
   e[0] = kb::ef_mul(red[0], st.mmf);
@@ -147,20 +167,23 @@ __global__ void __launch_bounds__(FIN_THREADS) k_eqsc_round_finish(const ef* __r
   const ef c = dts_sample_ext(st, fc.p16);
   st.sum = poly_eval_dev(p, NPTS + 1, c);
   st.mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(omr, kb::ef_sub(one, c)), kb::ef_mul(r, c)), st.mmf);
-  ch_out[st.round++] = c;
-  *stp = st;
+  if (threadIdx.x == 0) {
+    ch_out[st.round] = c;
+    st.round++;
+    *stp = st;
+  }
 }
 
 // Round of the product sumcheck (the inner sumcheck): sums at 0 and 2, the value at 1 from the
 // claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
-__global__ void __launch_bounds__(FIN_THREADS) k_prod_round_finish(const ef* __restrict__ partial, int nb,
+__global__ void __launch_bounds__(FIN_THREADS, 1) k_prod_round_finish(const ef* __restrict__ partial, int nb,
                                                                    const __grid_constant__ FinishConsts fc,
                                                                    DevRound* __restrict__ stp,
                                                                    uint32_t* __restrict__ proof,
                                                                    ef* __restrict__ ch_out) {
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, 2, red, scratch);
-  if (threadIdx.x) return;
+  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
   DevRound st = *stp;
   const ef y[3] = {red[0], kb::ef_sub(st.sum, red[0]), red[1]};
   ef p[3];
@@ -171,20 +194,23 @@ __global__ void __launch_bounds__(FIN_THREADS) k_prod_round_finish(const ef* __r
   for (int k = 0; k < 3; k++) dts_add_ext(st, proof, p[k], fc.p16);
   const ef c = dts_sample_ext(st, fc.p16);
   st.sum = poly_eval_dev(p, 3, c);
-  ch_out[st.round++] = c;
-  *stp = st;
+  if (threadIdx.x == 0) {
+    ch_out[st.round] = c;
+    st.round++;
+    *stp = st;
+  }
 }
 
 // Round of the WHIR folding sumcheck: the three values h(0), h(1), h(2) go to the proof as
 // they are; the next claim is h(r) by quadratic interpolation on 0, 1, 2.
-__global__ void __launch_bounds__(FIN_THREADS) k_whir_round_finish(const ef* __restrict__ partial, int nb,
+__global__ void __launch_bounds__(FIN_THREADS, 1) k_whir_round_finish(const ef* __restrict__ partial, int nb,
                                                                    const __grid_constant__ FinishConsts fc,
                                                                    DevRound* __restrict__ stp,
                                                                    uint32_t* __restrict__ proof,
                                                                    ef* __restrict__ ch_out) {
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, 3, red, scratch);
-  if (threadIdx.x) return;
+  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
   DevRound st = *stp;
   for (int k = 0; k < 3; k++) dts_add_ext(st, proof, red[k], fc.p16);
   const ef r = dts_sample_ext(st, fc.p16);
@@ -194,8 +220,11 @@ __global__ void __launch_bounds__(FIN_THREADS) k_whir_round_finish(const ef* __r
   const ef b = kb::ef_mul(kb::ef_mul(red[1], r), rm2);
   const ef c = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[2], r), rm1), fc.inv2);
   st.sum = kb::ef_add(kb::ef_sub(a, b), c);
-  ch_out[st.round++] = r;
-  *stp = st;
+  if (threadIdx.x == 0) {
+    ch_out[st.round] = r;
+    st.round++;
+    *stp = st;
+  }
 }
 
 // First level of the reduction of nb interleaved rows of k partial sums (partial[row * k + z]):
