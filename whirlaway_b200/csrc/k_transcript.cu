@@ -45,58 +45,77 @@ __device__ __forceinline__ uint32_t lane_word(const uint32_t (&s)[16], int i) {
   for (int j = 1; j < 16; j++) v = i == j ? s[j] : v;
   return v;
 }
-__device__ __forceinline__ void p16_warp(uint32_t (&s)[16], const kb::P16Consts& c) {
+// This lane's full-round constants (word i of each full round), loaded once per kernel: indexed
+// by the lane they would be divergent constant-cache loads inside the permutation.
+struct LaneRc {
+  uint32_t init[4], term[4];
+};
+__device__ __forceinline__ LaneRc lane_rc(const kb::P16Consts& c) {
+  const int i = threadIdx.x & 15;
+  LaneRc l;
+#pragma unroll
+  for (int r = 0; r < 4; r++) l.init[r] = c.ext_init[r * 16 + i], l.term[r] = c.ext_term[r * 16 + i];
+  return l;
+}
+__device__ __forceinline__ void p16_warp(uint32_t (&s)[16], const kb::P16Consts& c, const LaneRc& lr) {
   const int i = threadIdx.x & 15;
   uint32_t v = m4_lanes(lane_word(s, i), i);
-#pragma unroll 1
-  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, c.ext_init[r * 16 + i])), i);
+#pragma unroll
+  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, lr.init[r])), i);
 #pragma unroll
   for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
 #pragma unroll 4
   for (int r = 0; r < kb::P16Consts::RP; r++) kb::internal_layer_with0<16>(s, kb::cube(kb::add(s[0], c.internal[r])));
   v = lane_word(s, i);
-#pragma unroll 1
-  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, c.ext_term[r * 16 + i])), i);
+#pragma unroll
+  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, lr.term[r])), i);
 #pragma unroll
   for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
 }
 
-// The permutation runs on a register copy of the state (the challenger itself, indexed by its
-// buffer lengths, lives in local memory). Every lane of the calling warp takes part.
-__device__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p) {
+// The challenger stays in registers: its buffers are indexed only through unrolled selects
+// (a dynamic index would put the whole state in local memory). Every lane of the calling warp
+// takes part, with the same values.
+__device__ __forceinline__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p, const LaneRc& lr) {
   uint32_t s[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) s[i] = (i < 8 && i < c.in_len) ? c.in[i] : c.state[i];
   c.in_len = 0;
-  p16_warp(s, p);
+  p16_warp(s, p, lr);
 #pragma unroll
   for (int i = 0; i < 16; i++) c.state[i] = s[i];
 #pragma unroll
   for (int i = 0; i < 8; i++) c.out[i] = s[i];
   c.out_len = 8;
 }
-__device__ void dch_observe(DevChallenger& c, uint32_t x, const kb::P16Consts& p) {
+__device__ __forceinline__ void dch_observe(DevChallenger& c, uint32_t x, const kb::P16Consts& p, const LaneRc& lr) {
   c.out_len = 0;
-  c.in[c.in_len++] = x;
-  if (c.in_len == 8) dch_duplex(c, p);
+#pragma unroll
+  for (int j = 0; j < 8; j++) c.in[j] = j == c.in_len ? x : c.in[j];
+  if (++c.in_len == 8) dch_duplex(c, p, lr);
 }
-__device__ uint32_t dch_sample(DevChallenger& c, const kb::P16Consts& p) {
-  if (c.in_len || !c.out_len) dch_duplex(c, p);
-  return c.out[--c.out_len];
+__device__ __forceinline__ uint32_t dch_sample(DevChallenger& c, const kb::P16Consts& p, const LaneRc& lr) {
+  if (c.in_len || !c.out_len) dch_duplex(c, p, lr);
+  --c.out_len;
+  uint32_t v = c.out[0];
+#pragma unroll
+  for (int j = 1; j < 8; j++) v = j == c.out_len ? c.out[j] : v;
+  return v;
 }
 // Writes v to the proof and absorbs it (Transcript::add_ext).
-__device__ void dts_add_ext(DevRound& st, uint32_t* proof, const ef& v, const kb::P16Consts& p) {
-#pragma unroll 1
+__device__ __forceinline__ void dts_add_ext(DevRound& st, uint32_t* proof, const ef& v, const kb::P16Consts& p,
+                                            const LaneRc& lr) {
+#pragma unroll
   for (int i = 0; i < 8; i++) {
     if ((threadIdx.x & 31) == 0) proof[st.proof_len] = v.c[i];
     st.proof_len++;
-    dch_observe(st.ch, v.c[i], p);
+    dch_observe(st.ch, v.c[i], p, lr);
   }
 }
-__device__ ef dts_sample_ext(DevRound& st, const kb::P16Consts& p) {
+__device__ __forceinline__ ef dts_sample_ext(DevRound& st, const kb::P16Consts& p, const LaneRc& lr) {
   ef e;
-#pragma unroll 1
-  for (int i = 0; i < 8; i++) e.c[i] = dch_sample(st.ch, p);
+#pragma unroll
+  for (int i = 0; i < 8; i++) e.c[i] = dch_sample(st.ch, p, lr);
   return e;
 }
 
@@ -125,9 +144,21 @@ __device__ void reduce_sums(const ef* __restrict__ partial, int nb, int nsum, ef
   __syncthreads();
 }
 
-__device__ ef poly_eval_dev(const ef* c, int n, const ef& x) {
+template <int N>
+__device__ __forceinline__ ef poly_eval_dev(const ef (&c)[N], const ef& x) {
   ef r = kb::ef_zero();
-  for (int i = n - 1; i >= 0; i--) r = kb::ef_add(kb::ef_mul(r, x), c[i]);
+#pragma unroll
+  for (int i = N - 1; i >= 0; i--) r = kb::ef_add(kb::ef_mul(r, x), c[i]);
+  return r;
+}
+// c[k] of a small register array without a dynamic index.
+template <int N>
+__device__ __forceinline__ ef pick(const ef (&c)[N], int k) {
+  ef r = c[0];
+#pragma unroll
+  for (int i = 1; i < N; i++)
+#pragma unroll
+    for (int w = 0; w < 8; w++) r.c[w] = i == k ? c[i].c[w] : r.c[w];
   return r;
 }
 
@@ -145,27 +176,35 @@ __global__ void __launch_bounds__(FIN_THREADS, 1) k_eqsc_round_finish(const ef* 
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, NPTS - 1, red, scratch);
   if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
+  const LaneRc lr = lane_rc(fc.p16);
   DevRound st = *stp;
   ef e[NPTS];
   e[0] = kb::ef_mul(red[0], st.mmf);
+#pragma unroll
   for (int i = 2; i < NPTS; i++) e[i] = kb::ef_mul(red[i - 1], st.mmf);
   const ef one = kb::ef_one();
   const ef omr = kb::ef_sub(one, r);
   e[1] = kb::ef_mul(kb::ef_sub(st.sum, kb::ef_mul(e[0], omr)), rinv);
   ef q[NPTS];
+#pragma unroll
   for (int k = 0; k < NPTS; k++) q[k] = kb::ef_zero();
+#pragma unroll
   for (int i = 0; i < NPTS; i++)
+#pragma unroll
     for (int k = 0; k < NPTS; k++) q[k] = kb::ef_add(q[k], kb::ef_mul_f(e[i], fc.basis[NPTS - 3][i][k]));
   const ef lin = kb::ef_sub(kb::ef_add(r, r), one);  // (1 - r) + lin X
   ef p[NPTS + 1];
+#pragma unroll
   for (int k = 0; k <= NPTS; k++) p[k] = kb::ef_zero();
+#pragma unroll
   for (int k = 0; k < NPTS; k++) {
     p[k] = kb::ef_add(p[k], kb::ef_mul(q[k], omr));
     p[k + 1] = kb::ef_add(p[k + 1], kb::ef_mul(q[k], lin));
   }
-  for (int k = 0; k <= NPTS; k++) dts_add_ext(st, proof, p[k], fc.p16);
-  const ef c = dts_sample_ext(st, fc.p16);
-  st.sum = poly_eval_dev(p, NPTS + 1, c);
+#pragma unroll 1
+  for (int k = 0; k <= NPTS; k++) dts_add_ext(st, proof, pick(p, k), fc.p16, lr);
+  const ef c = dts_sample_ext(st, fc.p16, lr);
+  st.sum = poly_eval_dev(p, c);
   st.mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(omr, kb::ef_sub(one, c)), kb::ef_mul(r, c)), st.mmf);
   if (threadIdx.x == 0) {
     ch_out[st.round] = c;
@@ -184,16 +223,20 @@ __global__ void __launch_bounds__(FIN_THREADS, 1) k_prod_round_finish(const ef* 
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, 2, red, scratch);
   if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
+  const LaneRc lr = lane_rc(fc.p16);
   DevRound st = *stp;
   const ef y[3] = {red[0], kb::ef_sub(st.sum, red[0]), red[1]};
   ef p[3];
+#pragma unroll
   for (int k = 0; k < 3; k++) {
     p[k] = kb::ef_zero();
+#pragma unroll
     for (int i = 0; i < 3; i++) p[k] = kb::ef_add(p[k], kb::ef_mul_f(y[i], fc.basis[0][i][k]));
   }
-  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, p[k], fc.p16);
-  const ef c = dts_sample_ext(st, fc.p16);
-  st.sum = poly_eval_dev(p, 3, c);
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, pick(p, k), fc.p16, lr);
+  const ef c = dts_sample_ext(st, fc.p16, lr);
+  st.sum = poly_eval_dev(p, c);
   if (threadIdx.x == 0) {
     ch_out[st.round] = c;
     st.round++;
@@ -211,9 +254,12 @@ __global__ void __launch_bounds__(FIN_THREADS, 1) k_whir_round_finish(const ef* 
   __shared__ ef red[3], scratch[12];
   reduce_sums(partial, nb, 3, red, scratch);
   if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
+  const LaneRc lr = lane_rc(fc.p16);
   DevRound st = *stp;
-  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, red[k], fc.p16);
-  const ef r = dts_sample_ext(st, fc.p16);
+  const ef h[3] = {red[0], red[1], red[2]};
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, pick(h, k), fc.p16, lr);
+  const ef r = dts_sample_ext(st, fc.p16, lr);
   // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2
   const ef rm1 = kb::ef_sub_f(r, fc.one), rm2 = kb::ef_sub_f(r, fc.two);
   const ef a = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[0], rm1), rm2), fc.inv2);
