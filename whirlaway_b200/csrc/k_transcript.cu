@@ -20,109 +20,113 @@ namespace wl {
 namespace {
 
 constexpr int FIN_THREADS = 384;  // up to three sums, 128 threads each
+constexpr unsigned FULL = 0xffffffffu;
 
-// Poseidon2-16 in Montgomery form for one warp whose 32 lanes all hold the same state (the
-// transcript runs redundantly on every lane of warp 0, so every lane has every value). The
-// full rounds spread the state over 16 lanes (lane i, and its mirror i + 16, holds word i):
-// the S-boxes run side by side and the external layer is three in-chunk shuffles and two
-// cross-chunk shuffle sums. The partial rounds run on the whole state in every lane (only word
-// 0 takes the S-box, the other words' updates are independent of each other). The field values
-// are those of kb::p2_permute<16>: the same linear maps and S-box, evaluated in another order.
+// A round's finish runs as one warp over little code: a finishing kernel executes each of its
+// instructions only a few times, so straight-line code would spend most of its time fetching
+// instructions. The permutation, the absorption and the extension-field products are rolled
+// loops; the challenger lives in shared memory (lane 0 updates its buffers, lanes 0-15 the
+// state), and every lane of warp 0 computes the same round values.
+struct FinShared {
+  DevChallenger ch;
+  uint32_t rc[8][16];  // full-round constants: rounds 0-3 initial, 4-7 terminal
+  uint32_t sample[8];
+  ef red[3], scratch[12];
+};
+
+// a * b in F[X]/(X^8 - 3): kb::ef_mul behind a call, so that every product of a finish runs
+// the same few hundred instructions from the instruction cache.
+__device__ __noinline__ ef fin_mul(const ef a, const ef b) { return kb::ef_mul(a, b); }
+
 __device__ __forceinline__ uint32_t m4_lanes(uint32_t a, int i) {
   const int base = i & ~3;
-  const uint32_t b = __shfl_sync(0xffffffffu, a, base | ((i + 1) & 3), 16);
-  const uint32_t c = __shfl_sync(0xffffffffu, a, base | ((i + 2) & 3), 16);
-  const uint32_t d = __shfl_sync(0xffffffffu, a, base | ((i + 3) & 3), 16);
-  // row i of circ(2, 3, 1, 1) within the chunk: 2a + 3b + c + d
+  const uint32_t b = __shfl_sync(FULL, a, base | ((i + 1) & 3), 16);
+  const uint32_t c = __shfl_sync(FULL, a, base | ((i + 2) & 3), 16);
+  const uint32_t d = __shfl_sync(FULL, a, base | ((i + 3) & 3), 16);
+  // row i of circ(2, 3, 1, 1) within the chunk: 2a + 3b + c + d; then the sums over the chunks
   const uint32_t y = kb::add(kb::add(kb::add(a, b), kb::add(c, d)), kb::add(a, kb::dbl(b)));
-  uint32_t t = kb::add(y, __shfl_xor_sync(0xffffffffu, y, 4, 16));
-  t = kb::add(t, __shfl_xor_sync(0xffffffffu, t, 8, 16));
+  uint32_t t = kb::add(y, __shfl_xor_sync(FULL, y, 4, 16));
+  t = kb::add(t, __shfl_xor_sync(FULL, t, 8, 16));
   return kb::add(y, t);
 }
-__device__ __forceinline__ uint32_t lane_word(const uint32_t (&s)[16], int i) {
-  uint32_t v = s[0];
-#pragma unroll
-  for (int j = 1; j < 16; j++) v = i == j ? s[j] : v;
-  return v;
-}
-// This lane's full-round constants (word i of each full round), loaded once per kernel: indexed
-// by the lane they would be divergent constant-cache loads inside the permutation.
-struct LaneRc {
-  uint32_t init[4], term[4];
-};
-__device__ __forceinline__ LaneRc lane_rc(const kb::P16Consts& c) {
-  const int i = threadIdx.x & 15;
-  LaneRc l;
-#pragma unroll
-  for (int r = 0; r < 4; r++) l.init[r] = c.ext_init[r * 16 + i], l.term[r] = c.ext_term[r * 16 + i];
-  return l;
-}
-__device__ __forceinline__ void p16_warp(uint32_t (&s)[16], const kb::P16Consts& c, const LaneRc& lr) {
-  const int i = threadIdx.x & 15;
-  uint32_t v = m4_lanes(lane_word(s, i), i);
-#pragma unroll
-  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, lr.init[r])), i);
-#pragma unroll
-  for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
-#pragma unroll 4
-  for (int r = 0; r < kb::P16Consts::RP; r++) kb::internal_layer_with0<16>(s, kb::cube(kb::add(s[0], c.internal[r])));
-  v = lane_word(s, i);
-#pragma unroll
-  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, lr.term[r])), i);
-#pragma unroll
-  for (int j = 0; j < 16; j++) s[j] = __shfl_sync(0xffffffffu, v, j, 16);
-}
 
-// The challenger stays in registers: its buffers are indexed only through unrolled selects
-// (a dynamic index would put the whole state in local memory). Every lane of the calling warp
-// takes part, with the same values.
-__device__ __forceinline__ void dch_duplex(DevChallenger& c, const kb::P16Consts& p, const LaneRc& lr) {
+// Duplexing: Poseidon2-16 (Montgomery form, the values of kb::p2_permute<16>) of the state with
+// the pending inputs written over its first words. Full rounds across 16 lanes (lane i and its
+// mirror i + 16 hold word i), partial rounds on the whole state in every lane.
+__device__ __noinline__ void fin_duplex(FinShared& fs, const kb::P16Consts& c) {
+  const int lane = threadIdx.x & 31, i = lane & 15;
+  uint32_t v = (i < 8 && i < fs.ch.in_len) ? fs.ch.in[i] : fs.ch.state[i];
+  v = m4_lanes(v, i);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = m4_lanes(kb::cube(kb::add(v, fs.rc[r][i])), i);
   uint32_t s[16];
 #pragma unroll
-  for (int i = 0; i < 16; i++) s[i] = (i < 8 && i < c.in_len) ? c.in[i] : c.state[i];
-  c.in_len = 0;
-  p16_warp(s, p, lr);
+  for (int j = 0; j < 16; j++) s[j] = __shfl_sync(FULL, v, j, 16);
+#pragma unroll 1
+  for (int r = 0; r < kb::P16Consts::RP; r++) kb::internal_layer_with0<16>(s, kb::cube(kb::add(s[0], c.internal[r])));
+  v = s[0];
 #pragma unroll
-  for (int i = 0; i < 16; i++) c.state[i] = s[i];
-#pragma unroll
-  for (int i = 0; i < 8; i++) c.out[i] = s[i];
-  c.out_len = 8;
-}
-__device__ __forceinline__ void dch_observe(DevChallenger& c, uint32_t x, const kb::P16Consts& p, const LaneRc& lr) {
-  c.out_len = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) c.in[j] = j == c.in_len ? x : c.in[j];
-  if (++c.in_len == 8) dch_duplex(c, p, lr);
-}
-__device__ __forceinline__ uint32_t dch_sample(DevChallenger& c, const kb::P16Consts& p, const LaneRc& lr) {
-  if (c.in_len || !c.out_len) dch_duplex(c, p, lr);
-  --c.out_len;
-  uint32_t v = c.out[0];
-#pragma unroll
-  for (int j = 1; j < 8; j++) v = j == c.out_len ? c.out[j] : v;
-  return v;
-}
-// Writes v to the proof and absorbs it (Transcript::add_ext).
-__device__ __forceinline__ void dts_add_ext(DevRound& st, uint32_t* proof, const ef& v, const kb::P16Consts& p,
-                                            const LaneRc& lr) {
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    if ((threadIdx.x & 31) == 0) proof[st.proof_len] = v.c[i];
-    st.proof_len++;
-    dch_observe(st.ch, v.c[i], p, lr);
+  for (int j = 1; j < 16; j++) v = i == j ? s[j] : v;
+#pragma unroll 1
+  for (int r = 4; r < 8; r++) v = m4_lanes(kb::cube(kb::add(v, fs.rc[r][i])), i);
+  __syncwarp();
+  if (lane < 16) {
+    fs.ch.state[i] = v;
+    if (i < 8) fs.ch.out[i] = v;
   }
+  if (lane == 0) {
+    fs.ch.in_len = 0;
+    fs.ch.out_len = 8;
+  }
+  __syncwarp();
 }
-__device__ __forceinline__ ef dts_sample_ext(DevRound& st, const kb::P16Consts& p, const LaneRc& lr) {
+// Transcript::add_ext: the value goes to the proof (word offset *plen) and into the challenger.
+__device__ __noinline__ void fin_add_ext(FinShared& fs, const ef v, uint32_t* proof, uint32_t* plen,
+                                         const kb::P16Consts& c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int w = 0; w < 8; w++) {
+    uint32_t x = v.c[0];
+#pragma unroll
+    for (int u = 1; u < 8; u++) x = w == u ? v.c[u] : x;
+    if (lane == 0) {
+      proof[*plen + w] = x;
+      fs.ch.out_len = 0;
+      fs.ch.in[fs.ch.in_len] = x;
+      fs.ch.in_len++;
+    }
+    __syncwarp();
+    if (fs.ch.in_len == 8) fin_duplex(fs, c);
+  }
+  *plen += 8;
+}
+__device__ __noinline__ ef fin_sample_ext(FinShared& fs, const kb::P16Consts& c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int k = 0; k < 8; k++) {
+    if (fs.ch.in_len || !fs.ch.out_len) fin_duplex(fs, c);
+    if (lane == 0) {
+      fs.ch.out_len--;
+      fs.sample[k] = fs.ch.out[fs.ch.out_len];
+    }
+    __syncwarp();
+  }
   ef e;
 #pragma unroll
-  for (int i = 0; i < 8; i++) e.c[i] = dch_sample(st.ch, p, lr);
+  for (int k = 0; k < 8; k++) e.c[k] = fs.sample[k];
+  __syncwarp();
   return e;
 }
 
-// Sums of `nsum` interleaved partials (partial[b * nsum + z]) into red[z]; every thread of the
-// block takes part, the result is valid after the final barrier.
-__device__ void reduce_sums(const ef* __restrict__ partial, int nb, int nsum, ef* red, ef* scratch) {
-  const int z = threadIdx.x >> 7, t = threadIdx.x & 127;
+// Block prologue of every finishing kernel: the challenger and the full-round constants into
+// shared memory, and the `nsum` sums of nb interleaved partial rows (partial[row * nsum + z])
+// into fs.red. Returns false for the threads that take no part in the finish (warps >= 1).
+__device__ bool fin_begin(FinShared& fs, const DevRound* stp, const kb::P16Consts& c, const ef* __restrict__ partial,
+                          int nb, int nsum) {
+  const int tid = threadIdx.x;
+  if (tid < 128) fs.rc[tid >> 4][tid & 15] = (tid >> 4) < 4 ? c.ext_init[tid] : c.ext_term[tid - 64];
+  if (tid == 0) fs.ch = stp->ch;
+  const int z = tid >> 7, t = tid & 127;
   ef acc = kb::ef_zero();
   if (z < nsum) {
     int b = t;
@@ -134,31 +138,29 @@ __device__ void reduce_sums(const ef* __restrict__ partial, int nb, int nsum, ef
     for (; b < nb; b += 128) acc = kb::ef_add(acc, partial[size_t(b) * nsum + z]);
   }
   acc = warp_reduce_ef(acc);
-  if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = acc;
+  if ((tid & 31) == 0) fs.scratch[tid >> 5] = acc;
   __syncthreads();
   if (t == 0 && z < nsum) {
-    ef s = scratch[z * 4];
-    for (int w = 1; w < 4; w++) s = kb::ef_add(s, scratch[z * 4 + w]);
-    red[z] = s;
+    ef s = fs.scratch[z * 4];
+    for (int w = 1; w < 4; w++) s = kb::ef_add(s, fs.scratch[z * 4 + w]);
+    fs.red[z] = s;
   }
   __syncthreads();
+  return tid < 32;
 }
-
-template <int N>
-__device__ __forceinline__ ef poly_eval_dev(const ef (&c)[N], const ef& x) {
+// Block epilogue: the round's challenge and the updated state (lane 0).
+__device__ void fin_end(const FinShared& fs, DevRound* stp, DevRound& st, const ef& chal, ef* ch_out) {
+  if ((threadIdx.x & 31) == 0) {
+    st.ch = fs.ch;
+    ch_out[st.round] = chal;
+    st.round++;
+    *stp = st;
+  }
+}
+__device__ ef fin_poly_eval(const ef* p, int n, const ef& x) {
   ef r = kb::ef_zero();
-#pragma unroll
-  for (int i = N - 1; i >= 0; i--) r = kb::ef_add(kb::ef_mul(r, x), c[i]);
-  return r;
-}
-// c[k] of a small register array without a dynamic index.
-template <int N>
-__device__ __forceinline__ ef pick(const ef (&c)[N], int k) {
-  ef r = c[0];
-#pragma unroll
-  for (int i = 1; i < N; i++)
-#pragma unroll
-    for (int w = 0; w < 8; w++) r.c[w] = i == k ? c[i].c[w] : r.c[w];
+#pragma unroll 1
+  for (int i = n - 1; i >= 0; i--) r = kb::ef_add(fin_mul(r, x), p[i]);
   return r;
 }
 
@@ -169,108 +171,97 @@ __device__ __forceinline__ ef pick(const ef (&c)[N], int k) {
 // eq factor of the current variable, (1 - r) + (2r - 1) X: NPTS + 1 coefficients.
 template <int NPTS>
 __global__ void __launch_bounds__(FIN_THREADS, 1) k_eqsc_round_finish(const ef* __restrict__ partial, int nb, ef r,
-                                                                   ef rinv, const __grid_constant__ FinishConsts fc,
-                                                                   DevRound* __restrict__ stp,
-                                                                   uint32_t* __restrict__ proof,
-                                                                   ef* __restrict__ ch_out) {
-  __shared__ ef red[3], scratch[12];
-  reduce_sums(partial, nb, NPTS - 1, red, scratch);
-  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
-  const LaneRc lr = lane_rc(fc.p16);
+                                                                      ef rinv, const __grid_constant__ FinishConsts fc,
+                                                                      DevRound* __restrict__ stp,
+                                                                      uint32_t* __restrict__ proof,
+                                                                      ef* __restrict__ ch_out) {
+  __shared__ FinShared fs;
+  __shared__ ef e[NPTS], p[NPTS + 1];
+  if (!fin_begin(fs, stp, fc.p16, partial, nb, NPTS - 1)) return;
+  const int lane = threadIdx.x;
   DevRound st = *stp;
-  ef e[NPTS];
-  e[0] = kb::ef_mul(red[0], st.mmf);
-#pragma unroll
-  for (int i = 2; i < NPTS; i++) e[i] = kb::ef_mul(red[i - 1], st.mmf);
   const ef one = kb::ef_one();
   const ef omr = kb::ef_sub(one, r);
-  e[1] = kb::ef_mul(kb::ef_sub(st.sum, kb::ef_mul(e[0], omr)), rinv);
-  ef q[NPTS];
-#pragma unroll
-  for (int k = 0; k < NPTS; k++) q[k] = kb::ef_zero();
-#pragma unroll
-  for (int i = 0; i < NPTS; i++)
-#pragma unroll
-    for (int k = 0; k < NPTS; k++) q[k] = kb::ef_add(q[k], kb::ef_mul_f(e[i], fc.basis[NPTS - 3][i][k]));
-  const ef lin = kb::ef_sub(kb::ef_add(r, r), one);  // (1 - r) + lin X
-  ef p[NPTS + 1];
-#pragma unroll
-  for (int k = 0; k <= NPTS; k++) p[k] = kb::ef_zero();
-#pragma unroll
-  for (int k = 0; k < NPTS; k++) {
-    p[k] = kb::ef_add(p[k], kb::ef_mul(q[k], omr));
-    p[k + 1] = kb::ef_add(p[k + 1], kb::ef_mul(q[k], lin));
+  if (lane == 0) {
+    e[0] = fin_mul(fs.red[0], st.mmf);
+    for (int i = 2; i < NPTS; i++) e[i] = fin_mul(fs.red[i - 1], st.mmf);
+    e[1] = fin_mul(kb::ef_sub(st.sum, fin_mul(e[0], omr)), rinv);
+    const ef lin = kb::ef_sub(kb::ef_add(r, r), one);  // (1 - r) + lin X
+    for (int k = 0; k <= NPTS; k++) p[k] = kb::ef_zero();
+    for (int k = 0; k < NPTS; k++) {
+      ef q = kb::ef_zero();
+      for (int i = 0; i < NPTS; i++) q = kb::ef_add(q, kb::ef_mul_f(e[i], fc.basis[NPTS - 3][i][k]));
+      p[k] = kb::ef_add(p[k], fin_mul(q, omr));
+      p[k + 1] = kb::ef_add(p[k + 1], fin_mul(q, lin));
+    }
   }
+  __syncwarp();
+  uint32_t plen = st.proof_len;
 #pragma unroll 1
-  for (int k = 0; k <= NPTS; k++) dts_add_ext(st, proof, pick(p, k), fc.p16, lr);
-  const ef c = dts_sample_ext(st, fc.p16, lr);
-  st.sum = poly_eval_dev(p, c);
-  st.mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(omr, kb::ef_sub(one, c)), kb::ef_mul(r, c)), st.mmf);
-  if (threadIdx.x == 0) {
-    ch_out[st.round] = c;
-    st.round++;
-    *stp = st;
+  for (int k = 0; k <= NPTS; k++) fin_add_ext(fs, p[k], proof, &plen, fc.p16);
+  const ef c = fin_sample_ext(fs, fc.p16);
+  st.proof_len = plen;
+  if (lane == 0) {
+    st.sum = fin_poly_eval(p, NPTS + 1, c);
+    st.mmf = fin_mul(kb::ef_add(fin_mul(omr, kb::ef_sub(one, c)), fin_mul(r, c)), st.mmf);
   }
+  fin_end(fs, stp, st, c, ch_out);
 }
 
 // Round of the product sumcheck (the inner sumcheck): sums at 0 and 2, the value at 1 from the
 // claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
 __global__ void __launch_bounds__(FIN_THREADS, 1) k_prod_round_finish(const ef* __restrict__ partial, int nb,
-                                                                   const __grid_constant__ FinishConsts fc,
-                                                                   DevRound* __restrict__ stp,
-                                                                   uint32_t* __restrict__ proof,
-                                                                   ef* __restrict__ ch_out) {
-  __shared__ ef red[3], scratch[12];
-  reduce_sums(partial, nb, 2, red, scratch);
-  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
-  const LaneRc lr = lane_rc(fc.p16);
+                                                                      const __grid_constant__ FinishConsts fc,
+                                                                      DevRound* __restrict__ stp,
+                                                                      uint32_t* __restrict__ proof,
+                                                                      ef* __restrict__ ch_out) {
+  __shared__ FinShared fs;
+  __shared__ ef p[3];
+  if (!fin_begin(fs, stp, fc.p16, partial, nb, 2)) return;
+  const int lane = threadIdx.x;
   DevRound st = *stp;
-  const ef y[3] = {red[0], kb::ef_sub(st.sum, red[0]), red[1]};
-  ef p[3];
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    p[k] = kb::ef_zero();
-#pragma unroll
-    for (int i = 0; i < 3; i++) p[k] = kb::ef_add(p[k], kb::ef_mul_f(y[i], fc.basis[0][i][k]));
+  if (lane == 0) {
+    const ef y[3] = {fs.red[0], kb::ef_sub(st.sum, fs.red[0]), fs.red[1]};
+    for (int k = 0; k < 3; k++) {
+      ef v = kb::ef_zero();
+      for (int i = 0; i < 3; i++) v = kb::ef_add(v, kb::ef_mul_f(y[i], fc.basis[0][i][k]));
+      p[k] = v;
+    }
   }
+  __syncwarp();
+  uint32_t plen = st.proof_len;
 #pragma unroll 1
-  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, pick(p, k), fc.p16, lr);
-  const ef c = dts_sample_ext(st, fc.p16, lr);
-  st.sum = poly_eval_dev(p, c);
-  if (threadIdx.x == 0) {
-    ch_out[st.round] = c;
-    st.round++;
-    *stp = st;
-  }
+  for (int k = 0; k < 3; k++) fin_add_ext(fs, p[k], proof, &plen, fc.p16);
+  const ef c = fin_sample_ext(fs, fc.p16);
+  st.proof_len = plen;
+  if (lane == 0) st.sum = fin_poly_eval(p, 3, c);
+  fin_end(fs, stp, st, c, ch_out);
 }
 
 // Round of the WHIR folding sumcheck: the three values h(0), h(1), h(2) go to the proof as
 // they are; the next claim is h(r) by quadratic interpolation on 0, 1, 2.
 __global__ void __launch_bounds__(FIN_THREADS, 1) k_whir_round_finish(const ef* __restrict__ partial, int nb,
-                                                                   const __grid_constant__ FinishConsts fc,
-                                                                   DevRound* __restrict__ stp,
-                                                                   uint32_t* __restrict__ proof,
-                                                                   ef* __restrict__ ch_out) {
-  __shared__ ef red[3], scratch[12];
-  reduce_sums(partial, nb, 3, red, scratch);
-  if (threadIdx.x >= 32) return;  // warp 0 finishes the round, every lane the same values
-  const LaneRc lr = lane_rc(fc.p16);
+                                                                      const __grid_constant__ FinishConsts fc,
+                                                                      DevRound* __restrict__ stp,
+                                                                      uint32_t* __restrict__ proof,
+                                                                      ef* __restrict__ ch_out) {
+  __shared__ FinShared fs;
+  if (!fin_begin(fs, stp, fc.p16, partial, nb, 3)) return;
   DevRound st = *stp;
-  const ef h[3] = {red[0], red[1], red[2]};
+  uint32_t plen = st.proof_len;
 #pragma unroll 1
-  for (int k = 0; k < 3; k++) dts_add_ext(st, proof, pick(h, k), fc.p16, lr);
-  const ef r = dts_sample_ext(st, fc.p16, lr);
-  // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2
-  const ef rm1 = kb::ef_sub_f(r, fc.one), rm2 = kb::ef_sub_f(r, fc.two);
-  const ef a = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[0], rm1), rm2), fc.inv2);
-  const ef b = kb::ef_mul(kb::ef_mul(red[1], r), rm2);
-  const ef c = kb::ef_mul_f(kb::ef_mul(kb::ef_mul(red[2], r), rm1), fc.inv2);
-  st.sum = kb::ef_add(kb::ef_sub(a, b), c);
+  for (int k = 0; k < 3; k++) fin_add_ext(fs, fs.red[k], proof, &plen, fc.p16);
+  const ef r = fin_sample_ext(fs, fc.p16);
+  st.proof_len = plen;
   if (threadIdx.x == 0) {
-    ch_out[st.round] = r;
-    st.round++;
-    *stp = st;
+    // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2
+    const ef rm1 = kb::ef_sub_f(r, fc.one), rm2 = kb::ef_sub_f(r, fc.two);
+    const ef a = kb::ef_mul_f(fin_mul(fin_mul(fs.red[0], rm1), rm2), fc.inv2);
+    const ef b = fin_mul(fin_mul(fs.red[1], r), rm2);
+    const ef c = kb::ef_mul_f(fin_mul(fin_mul(fs.red[2], r), rm1), fc.inv2);
+    st.sum = kb::ef_add(kb::ef_sub(a, b), c);
   }
+  fin_end(fs, stp, st, r, ch_out);
 }
 
 // First level of the reduction of nb interleaved rows of k partial sums (partial[row * k + z]):
