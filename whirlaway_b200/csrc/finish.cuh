@@ -1,0 +1,390 @@
+// Device-side finish of a sumcheck round: the transcript step that follows the round's sums
+// (interpolation, absorption into the challenger, the sampled challenge, the next claim). Used
+// by the single-block finishing kernels (k_transcript.cu) and by the fold-and-evaluate kernels
+// whose last block finishes the round itself (k_sumcheck.cu).
+//
+// Warp 0 of the block runs a finish with its values spread over the lanes rather than
+// repeated in one: the challenger's 16-word state has word i in lanes i and i + 16, an
+// extension-field value has coordinate k in lanes k, k + 8, k + 16 and k + 24. A
+// Poseidon2-16 permutation then takes about a quarter of the cycles of the one-thread form
+// (each partial round's state sum is two warp reductions instead of fifteen modular
+// additions and sixteen diagonal products per lane), and an extension-field product about a
+// third (each lane forms one coordinate's eight-term dot product).
+#pragma once
+#include "kernels.h"
+
+namespace wl {
+namespace {
+
+constexpr unsigned FIN_FULL = 0xffffffffu;
+
+// Shared-memory part of a finish: the permutation's constants and the round's reduced sums.
+struct FinSmem {
+  uint32_t rc[8][16];               // full-round constants: rounds 0-3 initial, 4-7 terminal
+  uint32_t ci[kb::P16Consts::RP];  // partial-round constants
+  uint32_t diag[16];                // internal-layer diagonal (Montgomery form)
+  ef red[4];                        // the round's sums, reduced over the partial rows
+};
+
+// The challenger, spread over warp 0: state word (lane & 15), pending input (lane & 7),
+// squeezed output (lane & 7); the lengths are the same in every lane.
+struct FinCh {
+  uint32_t st, in, out;
+  int in_len, out_len;
+};
+
+__device__ __forceinline__ int fin_lane() { return threadIdx.x & 31; }
+
+// Every thread of the block may call it; a block barrier must follow before warp 0 uses sm.
+__device__ __forceinline__ void fin_load_consts(FinSmem& sm, const FinishConsts* __restrict__ fc) {
+  for (int t = threadIdx.x; t < 128 + kb::P16Consts::RP + 16; t += blockDim.x) {
+    if (t < 128)
+      sm.rc[t >> 4][t & 15] = (t >> 4) < 4 ? fc->p16.ext_init[t] : fc->p16.ext_term[t - 64];
+    else if (t < 128 + kb::P16Consts::RP)
+      sm.ci[t - 128] = fc->p16.internal[t - 128];
+    else
+      sm.diag[t - 128 - kb::P16Consts::RP] = kb::p2_diag<16>(t - 128 - kb::P16Consts::RP);
+  }
+}
+
+__device__ __forceinline__ FinCh fin_ch_load(const DevChallenger& c) {
+  const int l = fin_lane();
+  FinCh f;
+  f.st = c.state[l & 15];
+  f.in = c.in[l & 7];
+  f.out = c.out[l & 7];
+  f.in_len = c.in_len;
+  f.out_len = c.out_len;
+  return f;
+}
+__device__ __forceinline__ void fin_ch_store(DevChallenger& c, const FinCh& f) {
+  const int l = fin_lane();
+  if (l < 16) c.state[l] = f.st;
+  if (l < 8) {
+    c.in[l] = f.in;
+    c.out[l] = f.out;
+  }
+  if (l == 0) {
+    c.in_len = f.in_len;
+    c.out_len = f.out_len;
+  }
+}
+
+// External layer across the 16 lanes of a half-warp: row i of circ(2, 3, 1, 1) within the
+// 4-word chunk, then the sum of that position over the four chunks.
+__device__ __forceinline__ uint32_t fin_m4(uint32_t a, int i) {
+  const int base = i & ~3;
+  const uint32_t b = __shfl_sync(FIN_FULL, a, base | ((i + 1) & 3), 16);
+  const uint32_t c = __shfl_sync(FIN_FULL, a, base | ((i + 2) & 3), 16);
+  const uint32_t d = __shfl_sync(FIN_FULL, a, base | ((i + 3) & 3), 16);
+  const uint32_t y = kb::add(kb::add(kb::add(a, b), kb::add(c, d)), kb::add(a, kb::dbl(b)));
+  uint32_t t = kb::add(y, __shfl_xor_sync(FIN_FULL, y, 4, 16));
+  t = kb::add(t, __shfl_xor_sync(FIN_FULL, t, 8, 16));
+  return kb::add(y, t);
+}
+
+// Poseidon2-16 (Montgomery form; the values of kb::p2_permute<16>) of the state whose word
+// (lane & 15) is v. Partial rounds: word 0 is carried in every lane (a), the other words in
+// their lanes; the sum of words 1..15 is two warp reductions of their 16-bit halves (each total
+// below 2^20), recombined with 2^31 = 2^24 - 1 (mod p), and does not wait for the S-box.
+__device__ __noinline__ uint32_t fin_perm(uint32_t v, const FinSmem& sm) {
+  const int lane = fin_lane(), i = lane & 15;
+  const uint32_t d = sm.diag[i];
+  v = fin_m4(v, i);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) v = fin_m4(kb::cube(kb::add(v, sm.rc[r][i])), i);
+  uint32_t a = __shfl_sync(FIN_FULL, v, 0);
+  const bool contrib = lane >= 1 && lane < 16;
+#pragma unroll 1
+  for (int r = 0; r < kb::P16Consts::RP; r++) {
+    const uint32_t x0 = kb::cube(kb::add(a, sm.ci[r]));
+    const uint32_t w = contrib ? v : 0u;
+    const uint32_t lo = __reduce_add_sync(FIN_FULL, w & 0xffffu), hi = __reduce_add_sync(FIN_FULL, w >> 16);
+    uint32_t t = ((hi & 0x7fffu) << 16) + (hi >> 15) * 0xffffffu + lo;  // below 2^31 + 2^28 + 2^20 < 2p
+    t = kb::umin(t, t - kb::P);
+    const uint32_t S = kb::add(t, x0);
+    a = kb::sub(S, kb::dbl(x0));  // V_0 = -2
+    v = kb::add(kb::mul(v, d), S);
+  }
+  v = i == 0 ? a : v;
+#pragma unroll 1
+  for (int r = 4; r < 8; r++) v = fin_m4(kb::cube(kb::add(v, sm.rc[r][i])), i);
+  return v;
+}
+
+// Duplexing: the pending inputs overwrite the first in_len words of the state, which is
+// permuted; the rate part becomes the output.
+__device__ __forceinline__ void fin_duplex(FinCh& c, const FinSmem& sm) {
+  const int lane = fin_lane(), i = lane & 15;
+  c.st = fin_perm((i < 8 && i < c.in_len) ? c.in : c.st, sm);
+  c.out = __shfl_sync(FIN_FULL, c.st, lane & 7);
+  c.in_len = 0;
+  c.out_len = 8;
+}
+
+// Transcript::add_ext of the value x (coordinate lane & 7): the eight words go to
+// proof[plen..] and into the challenger, one observation each. With L words already pending,
+// the first 8 - L fill the rate and duplex, the other L are left pending (and the output is
+// then empty, as any observation leaves it).
+__device__ __forceinline__ void fin_observe_ext(FinCh& c, uint32_t x, uint32_t* __restrict__ proof, uint32_t plen,
+                                                const FinSmem& sm) {
+  const int lane = fin_lane(), k = lane & 7;
+  if (lane < 8) proof[plen + lane] = x;
+  const int L = c.in_len;
+  const uint32_t first = __shfl_sync(FIN_FULL, x, (k - L) & 7);  // lane k >= L: word k - L
+  c.in = k >= L ? first : c.in;
+  c.in_len = 8;
+  fin_duplex(c, sm);
+  if (L) {
+    const uint32_t second = __shfl_sync(FIN_FULL, x, (k + 8 - L) & 7);  // lane k < L: word k + 8 - L
+    c.in = k < L ? second : c.in;
+    c.in_len = L;
+    c.out_len = 0;
+  }
+}
+
+// Transcript::sample_ext: eight samples, each popped from the end of the output (duplexing
+// first when inputs are pending or the output is empty); sample k is coordinate k.
+__device__ __forceinline__ uint32_t fin_sample_ext(FinCh& c, const FinSmem& sm) {
+  const int k = fin_lane() & 7;
+  if (c.in_len || !c.out_len) fin_duplex(c, sm);
+  const int O = c.out_len;
+  const uint32_t a = __shfl_sync(FIN_FULL, c.out, (O - 1 - k) & 7);  // sample k < O: out[O - 1 - k]
+  if (O == 8) {
+    c.out_len = 0;
+    return a;
+  }
+  fin_duplex(c, sm);  // the output ran out after O samples
+  const uint32_t b = __shfl_sync(FIN_FULL, c.out, (7 - (k - O)) & 7);  // sample k >= O: out[7 - (k - O)]
+  c.out_len = O;
+  return k < O ? a : b;
+}
+
+// Extension-field product in F[X]/(X^8 - 3), coordinate (lane & 7) of a * b within each group
+// of eight lanes: the dot product of a with (b_k, ..., b_0, 3 b_7, ..., 3 b_{k+1}) in two lazy
+// halves of four terms.
+__device__ __noinline__ uint32_t fin_mul(uint32_t a, uint32_t b) {
+  const int lane = fin_lane(), k = lane & 7, g = lane & 24;
+  const uint32_t b3 = kb::add(kb::dbl(b), b);
+  uint64_t s0 = 0, s1 = 0;
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const uint32_t at = __shfl_sync(FIN_FULL, a, g | t);
+    const uint32_t x = __shfl_sync(FIN_FULL, b, g | ((k - t) & 7)), x3 = __shfl_sync(FIN_FULL, b3, g | ((k - t) & 7));
+    const uint32_t bb = t <= k ? x : x3;
+    if (t < 4)
+      s0 += kb::wmul(at, bb);
+    else
+      s1 += kb::wmul(at, bb);
+  }
+  return kb::add(kb::redc(s0), kb::redc(s1));
+}
+// The base-field constant c as an extension coordinate: c at coordinate 0, zero elsewhere.
+__device__ __forceinline__ uint32_t fin_base(uint32_t c) { return (fin_lane() & 7) == 0 ? c : 0u; }
+__device__ __forceinline__ uint32_t fin_coord(const ef& e) {
+  const int k = fin_lane() & 7;
+  uint32_t x = e.c[0];
+#pragma unroll
+  for (int u = 1; u < 8; u++) x = k == u ? e.c[u] : x;
+  return x;
+}
+
+// Sum over `nb` rows of `nsum` interleaved extension sums (partial[row * nsum + z], written by
+// other blocks of this grid or an earlier one: read past L1) into sm.red[z]. Every thread of
+// the block calls it; tmp holds blockDim.x values; sm.red is valid in warp 0 on return.
+__device__ __forceinline__ ef fin_ldcg(const ef* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  const uint4 u = __ldcg(q), v = __ldcg(q + 1);
+  ef e;
+  e.c[0] = u.x, e.c[1] = u.y, e.c[2] = u.z, e.c[3] = u.w;
+  e.c[4] = v.x, e.c[5] = v.y, e.c[6] = v.z, e.c[7] = v.w;
+  return e;
+}
+__device__ void fin_reduce_rows(const ef* __restrict__ partial, int nb, int nsum, FinSmem& sm, ef* tmp) {
+  const int t = threadIdx.x, T = int(blockDim.x / nsum) * nsum;
+  const int n = nb * nsum;
+  ef acc = kb::ef_zero();
+  if (t < T) {
+#pragma unroll 4
+    for (int j = t; j < n; j += T) acc = kb::ef_add(acc, fin_ldcg(partial + j));
+  }
+  tmp[t] = acc;
+  __syncthreads();
+  if (t < 32) {
+    const int z = t >> 3, k = t & 7;
+    if (z < nsum) {
+      uint32_t s = 0;
+      for (int u = z; u < T; u += nsum) s = kb::add(s, tmp[u].c[k]);
+      sm.red[z].c[k] = s;
+    }
+    __syncwarp();
+  }
+}
+
+// The round's finish proper (warp 0, every lane). The state st (challenger, claim, eq weight,
+// proof length, round) is read from and written back to a.st; the round polynomial goes to
+// a.proof, the challenge to a.ch_out[round].
+//
+// Round of a sumcheck with an eq factor (the AIR zerocheck's rounds >= 1: NPTS = 4; the
+// a*b - c zerocheck: NPTS = 3): the sums are at z = 0, 2, .., NPTS - 1, weighted by the eq
+// factor mmf of the variables already folded; the value at 1 follows from the claim,
+// e1 = (sum - e0 (1 - r)) / r, with r the eq challenge of the current variable. The round
+// polynomial is the interpolation on 0..NPTS-1 times (1 - r) + (2r - 1) X: NPTS + 1
+// coefficients.
+template <int NPTS>
+__device__ __noinline__ void fin_round_eqsc(const FinArgs& a, const FinSmem& sm) {
+  const int lane = fin_lane();
+  const FinishConsts* fc = a.fc;
+  DevRound* stp = a.st;
+  const int round = stp->round;
+  uint32_t plen = stp->proof_len;
+  FinCh c = fin_ch_load(stp->ch);
+  const uint32_t sum = fin_coord(stp->sum), mmf = fin_coord(stp->mmf);
+  const uint32_t r = fin_coord(a.req[round]), rinv = fin_coord(a.rinv[round]);
+  const uint32_t one = fin_base(kb::R_MOD_P);
+  const uint32_t omr = kb::sub(one, r), lin = kb::sub(kb::add(r, r), one);
+  uint32_t e[NPTS];
+  e[0] = fin_mul(sm.red[0].c[lane & 7], mmf);
+#pragma unroll
+  for (int i = 2; i < NPTS; i++) e[i] = fin_mul(sm.red[i - 1].c[lane & 7], mmf);
+  e[1] = fin_mul(kb::sub(sum, fin_mul(e[0], omr)), rinv);
+  uint32_t q[NPTS];
+#pragma unroll
+  for (int k = 0; k < NPTS; k++) {
+    q[k] = 0;
+#pragma unroll
+    for (int i = 0; i < NPTS; i++) q[k] = kb::add(q[k], kb::mul(e[i], fc->basis[NPTS - 3][i][k]));
+  }
+  uint32_t p[NPTS + 1];
+#pragma unroll
+  for (int k = 0; k <= NPTS; k++) {
+    uint32_t v = k < NPTS ? fin_mul(q[k], omr) : 0u;
+    if (k > 0) v = kb::add(v, fin_mul(q[k - 1], lin));
+    p[k] = v;
+    fin_observe_ext(c, v, a.proof, plen, sm);
+    plen += 8;
+  }
+  const uint32_t ch = fin_sample_ext(c, sm);
+  uint32_t s = p[NPTS];
+#pragma unroll
+  for (int k = NPTS - 1; k >= 0; k--) s = kb::add(fin_mul(s, ch), p[k]);
+  const uint32_t m2 = fin_mul(kb::add(fin_mul(omr, kb::sub(one, ch)), fin_mul(r, ch)), mmf);
+  __syncwarp();
+  fin_ch_store(stp->ch, c);
+  if (lane < 8) {
+    stp->sum.c[lane] = s;
+    stp->mmf.c[lane] = m2;
+    a.ch_out[round].c[lane] = ch;
+  }
+  if (lane == 0) {
+    stp->proof_len = plen;
+    stp->round = round + 1;
+  }
+}
+
+// Round of the product sumcheck (the inner sumcheck): sums at 0 and 2, the value at 1 from the
+// claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
+__device__ __noinline__ void fin_round_prod(const FinArgs& a, const FinSmem& sm) {
+  const int lane = fin_lane();
+  const FinishConsts* fc = a.fc;
+  DevRound* stp = a.st;
+  const int round = stp->round;
+  uint32_t plen = stp->proof_len;
+  FinCh c = fin_ch_load(stp->ch);
+  const uint32_t y0 = sm.red[0].c[lane & 7], y2 = sm.red[1].c[lane & 7];
+  const uint32_t y1 = kb::sub(fin_coord(stp->sum), y0);
+  uint32_t p[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    p[k] = kb::add(kb::add(kb::mul(y0, fc->basis[0][0][k]), kb::mul(y1, fc->basis[0][1][k])),
+                   kb::mul(y2, fc->basis[0][2][k]));
+    fin_observe_ext(c, p[k], a.proof, plen, sm);
+    plen += 8;
+  }
+  const uint32_t ch = fin_sample_ext(c, sm);
+  const uint32_t s = kb::add(fin_mul(kb::add(fin_mul(p[2], ch), p[1]), ch), p[0]);
+  __syncwarp();
+  fin_ch_store(stp->ch, c);
+  if (lane < 8) {
+    stp->sum.c[lane] = s;
+    a.ch_out[round].c[lane] = ch;
+  }
+  if (lane == 0) {
+    stp->proof_len = plen;
+    stp->round = round + 1;
+  }
+}
+
+// Round of the WHIR folding sumcheck: h(0), h(1), h(2) go to the proof as they are; the next
+// claim is h(r) by quadratic interpolation on 0, 1, 2:
+// h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2.
+__device__ __noinline__ void fin_round_whir(const FinArgs& a, const FinSmem& sm) {
+  const int lane = fin_lane();
+  const FinishConsts* fc = a.fc;
+  DevRound* stp = a.st;
+  const int round = stp->round;
+  uint32_t plen = stp->proof_len;
+  FinCh c = fin_ch_load(stp->ch);
+  uint32_t h[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    h[k] = sm.red[k].c[lane & 7];
+    fin_observe_ext(c, h[k], a.proof, plen, sm);
+    plen += 8;
+  }
+  const uint32_t r = fin_sample_ext(c, sm);
+  const uint32_t rm1 = kb::sub(r, fin_base(fc->one)), rm2 = kb::sub(r, fin_base(fc->two));
+  const uint32_t t0 = kb::mul(fin_mul(fin_mul(h[0], rm1), rm2), fc->inv2);
+  const uint32_t t1 = fin_mul(fin_mul(h[1], r), rm2);
+  const uint32_t t2 = kb::mul(fin_mul(fin_mul(h[2], r), rm1), fc->inv2);
+  const uint32_t s = kb::add(kb::sub(t0, t1), t2);
+  __syncwarp();
+  fin_ch_store(stp->ch, c);
+  if (lane < 8) {
+    stp->sum.c[lane] = s;
+    a.ch_out[round].c[lane] = r;
+  }
+  if (lane == 0) {
+    stp->proof_len = plen;
+    stp->round = round + 1;
+  }
+}
+
+__device__ __forceinline__ int fin_kind_sums_dev(int kind) { return kind == FIN_EQSC4 || kind == FIN_WHIR ? 3 : 2; }
+
+// Dispatch on the round kind (warp 0 only).
+__device__ __forceinline__ void fin_round(int kind, const FinArgs& a, const FinSmem& sm) {
+  if (kind == FIN_EQSC4)
+    fin_round_eqsc<4>(a, sm);
+  else if (kind == FIN_EQSC3)
+    fin_round_eqsc<3>(a, sm);
+  else if (kind == FIN_PROD)
+    fin_round_prod(a, sm);
+  else
+    fin_round_whir(a, sm);
+}
+
+// Epilogue of a kernel whose blocks each wrote one row of `nsum` partial sums (thread 0 of the
+// block, before the call): the block that arrives last reduces all gridDim.x rows and finishes
+// the round. Every thread of every block calls it, after its own stores.
+__device__ __forceinline__ void fin_last_block(int kind, const FinArgs& a, const ef* __restrict__ partial, int nsum) {
+  __shared__ FinSmem sm;
+  __shared__ ef tmp[FIN_MAX_THREADS];
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&a.st->arrived, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  fin_load_consts(sm, a.fc);
+  fin_reduce_rows(partial, gridDim.x, nsum, sm, tmp);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    fin_round(kind, a, sm);
+    if (threadIdx.x == 0) a.st->arrived = 0;  // for the next round's grid
+  }
+}
+
+}  // namespace
+}  // namespace wl

@@ -9,6 +9,7 @@
 // row and repeat the last (crates/air/src/utils.rs:140-160); neither is materialised.
 // Folded columns are extension-field arrays, column c at cols + c * len.
 #include <algorithm>
+#include "finish.cuh"
 #include "kernels.h"
 #include "limb_mma.cuh"
 
@@ -1580,7 +1581,7 @@ __global__ void k_prod_eval(const ef* __restrict__ a, const ef* __restrict__ b, 
 // every table is read once per round: thread x of this round (x < h, the tables' new length
 // being 2h) reads old entries x, x + h, x + 2h, x + 3h, writes the two folded entries x and
 // x + h, and accumulates the round polynomial's values. Grid-stride; one partial per block.
-constexpr int FE_THREADS = 256;
+constexpr int FE_THREADS = FIN_MAX_THREADS;
 __device__ __forceinline__ ef fe_lerp(const ef* t, size_t i, size_t L, const ef& r) {
   const ef lo = t[i];
   return ef_add(lo, ef_mul(r, ef_sub(t[i + L], lo)));
@@ -1591,7 +1592,7 @@ template <int NS>
 __global__ void __launch_bounds__(FE_THREADS) k_pair_fold_eval(const ef* __restrict__ a, const ef* __restrict__ b,
                                                                const ef* __restrict__ rptr, ef* __restrict__ na,
                                                                ef* __restrict__ nb, size_t h,
-                                                               ef* __restrict__ partial) {
+                                                               ef* __restrict__ partial, const FinArgs fin) {
   __shared__ ef scratch[32];
   const ef r = *rptr;
   const size_t L = 2 * h;
@@ -1617,6 +1618,7 @@ __global__ void __launch_bounds__(FE_THREADS) k_pair_fold_eval(const ef* __restr
   }
   s2 = block_reduce_ef(s2, scratch);
   if (threadIdx.x == 0) partial[size_t(blockIdx.x) * NS + NS - 1] = s2;
+  if (fin.st) fin_last_block(NS == 2 ? FIN_PROD : FIN_WHIR, fin, partial, NS);
 }
 // The a*b - c zerocheck's rounds >= 2: three columns (column q of old length 4h at q 4h, of new
 // length 2h at q 2h) and the eq table (old length 2h, the leading variable summed out into the
@@ -1624,7 +1626,7 @@ __global__ void __launch_bounds__(FE_THREADS) k_pair_fold_eval(const ef* __restr
 __global__ void __launch_bounds__(FE_THREADS) k_abc_fold_eval(const ef* __restrict__ cols, const ef* __restrict__ rptr,
                                                               const ef* __restrict__ eq_prev, ef* __restrict__ nc,
                                                               ef* __restrict__ eq_new, size_t h,
-                                                              ef* __restrict__ partial) {
+                                                              ef* __restrict__ partial, const FinArgs fin) {
   __shared__ ef scratch[32];
   const ef r = *rptr;
   const size_t L = 2 * h;
@@ -1650,6 +1652,7 @@ __global__ void __launch_bounds__(FE_THREADS) k_abc_fold_eval(const ef* __restri
   __syncthreads();
   s2 = block_reduce_ef(s2, scratch);
   if (threadIdx.x == 0) partial[size_t(blockIdx.x) * 2 + 1] = s2;
+  if (fin.st) fin_last_block(FIN_EQSC3, fin, partial, 2);
 }
 
 // ------------------------------------------------------------------ a*b - c
@@ -1972,19 +1975,22 @@ int fold_eval_blocks(size_t h) {
   return (int)std::max<size_t>(1, std::min<size_t>((h + FE_THREADS - 1) / FE_THREADS, size_t(sms) * 4));
 }
 void launch_pair_fold_eval(int nsums, const ef* a, const ef* b, const ef* r_dev, ef* na, ef* nb, size_t h,
-                           ef* partial, cudaStream_t s) {
+                           ef* partial, const FinArgs* fin, cudaStream_t s) {
   const int g = fold_eval_blocks(h);
+  const FinArgs f = fin ? *fin : FinArgs{};
   if (nsums == 2)
-    k_pair_fold_eval<2><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial);
+    k_pair_fold_eval<2><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial, f);
   else if (nsums == 3)
-    k_pair_fold_eval<3><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial);
+    k_pair_fold_eval<3><<<g, FE_THREADS, 0, s>>>(a, b, r_dev, na, nb, h, partial, f);
   else
     throw std::invalid_argument("fold-evaluate: 2 or 3 sums");
   WL_LAUNCH_CHECK();
 }
 void launch_abc_fold_eval(const ef* cols, const ef* r_dev, const ef* eq_prev, ef* nc, ef* eq_new, size_t h, ef* partial,
-                          cudaStream_t s) {
-  k_abc_fold_eval<<<fold_eval_blocks(h), FE_THREADS, 0, s>>>(cols, r_dev, eq_prev, nc, eq_new, h, partial);
+                          const FinArgs* fin, cudaStream_t s) {
+  const FinArgs f = fin ? *fin : FinArgs{};
+  if (fin && (!f.req || !f.rinv)) throw std::invalid_argument("fold-evaluate: eq-factor rounds need their eq challenges");
+  k_abc_fold_eval<<<fold_eval_blocks(h), FE_THREADS, 0, s>>>(cols, r_dev, eq_prev, nc, eq_new, h, partial, f);
   WL_LAUNCH_CHECK();
 }
 

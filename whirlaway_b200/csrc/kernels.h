@@ -152,10 +152,13 @@ void launch_fold2_dev(const ef* a, const ef* b, ef* oa, ef* ob, size_t half, con
 // form folds three columns (4h -> 2h) and the eq table (2h -> h: the leading variable summed
 // out) and sums (A B - C) eq at z = 0 and 2. fold_eval_blocks(h) partial rows.
 int fold_eval_blocks(size_t h);
+// With fin non-null the kernel's last block also finishes the round (kind FIN_PROD for 2 sums,
+// FIN_WHIR for 3, FIN_EQSC3 for the a*b - c form).
+struct FinArgs;
 void launch_pair_fold_eval(int nsums, const ef* a, const ef* b, const ef* r_dev, ef* na, ef* nb, size_t h,
-                           ef* partial, cudaStream_t s);
+                           ef* partial, const FinArgs* fin, cudaStream_t s);
 void launch_abc_fold_eval(const ef* cols, const ef* r_dev, const ef* eq_prev, ef* nc, ef* eq_new, size_t h, ef* partial,
-                          cudaStream_t s);
+                          const FinArgs* fin, cudaStream_t s);
 
 // --------------------------------------------------------------- a*b - c zerocheck
 void launch_abc0_eval(const uint32_t* a, const uint32_t* b, const uint32_t* c, int log_n, int k, int nz,
@@ -204,38 +207,49 @@ struct DevChallenger {
   int32_t in_len, out_len;
 };
 // State of a phase of sumcheck rounds run on the device: the challenger, the current claim,
-// the zerocheck's eq weight of the folded variables, the proof words appended so far and the
-// number of rounds finished (index of the next challenge).
+// the zerocheck's eq weight of the folded variables, the proof words appended so far, the
+// number of rounds finished (index of the next challenge) and the count of blocks of the
+// current round's kernel that have written their partial sums (the last one finishes the round).
 struct DevRound {
   DevChallenger ch;
   ef sum;
   ef mmf;
   uint32_t proof_len;
   int32_t round;
+  uint32_t arrived;
 };
-// Constants of the round-finishing kernels: Poseidon2-16 (Montgomery), the Lagrange bases on
-// the nodes 0..2 and 0..3 (basis[0][i][k], basis[1][i][k]: coefficient k of basis polynomial i)
-// and the Montgomery forms of 1, 2 and 1/2.
+// Constants of the round finish: Poseidon2-16 (Montgomery), the Lagrange bases on the nodes
+// 0..2 and 0..3 (basis[0][i][k], basis[1][i][k]: coefficient k of basis polynomial i) and the
+// Montgomery forms of 1, 2 and 1/2.
 struct FinishConsts {
   kb::P16Consts p16;
   uint32_t basis[2][4][4];
   uint32_t one, two, inv2;
 };
-// One round's finish on the device (one block): reduces `nb` interleaved partial sums, writes
-// the round polynomial to proof[st->proof_len..], absorbs it, samples the challenge into
-// ch_out[st->round] and updates st. Eq-factor rounds (npts 4: the AIR zerocheck, 3: the a*b - c
-// zerocheck) take the current variable's eq challenge r and its inverse; the product
-// sumcheck (inner sumcheck) and the WHIR folding sumcheck need no more.
+// Round kinds: eq-factor rounds with 4 computed points (the AIR zerocheck's rounds >= 1) or 3
+// (the a*b - c zerocheck), the product sumcheck (inner sumcheck), the WHIR folding sumcheck.
+enum FinKind { FIN_EQSC4 = 0, FIN_EQSC3 = 1, FIN_PROD = 2, FIN_WHIR = 3 };
+// Where a round's finish reads and writes, all in device memory: the phase state, the proof
+// words (appended at st->proof_len), the challenges (ch_out[st->round]), the constants and, for
+// the eq-factor rounds, every round's eq challenge r and its inverse (indexed by st->round).
+struct FinArgs {
+  DevRound* st;
+  uint32_t* proof;
+  ef* ch_out;
+  const FinishConsts* fc;
+  const ef* req;
+  const ef* rinv;
+};
+constexpr int FIN_MAX_THREADS = 256;  // block size of every kernel that finishes a round
 // First level of a reduction of nb interleaved rows of k <= 32 partial sums
 // (partial[row * k + z]) into at most max_blocks rows in out (coalesced reads, many blocks);
-// returns the number of rows written. The finishing kernels (and the host reads) then sum those.
+// returns the number of rows written. The finishing kernel (and the host reads) then sum those.
 int launch_reduce_wide(const ef* partial, int nb, int k, ef* out, int max_blocks, cudaStream_t s);
-void launch_eqsc_round_finish(int npts, const ef* partial, int nb, const ef& r, const ef& rinv,
-                              const FinishConsts& fc, DevRound* st, uint32_t* proof, ef* ch_out, cudaStream_t s);
-void launch_prod_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
-                              ef* ch_out, cudaStream_t s);
-void launch_whir_round_finish(const ef* partial, int nb, const FinishConsts& fc, DevRound* st, uint32_t* proof,
-                              ef* ch_out, cudaStream_t s);
+// One round's finish on the device (one block): reduces `nb` interleaved rows of the round's
+// sums (3 for FIN_EQSC4 and FIN_WHIR, 2 otherwise), writes the round polynomial to the proof,
+// absorbs it, samples the challenge and updates the phase state.
+void launch_round_finish(int kind, const ef* partial, int nb, const FinArgs& a, cudaStream_t s);
+int fin_kind_sums(int kind);
 
 // --------------------------------------------------------------- batched Merkle-path checks
 // One opening to check: word offsets (into the concatenated canonical proofs) of its row (128

@@ -379,42 +379,75 @@ FinishConsts finish_consts(const kb::P16Consts& p16) {
   return fc;
 }
 
-// A phase of sumcheck rounds whose transcript runs on the device (k_transcript.cu). The
-// challenger state and the claim go to the device at the start; the host then enqueues every
-// round (its sums, the finishing kernel, the fold at the sampled challenge) without waiting,
-// and finish() reads the state, the appended proof words and the challenges back in one copy,
+// A phase of sumcheck rounds whose transcript runs on the device (finish.cuh). The challenger
+// state, the claim, the finish constants and (for eq-factor rounds) every round's eq challenge
+// and its inverse go to the device in one copy at the start; the host then enqueues every
+// round (its sums, the finish, the fold at the sampled challenge) without waiting, and
+// finish() reads the state, the appended proof words and the challenges back in one copy,
 // leaving the host transcript exactly where the host-driven rounds would have left it.
 struct DevPhase {
   Context& ctx;
   Transcript& ts;
   int rounds;
   size_t words_per_round;
-  DBuf buf;  // [DevRound][challenges: rounds][proof words: rounds * words_per_round]
+  // [DevRound][FinishConsts][eq challenges][their inverses][challenges][proof words], each
+  // section 64-byte aligned
+  DBuf buf;
+  size_t off_fc = 0, off_req = 0, off_rinv = 0, off_ch = 0, off_words = 0, total = 0;
   DevRound* st = nullptr;
   ef* chs = nullptr;
   uint32_t* words = nullptr;
-  DevPhase(Context& c, Transcript& t, int nrounds, size_t wpr, const ef& sum, const ef& mmf)
+  FinArgs fin{};
+  static size_t up64(size_t x) { return (x + 63) & ~size_t(63); }
+  DevPhase(Context& c, Transcript& t, int nrounds, size_t wpr, const ef& sum, const ef& mmf, const kb::P16Consts& p16,
+           const ef* req = nullptr)
       : ctx(c), ts(t), rounds(nrounds), words_per_round(wpr) {
-    buf = DBuf(bytes(), ctx.stream);
-    st = buf.as<DevRound>();
-    chs = reinterpret_cast<ef*>(buf.as<char>() + sizeof(DevRound));
-    words = reinterpret_cast<uint32_t*>(chs + rounds);
-    DevRound h{};
-    memcpy(h.ch.state, ts.ch.state, sizeof(h.ch.state));
-    memcpy(h.ch.in, ts.ch.in, sizeof(h.ch.in));
-    memcpy(h.ch.out, ts.ch.out, sizeof(h.ch.out));
-    h.ch.in_len = ts.ch.in_len;
-    h.ch.out_len = ts.ch.out_len;
-    h.sum = sum;
-    h.mmf = mmf;
-    h.proof_len = 0;
-    h.round = 0;
-    ctx.to_device(st, &h, sizeof(h));
+    const size_t nq = req ? size_t(rounds) : 0;
+    off_fc = up64(sizeof(DevRound));
+    off_req = up64(off_fc + sizeof(FinishConsts));
+    off_rinv = up64(off_req + sizeof(ef) * nq);
+    off_ch = up64(off_rinv + sizeof(ef) * nq);
+    off_words = up64(off_ch + sizeof(ef) * rounds);
+    total = off_words + sizeof(uint32_t) * rounds * words_per_round;
+    buf = DBuf(total, ctx.stream);
+    char* base = buf.as<char>();
+    st = reinterpret_cast<DevRound*>(base);
+    chs = reinterpret_cast<ef*>(base + off_ch);
+    words = reinterpret_cast<uint32_t*>(base + off_words);
+    fin.st = st;
+    fin.proof = words;
+    fin.ch_out = chs;
+    fin.fc = reinterpret_cast<const FinishConsts*>(base + off_fc);
+    fin.req = req ? reinterpret_cast<const ef*>(base + off_req) : nullptr;
+    fin.rinv = req ? reinterpret_cast<const ef*>(base + off_rinv) : nullptr;
+    std::vector<char> h(off_ch, 0);
+    DevRound d{};
+    memcpy(d.ch.state, ts.ch.state, sizeof(d.ch.state));
+    memcpy(d.ch.in, ts.ch.in, sizeof(d.ch.in));
+    memcpy(d.ch.out, ts.ch.out, sizeof(d.ch.out));
+    d.ch.in_len = ts.ch.in_len;
+    d.ch.out_len = ts.ch.out_len;
+    d.sum = sum;
+    d.mmf = mmf;
+    memcpy(h.data(), &d, sizeof(d));
+    const FinishConsts fc = finish_consts(p16);
+    memcpy(h.data() + off_fc, &fc, sizeof(fc));
+    for (size_t q = 0; q < nq; q++) {
+      const ef ri = kb::ef_inv(req[q]);
+      memcpy(h.data() + off_req + sizeof(ef) * q, &req[q], sizeof(ef));
+      memcpy(h.data() + off_rinv + sizeof(ef) * q, &ri, sizeof(ef));
+    }
+    ctx.to_device(base, h.data(), h.size());
   }
-  size_t bytes() const { return sizeof(DevRound) + sizeof(ef) * rounds + sizeof(uint32_t) * rounds * words_per_round; }
+  // The round's finish as its own kernel, after an evaluation kernel that left nb partial rows.
+  void finish_round(int kind, const ef* partial, int nb) {
+    const ef* red = ctx.reduce_wide(partial, nb, fin_kind_sums(kind));
+    ProfScope _ps(ctx, "round_finish");
+    launch_round_finish(kind, red, nb, fin, ctx.stream);
+  }
   // Returns the challenges; *sum (and *mmf) receive the final claim (and eq weight).
   std::vector<ef> finish(ef* sum, ef* mmf) {
-    std::vector<char> h(bytes());
+    std::vector<char> h(total);
     ctx.to_host(h.data(), buf.as<void>(), h.size());
     DevRound d;
     memcpy(&d, h.data(), sizeof(d));
@@ -426,8 +459,8 @@ struct DevPhase {
     ts.ch.in_len = d.ch.in_len;
     ts.ch.out_len = d.ch.out_len;
     std::vector<ef> ch(rounds);
-    memcpy(ch.data(), h.data() + sizeof(DevRound), sizeof(ef) * rounds);
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(h.data() + sizeof(DevRound) + sizeof(ef) * rounds);
+    memcpy(ch.data(), h.data() + off_ch, sizeof(ef) * rounds);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(h.data() + off_words);
     for (int r = 0; r < rounds; r++) {
       ts.proof.insert(ts.proof.end(), w + r * words_per_round, w + (r + 1) * words_per_round);
       if (ts.log) ts.log->add("challenge", ts.proof.size(), ch[r].c, 8, true);
@@ -705,34 +738,31 @@ ef mle_eval_dev(Context& ctx, const ef* g, int m, const std::vector<ef>& pt) {
 void whir_sumcheck_dev(Context& ctx, Transcript& ts, DBuf& g, DBuf& w, int& m, ef& sigma, int rounds, int pow_bits,
                        const kb::P16Consts& p16, std::vector<ef>& rnd) {
   if (pow_bits == 0 && rounds > 0) {
-    const FinishConsts fc = finish_consts(p16);
-    DevPhase ph(ctx, ts, rounds, 24, sigma, kb::ef_one());
-    // round 0 evaluates the tables as they are; round t >= 1 folds at challenge t - 1 and
-    // evaluates in one pass; the last challenge's fold closes the block
+    DevPhase ph(ctx, ts, rounds, 24, sigma, kb::ef_one(), p16);
+    // round 0 evaluates the tables as they are (the finish its own kernel); round t >= 1 folds
+    // at challenge t - 1, evaluates and finishes in one kernel; the last challenge's fold
+    // closes the block
     for (int t = 0; t < rounds; t++) {
       const size_t half = size_t(1) << (m - 1 - t);
-      int nb;
-      ef* part;
       if (t == 0) {
-        nb = whir_sc_blocks(half);
-        part = ctx.partials(size_t(3) * nb);
-        ProfScope _ps(ctx, "whir_sc_eval");
-        launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream);
+        const int nb = whir_sc_blocks(half);
+        ef* part = ctx.partials(size_t(3) * nb);
+        {
+          ProfScope _ps(ctx, "whir_sc_eval");
+          launch_whir_sc_eval(g.as<ef>(), w.as<ef>(), half, part, ctx.stream);
+        }
+        ph.finish_round(FIN_WHIR, part, nb);
       } else {
-        nb = fold_eval_blocks(half);
-        part = ctx.partials(size_t(3) * nb);
+        ef* part = ctx.partials(size_t(3) * fold_eval_blocks(half));
         DBuf ng(sizeof(ef) * 2 * half, ctx.stream), nw(sizeof(ef) * 2 * half, ctx.stream);
         {
           ProfScope _ps(ctx, "fold_eval");
           launch_pair_fold_eval(3, g.as<ef>(), w.as<ef>(), ph.chs + (t - 1), ng.as<ef>(), nw.as<ef>(), half, part,
-                                ctx.stream);
+                                &ph.fin, ctx.stream);
         }
         g = std::move(ng);
         w = std::move(nw);
       }
-      int nr = nb;
-      const ef* red = ctx.reduce_wide(part, nr, 3);
-      { ProfScope _ps(ctx, "round_finish"); launch_whir_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, ctx.stream); }
     }
     {
       const size_t half = size_t(1) << (m - rounds);
@@ -978,18 +1008,14 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   if (zc_on_device && n - k >= 1) {
     // every round's transcript on the device: the sums, the finishing kernel (interpolation,
     // absorption, challenge) and the fold at the device-sampled challenge, one host wait
-    const FinishConsts fc = finish_consts(job.p16);
-    DevPhase ph(ctx, ts, n - k, 40, sum, mmf);
+    DevPhase ph(ctx, ts, n - k, 40, sum, mmf, job.p16, zc.data() + 1);
     for (int round = 1; round <= n - k; round++) {
       const int m = n - k - round + 1;
       const size_t half = size_t(1) << (m - 1);
       const int nb = zc_ef_blocks(m);
       ef* part = ctx.partials(size_t(nb) * 3);
       { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
-      const ef& r = zc[round];
-      int nr = nb;
-      const ef* red = ctx.reduce_wide(part, nr, 3);
-      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(4, red, nr, r, kb::ef_inv(r), fc, ph.st, ph.words, ph.chs, st); }
+      ph.finish_round(FIN_EQSC4, part, nb);
       DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
       DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
       { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), W + 1, half, ph.chs + (round - 1), st,
@@ -1102,34 +1128,31 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   ts.phase("inner_sumcheck");
   const bool inner_on_device = sumcheck_pow_bits(s.security_bits, 2) == 0;
   if (inner_on_device) {
-    const FinishConsts fc = finish_consts(job.p16);
-    DevPhase ph(ctx, ts, n, 24, inner_sum, kb::ef_one());
-    // round 0 evaluates A and B as they are, round r >= 1 folds them at challenge r - 1 and
-    // evaluates in one pass; the last challenge's fold leaves the final values
+    DevPhase ph(ctx, ts, n, 24, inner_sum, kb::ef_one(), job.p16);
+    // round 0 evaluates A and B as they are (the finish its own kernel); round r >= 1 folds
+    // them at challenge r - 1, evaluates and finishes in one kernel; the last challenge's fold
+    // leaves the final values
     for (int round = 0; round < n; round++) {
       const size_t half = N >> (round + 1);
-      int nb;
-      ef* part;
       if (round == 0) {
-        nb = prod_blocks(half);
-        part = ctx.partials(size_t(nb) * 2);
-        ProfScope _ps(ctx, "prod_eval");
-        launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st);
+        const int nb = prod_blocks(half);
+        ef* part = ctx.partials(size_t(nb) * 2);
+        {
+          ProfScope _ps(ctx, "prod_eval");
+          launch_prod_eval(A.as<ef>(), B.as<ef>(), half, part, st);
+        }
+        ph.finish_round(FIN_PROD, part, nb);
       } else {
-        nb = fold_eval_blocks(half);
-        part = ctx.partials(size_t(nb) * 2);
+        ef* part = ctx.partials(size_t(2) * fold_eval_blocks(half));
         DBuf na(sizeof(ef) * 2 * half, st), nbuf(sizeof(ef) * 2 * half, st);
         {
           ProfScope _ps(ctx, "fold_eval");
           launch_pair_fold_eval(2, A.as<ef>(), B.as<ef>(), ph.chs + (round - 1), na.as<ef>(), nbuf.as<ef>(), half, part,
-                                st);
+                                &ph.fin, st);
         }
         A = std::move(na);
         B = std::move(nbuf);
       }
-      int nr = nb;
-      const ef* red = ctx.reduce_wide(part, nr, 2);
-      { ProfScope _ps(ctx, "round_finish"); launch_prod_round_finish(red, nr, fc, ph.st, ph.words, ph.chs, st); }
     }
     {
       DBuf na(sizeof(ef), st), nbuf(sizeof(ef), st);
@@ -1397,8 +1420,7 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
   if (n - k >= 1 && sumcheck_pow_bits(128, 3) == 0) {
     // rounds >= 1 with the transcript on the device; per-round times from events recorded at
     // the round boundaries, read after the phase
-    const FinishConsts fc = finish_consts(p16);
-    DevPhase ph(ctx, ts, n - k, 32, sum, mmf);
+    DevPhase ph(ctx, ts, n - k, 32, sum, mmf, p16, r.data() + 1);
     std::vector<cudaEvent_t> ev(n - k + 1);
     for (auto& e : ev) WL_CUDA(cudaEventCreate(&e));
     WL_CUDA(cudaEventRecord(ev[0], st));
@@ -1408,29 +1430,25 @@ std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int n, i
     for (int round = 1; round <= n - k; round++) {
       const int m = n - k - round + 1;
       const size_t half = size_t(1) << (m - 1);
-      int nb;
-      ef* part;
       if (round == 1) {
-        nb = (int)((half + 31) / 32);
-        part = ctx.partials(size_t(nb) * 2);
-        ProfScope _ps(ctx, "abc_eval_ef");
-        launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st);
+        const int nb = (int)((half + 31) / 32);
+        ef* part = ctx.partials(size_t(nb) * 2);
+        {
+          ProfScope _ps(ctx, "abc_eval_ef");
+          launch_abc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), part, st);
+        }
+        ph.finish_round(FIN_EQSC3, part, nb);
       } else {
-        nb = fold_eval_blocks(half);
-        part = ctx.partials(size_t(nb) * 2);
+        ef* part = ctx.partials(size_t(2) * fold_eval_blocks(half));
         DBuf nc(sizeof(ef) * 3 * 2 * half, st), eqn(sizeof(ef) * half, st);
         {
           ProfScope _ps(ctx, "fold_eval");
           launch_abc_fold_eval(cols.as<ef>(), ph.chs + (round - 2), eqr.as<ef>(), nc.as<ef>(), eqn.as<ef>(), half, part,
-                               st);
+                               &ph.fin, st);
         }
         cols = std::move(nc);
         eqr = std::move(eqn);
       }
-      const ef& rr = r[round];
-      int nr = nb;
-      const ef* red = ctx.reduce_wide(part, nr, 2);
-      { ProfScope _ps(ctx, "round_finish"); launch_eqsc_round_finish(3, red, nr, rr, kb::ef_inv(rr), fc, ph.st, ph.words, ph.chs, st); }
       if (round == n - k) {
         DBuf nc(sizeof(ef) * 3, st);
         { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 3, 1, ph.chs + (round - 1), st); }
