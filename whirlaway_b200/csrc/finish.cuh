@@ -19,12 +19,17 @@ namespace {
 constexpr unsigned FIN_FULL = 0xffffffffu;
 
 // Shared-memory part of a finish: the permutation's constants and the round's reduced sums.
+// One instance per block (fin_sm), so that the finish code addresses it as shared memory.
 struct FinSmem {
-  uint32_t rc[8][16];               // full-round constants: rounds 0-3 initial, 4-7 terminal
-  uint32_t ci[kb::P16Consts::RP];  // partial-round constants
-  uint32_t diag[16];                // internal-layer diagonal (Montgomery form)
-  ef red[4];                        // the round's sums, reduced over the partial rows
+  uint32_t rc[8][16];                             // full-round constants: rounds 0-3 initial, 4-7 terminal
+  uint32_t ci[kb::P16Consts::RP];                 // partial-round constants
+  uint32_t diag[16];                              // internal-layer diagonal V_i (Montgomery form)
+  uint32_t dpow[16][kb::P16Consts::RP];           // V_i^j
+  uint32_t csum[kb::P16Consts::RP];               // V_1^j + ... + V_15^j
+  ef red[4];                                      // the round's sums, reduced over the partial rows
+  ef tmp[FIN_MAX_THREADS / 32];                   // per-warp partial sums of the reduction
 };
+__shared__ FinSmem fin_sm;
 
 // The challenger, spread over warp 0: state word (lane & 15), pending input (lane & 7),
 // squeezed output (lane & 7); the lengths are the same in every lane.
@@ -35,15 +40,22 @@ struct FinCh {
 
 __device__ __forceinline__ int fin_lane() { return threadIdx.x & 31; }
 
-// Every thread of the block may call it; a block barrier must follow before warp 0 uses sm.
-__device__ __forceinline__ void fin_load_consts(FinSmem& sm, const FinishConsts* __restrict__ fc) {
-  for (int t = threadIdx.x; t < 128 + kb::P16Consts::RP + 16; t += blockDim.x) {
-    if (t < 128)
-      sm.rc[t >> 4][t & 15] = (t >> 4) < 4 ? fc->p16.ext_init[t] : fc->p16.ext_term[t - 64];
-    else if (t < 128 + kb::P16Consts::RP)
-      sm.ci[t - 128] = fc->p16.internal[t - 128];
-    else
-      sm.diag[t - 128 - kb::P16Consts::RP] = kb::p2_diag<16>(t - 128 - kb::P16Consts::RP);
+// Every thread of the block may call it; a block barrier must follow before warp 0 uses fin_sm.
+__device__ __forceinline__ void fin_load_consts(const FinishConsts* __restrict__ fc) {
+  constexpr int RP = kb::P16Consts::RP;
+  for (int t = threadIdx.x; t < 128 + RP + 16 + 17 * RP; t += blockDim.x) {
+    if (t < 128) {
+      fin_sm.rc[t >> 4][t & 15] = (t >> 4) < 4 ? fc->p16.ext_init[t] : fc->p16.ext_term[t - 64];
+    } else if (t < 128 + RP) {
+      fin_sm.ci[t - 128] = fc->p16.internal[t - 128];
+    } else if (t < 128 + RP + 16) {
+      fin_sm.diag[t - 128 - RP] = kb::p2_diag<16>(t - 128 - RP);
+    } else if (t < 128 + RP + 16 + 16 * RP) {
+      const int q = t - 128 - RP - 16;
+      fin_sm.dpow[q / RP][q % RP] = fc->dpow[q / RP][q % RP];
+    } else {
+      fin_sm.csum[t - 128 - RP - 16 - 16 * RP] = fc->csum[t - 128 - RP - 16 - 16 * RP];
+    }
   }
 }
 
@@ -71,52 +83,84 @@ __device__ __forceinline__ void fin_ch_store(DevChallenger& c, const FinCh& f) {
 }
 
 // External layer across the 16 lanes of a half-warp: row i of circ(2, 3, 1, 1) within the
-// 4-word chunk, then the sum of that position over the four chunks.
+// 4-word chunk, plus the sum of that position over the four chunks (gathered in one step).
 __device__ __forceinline__ uint32_t fin_m4(uint32_t a, int i) {
   const int base = i & ~3;
   const uint32_t b = __shfl_sync(FIN_FULL, a, base | ((i + 1) & 3), 16);
   const uint32_t c = __shfl_sync(FIN_FULL, a, base | ((i + 2) & 3), 16);
   const uint32_t d = __shfl_sync(FIN_FULL, a, base | ((i + 3) & 3), 16);
   const uint32_t y = kb::add(kb::add(kb::add(a, b), kb::add(c, d)), kb::add(a, kb::dbl(b)));
-  uint32_t t = kb::add(y, __shfl_xor_sync(FIN_FULL, y, 4, 16));
-  t = kb::add(t, __shfl_xor_sync(FIN_FULL, t, 8, 16));
-  return kb::add(y, t);
+  const uint32_t y4 = __shfl_xor_sync(FIN_FULL, y, 4, 16), y8 = __shfl_xor_sync(FIN_FULL, y, 8, 16);
+  const uint32_t y12 = __shfl_xor_sync(FIN_FULL, y, 12, 16);
+  return kb::add(kb::add(kb::add(y, y4), kb::add(y8, y12)), y);
 }
 
 // Poseidon2-16 (Montgomery form; the values of kb::p2_permute<16>) of the state whose word
-// (lane & 15) is v. Partial rounds: word 0 is carried in every lane (a), the other words in
-// their lanes; the sum of words 1..15 is two warp reductions of their 16-bit halves (each total
-// below 2^20), recombined with 2^31 = 2^24 - 1 (mod p), and does not wait for the S-box.
-__device__ __noinline__ uint32_t fin_perm(uint32_t v, const FinSmem& sm) {
+// (lane & 15) is v.
+//
+// The partial rounds are rewritten so that only the S-box is serial. With x_r the S-box output
+// of round r, S_r the state sum after it and s_i the words after the first full rounds, word
+// i >= 1 after r rounds is V_i^r s_i + sum_{q<r} V_i^(r-1-q) S_q, so the sum of words 1..15
+// entering round r is T_r = M_r + sum_{q<r} C_(r-1-q) S_q with the moments
+// M_r = sum_i V_i^r s_i and C_k = sum_i V_i^k (C_0 = 15). Word 0 entering round r + 1 is
+// S_r - 2 x_r = T_r - x_r (V_0 = -2, S_r = x_r + T_r), so
+//   x_(r+1) = (T_r + c_(r+1) - x_r)^3,
+// one subtraction and a cube per round, while T_(r+1) = (M_(r+1) + sum_(q<r) C_(r-q) S_q) +
+// 15 S_r is formed beside it: lane j < 20 holds the bracket for T_j (its moment, to which
+// every S_q with q <= j - 2 is added as it appears) and hands it over by one shuffle. The
+// words themselves follow their own recurrence s_i <- V_i s_i + S_r off the chain.
+__device__ __noinline__ uint32_t fin_perm(uint32_t v) {
+  constexpr int RP = kb::P16Consts::RP;
   const int lane = fin_lane(), i = lane & 15;
-  const uint32_t d = sm.diag[i];
   v = fin_m4(v, i);
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) v = fin_m4(kb::cube(kb::add(v, sm.rc[r][i])), i);
-  uint32_t a = __shfl_sync(FIN_FULL, v, 0);
-  const bool contrib = lane >= 1 && lane < 16;
-#pragma unroll 1
-  for (int r = 0; r < kb::P16Consts::RP; r++) {
-    const uint32_t x0 = kb::cube(kb::add(a, sm.ci[r]));
-    const uint32_t w = contrib ? v : 0u;
-    const uint32_t lo = __reduce_add_sync(FIN_FULL, w & 0xffffu), hi = __reduce_add_sync(FIN_FULL, w >> 16);
-    uint32_t t = ((hi & 0x7fffu) << 16) + (hi >> 15) * 0xffffffu + lo;  // below 2^31 + 2^28 + 2^20 < 2p
-    t = kb::umin(t, t - kb::P);
-    const uint32_t S = kb::add(t, x0);
-    a = kb::sub(S, kb::dbl(x0));  // V_0 = -2
-    v = kb::add(kb::mul(v, d), S);
+  for (int r = 0; r < 4; r++) v = fin_m4(kb::cube(kb::add(v, fin_sm.rc[r][i])), i);
+  // moment M_lane = sum_{t=1..15} V_t^lane s_t (lanes < RP), four lazy groups of <= 4 products
+  const int j = lane < RP ? lane : 0;
+  uint64_t g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+#pragma unroll
+  for (int t = 1; t < 16; t++) {
+    const uint64_t pr = kb::wmul(__shfl_sync(FIN_FULL, v, t), fin_sm.dpow[t][j]);
+    if ((t & 3) == 0)
+      g0 += pr;
+    else if ((t & 3) == 1)
+      g1 += pr;
+    else if ((t & 3) == 2)
+      g2 += pr;
+    else
+      g3 += pr;
   }
-  v = i == 0 ? a : v;
+  uint32_t acc = kb::add(kb::add(kb::redc(g0), kb::redc(g1)), kb::add(kb::redc(g2), kb::redc(g3)));
+  const uint32_t d = fin_sm.diag[i], c0 = fin_sm.csum[0];  // C_0 = 15
+  uint32_t x = kb::cube(kb::add(__shfl_sync(FIN_FULL, v, 0), fin_sm.ci[0]));
+  uint32_t T = __shfl_sync(FIN_FULL, acc, 0);  // T_0 = M_0
 #pragma unroll 1
-  for (int r = 4; r < 8; r++) v = fin_m4(kb::cube(kb::add(v, sm.rc[r][i])), i);
+  for (int r = 0; r < RP - 1; r++) {
+    const uint32_t S = kb::add(x, T);
+    v = kb::add(kb::mul(v, d), S);
+    const uint32_t u = kb::sub(kb::add(T, fin_sm.ci[r + 1]), x);
+    const int k = lane - 1 - r;  // lane >= r + 2 takes C_(lane-1-r) S_r
+    const bool take = k >= 1 && lane < RP;
+    const uint32_t ck = fin_sm.csum[take ? k : 0];
+    acc = take ? kb::add(acc, kb::mul(ck, S)) : acc;
+    T = kb::add(__shfl_sync(FIN_FULL, acc, r + 1), kb::mul(S, c0));
+    x = kb::cube(u);
+  }
+  {
+    const uint32_t S = kb::add(x, T);
+    v = kb::add(kb::mul(v, d), S);
+    v = i == 0 ? kb::sub(T, x) : v;
+  }
+#pragma unroll 1
+  for (int r = 4; r < 8; r++) v = fin_m4(kb::cube(kb::add(v, fin_sm.rc[r][i])), i);
   return v;
 }
 
 // Duplexing: the pending inputs overwrite the first in_len words of the state, which is
 // permuted; the rate part becomes the output.
-__device__ __forceinline__ void fin_duplex(FinCh& c, const FinSmem& sm) {
+__device__ __forceinline__ void fin_duplex(FinCh& c) {
   const int lane = fin_lane(), i = lane & 15;
-  c.st = fin_perm((i < 8 && i < c.in_len) ? c.in : c.st, sm);
+  c.st = fin_perm((i < 8 && i < c.in_len) ? c.in : c.st);
   c.out = __shfl_sync(FIN_FULL, c.st, lane & 7);
   c.in_len = 0;
   c.out_len = 8;
@@ -126,15 +170,14 @@ __device__ __forceinline__ void fin_duplex(FinCh& c, const FinSmem& sm) {
 // proof[plen..] and into the challenger, one observation each. With L words already pending,
 // the first 8 - L fill the rate and duplex, the other L are left pending (and the output is
 // then empty, as any observation leaves it).
-__device__ __forceinline__ void fin_observe_ext(FinCh& c, uint32_t x, uint32_t* __restrict__ proof, uint32_t plen,
-                                                const FinSmem& sm) {
+__device__ __forceinline__ void fin_observe_ext(FinCh& c, uint32_t x, uint32_t* __restrict__ proof, uint32_t plen) {
   const int lane = fin_lane(), k = lane & 7;
   if (lane < 8) proof[plen + lane] = x;
   const int L = c.in_len;
   const uint32_t first = __shfl_sync(FIN_FULL, x, (k - L) & 7);  // lane k >= L: word k - L
   c.in = k >= L ? first : c.in;
   c.in_len = 8;
-  fin_duplex(c, sm);
+  fin_duplex(c);
   if (L) {
     const uint32_t second = __shfl_sync(FIN_FULL, x, (k + 8 - L) & 7);  // lane k < L: word k + 8 - L
     c.in = k < L ? second : c.in;
@@ -145,16 +188,16 @@ __device__ __forceinline__ void fin_observe_ext(FinCh& c, uint32_t x, uint32_t* 
 
 // Transcript::sample_ext: eight samples, each popped from the end of the output (duplexing
 // first when inputs are pending or the output is empty); sample k is coordinate k.
-__device__ __forceinline__ uint32_t fin_sample_ext(FinCh& c, const FinSmem& sm) {
+__device__ __forceinline__ uint32_t fin_sample_ext(FinCh& c) {
   const int k = fin_lane() & 7;
-  if (c.in_len || !c.out_len) fin_duplex(c, sm);
+  if (c.in_len || !c.out_len) fin_duplex(c);
   const int O = c.out_len;
   const uint32_t a = __shfl_sync(FIN_FULL, c.out, (O - 1 - k) & 7);  // sample k < O: out[O - 1 - k]
   if (O == 8) {
     c.out_len = 0;
     return a;
   }
-  fin_duplex(c, sm);  // the output ran out after O samples
+  fin_duplex(c);  // the output ran out after O samples
   const uint32_t b = __shfl_sync(FIN_FULL, c.out, (7 - (k - O)) & 7);  // sample k >= O: out[7 - (k - O)]
   c.out_len = O;
   return k < O ? a : b;
@@ -189,9 +232,7 @@ __device__ __forceinline__ uint32_t fin_coord(const ef& e) {
   return x;
 }
 
-// Sum over `nb` rows of `nsum` interleaved extension sums (partial[row * nsum + z], written by
-// other blocks of this grid or an earlier one: read past L1) into sm.red[z]. Every thread of
-// the block calls it; tmp holds blockDim.x values; sm.red is valid in warp 0 on return.
+// An extension element written by another block, read past L1.
 __device__ __forceinline__ ef fin_ldcg(const ef* p) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
   const uint4 u = __ldcg(q), v = __ldcg(q + 1);
@@ -200,22 +241,25 @@ __device__ __forceinline__ ef fin_ldcg(const ef* p) {
   e.c[4] = v.x, e.c[5] = v.y, e.c[6] = v.z, e.c[7] = v.w;
   return e;
 }
-__device__ void fin_reduce_rows(const ef* __restrict__ partial, int nb, int nsum, FinSmem& sm, ef* tmp) {
-  const int t = threadIdx.x, T = int(blockDim.x / nsum) * nsum;
-  const int n = nb * nsum;
+// Sum over `nb` rows of `nsum` interleaved extension sums (partial[row * nsum + z], written by
+// other blocks of this grid or an earlier one) into fin_sm.red[z]. Every thread of the block
+// calls it (blockDim.x a multiple of 32, at least 32 nsum); warp w sums rows of sum w % nsum,
+// then warp 0 adds the warps' totals; fin_sm.red is valid in warp 0 on return.
+__device__ void fin_reduce_rows(const ef* __restrict__ partial, int nb, int nsum) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int z = w % nsum, wz = w / nsum, nwz = (nw - 1 - z) / nsum + 1;  // warps wz of the nwz on sum z
   ef acc = kb::ef_zero();
-  if (t < T) {
 #pragma unroll 4
-    for (int j = t; j < n; j += T) acc = kb::ef_add(acc, fin_ldcg(partial + j));
-  }
-  tmp[t] = acc;
+  for (int row = wz * 32 + lane; row < nb; row += nwz * 32) acc = kb::ef_add(acc, fin_ldcg(partial + size_t(row) * nsum + z));
+  acc = warp_reduce_ef(acc);
+  if (lane == 0) fin_sm.tmp[w] = acc;
   __syncthreads();
-  if (t < 32) {
-    const int z = t >> 3, k = t & 7;
-    if (z < nsum) {
+  if (threadIdx.x < 32) {
+    const int zz = lane >> 3, k = lane & 7;
+    if (zz < nsum) {
       uint32_t s = 0;
-      for (int u = z; u < T; u += nsum) s = kb::add(s, tmp[u].c[k]);
-      sm.red[z].c[k] = s;
+      for (int u = zz; u < nw; u += nsum) s = kb::add(s, fin_sm.tmp[u].c[k]);
+      fin_sm.red[zz].c[k] = s;
     }
     __syncwarp();
   }
@@ -232,7 +276,7 @@ __device__ void fin_reduce_rows(const ef* __restrict__ partial, int nb, int nsum
 // polynomial is the interpolation on 0..NPTS-1 times (1 - r) + (2r - 1) X: NPTS + 1
 // coefficients.
 template <int NPTS>
-__device__ __noinline__ void fin_round_eqsc(const FinArgs& a, const FinSmem& sm) {
+__device__ __noinline__ void fin_round_eqsc(const FinArgs& a) {
   const int lane = fin_lane();
   const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
@@ -244,9 +288,9 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a, const FinSmem& sm)
   const uint32_t one = fin_base(kb::R_MOD_P);
   const uint32_t omr = kb::sub(one, r), lin = kb::sub(kb::add(r, r), one);
   uint32_t e[NPTS];
-  e[0] = fin_mul(sm.red[0].c[lane & 7], mmf);
+  e[0] = fin_mul(fin_sm.red[0].c[lane & 7], mmf);
 #pragma unroll
-  for (int i = 2; i < NPTS; i++) e[i] = fin_mul(sm.red[i - 1].c[lane & 7], mmf);
+  for (int i = 2; i < NPTS; i++) e[i] = fin_mul(fin_sm.red[i - 1].c[lane & 7], mmf);
   e[1] = fin_mul(kb::sub(sum, fin_mul(e[0], omr)), rinv);
   uint32_t q[NPTS];
 #pragma unroll
@@ -261,10 +305,10 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a, const FinSmem& sm)
     uint32_t v = k < NPTS ? fin_mul(q[k], omr) : 0u;
     if (k > 0) v = kb::add(v, fin_mul(q[k - 1], lin));
     p[k] = v;
-    fin_observe_ext(c, v, a.proof, plen, sm);
+    fin_observe_ext(c, v, a.proof, plen);
     plen += 8;
   }
-  const uint32_t ch = fin_sample_ext(c, sm);
+  const uint32_t ch = fin_sample_ext(c);
   uint32_t s = p[NPTS];
 #pragma unroll
   for (int k = NPTS - 1; k >= 0; k--) s = kb::add(fin_mul(s, ch), p[k]);
@@ -284,24 +328,24 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a, const FinSmem& sm)
 
 // Round of the product sumcheck (the inner sumcheck): sums at 0 and 2, the value at 1 from the
 // claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
-__device__ __noinline__ void fin_round_prod(const FinArgs& a, const FinSmem& sm) {
+__device__ __noinline__ void fin_round_prod(const FinArgs& a) {
   const int lane = fin_lane();
   const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
   const int round = stp->round;
   uint32_t plen = stp->proof_len;
   FinCh c = fin_ch_load(stp->ch);
-  const uint32_t y0 = sm.red[0].c[lane & 7], y2 = sm.red[1].c[lane & 7];
+  const uint32_t y0 = fin_sm.red[0].c[lane & 7], y2 = fin_sm.red[1].c[lane & 7];
   const uint32_t y1 = kb::sub(fin_coord(stp->sum), y0);
   uint32_t p[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     p[k] = kb::add(kb::add(kb::mul(y0, fc->basis[0][0][k]), kb::mul(y1, fc->basis[0][1][k])),
                    kb::mul(y2, fc->basis[0][2][k]));
-    fin_observe_ext(c, p[k], a.proof, plen, sm);
+    fin_observe_ext(c, p[k], a.proof, plen);
     plen += 8;
   }
-  const uint32_t ch = fin_sample_ext(c, sm);
+  const uint32_t ch = fin_sample_ext(c);
   const uint32_t s = kb::add(fin_mul(kb::add(fin_mul(p[2], ch), p[1]), ch), p[0]);
   __syncwarp();
   fin_ch_store(stp->ch, c);
@@ -318,7 +362,7 @@ __device__ __noinline__ void fin_round_prod(const FinArgs& a, const FinSmem& sm)
 // Round of the WHIR folding sumcheck: h(0), h(1), h(2) go to the proof as they are; the next
 // claim is h(r) by quadratic interpolation on 0, 1, 2:
 // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2.
-__device__ __noinline__ void fin_round_whir(const FinArgs& a, const FinSmem& sm) {
+__device__ __noinline__ void fin_round_whir(const FinArgs& a) {
   const int lane = fin_lane();
   const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
@@ -328,11 +372,11 @@ __device__ __noinline__ void fin_round_whir(const FinArgs& a, const FinSmem& sm)
   uint32_t h[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    h[k] = sm.red[k].c[lane & 7];
-    fin_observe_ext(c, h[k], a.proof, plen, sm);
+    h[k] = fin_sm.red[k].c[lane & 7];
+    fin_observe_ext(c, h[k], a.proof, plen);
     plen += 8;
   }
-  const uint32_t r = fin_sample_ext(c, sm);
+  const uint32_t r = fin_sample_ext(c);
   const uint32_t rm1 = kb::sub(r, fin_base(fc->one)), rm2 = kb::sub(r, fin_base(fc->two));
   const uint32_t t0 = kb::mul(fin_mul(fin_mul(h[0], rm1), rm2), fc->inv2);
   const uint32_t t1 = fin_mul(fin_mul(h[1], r), rm2);
@@ -353,35 +397,35 @@ __device__ __noinline__ void fin_round_whir(const FinArgs& a, const FinSmem& sm)
 __device__ __forceinline__ int fin_kind_sums_dev(int kind) { return kind == FIN_EQSC4 || kind == FIN_WHIR ? 3 : 2; }
 
 // Dispatch on the round kind (warp 0 only).
-__device__ __forceinline__ void fin_round(int kind, const FinArgs& a, const FinSmem& sm) {
+__device__ __forceinline__ void fin_round(int kind, const FinArgs& a) {
   if (kind == FIN_EQSC4)
-    fin_round_eqsc<4>(a, sm);
+    fin_round_eqsc<4>(a);
   else if (kind == FIN_EQSC3)
-    fin_round_eqsc<3>(a, sm);
+    fin_round_eqsc<3>(a);
   else if (kind == FIN_PROD)
-    fin_round_prod(a, sm);
+    fin_round_prod(a);
   else
-    fin_round_whir(a, sm);
+    fin_round_whir(a);
 }
 
 // Epilogue of a kernel whose blocks each wrote one row of `nsum` partial sums (thread 0 of the
 // block, before the call): the block that arrives last reduces all gridDim.x rows and finishes
 // the round. Every thread of every block calls it, after its own stores.
 __device__ __forceinline__ void fin_last_block(int kind, const FinArgs& a, const ef* __restrict__ partial, int nsum) {
-  __shared__ FinSmem sm;
-  __shared__ ef tmp[FIN_MAX_THREADS];
   __shared__ int last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&a.st->arrived, 1u) == gridDim.x - 1;
+  __syncthreads();  // thread 0 has written this block's row
+  if (threadIdx.x == 0) {
+    __threadfence();  // the row before the count
+    last = atomicAdd(&a.st->arrived, 1u) == gridDim.x - 1;
+    if (last) __threadfence();  // every other row is visible to this block's reads
+  }
   __syncthreads();
   if (!last) return;
-  __threadfence();
-  fin_load_consts(sm, a.fc);
-  fin_reduce_rows(partial, gridDim.x, nsum, sm, tmp);
+  fin_load_consts(a.fc);
+  fin_reduce_rows(partial, gridDim.x, nsum);
   __syncthreads();
   if (threadIdx.x < 32) {
-    fin_round(kind, a, sm);
+    fin_round(kind, a);
     if (threadIdx.x == 0) a.st->arrived = 0;  // for the next round's grid
   }
 }
