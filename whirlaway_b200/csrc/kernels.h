@@ -219,16 +219,12 @@ struct DevRound {
   uint32_t arrived;
 };
 // Constants of the round finish: Poseidon2-16 (Montgomery), the Lagrange bases on the nodes
-// 0..2 and 0..3 (basis[0][i][k], basis[1][i][k]: coefficient k of basis polynomial i), the
-// Montgomery forms of 1, 2 and 1/2, and for the partial rounds the powers of the internal
-// diagonal, dpow[i][j] = V_i^j (i = 1..15, j < 20; row 0 unused) and their column sums
-// csum[j] = V_1^j + ... + V_15^j (Montgomery form).
+// 0..2 and 0..3 (basis[0][i][k], basis[1][i][k]: coefficient k of basis polynomial i) and the
+// Montgomery forms of 1, 2 and 1/2.
 struct FinishConsts {
   kb::P16Consts p16;
   uint32_t basis[2][4][4];
   uint32_t one, two, inv2;
-  uint32_t dpow[16][kb::P16Consts::RP];
-  uint32_t csum[kb::P16Consts::RP];
 };
 // Round kinds: eq-factor rounds with 4 computed points (the AIR zerocheck's rounds >= 1) or 3
 // (the a*b - c zerocheck), the product sumcheck (inner sumcheck), the WHIR folding sumcheck.

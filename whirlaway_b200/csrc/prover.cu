@@ -365,21 +365,6 @@ DBuf eq_table_dev(Context& ctx, const std::vector<ef>& pt) {
 DBuf scalar_dev(Context& ctx, const ef& v) { return upload(ctx, std::vector<ef>{v}); }
 
 // Constants of the round-finishing kernels for one proof.
-// The powers of the Poseidon2-16 internal diagonal that the round finish's partial rounds use
-// (V_i^j for i = 1..15, j < 20, and their sums over i; Montgomery form).
-void fill_partial_round_powers(FinishConsts& fc) {
-  constexpr int RP = kb::P16Consts::RP;
-  for (int j = 0; j < RP; j++) fc.csum[j] = 0;
-  for (int j = 0; j < RP; j++) fc.dpow[0][j] = 0;
-  for (int i = 1; i < 16; i++) {
-    uint32_t pw = kb::R_MOD_P;
-    for (int j = 0; j < RP; j++) {
-      fc.dpow[i][j] = pw;
-      fc.csum[j] = kb::add(fc.csum[j], pw);
-      pw = kb::mul(pw, kb::p2_diag<16>(i));
-    }
-  }
-}
 FinishConsts finish_consts(const kb::P16Consts& p16) {
   FinishConsts fc;
   fc.p16 = p16;
@@ -391,7 +376,6 @@ FinishConsts finish_consts(const kb::P16Consts& p16) {
   fc.one = fm(1);
   fc.two = fm(2);
   fc.inv2 = kb::inv_m(fm(2));
-  fill_partial_round_powers(fc);
   return fc;
 }
 
