@@ -24,6 +24,9 @@ struct FinSmem {
   uint32_t rc[8][16];                             // full-round constants: rounds 0-3 initial, 4-7 terminal
   uint32_t ci[kb::P16Consts::RP];                 // partial-round constants
   uint32_t diag[16];                              // internal-layer diagonal V_i (Montgomery form)
+  uint32_t basis[2][4][4], one, two, inv2;        // FinishConsts' interpolation constants
+  DevRound st;                                    // the phase state on entry
+  ef r, rinv;                                     // eq-factor rounds: the round's eq challenge and inverse
   ef red[4];                                      // the round's sums, reduced over the partial rows
   ef tmp[FIN_MAX_THREADS / 32];                   // per-warp partial sums of the reduction
 };
@@ -38,16 +41,38 @@ struct FinCh {
 
 __device__ __forceinline__ int fin_lane() { return threadIdx.x & 31; }
 
-// Every thread of the block may call it; a block barrier must follow before warp 0 uses fin_sm.
-__device__ __forceinline__ void fin_load_consts(const FinishConsts* __restrict__ fc) {
+// Everything the finish reads, into fin_sm, by every thread of the block at once (the loads
+// are independent, so their latencies overlap; warp 0 then reads shared memory only). A block
+// barrier must follow before warp 0 uses fin_sm.
+__device__ __forceinline__ void fin_load(int kind, const FinArgs& a) {
   constexpr int RP = kb::P16Consts::RP;
-  for (int t = threadIdx.x; t < 128 + RP + 16; t += blockDim.x) {
-    if (t < 128)
+  constexpr int NST = int(sizeof(DevRound) / 4);
+  constexpr int A = 128, B = A + RP, C = B + 16, D = C + 32, E = D + NST, F = E + 16;
+  const FinishConsts* __restrict__ fc = a.fc;
+  const bool eq = kind == FIN_EQSC4 || kind == FIN_EQSC3;
+  for (int t = threadIdx.x; t < F; t += blockDim.x) {
+    if (t < A) {
       fin_sm.rc[t >> 4][t & 15] = (t >> 4) < 4 ? fc->p16.ext_init[t] : fc->p16.ext_term[t - 64];
-    else if (t < 128 + RP)
-      fin_sm.ci[t - 128] = fc->p16.internal[t - 128];
-    else
-      fin_sm.diag[t - 128 - RP] = kb::p2_diag<16>(t - 128 - RP);
+    } else if (t < B) {
+      fin_sm.ci[t - A] = fc->p16.internal[t - A];
+    } else if (t < C) {
+      fin_sm.diag[t - B] = kb::p2_diag<16>(t - B);
+    } else if (t < D) {
+      (&fin_sm.basis[0][0][0])[t - C] = (&fc->basis[0][0][0])[t - C];
+    } else if (t < E) {
+      reinterpret_cast<uint32_t*>(&fin_sm.st)[t - D] = reinterpret_cast<const uint32_t*>(a.st)[t - D];
+    } else if (eq) {
+      const int q = t - E, round = a.st->round;
+      if (q < 8)
+        fin_sm.r.c[q] = a.req[round].c[q];
+      else
+        fin_sm.rinv.c[q - 8] = a.rinv[round].c[q - 8];
+    }
+  }
+  if (threadIdx.x == 0) {
+    fin_sm.one = fc->one;
+    fin_sm.two = fc->two;
+    fin_sm.inv2 = fc->inv2;
   }
 }
 
@@ -169,8 +194,9 @@ __device__ __forceinline__ uint32_t fin_sample_ext(FinCh& c) {
 
 // Extension-field product in F[X]/(X^8 - 3), coordinate (lane & 7) of a * b within each group
 // of eight lanes: the dot product of a with (b_k, ..., b_0, 3 b_7, ..., 3 b_{k+1}) in two lazy
-// halves of four terms.
-__device__ __noinline__ uint32_t fin_mul(uint32_t a, uint32_t b) {
+// halves of four terms. Inlined: as a call it measured twice the cycles (the call saves and
+// restores the caller's live registers).
+__device__ __forceinline__ uint32_t fin_mul(uint32_t a, uint32_t b) {
   const int lane = fin_lane(), k = lane & 7, g = lane & 24;
   const uint32_t b3 = kb::add(kb::dbl(b), b);
   uint64_t s0 = 0, s1 = 0;
@@ -188,13 +214,8 @@ __device__ __noinline__ uint32_t fin_mul(uint32_t a, uint32_t b) {
 }
 // The base-field constant c as an extension coordinate: c at coordinate 0, zero elsewhere.
 __device__ __forceinline__ uint32_t fin_base(uint32_t c) { return (fin_lane() & 7) == 0 ? c : 0u; }
-__device__ __forceinline__ uint32_t fin_coord(const ef& e) {
-  const int k = fin_lane() & 7;
-  uint32_t x = e.c[0];
-#pragma unroll
-  for (int u = 1; u < 8; u++) x = k == u ? e.c[u] : x;
-  return x;
-}
+// Coordinate (lane & 7) of an extension element in shared memory.
+__device__ __forceinline__ uint32_t fin_coord(const ef& e) { return e.c[fin_lane() & 7]; }
 
 // An extension element written by another block, read past L1.
 __device__ __forceinline__ ef fin_ldcg(const ef* p) {
@@ -242,13 +263,12 @@ __device__ void fin_reduce_rows(const ef* __restrict__ partial, int nb, int nsum
 template <int NPTS>
 __device__ __noinline__ void fin_round_eqsc(const FinArgs& a) {
   const int lane = fin_lane();
-  const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
-  const int round = stp->round;
-  uint32_t plen = stp->proof_len;
-  FinCh c = fin_ch_load(stp->ch);
-  const uint32_t sum = fin_coord(stp->sum), mmf = fin_coord(stp->mmf);
-  const uint32_t r = fin_coord(a.req[round]), rinv = fin_coord(a.rinv[round]);
+  const int round = fin_sm.st.round;
+  uint32_t plen = fin_sm.st.proof_len;
+  FinCh c = fin_ch_load(fin_sm.st.ch);
+  const uint32_t sum = fin_coord(fin_sm.st.sum), mmf = fin_coord(fin_sm.st.mmf);
+  const uint32_t r = fin_coord(fin_sm.r), rinv = fin_coord(fin_sm.rinv);
   const uint32_t one = fin_base(kb::R_MOD_P);
   const uint32_t omr = kb::sub(one, r), lin = kb::sub(kb::add(r, r), one);
   uint32_t e[NPTS];
@@ -261,7 +281,7 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a) {
   for (int k = 0; k < NPTS; k++) {
     q[k] = 0;
 #pragma unroll
-    for (int i = 0; i < NPTS; i++) q[k] = kb::add(q[k], kb::mul(e[i], fc->basis[NPTS - 3][i][k]));
+    for (int i = 0; i < NPTS; i++) q[k] = kb::add(q[k], kb::mul(e[i], fin_sm.basis[NPTS - 3][i][k]));
   }
   uint32_t p[NPTS + 1];
 #pragma unroll
@@ -269,7 +289,10 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a) {
     uint32_t v = k < NPTS ? fin_mul(q[k], omr) : 0u;
     if (k > 0) v = kb::add(v, fin_mul(q[k - 1], lin));
     p[k] = v;
-    fin_observe_ext(c, v, a.proof, plen);
+  }
+#pragma unroll
+  for (int k = 0; k <= NPTS; k++) {
+    fin_observe_ext(c, p[k], a.proof, plen);
     plen += 8;
   }
   const uint32_t ch = fin_sample_ext(c);
@@ -294,18 +317,19 @@ __device__ __noinline__ void fin_round_eqsc(const FinArgs& a) {
 // claim; the round polynomial (3 coefficients) interpolates 0, 1, 2.
 __device__ __noinline__ void fin_round_prod(const FinArgs& a) {
   const int lane = fin_lane();
-  const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
-  const int round = stp->round;
-  uint32_t plen = stp->proof_len;
-  FinCh c = fin_ch_load(stp->ch);
+  const int round = fin_sm.st.round;
+  uint32_t plen = fin_sm.st.proof_len;
+  FinCh c = fin_ch_load(fin_sm.st.ch);
   const uint32_t y0 = fin_sm.red[0].c[lane & 7], y2 = fin_sm.red[1].c[lane & 7];
-  const uint32_t y1 = kb::sub(fin_coord(stp->sum), y0);
+  const uint32_t y1 = kb::sub(fin_coord(fin_sm.st.sum), y0);
   uint32_t p[3];
 #pragma unroll
+  for (int k = 0; k < 3; k++)
+    p[k] = kb::add(kb::add(kb::mul(y0, fin_sm.basis[0][0][k]), kb::mul(y1, fin_sm.basis[0][1][k])),
+                   kb::mul(y2, fin_sm.basis[0][2][k]));
+#pragma unroll
   for (int k = 0; k < 3; k++) {
-    p[k] = kb::add(kb::add(kb::mul(y0, fc->basis[0][0][k]), kb::mul(y1, fc->basis[0][1][k])),
-                   kb::mul(y2, fc->basis[0][2][k]));
     fin_observe_ext(c, p[k], a.proof, plen);
     plen += 8;
   }
@@ -328,11 +352,10 @@ __device__ __noinline__ void fin_round_prod(const FinArgs& a) {
 // h(r) = h0 (r-1)(r-2)/2 - h1 r (r-2) + h2 r (r-1)/2.
 __device__ __noinline__ void fin_round_whir(const FinArgs& a) {
   const int lane = fin_lane();
-  const FinishConsts* fc = a.fc;
   DevRound* stp = a.st;
-  const int round = stp->round;
-  uint32_t plen = stp->proof_len;
-  FinCh c = fin_ch_load(stp->ch);
+  const int round = fin_sm.st.round;
+  uint32_t plen = fin_sm.st.proof_len;
+  FinCh c = fin_ch_load(fin_sm.st.ch);
   uint32_t h[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -341,10 +364,10 @@ __device__ __noinline__ void fin_round_whir(const FinArgs& a) {
     plen += 8;
   }
   const uint32_t r = fin_sample_ext(c);
-  const uint32_t rm1 = kb::sub(r, fin_base(fc->one)), rm2 = kb::sub(r, fin_base(fc->two));
-  const uint32_t t0 = kb::mul(fin_mul(fin_mul(h[0], rm1), rm2), fc->inv2);
+  const uint32_t rm1 = kb::sub(r, fin_base(fin_sm.one)), rm2 = kb::sub(r, fin_base(fin_sm.two));
+  const uint32_t t0 = kb::mul(fin_mul(fin_mul(h[0], rm1), rm2), fin_sm.inv2);
   const uint32_t t1 = fin_mul(fin_mul(h[1], r), rm2);
-  const uint32_t t2 = kb::mul(fin_mul(fin_mul(h[2], r), rm1), fc->inv2);
+  const uint32_t t2 = kb::mul(fin_mul(fin_mul(h[2], r), rm1), fin_sm.inv2);
   const uint32_t s = kb::add(kb::sub(t0, t1), t2);
   __syncwarp();
   fin_ch_store(stp->ch, c);
@@ -385,7 +408,7 @@ __device__ __forceinline__ void fin_last_block(int kind, const FinArgs& a, const
   }
   __syncthreads();
   if (!last) return;
-  fin_load_consts(a.fc);
+  fin_load(kind, a);
   fin_reduce_rows(partial, gridDim.x, nsum);
   __syncthreads();
   if (threadIdx.x < 32) {

@@ -25,7 +25,7 @@ namespace {
 // One round's finish as its own kernel: the block reduces the partial rows, warp 0 finishes.
 __global__ void __launch_bounds__(FIN_MAX_THREADS, 1) k_round_finish(int kind, const ef* __restrict__ partial, int nb,
                                                                      const FinArgs a) {
-  fin_load_consts(a.fc);
+  fin_load(kind, a);
   fin_reduce_rows(partial, nb, fin_kind_sums_dev(kind));
   __syncthreads();
   if (threadIdx.x < 32) fin_round(kind, a);
