@@ -104,6 +104,44 @@ wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t*
 wl_status wl_prove_witness(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants,
                            const wl_witness* w, uint32_t* proof_out, size_t* proof_len, double* timings_ms);
 
+/* An AIR beyond the built-in Poseidon2 one, given as a constraint program. It replaces the
+ * reference's AirTable over an arbitrary p3-air Air (crates/air/src/table.rs:15-60,
+ * crates/air/src/prove.rs:49-226, crates/air/src/verify.rs:55-249). There are n_columns witness
+ * columns, and the constraints are evaluated on every row's up values (the row; the last row
+ * repeats the one before it) and down values (the next row; the last row repeats itself), as
+ * crates/air/src/utils.rs:140-160 builds them.
+ * `ops` holds n_ops instructions of three int32 (op, a, b); instruction i computes value v_i:
+ *   WL_AIR_UP c, WL_AIR_DOWN c    column c's up / down value (c < n_columns)
+ *   WL_AIR_CONST j                consts[j] (canonical, j < n_consts)
+ *   WL_AIR_ADD, _SUB, _MUL a b    v_a op v_b (a, b < i)
+ *   WL_AIR_EMIT a                 the next constraint is v_a (v_i = v_a)
+ * The EMITs, in order, are the n_constraints constraints, batched as sum_i alpha^i C_i.
+ * constraint_degree (1..3) bounds every constraint's degree. At most 64 values may be live at
+ * once (the device interpreter's register file); n_columns <= 32767. No preprocessed columns. */
+enum { WL_AIR_UP = 0, WL_AIR_DOWN = 1, WL_AIR_CONST = 2, WL_AIR_ADD = 3, WL_AIR_SUB = 4, WL_AIR_MUL = 5,
+       WL_AIR_EMIT = 6 };
+typedef struct {
+  int32_t n_columns;
+  int32_t n_constraints;
+  int32_t constraint_degree;
+  int32_t n_ops;
+  const int32_t* ops;
+  int32_t n_consts;
+  const uint32_t* consts;
+} wl_air_program;
+/* Proves the program's AIR for a host witness (n_columns x 2^log_n canonical values,
+ * column-major). hash_constants: Poseidon16 (148) | Poseidon24 (215) constants, as in a
+ * constants blob after its AIR part. No reference counterpart beyond AirTable::prove. */
+wl_status wl_prove_program(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* hash_constants,
+                           const wl_air_program* program, int32_t log_n, const uint32_t* witness_colmajor,
+                           uint32_t* proof_out, size_t* proof_len);
+/* Verifies such a proof on the host (AirTable::verify); returns WL_OK or the verifier's error. */
+wl_status wl_verify_program(const wl_air_settings* settings, const uint32_t* hash_constants,
+                            const wl_air_program* program, int32_t log_n, const uint32_t* proof, size_t proof_len);
+/* Upper bound of the proof length (u32 words) of wl_prove_program. */
+wl_status wl_program_proof_len_bound(const wl_air_settings* settings, const wl_air_program* program, int32_t log_n,
+                                     size_t* out);
+
 /* Batch of independent proofs (each with its own witness and transcript), run back to back
  * on the context's stream; proofs are written at proof_out + i * stride. */
 wl_status wl_prove_batch(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* constants, int32_t n,

@@ -8,6 +8,8 @@
 // round, in permutation order: 148 constraints, all of degree 3. The AIR reads the
 // local row only (no transition constraints), so the "down" half of the zerocheck
 // point is not used by the constraint polynomial.
+#include <stdexcept>
+
 #include "oracle.h"
 
 namespace wlo {
@@ -86,6 +88,52 @@ EF air_eval_base(const AirConstants& c, const F* up, const std::vector<EF>& alph
 }
 EF air_eval_ext(const AirConstants& c, const EF* up, const std::vector<EF>& alphas) {
   return air_eval_t<EF>(c, up, alphas);
+}
+
+// ---------------------------------------------------------------- constraint programs
+template <class T>
+static EF program_eval_t(const ProgramAirSpec& p, const T* ud, const std::vector<EF>& alphas) {
+  std::vector<T> v(p.code.size());
+  EF acc;
+  int ci = 0;
+  for (size_t i = 0; i < p.code.size(); i++) {
+    const AirInstr& in = p.code[i];
+    switch (in.op) {
+      case AIR_OP_UP: v[i] = ud[in.a]; break;
+      case AIR_OP_DOWN: v[i] = ud[p.W + in.a]; break;
+      case AIR_OP_CONST: v[i] = T(p.consts[in.a]); break;
+      case AIR_OP_ADD: v[i] = v[in.a] + v[in.b]; break;
+      case AIR_OP_SUB: v[i] = v[in.a] - v[in.b]; break;
+      case AIR_OP_MUL: v[i] = v[in.a] * v[in.b]; break;
+      default:  // AIR_OP_EMIT
+        acc += alphas[ci++] * v[in.a];
+        v[i] = v[in.a];
+        break;
+    }
+  }
+  return acc;
+}
+EF ProgramAirSpec::eval_base(const F* ud, const std::vector<EF>& a) const { return program_eval_t<F>(*this, ud, a); }
+EF ProgramAirSpec::eval_ext(const EF* ud, const std::vector<EF>& a) const { return program_eval_t<EF>(*this, ud, a); }
+void ProgramAirSpec::check() const {
+  if (W < 1 || NC < 1 || deg < 1 || deg > 3) throw std::runtime_error("AIR program: bad width, count or degree");
+  int emits = 0;
+  for (size_t i = 0; i < code.size(); i++) {
+    const AirInstr& in = code[i];
+    const bool two = in.op == AIR_OP_ADD || in.op == AIR_OP_SUB || in.op == AIR_OP_MUL;
+    if (in.op == AIR_OP_UP || in.op == AIR_OP_DOWN) {
+      if (in.a < 0 || in.a >= W) throw std::runtime_error("AIR program: column out of range");
+    } else if (in.op == AIR_OP_CONST) {
+      if (in.a < 0 || in.a >= (int)consts.size()) throw std::runtime_error("AIR program: constant out of range");
+    } else if (two || in.op == AIR_OP_EMIT) {
+      if (in.a < 0 || in.a >= (int)i || (two && (in.b < 0 || in.b >= (int)i)))
+        throw std::runtime_error("AIR program: operand is not an earlier value");
+      emits += in.op == AIR_OP_EMIT;
+    } else {
+      throw std::runtime_error("AIR program: unknown instruction");
+    }
+  }
+  if (emits != NC) throw std::runtime_error("AIR program: constraint count mismatch");
 }
 
 }  // namespace wlo

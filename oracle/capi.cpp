@@ -49,6 +49,18 @@ Poseidon2 perm_from(int width, const uint32_t* c) {
 }
 // constants blob: AIR (148) | P16 (148) | P24 (215)
 constexpr int AIR_NC = 2 * 4 * 16 + 20, P16_NC = 8 * 16 + 20, P24_NC = 8 * 24 + 23;
+// A constraint program from flat arrays: ops holds (op, a, b) per instruction.
+ProgramAirSpec program_from(int W, int n_constraints, int degree, int n_ops, const int32_t* ops, int n_consts,
+                            const uint32_t* consts) {
+  ProgramAirSpec p;
+  p.W = W;
+  p.NC = n_constraints;
+  p.deg = degree;
+  for (int i = 0; i < n_ops; i++) p.code.push_back({ops[3 * i], ops[3 * i + 1], ops[3 * i + 2]});
+  for (int i = 0; i < n_consts; i++) p.consts.push_back(F(consts[i]));
+  p.check();
+  return p;
+}
 }  // namespace
 
 extern "C" {
@@ -123,6 +135,43 @@ int wlo_verify(const int32_t* settings, const uint32_t* constants, int log_n, co
     std::vector<F> pr(proof_len);
     for (size_t i = 0; i < proof_len; i++) pr[i] = F::raw(proof[i] % P);
     return verify_air(s, a, h, log_n, pr);
+  } catch (const std::exception&) {
+    return 100;
+  }
+}
+
+// An AIR given as a constraint program (hash_consts: P16 (148) | P24 (215)); witness: W
+// columns of 2^log_n values, column-major.
+int wlo_prove_program(const int32_t* settings, const uint32_t* hash_consts, int W, int n_constraints, int degree,
+                      int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int log_n,
+                      const uint32_t* witness, uint32_t* proof, size_t* proof_len) {
+  try {
+    Settings s = settings_from(settings);
+    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts);
+    Hashes h{perm_from(16, hash_consts), perm_from(24, hash_consts + P16_NC)};
+    size_t N = size_t(1) << log_n;
+    std::vector<F> w(size_t(W) * N);
+    for (size_t i = 0; i < w.size(); i++) w[i] = F::raw(witness[i]);
+    std::vector<F> pr = prove_air_spec(s, air, h, log_n, w);
+    if (*proof_len < pr.size()) { *proof_len = pr.size(); return -2; }
+    for (size_t i = 0; i < pr.size(); i++) proof[i] = pr[i].v;
+    *proof_len = pr.size();
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
+
+int wlo_verify_program(const int32_t* settings, const uint32_t* hash_consts, int W, int n_constraints, int degree,
+                       int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int log_n,
+                       const uint32_t* proof, size_t proof_len) {
+  try {
+    Settings s = settings_from(settings);
+    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts);
+    Hashes h{perm_from(16, hash_consts), perm_from(24, hash_consts + P16_NC)};
+    std::vector<F> pr(proof_len);
+    for (size_t i = 0; i < proof_len; i++) pr[i] = F::raw(proof[i] % P);
+    return verify_air_spec(s, air, h, log_n, pr);
   } catch (const std::exception&) {
     return 100;
   }

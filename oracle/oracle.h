@@ -168,6 +168,52 @@ void air_trace_row(const AirConstants& c, const F* input16, F* row);
 EF air_eval_base(const AirConstants& c, const F* up, const std::vector<EF>& alphas);
 EF air_eval_ext(const AirConstants& c, const EF* up, const std::vector<EF>& alphas);
 
+// ---------------------------------------------------------------- AIRs in general
+// What the AIR prover and verifier need of an AIR (crates/air/src/table.rs:15-60: width,
+// constraint count, constraint degree; the constraints as p3-air's ConstraintFolder sees
+// them): the batched value sum_i alphas[i] C_i over a point holding the up values of the W
+// columns followed by their down values (crates/air/src/utils.rs:140-160).
+struct AirSpec {
+  virtual ~AirSpec() = default;
+  virtual int columns() const = 0;
+  virtual int constraints() const = 0;
+  virtual int degree() const = 0;
+  virtual EF eval_base(const F* ud, const std::vector<EF>& alphas) const = 0;
+  virtual EF eval_ext(const EF* ud, const std::vector<EF>& alphas) const = 0;
+};
+// The Poseidon2-KoalaBear width-16 AIR above (reads the up values only).
+struct Poseidon2AirSpec : AirSpec {
+  const AirConstants& c;
+  explicit Poseidon2AirSpec(const AirConstants& k) : c(k) {}
+  int columns() const override { return AIR_COLS; }
+  int constraints() const override { return AIR_CONSTRAINTS; }
+  int degree() const override { return 3; }
+  EF eval_base(const F* ud, const std::vector<EF>& a) const override { return air_eval_base(c, ud, a); }
+  EF eval_ext(const EF* ud, const std::vector<EF>& a) const override { return air_eval_ext(c, ud, a); }
+};
+// An AIR given as a constraint program: instruction i computes value v_i from
+//   UP c / DOWN c (column c's up / down value), CONST j (consts[j]),
+//   ADD / SUB / MUL a b (v_a op v_b, a and b < i), EMIT a (the next constraint is v_a; v_i = v_a).
+// The constraints are the EMITs in program order.
+enum AirOpCode { AIR_OP_UP = 0, AIR_OP_DOWN = 1, AIR_OP_CONST = 2, AIR_OP_ADD = 3, AIR_OP_SUB = 4, AIR_OP_MUL = 5,
+                 AIR_OP_EMIT = 6 };
+struct AirInstr {
+  int op, a, b;
+};
+struct ProgramAirSpec : AirSpec {
+  int W = 0, NC = 0, deg = 0;
+  std::vector<AirInstr> code;
+  std::vector<F> consts;
+  int columns() const override { return W; }
+  int constraints() const override { return NC; }
+  int degree() const override { return deg; }
+  EF eval_base(const F* ud, const std::vector<EF>& a) const override;
+  EF eval_ext(const EF* ud, const std::vector<EF>& a) const override;
+  // Throws unless every operand refers to an earlier value, a column < W or a constant, and
+  // the EMITs number NC.
+  void check() const;
+};
+
 // ---------------------------------------------------------------- settings
 struct Settings {
   int security_bits = 128;
@@ -223,9 +269,12 @@ struct Hashes {
 struct ProveTimings { double commit = 0, zerocheck = 0, inner = 0, whir = 0; };
 std::vector<F> prove_air(const Settings& s, const AirConstants& air, const Hashes& h, int log_n,
                          const std::vector<F>& witness_colmajor, ProveTimings* t = nullptr);
+std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n,
+                              const std::vector<F>& witness_colmajor, ProveTimings* t = nullptr);
 enum VerifyStatus { V_OK = 0, V_INVALID_PCS_COMMITMENT = 1, V_INVALID_PCS_OPENING = 2, V_FS = 3,
                     V_SUMCHECK = 4, V_BOUNDARY = 5, V_SUM_MISMATCH = 6 };
 int verify_air(const Settings& s, const AirConstants& air, const Hashes& h, int log_n, const std::vector<F>& proof);
+int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n, const std::vector<F>& proof);
 
 // Standalone zerocheck of eq(r,x) * (a*b - c) (a, b, c base-field multilinears).
 std::vector<F> prove_abc(const Poseidon2& p16, int log_n, int skips, const std::vector<F>& a,

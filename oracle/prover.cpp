@@ -197,11 +197,11 @@ static Cols sumcheck_prove(int skips, const std::vector<std::vector<NF>>& mls, c
 
 // ------------------------------------------------------------ computations
 struct AirComputation : Computation {
-  const AirConstants& c;
+  const AirSpec& air;
   const std::vector<EF>& alphas;
-  AirComputation(const AirConstants& c, const std::vector<EF>& a) : c(c), alphas(a) {}
-  EF eval_f(const F* pt) const override { return air_eval_base(c, pt, alphas); }
-  EF eval_e(const EF* pt) const override { return air_eval_ext(c, pt, alphas); }
+  AirComputation(const AirSpec& a, const std::vector<EF>& al) : air(a), alphas(al) {}
+  EF eval_f(const F* pt) const override { return air.eval_base(pt, alphas); }
+  EF eval_e(const EF* pt) const override { return air.eval_ext(pt, alphas); }
 };
 struct ProductComputation : Computation {  // InnerSumcheckCircuit (crates/air/src/prove.rs:229-235)
   EF eval_f(const F* pt) const override { return EF(pt[0] * pt[1]); }
@@ -243,7 +243,12 @@ static double now_s() {
 
 std::vector<F> prove_air(const Settings& s, const AirConstants& air, const Hashes& h, int log_n,
                          const std::vector<F>& witness, ProveTimings* tm) {
-  const int W = AIR_COLS, n = log_n, k = s.univariate_skips;
+  return prove_air_spec(s, Poseidon2AirSpec(air), h, log_n, witness, tm);
+}
+
+std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n,
+                              const std::vector<F>& witness, ProveTimings* tm) {
+  const int W = air.columns(), NC = air.constraints(), n = log_n, k = s.univariate_skips;
   if (k >= n) throw std::runtime_error("univariate_skips must be < log_n_rows");
   const size_t N = size_t(1) << n;
   if (witness.size() != size_t(W) * N) throw std::runtime_error("witness size mismatch");
@@ -261,11 +266,11 @@ std::vector<F> prove_air(const Settings& s, const AirConstants& air, const Hashe
   double t1 = now_s();
 
   // 2) batching scalars and zerocheck challenges
-  ts.grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(AIR_CONSTRAINTS))));
+  ts.grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(NC))));
   EF alpha = ts.sample_ext();
-  std::vector<EF> alphas(AIR_CONSTRAINTS);
+  std::vector<EF> alphas(NC);
   alphas[0] = ef_one();
-  for (int i = 1; i < AIR_CONSTRAINTS; i++) alphas[i] = alphas[i - 1] * alpha;
+  for (int i = 1; i < NC; i++) alphas[i] = alphas[i - 1] * alpha;
   ts.grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - n)));
   std::vector<EF> zc(n + 1 - k);
   for (auto& x : zc) x = ts.sample_ext();
@@ -282,7 +287,7 @@ std::vector<F> prove_air(const Settings& s, const AirConstants& air, const Hashe
   }
   AirComputation comp(air, alphas);
   ScState st;
-  Cols fin = sumcheck_prove<F>(k, ud, comp, 3, &zc, true, ts, EF(), n - k + 1, s.security_bits, st);
+  Cols fin = sumcheck_prove<F>(k, ud, comp, air.degree(), &zc, true, ts, EF(), n - k + 1, s.security_bits, st);
   std::vector<EF> zc_ch = st.challenges;
   double t2 = now_s();
 

@@ -71,7 +71,11 @@ static EF matrix_down_lde(const std::vector<EF>& pt) {
 }
 
 int verify_air(const Settings& s, const AirConstants& air, const Hashes& h, int log_n, const std::vector<F>& proof) {
-  const int W = AIR_COLS, n = log_n, k = s.univariate_skips;
+  return verify_air_spec(s, Poseidon2AirSpec(air), h, log_n, proof);
+}
+
+int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n, const std::vector<F>& proof) {
+  const int W = air.columns(), NC = air.constraints(), n = log_n, k = s.univariate_skips;
   const int logW = log2_up(W);
   WhirConfig cfg = WhirConfig::build(n + logW, s);
   Transcript ts(&h.p16);
@@ -80,15 +84,16 @@ int verify_air(const Settings& s, const AirConstants& air, const Hashes& h, int 
   Digest root;
   std::vector<std::pair<std::vector<EF>, EF>> ood;
   if (!whir_parse_commitment(cfg, ts, root, ood)) return V_INVALID_PCS_COMMITMENT;
-  if (!ts.check_grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(AIR_CONSTRAINTS))))) return V_FS;
+  if (!ts.check_grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(NC))))) return V_FS;
   EF alpha = ts.sample_ext();
   if (!ts.check_grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - n)))) return V_FS;
   std::vector<EF> zc(n - k + 1);
   for (auto& x : zc) x = ts.sample_ext();
 
   // verify_with_univariate_skip(degree = constraint_degree + 1)
-  std::vector<int> degs{4 * ((1 << k) - 1)}, sets{1 << k};
-  for (int i = 0; i < n - k; i++) { degs.push_back(4); sets.push_back(2); }
+  const int d1 = air.degree() + 1;
+  std::vector<int> degs{d1 * ((1 << k) - 1)}, sets{1 << k};
+  for (int i = 0; i < n - k; i++) { degs.push_back(d1); sets.push_back(2); }
   ScClaim outer;
   if (int e = verify_core(ts, degs, sets, s.security_bits, outer)) return e;
   if (!outer.sum.is_zero()) return V_SUM_MISMATCH;
@@ -103,10 +108,10 @@ int verify_air(const Settings& s, const AirConstants& air, const Hashes& h, int 
   }
   std::vector<EF> global(2 * W);
   for (int c = 0; c < W; c++) { global[c] = wup[c]; global[W + c] = wdown[c]; }
-  std::vector<EF> alphas(AIR_CONSTRAINTS);
+  std::vector<EF> alphas(NC);
   alphas[0] = ef_one();
-  for (int i = 1; i < AIR_CONSTRAINTS; i++) alphas[i] = alphas[i - 1] * alpha;
-  EF constraint_eval = air_eval_ext(air, global.data(), alphas);
+  for (int i = 1; i < NC; i++) alphas[i] = alphas[i - 1] * alpha;
+  EF constraint_eval = air.eval_ext(global.data(), alphas);
   EF dot;
   for (int i = 0; i < (1 << k); i++) dot += zc_sel[i] * outer_sel[i];
   std::vector<EF> zc_tail(zc.begin() + 1, zc.end()), outer_tail(outer.point.begin() + 1, outer.point.end());

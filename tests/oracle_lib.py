@@ -29,6 +29,10 @@ class Oracle:
         lib.wlo_prove_abc.argtypes = [_u32p, ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, _u32p,
                                       ctypes.POINTER(ctypes.c_size_t)]
         lib.wlo_verify_abc.argtypes = [_u32p, ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_size_t]
+        prog_args = [_i32p, _u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, _u32p,
+                     ctypes.c_int]
+        lib.wlo_prove_program.argtypes = prog_args + [_u32p, _u32p, ctypes.POINTER(ctypes.c_size_t)]
+        lib.wlo_verify_program.argtypes = prog_args + [_u32p, ctypes.c_size_t]
         lib.wlo_chacha_block.argtypes = [_u32p, ctypes.c_uint64, ctypes.c_int, _u32p]
         lib.wlo_stdrng_u32.argtypes = [ctypes.c_uint64, _u32p, ctypes.c_size_t]
         lib.wlo_poseidon2.argtypes = [ctypes.c_int, _u32p, _u32p]
@@ -65,6 +69,28 @@ class Oracle:
         s = settings.ctypes.data_as(_i32p) if settings is not None else None
         proof = np.ascontiguousarray(proof, dtype=np.uint32)
         return self.lib.wlo_verify(s, _p(consts), log_n, _p(proof), proof.size)
+
+    def _program_args(self, settings, hash_consts, prog, log_n):
+        s = settings.ctypes.data_as(_i32p) if settings is not None else None
+        hc = np.ascontiguousarray(hash_consts, np.uint32)
+        return [s, _p(hc), prog.width, prog.n_constraints, prog.degree, prog.ops.shape[0],
+                prog.ops.ctypes.data_as(_i32p), prog.consts.size, _p(prog.consts), log_n], hc
+
+    def prove_program(self, log_n, hash_consts, prog, witness, settings=None):
+        """A proof for the AIR given as a constraint program (hash_consts: P16 | P24 constants)."""
+        args, keep = self._program_args(settings, hash_consts, prog, log_n)
+        w = np.ascontiguousarray(witness, np.uint32)
+        cap = 1 << 22
+        out = np.zeros(cap, np.uint32)
+        n = ctypes.c_size_t(cap)
+        rc = self.lib.wlo_prove_program(*args, _p(w), _p(out), ctypes.byref(n))
+        assert rc == 0, rc
+        return out[: n.value].copy()
+
+    def verify_program(self, log_n, hash_consts, prog, proof, settings=None):
+        args, keep = self._program_args(settings, hash_consts, prog, log_n)
+        proof = np.ascontiguousarray(proof, dtype=np.uint32)
+        return self.lib.wlo_verify_program(*args, _p(proof), proof.size)
 
     def prove_abc(self, p16, log_n, skips, a, b, c):
         cap = 1 << 16

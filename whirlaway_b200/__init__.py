@@ -36,6 +36,20 @@ class ProverError(RuntimeError):
         super().__init__(f"{STATUS.get(status, status)}: {message}")
 
 
+class _AirProgram(ctypes.Structure):
+    _fields_ = [("n_columns", ctypes.c_int32), ("n_constraints", ctypes.c_int32),
+                ("constraint_degree", ctypes.c_int32), ("n_ops", ctypes.c_int32),
+                ("ops", ctypes.POINTER(ctypes.c_int32)), ("n_consts", ctypes.c_int32),
+                ("consts", ctypes.POINTER(ctypes.c_uint32))]
+
+
+def _program_c(prog):
+    """The C description of an air_program.AirProgram (the arrays stay owned by prog)."""
+    return _AirProgram(prog.width, prog.n_constraints, prog.degree, prog.ops.shape[0],
+                       prog.ops.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), prog.consts.size,
+                       prog.consts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+
+
 class _Settings(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in (
         "security_bits", "log_inv_rate", "fold_first", "fold_rest", "univariate_skips",
@@ -100,6 +114,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                          _sizep, vp]),
         "wl_proof_footprint_bytes": (ctypes.c_uint64, [ctypes.POINTER(_Settings), ctypes.c_int32]),
         "wl_verify": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32, _u32p, ctypes.c_size_t]),
+        "wl_prove_program": (ctypes.c_int, [vp, ctypes.POINTER(_Settings), _u32p, ctypes.POINTER(_AirProgram),
+                                            ctypes.c_int32, _u32p, _u32p, _sizep]),
+        "wl_verify_program": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.POINTER(_AirProgram),
+                                             ctypes.c_int32, _u32p, ctypes.c_size_t]),
+        "wl_program_proof_len_bound": (ctypes.c_int, [ctypes.POINTER(_Settings), ctypes.POINTER(_AirProgram),
+                                                      ctypes.c_int32, _sizep]),
         "wl_sumcheck_abc_verify": (ctypes.c_int, [_u32p, ctypes.c_int32, ctypes.c_int32, _u32p, ctypes.c_size_t]),
         "wl_verify_batch": (ctypes.c_int, [ctypes.POINTER(_Settings), _u32p, ctypes.c_int32,
                                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_u32p), _sizep,
@@ -329,6 +349,38 @@ class AirTable:
         if w.log_n != self.log_n:
             raise ValueError("witness height does not match the table")
         return self._call(self.ctx._lib.wl_prove_witness, w.handle)
+
+
+def prove_program(ctx: Context, hash_constants: np.ndarray, program, log_n: int, witness_colmajor: np.ndarray,
+                  settings: AirSettings = AirSettings()) -> np.ndarray:
+    """AirTable::prove for an AIR given as a constraint program (air_program.AirProgram) with a
+    host witness (program.width columns of 2^log_n canonical values, column-major);
+    hash_constants: the Poseidon16 | Poseidon24 constants (363 u32). Returns proof_data."""
+    lib = ctx._lib
+    pc = _program_c(program)
+    hc = np.ascontiguousarray(hash_constants, dtype=np.uint32)
+    w = np.ascontiguousarray(witness_colmajor, dtype=np.uint32).reshape(-1)
+    if w.size != program.width << log_n:
+        raise ValueError("witness must hold program.width columns of 2^log_n values")
+    cap = ctypes.c_size_t()
+    ctx.check(lib.wl_program_proof_len_bound(ctypes.byref(settings._c()), ctypes.byref(pc), log_n, ctypes.byref(cap)),
+              "program_proof_len_bound")
+    out = np.zeros(cap.value, np.uint32)
+    n = ctypes.c_size_t(cap.value)
+    ctx.check(lib.wl_prove_program(ctx.handle, ctypes.byref(settings._c()), _ptr(hc), ctypes.byref(pc), log_n, _ptr(w),
+                                   _ptr(out), ctypes.byref(n)), "prove_program")
+    return out[: n.value].copy()
+
+
+def verify_program(hash_constants: np.ndarray, program, log_n: int, proof: np.ndarray,
+                   settings: AirSettings = AirSettings()) -> int:
+    """AirTable::verify for a constraint-program AIR on the host: 0 when accepted, else the
+    verifier status (as verify)."""
+    pc = _program_c(program)
+    hc = np.ascontiguousarray(hash_constants, dtype=np.uint32)
+    pr = np.ascontiguousarray(proof, dtype=np.uint32)
+    return load_library().wl_verify_program(ctypes.byref(settings._c()), _ptr(hc), ctypes.byref(pc), log_n, _ptr(pr),
+                                            pr.size)
 
 
 def sumcheck_abc_prove(ctx: Context, p16_constants: np.ndarray, log_n: int, skips: int, a, b, c, device=False):

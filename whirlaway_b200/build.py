@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libwhirlaway_b200.so")
-SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_transcript.cu", "k_verify.cu", "prover.cu", "server.cu", "noalloc.cu", "verifier.cu", "capi.cu",
-           "host_perm.cpp", "tuner.cpp"]
+SOURCES = ["k_commit.cu", "k_sumcheck.cu", "k_whir.cu", "k_transcript.cu", "k_verify.cu", "k_program.cu", "prover.cu",
+           "server.cu", "noalloc.cu", "verifier.cu", "capi.cu", "air_program.cu", "host_perm.cpp", "tuner.cpp"]
 # Integer-pipe throughput probes: a separate library that only the benchmark loads.
 PROBE_SRC = os.path.join("probe", "int_peaks.cu")
 PROBE_LIB = os.path.join(OUT_DIR, "libwl_probe.so")

@@ -1,0 +1,39 @@
+// AIRs beyond the built-in Poseidon2-KoalaBear one, given as constraint programs (the
+// reference proves any p3-air Air through AirTable, crates/air/src/table.rs:15-60). A program
+// is a list of SSA instructions over the up and down values of the W columns
+// (crates/air/src/utils.rs:140-160); its EMITs, in order, are the constraints batched as
+// sum_i alpha^i C_i. For the device the SSA values are assigned to a small register file
+// (linear scan: a value's register is freed after its last use), so that the interpreter
+// kernels keep PROG_MAX_REGS values per thread.
+#pragma once
+#include <vector_types.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "kb.cuh"
+
+namespace wl {
+
+enum ProgOp { PROG_UP = 0, PROG_DOWN = 1, PROG_CONST = 2, PROG_ADD = 3, PROG_SUB = 4, PROG_MUL = 5, PROG_EMIT = 6 };
+constexpr int PROG_MAX_REGS = 64;
+
+struct ProgramAir {
+  int W = 0, NC = 0, degree = 0;
+  std::vector<int32_t> ops;      // (op, a, b) per instruction, as given
+  std::vector<uint32_t> consts;  // Montgomery form
+  // Device form: x = op | dst << 8 | a << 16 (a: a column, a constant or a register), y = b (a
+  // register); EMIT's register is its operand's.
+  std::vector<uint2> code;
+  int nregs = 0;
+
+  // Validates (columns and constants in range, operands earlier values, NC EMITs, degree
+  // 1..3, at most PROG_MAX_REGS live values) and compiles; throws std::invalid_argument.
+  // consts_canonical: the constants as canonical values.
+  static ProgramAir build(int W, int n_constraints, int degree, int n_ops, const int32_t* ops, int n_consts,
+                          const uint32_t* consts_canonical);
+  // sum_i alphas[i] C_i at a point of up values up[0..W) and down values down[0..W).
+  kb::ef eval_ef(const kb::ef* up, const kb::ef* down, const kb::ef* alphas) const;
+};
+
+}  // namespace wl

@@ -261,6 +261,67 @@ wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* consta
   });
 }
 
+namespace {
+// A constraint program from its C description (throws std::invalid_argument when malformed).
+wl::ProgramAir program_from(const wl_air_program* p) {
+  if (!p) throw std::invalid_argument("program is NULL");
+  return wl::ProgramAir::build(p->n_columns, p->n_constraints, p->constraint_degree, p->n_ops, p->ops, p->n_consts,
+                               p->consts);
+}
+wl::ProofJob make_program_job(const wl_air_settings* s, const uint32_t* hash_constants, int log_n,
+                              const wl::ProgramAir* prog) {
+  wl::ProofJob job;
+  job.settings = to_settings(s);
+  job.log_n = log_n;
+  job.p16 = wl::perm_consts_from<16>(hash_constants);
+  job.p24 = wl::perm_consts_from<24>(hash_constants + wl::N_P16_CONSTS);
+  job.prog = prog;
+  return job;
+}
+}  // namespace
+
+wl_status wl_prove_program(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* hash_constants,
+                           const wl_air_program* program, int32_t log_n, const uint32_t* witness,
+                           uint32_t* proof_out, size_t* proof_len) {
+  if (!ctx) return WL_E_INVALID_ARG;
+  std::string why;
+  if (!settings_ok(s, log_n, why)) return fail(ctx, WL_E_INVALID_ARG, why);
+  if (!witness || !hash_constants || !program || !proof_len) return fail(ctx, WL_E_INVALID_ARG, "NULL argument");
+  return guarded(ctx, [&] {
+    const wl::ProgramAir prog = program_from(program);
+    const wl::ProofJob job = make_program_job(s, hash_constants, log_n, &prog);
+    std::vector<uint32_t> pr = wl::prove_air_host(*ctx->c, job, witness, nullptr);
+    return emit_proof(ctx, pr, proof_out, proof_len);
+  });
+}
+
+wl_status wl_verify_program(const wl_air_settings* s, const uint32_t* hash_constants, const wl_air_program* program,
+                            int32_t log_n, const uint32_t* proof, size_t proof_len) {
+  std::string why;
+  if (!hash_constants || !program || (!proof && proof_len) || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
+  for (size_t i = 0; i < proof_len; i++)
+    if (proof[i] >= kb::P) return WL_E_INVALID_ARG;
+  return guarded(nullptr, [&] {
+    const wl::ProgramAir prog = program_from(program);
+    const wl::ProofJob job = make_program_job(s, hash_constants, log_n, &prog);
+    return wl_status(wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len, nullptr, 0,
+                                          nullptr, &prog));
+  });
+}
+
+wl_status wl_program_proof_len_bound(const wl_air_settings* s, const wl_air_program* program, int32_t log_n,
+                                     size_t* out) {
+  std::string why;
+  if (!out || !program || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
+  try {
+    const wl::ProgramAir prog = program_from(program);
+    *out = wl::proof_len_bound(to_settings(s), log_n, prog.W, prog.degree);
+    return WL_OK;
+  } catch (...) {
+    return WL_E_INVALID_ARG;
+  }
+}
+
 wl_status wl_prove_batch(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* constants, int32_t n,
                          const wl_witness* const* ws, uint32_t* proof_out, size_t stride, size_t* proof_lens) {
   if (!ctx || !ws || !proof_out || !proof_lens || n < 0) return fail(ctx, WL_E_INVALID_ARG, "bad batch arguments");

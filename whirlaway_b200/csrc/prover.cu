@@ -836,13 +836,13 @@ std::vector<uint32_t> to_canonical(const std::vector<uint32_t>& v) {
 
 }  // namespace
 
-size_t proof_len_bound(const Settings& s, int log_n) {
-  WhirSchedule w = WhirSchedule::build(log_n + AIR_LOG_W, s);
+size_t proof_len_bound(const Settings& s, int log_n, int W, int degree) {
+  WhirSchedule w = WhirSchedule::build(log_n + log2_up(size_t(W)), s);
   const int k = s.univariate_skips;
   size_t n = 8 + 8 * w.c[0].ood;                              // root + OOD answers
-  n += 8 * size_t(4 * ((1 << k) - 1) + 1);                    // zerocheck round 0
-  n += 8 * size_t(5) * (log_n - k);                           // zerocheck rounds >= 1
-  n += 8 * size_t(2 * AIR_W) + 8 * (size_t(1) << k);          // inner sums, sub-evaluations
+  n += 8 * size_t((degree + 1) * ((1 << k) - 1) + 1);         // zerocheck round 0
+  n += 8 * size_t(degree + 2) * (log_n - k);                  // zerocheck rounds >= 1
+  n += 8 * size_t(2 * W) + 8 * (size_t(1) << k);              // inner sums, sub-evaluations
   n += 8 * size_t(3) * log_n;                                 // inner sumcheck
   n += 16;                                                    // grinding witnesses (generous)
   n += 8 * 3 * size_t(w.num_vars);                            // WHIR sumcheck messages
@@ -855,14 +855,123 @@ size_t proof_len_bound(const Settings& s, int log_n) {
   return n;
 }
 
+// The zerocheck of an AIR given as a constraint program (air_program.h), round for round as
+// crates/sumcheck/src/prove.rs:97-254 runs it on the 2W up/down columns: the sums from the
+// interpreter kernels, the round polynomial and challenge on the host transcript, the fold of
+// all 2W columns after every round; the last folds are the up and down evaluations.
+void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const ProgramAir& prog, const uint32_t* wit,
+                       const DBuf& d_alphas, const std::vector<ef>& zc, const DBuf& eq0, std::vector<ef>& challenges,
+                       std::vector<ef>& up, std::vector<ef>& down) {
+  const Settings& s = job.settings;
+  const int n = job.log_n, k = s.univariate_skips, W = prog.W, d = prog.degree, nsk = 1 << k, R = n - k;
+  const size_t S = size_t(1) << R;
+  cudaStream_t st = ctx.stream;
+  const int n_code = (int)prog.code.size();
+  DBuf code = upload(ctx, prog.code);
+  std::vector<uint32_t> cv = prog.consts;
+  if (cv.empty()) cv.push_back(0);
+  DBuf consts = upload(ctx, cv);
+  const auto& sel = lagrange_basis_cached(nsk);
+  // round 0: the values at z < 2^k vanish; the kernel sums z = 2^k .. d (2^k - 1)
+  const int nz = d * (nsk - 1) - nsk + 1;
+  std::vector<ef> ys(nsk, kb::ef_zero());
+  if (nz > 0) {
+    std::vector<uint32_t> lw(size_t(nz) * nsk);
+    for (int zi = 0; zi < nz; zi++)
+      for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
+    DBuf d_lw = upload(ctx, lw);
+    const int B = prog_zc_blocks(S);
+    ef* part = ctx.partials(size_t(B) * nz);
+    {
+      ProfScope _ps(ctx, "prog_zc0");
+      launch_prog_zc0(wit, n, k, code.as<uint2>(), n_code, consts.as<uint32_t>(), nz, d_lw.as<uint32_t>(),
+                      eq0.as<ef>(), d_alphas.as<ef>(), part, st);
+    }
+    const std::vector<ef> sums = reduce_to_host(ctx, part, B, nz);
+    ys.insert(ys.end(), sums.begin(), sums.end());
+  }
+  std::vector<ef> p = interpolate(lagrange_basis_cached((int)ys.size()), ys);
+  std::vector<ef> qv(nsk);
+  for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], zc[0]);
+  p = poly_mul(p, interpolate(sel, qv));
+  const int deg0 = (d + 1) * (nsk - 1);
+  p.resize(deg0 + 1, kb::ef_zero());
+  ts.add_ext(p.data(), p.size());
+  const ef r0 = ts.sample_ext();
+  challenges.push_back(r0);
+  ef sum = poly_eval(p, r0);
+  grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, deg0));
+  std::vector<ef> selr(nsk);
+  ef mmf = kb::ef_zero();
+  for (int i = 0; i < nsk; i++) {
+    selr[i] = upoly_eval(sel[i], r0);
+    mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
+  }
+  DBuf cols(sizeof(ef) * size_t(2 * W) * S, st);
+  {
+    DBuf d_sel = upload(ctx, selr);
+    ProfScope _ps(ctx, "prog_fold0");
+    launch_prog_fold0(wit, n, k, W, d_sel.as<ef>(), cols.as<ef>(), st);
+  }
+  // rounds >= 1: sums at z = 0, 2, .., d; z = 1 from the claim
+  DBuf eqr;
+  if (R >= 1) {
+    eqr = DBuf(sizeof(ef) * (S / 2), st);
+    launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2);
+  }
+  const auto& basis = lagrange_basis_cached(d + 1);
+  for (int round = 1; round <= R; round++) {
+    const int m = R - round + 1;
+    const size_t half = size_t(1) << (m - 1);
+    const int B = prog_zc_blocks(half);
+    ef* part = ctx.partials(size_t(B) * d);
+    {
+      ProfScope _ps(ctx, "prog_zc_ef");
+      launch_prog_zc_ef(cols.as<ef>(), m, W, code.as<uint2>(), n_code, consts.as<uint32_t>(), d, eqr.as<ef>(),
+                        d_alphas.as<ef>(), part, st);
+    }
+    const std::vector<ef> sz = reduce_to_host(ctx, part, B, d);
+    const ef& r = zc[round];
+    std::vector<ef> e(d + 1);
+    e[0] = kb::ef_mul(sz[0], mmf);
+    for (int z = 2; z <= d; z++) e[z] = kb::ef_mul(sz[z - 1], mmf);
+    e[1] = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(e[0], kb::ef_sub(kb::ef_one(), r))), kb::ef_inv(r));
+    std::vector<ef> q = interpolate(basis, e);
+    q = poly_mul(q, {kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_add(r, r), kb::ef_one())});
+    q.resize(d + 2, kb::ef_zero());
+    ts.add_ext(q.data(), q.size());
+    const ef c = ts.sample_ext();
+    challenges.push_back(c);
+    sum = poly_eval(q, c);
+    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, d + 1));
+    mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
+                     mmf);
+    DBuf nc(sizeof(ef) * size_t(2 * W) * half, st);
+    DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+    {
+      ProfScope _ps(ctx, "fold");
+      launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), 2 * W, half, c, st, half >= 2 ? eqr.as<ef>() : nullptr,
+                          eqn.as<ef>(), half / 2);
+    }
+    cols = std::move(nc);
+    eqr = std::move(eqn);
+  }
+  std::vector<ef> fin(size_t(2) * W);
+  ctx.to_host(fin.data(), cols.as<ef>(), sizeof(ef) * fin.size());
+  up.assign(fin.begin(), fin.begin() + W);
+  down.assign(fin.begin() + W, fin.end());
+}
+
 std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit, Timings* tm,
                                 const std::vector<cudaEvent_t>* tile_ready) {
   const Settings& s = job.settings;
-  const int n = job.log_n, k = s.univariate_skips, W = AIR_W;
+  const ProgramAir* prog = job.prog;
+  const int n = job.log_n, k = s.univariate_skips, W = prog ? prog->W : AIR_W;
+  const int NC = prog ? prog->NC : AIR_NC, LOGW = log2_up(size_t(W));
   if (k >= n) throw std::invalid_argument("univariate_skips must be smaller than log_n_rows");
   if (s.fold_first != 7 || s.fold_rest != 4) throw std::invalid_argument("folding factors other than (7, 4)");
   const size_t N = size_t(1) << n, S = N >> k;
-  const int m0 = n + AIR_LOG_W;
+  const int m0 = n + LOGW;
   const WhirSchedule ws = WhirSchedule::build(m0, s);
   cudaStream_t st = ctx.stream;
   Transcript ts(&job.p16);
@@ -916,16 +1025,16 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
 
   // ---------------------------------------------------------------- 2) challenges
   ts.phase("batching");
-  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, log2_up(AIR_NC)));
+  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, log2_up(size_t(NC))));
   ef alpha = ts.sample_ext();
-  std::vector<ef> alphas(AIR_NC);
+  std::vector<ef> alphas(NC);
   alphas[0] = kb::ef_one();
-  for (int i = 1; i < AIR_NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
+  for (int i = 1; i < NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
   DBuf d_alphas = upload(ctx, alphas);
   // beta_f = MDS^T alpha_f for the 8 full rounds (constraints 16f.. for the beginning rounds,
   // 84 + 16(f - 4).. for the ending rounds); MDS = circ(2 M4, M4, M4, M4).
   std::vector<ef> betas(8 * 16, kb::ef_zero());
-  {
+  if (!prog) {
     static const int M4[4][4] = {{2, 3, 1, 1}, {1, 2, 3, 1}, {1, 1, 2, 3}, {3, 1, 1, 2}};
     for (int f = 0; f < 8; f++) {
       const int c0 = f < 4 ? 16 * f : 84 + 16 * (f - 4);
@@ -952,148 +1061,156 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
   std::vector<ef> zc_tail(zc.begin() + 1, zc.end());
   DBuf eq0 = eq_table_dev(ctx, zc_tail);
   std::vector<ef> challenges;
-  ef sum = kb::ef_zero();
-  ef mmf = kb::ef_one();
-  DBuf cols;
-  // the committed-column combination sum_i alpha_i col_(17+i) of every row; folded, it is the
-  // last of the W + 1 columns of the rounds >= 1
-  DBuf arow(sizeof(ef) * N, st);
-  {
-    std::vector<uint32_t> lw(size_t(nz) * nsk);
-    for (int zi = 0; zi < nz; zi++)
-      for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
-    DBuf d_lw = upload(ctx, lw);
-    const int nb = zc0_blocks(n, k), nbr = zc0_row_blocks(n);
-    ef* part = ctx.partials(size_t(nb + nbr) * nz);
+  std::vector<ef> inner_up(W), inner_down(W);
+  if (prog) {
+    zerocheck_program(ctx, ts, job, *prog, wit, d_alphas, zc, eq0, challenges, inner_up, inner_down);
+  } else {
+    ef sum = kb::ef_zero();
+    ef mmf = kb::ef_one();
+    DBuf cols;
+    // the committed-column combination sum_i alpha_i col_(17+i) of every row; folded, it is the
+    // last of the W + 1 columns of the rounds >= 1
+    DBuf arow(sizeof(ef) * N, st);
     {
-      DBuf q(sizeof(uint32_t) * ZC0_NQ * N, st);
-      { ProfScope _ps(ctx, "zc0_rows"); launch_zc0_rows(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, q.as<uint32_t>(), part + size_t(nb) * nz, arow.as<ef>(), st); }
-      { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, q.as<uint32_t>(), n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+      std::vector<uint32_t> lw(size_t(nz) * nsk);
+      for (int zi = 0; zi < nz; zi++)
+        for (int j = 0; j < nsk; j++) lw[size_t(zi) * nsk + j] = upoly_eval_f(sel[j], fm(nsk + zi));
+      DBuf d_lw = upload(ctx, lw);
+      const int nb = zc0_blocks(n, k), nbr = zc0_row_blocks(n);
+      ef* part = ctx.partials(size_t(nb + nbr) * nz);
+      {
+        DBuf q(sizeof(uint32_t) * ZC0_NQ * N, st);
+        { ProfScope _ps(ctx, "zc0_rows"); launch_zc0_rows(wit, n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), job.air, q.as<uint32_t>(), part + size_t(nb) * nz, arow.as<ef>(), st); }
+        { ProfScope _ps(ctx, "zc0_eval"); launch_zc0_eval(wit, q.as<uint32_t>(), n, k, nz, d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+      }
+      std::vector<ef> sums = reduce_to_host(ctx, part, nb + nbr, nz);
+      std::vector<ef> ys(nsk, kb::ef_zero());
+      ys.insert(ys.end(), sums.begin(), sums.end());
+      std::vector<ef> p = interpolate(lagrange_basis_cached((int)ys.size()), ys);
+      std::vector<ef> qv(nsk);
+      for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], zc[0]);
+      p = poly_mul(p, interpolate(sel, qv));
+      const int deg = 4 * (nsk - 1);
+      p.resize(deg + 1, kb::ef_zero());
+      ts.add_ext(p.data(), p.size());
+      ef r0 = ts.sample_ext();
+      challenges.push_back(r0);
+      sum = poly_eval(p, r0);
+      grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, deg));
+      std::vector<ef> selr(nsk);
+      mmf = kb::ef_zero();
+      for (int i = 0; i < nsk; i++) {
+        selr[i] = upoly_eval(sel[i], r0);
+        mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
+      }
+      DBuf d_sel = upload(ctx, selr);
+      cols = DBuf(sizeof(ef) * size_t(W + 1) * S, st);
+      { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
+      { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold_ef(arow.as<ef>(), n, k, d_sel.as<ef>(), cols.as<ef>() + size_t(W) * S, st); }
+      arow.reset();
     }
-    std::vector<ef> sums = reduce_to_host(ctx, part, nb + nbr, nz);
-    std::vector<ef> ys(nsk, kb::ef_zero());
-    ys.insert(ys.end(), sums.begin(), sums.end());
-    std::vector<ef> p = interpolate(lagrange_basis_cached((int)ys.size()), ys);
-    std::vector<ef> qv(nsk);
-    for (int i = 0; i < nsk; i++) qv[i] = upoly_eval(sel[i], zc[0]);
-    p = poly_mul(p, interpolate(sel, qv));
-    const int deg = 4 * (nsk - 1);
-    p.resize(deg + 1, kb::ef_zero());
-    ts.add_ext(p.data(), p.size());
-    ef r0 = ts.sample_ext();
-    challenges.push_back(r0);
-    sum = poly_eval(p, r0);
-    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, deg));
-    std::vector<ef> selr(nsk);
-    mmf = kb::ef_zero();
-    for (int i = 0; i < nsk; i++) {
-      selr[i] = upoly_eval(sel[i], r0);
-      mmf = kb::ef_add(mmf, kb::ef_mul(qv[i], selr[i]));
+    const auto basis4 = lagrange_basis_cached(4);
+    // eq table of round r (over zc[1+r..]) = eq table of round r-1 with its leading variable
+    // summed out; each fold below carries it along.
+    DBuf eqr;
+    if (n - k >= 1) {
+      eqr = DBuf(sizeof(ef) * (S / 2), st);
+      { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
     }
-    DBuf d_sel = upload(ctx, selr);
-    cols = DBuf(sizeof(ef) * size_t(W + 1) * S, st);
-    { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold(wit, n, k, d_sel.as<ef>(), cols.as<ef>(), st); }
-    { ProfScope _ps(ctx, "zc0_fold"); launch_zc0_fold_ef(arow.as<ef>(), n, k, d_sel.as<ef>(), cols.as<ef>() + size_t(W) * S, st); }
-    arow.reset();
-  }
-  const auto basis4 = lagrange_basis_cached(4);
-  // eq table of round r (over zc[1+r..]) = eq table of round r-1 with its leading variable
-  // summed out; each fold below carries it along.
-  DBuf eqr;
-  if (n - k >= 1) {
-    eqr = DBuf(sizeof(ef) * (S / 2), st);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2); }
-  }
-  const bool zc_on_device = sumcheck_pow_bits(s.security_bits, 4) == 0;
-  if (zc_on_device && n - k >= 1) {
-    // every round's transcript on the device: the sums, the finishing kernel (interpolation,
-    // absorption, challenge) and the fold at the device-sampled challenge, one host wait
-    DevPhase ph(ctx, ts, n - k, 40, sum, mmf, job.p16, zc.data() + 1);
-    for (int round = 1; round <= n - k; round++) {
-      const int m = n - k - round + 1;
+    const bool zc_on_device = sumcheck_pow_bits(s.security_bits, 4) == 0;
+    if (zc_on_device && n - k >= 1) {
+      // every round's transcript on the device: the sums, the finishing kernel (interpolation,
+      // absorption, challenge) and the fold at the device-sampled challenge, one host wait
+      DevPhase ph(ctx, ts, n - k, 40, sum, mmf, job.p16, zc.data() + 1);
+      for (int round = 1; round <= n - k; round++) {
+        const int m = n - k - round + 1;
+        const size_t half = size_t(1) << (m - 1);
+        const int nb = zc_ef_blocks(m);
+        ef* part = ctx.partials(size_t(nb) * 3);
+        { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
+        ph.finish_round(FIN_EQSC4, part, nb);
+        DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
+        DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+        { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), W + 1, half, ph.chs + (round - 1), st,
+                                                      half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
+        cols = std::move(nc);
+        eqr = std::move(eqn);
+      }
+      const std::vector<ef> ch = ph.finish(&sum, &mmf);
+      challenges.insert(challenges.end(), ch.begin(), ch.end());
+    }
+    for (int round = 1; !zc_on_device && round <= n - k; round++) {
+      const int m = n - k - round + 1;  // variables of the current columns
       const size_t half = size_t(1) << (m - 1);
       const int nb = zc_ef_blocks(m);
       ef* part = ctx.partials(size_t(nb) * 3);
       { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
-      ph.finish_round(FIN_EQSC4, part, nb);
+      std::vector<ef> s3 = reduce_to_host(ctx, part, nb, 3);
+      const ef& r = zc[round];
+      ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
+      ef e1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(e0, kb::ef_sub(kb::ef_one(), r))), kb::ef_inv(r));
+      std::vector<ef> p = interpolate(basis4, {e0, e1, e2, e3});
+      p = poly_mul(p, {kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_add(r, r), kb::ef_one())});
+      ts.add_ext(p.data(), p.size());
+      ef c = ts.sample_ext();
+      challenges.push_back(c);
+      sum = poly_eval(p, c);
+      grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 4));
+      mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
+                       mmf);
       DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
       DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-      { ProfScope _ps(ctx, "fold"); launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), W + 1, half, ph.chs + (round - 1), st,
-                                                    half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
+      { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), W + 1, half, c, st,
+                                                     half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
       cols = std::move(nc);
       eqr = std::move(eqn);
     }
-    const std::vector<ef> ch = ph.finish(&sum, &mmf);
-    challenges.insert(challenges.end(), ch.begin(), ch.end());
+    // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
+    // The zerocheck's returned challenges replace the eq challenges from here on
+    // (crates/air/src/prove.rs:114 rebinds zerocheck_challenges).
+    const std::vector<ef> rtail(challenges.begin() + 1, challenges.end());
+    {
+      std::vector<ef> selr(nsk);
+      for (int i = 0; i < nsk; i++) selr[i] = upoly_eval(sel[i], challenges[0]);
+      DBuf d_sel = upload(ctx, selr);
+      const int ll_t = std::min(12, n - k), lh_t = n - k - ll_t;
+      EqPair et = eq_pair(ctx, rtail, lh_t);
+      const size_t plen = size_t(W) * (1 + (size_t(nsk) << lh_t));
+      DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
+      DBuf limbs(size_t(64) << ll_t, st);
+      {
+        ProfScope _ps(ctx, "inner_sums");
+        tuned(ctx, TUNE_INNER, uint64_t(n) | uint64_t(k) << 8, [&](int plan) {
+          launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(),
+                            limbs.as<uint8_t>(), st, plan, ctx.pipe_timeouts);
+        });
+      }
+      unsigned timeouts = 0;
+      ctx.to_host_many({{inner_up.data(), up.as<ef>(), sizeof(ef) * W}, {inner_down.data(), down.as<ef>(), sizeof(ef) * W},
+                        {&timeouts, ctx.pipe_timeouts, sizeof(unsigned)}});
+      if (timeouts) throw std::runtime_error("inner sums: a bounded pipeline wait ran out on the device");
+    }
+    cols.reset();
   }
-  for (int round = 1; !zc_on_device && round <= n - k; round++) {
-    const int m = n - k - round + 1;  // variables of the current columns
-    const size_t half = size_t(1) << (m - 1);
-    const int nb = zc_ef_blocks(m);
-    ef* part = ctx.partials(size_t(nb) * 3);
-    { ProfScope _ps(ctx, zc_eval_is_dense(m) ? "zc_eval_dense" : "zc_eval_ef"); launch_zc_eval_ef(cols.as<ef>(), m, eqr.as<ef>(), d_alphas.as<ef>(), d_betas.as<ef>(), job.air, part, st); }
-    std::vector<ef> s3 = reduce_to_host(ctx, part, nb, 3);
-    const ef& r = zc[round];
-    ef e0 = kb::ef_mul(s3[0], mmf), e2 = kb::ef_mul(s3[1], mmf), e3 = kb::ef_mul(s3[2], mmf);
-    ef e1 = kb::ef_mul(kb::ef_sub(sum, kb::ef_mul(e0, kb::ef_sub(kb::ef_one(), r))), kb::ef_inv(r));
-    std::vector<ef> p = interpolate(basis4, {e0, e1, e2, e3});
-    p = poly_mul(p, {kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_add(r, r), kb::ef_one())});
-    ts.add_ext(p.data(), p.size());
-    ef c = ts.sample_ext();
-    challenges.push_back(c);
-    sum = poly_eval(p, c);
-    grind(ctx, ts, job.p16, sumcheck_pow_bits(s.security_bits, 4));
-    mmf = kb::ef_mul(kb::ef_add(kb::ef_mul(kb::ef_sub(kb::ef_one(), r), kb::ef_sub(kb::ef_one(), c)), kb::ef_mul(r, c)),
-                     mmf);
-    DBuf nc(sizeof(ef) * size_t(W + 1) * half, st);
-    DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
-    { ProfScope _ps(ctx, "fold"); launch_fold_cols_at(cols.as<ef>(), nc.as<ef>(), W + 1, half, c, st,
-                                                   half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2); }
-    cols = std::move(nc);
-    eqr = std::move(eqn);
-  }
-  // inner sums: every up / down column evaluated at (r_0 over the skipped variables, r_tail)
-  // The zerocheck's returned challenges replace the eq challenges from here on
-  // (crates/air/src/prove.rs:114 rebinds zerocheck_challenges).
-  std::vector<ef> inner_up(W), inner_down(W);
   const std::vector<ef> rtail(challenges.begin() + 1, challenges.end());
   DBuf eqt = eq_table_dev(ctx, rtail);
-  {
-    std::vector<ef> selr(nsk);
-    for (int i = 0; i < nsk; i++) selr[i] = upoly_eval(sel[i], challenges[0]);
-    DBuf d_sel = upload(ctx, selr);
-    const int ll_t = std::min(12, n - k), lh_t = n - k - ll_t;
-    EqPair et = eq_pair(ctx, rtail, lh_t);
-    const size_t plen = size_t(W) * (1 + (size_t(nsk) << lh_t));
-    DBuf up(sizeof(ef) * plen, st), down(sizeof(ef) * plen, st);
-    DBuf limbs(size_t(64) << ll_t, st);
-    {
-      ProfScope _ps(ctx, "inner_sums");
-      tuned(ctx, TUNE_INNER, uint64_t(n) | uint64_t(k) << 8, [&](int plan) {
-        launch_inner_sums(wit, n, k, ll_t, et.hi.as<ef>(), et.lo.as<ef>(), d_sel.as<ef>(), up.as<ef>(), down.as<ef>(),
-                          limbs.as<uint8_t>(), st, plan, ctx.pipe_timeouts);
-      });
-    }
-    unsigned timeouts = 0;
-    ctx.to_host_many({{inner_up.data(), up.as<ef>(), sizeof(ef) * W}, {inner_down.data(), down.as<ef>(), sizeof(ef) * W},
-                      {&timeouts, ctx.pipe_timeouts, sizeof(unsigned)}});
-    if (timeouts) throw std::runtime_error("inner sums: a bounded pipeline wait ran out on the device");
-  }
-  cols.reset();
   const double t2 = now_ms();
 
   // ---------------------------------------------------------------- 4) inner sumcheck
   ts.phase("inner_sums");
   ts.add_ext(inner_up.data(), W);
   ts.add_ext(inner_down.data(), W);
-  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, AIR_LOG_W));
-  std::vector<ef> cbs(AIR_LOG_W);
+  grind(ctx, ts, job.p16, batching_pow_bits(s.security_bits, LOGW));
+  std::vector<ef> cbs(LOGW);
   for (auto& x : cbs) x = ts.sample_ext();
   std::vector<ef> eqc = eq_table_host(cbs);
   eqc.resize(W);
   DBuf d_eqc = upload(ctx, eqc);
   DBuf B(sizeof(ef) * N, st);
-  {
+  if (prog) {
+    ProfScope _ps(ctx, "batch_cols");
+    launch_batch_cols_generic(wit, n, W, d_eqc.as<ef>(), B.as<ef>(), st);
+  } else {
     DBuf limbs(colsum_limb_bytes(W), st);
     ProfScope _ps(ctx, "batch_cols");
     launch_batch_cols_mma(wit, n, d_eqc.as<ef>(), B.as<ef>(), limbs.as<uint8_t>(), st);
@@ -1306,6 +1423,15 @@ std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_
 
 std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const uint32_t* wit_host, Timings* tm) {
   const size_t N = size_t(1) << job.log_n;
+  if (job.prog) {
+    // a constraint-program AIR: the whole witness, then the proof
+    const size_t words = N * size_t(job.prog->W);
+    DBuf wit(sizeof(uint32_t) * words, ctx.stream);
+    WL_CUDA(cudaMemcpyAsync(wit.as<uint32_t>(), wit_host, sizeof(uint32_t) * words, cudaMemcpyHostToDevice,
+                            ctx.stream));
+    launch_to_mont(wit.as<uint32_t>(), words, ctx.stream);
+    return prove_air(ctx, job, wit.as<uint32_t>(), tm);
+  }
   DBuf wit(sizeof(uint32_t) * N * AIR_W, ctx.stream);
   // the copy stream must not start before the allocation is usable
   cudaEvent_t alloc_done;

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "host.h"
+#include "air_program.h"
 #include "kernels.h"
 
 namespace wl {
@@ -127,6 +128,9 @@ struct ProofJob {
   AirConsts air;
   kb::P16Consts p16;
   kb::P24Consts p24;
+  // An AIR given as a constraint program instead of the built-in Poseidon2 AIR (its witness
+  // has prog->W columns; `air` is unused).
+  const ProgramAir* prog = nullptr;
 };
 
 // Proves with a device-resident, Montgomery-form, column-major witness (165 columns of
@@ -146,6 +150,8 @@ std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const ui
 std::vector<uint32_t> prove_abc(Context& ctx, const kb::P16Consts& p16, int log_n, int skips, const uint32_t* a,
                                 const uint32_t* b, const uint32_t* c, std::vector<float>* round_ms);
 
-size_t proof_len_bound(const Settings& s, int log_n);
+// Upper bound of the proof length (u32 words) for an AIR of W columns and constraint degree
+// `degree` (the built-in one by default).
+size_t proof_len_bound(const Settings& s, int log_n, int W = AIR_W, int degree = 3);
 
 }  // namespace wl

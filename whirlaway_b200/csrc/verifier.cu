@@ -369,9 +369,10 @@ class WhirVerifier {
 
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
                      int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log, int threads,
-                     std::vector<MerkleOpening>* defer) {
-  const int k = s.univariate_skips, W = AIR_W, nsk = 1 << k;
-  const WhirSchedule ws = WhirSchedule::build(n + AIR_LOG_W, s);
+                     std::vector<MerkleOpening>* defer, const ProgramAir* prog) {
+  const int k = s.univariate_skips, W = prog ? prog->W : AIR_W, nsk = 1 << k;
+  const int NC = prog ? prog->NC : AIR_NC, LOGW = log2_up(size_t(W)), d1 = (prog ? prog->degree : 3) + 1;
+  const WhirSchedule ws = WhirSchedule::build(n + LOGW, s);
   ProofReader rd(&p16, proof, proof_len, log);
   for (uint32_t x : ws.domain_separator()) rd.ch.observe(kb::to_mont(x));
   rd.phase("commit");
@@ -382,15 +383,15 @@ int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Const
   if (!whir.parse_commitment(root, ood_pts, ood_vals)) return VERIFY_PCS_COMMITMENT;
 
   rd.phase("batching");
-  if (!rd.pow(batching_pow_bits(s.security_bits, log2_up(AIR_NC)))) return VERIFY_FS;
+  if (!rd.pow(batching_pow_bits(s.security_bits, log2_up(size_t(NC))))) return VERIFY_FS;
   const ef alpha = rd.sample();
   if (!rd.pow(batching_pow_bits(s.security_bits, n))) return VERIFY_FS;
   std::vector<ef> zc(n - k + 1);
   for (auto& x : zc) x = rd.sample();
 
-  // zerocheck with univariate skip: degree (3 + 1) per variable
-  std::vector<int> deg{4 * (nsk - 1)}, set{nsk};
-  for (int i = 0; i < n - k; i++) deg.push_back(4), set.push_back(2);
+  // zerocheck with univariate skip: degree (constraint degree + 1) per variable
+  std::vector<int> deg{d1 * (nsk - 1)}, set{nsk};
+  for (int i = 0; i < n - k; i++) deg.push_back(d1), set.push_back(2);
   Claim outer;
   rd.phase("zerocheck");
   if (!sumcheck_rounds(rd, deg, set, s.security_bits, outer)) return VERIFY_SUMCHECK;
@@ -406,17 +407,18 @@ int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Const
     outer_sel[i] = upoly_eval(sel[i], outer.point[0]);
     sel_dot = kb::ef_add(sel_dot, kb::ef_mul(upoly_eval(sel[i], zc[0]), outer_sel[i]));
   }
-  std::vector<ef> alphas(AIR_NC);
+  std::vector<ef> alphas(NC);
   alphas[0] = kb::ef_one();
-  for (int i = 1; i < AIR_NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
-  const ef constraints = air_eval_ef(air, alphas.data(), [&](int c) { return up[c]; });
+  for (int i = 1; i < NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
+  const ef constraints = prog ? prog->eval_ef(up.data(), down.data(), alphas.data())
+                              : air_eval_ef(air, alphas.data(), [&](int c) { return up[c]; });
   const std::vector<ef> zc_tail(zc.begin() + 1, zc.end()), outer_tail(outer.point.begin() + 1, outer.point.end());
   if (!kb::ef_eq(kb::ef_mul(kb::ef_mul(sel_dot, eq_eval(zc_tail, outer_tail)), constraints), outer.value))
     return VERIFY_SUM_MISMATCH;
 
   // column batching and the up/down combination
   if (!rd.pow(batching_pow_bits(s.security_bits, log2_up(W)))) return VERIFY_FS;
-  std::vector<ef> cbs(AIR_LOG_W);
+  std::vector<ef> cbs(LOGW);
   for (auto& x : cbs) x = rd.sample();
   const ef alpha2 = rd.sample();
   std::vector<ef> sub(nsk);

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "air_program.h"
 #include "host.h"
 
 namespace wl {
@@ -37,9 +38,11 @@ struct MerkleOpening {
 // The verdict is then: if a listed opening fails, the proof is an opening error
 // (VERIFY_PCS_OPENING), whatever the returned outcome, because every listed opening comes
 // before the check that ended the replay; otherwise the returned outcome.
+// With `prog`, the proof is of that constraint-program AIR (`air` is unused).
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
                      int log_n, const uint32_t* proof, size_t proof_len, TranscriptLog* log = nullptr,
-                     int threads = 0, std::vector<MerkleOpening>* defer = nullptr);
+                     int threads = 0, std::vector<MerkleOpening>* defer = nullptr,
+                     const ProgramAir* prog = nullptr);
 int verify_abc_proof(const kb::P16Consts& p16, int log_n, int skips, const uint32_t* proof, size_t proof_len);
 
 }  // namespace wl
