@@ -117,7 +117,10 @@ wl_status wl_prove_witness(wl_ctx* ctx, const wl_air_settings* settings, const u
  *   WL_AIR_EMIT a                 the next constraint is v_a (v_i = v_a)
  * The EMITs, in order, are the n_constraints constraints, batched as sum_i alpha^i C_i.
  * constraint_degree (1..3) bounds every constraint's degree. At most 64 values may be live at
- * once (the device interpreter's register file); n_columns <= 32767. No preprocessed columns. */
+ * once (the device interpreter's register file); n_columns <= 32767. The first n_preprocessed
+ * columns are preprocessed (AirTable::preprocessed_columns, crates/air/src/table.rs:19): fixed
+ * by the AIR, given with the program, in the zerocheck but not committed; the verifier
+ * evaluates them itself (crates/air/src/verify.rs:119-135). */
 enum { WL_AIR_UP = 0, WL_AIR_DOWN = 1, WL_AIR_CONST = 2, WL_AIR_ADD = 3, WL_AIR_SUB = 4, WL_AIR_MUL = 5,
        WL_AIR_EMIT = 6 };
 typedef struct {
@@ -128,9 +131,11 @@ typedef struct {
   const int32_t* ops;
   int32_t n_consts;
   const uint32_t* consts;
+  int32_t n_preprocessed;       /* the first n_preprocessed columns are preprocessed (may be 0) */
+  const uint32_t* preprocessed; /* their values: n_preprocessed x 2^log_n, canonical, column-major */
 } wl_air_program;
-/* Proves the program's AIR for a host witness (n_columns x 2^log_n canonical values,
- * column-major). hash_constants: Poseidon16 (148) | Poseidon24 (215) constants, as in a
+/* Proves the program's AIR for a host witness (the n_columns - n_preprocessed witness columns,
+ * each 2^log_n canonical values, column-major). hash_constants: Poseidon16 (148) | Poseidon24 (215) constants, as in a
  * constants blob after its AIR part. No reference counterpart beyond AirTable::prove. */
 wl_status wl_prove_program(wl_ctx* ctx, const wl_air_settings* settings, const uint32_t* hash_constants,
                            const wl_air_program* program, int32_t log_n, const uint32_t* witness_colmajor,

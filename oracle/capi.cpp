@@ -50,14 +50,18 @@ Poseidon2 perm_from(int width, const uint32_t* c) {
 // constants blob: AIR (148) | P16 (148) | P24 (215)
 constexpr int AIR_NC = 2 * 4 * 16 + 20, P16_NC = 8 * 16 + 20, P24_NC = 8 * 24 + 23;
 // A constraint program from flat arrays: ops holds (op, a, b) per instruction.
+// The first n_pre columns are preprocessed: pre holds them (n_pre columns of 2^log_n values).
 ProgramAirSpec program_from(int W, int n_constraints, int degree, int n_ops, const int32_t* ops, int n_consts,
-                            const uint32_t* consts) {
+                            const uint32_t* consts, int n_pre, const uint32_t* pre, int log_n) {
   ProgramAirSpec p;
   p.W = W;
   p.NC = n_constraints;
   p.deg = degree;
+  p.P = n_pre;
   for (int i = 0; i < n_ops; i++) p.code.push_back({ops[3 * i], ops[3 * i + 1], ops[3 * i + 2]});
   for (int i = 0; i < n_consts; i++) p.consts.push_back(F(consts[i]));
+  if (n_pre < 0 || n_pre >= W) throw std::runtime_error("AIR program: bad preprocessed column count");
+  for (size_t i = 0; i < (size_t(n_pre) << log_n); i++) p.pre.push_back(F(pre[i]));
   p.check();
   return p;
 }
@@ -140,17 +144,18 @@ int wlo_verify(const int32_t* settings, const uint32_t* constants, int log_n, co
   }
 }
 
-// An AIR given as a constraint program (hash_consts: P16 (148) | P24 (215)); witness: W
+// An AIR given as a constraint program (hash_consts: P16 (148) | P24 (215)); its first n_pre
+// columns are preprocessed (pre: n_pre columns of 2^log_n values); witness: the other W - n_pre
 // columns of 2^log_n values, column-major.
 int wlo_prove_program(const int32_t* settings, const uint32_t* hash_consts, int W, int n_constraints, int degree,
-                      int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int log_n,
-                      const uint32_t* witness, uint32_t* proof, size_t* proof_len) {
+                      int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int n_pre,
+                      const uint32_t* pre, int log_n, const uint32_t* witness, uint32_t* proof, size_t* proof_len) {
   try {
     Settings s = settings_from(settings);
-    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts);
+    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts, n_pre, pre, log_n);
     Hashes h{perm_from(16, hash_consts), perm_from(24, hash_consts + P16_NC)};
     size_t N = size_t(1) << log_n;
-    std::vector<F> w(size_t(W) * N);
+    std::vector<F> w(size_t(W - n_pre) * N);
     for (size_t i = 0; i < w.size(); i++) w[i] = F::raw(witness[i]);
     std::vector<F> pr = prove_air_spec(s, air, h, log_n, w);
     if (*proof_len < pr.size()) { *proof_len = pr.size(); return -2; }
@@ -163,11 +168,11 @@ int wlo_prove_program(const int32_t* settings, const uint32_t* hash_consts, int 
 }
 
 int wlo_verify_program(const int32_t* settings, const uint32_t* hash_consts, int W, int n_constraints, int degree,
-                       int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int log_n,
-                       const uint32_t* proof, size_t proof_len) {
+                       int n_ops, const int32_t* ops, int n_consts, const uint32_t* consts, int n_pre,
+                       const uint32_t* pre, int log_n, const uint32_t* proof, size_t proof_len) {
   try {
     Settings s = settings_from(settings);
-    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts);
+    ProgramAirSpec air = program_from(W, n_constraints, degree, n_ops, ops, n_consts, consts, n_pre, pre, log_n);
     Hashes h{perm_from(16, hash_consts), perm_from(24, hash_consts + P16_NC)};
     std::vector<F> pr(proof_len);
     for (size_t i = 0; i < proof_len; i++) pr[i] = F::raw(proof[i] % P);

@@ -176,6 +176,11 @@ EF air_eval_ext(const AirConstants& c, const EF* up, const std::vector<EF>& alph
 struct AirSpec {
   virtual ~AirSpec() = default;
   virtual int columns() const = 0;
+  // Preprocessed columns (crates/air/src/table.rs:19,59-70): the first preprocessed() of the
+  // columns are fixed by the AIR (preprocessed_column(c): 2^log_n values); they take part in the
+  // zerocheck but are not committed, and the verifier evaluates them itself.
+  virtual int preprocessed() const { return 0; }
+  virtual const F* preprocessed_column(int c, size_t N) const { return nullptr; }
   virtual int constraints() const = 0;
   virtual int degree() const = 0;
   virtual EF eval_base(const F* ud, const std::vector<EF>& alphas) const = 0;
@@ -201,10 +206,16 @@ struct AirInstr {
   int op, a, b;
 };
 struct ProgramAirSpec : AirSpec {
-  int W = 0, NC = 0, deg = 0;
+  int W = 0, NC = 0, deg = 0, P = 0;
   std::vector<AirInstr> code;
   std::vector<F> consts;
+  std::vector<F> pre;  // P columns of 2^log_n values
   int columns() const override { return W; }
+  int preprocessed() const override { return P; }
+  const F* preprocessed_column(int c, size_t N) const override {
+    if (pre.size() != size_t(P) * N) throw std::runtime_error("AIR program: preprocessed columns of the wrong height");
+    return pre.data() + size_t(c) * N;
+  }
   int constraints() const override { return NC; }
   int degree() const override { return deg; }
   EF eval_base(const F* ud, const std::vector<EF>& a) const override;

@@ -248,11 +248,13 @@ std::vector<F> prove_air(const Settings& s, const AirConstants& air, const Hashe
 
 std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n,
                               const std::vector<F>& witness, ProveTimings* tm) {
-  const int W = air.columns(), NC = air.constraints(), n = log_n, k = s.univariate_skips;
+  // W: all columns (the preprocessed ones first); Ww: the witness columns, the committed ones
+  const int W = air.columns(), NC = air.constraints(), P = air.preprocessed(), Ww = W - P, n = log_n,
+            k = s.univariate_skips;
   if (k >= n) throw std::runtime_error("univariate_skips must be < log_n_rows");
   const size_t N = size_t(1) << n;
-  if (witness.size() != size_t(W) * N) throw std::runtime_error("witness size mismatch");
-  const int logW = log2_up(W);
+  if (Ww < 1 || witness.size() != size_t(Ww) * N) throw std::runtime_error("witness size mismatch");
+  const int logW = log2_up(Ww);
   WhirConfig cfg = WhirConfig::build(n + logW, s);
   Transcript ts(&h.p16);
   for (F x : cfg.domain_separator()) ts.ch.observe(x);
@@ -278,7 +280,7 @@ std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashe
   // 3) zerocheck over the up/down columns (crates/air/src/utils.rs:140-160)
   std::vector<std::vector<F>> ud(2 * W);
   for (int c = 0; c < W; c++) {
-    const F* col = &witness[size_t(c) * N];
+    const F* col = c < P ? air.preprocessed_column(c, N) : &witness[size_t(c - P) * N];
     ud[c].assign(col, col + N);
     ud[c][N - 1] = ud[c][N - 2];
     ud[W + c].assign(col + 1, col + N);
@@ -292,10 +294,10 @@ std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashe
   double t2 = now_s();
 
   // 4) inner sums and the inner sumcheck
-  std::vector<EF> up(W), down(W);
-  for (int c = 0; c < W; c++) { up[c] = fin[c][0]; down[c] = fin[W + c][0]; }
-  ts.add_ext(up.data(), W);
-  ts.add_ext(down.data(), W);
+  std::vector<EF> up(Ww), down(Ww);
+  for (int c = 0; c < Ww; c++) { up[c] = fin[P + c][0]; down[c] = fin[W + P + c][0]; }
+  ts.add_ext(up.data(), Ww);
+  ts.add_ext(down.data(), Ww);
   ts.grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - logW)));
   std::vector<EF> cbs(logW);
   for (auto& x : cbs) x = ts.sample_ext();
@@ -304,7 +306,7 @@ std::vector<F> prove_air_spec(const Settings& s, const AirSpec& air, const Hashe
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < (int64_t)N; i++) {
     EF acc;
-    for (int c = 0; c < W; c++) acc += eqc[c] * witness[size_t(c) * N + i];
+    for (int c = 0; c < Ww; c++) acc += eqc[c] * witness[size_t(c) * N + i];
     batched[i] = acc;
   }
   EF alpha2 = ts.sample_ext();

@@ -75,8 +75,9 @@ int verify_air(const Settings& s, const AirConstants& air, const Hashes& h, int 
 }
 
 int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int log_n, const std::vector<F>& proof) {
-  const int W = air.columns(), NC = air.constraints(), n = log_n, k = s.univariate_skips;
-  const int logW = log2_up(W);
+  const int W = air.columns(), NC = air.constraints(), P = air.preprocessed(), Ww = W - P, n = log_n,
+            k = s.univariate_skips;
+  const int logW = log2_up(Ww);
   WhirConfig cfg = WhirConfig::build(n + logW, s);
   Transcript ts(&h.p16);
   ts.proof = proof;
@@ -98,16 +99,36 @@ int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int 
   if (int e = verify_core(ts, degs, sets, s.security_bits, outer)) return e;
   if (!outer.sum.is_zero()) return V_SUM_MISMATCH;
 
-  std::vector<EF> wup(W), wdown(W);
-  if (!ts.next_ext(wup.data(), W) || !ts.next_ext(wdown.data(), W)) return V_FS;
+  std::vector<EF> wup(Ww), wdown(Ww);
+  if (!ts.next_ext(wup.data(), Ww) || !ts.next_ext(wdown.data(), Ww)) return V_FS;
   auto sel = univariate_selectors(k);
   std::vector<EF> outer_sel(1 << k), zc_sel(1 << k);
   for (int i = 0; i < (1 << k); i++) {
     outer_sel[i] = upoly_eval(sel[i], outer.point[0]);
     zc_sel[i] = upoly_eval(sel[i], zc[0]);
   }
+  // the preprocessed columns' up / down versions folded over the skipped variables at the
+  // outer challenge and evaluated at its tail (crates/air/src/verify.rs:119-135)
   std::vector<EF> global(2 * W);
-  for (int c = 0; c < W; c++) { global[c] = wup[c]; global[W + c] = wdown[c]; }
+  const size_t N = size_t(1) << n, S = N >> k;
+  const std::vector<EF> otail(outer.point.begin() + 1, outer.point.end());
+  for (int c = 0; c < P; c++) {
+    const F* col = air.preprocessed_column(c, N);
+    for (int half = 0; half < 2; half++) {
+      std::vector<EF> f(S);
+      for (size_t x = 0; x < S; x++) {
+        EF acc;
+        for (int j = 0; j < (1 << k); j++) {
+          const size_t r = size_t(j) * S + x;
+          const size_t src = half == 0 ? (r == N - 1 ? N - 2 : r) : (r == N - 1 ? r : r + 1);
+          acc += outer_sel[j] * col[src];
+        }
+        f[x] = acc;
+      }
+      global[half * W + c] = mle_evaluate(f, otail);
+    }
+  }
+  for (int c = 0; c < Ww; c++) { global[P + c] = wup[c]; global[W + P + c] = wdown[c]; }
   std::vector<EF> alphas(NC);
   alphas[0] = ef_one();
   for (int i = 1; i < NC; i++) alphas[i] = alphas[i - 1] * alpha;
@@ -117,7 +138,7 @@ int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int 
   std::vector<EF> zc_tail(zc.begin() + 1, zc.end()), outer_tail(outer.point.begin() + 1, outer.point.end());
   if (dot * eq_poly(zc_tail, outer_tail) * constraint_eval != outer.value) return V_SUM_MISMATCH;
 
-  if (!ts.check_grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(W))))) return V_FS;
+  if (!ts.check_grind(std::max(0, s.security_bits - std::max(0, 31 * EXT_D - log2_up(Ww))))) return V_FS;
   std::vector<EF> cbs(logW);
   for (auto& x : cbs) x = ts.sample_ext();
   EF alpha2 = ts.sample_ext();
@@ -126,7 +147,7 @@ int verify_air_spec(const Settings& s, const AirSpec& air, const Hashes& h, int 
   std::vector<EF> eqc = eval_eq(cbs);
   EF lhs, su, sd;
   for (int i = 0; i < (1 << k); i++) lhs += sub[i] * outer_sel[i];
-  for (int c = 0; c < W; c++) { su += wup[c] * eqc[c]; sd += wdown[c] * eqc[c]; }
+  for (int c = 0; c < Ww; c++) { su += wup[c] * eqc[c]; sd += wdown[c] * eqc[c]; }
   if (lhs != su + sd * alpha2) return V_SUM_MISMATCH;
   std::vector<EF> eps(k);
   for (auto& x : eps) x = ts.sample_ext();

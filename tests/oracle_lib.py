@@ -30,7 +30,7 @@ class Oracle:
                                       ctypes.POINTER(ctypes.c_size_t)]
         lib.wlo_verify_abc.argtypes = [_u32p, ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_size_t]
         prog_args = [_i32p, _u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, _u32p,
-                     ctypes.c_int]
+                     ctypes.c_int, _u32p, ctypes.c_int]
         lib.wlo_prove_program.argtypes = prog_args + [_u32p, _u32p, ctypes.POINTER(ctypes.c_size_t)]
         lib.wlo_verify_program.argtypes = prog_args + [_u32p, ctypes.c_size_t]
         lib.wlo_chacha_block.argtypes = [_u32p, ctypes.c_uint64, ctypes.c_int, _u32p]
@@ -70,15 +70,18 @@ class Oracle:
         proof = np.ascontiguousarray(proof, dtype=np.uint32)
         return self.lib.wlo_verify(s, _p(consts), log_n, _p(proof), proof.size)
 
-    def _program_args(self, settings, hash_consts, prog, log_n):
+    def _program_args(self, settings, hash_consts, prog, log_n, preprocessed):
         s = settings.ctypes.data_as(_i32p) if settings is not None else None
         hc = np.ascontiguousarray(hash_consts, np.uint32)
+        pre = np.ascontiguousarray(preprocessed if preprocessed is not None else np.zeros(1, np.uint32), np.uint32)
+        npre = 0 if preprocessed is None else pre.size >> log_n
         return [s, _p(hc), prog.width, prog.n_constraints, prog.degree, prog.ops.shape[0],
-                prog.ops.ctypes.data_as(_i32p), prog.consts.size, _p(prog.consts), log_n], hc
+                prog.ops.ctypes.data_as(_i32p), prog.consts.size, _p(prog.consts), npre, _p(pre), log_n], (hc, pre)
 
-    def prove_program(self, log_n, hash_consts, prog, witness, settings=None):
-        """A proof for the AIR given as a constraint program (hash_consts: P16 | P24 constants)."""
-        args, keep = self._program_args(settings, hash_consts, prog, log_n)
+    def prove_program(self, log_n, hash_consts, prog, witness, settings=None, preprocessed=None):
+        """A proof for the AIR given as a constraint program (hash_consts: P16 | P24 constants);
+        preprocessed: its first columns' values (n_pre x 2^log_n), witness the other columns."""
+        args, keep = self._program_args(settings, hash_consts, prog, log_n, preprocessed)
         w = np.ascontiguousarray(witness, np.uint32)
         cap = 1 << 22
         out = np.zeros(cap, np.uint32)
@@ -87,8 +90,8 @@ class Oracle:
         assert rc == 0, rc
         return out[: n.value].copy()
 
-    def verify_program(self, log_n, hash_consts, prog, proof, settings=None):
-        args, keep = self._program_args(settings, hash_consts, prog, log_n)
+    def verify_program(self, log_n, hash_consts, prog, proof, settings=None, preprocessed=None):
+        args, keep = self._program_args(settings, hash_consts, prog, log_n, preprocessed)
         proof = np.ascontiguousarray(proof, dtype=np.uint32)
         return self.lib.wlo_verify_program(*args, _p(proof), proof.size)
 

@@ -2,8 +2,9 @@
 
 CPU: the oracle proves the Poseidon2 AIR written as a program to the same proof words as its
 built-in Poseidon2 AIR (pinning the program semantics to the pinned AIR); oracle proofs of
-other program AIRs (transitions over the down values, degrees 1 to 3) are accepted by the
-oracle's and by the library's host verifiers, and proofs of broken witnesses are rejected.
+other program AIRs (transitions over the down values, degrees 1 to 3, preprocessed columns)
+are accepted by the oracle's and by the library's host verifiers, and proofs of broken
+witnesses (or checked against other preprocessed values) are rejected.
 GPU: the library's proofs equal the oracle's word for word.
 """
 import numpy as np
@@ -77,6 +78,26 @@ def mul_air(log_n, seed=2):
 AIRS = {"cubic": cubic_air, "fib": fib_air, "mul": mul_air}
 
 
+def pre_air(log_n, seed=3):
+    """Two preprocessed columns, f (1 on row 0) and r (fixed values), and the witness x, y with
+    f x = 0 (x starts at 0), x' = x + r, y = x r + f. Returns (program, witness, preprocessed)."""
+    n = 1 << log_n
+    rng = np.random.default_rng(seed)
+    f = np.zeros(n, np.uint64)
+    f[0] = 1
+    r = rng.integers(0, P, n).astype(np.uint64)
+    x = np.zeros(n, np.uint64)
+    for i in range(n - 1):
+        x[i + 1] = (x[i] + r[i]) % P
+    y = (x * r + f) % P
+    b = ap.AirBuilder(4, preprocessed=2)
+    F, R, X, Y = (b.up(c) for c in range(4))
+    b.assert_zero(F * X)
+    b.assert_zero(b.down(2) - X - R)
+    b.assert_zero(Y - X * R - F)
+    return b.build(), np.concatenate([x, y]).astype(np.uint32), np.concatenate([f, r]).astype(np.uint32)
+
+
 @pytest.fixture(scope="module")
 def oracle():
     return oracle_lib.load()
@@ -147,6 +168,23 @@ def test_broken_witness_rejected(oracle, hash_consts, name):
     assert wl.verify_program(hash_consts, prog, log_n, proof, wl_settings()) != 0
 
 
+@pytest.mark.parametrize("log_n,skips", [(8, 2), (10, 4)])
+def test_preprocessed_columns(oracle, hash_consts, log_n, skips):
+    import whirlaway_b200 as wl
+    prog, w, pre = pre_air(log_n)
+    assert prog.n_preprocessed == 2
+    assert prog.evaluate_rows(w, log_n, pre).max() == 0
+    s = settings_arr(skips)
+    proof = oracle.prove_program(log_n, hash_consts, prog, w, s, preprocessed=pre)
+    assert oracle.verify_program(log_n, hash_consts, prog, proof, s, preprocessed=pre) == 0
+    assert wl.verify_program(hash_consts, prog, log_n, proof, wl_settings(skips), preprocessed=pre) == 0
+    # other preprocessed values: the proof no longer verifies
+    other = pre.copy()
+    other[(1 << log_n) + 5] = (int(other[(1 << log_n) + 5]) + 1) % P
+    assert oracle.verify_program(log_n, hash_consts, prog, proof, s, preprocessed=other) != 0
+    assert wl.verify_program(hash_consts, prog, log_n, proof, wl_settings(skips), preprocessed=other) != 0
+
+
 def test_malformed_programs_rejected(hash_consts):
     import whirlaway_b200 as wl
     prog, w = fib_air(8)
@@ -174,6 +212,17 @@ def test_gpu_program_matches_oracle(oracle, hash_consts, name, log_n, skips):
         got = wl.prove_program(ctx, hash_consts, prog, log_n, w, wl_settings(skips))
     assert np.array_equal(got, want)
     assert wl.verify_program(hash_consts, prog, log_n, got, wl_settings(skips)) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("log_n,skips", [(8, 2), (12, 4)])
+def test_gpu_preprocessed_matches_oracle(oracle, hash_consts, log_n, skips):
+    import whirlaway_b200 as wl
+    prog, w, pre = pre_air(log_n)
+    want = oracle.prove_program(log_n, hash_consts, prog, w, settings_arr(skips), preprocessed=pre)
+    with wl.Context(0) as ctx:
+        got = wl.prove_program(ctx, hash_consts, prog, log_n, w, wl_settings(skips), preprocessed=pre)
+    assert np.array_equal(got, want)
 
 
 @pytest.mark.gpu

@@ -40,14 +40,25 @@ class _AirProgram(ctypes.Structure):
     _fields_ = [("n_columns", ctypes.c_int32), ("n_constraints", ctypes.c_int32),
                 ("constraint_degree", ctypes.c_int32), ("n_ops", ctypes.c_int32),
                 ("ops", ctypes.POINTER(ctypes.c_int32)), ("n_consts", ctypes.c_int32),
-                ("consts", ctypes.POINTER(ctypes.c_uint32))]
+                ("consts", ctypes.POINTER(ctypes.c_uint32)), ("n_preprocessed", ctypes.c_int32),
+                ("preprocessed", ctypes.POINTER(ctypes.c_uint32))]
 
 
-def _program_c(prog):
-    """The C description of an air_program.AirProgram (the arrays stay owned by prog)."""
-    return _AirProgram(prog.width, prog.n_constraints, prog.degree, prog.ops.shape[0],
-                       prog.ops.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), prog.consts.size,
-                       prog.consts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+def _program_c(prog, preprocessed, log_n):
+    """The C description of an air_program.AirProgram and its preprocessed columns (returns the
+    struct and the array it points into, which the caller keeps alive)."""
+    pre = np.zeros(1, np.uint32)
+    if prog.n_preprocessed:
+        if preprocessed is None:
+            raise ValueError("the program has preprocessed columns: pass their values")
+        pre = np.ascontiguousarray(preprocessed, dtype=np.uint32).reshape(-1)
+        if pre.size != prog.n_preprocessed << log_n:
+            raise ValueError("preprocessed must hold n_preprocessed columns of 2^log_n values")
+    c = _AirProgram(prog.width, prog.n_constraints, prog.degree, prog.ops.shape[0],
+                    prog.ops.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), prog.consts.size,
+                    prog.consts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), prog.n_preprocessed,
+                    pre.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    return c, pre
 
 
 class _Settings(ctypes.Structure):
@@ -352,16 +363,17 @@ class AirTable:
 
 
 def prove_program(ctx: Context, hash_constants: np.ndarray, program, log_n: int, witness_colmajor: np.ndarray,
-                  settings: AirSettings = AirSettings()) -> np.ndarray:
+                  settings: AirSettings = AirSettings(), preprocessed=None) -> np.ndarray:
     """AirTable::prove for an AIR given as a constraint program (air_program.AirProgram) with a
-    host witness (program.width columns of 2^log_n canonical values, column-major);
+    host witness (the program's witness columns, width - n_preprocessed of them, 2^log_n
+    canonical values each, column-major) and the values of its preprocessed columns, if any;
     hash_constants: the Poseidon16 | Poseidon24 constants (363 u32). Returns proof_data."""
     lib = ctx._lib
-    pc = _program_c(program)
+    pc, keep = _program_c(program, preprocessed, log_n)
     hc = np.ascontiguousarray(hash_constants, dtype=np.uint32)
     w = np.ascontiguousarray(witness_colmajor, dtype=np.uint32).reshape(-1)
-    if w.size != program.width << log_n:
-        raise ValueError("witness must hold program.width columns of 2^log_n values")
+    if w.size != (program.width - program.n_preprocessed) << log_n:
+        raise ValueError("witness must hold the program's witness columns of 2^log_n values")
     cap = ctypes.c_size_t()
     ctx.check(lib.wl_program_proof_len_bound(ctypes.byref(settings._c()), ctypes.byref(pc), log_n, ctypes.byref(cap)),
               "program_proof_len_bound")
@@ -373,10 +385,10 @@ def prove_program(ctx: Context, hash_constants: np.ndarray, program, log_n: int,
 
 
 def verify_program(hash_constants: np.ndarray, program, log_n: int, proof: np.ndarray,
-                   settings: AirSettings = AirSettings()) -> int:
+                   settings: AirSettings = AirSettings(), preprocessed=None) -> int:
     """AirTable::verify for a constraint-program AIR on the host: 0 when accepted, else the
     verifier status (as verify)."""
-    pc = _program_c(program)
+    pc, keep = _program_c(program, preprocessed, log_n)
     hc = np.ascontiguousarray(hash_constants, dtype=np.uint32)
     pr = np.ascontiguousarray(proof, dtype=np.uint32)
     return load_library().wl_verify_program(ctypes.byref(settings._c()), _ptr(hc), ctypes.byref(pc), log_n, _ptr(pr),

@@ -18,7 +18,9 @@ from Python expressions (shared subexpressions are emitted once).
     b.assert_zero(b.down(1) - x)
     prog = b.build()                    # 2 columns, 2 constraints, degree 3
 
-Constraint degrees 1 to 3 are supported.
+Constraint degrees 1 to 3 are supported. The first `preprocessed` columns of an AIR may be
+preprocessed (AirTable::preprocessed_columns, crates/air/src/table.rs:19): fixed by the AIR,
+given with the program when proving and verifying, part of the zerocheck but not committed.
 """
 import numpy as np
 
@@ -67,23 +69,30 @@ class Expr:
 
 
 class AirProgram:
-    """W columns, the constraint count, the degree, the instructions (int32 rows (op, a, b))
-    and the constants (canonical u32)."""
+    """W columns (the first n_preprocessed of them preprocessed), the constraint count, the
+    degree, the instructions (int32 rows (op, a, b)) and the constants (canonical u32)."""
 
-    def __init__(self, width, n_constraints, degree, ops, consts):
+    def __init__(self, width, n_constraints, degree, ops, consts, n_preprocessed=0):
         self.width = int(width)
         self.n_constraints = int(n_constraints)
         self.degree = int(degree)
+        self.n_preprocessed = int(n_preprocessed)
+        if not 0 <= self.n_preprocessed < self.width:
+            raise ValueError("0 <= preprocessed columns < columns")
         self.ops = np.ascontiguousarray(ops, dtype=np.int32).reshape(-1, 3)
         self.consts = np.ascontiguousarray(consts, dtype=np.uint32)
         if not 1 <= self.degree <= 3:
             raise ValueError("constraint degree must be 1, 2 or 3")
 
-    def evaluate_rows(self, witness, log_n):
-        """The constraint values of every up/down row pair of a column-major witness (a
-        host-side check for tests and examples; returns an (n_constraints, 2^log_n) array)."""
+    def evaluate_rows(self, witness, log_n, preprocessed=None):
+        """The constraint values of every up/down row pair of a column-major witness (after the
+        preprocessed columns, if any; a host-side check for tests and examples; returns an
+        (n_constraints, 2^log_n) array)."""
         n = 1 << log_n
-        w = np.asarray(witness, dtype=np.uint64).reshape(self.width, n)
+        w = np.asarray(witness, dtype=np.uint64).reshape(-1, n)
+        if self.n_preprocessed:
+            w = np.concatenate([np.asarray(preprocessed, dtype=np.uint64).reshape(self.n_preprocessed, n), w])
+        w = w.reshape(self.width, n)
         up = w.copy()
         up[:, n - 1] = w[:, n - 2]
         down = np.concatenate([w[:, 1:], w[:, n - 1:]], axis=1)
@@ -109,12 +118,14 @@ class AirProgram:
 
 
 class AirBuilder:
-    """Writes a constraint program over `width` columns."""
+    """Writes a constraint program over `width` columns, the first `preprocessed` of them
+    preprocessed."""
 
-    def __init__(self, width):
+    def __init__(self, width, preprocessed=0):
         if width < 1:
             raise ValueError("an AIR needs at least one column")
         self.width = width
+        self.preprocessed = preprocessed
         self.ops = []
         self.consts = []
         self._const_idx = {}
@@ -170,7 +181,7 @@ class AirBuilder:
         if d < self.max_degree:
             raise ValueError("declared degree below a constraint's degree")
         return AirProgram(self.width, self.n_constraints, d, np.array(self.ops, dtype=np.int32).reshape(-1, 3),
-                          np.array(self.consts, dtype=np.uint32))
+                          np.array(self.consts, dtype=np.uint32), self.preprocessed)
 
 
 def _poseidon2_diag16():

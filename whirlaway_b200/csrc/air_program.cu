@@ -89,6 +89,19 @@ ProgramAir ProgramAir::build(int W, int n_constraints, int degree, int n_ops, co
   return p;
 }
 
+void ProgramAir::set_preprocessed(int n_pre, const uint32_t* values, int log_n) {
+  if (n_pre < 0 || n_pre >= W) throw std::invalid_argument("AIR program: 0 <= preprocessed columns < columns");
+  if (n_pre > 0 && !values) throw std::invalid_argument("AIR program: preprocessed columns missing");
+  const size_t n = size_t(n_pre) << log_n;
+  P = n_pre;
+  pre_log_n = log_n;
+  pre.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    if (values[i] >= kb::P) throw std::invalid_argument("AIR program: preprocessed value not below p");
+    pre[i] = kb::to_mont(values[i]);
+  }
+}
+
 kb::ef ProgramAir::eval_ef(const kb::ef* up, const kb::ef* down, const kb::ef* alphas) const {
   const size_t n = ops.size() / 3;
   std::vector<kb::ef> v(n);

@@ -20,8 +20,11 @@ constexpr int PROG_MAX_REGS = 64;
 
 struct ProgramAir {
   int W = 0, NC = 0, degree = 0;
+  int P = 0;                     // preprocessed columns: the first P of the W
   std::vector<int32_t> ops;      // (op, a, b) per instruction, as given
   std::vector<uint32_t> consts;  // Montgomery form
+  std::vector<uint32_t> pre;     // the preprocessed columns, P x 2^log_n, Montgomery form
+  int pre_log_n = -1;
   // Device form: x = op | dst << 8 | a << 16 (a: a column, a constant or a register), y = b (a
   // register); EMIT's register is its operand's.
   std::vector<uint2> code;
@@ -32,6 +35,12 @@ struct ProgramAir {
   // consts_canonical: the constants as canonical values.
   static ProgramAir build(int W, int n_constraints, int degree, int n_ops, const int32_t* ops, int n_consts,
                           const uint32_t* consts_canonical);
+  // The first P columns are preprocessed (crates/air/src/table.rs:19,59-70): fixed by the AIR,
+  // part of the zerocheck, not committed; values: P columns of 2^log_n canonical values.
+  // Throws std::invalid_argument unless 0 <= P < W and every value is below p.
+  void set_preprocessed(int n_pre, const uint32_t* values_canonical, int log_n);
+  // Witness (committed) columns.
+  int witness_columns() const { return W - P; }
   // sum_i alphas[i] C_i at a point of up values up[0..W) and down values down[0..W).
   kb::ef eval_ef(const kb::ef* up, const kb::ef* down, const kb::ef* alphas) const;
 };

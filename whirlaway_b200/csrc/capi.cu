@@ -263,10 +263,12 @@ wl_status wl_prove(wl_ctx* ctx, const wl_air_settings* s, const uint32_t* consta
 
 namespace {
 // A constraint program from its C description (throws std::invalid_argument when malformed).
-wl::ProgramAir program_from(const wl_air_program* p) {
+wl::ProgramAir program_from(const wl_air_program* p, int log_n) {
   if (!p) throw std::invalid_argument("program is NULL");
-  return wl::ProgramAir::build(p->n_columns, p->n_constraints, p->constraint_degree, p->n_ops, p->ops, p->n_consts,
-                               p->consts);
+  wl::ProgramAir prog = wl::ProgramAir::build(p->n_columns, p->n_constraints, p->constraint_degree, p->n_ops, p->ops,
+                                              p->n_consts, p->consts);
+  prog.set_preprocessed(p->n_preprocessed, p->preprocessed, log_n);
+  return prog;
 }
 wl::ProofJob make_program_job(const wl_air_settings* s, const uint32_t* hash_constants, int log_n,
                               const wl::ProgramAir* prog) {
@@ -288,7 +290,7 @@ wl_status wl_prove_program(wl_ctx* ctx, const wl_air_settings* s, const uint32_t
   if (!settings_ok(s, log_n, why)) return fail(ctx, WL_E_INVALID_ARG, why);
   if (!witness || !hash_constants || !program || !proof_len) return fail(ctx, WL_E_INVALID_ARG, "NULL argument");
   return guarded(ctx, [&] {
-    const wl::ProgramAir prog = program_from(program);
+    const wl::ProgramAir prog = program_from(program, log_n);
     const wl::ProofJob job = make_program_job(s, hash_constants, log_n, &prog);
     std::vector<uint32_t> pr = wl::prove_air_host(*ctx->c, job, witness, nullptr);
     return emit_proof(ctx, pr, proof_out, proof_len);
@@ -302,7 +304,7 @@ wl_status wl_verify_program(const wl_air_settings* s, const uint32_t* hash_const
   for (size_t i = 0; i < proof_len; i++)
     if (proof[i] >= kb::P) return WL_E_INVALID_ARG;
   return guarded(nullptr, [&] {
-    const wl::ProgramAir prog = program_from(program);
+    const wl::ProgramAir prog = program_from(program, log_n);
     const wl::ProofJob job = make_program_job(s, hash_constants, log_n, &prog);
     return wl_status(wl::verify_air_proof(job.settings, job.air, job.p16, job.p24, log_n, proof, proof_len, nullptr, 0,
                                           nullptr, &prog));
@@ -314,7 +316,7 @@ wl_status wl_program_proof_len_bound(const wl_air_settings* s, const wl_air_prog
   std::string why;
   if (!out || !program || !settings_ok(s, log_n, why)) return WL_E_INVALID_ARG;
   try {
-    const wl::ProgramAir prog = program_from(program);
+    const wl::ProgramAir prog = program_from(program, log_n);
     *out = wl::proof_len_bound(to_settings(s), log_n, prog.W, prog.degree);
     return WL_OK;
   } catch (...) {

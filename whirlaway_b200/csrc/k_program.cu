@@ -34,7 +34,8 @@ __device__ __forceinline__ void prog_decode(uint2 in, int& op, int& dst, uint32_
   b = int(in.y);
 }
 
-__global__ void __launch_bounds__(PROG_THREADS) k_prog_zc0(const uint32_t* __restrict__ wit, int log_n, int k,
+__global__ void __launch_bounds__(PROG_THREADS) k_prog_zc0(const uint32_t* __restrict__ wit,
+                                                           const uint32_t* __restrict__ pre, int P, int log_n, int k,
                                                            const uint2* __restrict__ code, int n_code,
                                                            const uint32_t* __restrict__ consts,
                                                            const uint32_t* __restrict__ lw, const ef* __restrict__ eq,
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(PROG_THREADS) k_prog_zc0(const uint32_t* __res
       uint32_t a;
       prog_decode(__ldg(code + i), op, dst, a, b);
       if (op == PROG_UP || op == PROG_DOWN) {
-        const uint32_t* col = wit + size_t(a) * N;
+        const uint32_t* col = int(a) < P ? pre + size_t(a) * N : wit + size_t(int(a) - P) * N;
         uint64_t g[4] = {0, 0, 0, 0};  // at most four products of values below p per group
         for (int j = 0; j < nsk; j++) {
           const size_t r = size_t(j) * S + x;
@@ -85,9 +86,10 @@ __global__ void __launch_bounds__(PROG_THREADS) k_prog_zc0(const uint32_t* __res
 }
 
 // The 2W up/down columns folded over the skipped variables: out[c * S + x] =
-// sum_j sel[j] ud_c[j S + x] (c < W: up versions, c >= W: down versions).
-__global__ void k_prog_fold0(const uint32_t* __restrict__ wit, int log_n, int k, int W, const ef* __restrict__ sel,
-                             ef* __restrict__ out) {
+// sum_j sel[j] ud_c[j S + x] (c < W: up versions, c >= W: down versions). Columns below P are
+// the preprocessed ones (pre), the others the witness's (wit, column c - P).
+__global__ void k_prog_fold0(const uint32_t* __restrict__ wit, const uint32_t* __restrict__ pre, int P, int log_n,
+                             int k, int W, const ef* __restrict__ sel, ef* __restrict__ out) {
   __shared__ ef s_s[16];
   const int nsk = 1 << k;
   if (threadIdx.x < nsk) s_s[threadIdx.x] = sel[threadIdx.x];
@@ -95,7 +97,8 @@ __global__ void k_prog_fold0(const uint32_t* __restrict__ wit, int log_n, int k,
   const size_t N = size_t(1) << log_n, S = N >> k;
   const int c = blockIdx.y;
   const bool up = c < W;
-  const uint32_t* col = wit + size_t(up ? c : c - W) * N;
+  const int cc = up ? c : c - W;
+  const uint32_t* col = cc < P ? pre + size_t(cc) * N : wit + size_t(cc - P) * N;
   for (size_t x = size_t(blockIdx.x) * blockDim.x + threadIdx.x; x < S; x += size_t(gridDim.x) * blockDim.x) {
     ef acc = ef_zero();
     for (int j = 0; j < nsk; j++) {
@@ -176,19 +179,21 @@ int prog_zc_blocks(size_t rows) {
   return (int)std::max<size_t>(1, std::min<size_t>((rows + PROG_THREADS - 1) / PROG_THREADS, size_t(prog_sm_count()) * 4));
 }
 
-void launch_prog_zc0(const uint32_t* wit, int log_n, int k, const uint2* code, int n_code, const uint32_t* consts,
-                     int nz, const uint32_t* lw, const ef* eq, const ef* alphas, ef* partial, cudaStream_t s) {
+void launch_prog_zc0(const uint32_t* wit, const uint32_t* pre, int P, int log_n, int k, const uint2* code, int n_code,
+                     const uint32_t* consts, int nz, const uint32_t* lw, const ef* eq, const ef* alphas, ef* partial,
+                     cudaStream_t s) {
   if (k < 1 || k > 4 || k >= log_n) throw std::invalid_argument("program zerocheck: 1 <= skips <= 4, below log_n");
   if (nz < 1) return;
   const dim3 grid(prog_zc_blocks(size_t(1) << (log_n - k)), nz);
-  k_prog_zc0<<<grid, PROG_THREADS, 0, s>>>(wit, log_n, k, code, n_code, consts, lw, eq, alphas, partial);
+  k_prog_zc0<<<grid, PROG_THREADS, 0, s>>>(wit, pre, P, log_n, k, code, n_code, consts, lw, eq, alphas, partial);
   WL_LAUNCH_CHECK();
 }
 
-void launch_prog_fold0(const uint32_t* wit, int log_n, int k, int W, const ef* sel, ef* out, cudaStream_t s) {
+void launch_prog_fold0(const uint32_t* wit, const uint32_t* pre, int P, int log_n, int k, int W, const ef* sel, ef* out,
+                       cudaStream_t s) {
   const size_t S = size_t(1) << (log_n - k);
   const dim3 grid((unsigned)std::max<size_t>(1, std::min<size_t>((S + 255) / 256, 1024)), 2 * W);
-  k_prog_fold0<<<grid, 256, 0, s>>>(wit, log_n, k, W, sel, out);
+  k_prog_fold0<<<grid, 256, 0, s>>>(wit, pre, P, log_n, k, W, sel, out);
   WL_LAUNCH_CHECK();
 }
 

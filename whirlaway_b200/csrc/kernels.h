@@ -253,17 +253,19 @@ int fin_kind_sums(int kind);
 
 // --------------------------------------------------------------- constraint-program AIRs
 // Zerocheck kernels for AIRs given as constraint programs (air_program.h; code, consts: the
-// compiled instructions and Montgomery constants in device memory). Round 0: wit holds the W
-// columns (2^log_n Montgomery values each); lw the nz points' Lagrange weights (nz x 2^k, z =
+// compiled instructions and Montgomery constants in device memory). Round 0: of the W columns
+// (2^log_n Montgomery values each) the first P are in pre, the others in wit; lw the nz points' Lagrange weights (nz x 2^k, z =
 // 2^k ..); eq the eq table over the rows of the subcube (2^(log_n - k)); partial[b * nz + z] over
 // B = prog_zc_blocks(2^(log_n - k)) blocks. launch_prog_fold0 folds the 2W up/down columns over the
 // skipped variables with the weights sel (2^k extension values) into out[c * 2^(log_n - k) + x].
 // Rounds >= 1: cols holds 2W extension columns of 2^m; sums at the npts points 0, 2, 3, ..
 // weighted by eq (2^(m - 1)), partial[b * npts + z] over B = prog_zc_blocks(2^(m - 1)) blocks.
 int prog_zc_blocks(size_t rows);
-void launch_prog_zc0(const uint32_t* wit, int log_n, int k, const uint2* code, int n_code, const uint32_t* consts,
-                     int nz, const uint32_t* lw, const ef* eq, const ef* alphas, ef* partial, cudaStream_t s);
-void launch_prog_fold0(const uint32_t* wit, int log_n, int k, int W, const ef* sel, ef* out, cudaStream_t s);
+void launch_prog_zc0(const uint32_t* wit, const uint32_t* pre, int P, int log_n, int k, const uint2* code, int n_code,
+                     const uint32_t* consts, int nz, const uint32_t* lw, const ef* eq, const ef* alphas, ef* partial,
+                     cudaStream_t s);
+void launch_prog_fold0(const uint32_t* wit, const uint32_t* pre, int P, int log_n, int k, int W, const ef* sel, ef* out,
+                       cudaStream_t s);
 void launch_prog_zc_ef(const ef* cols, int m, int W, const uint2* code, int n_code, const uint32_t* consts, int npts,
                        const ef* eq, const ef* alphas, ef* partial, cudaStream_t s);
 // The inner phase's batched column over W columns: out[i] = sum_c eqc[c] wit[c 2^log_n + i].

@@ -859,18 +859,22 @@ size_t proof_len_bound(const Settings& s, int log_n, int W, int degree) {
 // crates/sumcheck/src/prove.rs:97-254 runs it on the 2W up/down columns: the sums from the
 // interpreter kernels, the round polynomial and challenge on the host transcript, the fold of
 // all 2W columns after every round; the last folds are the up and down evaluations.
+// The first P of the W columns are preprocessed (in the zerocheck, not committed): up and down
+// receive the witness columns' evaluations only.
 void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const ProgramAir& prog, const uint32_t* wit,
                        const DBuf& d_alphas, const std::vector<ef>& zc, const DBuf& eq0, std::vector<ef>& challenges,
                        std::vector<ef>& up, std::vector<ef>& down) {
   const Settings& s = job.settings;
-  const int n = job.log_n, k = s.univariate_skips, W = prog.W, d = prog.degree, nsk = 1 << k, R = n - k;
+  const int n = job.log_n, k = s.univariate_skips, W = prog.W, P = prog.P, d = prog.degree, nsk = 1 << k, R = n - k;
   const size_t S = size_t(1) << R;
   cudaStream_t st = ctx.stream;
+  if (P > 0 && prog.pre_log_n != n) throw std::invalid_argument("AIR program: preprocessed columns of another height");
   const int n_code = (int)prog.code.size();
   DBuf code = upload(ctx, prog.code);
   std::vector<uint32_t> cv = prog.consts;
   if (cv.empty()) cv.push_back(0);
   DBuf consts = upload(ctx, cv);
+  DBuf pre = P > 0 ? upload(ctx, prog.pre) : DBuf(sizeof(uint32_t), st);
   const auto& sel = lagrange_basis_cached(nsk);
   // round 0: the values at z < 2^k vanish; the kernel sums z = 2^k .. d (2^k - 1)
   const int nz = d * (nsk - 1) - nsk + 1;
@@ -884,8 +888,8 @@ void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const 
     ef* part = ctx.partials(size_t(B) * nz);
     {
       ProfScope _ps(ctx, "prog_zc0");
-      launch_prog_zc0(wit, n, k, code.as<uint2>(), n_code, consts.as<uint32_t>(), nz, d_lw.as<uint32_t>(),
-                      eq0.as<ef>(), d_alphas.as<ef>(), part, st);
+      launch_prog_zc0(wit, pre.as<uint32_t>(), P, n, k, code.as<uint2>(), n_code, consts.as<uint32_t>(), nz,
+                      d_lw.as<uint32_t>(), eq0.as<ef>(), d_alphas.as<ef>(), part, st);
     }
     const std::vector<ef> sums = reduce_to_host(ctx, part, B, nz);
     ys.insert(ys.end(), sums.begin(), sums.end());
@@ -911,7 +915,7 @@ void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const 
   {
     DBuf d_sel = upload(ctx, selr);
     ProfScope _ps(ctx, "prog_fold0");
-    launch_prog_fold0(wit, n, k, W, d_sel.as<ef>(), cols.as<ef>(), st);
+    launch_prog_fold0(wit, pre.as<uint32_t>(), P, n, k, W, d_sel.as<ef>(), cols.as<ef>(), st);
   }
   // rounds >= 1: sums at z = 0, 2, .., d; z = 1 from the claim
   DBuf eqr;
@@ -958,15 +962,15 @@ void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const 
   }
   std::vector<ef> fin(size_t(2) * W);
   ctx.to_host(fin.data(), cols.as<ef>(), sizeof(ef) * fin.size());
-  up.assign(fin.begin(), fin.begin() + W);
-  down.assign(fin.begin() + W, fin.end());
+  up.assign(fin.begin() + P, fin.begin() + W);
+  down.assign(fin.begin() + W + P, fin.end());
 }
 
 std::vector<uint32_t> prove_air(Context& ctx, const ProofJob& job, const uint32_t* wit, Timings* tm,
                                 const std::vector<cudaEvent_t>* tile_ready) {
   const Settings& s = job.settings;
   const ProgramAir* prog = job.prog;
-  const int n = job.log_n, k = s.univariate_skips, W = prog ? prog->W : AIR_W;
+  const int n = job.log_n, k = s.univariate_skips, W = prog ? prog->witness_columns() : AIR_W;
   const int NC = prog ? prog->NC : AIR_NC, LOGW = log2_up(size_t(W));
   if (k >= n) throw std::invalid_argument("univariate_skips must be smaller than log_n_rows");
   if (s.fold_first != 7 || s.fold_rest != 4) throw std::invalid_argument("folding factors other than (7, 4)");
@@ -1425,7 +1429,7 @@ std::vector<uint32_t> prove_air_host(Context& ctx, const ProofJob& job, const ui
   const size_t N = size_t(1) << job.log_n;
   if (job.prog) {
     // a constraint-program AIR: the whole witness, then the proof
-    const size_t words = N * size_t(job.prog->W);
+    const size_t words = N * size_t(job.prog->witness_columns());
     DBuf wit(sizeof(uint32_t) * words, ctx.stream);
     WL_CUDA(cudaMemcpyAsync(wit.as<uint32_t>(), wit_host, sizeof(uint32_t) * words, cudaMemcpyHostToDevice,
                             ctx.stream));

@@ -370,8 +370,11 @@ class WhirVerifier {
 int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Consts& p16, const kb::P24Consts& p24,
                      int n, const uint32_t* proof, size_t proof_len, TranscriptLog* log, int threads,
                      std::vector<MerkleOpening>* defer, const ProgramAir* prog) {
-  const int k = s.univariate_skips, W = prog ? prog->W : AIR_W, nsk = 1 << k;
+  // W: the witness (committed) columns; the program's first P columns are preprocessed
+  const int k = s.univariate_skips, W = prog ? prog->witness_columns() : AIR_W, nsk = 1 << k;
   const int NC = prog ? prog->NC : AIR_NC, LOGW = log2_up(size_t(W)), d1 = (prog ? prog->degree : 3) + 1;
+  const int P = prog ? prog->P : 0;
+  if (P > 0 && prog->pre_log_n != n) return VERIFY_FS;
   const WhirSchedule ws = WhirSchedule::build(n + LOGW, s);
   ProofReader rd(&p16, proof, proof_len, log);
   for (uint32_t x : ws.domain_separator()) rd.ch.observe(kb::to_mont(x));
@@ -410,8 +413,34 @@ int verify_air_proof(const Settings& s, const AirConsts& air, const kb::P16Const
   std::vector<ef> alphas(NC);
   alphas[0] = kb::ef_one();
   for (int i = 1; i < NC; i++) alphas[i] = kb::ef_mul(alphas[i - 1], alpha);
-  const ef constraints = prog ? prog->eval_ef(up.data(), down.data(), alphas.data())
-                              : air_eval_ef(air, alphas.data(), [&](int c) { return up[c]; });
+  ef constraints;
+  if (prog) {
+    // the preprocessed columns' up / down versions folded over the skipped variables at the
+    // outer challenge and evaluated at its tail (crates/air/src/verify.rs:119-135)
+    const size_t N = size_t(1) << n, S = N >> k;
+    const std::vector<ef> otail(outer.point.begin() + 1, outer.point.end());
+    std::vector<ef> gup(P + W), gdown(P + W);
+    for (int c = 0; c < P; c++) {
+      const uint32_t* col = prog->pre.data() + size_t(c) * N;
+      for (int half = 0; half < 2; half++) {
+        std::vector<ef> f(S);
+        for (size_t x = 0; x < S; x++) {
+          ef acc = kb::ef_zero();
+          for (int j = 0; j < nsk; j++) {
+            const size_t r = size_t(j) * S + x;
+            const size_t src = half == 0 ? (r == N - 1 ? N - 2 : r) : (r == N - 1 ? r : r + 1);
+            acc = kb::ef_add(acc, kb::ef_mul_f(outer_sel[j], col[src]));
+          }
+          f[x] = acc;
+        }
+        (half == 0 ? gup : gdown)[c] = mle_eval(f, otail);
+      }
+    }
+    for (int c = 0; c < W; c++) gup[P + c] = up[c], gdown[P + c] = down[c];
+    constraints = prog->eval_ef(gup.data(), gdown.data(), alphas.data());
+  } else {
+    constraints = air_eval_ef(air, alphas.data(), [&](int c) { return up[c]; });
+  }
   const std::vector<ef> zc_tail(zc.begin() + 1, zc.end()), outer_tail(outer.point.begin() + 1, outer.point.end());
   if (!kb::ef_eq(kb::ef_mul(kb::ef_mul(sel_dot, eq_eval(zc_tail, outer_tail)), constraints), outer.value))
     return VERIFY_SUM_MISMATCH;
