@@ -203,8 +203,10 @@ def test_malformed_programs_rejected(hash_consts):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(AIRS))
-@pytest.mark.parametrize("log_n,skips", [(8, 1), (10, 4), (12, 3)])
+@pytest.mark.parametrize("log_n,skips", [(8, 1), (10, 4), (12, 3), (18, 1)])
 def test_gpu_program_matches_oracle(oracle, hash_consts, name, log_n, skips):
+    """(18, 1): 2^17 rows per round-0 point, more than the interpreter grid's threads, so the
+    grid-stride loops and the multi-block reductions run."""
     import whirlaway_b200 as wl
     prog, w = AIRS[name](log_n)
     want = oracle.prove_program(log_n, hash_consts, prog, w, settings_arr(skips))
