@@ -61,14 +61,15 @@ struct NttLane {
   int Bp;
 };
 
-// One register round: stages b0..b0+RB-1 (local numbering) on the groups of 2^RB points
-// j = base + (k << b0) handled by this warp. `tws` is this lane's twiddle table: entry
+// One register round: stages b0..b0+RB-1 (local numbering, b0 = B0) on the groups of 2^RB
+// points j = base + (k << b0) handled by this warp, in a pass of BP stages (both compile-time,
+// so the shared-memory and twiddle offsets below are immediates). `tws` is this lane's twiddle table: entry
 // 2^tl - 1 + r is the factor of local stage tl for j mod 2^tl = r. Addresses are formed
 // once per group (a base pointer and a stride); the source range is checked once per group.
-template <int RB, int IN, int OUT>
-__device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, int b0, int warp, bool active) {
-  constexpr int R = 1 << RB;
-  const uint32_t groups = 1u << (ln.Bp - RB);
+template <int RB, int B0, int BP, int IN, int OUT>
+__device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, int warp, bool active) {
+  constexpr int R = 1 << RB, b0 = B0;
+  constexpr uint32_t groups = 1u << (BP - RB);
   for (uint32_t g = warp; g < groups; g += NTT_WARPS) {
     const uint32_t base = (g & ((1u << b0) - 1)) | ((g >> b0) << (b0 + RB));
     if (!active) continue;
@@ -120,25 +121,28 @@ __device__ __forceinline__ void ntt_round(const NttLane& ln, const uint2* tws, i
   }
 }
 
-template <int IN, int OUT>
-__device__ __forceinline__ void ntt_round_rb(int rb, const NttLane& ln, const uint2* tws, int b0, int warp,
-                                             bool active) {
-  switch (rb) {
-    case 0: ntt_round<0, IN, OUT>(ln, tws, b0, warp, active); break;
-    case 1: ntt_round<1, IN, OUT>(ln, tws, b0, warp, active); break;
-    case 2: ntt_round<2, IN, OUT>(ln, tws, b0, warp, active); break;
-    case 3: ntt_round<3, IN, OUT>(ln, tws, b0, warp, active); break;
-    default: ntt_round<4, IN, OUT>(ln, tws, b0, warp, active); break;
+// The two register rounds of a pass of BP stages (ceil(BP/2) then floor(BP/2) stages, one
+// shared-memory exchange between them); the first reads from IN, the last writes the codeword.
+template <int BP, int IN>
+__device__ __forceinline__ void ntt_rounds(const NttLane& ln, const uint2* tws, int warp, bool active) {
+  constexpr int RB1 = (BP + 1) / 2, RB2 = BP - RB1;
+  if constexpr (RB2 == 0) {
+    ntt_round<RB1, 0, BP, IN, IO_GLOBAL>(ln, tws, warp, active);
+  } else {
+    ntt_round<RB1, 0, BP, IN, IO_SMEM>(ln, tws, warp, active);
+    __syncthreads();
+    ntt_round<RB2, RB1, BP, IO_SMEM, IO_GLOBAL>(ln, tws, warp, active);
   }
 }
 
 // One pass over stages Bs+1..Bs+Bp (global numbering) for the lines of one tile.
 // blockIdx.x = (hi group << (Bs - lr_log)) | lo group; 2^lr_log lo values and 2^hg_log hi
 // values per block. The first pass (FROM_SRC, Bs = rho) reads the commitment source.
-template <bool FROM_SRC>
+template <bool FROM_SRC, int BP>
 __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint32_t* __restrict__ data, int T,
-                                                            int Bs, int Bp, int rb1, int lr_log, int hg_log,
+                                                            int Bs, int lr_log, int hg_log,
                                                             const uint2* __restrict__ tw, int tile0) {
+  constexpr int Bp = BP;
   const int tile = tile0 + blockIdx.y;
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t npts = 1u << Bp, ntw = npts - 1;
@@ -173,16 +177,7 @@ __global__ void __launch_bounds__(NTT_WARPS * 32) k_ntt_pass(LdeSource in, uint3
   ln.X = sm + lane;
   ln.Bp = Bp;
   const uint2* tws = TW + l * ntw;
-  const int rb2 = Bp - rb1;
-  if (rb2 == 0) {
-    if (FROM_SRC) ntt_round_rb<IO_SRC, IO_GLOBAL>(rb1, ln, tws, 0, warp, active);
-    else ntt_round_rb<IO_GLOBAL, IO_GLOBAL>(rb1, ln, tws, 0, warp, active);
-    return;
-  }
-  if (FROM_SRC) ntt_round_rb<IO_SRC, IO_SMEM>(rb1, ln, tws, 0, warp, active);
-  else ntt_round_rb<IO_GLOBAL, IO_SMEM>(rb1, ln, tws, 0, warp, active);
-  __syncthreads();
-  ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb2, ln, tws, rb1, warp, active);
+  ntt_rounds<BP, FROM_SRC ? IO_SRC : IO_GLOBAL>(ln, tws, warp, active);
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem) {
@@ -200,9 +195,11 @@ __device__ __forceinline__ void cp_async_wait16() { asm volatile("cp.async.wait_
 // one is transformed: the first register round reads and writes shared memory in place, the
 // second writes the codeword. Twiddles are reloaded when the lo group changes.
 constexpr int NTT_ASYNC_BLOCKS_PER_SM = 4;
-__global__ void __launch_bounds__(NTT_WARPS * 32, NTT_ASYNC_BLOCKS_PER_SM) k_ntt_pass_async(uint32_t* __restrict__ data, int T, int Bs, int Bp,
-                                                                  int rb1, const uint2* __restrict__ tw, int tile0,
-                                                                  int tiles, uint32_t nlines, uint32_t per_block) {
+template <int BP>
+__global__ void __launch_bounds__(NTT_WARPS * 32, NTT_ASYNC_BLOCKS_PER_SM)
+    k_ntt_pass_async(uint32_t* __restrict__ data, int T, int Bs, const uint2* __restrict__ tw, int tile0, int tiles,
+                     uint32_t nlines, uint32_t per_block) {
+  constexpr int Bp = BP;
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t npts = 1u << Bp, ntw = npts - 1;
   uint2* TW = reinterpret_cast<uint2*>(sm + (npts << 6));  // [4][2^Bp - 1]
@@ -232,7 +229,6 @@ __global__ void __launch_bounds__(NTT_WARPS * 32, NTT_ASYNC_BLOCKS_PER_SM) k_ntt
     }
     cp_async_commit16();
   };
-  const int rb2 = Bp - rb1;
   uint32_t cur_lg = ~0u;
   prefetch(first, sm);
   for (uint32_t id = first, it = 0; id < last; id++, it++) {
@@ -267,13 +263,7 @@ __global__ void __launch_bounds__(NTT_WARPS * 32, NTT_ASYNC_BLOCKS_PER_SM) k_ntt
     ln.X = X + lane;
     ln.Bp = Bp;
     const uint2* tws = TW + l * ntw;
-    if (rb2 == 0) {
-      ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb1, ln, tws, 0, warp, true);
-    } else {
-      ntt_round_rb<IO_SMEM, IO_SMEM>(rb1, ln, tws, 0, warp, true);
-      __syncthreads();
-      ntt_round_rb<IO_SMEM, IO_GLOBAL>(rb2, ln, tws, rb1, warp, true);
-    }
+    ntt_rounds<BP, IO_SMEM>(ln, tws, warp, true);
     __syncthreads();  // X is free for the prefetch two lines ahead
   }
 }
@@ -619,6 +609,7 @@ int ntt_sm_count() {
 }
 // Opts the double-buffered pass into more than 48 KB of dynamic shared memory (once per
 // device and size).
+template <int BP>
 void ntt_async_smem_limit(size_t bytes) {
   if (bytes <= 48 * 1024) return;
   static std::mutex mu;
@@ -627,8 +618,47 @@ void ntt_async_smem_limit(size_t bytes) {
   WL_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (done[dev] >= bytes) return;
-  WL_CUDA(cudaFuncSetAttribute(k_ntt_pass_async, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  WL_CUDA(cudaFuncSetAttribute(k_ntt_pass_async<BP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
   done[dev] = bytes;
+}
+// Launches one pass of BP stages: the first (from the commitment source), a later one-shot
+// pass, or the double-buffered persistent pass.
+enum NttPassKind { NTT_FIRST, NTT_LATER, NTT_ASYNC };
+struct NttPassArgs {
+  LdeSource in;
+  uint32_t* out;
+  int T, Bs, lr_log, hg_log, tile0, tiles;
+  const uint2* tw;
+  dim3 grid;
+  size_t smem;
+  uint32_t nlines, per;
+};
+template <int BP>
+void ntt_pass_launch(NttPassKind kind, const NttPassArgs& a, cudaStream_t s) {
+  if (kind == NTT_FIRST) {
+    k_ntt_pass<true, BP><<<a.grid, NTT_WARPS * 32, a.smem, s>>>(a.in, a.out, a.T, a.Bs, a.lr_log, a.hg_log, a.tw,
+                                                                 a.tile0);
+  } else if (kind == NTT_LATER) {
+    k_ntt_pass<false, BP><<<a.grid, NTT_WARPS * 32, a.smem, s>>>(a.in, a.out, a.T, a.Bs, a.lr_log, a.hg_log, a.tw,
+                                                                  a.tile0);
+  } else {
+    ntt_async_smem_limit<BP>(a.smem);
+    k_ntt_pass_async<BP><<<a.grid, NTT_WARPS * 32, a.smem, s>>>(a.out, a.T, a.Bs, a.tw, a.tile0, a.tiles, a.nlines,
+                                                                 a.per);
+  }
+}
+void ntt_pass_dispatch(int Bp, NttPassKind kind, const NttPassArgs& a, cudaStream_t s) {
+  switch (Bp) {
+    case 1: ntt_pass_launch<1>(kind, a, s); break;
+    case 2: ntt_pass_launch<2>(kind, a, s); break;
+    case 3: ntt_pass_launch<3>(kind, a, s); break;
+    case 4: ntt_pass_launch<4>(kind, a, s); break;
+    case 5: ntt_pass_launch<5>(kind, a, s); break;
+    case 6: ntt_pass_launch<6>(kind, a, s); break;
+    case 7: ntt_pass_launch<7>(kind, a, s); break;
+    case 8: ntt_pass_launch<8>(kind, a, s); break;
+    default: throw std::runtime_error("NTT pass of 1..8 stages");
+  }
 }
 }  // namespace
 
@@ -648,7 +678,6 @@ void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_
   int Bs = in.rho, left = in.L;
   for (int p = 0; p < np; p++) {
     const int Bp = (left + (np - p) - 1) / (np - p);
-    const int rb1 = (Bp + 1) / 2;
     const int lr_log = Bs < 2 ? Bs : 2;
     const int hi_bits = T - Bs - Bp;
     const int hg_log = (2 - lr_log) < hi_bits ? (2 - lr_log) : hi_bits;
@@ -658,18 +687,17 @@ void launch_lde(const LdeSource& in, uint32_t* out, const uint2* tw, cudaStream_
     const size_t smem2 = ((size_t(64) << Bp) + size_t(8) * ((1u << Bp) - 1)) * 4;
     const uint32_t per_sm = std::min<uint32_t>(async_per_sm, uint32_t((227 * 1024) / (smem2 + 1024)));
     const uint32_t nblk = uint32_t(ntt_sm_count()) * std::max<uint32_t>(per_sm, 1);
+    NttPassArgs a{in, out, T, Bs, lr_log, hg_log, tile_begin, tiles, tw, dim3(gx, tiles), smem, nlines, 0};
     if (p == 0) {
-      k_ntt_pass<true><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
-                                                                      tile_begin);
+      ntt_pass_dispatch(Bp, NTT_FIRST, a, s);
     } else if (lr_log == 2 && hg_log == 0 && nlines >= 4 * nblk) {
       // enough lines for every block to pipeline several: the double-buffered kernel
-      const uint32_t per = (nlines + nblk - 1) / nblk;
-      ntt_async_smem_limit(smem2);
-      k_ntt_pass_async<<<(nlines + per - 1) / per, NTT_WARPS * 32, smem2, s>>>(out, T, Bs, Bp, rb1, tw, tile_begin,
-                                                                               tiles, nlines, per);
+      a.per = (nlines + nblk - 1) / nblk;
+      a.grid = dim3((nlines + a.per - 1) / a.per);
+      a.smem = smem2;
+      ntt_pass_dispatch(Bp, NTT_ASYNC, a, s);
     } else {
-      k_ntt_pass<false><<<dim3(gx, tiles), NTT_WARPS * 32, smem, s>>>(in, out, T, Bs, Bp, rb1, lr_log, hg_log, tw,
-                                                                       tile_begin);
+      ntt_pass_dispatch(Bp, NTT_LATER, a, s);
     }
     WL_LAUNCH_CHECK();
     Bs += Bp;
