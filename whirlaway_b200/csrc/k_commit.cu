@@ -449,12 +449,17 @@ __device__ __forceinline__ uint32_t mds16_lanes(uint32_t a, int i) {
   t = kb::add(t, __shfl_xor_sync(0xffffffffu, t, 8, 16));
   return kb::add(y, t);
 }
-__device__ uint32_t p2_permute16_lanes(uint32_t v, const kb::P16Consts& c) {
+// rc_s: the full-round constants in shared memory (initial rounds at 0, terminal at 64): each
+// lane reads its own word, which from the constant bank would serialise across the warp.
+__device__ __forceinline__ void stage_p16_full_rounds(uint32_t* rc_s, const kb::P16Consts& c) {
+  for (int q = threadIdx.x; q < 128; q += blockDim.x) rc_s[q] = q < 64 ? c.ext_init[q] : c.ext_term[q - 64];
+}
+__device__ uint32_t p2_permute16_lanes(uint32_t v, const uint32_t* rc_s, const kb::P16Consts& c) {
   const int i = threadIdx.x & 15;
   const uint32_t dg = kb::p2_diag<16>(i);
   v = mds16_lanes(v, i);
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + c.ext_init[r * 16 + i]), i);
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + rc_s[r * 16 + i]), i);
 #pragma unroll 1
   for (int r = 0; r < 20; r++) {
     if (i == 0) v = kb::cube_fq(v + c.internal[r]);
@@ -464,12 +469,15 @@ __device__ uint32_t p2_permute16_lanes(uint32_t v, const kb::P16Consts& c) {
     v = kb::add(kb::mul(v, dg), sum);
   }
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + c.ext_term[r * 16 + i]), i);
+  for (int r = 0; r < 4; r++) v = mds16_lanes(kb::cube_fq(v + rc_s[64 + r * 16 + i]), i);
   return v;
 }
 
 // One level l of the tree, 16 lanes per compression (grid covers 16 * 2^(LL-l) threads).
 __global__ void k_merkle_level_lanes(uint32_t* __restrict__ tree, int LL, int l, const __grid_constant__ kb::P16Consts c) {
+  __shared__ uint32_t rc_s[128];
+  stage_p16_full_rounds(rc_s, c);
+  __syncthreads();
   const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const size_t m = t >> 4;
   const int i = threadIdx.x & 15;
@@ -478,20 +486,23 @@ __global__ void k_merkle_level_lanes(uint32_t* __restrict__ tree, int LL, int l,
   const size_t warp_first = (t & ~size_t(31)) >> 4;
   if (warp_first >= cnt) return;  // whole warp idle (uniform per warp)
   uint32_t v = act ? tree[(tree_off(LL, l - 1) + 2 * m) * 8 + i] : 0u;
-  v = p2_permute16_lanes(v, c);
+  v = p2_permute16_lanes(v, rc_s, c);
   if (act && i < 8) tree[(tree_off(LL, l) + m) * 8 + i] = v;
 }
 
 // Levels l0+1 .. LL in one block of 1024 threads (at most 64 compressions per level).
 __global__ void __launch_bounds__(1024) k_merkle_top(uint32_t* __restrict__ tree, int LL, int l0,
                                                      const __grid_constant__ kb::P16Consts c) {
+  __shared__ uint32_t rc_s[128];
+  stage_p16_full_rounds(rc_s, c);
+  __syncthreads();
   const int g = threadIdx.x >> 4, i = threadIdx.x & 15;
   for (int l = l0 + 1; l <= LL; l++) {
     const int cnt = 1 << (LL - l);
     if ((threadIdx.x >> 5) * 2 < cnt) {  // warps holding at least one live compression
       const bool act = g < cnt;
       uint32_t v = act ? tree[(tree_off(LL, l - 1) + 2 * size_t(g)) * 8 + i] : 0u;
-      v = p2_permute16_lanes(v, c);
+      v = p2_permute16_lanes(v, rc_s, c);
       if (act && i < 8) tree[(tree_off(LL, l) + g) * 8 + i] = v;
     }
     __syncthreads();
