@@ -191,14 +191,32 @@ def test_malformed_programs_rejected(hash_consts):
     bad = ap.AirProgram(prog.width, prog.n_constraints, prog.degree, prog.ops.copy(), prog.consts)
     bad.ops[2, 1] = 5  # an operand that is not an earlier value
     assert wl.verify_program(hash_consts, bad, 8, np.zeros(8, np.uint32), wl_settings()) == 1
+    # 70 values live at once (all made before they are summed): beyond the device interpreter's
+    # 64 registers, so the library rejects the program as an argument error
     wide = ap.AirBuilder(1)
-    vals = [wide.up(0) + i for i in range(70)]  # 70 values live at once
-    acc = vals[0]
-    for v in vals[1:]:
-        acc = acc * v
-    wide.assert_zero(acc - acc)
-    with pytest.raises(Exception):
-        wl.verify_program(hash_consts, wide.build(3), 8, np.zeros(8, np.uint32), wl_settings())
+    vals = [wide.up(0) + i for i in range(1, 71)]
+    acc = vals[-1]
+    for v in reversed(vals[:-1]):
+        acc = acc + v
+    wide.assert_zero(acc)
+    prog_wide = wide.build()
+    assert prog_wide.degree == 1
+    assert wl.verify_program(hash_consts, prog_wide, 8, np.zeros(8, np.uint32), wl_settings()) == 1
+    # a constant that is not a canonical field element, and no EMIT for a declared constraint
+    b = ap.AirBuilder(2)
+    b.assert_zero(b.up(0) - b.up(1))
+    p2 = b.build()
+    bad_c = ap.AirProgram(2, 1, 1, p2.ops, np.array([P], np.uint32))
+    bad_c.ops = np.array([[ap.OP_CONST, 0, 0], [ap.OP_EMIT, 0, 0]], np.int32)
+    assert wl.verify_program(hash_consts, bad_c, 8, np.zeros(8, np.uint32), wl_settings()) == 1
+    two = ap.AirProgram(2, 2, 1, p2.ops, p2.consts)
+    assert wl.verify_program(hash_consts, two, 8, np.zeros(8, np.uint32), wl_settings()) == 1
+    with pytest.raises(ValueError):
+        ap.AirProgram(2, 1, 1, p2.ops, p2.consts, n_preprocessed=2)
+    # preprocessed values must come with a program that has preprocessed columns
+    prog_pre, _, _ = pre_air(8)
+    with pytest.raises(ValueError):
+        wl.verify_program(hash_consts, prog_pre, 8, np.zeros(8, np.uint32), wl_settings())
 
 
 @pytest.mark.gpu
