@@ -152,6 +152,9 @@ int main() {
       for (int i = 0; i < W; i++) sc[i] = s[i];
       if (w) p2_permute_fq<24>(sc, p2_consts_canonical(c24)); else p2_permute_fq<16>(sc, p2_consts_canonical(c16));
       for (int i = 0; i < W; i++) if (sc[i] != r[i]) { b8++; break; }
+      for (int i = 0; i < W; i++) sc[i] = s[i];  // full rounds in fp64
+      if (w) p2_permute_fd<24>(sc, p2_consts_fd(c24)); else p2_permute_fd<16>(sc, p2_consts_fd(c16));
+      for (int i = 0; i < W; i++) if (sc[i] != r[i]) { b8++; break; }
       for (int i = 0; i < W; i++) s[i] = to_mont(s[i]);
       uint32_t sv[16];
       for (int i = 0; i < 16; i++) sv[i] = s[i];
@@ -162,6 +165,28 @@ int main() {
         for (int i = 0; i < 16; i++) if (sv[i] != s[i]) { b8++; break; }
       }
     }
+  }
+  // the fp64 S-box and canonical reduction over the whole input range of the fp64 full rounds:
+  // signed integers below 49 * 2^32 + p in magnitude, at the ends and at random
+  {
+    const int64_t zmax = 49 * (int64_t(1) << 32) + P;
+    auto cube_ref = [&](int64_t z) {
+      const uint32_t u = uint32_t(((z % int64_t(P)) + int64_t(P)) % int64_t(P));
+      return pm(pm(u, u), u);
+    };
+    auto check = [&](int64_t z) {
+      const double zd = double(z);
+      const double c = sbox_fd(zd);
+      const int64_t ci = int64_t(c);
+      if (double(ci) != c || ci <= -int64_t(P) || ci >= int64_t(P) ||
+          uint32_t(((ci % int64_t(P)) + int64_t(P)) % int64_t(P)) != cube_ref(z)) b7++;
+      if (fd_canonical(zd) != uint32_t(((z % int64_t(P)) + int64_t(P)) % int64_t(P))) b7++;
+    };
+    for (int64_t e : {int64_t(0), int64_t(1), int64_t(P) - 1, int64_t(P), int64_t(P) + 1, zmax - 1, int64_t(1) << 32})
+      check(e), check(-e);
+    for (int64_t k = -60; k <= 60; k++) check(k * int64_t(P)), check(k * int64_t(P) + 1), check(k * int64_t(P) - 1),
+        check(k * int64_t(P) + (int64_t(P) >> 1)), check(k * int64_t(P) - (int64_t(P) >> 1));
+    for (int it = 0; it < 1000000; it++) check(int64_t(g() % uint64_t(2 * zmax - 1)) - (zmax - 1));
   }
   printf("add %ld sub %ld mul %ld diag %ld halve %ld redc %ld cube %ld permute %ld\n", b1,b2,b3,b4,b5,b6,b7,b8);
   return (b1 + b2 + b3 + b4 + b5 + b6 + b7 + b8) ? 1 : 0;

@@ -324,7 +324,7 @@ __device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ lde, int
 }
 
 // The tree holds canonical digests: the permutations run in the canonical domain (see
-// p2_permute_fq), the absorbed LDE entries are converted from Montgomery form, and the host
+// p2_permute_fd), the absorbed LDE entries are converted from Montgomery form, and the host
 // converts the root and the opened digests back.
 //
 // Absorbs chunk ch of LDE row `row` into the sponge state st (the chunk overwrites the rate
@@ -334,7 +334,7 @@ __device__ __forceinline__ void leaf_chunk(const uint32_t* __restrict__ lde, int
 // chunk ch is the signed sum of the chunks below it, and bits below 4 are transformed inside
 // the chunk. Then the permutation.
 __device__ __forceinline__ void leaf_absorb(const uint32_t* __restrict__ lde, int T, size_t row, int n_cols,
-                                            int log_elem, int ch, const kb::P24Consts& c, uint32_t* st) {
+                                            int log_elem, int ch, const kb::P2ConstsFd<24>& c, uint32_t* st) {
   const int cmask = log_elem <= 4 ? 7 : (7 << (log_elem - 4)) & 7;  // chunk bits in the transform
   leaf_chunk(lde, T, row, n_cols, ch, 0, st);
   const int m = ch & cmask;
@@ -356,7 +356,7 @@ __device__ __forceinline__ void leaf_absorb(const uint32_t* __restrict__ lde, in
   }
 #pragma unroll
   for (int i = 0; i < 16; i++) st[i] = kb::from_mont(st[i]);
-  kb::p2_permute_fq<24>(st, c);
+  kb::p2_permute_fd<24>(st, c);
 }
 
 // Leaf digests (level 0 of the tree), one row per thread: each thread hashes one row of 128
@@ -365,7 +365,7 @@ __device__ __forceinline__ void leaf_absorb(const uint32_t* __restrict__ lde, in
 // registers).
 template <int ROWS>
 __global__ void __launch_bounds__(ROWS) k_leaf_hash(const uint32_t* __restrict__ lde, int T, int n_cols,
-                                                    int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                    int log_elem, const __grid_constant__ kb::P2ConstsFd<24> c,
                                                     uint32_t* __restrict__ tree) {
   const size_t row0 = size_t(blockIdx.x) * ROWS;
   const size_t rows = size_t(1) << T;
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(ROWS) k_leaf_hash(const uint32_t* __restrict__
 // as soon as the LDE tiles it reads exist. The last chunk writes the digests.
 template <int ROWS>
 __global__ void __launch_bounds__(ROWS) k_leaf_absorb(const uint32_t* __restrict__ lde, int T, int n_cols,
-                                                      int log_elem, const __grid_constant__ kb::P24Consts c,
+                                                      int log_elem, const __grid_constant__ kb::P2ConstsFd<24> c,
                                                       int ch, uint32_t* __restrict__ cap,
                                                       uint32_t* __restrict__ tree) {
   const size_t row = size_t(blockIdx.x) * ROWS + threadIdx.x;
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(ROWS) k_leaf_absorb(const uint32_t* __restrict
 }
 
 // Level l of the tree from level l - 1, one 2-to-1 compression per thread.
-__global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const __grid_constant__ kb::P16Consts c) {
+__global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const __grid_constant__ kb::P2ConstsFd<16> c) {
   const size_t m = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (m >= (size_t(1) << (LL - l))) return;
   const uint4* src = reinterpret_cast<const uint4*>(tree + (tree_off(LL, l - 1) + 2 * m) * 8);
@@ -425,7 +425,7 @@ __global__ void k_merkle_level(uint32_t* __restrict__ tree, int LL, int l, const
     const uint4 u = src[q];
     st[4 * q] = u.x, st[4 * q + 1] = u.y, st[4 * q + 2] = u.z, st[4 * q + 3] = u.w;
   }
-  kb::p2_permute_fq<16>(st, c);
+  kb::p2_permute_fd<16>(st, c);
   uint4* o = reinterpret_cast<uint4*>(tree + (tree_off(LL, l) + m) * 8);
   o[0] = make_uint4(st[0], st[1], st[2], st[3]);
   o[1] = make_uint4(st[4], st[5], st[6], st[7]);
@@ -729,7 +729,7 @@ void launch_leaf_hash(const uint32_t* lde, size_t rows, int n_cols, int elem, co
                       uint32_t* tree, int LL, cudaStream_t s, int rows_choice) {
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
-  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
+  const kb::P2ConstsFd<24> p24c = kb::p2_consts_fd(p24);
   switch (rows_choice) {
     case 0: k_leaf_hash<64><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(lde, LL, n_cols, log_elem, p24c, tree); break;
     case 2: k_leaf_hash<256><<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(lde, LL, n_cols, log_elem, p24c, tree); break;
@@ -743,7 +743,7 @@ void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, 
   const int log_elem = elem == 8 ? 3 : 0;
   if (rows != (size_t(1) << LL) || n_cols % 8) throw std::runtime_error("Merkle leaves: 2^LL rows, columns in tiles of 8");
   if (ch < 0 || ch > 7) throw std::invalid_argument("leaf chunk out of range");
-  const kb::P24Consts p24c = kb::p2_consts_canonical(p24);
+  const kb::P2ConstsFd<24> p24c = kb::p2_consts_fd(p24);
   switch (rows_choice) {
     case 0: k_leaf_absorb<64><<<(unsigned)((rows + 63) / 64), 64, 0, s>>>(lde, LL, n_cols, log_elem, p24c, ch, cap, tree); break;
     case 2: k_leaf_absorb<256><<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(lde, LL, n_cols, log_elem, p24c, ch, cap, tree); break;
@@ -754,6 +754,7 @@ void launch_leaf_absorb(const uint32_t* lde, size_t rows, int n_cols, int elem, 
 
 void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cudaStream_t s, int plan) {
   const kb::P16Consts p16c = kb::p2_consts_canonical(p16);
+  const kb::P2ConstsFd<16> p16d = kb::p2_consts_fd(p16);
   // Wide levels: one launch each, one compression per thread. Narrower levels: 16 lanes per
   // compression. The last levels (at most 128 digests) in one block. The plan sets the width
   // from which a level runs one compression per thread: 2^11, 2^13 (default) or 2^15 digests.
@@ -761,7 +762,7 @@ void launch_merkle_levels(uint32_t* tree, int LL, const kb::P16Consts& p16, cuda
   int l0 = 0;
   while (l0 < LL && LL - l0 - 1 >= flat_min) {
     const size_t cnt = size_t(1) << (LL - l0 - 1);
-    k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16c);
+    k_merkle_level<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(tree, LL, l0 + 1, p16d);
     WL_LAUNCH_CHECK();
     l0++;
   }

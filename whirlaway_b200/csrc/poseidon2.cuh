@@ -369,6 +369,112 @@ inline P2Consts<W> p2_consts_canonical(const P2Consts<W>& m) {
   return c;
 }
 
+// ---------------------------------------------------------------- fp64 full rounds
+// The full rounds can hold the state as fp64 values that are exact integers. The external
+// linear layer is then nine additions per four words plus the column sums, with no reduction:
+// its rows sum to 49, so inputs below 2^32 in magnitude give outputs below 2^38, far inside
+// the 53-bit mantissa. The S-box takes such a value z unreduced: fl(z^2) is within 2^23 of z^2
+// (z^2 < 2^76), so fq_quot(z * z) = round(z^2 / p) up to an error below 2^-7 and z^2 - q p
+// lies in (-p, p); it is formed from low words, z mod 2^32 being the low word of
+// z + 1.5 * 2^52. The second product r z (|r| < p) likewise. The cube is left as a signed
+// residue in (-p, p), which the next linear layer takes as it is. The partial rounds run on
+// 32-bit words as in p2_permute_fq (their internal layer multiplies by 2^-k, which fp64 cannot
+// hold exactly). Round constants are fp64 copies of the canonical ones.
+template <int W>
+struct P2ConstsFd {
+  static constexpr int RP = P2Consts<W>::RP;
+  double ext_init[4 * W];
+  double ext_term[4 * W];
+  uint32_t internal[RP];
+};
+template <int W>
+inline P2ConstsFd<W> p2_consts_fd(const P2Consts<W>& m) {
+  P2ConstsFd<W> c;
+  for (int i = 0; i < 4 * W; i++) c.ext_init[i] = double(from_mont(m.ext_init[i])), c.ext_term[i] = double(from_mont(m.ext_term[i]));
+  for (int i = 0; i < P2Consts<W>::RP; i++) c.internal[i] = from_mont(m.internal[i]);
+  return c;
+}
+
+// z mod 2^32 for an integer-valued z with |z| < 2^51.
+KB_HD uint32_t fd_low(double z) {
+#ifdef __CUDA_ARCH__
+  return uint32_t(__double2loint(z + FQ_ROUND));
+#else
+  const double y = z + FQ_ROUND;
+  uint64_t bits;
+  std::memcpy(&bits, &y, sizeof bits);
+  return uint32_t(bits);
+#endif
+}
+// z^3 mod p as a signed residue in (-p, p), for an integer-valued z with |z| < 2^38.
+KB_HD double sbox_fd(double z) {
+  const uint32_t zi = fd_low(z);
+  const uint32_t r2 = zi * zi - fq_quot(z * z) * P;  // z^2 mod p in (-p, p)
+  const double r2d = fq_from_i32(r2);
+  const uint32_t r3 = r2 * zi - fq_quot(r2d * z) * P;  // z^3 mod p in (-p, p)
+  return fq_from_i32(r3);
+}
+// The canonical residue of an integer-valued z with |z| < 2^38: z - round(z / p) p lies in
+// [-p/2, p/2], and umin maps its negative values to r + p.
+KB_HD uint32_t fd_canonical(double z) {
+  const uint32_t r = fd_low(z) - fq_quot(z) * P;
+  return umin(r, r + P);
+}
+
+template <int W>
+KB_HD void mds_light_fd(double* s) {
+#pragma unroll
+  for (int c = 0; c < W; c += 4) {
+    const double x0 = s[c], x1 = s[c + 1], x2 = s[c + 2], x3 = s[c + 3];
+    const double t01 = x0 + x1, t23 = x2 + x3, t0123 = t01 + t23;
+    const double t01123 = t0123 + x1, t01233 = t0123 + x3;
+    s[c + 3] = t01233 + 2.0 * x0;
+    s[c + 1] = t01123 + 2.0 * x2;
+    s[c + 0] = t01123 + t01;
+    s[c + 2] = t01233 + t23;
+  }
+  double sums[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    double a = s[k] + s[4 + k];
+#pragma unroll
+    for (int j = 2; j < W / 4; j++) a += s[4 * j + k];
+    sums[k] = a;
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] += sums[i & 3];
+}
+
+// The permutation on canonical values (the same map as p2_permute_fq), full rounds in fp64.
+template <int W>
+KB_HD void p2_permute_fd(uint32_t* s, const P2ConstsFd<W>& c) {
+  double d[W];
+#pragma unroll
+  for (int i = 0; i < W; i++) d[i] = fq_from_u32(s[i]);
+  mds_light_fd<W>(d);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) d[i] = sbox_fd(d[i] + c.ext_init[r * W + i]);
+    mds_light_fd<W>(d);
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = fd_canonical(d[i]);
+#pragma unroll 1
+  for (int r = 0; r < P2ConstsFd<W>::RP; r++) internal_layer_lazy_with0<W>(s, cube_fq(s[0] + c.internal[r]));
+  // words 9.. leave the lazy layer below 2p + 2^24 < 2^32: exact as fp64 without reduction
+#pragma unroll
+  for (int i = 0; i < W; i++) d[i] = fq_from_u32(s[i]);
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < W; i++) d[i] = sbox_fd(d[i] + c.ext_term[r * W + i]);
+    mds_light_fd<W>(d);
+  }
+#pragma unroll
+  for (int i = 0; i < W; i++) s[i] = fd_canonical(d[i]);
+}
+
 // Extension-field versions of the linear layers (constraint evaluation over EF).
 KB_HD void mds_light_ef16(ef* s) {
 #pragma unroll

@@ -55,12 +55,12 @@ __global__ void k_probe_mul(uint32_t seed, int iters, uint32_t* out) {
   out[tid] = x;
 }
 
-__global__ void k_probe_p24(const __grid_constant__ kb::P24Consts c, int iters, uint32_t* out) {
+__global__ void k_probe_p24(const __grid_constant__ kb::P2ConstsFd<24> c, int iters, uint32_t* out) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t s[24];
 #pragma unroll
   for (int i = 0; i < 24; i++) s[i] = (tid * 24u + i) % kb::P;
-  for (int it = 0; it < iters; it++) kb::p2_permute_fq<24>(s, c);
+  for (int it = 0; it < iters; it++) kb::p2_permute_fd<24>(s, c);
   uint32_t x = 0;
 #pragma unroll
   for (int i = 0; i < 24; i++) x ^= s[i];
@@ -115,8 +115,8 @@ extern "C" int wlp_int_peaks(int device, const uint32_t* constants, double* modm
   }
   if (err == cudaSuccess) {
     const int threads = 128, iters = 32;
-    const kb::P24Consts cc =
-        kb::p2_consts_canonical(wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS));
+    const kb::P2ConstsFd<24> cc =
+        kb::p2_consts_fd(wl::perm_consts_from<24>(constants + wl::N_AIR_CONSTS + wl::N_P16_CONSTS));
     const float ms = time_best(s, [&] { k_probe_p24<<<blocks, threads, 0, s>>>(cc, iters, out); }, 5, err);
     if (p24_per_s) *p24_per_s = double(blocks) * threads * iters / (ms * 1e-3);
   }
