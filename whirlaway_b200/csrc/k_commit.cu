@@ -558,23 +558,32 @@ struct GrindState {
   uint32_t in[8];
 };
 
-__global__ void k_grind(const __grid_constant__ kb::P16Consts c, const __grid_constant__ GrindState g, int inlen,
-                        int bits, uint32_t base, uint32_t count, uint32_t* result) {
-  uint32_t off = blockIdx.x * blockDim.x + threadIdx.x;
-  if (off >= count) return;
-  uint32_t w = base + off;
-  if (w >= kb::P) return;
-  uint32_t st[16];
+// Grinding: the smallest w in [base, base + count), below p, for which the challenger (state
+// st, input buffer in[0..inlen)) samples `bits` zero bits after observing w. The words are
+// canonical, the permutation runs in the canonical domain. Thread t tries base + t, then
+// base + t + G, ... (G threads in the grid) and stops at the first candidate above a witness
+// already found: every candidate below the smallest witness is tried, so the result does not
+// depend on the order in which the threads run, and the search ends soon after the first hit
+// instead of covering the whole batch.
+__global__ void __launch_bounds__(256) k_grind(const __grid_constant__ kb::P2ConstsFd<16> c,
+                                               const __grid_constant__ GrindState g, int inlen, int bits,
+                                               uint32_t base, uint32_t count, uint32_t* result) {
+  const uint32_t G = gridDim.x * blockDim.x;
+  const uint32_t mask = (1u << bits) - 1;
+  for (uint32_t off = blockIdx.x * blockDim.x + threadIdx.x; off < count; off += G) {
+    const uint32_t w = base + off;
+    if (w >= kb::P) return;
+    if (*reinterpret_cast<volatile const uint32_t*>(result) < w) return;  // a smaller witness is known
+    uint32_t st[16];
 #pragma unroll
-  for (int i = 0; i < 16; i++) st[i] = g.st[i];
-  for (int i = 0; i < inlen; i++) st[i] = g.in[i];
-  uint32_t wm = kb::to_mont(w);
+    for (int i = 0; i < 16; i++) st[i] = g.st[i];
+    for (int i = 0; i < inlen; i++) st[i] = g.in[i];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
-    if (i == inlen) st[i] = wm;
-  kb::p2_permute<16>(st, c);
-  uint32_t v = kb::from_mont(st[7]);
-  if ((v & ((1u << bits) - 1)) == 0) atomicMin(result, w);
+    for (int i = 0; i < 8; i++)
+      if (i == inlen) st[i] = w;
+    kb::p2_permute_fd<16>(st, c);
+    if ((st[7] & mask) == 0) atomicMin(result, w);
+  }
 }
 
 __global__ void k_to_mont(uint32_t* x, size_t n) {
@@ -794,10 +803,14 @@ void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int 
 
 void launch_grind(const kb::P16Consts& p16, const uint32_t* state16, const uint32_t* inbuf, int inlen, int bits,
                   uint32_t base, uint32_t count, uint32_t* result, cudaStream_t s) {
+  if (bits < 1 || bits > 31 || inlen < 0 || inlen > 7) throw std::invalid_argument("grinding: bits 1..31, inlen 0..7");
   GrindState g;
-  for (int i = 0; i < 16; i++) g.st[i] = state16[i];
-  for (int i = 0; i < 8; i++) g.in[i] = i < inlen ? inbuf[i] : 0;
-  k_grind<<<(count + 255) / 256, 256, 0, s>>>(p16, g, inlen, bits, base, count, result);
+  for (int i = 0; i < 16; i++) g.st[i] = kb::from_mont(state16[i]);
+  for (int i = 0; i < 8; i++) g.in[i] = i < inlen ? kb::from_mont(inbuf[i]) : 0;
+  // about 2^bits threads: the first witness lies near 2^bits, so most searches end within
+  // one or two passes of the grid
+  const uint32_t threads = std::max<uint32_t>(256, std::min<uint32_t>(count, 1u << std::min(bits, 20)));
+  k_grind<<<(threads + 255) / 256, 256, 0, s>>>(kb::p2_consts_fd(p16), g, inlen, bits, base, count, result);
   WL_LAUNCH_CHECK();
 }
 

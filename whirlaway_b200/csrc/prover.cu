@@ -476,9 +476,10 @@ struct DevPhase {
 void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
   if (bits <= 0) return;
   DBuf res(sizeof(uint32_t), ctx.stream);
-  // 2^(bits+1) candidates per batch: a witness is missed with probability e^-2 (one more
-  // round trip then), for half the device work of a batch that almost never misses
-  const uint32_t batch = 1u << std::min(22, bits + 1);
+  // 2^(bits+3) candidates per batch: a witness is missed with probability e^-8 (one more
+  // round trip then); the search stops soon after the first witness, so a larger batch costs
+  // no device work
+  const uint32_t batch = 1u << std::min(24, bits + 3);
   for (uint64_t base = 0; base < kb::P; base += batch) {
     uint32_t init = UINT32_MAX;
     ctx.to_device(res.as<void>(), &init, 4);
