@@ -802,14 +802,12 @@ void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int 
 }
 
 void launch_grind(const kb::P16Consts& p16, const uint32_t* state16, const uint32_t* inbuf, int inlen, int bits,
-                  uint32_t base, uint32_t count, uint32_t* result, cudaStream_t s) {
+                  uint32_t base, uint32_t count, uint32_t threads, uint32_t* result, cudaStream_t s) {
   if (bits < 1 || bits > 31 || inlen < 0 || inlen > 7) throw std::invalid_argument("grinding: bits 1..31, inlen 0..7");
   GrindState g;
   for (int i = 0; i < 16; i++) g.st[i] = kb::from_mont(state16[i]);
   for (int i = 0; i < 8; i++) g.in[i] = i < inlen ? kb::from_mont(inbuf[i]) : 0;
-  // about 2^bits threads: the first witness lies near 2^bits, so most searches end within
-  // one or two passes of the grid
-  const uint32_t threads = std::max<uint32_t>(256, std::min<uint32_t>(count, 1u << std::min(bits, 20)));
+  threads = std::max<uint32_t>(256, std::min<uint32_t>(count, threads));
   k_grind<<<(threads + 255) / 256, 256, 0, s>>>(kb::p2_consts_fd(p16), g, inlen, bits, base, count, result);
   WL_LAUNCH_CHECK();
 }

@@ -72,8 +72,11 @@ void launch_gather_u32(const uint32_t* src, const uint64_t* idx, int width, int 
 
 // --------------------------------------------------------------- PoW
 // Smallest w in [base, base + count) with from_mont(sample) & mask == 0 after observing w.
+// The smallest witness in [base, base + count) into *result (UINT32_MAX if none), searched by
+// `threads` threads in increasing order with an early stop (any thread count gives the same
+// result).
 void launch_grind(const kb::P16Consts& p16, const uint32_t* state16, const uint32_t* inbuf, int inlen, int bits,
-                  uint32_t base, uint32_t count, uint32_t* result, cudaStream_t s);
+                  uint32_t base, uint32_t count, uint32_t threads, uint32_t* result, cudaStream_t s);
 
 // --------------------------------------------------------------- eq tables / reductions
 void launch_eq_table(const ef* point, int nvars, ef* out, cudaStream_t s);

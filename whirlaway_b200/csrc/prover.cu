@@ -480,10 +480,13 @@ void grind(Context& ctx, Transcript& ts, const kb::P16Consts& p16, int bits) {
   // round trip then); the search stops soon after the first witness, so a larger batch costs
   // no device work
   const uint32_t batch = 1u << std::min(24, bits + 3);
+  // the first witness lies near 2^bits: 2^(bits+1) threads find it in one pass of the grid
+  // almost always; 2^(bits-2) threads take a few passes and stop about 2^bits candidates in
+  const uint32_t threads = ctx.grind_lean ? 1u << std::max(8, bits - 2) : 1u << std::min(20, bits + 1);
   for (uint64_t base = 0; base < kb::P; base += batch) {
     uint32_t init = UINT32_MAX;
     ctx.to_device(res.as<void>(), &init, 4);
-    { ProfScope _ps(ctx, "grind"); launch_grind(p16, ts.ch.state, ts.ch.in, ts.ch.in_len, bits, (uint32_t)base, batch, res.as<uint32_t>(),
+    { ProfScope _ps(ctx, "grind"); launch_grind(p16, ts.ch.state, ts.ch.in, ts.ch.in_len, bits, (uint32_t)base, batch, threads, res.as<uint32_t>(),
                  ctx.stream); }
     uint32_t r;
     ctx.to_host(&r, res.as<uint32_t>(), 4);

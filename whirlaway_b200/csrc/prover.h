@@ -83,6 +83,10 @@ struct Context {
   // When set, the first proof of each table shape tunes the commitment's launch plans (see
   // tuner.h); server workers leave it off and use the plans a tuning context has kept.
   bool autotune = true;
+  // Grinding threads: false (default) = about 2^(bits+1), one pass of the grid almost always
+  // finds the witness (the shortest search); true = about 2^(bits-2), a few passes but less
+  // than half the permutations on average (server workers, whose device time is what counts).
+  bool grind_lean = false;
   // When set, prove_air records a per-phase transcript log of each proof into last_dump (JSON).
   bool dump_transcript = false;
   std::string last_dump;

@@ -58,6 +58,7 @@ Server::Server(int device, int workers, uint64_t hbm_budget) : device_(device), 
     if (const char* v = std::getenv("WL_WORKER_POLL_US")) contexts_.back()->block_after_us = std::atoi(v);
     contexts_.back()->set_cache_limit(0);  // admission counts running proofs only: no cached buffers
     contexts_.back()->autotune = false;    // concurrent proofs would disturb the timings
+    contexts_.back()->grind_lean = true;   // device time, not one search's latency, is what counts
   }
   // The budget is reserved in the stream-ordered pool up front (one allocation, freed at once;
   // the pool keeps it and carves the workers' buffers from it). Growing the pool while proofs
