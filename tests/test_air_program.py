@@ -7,6 +7,10 @@ are accepted by the oracle's and by the library's host verifiers, and proofs of 
 witnesses (or checked against other preprocessed values) are rejected.
 GPU: the library's proofs equal the oracle's word for word.
 """
+import os
+import shutil
+import subprocess
+
 import numpy as np
 import pytest
 
@@ -107,6 +111,22 @@ def oracle():
 def hash_consts(oracle):
     c, _ = oracle.workload(2, 0)
     return c[148:]
+
+
+def test_program_compiler_on_host(tmp_path):
+    """The compiled device code (registers, constants as immediates) run by a host restatement
+    of the interpreter kernels equals the program evaluated instruction by instruction."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    nvcc = shutil.which("nvcc")
+    if nvcc is None:
+        pytest.skip("no CUDA toolkit (vector types header)")
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "include")
+    exe = tmp_path / "program_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(root, "whirlaway_b200", "csrc"),
+                    "-I", cuda_inc, os.path.join(root, "tests", "program_host_check.cpp"),
+                    "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
 
 
 def test_builder_degrees_and_checks():

@@ -48,10 +48,41 @@ ProgramAir ProgramAir::build(int W, int n_constraints, int degree, int n_ops, co
     }
   }
   if (emits != n_constraints) throw std::invalid_argument("AIR program: EMIT count differs from the constraint count");
+  // Instructions with exactly one constant operand take the constant as an immediate:
+  // MUL -> MULC, ADD -> ADDC, SUB(x, c) -> ADDC(x, -c). kind[i]: the device op, other[i]: the
+  // non-constant operand, imm[i]: the constant (Montgomery form).
+  auto const_of = [&](int v) { return ops[3 * root[v]] == PROG_CONST ? ops[3 * root[v] + 1] : -1; };
+  std::vector<int> kind(n_ops), other(n_ops, -1);
+  std::vector<uint32_t> imm(n_ops, 0);
   for (int i = 0; i < n_ops; i++) {
     const int op = ops[3 * i], a = ops[3 * i + 1], b = ops[3 * i + 2];
-    if (op >= PROG_ADD) last[root[a]] = std::max(last[root[a]], i);
-    if (op >= PROG_ADD && op <= PROG_MUL) last[root[b]] = std::max(last[root[b]], i);
+    kind[i] = op;
+    if (op != PROG_ADD && op != PROG_SUB && op != PROG_MUL) continue;
+    const int ca = const_of(a), cb = const_of(b);
+    if ((ca >= 0) == (cb >= 0)) continue;  // no constant, or two
+    if (op == PROG_SUB && ca >= 0) continue;  // c - x stays general
+    const int x = ca >= 0 ? b : a;
+    const uint32_t c = p.consts[ca >= 0 ? ca : cb];
+    kind[i] = op == PROG_MUL ? PROG_MULC : PROG_ADDC;
+    other[i] = x;
+    imm[i] = op == PROG_SUB ? kb::neg(c) : c;
+  }
+  // operands read from registers (MULC / ADDC read one)
+  auto reads = [&](int i, int& r0, int& r1) {
+    const int op = ops[3 * i], a = ops[3 * i + 1], b = ops[3 * i + 2];
+    r0 = r1 = -1;
+    if (kind[i] == PROG_MULC || kind[i] == PROG_ADDC) {
+      r0 = root[other[i]];
+    } else if (op >= PROG_ADD) {
+      r0 = root[a];
+      if (op <= PROG_MUL) r1 = root[b];
+    }
+  };
+  for (int i = 0; i < n_ops; i++) {
+    int r0, r1;
+    reads(i, r0, r1);
+    if (r0 >= 0) last[r0] = std::max(last[r0], i);
+    if (r1 >= 0) last[r1] = std::max(last[r1], i);
   }
   // linear scan: operands are read before the result is written, so a register whose last
   // use is this instruction can take the result
@@ -67,15 +98,16 @@ ProgramAir ProgramAir::build(int W, int n_constraints, int degree, int n_ops, co
       throw std::invalid_argument("AIR program: more than " + std::to_string(PROG_MAX_REGS) + " values live at once");
     return next++;
   };
-  p.code.resize(n_ops);
+  p.code.reserve(n_ops);
   for (int i = 0; i < n_ops; i++) {
-    const int op = ops[3 * i], a = ops[3 * i + 1], b = ops[3 * i + 2];
-    uint32_t ra = 0, rb = 0;
-    if (op >= PROG_ADD) ra = uint32_t(reg[root[a]]);
-    if (op >= PROG_ADD && op <= PROG_MUL) rb = uint32_t(reg[root[b]]);
+    const int op = ops[3 * i], a = ops[3 * i + 1];
+    if (op == PROG_CONST && last[i] < 0) continue;  // read only as an immediate (or never)
+    int r0, r1;
+    reads(i, r0, r1);
+    const uint32_t ra = r0 >= 0 ? uint32_t(reg[r0]) : 0u, rb = r1 >= 0 ? uint32_t(reg[r1]) : 0u;
     // free the operands that die here (once each)
-    if (op >= PROG_ADD && last[root[a]] == i) free_regs.push_back(reg[root[a]]);
-    if (op >= PROG_ADD && op <= PROG_MUL && last[root[b]] == i && root[b] != root[a]) free_regs.push_back(reg[root[b]]);
+    if (r0 >= 0 && last[r0] == i) free_regs.push_back(reg[r0]);
+    if (r1 >= 0 && last[r1] == i && r1 != r0) free_regs.push_back(reg[r1]);
     uint32_t dst = 0;
     if (op != PROG_EMIT) {
       reg[i] = take();
@@ -83,7 +115,8 @@ ProgramAir ProgramAir::build(int W, int n_constraints, int degree, int n_ops, co
       if (last[i] < 0) free_regs.push_back(reg[i]);  // never read
     }
     const uint32_t aa = op <= PROG_CONST ? uint32_t(a) : ra;
-    p.code[i] = make_uint2(uint32_t(op) | dst << 8 | aa << 16, rb);
+    const uint32_t y = (kind[i] == PROG_MULC || kind[i] == PROG_ADDC) ? imm[i] : rb;
+    p.code.push_back(make_uint2(uint32_t(kind[i]) | dst << 8 | aa << 16, y));
   }
   p.nregs = next;
   return p;

@@ -16,6 +16,10 @@
 namespace wl {
 
 enum ProgOp { PROG_UP = 0, PROG_DOWN = 1, PROG_CONST = 2, PROG_ADD = 3, PROG_SUB = 4, PROG_MUL = 5, PROG_EMIT = 6 };
+// Device-only forms for an operand that is a constant (the constant's Montgomery value in y):
+// value * c and value + c (x - c is value + (-c)). Over the extension they are a product and a
+// sum by a base-field element, an eighth of the work of the general forms.
+enum ProgDevOp { PROG_MULC = 7, PROG_ADDC = 8 };
 constexpr int PROG_MAX_REGS = 64;
 
 struct ProgramAir {
@@ -26,7 +30,8 @@ struct ProgramAir {
   std::vector<uint32_t> pre;     // the preprocessed columns, P x 2^log_n, Montgomery form
   int pre_log_n = -1;
   // Device form: x = op | dst << 8 | a << 16 (a: a column, a constant or a register), y = b (a
-  // register); EMIT's register is its operand's.
+  // register, or for MULC / ADDC the constant's Montgomery value); EMIT's register is its
+  // operand's. A constant read only as such an operand has no instruction and no register.
   std::vector<uint2> code;
   int nregs = 0;
 

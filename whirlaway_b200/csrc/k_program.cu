@@ -1,7 +1,9 @@
 // Zerocheck kernels for AIRs given as constraint programs (air_program.h): an interpreter over a
 // per-thread register file of PROG_MAX_REGS values, one thread per row of the current cube,
 // blockIdx.y the evaluation point. The program's instructions are read by every thread of a
-// warp at once (one broadcast load each); the register file lives in local memory.
+// warp at once (one broadcast load each); the register file lives in local memory. An
+// operand that is a constant comes as an immediate (MULC, ADDC): over the extension a product
+// by a base-field element instead of a full extension product.
 //
 // Round 0 (univariate skip over the top k variables) reads the witness: column c's value at
 // point z and row x of the subcube is sum_j L_j(z) col[j S + x] over the 2^k rows of its coset,
@@ -75,6 +77,10 @@ __global__ void __launch_bounds__(PROG_THREADS) k_prog_zc0(const uint32_t* __res
       } else if (op == PROG_MUL) {
         const uint32_t u = reg[a], v = reg[b];
         reg[dst] = kb::mul(u, v);
+      } else if (op == PROG_MULC) {
+        reg[dst] = kb::mul(reg[a], uint32_t(b));
+      } else if (op == PROG_ADDC) {
+        reg[dst] = kb::add(reg[a], uint32_t(b));
       } else {  // PROG_EMIT
         acc = ef_add(acc, ef_mul_f(alphas[ci++], reg[a]));
       }
@@ -145,6 +151,12 @@ __global__ void __launch_bounds__(PROG_THREADS) k_prog_zc_ef(const ef* __restric
       } else if (op == PROG_MUL) {
         const ef u = reg[a], v = reg[b];
         reg[dst] = ef_mul(u, v);
+      } else if (op == PROG_MULC) {
+        reg[dst] = ef_mul_f(reg[a], uint32_t(b));
+      } else if (op == PROG_ADDC) {
+        ef v = reg[a];
+        v.c[0] = kb::add(v.c[0], uint32_t(b));
+        reg[dst] = v;
       } else {  // PROG_EMIT
         acc = ef_add(acc, ef_mul(alphas[ci++], reg[a]));
       }

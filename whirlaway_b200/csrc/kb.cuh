@@ -7,7 +7,16 @@
 // are folded with a single Montgomery reduction, which roughly halves the instruction
 // count of an extension-field product against one reduction per product.
 #pragma once
+#ifdef __CUDACC_RTC__
+// runtime compilation (the generated constraint kernels): no host headers
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+typedef int int32_t;
+typedef long long int64_t;
+typedef unsigned char uint8_t;
+#else
 #include <cstdint>
+#endif
 
 #ifdef __CUDACC__
 #define KB_HD __host__ __device__ __forceinline__
