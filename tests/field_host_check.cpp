@@ -148,11 +148,8 @@ int main() {
         for (int i = 0; i < W; i++) r[i] = cub(uint32_t((uint64_t(r[i]) + from_mont(et[rd * W + i])) % P));
         mds(r);
       }
-      uint32_t sc[24];  // the canonical-domain permutation of the Merkle hashes
+      uint32_t sc[24];  // the canonical-domain permutation of the Merkle hashes (full rounds in fp64)
       for (int i = 0; i < W; i++) sc[i] = s[i];
-      if (w) p2_permute_fq<24>(sc, p2_consts_canonical(c24)); else p2_permute_fq<16>(sc, p2_consts_canonical(c16));
-      for (int i = 0; i < W; i++) if (sc[i] != r[i]) { b8++; break; }
-      for (int i = 0; i < W; i++) sc[i] = s[i];  // full rounds in fp64
       if (w) p2_permute_fd<24>(sc, p2_consts_fd(c24)); else p2_permute_fd<16>(sc, p2_consts_fd(c16));
       for (int i = 0; i < W; i++) if (sc[i] != r[i]) { b8++; break; }
       for (int i = 0; i < W; i++) s[i] = to_mont(s[i]);

@@ -341,26 +341,7 @@ KB_HD void internal_lazy_finish(uint32_t* s) {
   }
 }
 
-// The permutation on canonical values with canonical round constants (p2_consts_canonical).
-template <int W>
-KB_HD void p2_permute_fq(uint32_t* s, const P2Consts<W>& c) {
-  mds_light<W>(s);
-#pragma unroll 1
-  for (int r = 0; r < 4; r++) {
-#pragma unroll
-    for (int i = 0; i < W; i++) s[i] = cube_fq(s[i] + c.ext_init[r * W + i]);
-    mds_light<W>(s);
-  }
-#pragma unroll 1
-  for (int r = 0; r < P2Consts<W>::RP; r++) internal_layer_lazy_with0<W>(s, cube_fq(s[0] + c.internal[r]));
-  internal_lazy_finish<W>(s);
-#pragma unroll 1
-  for (int r = 0; r < 4; r++) {
-#pragma unroll
-    for (int i = 0; i < W; i++) s[i] = cube_fq(s[i] + c.ext_term[r * W + i]);
-    mds_light<W>(s);
-  }
-}
+// Canonical round constants (the canonical-domain S-box and lane kernels).
 template <int W>
 inline P2Consts<W> p2_consts_canonical(const P2Consts<W>& m) {
   P2Consts<W> c;
@@ -378,8 +359,9 @@ inline P2Consts<W> p2_consts_canonical(const P2Consts<W>& m) {
 // lies in (-p, p); it is formed from low words, z mod 2^32 being the low word of
 // z + 1.5 * 2^52. The second product r z (|r| < p) likewise. The cube is left as a signed
 // residue in (-p, p), which the next linear layer takes as it is. The partial rounds run on
-// 32-bit words as in p2_permute_fq (their internal layer multiplies by 2^-k, which fp64 cannot
-// hold exactly). Round constants are fp64 copies of the canonical ones.
+// 32-bit words with the canonical-domain S-box and the lazy internal layer (which multiplies
+// by 2^-k, which fp64 cannot hold exactly). Round constants are fp64 copies of the canonical
+// ones.
 template <int W>
 struct P2ConstsFd {
   static constexpr int RP = P2Consts<W>::RP;
@@ -445,7 +427,8 @@ KB_HD void mds_light_fd(double* s) {
   for (int i = 0; i < W; i++) s[i] += sums[i & 3];
 }
 
-// The permutation on canonical values (the same map as p2_permute_fq), full rounds in fp64.
+// The permutation on canonical values (the map p2_permute computes on Montgomery forms),
+// full rounds in fp64.
 template <int W>
 KB_HD void p2_permute_fd(uint32_t* s, const P2ConstsFd<W>& c) {
   double d[W];
