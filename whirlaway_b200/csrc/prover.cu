@@ -861,8 +861,9 @@ size_t proof_len_bound(const Settings& s, int log_n, int W, int degree) {
 
 // The zerocheck of an AIR given as a constraint program (air_program.h), round for round as
 // crates/sumcheck/src/prove.rs:97-254 runs it on the 2W up/down columns: the sums from the
-// interpreter kernels, the round polynomial and challenge on the host transcript, the fold of
-// all 2W columns after every round; the last folds are the up and down evaluations.
+// interpreter kernels, the round polynomial and challenge on the device transcript (degrees 2
+// and 3; the host transcript for round 0, degree 1 and rounds that grind), the fold of all 2W
+// columns after every round; the last folds are the up and down evaluations.
 // The first P of the W columns are preprocessed (in the zerocheck, not committed): up and down
 // receive the witness columns' evaluations only.
 void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const ProgramAir& prog, const uint32_t* wit,
@@ -927,8 +928,38 @@ void zerocheck_program(Context& ctx, Transcript& ts, const ProofJob& job, const 
     eqr = DBuf(sizeof(ef) * (S / 2), st);
     launch_fold_cols(nullptr, nullptr, 0, 0, nullptr, st, eq0.as<ef>(), eqr.as<ef>(), S / 2);
   }
+  // Degrees 2 and 3 without grinding: every round's transcript on the device (the finishing
+  // kernel of an eq-factor round with d + 1 points), one host wait for the phase.
+  const bool on_device = R >= 1 && (d == 2 || d == 3) && sumcheck_pow_bits(s.security_bits, d + 1) == 0;
+  if (on_device) {
+    const int kind = d == 3 ? FIN_EQSC4 : FIN_EQSC3;
+    DevPhase ph(ctx, ts, R, size_t(8) * (d + 2), sum, mmf, job.p16, zc.data() + 1);
+    for (int round = 1; round <= R; round++) {
+      const int m = R - round + 1;
+      const size_t half = size_t(1) << (m - 1);
+      const int B = prog_zc_blocks(half);
+      ef* part = ctx.partials(size_t(B) * d);
+      {
+        ProfScope _ps(ctx, "prog_zc_ef");
+        launch_prog_zc_ef(cols.as<ef>(), m, W, code.as<uint2>(), n_code, consts.as<uint32_t>(), d, eqr.as<ef>(),
+                          d_alphas.as<ef>(), part, st);
+      }
+      ph.finish_round(kind, part, B);
+      DBuf nc(sizeof(ef) * size_t(2 * W) * half, st);
+      DBuf eqn(sizeof(ef) * std::max<size_t>(half / 2, 1), st);
+      {
+        ProfScope _ps(ctx, "fold");
+        launch_fold_cols_dev(cols.as<ef>(), nc.as<ef>(), 2 * W, half, ph.chs + (round - 1), st,
+                             half >= 2 ? eqr.as<ef>() : nullptr, eqn.as<ef>(), half / 2);
+      }
+      cols = std::move(nc);
+      eqr = std::move(eqn);
+    }
+    const std::vector<ef> ch = ph.finish(&sum, &mmf);
+    challenges.insert(challenges.end(), ch.begin(), ch.end());
+  }
   const auto& basis = lagrange_basis_cached(d + 1);
-  for (int round = 1; round <= R; round++) {
+  for (int round = 1; !on_device && round <= R; round++) {
     const int m = R - round + 1;
     const size_t half = size_t(1) << (m - 1);
     const int B = prog_zc_blocks(half);
