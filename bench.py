@@ -260,7 +260,18 @@ def whir_rows_hashed(log_n):
     return rows
 
 
-def roofline(profile, breakdown, log_n, peaks, hbm_peak_gbs, steps):
+def read_hbm_peak():
+    """The HBM copy peak (GB/s) the roofline is measured against, and where it comes from: the
+    measured figure in MEASURED_PEAKS.json when the file is there, else a fallback of 6.65 TB/s
+    (a STREAM-style copy measured earlier on a B200)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, "fallback: 6.65 TB/s, a copy measured earlier on a B200 (MEASURED_PEAKS.json absent)"
+
+
+def roofline(profile, breakdown, log_n, peaks, hbm_peak_gbs, steps, hbm_source):
     """Roofline of the dominant kernel class: its CUDA-event time over the timed region
     (`profile`), its share of all kernel time from a fully profiled proof (`breakdown`)."""
     name, (ms, launches) = max(profile.items(), key=lambda kv: kv[1][0])
@@ -297,7 +308,7 @@ def roofline(profile, breakdown, log_n, peaks, hbm_peak_gbs, steps):
                                                      "registers: the cost of memory and orchestration only"},
                     "hbm": {"achieved": byts / (ms * 1e-3) / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
                             "frac": byts / (ms * 1e-3) / 1e9 / hbm_peak_gbs,
-                            "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+                            "peak_source": hbm_source}})
         return out
     if name == "leaf_hash":
         work = sum(rows) * 8 * P24_MODMUL * steps
@@ -318,7 +329,7 @@ def roofline(profile, breakdown, log_n, peaks, hbm_peak_gbs, steps):
                     "peak_source": "hardware: 32-bit multiplies (mul.lo / mul.hi probes), two of each per Montgomery product",
                     "hbm": {"achieved": byts / (ms * 1e-3) / 1e9, "peak": hbm_peak_gbs, "unit": "GB/s",
                             "frac": byts / (ms * 1e-3) / 1e9 / hbm_peak_gbs,
-                            "peak_source": "MEASURED_PEAKS.json hbm_gbs"}})
+                            "peak_source": hbm_source}})
     return out
 
 
@@ -619,11 +630,7 @@ def run_ours(args, world, rank, local):
     verified = wl.verify(consts, log_n, proof) == 0
     if rank != 0:
         return
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            hbm_peak = json.load(f)["hbm_gbs"]
-    except (OSError, KeyError, ValueError):
-        hbm_peak = 6650.0
+    hbm_peak, hbm_source = read_hbm_peak()
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cl = min(args.cpu_sample_log_n, log_n)
@@ -647,7 +654,7 @@ def run_ours(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear Montgomery; exact modular integer)",
         "data": "synthetic", "config": workload_config(log_n), "verified": bool(verified),
         "e2e": e2e, "e2e_host_witness": e2e_wit, "gpu_launches": launches, "clocks": clocks,
-        "roofline": roofline(profile, breakdown, log_n, peaks, hbm_peak, args.steps),
+        "roofline": roofline(profile, breakdown, log_n, peaks, hbm_peak, args.steps, hbm_source),
         "cpu_baseline": cpu,
         "published_reference": {"value": 75000.0, "unit": "perms/s", "hardware": "Intel i9-12900H (CPU prover)",
                                 "source": "reference README.md:20", "log_n_rows": 18},
