@@ -5,10 +5,13 @@
 // each against a plain modular reference. Built and run by tests/test_boundary.py.
 #include <cstdio>
 #include <random>
+#include <vector>
 #include <type_traits>
 #include "poseidon2.cuh"
 namespace wl {
 void host_p16_permute(uint32_t* s, const kb::P16Consts& c);
+void host_p24_permute_many(uint32_t* states, size_t n, const kb::P24Consts& c);
+void host_p16_permute_many(uint32_t* states, size_t n, const kb::P16Consts& c);
 }
 using namespace kb;
 int main() {
@@ -161,6 +164,27 @@ int main() {
         wl::host_p16_permute(sv, c16);
         for (int i = 0; i < 16; i++) if (sv[i] != s[i]) { b8++; break; }
       }
+    }
+  }
+  // batches of independent permutations (sixteen per vector, lane = instance; ragged last
+  // group) against one at a time
+  for (int w = 0; w < 2; w++) {
+    const int W = w ? 24 : 16;
+    P16Consts c16;
+    P24Consts c24;
+    uint32_t* ei = w ? c24.ext_init : c16.ext_init;
+    uint32_t* et = w ? c24.ext_term : c16.ext_term;
+    uint32_t* in = w ? c24.internal : c16.internal;
+    for (int i = 0; i < 4 * W; i++) ei[i] = to_mont(g() % P), et[i] = to_mont(g() % P);
+    for (int i = 0; i < (w ? 23 : 20); i++) in[i] = to_mont(g() % P);
+    for (size_t n : {size_t(1), size_t(15), size_t(16), size_t(17), size_t(40)}) {
+      std::vector<uint32_t> many(n * W), one(n * W);
+      for (size_t i = 0; i < n * W; i++) many[i] = one[i] = (i % 7 == 3) ? P - 1 : uint32_t(g() % P);
+      if (w) wl::host_p24_permute_many(many.data(), n, c24); else wl::host_p16_permute_many(many.data(), n, c16);
+      for (size_t j = 0; j < n; j++) {
+        if (w) p2_permute<24>(one.data() + 24 * j, c24); else p2_permute<16>(one.data() + 16 * j, c16);
+      }
+      if (many != one) b8++;
     }
   }
   // the fp64 S-box and canonical reduction over the whole input range of the fp64 full rounds:

@@ -64,6 +64,10 @@ inline double host_now_ms() {
 // sponge once eight are buffered; samples pop from the end of the last squeeze.
 // Poseidon2-16 on the host (host_perm.cpp): AVX-512 when the CPU has it, else scalar.
 void host_p16_permute(uint32_t* s, const kb::P16Consts& c);
+// n independent permutations of states laid out one after the other (W words each), sixteen at
+// a time with AVX-512 when the CPU has it; the same map as kb::p2_permute<W>.
+void host_p24_permute_many(uint32_t* states, size_t n, const kb::P24Consts& c);
+void host_p16_permute_many(uint32_t* states, size_t n, const kb::P16Consts& c);
 
 struct HostChallenger {
   const kb::P16Consts* perm = nullptr;

@@ -6,6 +6,8 @@
 // in-lane shuffles and the internal layer's sum is a horizontal add. The result is the same
 // permutation as kb::p2_permute<16> (checked bit for bit in the tests); without AVX-512
 // the scalar version runs.
+// For the verifier's Merkle checks (many independent leaf sponges and compressions), batches
+// of Poseidon2-24 / Poseidon2-16 run sixteen at a time with one instance per lane.
 #include <immintrin.h>
 
 #include <cstdint>
@@ -87,6 +89,67 @@ WL_AVX512 void permute16_avx512(uint32_t* s, const kb::P16Consts& c) {
   _mm512_storeu_si512(s, x);
 }
 
+// ---- sixteen independent permutations: lane j of every vector is instance j, vector i holds
+// word i of the sixteen states (the Merkle checks of the verifier hash many rows and paths).
+template <int W>
+WL_AVX512 inline void vmds_x16(const V& k, __m512i* x) {
+  for (int c = 0; c < W; c += 4) {
+    const __m512i x0 = x[c], x1 = x[c + 1], x2 = x[c + 2], x3 = x[c + 3];
+    const __m512i t01 = vadd(k, x0, x1), t23 = vadd(k, x2, x3), t0123 = vadd(k, t01, t23);
+    const __m512i t01123 = vadd(k, t0123, x1), t01233 = vadd(k, t0123, x3);
+    x[c + 3] = vadd(k, t01233, vadd(k, x0, x0));
+    x[c + 1] = vadd(k, t01123, vadd(k, x2, x2));
+    x[c + 0] = vadd(k, t01123, t01);
+    x[c + 2] = vadd(k, t01233, t23);
+  }
+  __m512i sums[4];
+  for (int j = 0; j < 4; j++) {
+    __m512i a = x[j];
+    for (int c = 4 + j; c < W; c += 4) a = vadd(k, a, x[c]);
+    sums[j] = a;
+  }
+  for (int i = 0; i < W; i++) x[i] = vadd(k, x[i], sums[i & 3]);
+}
+
+template <int W>
+WL_AVX512 void permute_x16(__m512i* x, const kb::P2Consts<W>& c) {
+  V k;
+  k.p = _mm512_set1_epi32((int)kb::P);
+  k.pinv = _mm512_set1_epi32((int)kb::PINV);
+  vmds_x16<W>(k, x);
+  for (int r = 0; r < 4; r++) {
+    for (int i = 0; i < W; i++) x[i] = vcube(k, vadd(k, x[i], _mm512_set1_epi32((int)c.ext_init[r * W + i])));
+    vmds_x16<W>(k, x);
+  }
+  for (int r = 0; r < kb::P2Consts<W>::RP; r++) {
+    x[0] = vcube(k, vadd(k, x[0], _mm512_set1_epi32((int)c.internal[r])));
+    __m512i sum = x[0];
+    for (int i = 1; i < W; i++) sum = vadd(k, sum, x[i]);
+    for (int i = 0; i < W; i++) x[i] = vadd(k, vmul(k, x[i], _mm512_set1_epi32((int)kb::p2_diag<W>(i))), sum);
+  }
+  for (int r = 0; r < 4; r++) {
+    for (int i = 0; i < W; i++) x[i] = vcube(k, vadd(k, x[i], _mm512_set1_epi32((int)c.ext_term[r * W + i])));
+    vmds_x16<W>(k, x);
+  }
+}
+
+// n states of W words each (contiguous), in groups of sixteen (the last group padded).
+template <int W>
+WL_AVX512 void permute_many_avx512(uint32_t* states, size_t n, const kb::P2Consts<W>& c) {
+  alignas(64) uint32_t t[W][16];
+  __m512i x[W];
+  for (size_t g = 0; g < n; g += 16) {
+    const size_t m = n - g < 16 ? n - g : 16;
+    for (size_t j = 0; j < 16; j++)
+      for (int i = 0; i < W; i++) t[i][j] = j < m ? states[(g + j) * W + i] : 0u;
+    for (int i = 0; i < W; i++) x[i] = _mm512_load_si512(t[i]);
+    permute_x16<W>(x, c);
+    for (int i = 0; i < W; i++) _mm512_store_si512(t[i], x[i]);
+    for (size_t j = 0; j < m; j++)
+      for (int i = 0; i < W; i++) states[(g + j) * W + i] = t[i][j];
+  }
+}
+
 bool have_avx512() {
   static const bool ok = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
                          __builtin_cpu_supports("avx512dq") && __builtin_cpu_supports("avx512vl");
@@ -105,5 +168,20 @@ void host_p16_permute(uint32_t* s, const kb::P16Consts& c) {
 
 // The portable version, for comparisons.
 void host_p16_permute_scalar(uint32_t* s, const kb::P16Consts& c) { kb::p2_permute<16>(s, c); }
+
+void host_p24_permute_many(uint32_t* states, size_t n, const kb::P24Consts& c) {
+  if (have_avx512()) {
+    permute_many_avx512<24>(states, n, c);
+  } else {
+    for (size_t i = 0; i < n; i++) kb::p2_permute<24>(states + 24 * i, c);
+  }
+}
+void host_p16_permute_many(uint32_t* states, size_t n, const kb::P16Consts& c) {
+  if (have_avx512()) {
+    permute_many_avx512<16>(states, n, c);
+  } else {
+    for (size_t i = 0; i < n; i++) kb::p2_permute<16>(states + 16 * i, c);
+  }
+}
 
 }  // namespace wl

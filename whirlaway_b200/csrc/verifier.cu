@@ -142,26 +142,37 @@ ef matrix_down(const std::vector<ef>& pt) { return kb::ef_add(successor(pt), ef_
 
 // ---------------------------------------------------------------- WHIR
 using Digest = std::array<uint32_t, 8>;
-// Leaf: PaddingFreeSponge over Poseidon2-24 (rate 16, zero capacity) of a 128-value row.
-Digest leaf_digest(const uint32_t* row, const kb::P24Consts& p24) {
-  uint32_t s[24] = {0};
+// Merkle checks of queries [i0, i1) of a round: the leaf sponges (PaddingFreeSponge over
+// Poseidon2-24, rate 16, zero capacity, of each 128-value row) and then, level by level, the
+// 2-to-1 compressions (the first 8 words of Poseidon2-16(left || right)) of every query at once,
+// as batches of independent permutations (sixteen per vector with AVX-512). ok[i] = 1 when the
+// path of query i ends at the root.
+void merkle_check_range(const uint32_t* rows, const uint32_t* paths, const uint32_t* q, size_t i0, size_t i1, int ll,
+                        const Digest& root, const kb::P24Consts& p24, const kb::P16Consts& p16, char* ok) {
+  const size_t m = i1 - i0, rl = 128, pl = size_t(8) * ll;
+  std::vector<uint32_t> st(m * 24, 0u);
   for (int c = 0; c < 8; c++) {
-    for (int i = 0; i < 16; i++) s[i] = row[16 * c + i];
-    kb::p2_permute<24>(s, p24);
+    for (size_t j = 0; j < m; j++)
+      for (int i = 0; i < 16; i++) st[j * 24 + i] = rows[(i0 + j) * rl + 16 * c + i];
+    host_p24_permute_many(st.data(), m, p24);
   }
-  Digest d;
-  for (int i = 0; i < 8; i++) d[i] = s[i];
-  return d;
-}
-// 2-to-1 compression: the first 8 words of Poseidon2-16(left || right) (the transcript's host
-// permutation: AVX-512 when the CPU has it).
-Digest compress(const Digest& l, const Digest& r, const kb::P16Consts& p16) {
-  uint32_t s[16];
-  for (int i = 0; i < 8; i++) s[i] = l[i], s[8 + i] = r[i];
-  host_p16_permute(s, p16);
-  Digest d;
-  for (int i = 0; i < 8; i++) d[i] = s[i];
-  return d;
+  std::vector<uint32_t> cur(m * 8), s16(m * 16);
+  for (size_t j = 0; j < m; j++)
+    for (int e = 0; e < 8; e++) cur[j * 8 + e] = st[j * 24 + e];
+  for (int l = 0; l < ll; l++) {
+    for (size_t j = 0; j < m; j++) {
+      const uint32_t* sib = paths + (i0 + j) * pl + size_t(l) * 8;
+      const bool right = (q[i0 + j] >> l) & 1;  // the current node is the right child
+      for (int e = 0; e < 8; e++) {
+        s16[j * 16 + e] = right ? sib[e] : cur[j * 8 + e];
+        s16[j * 16 + 8 + e] = right ? cur[j * 8 + e] : sib[e];
+      }
+    }
+    host_p16_permute_many(s16.data(), m, p16);
+    for (size_t j = 0; j < m; j++)
+      for (int e = 0; e < 8; e++) cur[j * 8 + e] = s16[j * 16 + e];
+  }
+  for (size_t j = 0; j < m; j++) ok[i0 + j] = std::equal(root.begin(), root.end(), cur.begin() + j * 8) ? 1 : 0;
 }
 
 struct Constraint {
@@ -311,42 +322,51 @@ class WhirVerifier {
     const std::vector<ef>& r = blocks_.back();
     folded.assign(nq, kb::ef_zero());
     std::vector<char> good(nq, 0);
-    auto check = [&](size_t i) {
-      const uint32_t* row = &rows[i * rl];
-      const uint32_t* path = &paths[i * pl];
-      if (!defer_) {
-        Digest cur = leaf_digest(row, p24_);
-        for (int l = 0; l < ll; l++) {
-          Digest sib;
-          for (int e = 0; e < 8; e++) sib[e] = path[size_t(l) * 8 + e];
-          cur = ((q[i] >> l) & 1) ? compress(sib, cur, p16_) : compress(cur, sib, p16_);
+    // The fold v[p] <- v[p] + r_j v[p + h] (top variable first) of a row is sum_p row[p] m[p]
+    // with m[p] the product of r_j over the bits j of p (bit k-1-j for r_j): one table per
+    // round, then an extension x base product per value for base-field rows.
+    const int k = rc.fold;
+    std::vector<ef> m(size_t(1) << k, kb::ef_one());
+    for (int j = 0; j < k; j++) {
+      const size_t bit = size_t(1) << (k - 1 - j);
+      for (size_t p = 0; p < m.size(); p++)
+        if (p & bit) m[p] = kb::ef_mul(m[p], r[j]);
+    }
+    // queries in chunks of 32: the chunk's Merkle paths as batched permutations, then its folds
+    constexpr size_t CHUNK = 32;
+    auto check = [&](size_t i0, size_t i1) {
+      if (defer_) {
+        for (size_t i = i0; i < i1; i++) good[i] = 1;
+      } else {
+        merkle_check_range(rows.data(), paths.data(), q.data(), i0, i1, ll, root, p24_, p16_, good.data());
+      }
+      for (size_t i = i0; i < i1; i++) {
+        if (!good[i]) continue;
+        const uint32_t* row = &rows[i * rl];
+        ef acc = kb::ef_zero();
+        for (size_t p = 0; p < m.size(); p++) {
+          if (elem == 1) {
+            acc = kb::ef_add(acc, kb::ef_mul_f(m[p], row[p]));
+          } else {
+            ef v = kb::ef_zero();
+            for (int e = 0; e < elem; e++) v.c[e] = row[p * elem + e];
+            acc = kb::ef_add(acc, kb::ef_mul(m[p], v));
+          }
         }
-        if (cur != root) return;
+        folded[i] = acc;
       }
-      const int k = rc.fold;
-      std::vector<ef> v(size_t(1) << k);
-      for (size_t p = 0; p < v.size(); p++) {
-        v[p] = kb::ef_zero();
-        for (int e = 0; e < elem; e++) v[p].c[e] = row[p * elem + e];
-      }
-      for (int j = 0; j < k; j++) {
-        const size_t h = v.size() / 2;
-        for (size_t p = 0; p < h; p++) v[p] = kb::ef_add(v[p], kb::ef_mul(r[j], v[p + h]));
-        v.resize(h);
-      }
-      folded[i] = v[0];
-      good[i] = 1;
     };
+    const size_t nchunks = (nq + CHUNK - 1) / CHUNK;
     const unsigned hw = std::thread::hardware_concurrency();
     const size_t cap = threads_ > 0 ? size_t(threads_) : std::min<size_t>(hw ? hw : 1, 16);
-    const size_t T = std::min<size_t>(cap, (nq + 7) / 8);
+    const size_t T = std::min<size_t>(cap, nchunks);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+      for (size_t c = next++; c < nchunks; c = next++) check(c * CHUNK, std::min(nq, (c + 1) * CHUNK));
+    };
     if (T <= 1) {
-      for (size_t i = 0; i < nq; i++) check(i);
+      work();
     } else {
-      std::atomic<size_t> next{0};
-      auto work = [&] {
-        for (size_t i = next++; i < nq; i = next++) check(i);
-      };
       run_on_threads(T, work);
     }
     for (size_t i = 0; i < nq; i++)
