@@ -84,28 +84,43 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 20  # several samples inside a timed region of a few proofs
+
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.path = None
+        self.skip = 0
+        self.interval_ms = self.INTERVAL_MS
+
+    def _lines(self):
+        with open(self.path) as f:
+            return f.read().split("\n")[:-1]  # complete lines only
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-            return
-        # nvidia-smi's start-up (driver and NVML initialisation) must not overlap the timed
-        # region: wait for its first sample line before returning
-        t0 = time.time()
-        while time.time() - t0 < 5.0 and self.proc.poll() is None:
-            if os.path.getsize(self.path) > 0:
+        # the short interval first; should nvidia-smi refuse it, the next one
+        for interval in (self.INTERVAL_MS, 100):
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                     "-lms", str(interval)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
+                return
+            self.interval_ms = interval
+            # nvidia-smi's start-up (driver and NVML initialisation) must not overlap the timed
+            # region: wait for its first sample line before returning; the lines written so far
+            # precede the region and are left out
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None:
+                if os.path.getsize(self.path) > 0 and self._lines():
+                    break
+                time.sleep(0.005)
+            if self._lines() or self.proc.poll() is None:
                 break
-            time.sleep(0.02)
+        self.skip = len(self._lines())
 
     def stop(self):
         if self.proc is None:
@@ -115,25 +130,29 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        lines = self._lines()
+        os.unlink(self.path)
+        in_region = lines[self.skip:]
+        # a region shorter than the interval has no sample of its own: the one just before it
+        use = in_region if in_region else lines[-1:]
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1].split()[0]))
-                    smax.append(float(parts[2].split()[0]))
-                    power.append(float(parts[3].split()[0]))
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(n)
-        os.unlink(self.path)
+        for line in use:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+                power.append(float(parts[3].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+                "reasons": sorted(reasons), "samples": len(sm), "samples_in_region": bool(in_region),
+                "interval_ms": self.interval_ms, "power_w_max": max(power) if power else None}
 
 
 # ----------------------------------------------------------------------------- distributed

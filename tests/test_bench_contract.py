@@ -1,9 +1,11 @@
 """CPU checks of bench.py's reporting logic (no GPU): the roofline object carries the keys the
-benchmark line promises, its fraction is achieved / peak, and the HBM peak names its source
-(the measured figure when MEASURED_PEAKS.json is there, the fallback otherwise)."""
+benchmark line promises, its fraction is achieved / peak, the HBM peak names its source (the
+measured figure when MEASURED_PEAKS.json is there, the fallback otherwise), and the clock
+sampler reads samples taken inside the timed region (against an nvidia-smi stand-in)."""
 import json
 import os
 import sys
+import time
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
@@ -36,3 +38,41 @@ def test_roofline_object():
     assert r["hbm"]["peak"] == 6650.0 and r["hbm"]["peak_source"] == "fallback: test"
     # a Montgomery product takes two low-word and two high-word multiplies
     assert abs(r["peak"] * 1e12 - 1.0 / (2 / PEAKS["mul_lo_per_s"] + 2 / PEAKS["mul_hi_per_s"])) < 1.0
+
+
+def _fake_smi(tmp_path, reasons):
+    """An nvidia-smi stand-in that prints one sample line every 10 ms until it is stopped."""
+    script = tmp_path / "nvidia-smi"
+    line = "0, 1965 MHz, 1965 MHz, 350.00 W, 0x0, " + ", ".join(reasons)
+    script.write_text("#!" + sys.executable + "\n"
+                      "import sys, time\n"
+                      "while True:\n"
+                      f"    print({line!r}, flush=True)\n"
+                      "    time.sleep(0.01)\n")
+    script.chmod(0o755)
+    return str(tmp_path)
+
+
+def test_clock_sampler_reads_the_timed_region(tmp_path, monkeypatch):
+    idle = ["Not Active"] * 4
+    monkeypatch.setenv("PATH", _fake_smi(tmp_path, idle) + os.pathsep + os.environ["PATH"])
+    s = bench.ClockSampler(0)
+    s.start()
+    time.sleep(0.25)
+    c = s.stop()
+    assert c["samples_in_region"] and c["samples"] >= 5
+    assert c["sm_mhz"] == 1965.0 and c["sm_max_mhz"] == 1965.0 and c["reasons"] == []
+    # a region shorter than the interval keeps the sample just before it
+    s = bench.ClockSampler(0)
+    s.start()
+    c = s.stop()
+    assert c["samples"] >= 1 and c["sm_mhz"] == 1965.0
+
+
+def test_clock_sampler_reports_throttle_reasons(tmp_path, monkeypatch):
+    capped = ["Not Active", "Not Active", "Not Active", "Active"]
+    monkeypatch.setenv("PATH", _fake_smi(tmp_path, capped) + os.pathsep + os.environ["PATH"])
+    s = bench.ClockSampler(0)
+    s.start()
+    time.sleep(0.1)
+    assert s.stop()["reasons"] == ["sw_power_cap"]
