@@ -221,3 +221,20 @@ def test_verify_batch_device_matches_host(oracle, wl, ctx):
     assert all(h != 0 for h in host[3:])
     assert host[3] == OPENING and host[4] == OPENING
     assert dev == host
+
+
+@pytest.mark.parametrize("kw", [{"log_inv_rate": 3}, {"univariate_skips": 2}, {"security_bits": 100},
+                                {"rs_domain_initial_reduction": 3}, {"log_inv_rate": 2, "univariate_skips": 3}])
+def test_merkle_batches_under_other_settings(wl, oracle, kw):
+    """The Merkle checks hash a round's queries as batches of permutations (sixteen per vector,
+    ragged last batch): honest proofs under other rates, skips, security levels and domain
+    reductions are accepted alone and in a batch, and a changed word of the last path is an
+    opening failure."""
+    log_n = 10
+    s = wl.AirSettings(**kw)
+    consts, _, proof = honest(oracle, log_n, s.as_array())
+    assert wl.verify(consts, log_n, proof, s) == OK
+    bad = proof.copy()
+    bad[-3] = (int(bad[-3]) + 1) % P
+    assert wl.verify(consts, log_n, bad, s) == OPENING
+    assert wl.verify_batch(consts, [(log_n, proof), (log_n, bad), (log_n, proof)], s, threads=2) == [OK, OPENING, OK]
